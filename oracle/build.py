@@ -1,0 +1,40 @@
+"""ORACLE -- test infrastructure only. Builds the oracle libraries.
+
+* oracle/_build/libkmeans_oracle.so from oracle/kmeans_oracle.c (always);
+* oracle/_ref/libkmeans_daal_ref.so from the reference tree via
+  oracle/ref/Makefile, when that tree is present (it is absent on GPU hosts,
+  which use the prebuilt library that travels with the working tree).
+"""
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATED_LIB = os.path.join(HERE, "_build", "libkmeans_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libkmeans_daal_ref.so")
+REFERENCE_TREE = os.environ.get("ONEDAL_REFERENCE_TREE", "/root/reference")
+
+
+def build_restated(force: bool = False) -> str:
+    src = os.path.join(HERE, "kmeans_oracle.c")
+    if force or not os.path.exists(RESTATED_LIB) or os.path.getmtime(RESTATED_LIB) < os.path.getmtime(src):
+        os.makedirs(os.path.dirname(RESTATED_LIB), exist_ok=True)
+        subprocess.check_call(["gcc", "-O2", "-fopenmp", "-fPIC", "-shared", "-std=c11",
+                               "-o", RESTATED_LIB, src])
+    return RESTATED_LIB
+
+
+def build_reference() -> str | None:
+    if not os.path.isdir(os.path.join(REFERENCE_TREE, "cpp", "daal")):
+        return REF_LIB if os.path.exists(REF_LIB) else None
+    subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "ref"), f"REF={REFERENCE_TREE}",
+                           f"-j{os.cpu_count() or 4}"])
+    return REF_LIB
+
+
+def build_all() -> None:
+    build_restated()
+    build_reference()
+
+
+if __name__ == "__main__":
+    build_all()

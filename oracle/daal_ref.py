@@ -1,0 +1,98 @@
+"""ORACLE -- test infrastructure only. ctypes binding of the reference's own DAAL
+k-means Lloyd kernel (KMeansBatchKernel<lloydDense, F, avx2>,
+cpp/daal/src/algorithms/kmeans/kmeans_lloyd_batch_impl.i:48-242), compiled from
+the reference sources by oracle/ref/Makefile into oracle/_ref/.
+
+It is called exactly as the oneAPI CPU backend calls it
+(cpp/oneapi/dal/algo/kmeans/backend/cpu/train_kernel_lloyd.cpp:71-144 for
+train, backend/cpu/infer_kernel.cpp:52-116 for infer). Threading comes from a
+std::thread shim with DAAL's static split, so FP32 results depend only on the
+thread count passed here.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_lib = None
+
+# services::ErrorKMeansNumberOfClustersIsTooLarge, from DAAL's error-id enum
+# (cpp/daal/include/services/error_indexes.h); reported through status_code.
+
+
+class ReferenceUnavailable(RuntimeError):
+    pass
+
+
+class ReferenceError_(RuntimeError):
+    def __init__(self, code):
+        super().__init__(f"DAAL kernel returned error id {code}")
+        self.code = code
+
+
+def available() -> bool:
+    return os.path.exists(_build.REF_LIB)
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise ReferenceUnavailable(f"{_build.REF_LIB} is not built (make -C oracle/ref)")
+        _lib = ctypes.CDLL(_build.REF_LIB)
+        P, I64, D = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double
+        for sfx in ("f64", "f32"):
+            getattr(_lib, f"daalref_train_{sfx}").argtypes = [P, I64, I64, P, I64, I64, D, P, P, P, P, P]
+            getattr(_lib, f"daalref_infer_{sfx}").argtypes = [P, I64, I64, P, I64, ctypes.c_int, P, P, P]
+        _lib.daalref_set_threads.argtypes = [ctypes.c_int]
+    return _lib
+
+
+def set_threads(t: int) -> int:
+    return _load().daalref_set_threads(int(t))
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _sfx(dtype):
+    return {np.dtype(np.float64): "f64", np.dtype(np.float32): "f32"}[np.dtype(dtype)]
+
+
+def train(X, C0, max_iteration_count=100, accuracy_threshold=0.0):
+    """Returns (centroids, responses int32, objective, iteration_count)."""
+    lib = _load()
+    X = np.ascontiguousarray(X)
+    C0 = np.ascontiguousarray(C0, dtype=X.dtype)
+    n, d = X.shape
+    k = C0.shape[0]
+    C = np.empty_like(C0)
+    lab = np.empty(n, np.int32)
+    obj = np.zeros(1, X.dtype)
+    it = np.zeros(1, np.int64)
+    code = np.zeros(1, np.int32)
+    rc = getattr(lib, f"daalref_train_{_sfx(X.dtype)}")(_p(X), n, d, _p(C0), k, int(max_iteration_count),
+                                                         float(accuracy_threshold), _p(C), _p(lab), _p(obj), _p(it),
+                                                         _p(code))
+    if rc != 0:
+        raise ReferenceError_(int(code[0]))
+    return C, lab, float(obj[0]), int(it[0])
+
+
+def infer(X, C, compute_objective=True):
+    """Returns (responses int32, objective or None)."""
+    lib = _load()
+    X = np.ascontiguousarray(X)
+    C = np.ascontiguousarray(C, dtype=X.dtype)
+    n, d = X.shape
+    lab = np.empty(n, np.int32)
+    obj = np.zeros(1, X.dtype)
+    code = np.zeros(1, np.int32)
+    rc = getattr(lib, f"daalref_infer_{_sfx(X.dtype)}")(_p(X), n, d, _p(C), C.shape[0],
+                                                         int(bool(compute_objective)), _p(lab), _p(obj), _p(code))
+    if rc != 0:
+        raise ReferenceError_(int(code[0]))
+    return lab, (float(obj[0]) if compute_objective else None)

@@ -1,0 +1,148 @@
+"""ORACLE -- test infrastructure only. ctypes binding of the plain-C restatement
+of oneDAL's dense k-means Lloyd kernel (oracle/kmeans_oracle.c).
+
+The algorithm follows cpp/daal/src/algorithms/kmeans/kmeans_lloyd_batch_impl.i:48-242
+(loop, merge, reseed, convergence), kmeans_lloyd_impl.i:54-496 (scoring, sums,
+candidates) and kmeans_lloyd_postprocessing.h:64-183 (final responses, exact
+objective); the C file cites each step.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_lib = None
+
+OK, EINVAL, ENOMEM, ETOO_MANY_EMPTY = 0, 1, 2, 3
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+class TooManyEmptyClusters(OracleError):
+    """DAAL's ErrorKMeansNumberOfClustersIsTooLarge (kmeans_lloyd_batch_impl.i:171)."""
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        path = _build.RESTATED_LIB
+        if not os.path.exists(path):
+            path = _build.build_restated()
+        _lib = ctypes.CDLL(path)
+        P, I64, D = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double
+        for sfx in ("f64", "f32"):
+            getattr(_lib, f"kmo_train_{sfx}").argtypes = [P, I64, I64, P, I64, I64, D, P, P, P, P]
+            getattr(_lib, f"kmo_infer_{sfx}").argtypes = [P, I64, I64, P, I64, ctypes.c_int, P, P]
+            getattr(_lib, f"kmo_step_{sfx}").argtypes = [P, I64, I64, P, I64, P, P, P, P, P]
+            getattr(_lib, f"kmo_assign_{sfx}").argtypes = [P, I64, I64, P, I64, P, P, P]
+            getattr(_lib, f"kmo_objective_{sfx}").argtypes = [P, I64, I64, P, I64, P]
+        _lib.kmo_objective_f64.restype = ctypes.c_double
+        _lib.kmo_objective_f32.restype = ctypes.c_float
+        _lib.kmo_assign_f32_in_f64.argtypes = [P, I64, I64, P, I64, P, P, P]
+    return _lib
+
+
+def _sfx(dtype):
+    dtype = np.dtype(dtype)
+    if dtype == np.float64:
+        return "f64"
+    if dtype == np.float32:
+        return "f32"
+    raise TypeError(f"oracle supports float32/float64, got {dtype}")
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _check(rc):
+    if rc == ETOO_MANY_EMPTY:
+        raise TooManyEmptyClusters("number of clusters is too large (candidates ran out)")
+    if rc != OK:
+        raise OracleError(f"oracle error {rc}")
+
+
+def train(X, C0, max_iteration_count=100, accuracy_threshold=0.0):
+    """Returns (centroids, responses int32, objective, iteration_count)."""
+    lib = _load()
+    X = np.ascontiguousarray(X)
+    C0 = np.ascontiguousarray(C0, dtype=X.dtype)
+    n, d = X.shape
+    k = C0.shape[0]
+    C = np.empty_like(C0)
+    lab = np.empty(n, np.int32)
+    obj = np.zeros(1, X.dtype)
+    it = np.zeros(1, np.int64)
+    sfx = _sfx(X.dtype)
+    _check(getattr(lib, f"kmo_train_{sfx}")(_p(X), n, d, _p(C0), k, int(max_iteration_count),
+                                            float(accuracy_threshold), _p(C), _p(lab), _p(obj), _p(it)))
+    return C, lab, float(obj[0]), int(it[0])
+
+
+def infer(X, C, compute_objective=True):
+    """Returns (responses int32, objective or None)."""
+    lib = _load()
+    X = np.ascontiguousarray(X)
+    C = np.ascontiguousarray(C, dtype=X.dtype)
+    n, d = X.shape
+    lab = np.empty(n, np.int32)
+    obj = np.zeros(1, X.dtype)
+    _check(getattr(lib, f"kmo_infer_{_sfx(X.dtype)}")(_p(X), n, d, _p(C), C.shape[0], int(bool(compute_objective)),
+                                                      _p(lab), _p(obj)))
+    return lab, (float(obj[0]) if compute_objective else None)
+
+
+def step(X, C_in):
+    """One Lloyd update from C_in. Returns (C_out, labels under C_in, shift, n_empty, goal)."""
+    lib = _load()
+    X = np.ascontiguousarray(X)
+    C_in = np.ascontiguousarray(C_in, dtype=X.dtype)
+    n, d = X.shape
+    k = C_in.shape[0]
+    C = np.empty_like(C_in)
+    lab = np.empty(n, np.int32)
+    shift = np.zeros(1, X.dtype)
+    ne = np.zeros(1, np.int64)
+    goal = np.zeros(1, X.dtype)
+    _check(getattr(lib, f"kmo_step_{_sfx(X.dtype)}")(_p(X), n, d, _p(C_in), k, _p(C), _p(lab), _p(shift), _p(ne),
+                                                     _p(goal)))
+    return C, lab, float(shift[0]), int(ne[0]), float(goal[0])
+
+
+def assign(X, C):
+    """Labels plus best / second-best score (0.5||c||^2 - x.c) per row, in X's precision."""
+    lib = _load()
+    X = np.ascontiguousarray(X)
+    C = np.ascontiguousarray(C, dtype=X.dtype)
+    n, d = X.shape
+    lab = np.empty(n, np.int32)
+    best = np.empty(n, X.dtype)
+    second = np.empty(n, X.dtype)
+    _check(getattr(lib, f"kmo_assign_{_sfx(X.dtype)}")(_p(X), n, d, _p(C), C.shape[0], _p(lab), _p(best), _p(second)))
+    return lab, best, second
+
+
+def assign_f32_in_f64(X, C):
+    """The FP64 oracle's labels / best / second scores for float32 inputs."""
+    lib = _load()
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    C = np.ascontiguousarray(C, dtype=np.float32)
+    n, d = X.shape
+    lab = np.empty(n, np.int32)
+    best = np.empty(n, np.float64)
+    second = np.empty(n, np.float64)
+    _check(lib.kmo_assign_f32_in_f64(_p(X), n, d, _p(C), C.shape[0], _p(lab), _p(best), _p(second)))
+    return lab, best, second
+
+
+def objective(X, C, labels):
+    lib = _load()
+    X = np.ascontiguousarray(X)
+    C = np.ascontiguousarray(C, dtype=X.dtype)
+    labels = np.ascontiguousarray(labels, dtype=np.int32)
+    n, d = X.shape
+    return float(getattr(lib, f"kmo_objective_{_sfx(X.dtype)}")(_p(X), n, d, _p(C), C.shape[0], _p(labels)))

@@ -1,0 +1,145 @@
+"""Generates the golden fixtures in tests/golden/ from the reference project.
+
+Run in a container where the reference tree is mounted:
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+Sources (paths inside the reference project):
+
+* gold.json -- the "train/infer on gold data" known-answer test:
+  cpp/oneapi/dal/algo/kmeans/test/data.hpp:26-184 (100x3 data, k=3 initial and
+  expected centroids, expected responses, objective 241.3593613), exercised by
+  cpp/oneapi/dal/algo/kmeans/test/fixture.hpp:156-203 (100 iterations, eps 0,
+  centroid/objective rel tol 1e-7, responses exact up to centroid matching).
+* empty_clusters.json -- "kmeans empty clusters test",
+  cpp/oneapi/dal/algo/kmeans/test/fixture.hpp:205-219 (1 iteration).
+* smoke_infer.json -- the infer half of the smoke test,
+  cpp/oneapi/dal/algo/kmeans/test/fixture.hpp:221-252 (objective 4).
+* example_dense.npz -- the k-means example's data and initial centroids
+  (data/kmeans_dense_train_data.csv, data/kmeans_dense_train_centroids.csv, used
+  by examples/oneapi/cpp/source/kmeans/kmeans_lloyd_dense_batch.cpp with k=20,
+  5 iterations, eps 0.001) plus the outputs of the reference DAAL kernel built
+  from source (oracle/_ref) on it, in float64 and float32.
+* daal_ref_c1.npz -- outputs of the reference kernel on a reduced seeded
+  Gaussian-blob workload shaped like the plain CPU configuration (d=20, k=20,
+  init = first k rows, eps 0), float64 and float32, so the restated oracle can
+  be re-checked where the reference tree is absent.
+"""
+import argparse
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+
+def _numbers(text):
+    return [float(v) for v in re.findall(r"-?\d+\.?\d*(?:[eE][-+]?\d+)?", text)]
+
+
+def _array_after(src, anchor, start=0):
+    """Numbers inside the first {...} initializer following `anchor`."""
+    i = src.index(anchor, start)
+    j = src.index("{", src.index("=", i))
+    k = src.index("}", j)
+    body = re.sub(r"//[^\n]*", "", src[j + 1:k])
+    return _numbers(body), k
+
+
+def gold(ref):
+    src = open(os.path.join(ref, "cpp/oneapi/dal/algo/kmeans/test/data.hpp")).read()
+    data, _ = _array_after(src, "get_data()")
+    init, _ = _array_after(src, "get_initial_centroids()")
+    expc, _ = _array_after(src, "get_expected_centroids()")
+    resp, _ = _array_after(src, "get_expected_responses()")
+    m = re.search(r"get_expected_objective\(\)\s*{\s*return\s*([0-9.eE+-]+)", src)
+    obj = float(m.group(1))
+    assert len(data) == 300 and len(init) == 9 and len(expc) == 9 and len(resp) == 100
+    return {
+        "source": "cpp/oneapi/dal/algo/kmeans/test/data.hpp:26-184; fixture.hpp:156-203",
+        "row_count": 100, "column_count": 3, "cluster_count": 3,
+        "max_iteration_count": 100, "accuracy_threshold": 0.0,
+        "data": data, "initial_centroids": init, "expected_centroids": expc,
+        "expected_responses": [int(v) for v in resp], "expected_objective": obj,
+        "rel_tol": 1e-7,
+    }
+
+
+def empty_clusters(ref):
+    src = open(os.path.join(ref, "cpp/oneapi/dal/algo/kmeans/test/fixture.hpp")).read()
+    s = src.index("void check_empty_clusters()")
+    data, p = _array_after(src, "data[]", s)
+    init, p = _array_after(src, "initial_centroids[]", p)
+    fin, p = _array_after(src, "final_centroids[]", p)
+    resp, p = _array_after(src, "responses[]", p)
+    return {
+        "source": "cpp/oneapi/dal/algo/kmeans/test/fixture.hpp:205-219",
+        "row_count": 10, "column_count": 1, "cluster_count": 3,
+        "max_iteration_count": 1, "accuracy_threshold": 0.0,
+        "data": data, "initial_centroids": init, "expected_centroids": fin,
+        "expected_responses": [int(v) for v in resp],
+    }
+
+
+def smoke_infer(ref):
+    src = open(os.path.join(ref, "cpp/oneapi/dal/algo/kmeans/test/fixture.hpp")).read()
+    s = src.index("void check_on_smoke_data()")
+    data, p = _array_after(src, "data[]", s)
+    fin, p = _array_after(src, "final_centroids[]", p)
+    resp, p = _array_after(src, "responses[]", p)
+    m = re.search(r"expected_obj_function\s*=\s*([0-9.]+)", src[s:])
+    return {
+        "source": "cpp/oneapi/dal/algo/kmeans/test/fixture.hpp:221-252 (infer half)",
+        "row_count": 8, "column_count": 2, "cluster_count": 2,
+        "data": data, "centroids": fin, "expected_responses": [int(v) for v in resp],
+        "expected_objective": float(m.group(1)), "rel_tol": 1e-5,
+    }
+
+
+def blobs_c1(n, seed):
+    """Seeded mixture of 20 isotropic Gaussian blobs (std 1) in d=20, centres U[-10,10]."""
+    rng = np.random.default_rng(seed)
+    k, d = 20, 20
+    centres = rng.uniform(-10, 10, size=(k, d))
+    lab = rng.integers(0, k, size=n)
+    return centres[lab] + rng.standard_normal((n, d))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    ref = args.reference
+
+    for name, fn in (("gold.json", gold), ("empty_clusters.json", empty_clusters), ("smoke_infer.json", smoke_infer)):
+        with open(os.path.join(HERE, name), "w") as f:
+            json.dump(fn(ref), f, indent=1)
+
+    from oracle import build, daal_ref
+    build.build_reference()
+    daal_ref.set_threads(1)
+
+    X = np.loadtxt(os.path.join(ref, "data/kmeans_dense_train_data.csv"), delimiter=",", dtype=np.float64)
+    C0 = np.loadtxt(os.path.join(ref, "data/kmeans_dense_train_centroids.csv"), delimiter=",", dtype=np.float64)
+    out = {"X": X, "C0": C0}
+    for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+        C, lab, obj, it = daal_ref.train(X.astype(dt), C0.astype(dt), 5, 0.001)
+        out.update({f"C_{tag}": C, f"labels_{tag}": lab, f"obj_{tag}": obj, f"iters_{tag}": it})
+    np.savez_compressed(os.path.join(HERE, "example_dense.npz"), **out)
+
+    X = blobs_c1(20000, 1001)
+    out = {"seed": 1001, "n": 20000}
+    for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+        Xd = X.astype(dt)
+        C, lab, obj, it = daal_ref.train(Xd, Xd[:20].copy(), 50, 0.0)
+        out.update({f"C_{tag}": C, f"labels_{tag}": lab.astype(np.uint8), f"obj_{tag}": obj, f"iters_{tag}": it})
+    np.savez_compressed(os.path.join(HERE, "daal_ref_c1.npz"), **out)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
