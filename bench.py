@@ -1,0 +1,328 @@
+"""Benchmark: k-means Lloyd iterations/s on the precision workload
+(n=20,000,000, d=128, k=1024, float32 input), one B200 per rank.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form bf16x3|plain] [--impl b200|reference]
+
+A step is one Lloyd iteration (assignment + centroid update) over all rows,
+inputs resident in HBM (10.24 GB of rows, far larger than the 126 MB L2, so no
+L2 flush is needed between steps). `value` = whole-job iterations/s timed with
+CUDA events on the launching stream between barriers, max over ranks. `e2e` is
+the same metric through the public API (kmeans.train on pinned host buffers:
+host->device copy of the rows, the K iterations, the final responses/objective
+pass and the device->host copy of centroids and responses inside the timed
+region). `roofline` is for the dominant kernel (the assignment), its per-launch
+duration measured with CUDA events recorded by the library on its stream.
+`cpu_baseline` is the reference's own DAAL kernel (oracle/_ref) on the host cores.
+
+With --impl reference, rank 0 times the reference DAAL kernel on the host cores
+(a bounded row sample of the same workload, scaled to the full row count) and
+prints the same metric; other ranks exit.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Lloyd iter/s n=20M,d=128,k=1024 BF16-TC vs FP32 plain; p50/p99 infer latency"
+UNIT = "iter/s"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_iters_per_s(X_host, C0_host, n_full, iters, threads):
+    """Reference DAAL kernel on a row sample: per-iteration time from a train with
+    `iters` iterations minus an infer pass (the train's final responses+objective)."""
+    from oracle import daal_ref
+    daal_ref.set_threads(threads)
+    t0 = time.perf_counter()
+    daal_ref.infer(X_host, C0_host, True)
+    t_inf = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    _, _, _, it = daal_ref.train(X_host, C0_host, iters, 0.0)
+    t_tr = time.perf_counter() - t0
+    per_iter = max(t_tr - t_inf, 1e-9) / max(it, 1)
+    scale = n_full / X_host.shape[0]
+    return 1.0 / (per_iter * scale), per_iter, it
+
+
+def make_workload(device, n=None):
+    import torch
+    from onedal_b200 import workloads
+    X, C0 = workloads.make(workloads.PRECISION, device, n=n)
+    torch.cuda.synchronize()
+    return X, C0
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+    from onedal_b200 import workloads
+    w = workloads.PRECISION
+    n_sample = args.cpu_sample_rows
+    X, C0 = workloads.make(w, "cpu", n=n_sample)
+    Xh = X.numpy()
+    Ch = C0.numpy()
+    threads = os.cpu_count() or 1
+    from oracle import daal_ref
+    if not daal_ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference kernel library oracle/_ref not built"}))
+        return
+    daal_ref.set_threads(threads)
+    # warm-up: W single iterations
+    for _ in range(args.warmup):
+        daal_ref.train(Xh, Ch, 1, 0.0)
+    v, per_iter, it = cpu_reference_iters_per_s(Xh, Ch, w.n, args.steps, threads)
+    sample = f"{n_sample} of {w.n} rows (same generator), {it} iterations, scaled by rows"
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_iter * (w.n / n_sample) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "precision n=20000000 d=128 k=1024 float32, 10% bisector near-ties",
+                   "n": w.n, "d": w.d, "k": w.k, "form": "DAAL lloydDense float (OpenBLAS sgemm)"},
+        "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_b200(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from onedal_b200 import _native, kmeans, workloads
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    w = workloads.PRECISION
+    form = _native.KMB_FORM_BF16X3 if args.form == "bf16x3" else _native.KMB_FORM_PLAIN
+
+    X, C0 = make_workload("cuda")
+    n, d = X.shape
+    k = C0.shape[0]
+    ctx = _native.context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    labels = torch.empty(n, dtype=torch.int32, device="cuda")
+    C = C0.clone()
+
+    def iterate(T, Cbuf):
+        p = _native.kmb_params(k, T, 0.0, form, 0)
+        it = ctypes.c_int64()
+        st = _native.kmb_stats()
+        ctx.check(ctx.lib.kmb_lloyd_iterate(ctx.handle, _native.KMB_F32, X.data_ptr(), n, d, Cbuf.data_ptr(),
+                                            ctypes.byref(p), labels.data_ptr(), ctypes.byref(it), ctypes.byref(st)))
+        return it.value, st
+
+    # warm-up
+    iterate(args.warmup, C)
+    torch.cuda.synchronize()
+    C.copy_(C0)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ctx.check(ctx.lib.kmb_context_set_kernel_timing(ctx.handle, 1))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    iters_done, st = iterate(args.steps, C)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    kernel_id = 1 if form == _native.KMB_FORM_BF16X3 else 0
+    kt = ctypes.c_double()
+    kl = ctypes.c_int64()
+    ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, kernel_id, ctypes.byref(kt), ctypes.byref(kl)))
+    ut = ctypes.c_double()
+    ul = ctypes.c_int64()
+    ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 2, ctypes.byref(ut), ctypes.byref(ul)))
+    ctx.check(ctx.lib.kmb_context_set_kernel_timing(ctx.handle, 0))
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = iters_done / (ms / 1e3)
+
+    # Plain-form comparison (the north-star ratio) on the same data, when timing the BF16 form.
+    plain_value = None
+    if form == _native.KMB_FORM_BF16X3 and args.plain_steps > 0:
+        C.copy_(C0)
+        e0.record(stream)
+        p = _native.kmb_params(k, args.plain_steps, 0.0, _native.KMB_FORM_PLAIN, 0)
+        it = ctypes.c_int64()
+        ctx.check(ctx.lib.kmb_lloyd_iterate(ctx.handle, _native.KMB_F32, X.data_ptr(), n, d, C.data_ptr(),
+                                            ctypes.byref(p), labels.data_ptr(), ctypes.byref(it), None))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain_value = it.value / (e0.elapsed_time(e1) / 1e3)
+
+    # Roofline of the dominant kernel.
+    peaks, peak_src = load_peaks()
+    flops_per_launch = 2.0 * n * k * d
+    avg_kernel_s = (kt.value / max(kl.value, 1)) / 1e3
+    achieved_tflops = flops_per_launch / avg_kernel_s / 1e12 if kl.value else None
+    if form == _native.KMB_FORM_BF16X3:
+        peak = peaks["bf16_tflops_sustained"]
+        peak_note = f"bf16 dense sustained ({peak_src})"
+    else:
+        # FP32 FFMA issue peak: 148 SMs x 128 lanes x 2 flop x max SM clock (no measured figure exists).
+        peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+        peak_note = "fp32 FFMA issue peak at max SM clock (148x128x2xclock)"
+    roofline = {"bound": "tensor" if form == _native.KMB_FORM_BF16X3 else "fp32_fma", "achieved": achieved_tflops,
+                "peak": peak, "unit": "TFLOP/s", "frac": (achieved_tflops / peak) if achieved_tflops else None,
+                "traffic": args.traffic_bytes, "peak_source": peak_note,
+                "kernel_ms_avg": avg_kernel_s * 1e3, "kernel_launches": kl.value,
+                "update_ms_avg": (ut.value / max(ul.value, 1)), "algorithmic_flops_per_launch": flops_per_launch,
+                "algorithmic_bytes_per_launch": n * d * 4 + 4 * n}
+
+    # e2e through the public API with pinned host buffers.
+    e2e = None
+    if rank == 0 and args.e2e:
+        Xh = torch.empty((n, d), dtype=torch.float32, pin_memory=True)
+        Xh.copy_(X)
+        C0h = C0.cpu().numpy()
+        Xn = Xh.numpy()
+        desc = kmeans.descriptor(np.float32).set_cluster_count(k).set_max_iteration_count(args.steps) \
+            .set_compute_form(form)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = kmeans.train(desc, Xn, C0h)
+        t1 = time.perf_counter()
+        T = max(r.get_iteration_count(), 1)
+        e2e = {"value": T / (t1 - t0), "unit": UNIT, "h2d_bytes_per_step": (n * d * 4 + k * d * 4) // T,
+               "d2h_bytes_per_step": (n * 4 + k * d * 4 + 8) // T,
+               "note": "one kmeans.train call on pinned host rows: H2D, iterations, final responses + objective, D2H"}
+        del Xh
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_sample_rows > 0:
+        from oracle import daal_ref
+        if daal_ref.available():
+            ns = args.cpu_sample_rows
+            Xs = X[:ns].cpu().numpy()
+            v, per_iter, it = cpu_reference_iters_per_s(Xs, C0.cpu().numpy(), n, 2, os.cpu_count() or 1)
+            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"first {ns} of {n} rows, {it} Lloyd iterations of the reference DAAL kernel "
+                             f"(OpenBLAS sgemm, std::thread shim), per-iteration time scaled by rows"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value * (world if False else 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / max(iters_done, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "precision n=20000000 d=128 k=1024 float32, 1024 blobs std 1 in U[-5,5]^128, "
+                                   "10% bisector near-ties", "n": n, "d": d, "k": k,
+                       "form": args.form, "iterations_completed": iters_done,
+                       "l2": "inputs (10.24 GB) larger than L2; no flush"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": None, "clocks": clocks,
+            "plain_fp32_value": plain_value,
+            "bf16_over_plain": (value / plain_value) if plain_value else None,
+            "recheck_rows_last_iteration": st.rechecked_rows,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--form", default="plain", choices=["bf16x3", "plain"])
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample-rows", type=int, default=200_000)
+    ap.add_argument("--traffic-bytes", type=float, default=None)
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,168 @@
+/*
+ * onedal_b200_kmeans.h -- C ABI of the B200-native k-means Lloyd (dense) path.
+ *
+ * This library is the compute engine behind oneDAL's unchanged
+ *   oneapi::dal::train(kmeans::descriptor<F, method::lloyd_dense>, data[, init])
+ *   oneapi::dal::infer(kmeans::descriptor<F, method::lloyd_dense>, model, data)
+ * for F in {float, double}. In the reference those calls end in the
+ * host-policy dispatcher specialisations
+ *   kmeans::detail::v1::train_ops_dispatcher<host_policy, F, lloyd_dense, clustering>
+ *     (declared cpp/oneapi/dal/algo/kmeans/detail/train_ops.hpp:25-30,
+ *      defined   cpp/oneapi/dal/algo/kmeans/detail/train_ops.cpp:24-42)
+ *   kmeans::detail::v1::infer_ops_dispatcher<host_policy, F, lloyd_dense, clustering>
+ *     (declared cpp/oneapi/dal/algo/kmeans/detail/infer_ops.hpp:25-30,
+ *      defined   cpp/oneapi/dal/algo/kmeans/detail/infer_ops.cpp:26-43)
+ * which run DAAL's KMeansBatchKernel<lloydDense, F, cpu>
+ * (cpp/daal/src/algorithms/kmeans/kmeans_lloyd_batch_impl.i:48-242).
+ * A replacement dispatcher calls kmb_train / kmb_infer below; INTEGRATION.md
+ * shows that binding. All entry points are synchronous with respect to the
+ * host unless stated otherwise, take plain pointers and sizes, and return a
+ * kmb_status. Matrices are dense row-major (rows x columns).
+ */
+#ifndef ONEDAL_B200_KMEANS_H
+#define ONEDAL_B200_KMEANS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define KMB_API __attribute__((visibility("default")))
+#else
+#define KMB_API
+#endif
+
+/* Status codes. The dispatcher maps them onto the reference's exception types
+ * (cpp/oneapi/dal/backend/interop/error_converter.cpp:136-254):
+ * KMB_EINVAL -> invalid_argument / domain_error, KMB_ENOMEM -> bad_alloc,
+ * KMB_ETOO_MANY_EMPTY -> domain_error (DAAL ErrorKMeansNumberOfClustersIsTooLarge,
+ * kmeans_lloyd_batch_impl.i:171), others -> internal_error. */
+typedef enum kmb_status {
+    KMB_OK = 0,
+    KMB_EINVAL = 1,
+    KMB_ENOMEM = 2,
+    KMB_ECUDA = 3,
+    KMB_ETIMEDOUT = 4,
+    KMB_ETOO_MANY_EMPTY = 5,
+    KMB_EUNSUPPORTED = 6
+} kmb_status;
+
+/* Element type of data and centroids: the descriptor's float_t. */
+typedef enum kmb_dtype { KMB_F32 = 0, KMB_F64 = 1 } kmb_dtype;
+
+/* Where the caller's buffers live. */
+typedef enum kmb_memory { KMB_MEM_HOST = 0, KMB_MEM_DEVICE = 1 } kmb_memory;
+
+/* How the x.c contraction is computed.
+ * KMB_FORM_PLAIN : the drop-in. F-precision FMA (FP32 or FP64) distance with a
+ *                  fused per-row argmin; lowest index wins ties.
+ * KMB_FORM_BF16X3: FP32 data only. Split-BF16 (hi+lo, three products) tcgen05
+ *                  tensor-core contraction with FP32 accumulation in TMEM; every
+ *                  row whose top-2 gap is inside the derived error bound is
+ *                  rechecked exactly in FP64, so responses equal the FP64
+ *                  oracle's. */
+typedef enum kmb_form { KMB_FORM_PLAIN = 0, KMB_FORM_BF16X3 = 1 } kmb_form;
+
+typedef struct kmb_context kmb_context;
+
+/* Lloyd parameters: the descriptor fields of
+ * cpp/oneapi/dal/algo/kmeans/common.hpp:175-240 (defaults common.cpp:36-42). */
+typedef struct kmb_params {
+    int64_t cluster_count;       /* k > 0                                   */
+    int64_t max_iteration_count; /* >= 0                                    */
+    double accuracy_threshold;   /* >= 0; stop when sum ||c_old-c_new||^2 <= it */
+    int32_t form;                /* kmb_form                                */
+    int32_t recheck;             /* PLAIN form: 1 = FP64 recheck of near-ties */
+} kmb_params;
+
+/* Per-call diagnostics (optional output of the train/infer calls). */
+typedef struct kmb_stats {
+    int64_t rechecked_rows;   /* rows re-scored in FP64 in the last assignment  */
+    int64_t changed_by_recheck;
+    int64_t empty_cluster_events; /* clusters reseeded over the whole train  */
+    double last_shift;        /* sum ||c_old - c_new||^2 of the last update     */
+} kmb_stats;
+
+/* Context: one CUDA device, one stream, a workspace that grows on demand.
+ * A context is not thread-safe; use one per host thread. */
+KMB_API int kmb_context_create(int device, kmb_context **out);
+KMB_API int kmb_context_destroy(kmb_context *ctx);
+/* Use the caller's cudaStream_t (passed as void*) instead of the context's own. */
+KMB_API int kmb_context_set_stream(kmb_context *ctx, void *cuda_stream);
+KMB_API const char *kmb_context_last_error(const kmb_context *ctx);
+KMB_API const char *kmb_status_string(int status);
+/* Frees the cached workspace. */
+KMB_API int kmb_context_release_workspace(kmb_context *ctx);
+
+/* Train: replaces train_ops_dispatcher<host_policy, F, lloyd_dense, clustering>
+ * (cpp/oneapi/dal/algo/kmeans/detail/train_ops.cpp:24-42 ->
+ *  backend/cpu/train_kernel_lloyd.cpp:84-144).
+ * X: n x d, C0: k x d initial centroids (required; k-means++ init is not on
+ * this path). Outputs: C_out k x d, responses n (int32, against the final
+ * centroids), objective = exact sum ||x - c_label||^2 (FP64 accumulation),
+ * iteration_count. Pointers are host or device memory per `memory`.
+ * stats may be NULL. */
+KMB_API int kmb_train(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, const void *C0,
+                      const kmb_params *params, void *C_out, int32_t *responses, double *objective,
+                      int64_t *iteration_count, kmb_stats *stats);
+
+/* Infer: replaces infer_ops_dispatcher<host_policy, F, lloyd_dense, clustering>
+ * (cpp/oneapi/dal/algo/kmeans/detail/infer_ops.cpp:26-43 ->
+ *  backend/cpu/infer_kernel.cpp:52-116). responses against C (k x d);
+ * objective only when compute_objective != 0 (may be NULL otherwise). */
+KMB_API int kmb_infer(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, const void *C,
+                      int64_t k, int32_t form, int32_t compute_objective, int32_t *responses, double *objective,
+                      kmb_stats *stats);
+
+/* One Lloyd update from C_in, device memory only (lock-step parity checks and
+ * the sharded multi-GPU driver): labels under C_in, C_out, the centroid shift
+ * and the number of empty clusters reseeded. Mirrors one pass of the loop body
+ * kmeans_lloyd_batch_impl.i:117-212. */
+KMB_API int kmb_lloyd_step(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, const void *C_in,
+                           int64_t k, int32_t form, int32_t recheck, void *C_out, int32_t *labels, double *shift,
+                           int64_t *n_empty);
+
+/* Partial statistics for row-sharded (SPMD) training, device memory only:
+ * labels of this shard's rows under C (k x d), FP64 per-cluster sums
+ * sums (k x d), counts (k, int64) and the shard's sum of squared distances.
+ * The caller all-reduces sums/counts across shards, then calls
+ * kmb_finalize_centroids. The reference's SPMD path performs the same
+ * exchange (cpp/oneapi/dal/algo/kmeans/backend/gpu/cluster_updater.hpp:117-153). */
+KMB_API int kmb_partial_sums(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, const void *C,
+                             int64_t k, int32_t form, int32_t *labels, double *sums, int64_t *counts,
+                             double *sq_distances, float *row_sq_distance);
+
+/* Centroids from all-reduced sums/counts (device memory): c_j = sums_j / counts_j
+ * rounded to F; clusters with count 0 keep C_in and are listed (ascending) in
+ * empty_ids (k int32, device) with *n_empty set; shift = sum over non-empty
+ * clusters of ||c_old - c_new||^2. */
+KMB_API int kmb_finalize_centroids(kmb_context *ctx, int dtype, const double *sums, const int64_t *counts,
+                                   const void *C_in, int64_t k, int64_t d, void *C_out, double *shift,
+                                   int32_t *empty_ids, int64_t *n_empty);
+
+/* Lloyd iterations only, in place, device memory: C (k x d) holds the initial
+ * centroids on entry and the updated ones on return; labels (n) receive the
+ * assignment of the last completed update. Runs up to max_iteration_count
+ * updates, stopping early on the accuracy threshold exactly as kmb_train's
+ * loop (kmeans_lloyd_batch_impl.i:117-213), without the final responses /
+ * objective pass. Used by the benchmark and the serving loop's small trains. */
+KMB_API int kmb_lloyd_iterate(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, void *C,
+                              const kmb_params *params, int32_t *labels, int64_t *iteration_count, kmb_stats *stats);
+
+/* Kernel timing: when enabled, CUDA events are recorded on the launching
+ * stream around every launch of the dominant assignment kernel; the totals are
+ * read (synchronising) with kmb_context_kernel_time and cleared by enabling
+ * again. kernel: 0 = plain assignment, 1 = tensor-core assignment, 2 = update. */
+KMB_API int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled);
+KMB_API int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int64_t *launches);
+
+/* Library version string. */
+KMB_API const char *kmb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ONEDAL_B200_KMEANS_H */

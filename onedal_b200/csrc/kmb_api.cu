@@ -1,0 +1,599 @@
+// C ABI of the B200 k-means Lloyd path: context, workspace and the host driver
+// of the Lloyd loop (declared in include/onedal_b200_kmeans.h).
+//
+// Host driver semantics follow DAAL's KMeansBatchKernel::compute
+// (cpp/daal/src/algorithms/kmeans/kmeans_lloyd_batch_impl.i:48-242):
+//   for it < T: assign under C, update (sums, reseed, shift), stop if shift <= eps
+//   then responses against the final centroids + exact objective.
+// The whole loop is enqueued on one stream; a device-side LoopState carries the
+// convergence flag so later iterations become no-ops, and the host only reads
+// it back every few iterations.
+#include "kmb_internal.cuh"
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+struct kmb_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    kmb::Workspace ws;
+    std::string last_error;
+    kmb::LoopState *h_state = nullptr;  // pinned mirror of the device states
+    // kernel timing (kmb_context_set_kernel_timing)
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used[3];
+
+    cudaEvent_t take_event() {
+        if (!ev_pool.empty()) {
+            cudaEvent_t e = ev_pool.back();
+            ev_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void recycle_events() {
+        for (auto &v : ev_used) {
+            for (auto &pr : v) {
+                ev_pool.push_back(pr.first);
+                ev_pool.push_back(pr.second);
+            }
+            v.clear();
+        }
+    }
+};
+
+// RAII: records a start/stop event pair around one kernel launch when timing is on.
+struct KernelTimer {
+    kmb_context *ctx;
+    int which;
+    cudaEvent_t a = nullptr, b = nullptr;
+    KernelTimer(kmb_context *c, int w) : ctx(c), which(w) {
+        if (ctx->timing) {
+            a = ctx->take_event();
+            b = ctx->take_event();
+            cudaEventRecord(a, ctx->stream);
+        }
+    }
+    ~KernelTimer() {
+        if (ctx->timing) {
+            cudaEventRecord(b, ctx->stream);
+            ctx->ev_used[which].emplace_back(a, b);
+        }
+    }
+};
+
+namespace kmb {
+
+bool Workspace::ensure(DevBuf &b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return true;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    // round up to 2 MiB to limit reallocations
+    const size_t rounded = (bytes + (size_t(2) << 20) - 1) / (size_t(2) << 20) * (size_t(2) << 20);
+    if (cudaMalloc(&b.ptr, rounded) != cudaSuccess) {
+        cudaGetLastError();
+        b.ptr = nullptr;
+        return false;
+    }
+    b.bytes = rounded;
+    return true;
+}
+
+void Workspace::release() {
+    DevBuf *all[] = {&X, &C0, &Cout, &labels, &d2, &xnorm, &Ccur, &Cnew, &Ct, &h, &queue, &H, &Gs,
+                     &counts, &offsets, &piece_base, &perm, &records, &shift_part, &empty_flag, &empty_ids,
+                     &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo};
+    for (DevBuf *b : all) {
+        if (b->ptr) cudaFree(b->ptr);
+        b->ptr = nullptr;
+        b->bytes = 0;
+    }
+}
+
+}  // namespace kmb
+
+namespace {
+
+using kmb::LoopState;
+using kmb::RecheckEntry;
+
+int fail(kmb_context *ctx, int status, const char *fmt, ...) {
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return status;
+}
+
+int cuda_fail(kmb_context *ctx, cudaError_t e, const char *where) {
+    return fail(ctx, KMB_ECUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+#define KMB_CUDA(call)                                                    \
+    do {                                                                  \
+        cudaError_t e_ = (call);                                          \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);          \
+    } while (0)
+
+constexpr int64_t kBN = 128;  // cluster tile of the plain kernel
+constexpr int64_t kBK = 8;
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// Buffers shared by train/infer/step. Returns KMB_OK or KMB_ENOMEM.
+template <typename F>
+int ensure_common(kmb_context *ctx, int64_t n, int64_t d, int64_t k, bool recheck) {
+    kmb::Workspace &ws = ctx->ws;
+    const int64_t kpad = round_up(k, kBN), dpad = round_up(d, kBK);
+    bool ok = true;
+    ok &= ws.ensure(ws.labels, sizeof(int32_t) * n);
+    ok &= ws.ensure(ws.d2, sizeof(F) * n);
+    ok &= ws.ensure(ws.xnorm, sizeof(F) * n);
+    ok &= ws.ensure(ws.Ccur, sizeof(F) * k * d);
+    ok &= ws.ensure(ws.Cnew, sizeof(F) * k * d);
+    ok &= ws.ensure(ws.Ct, sizeof(F) * kpad * dpad);
+    ok &= ws.ensure(ws.h, sizeof(F) * kpad);
+    ok &= ws.ensure(ws.scalars, sizeof(kmb::DevScalars));
+    ok &= ws.ensure(ws.state, sizeof(LoopState) * 2);
+    if (recheck) ok &= ws.ensure(ws.queue, sizeof(RecheckEntry) * n);
+    if (!ok) return fail(ctx, KMB_ENOMEM, "device allocation failed (n=%lld d=%lld k=%lld)", (long long)n,
+                         (long long)d, (long long)k);
+    return KMB_OK;
+}
+
+__global__ void reset_iteration_kernel(LoopState *st) {
+    if (st->done) return;
+    st->n_recheck = 0;
+    st->n_changed = 0;
+}
+
+__global__ void account_recheck_kernel(LoopState *st) {
+    if (st->done) return;
+    st->rechecked_total += st->n_recheck;
+}
+
+// One assignment pass of the plain form (+ optional FP64 recheck) under C.
+template <typename F>
+void assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, int64_t k, bool recheck,
+                 int32_t *labels, F *d2, LoopState *st) {
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    const int64_t kpad = round_up(k, kBN);
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    reset_iteration_kernel<<<1, 1, 0, s>>>(st);
+    kmb::launch_prep_centroids<F>(C, k, d, kpad, (F *)ws.Ct.ptr, (F *)ws.h.ptr, &sc->cnorm_max, st, s);
+    {
+        KernelTimer timer(ctx, 0);
+        kmb::launch_assign_plain<F>(X, n, d, (const F *)ws.Ct.ptr, (const F *)ws.h.ptr, k, kpad,
+                                    (const F *)ws.xnorm.ptr, &sc->cnorm_max, labels, d2,
+                                    recheck ? (RecheckEntry *)ws.queue.ptr : nullptr, st, s);
+    }
+    if (recheck) {
+        kmb::launch_recheck<F>(X, n, d, C, k, (const RecheckEntry *)ws.queue.ptr, labels, d2,
+                               (const F *)ws.xnorm.ptr, st, s);
+        account_recheck_kernel<<<1, 1, 0, s>>>(st);
+    }
+}
+
+template <typename F>
+int upload(kmb_context *ctx, kmb::DevBuf &buf, const void *src, size_t bytes, const F **out) {
+    if (!ctx->ws.ensure(buf, bytes)) return fail(ctx, KMB_ENOMEM, "device allocation of %zu bytes failed", bytes);
+    KMB_CUDA(cudaMemcpyAsync(buf.ptr, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    *out = (const F *)buf.ptr;
+    return KMB_OK;
+}
+
+int check_form(kmb_context *ctx, int dtype, int form) {
+    if (form != KMB_FORM_PLAIN && form != KMB_FORM_BF16X3) return fail(ctx, KMB_EINVAL, "unknown form %d", form);
+    if (form == KMB_FORM_BF16X3 && dtype != KMB_F32)
+        return fail(ctx, KMB_EINVAL, "the BF16x3 tensor-core form takes float32 data");
+    return KMB_OK;
+}
+
+void init_state(LoopState &h, double eps) {
+    std::memset(&h, 0, sizeof(h));
+    h.eps = eps;
+}
+
+// The Lloyd loop on device-resident X and centroids C (updated in place).
+// The host peeks at the device convergence flag every few iterations.
+template <typename F>
+int run_loop(kmb_context *ctx, const F *X, int64_t n, int64_t d, F *C, const kmb_params *p,
+             const kmb::UpdatePlan &plan, int32_t *labels, bool recheck) {
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    const int64_t k = p->cluster_count;
+    F *Cnew = (F *)ws.Cnew.ptr;
+    F *d2 = (F *)ws.d2.ptr;
+    LoopState *st = (LoopState *)ws.state.ptr;
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    init_state(ctx->h_state[0], p->accuracy_threshold);
+    KMB_CUDA(cudaMemcpyAsync(st, ctx->h_state, sizeof(LoopState), cudaMemcpyHostToDevice, s));
+    KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
+    kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
+    const int64_t T = p->max_iteration_count;
+    int64_t enq = 0;
+    int64_t batch = 2;
+    while (enq < T) {
+        const int64_t upto = std::min(T, enq + batch);
+        for (; enq < upto; ++enq) {
+            assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, d2, st);
+            KernelTimer timer(ctx, 2);
+            kmb::launch_update<F>(X, plan, labels, d2, C, Cnew, ws, st, /*commit=*/true, s);
+        }
+        KMB_CUDA(cudaGetLastError());
+        if (enq < T) {
+            KMB_CUDA(cudaMemcpyAsync(ctx->h_state, st, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaStreamSynchronize(s));
+            if (ctx->h_state[0].done) break;
+            batch = std::min<int64_t>(batch * 2, 8);
+        }
+    }
+    return KMB_OK;
+}
+
+template <typename F>
+int iterate_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, void *Cv, const kmb_params *p,
+                 int32_t *labels, int64_t *iteration_count, kmb_stats *stats) {
+    const int64_t k = p->cluster_count;
+    if (p->form == KMB_FORM_BF16X3) return fail(ctx, KMB_EUNSUPPORTED, "BF16x3 form is not built in this library");
+    const bool recheck = p->recheck != 0;
+    int rc = ensure_common<F>(ctx, n, d, k, recheck);
+    if (rc) return rc;
+    kmb::UpdatePlan plan = kmb::make_update_plan(n, k, d);
+    if (!kmb::ensure_update_buffers(ctx->ws, plan, sizeof(F))) return fail(ctx, KMB_ENOMEM, "update buffers");
+    int32_t *lab = labels ? labels : (int32_t *)ctx->ws.labels.ptr;
+    if ((rc = run_loop<F>(ctx, (const F *)Xv, n, d, (F *)Cv, p, plan, lab, recheck))) return rc;
+    KMB_CUDA(cudaMemcpyAsync(ctx->h_state, ctx->ws.state.ptr, sizeof(LoopState), cudaMemcpyDeviceToHost, ctx->stream));
+    KMB_CUDA(cudaStreamSynchronize(ctx->stream));
+    const LoopState &hs = ctx->h_state[0];
+    if (hs.error) return fail(ctx, hs.error, "device loop failed (status %d)", hs.error);
+    if (iteration_count) *iteration_count = hs.iterations;
+    if (stats) {
+        stats->rechecked_rows = hs.rechecked_total;
+        stats->changed_by_recheck = hs.n_changed;
+        stats->empty_cluster_events = hs.empty_events;
+        stats->last_shift = hs.shift;
+    }
+    return KMB_OK;
+}
+
+template <typename F>
+int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t d, const void *C0v,
+               const kmb_params *p, void *C_out, int32_t *responses, double *objective, int64_t *iteration_count,
+               kmb_stats *stats) {
+    const int64_t k = p->cluster_count;
+    const bool tc = p->form == KMB_FORM_BF16X3;
+    if (tc) return fail(ctx, KMB_EUNSUPPORTED, "BF16x3 form is not built in this library");
+    const bool recheck = p->recheck != 0 || tc;
+    int rc = ensure_common<F>(ctx, n, d, k, recheck);
+    if (rc) return rc;
+    kmb::UpdatePlan plan = kmb::make_update_plan(n, k, d);
+    if (!kmb::ensure_update_buffers(ctx->ws, plan, sizeof(F))) return fail(ctx, KMB_ENOMEM, "update buffers");
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+
+    const F *X = (const F *)Xv;
+    const F *C0 = (const F *)C0v;
+    if (memory == KMB_MEM_HOST) {
+        if ((rc = upload<F>(ctx, ws.X, Xv, sizeof(F) * n * d, &X))) return rc;
+        if ((rc = upload<F>(ctx, ws.C0, C0v, sizeof(F) * k * d, &C0))) return rc;
+    }
+    int32_t *labels = (memory == KMB_MEM_DEVICE && responses) ? responses : (int32_t *)ws.labels.ptr;
+    F *Ccur = (F *)ws.Ccur.ptr;
+    F *d2 = (F *)ws.d2.ptr;
+    LoopState *st = (LoopState *)ws.state.ptr;
+    LoopState *st_final = st + 1;
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+
+    init_state(ctx->h_state[1], 0.0);
+    KMB_CUDA(cudaMemcpyAsync(st + 1, &ctx->h_state[1], sizeof(LoopState), cudaMemcpyHostToDevice, s));
+    KMB_CUDA(cudaMemcpyAsync(Ccur, C0, sizeof(F) * k * d, cudaMemcpyDeviceToDevice, s));
+    if ((rc = run_loop<F>(ctx, X, n, d, Ccur, p, plan, labels, recheck))) return rc;
+    // Responses against the final centroids, then the exact objective.
+    assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, d2, st_final);
+    double *obj_dev = &sc->objective;
+    kmb::launch_objective<F>(X, n, d, Ccur, labels, (double *)ws.obj_part.ptr, obj_dev, s);
+    KMB_CUDA(cudaGetLastError());
+
+    const cudaMemcpyKind out_kind = memory == KMB_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (C_out) KMB_CUDA(cudaMemcpyAsync(C_out, Ccur, sizeof(F) * k * d, out_kind, s));
+    if (responses && labels != responses)
+        KMB_CUDA(cudaMemcpyAsync(responses, labels, sizeof(int32_t) * n, out_kind, s));
+    double obj_h = 0.0;
+    KMB_CUDA(cudaMemcpyAsync(&obj_h, obj_dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaMemcpyAsync(ctx->h_state, st, sizeof(LoopState) * 2, cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaStreamSynchronize(s));
+    const LoopState &hs = ctx->h_state[0];
+    if (hs.error) return fail(ctx, hs.error, "device loop failed (status %d)", hs.error);
+    if (objective) *objective = obj_h;
+    if (iteration_count) *iteration_count = hs.iterations;
+    if (stats) {
+        stats->rechecked_rows = ctx->h_state[1].n_recheck;
+        stats->changed_by_recheck = ctx->h_state[1].n_changed;
+        stats->empty_cluster_events = hs.empty_events;
+        stats->last_shift = hs.shift;
+    }
+    return KMB_OK;
+}
+
+template <typename F>
+int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t d, const void *Cv, int64_t k,
+               int32_t form, int32_t compute_objective, int32_t *responses, double *objective, kmb_stats *stats) {
+    const bool tc = form == KMB_FORM_BF16X3;
+    if (tc) return fail(ctx, KMB_EUNSUPPORTED, "BF16x3 form is not built in this library");
+    const bool recheck = tc;
+    int rc = ensure_common<F>(ctx, n, d, k, recheck);
+    if (rc) return rc;
+    if (!ctx->ws.ensure(ctx->ws.obj_part, sizeof(double) * 148 * 8)) return fail(ctx, KMB_ENOMEM, "objective");
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    const F *X = (const F *)Xv;
+    const F *C = (const F *)Cv;
+    if (memory == KMB_MEM_HOST) {
+        if ((rc = upload<F>(ctx, ws.X, Xv, sizeof(F) * n * d, &X))) return rc;
+        if ((rc = upload<F>(ctx, ws.C0, Cv, sizeof(F) * k * d, &C))) return rc;
+    }
+    int32_t *labels = (memory == KMB_MEM_DEVICE && responses) ? responses : (int32_t *)ws.labels.ptr;
+    LoopState *st = (LoopState *)ws.state.ptr + 1;
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    init_state(ctx->h_state[1], 0.0);
+    KMB_CUDA(cudaMemcpyAsync(st, &ctx->h_state[1], sizeof(LoopState), cudaMemcpyHostToDevice, s));
+    KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
+    kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
+    assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, (F *)ws.d2.ptr, st);
+    if (compute_objective)
+        kmb::launch_objective<F>(X, n, d, C, labels, (double *)ws.obj_part.ptr, &sc->objective, s);
+    KMB_CUDA(cudaGetLastError());
+    const cudaMemcpyKind out_kind = memory == KMB_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (responses && labels != responses)
+        KMB_CUDA(cudaMemcpyAsync(responses, labels, sizeof(int32_t) * n, out_kind, s));
+    double obj_h = 0.0;
+    KMB_CUDA(cudaMemcpyAsync(&obj_h, &sc->objective, sizeof(double), cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaMemcpyAsync(&ctx->h_state[1], st, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaStreamSynchronize(s));
+    if (compute_objective && objective) *objective = obj_h;
+    if (stats) {
+        stats->rechecked_rows = ctx->h_state[1].n_recheck;
+        stats->changed_by_recheck = ctx->h_state[1].n_changed;
+        stats->empty_cluster_events = 0;
+        stats->last_shift = 0.0;
+    }
+    return KMB_OK;
+}
+
+template <typename F>
+int step_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, const void *Cin, int64_t k, int32_t form,
+              int32_t recheck_flag, void *C_out, int32_t *labels, double *shift, int64_t *n_empty) {
+    const bool tc = form == KMB_FORM_BF16X3;
+    if (tc) return fail(ctx, KMB_EUNSUPPORTED, "BF16x3 form is not built in this library");
+    const bool recheck = recheck_flag != 0 || tc;
+    int rc = ensure_common<F>(ctx, n, d, k, recheck);
+    if (rc) return rc;
+    kmb::UpdatePlan plan = kmb::make_update_plan(n, k, d);
+    if (!kmb::ensure_update_buffers(ctx->ws, plan, sizeof(F))) return fail(ctx, KMB_ENOMEM, "update buffers");
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    const F *X = (const F *)Xv;
+    F *Ccur = (F *)ws.Ccur.ptr;
+    LoopState *st = (LoopState *)ws.state.ptr;
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    init_state(ctx->h_state[0], 0.0);
+    KMB_CUDA(cudaMemcpyAsync(st, ctx->h_state, sizeof(LoopState), cudaMemcpyHostToDevice, s));
+    KMB_CUDA(cudaMemcpyAsync(Ccur, Cin, sizeof(F) * k * d, cudaMemcpyDeviceToDevice, s));
+    KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
+    kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
+    assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, (F *)ws.d2.ptr, st);
+    kmb::launch_update<F>(X, plan, labels, (const F *)ws.d2.ptr, Ccur, (F *)C_out, ws, st, /*commit=*/false, s);
+    KMB_CUDA(cudaGetLastError());
+    KMB_CUDA(cudaMemcpyAsync(ctx->h_state, st, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaStreamSynchronize(s));
+    if (ctx->h_state[0].error) return fail(ctx, ctx->h_state[0].error, "device step failed");
+    if (shift) *shift = ctx->h_state[0].shift;
+    if (n_empty) *n_empty = ctx->h_state[0].n_empty;
+    return KMB_OK;
+}
+
+int validate_shapes(kmb_context *ctx, int dtype, int64_t n, int64_t d, int64_t k) {
+    if (!ctx) return KMB_EINVAL;
+    if (dtype != KMB_F32 && dtype != KMB_F64) return fail(ctx, KMB_EINVAL, "unknown dtype %d", dtype);
+    if (n <= 0) return fail(ctx, KMB_EINVAL, "input data is empty");
+    if (n > INT32_MAX) return fail(ctx, KMB_EINVAL, "row count exceeds INT32_MAX");
+    if (d <= 0) return fail(ctx, KMB_EINVAL, "column count must be positive");
+    if (k <= 0 || k > INT32_MAX) return fail(ctx, KMB_EINVAL, "cluster count must be in (0, INT32_MAX]");
+    if (k > n) return fail(ctx, KMB_EINVAL, "cluster count exceeds data row count");
+    return KMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *kmb_version(void) { return "onedal_b200 kmeans 0.1 (sm_100a)"; }
+
+const char *kmb_status_string(int status) {
+    switch (status) {
+        case KMB_OK: return "ok";
+        case KMB_EINVAL: return "invalid argument";
+        case KMB_ENOMEM: return "out of device memory";
+        case KMB_ECUDA: return "CUDA error";
+        case KMB_ETIMEDOUT: return "timed out";
+        case KMB_ETOO_MANY_EMPTY: return "number of clusters is too large (too many empty clusters)";
+        case KMB_EUNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+int kmb_context_create(int device, kmb_context **out) {
+    if (!out) return KMB_EINVAL;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return KMB_ECUDA;
+    }
+    kmb_context *ctx = new (std::nothrow) kmb_context;
+    if (!ctx) return KMB_ENOMEM;
+    ctx->device = device;
+    ctx->ws.device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_state, sizeof(LoopState) * 2) != cudaSuccess) {
+        cudaGetLastError();
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return KMB_ECUDA;
+    }
+    ctx->own_stream = true;
+    *out = ctx;
+    return KMB_OK;
+}
+
+int kmb_context_destroy(kmb_context *ctx) {
+    if (!ctx) return KMB_EINVAL;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->ws.release();
+    ctx->recycle_events();
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->h_state) cudaFreeHost(ctx->h_state);
+    delete ctx;
+    return KMB_OK;
+}
+
+int kmb_context_set_stream(kmb_context *ctx, void *cuda_stream) {
+    if (!ctx) return KMB_EINVAL;
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    ctx->stream = (cudaStream_t)cuda_stream;
+    ctx->own_stream = false;
+    return KMB_OK;
+}
+
+const char *kmb_context_last_error(const kmb_context *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int kmb_context_release_workspace(kmb_context *ctx) {
+    if (!ctx) return KMB_EINVAL;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->ws.release();
+    return KMB_OK;
+}
+
+int kmb_train(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, const void *C0,
+              const kmb_params *params, void *C_out, int32_t *responses, double *objective, int64_t *iteration_count,
+              kmb_stats *stats) {
+    if (!ctx || !params) return KMB_EINVAL;
+    ctx->last_error.clear();
+    int rc = validate_shapes(ctx, dtype, n, d, params->cluster_count);
+    if (rc) return rc;
+    if (params->max_iteration_count < 0) return fail(ctx, KMB_EINVAL, "max_iteration_count must be >= 0");
+    if (!(params->accuracy_threshold >= 0.0)) return fail(ctx, KMB_EINVAL, "accuracy_threshold must be >= 0");
+    if ((rc = check_form(ctx, dtype, params->form))) return rc;
+    if (!X || !C0) return fail(ctx, KMB_EINVAL, "data and initial centroids are required");
+    if (memory != KMB_MEM_HOST && memory != KMB_MEM_DEVICE) return fail(ctx, KMB_EINVAL, "unknown memory kind");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    if (dtype == KMB_F32)
+        return train_impl<float>(ctx, memory, X, n, d, C0, params, C_out, responses, objective, iteration_count, stats);
+    return train_impl<double>(ctx, memory, X, n, d, C0, params, C_out, responses, objective, iteration_count, stats);
+}
+
+int kmb_infer(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, const void *C, int64_t k,
+              int32_t form, int32_t compute_objective, int32_t *responses, double *objective, kmb_stats *stats) {
+    if (!ctx) return KMB_EINVAL;
+    ctx->last_error.clear();
+    if (dtype != KMB_F32 && dtype != KMB_F64) return fail(ctx, KMB_EINVAL, "unknown dtype %d", dtype);
+    if (n <= 0) return fail(ctx, KMB_EINVAL, "input data is empty");
+    if (n > INT32_MAX) return fail(ctx, KMB_EINVAL, "row count exceeds INT32_MAX");
+    if (d <= 0 || k <= 0 || k > INT32_MAX) return fail(ctx, KMB_EINVAL, "bad centroid shape");
+    int rc = check_form(ctx, dtype, form);
+    if (rc) return rc;
+    if (!X || !C) return fail(ctx, KMB_EINVAL, "data and centroids are required");
+    if (memory != KMB_MEM_HOST && memory != KMB_MEM_DEVICE) return fail(ctx, KMB_EINVAL, "unknown memory kind");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    if (dtype == KMB_F32)
+        return infer_impl<float>(ctx, memory, X, n, d, C, k, form, compute_objective, responses, objective, stats);
+    return infer_impl<double>(ctx, memory, X, n, d, C, k, form, compute_objective, responses, objective, stats);
+}
+
+int kmb_lloyd_step(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, const void *C_in, int64_t k,
+                   int32_t form, int32_t recheck, void *C_out, int32_t *labels, double *shift, int64_t *n_empty) {
+    if (!ctx) return KMB_EINVAL;
+    ctx->last_error.clear();
+    int rc = validate_shapes(ctx, dtype, n, d, k);
+    if (rc) return rc;
+    if ((rc = check_form(ctx, dtype, form))) return rc;
+    if (!X || !C_in || !C_out || !labels) return fail(ctx, KMB_EINVAL, "null device pointer");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    if (dtype == KMB_F32) return step_impl<float>(ctx, X, n, d, C_in, k, form, recheck, C_out, labels, shift, n_empty);
+    return step_impl<double>(ctx, X, n, d, C_in, k, form, recheck, C_out, labels, shift, n_empty);
+}
+
+int kmb_lloyd_iterate(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, void *C,
+                      const kmb_params *params, int32_t *labels, int64_t *iteration_count, kmb_stats *stats) {
+    if (!ctx || !params) return KMB_EINVAL;
+    ctx->last_error.clear();
+    int rc = validate_shapes(ctx, dtype, n, d, params->cluster_count);
+    if (rc) return rc;
+    if (params->max_iteration_count < 0) return fail(ctx, KMB_EINVAL, "max_iteration_count must be >= 0");
+    if (!(params->accuracy_threshold >= 0.0)) return fail(ctx, KMB_EINVAL, "accuracy_threshold must be >= 0");
+    if ((rc = check_form(ctx, dtype, params->form))) return rc;
+    if (!X || !C) return fail(ctx, KMB_EINVAL, "null device pointer");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    if (dtype == KMB_F32) return iterate_impl<float>(ctx, X, n, d, C, params, labels, iteration_count, stats);
+    return iterate_impl<double>(ctx, X, n, d, C, params, labels, iteration_count, stats);
+}
+
+int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled) {
+    if (!ctx) return KMB_EINVAL;
+    cudaStreamSynchronize(ctx->stream);
+    ctx->recycle_events();
+    ctx->timing = enabled != 0;
+    return KMB_OK;
+}
+
+int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int64_t *launches) {
+    if (!ctx || kernel < 0 || kernel > 2) return KMB_EINVAL;
+    double tot = 0.0;
+    for (auto &pr : ctx->ev_used[kernel]) {
+        if (cudaEventSynchronize(pr.second) != cudaSuccess) return cuda_fail(ctx, cudaGetLastError(), "event");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, pr.first, pr.second);
+        tot += ms;
+    }
+    if (total_ms) *total_ms = tot;
+    if (launches) *launches = (int64_t)ctx->ev_used[kernel].size();
+    return KMB_OK;
+}
+
+int kmb_partial_sums(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, const void *C, int64_t k,
+                     int32_t form, int32_t *labels, double *sums, int64_t *counts, double *sq_distances,
+                     float *row_sq_distance) {
+    (void)ctx; (void)dtype; (void)X; (void)n; (void)d; (void)C; (void)k; (void)form; (void)labels; (void)sums;
+    (void)counts; (void)sq_distances; (void)row_sq_distance;
+    return KMB_EUNSUPPORTED;
+}
+
+int kmb_finalize_centroids(kmb_context *ctx, int dtype, const double *sums, const int64_t *counts, const void *C_in,
+                           int64_t k, int64_t d, void *C_out, double *shift, int32_t *empty_ids, int64_t *n_empty) {
+    (void)ctx; (void)dtype; (void)sums; (void)counts; (void)C_in; (void)k; (void)d; (void)C_out; (void)shift;
+    (void)empty_ids; (void)n_empty;
+    return KMB_EUNSUPPORTED;
+}
+
+}  // extern "C"

@@ -1,0 +1,351 @@
+// Plain-form assignment: fused x.c contraction + per-row argmin (FP32 / FP64 FMA).
+//
+// Replaces, for every row block, DAAL's
+//   buf = clSq - X_b * C^T  (xxgemm, α = -1, β = 1) followed by a strict-'<'
+//   argmin scan over clusters
+// (cpp/daal/src/algorithms/kmeans/kmeans_lloyd_impl.i:174-216 in the update loop and
+//  cpp/daal/src/algorithms/kmeans/kmeans_lloyd_postprocessing.h:95-130 for the final
+//  responses). The n x k score matrix is never materialised: each CTA owns a
+// 128-row tile, streams 128-cluster tiles of C^T through shared memory and keeps
+// a running (best, index, second, index2, third) per row in registers.
+//
+// Scores are h_j - x.c_j with h_j = 0.5 ||c_j||^2 (the DAAL form); ties resolve to
+// the lowest cluster index. Rows whose best/second gap lies inside the derived
+// rounding bound are queued for an FP64 recheck when a queue is given.
+#include "kmb_internal.cuh"
+
+#include <float.h>
+
+namespace kmb {
+namespace {
+
+constexpr int BM = 128;  // rows per CTA
+constexpr int BN = 128;  // clusters per N-tile
+constexpr int BK = 8;    // contraction chunk
+constexpr int NT = 256;  // threads
+constexpr int PAD = 4;   // smem row padding (keeps 16-byte alignment, breaks bank conflicts)
+
+template <typename F> struct Vec4;
+template <> struct Vec4<float> { using T = float4; };
+template <> struct Vec4<double> { using T = double4; };
+
+template <typename F> __device__ __forceinline__ F f_inf();
+template <> __device__ __forceinline__ float f_inf<float>() { return __int_as_float(0x7f800000); }
+template <> __device__ __forceinline__ double f_inf<double>() { return __longlong_as_double(0x7ff0000000000000LL); }
+
+template <typename F> __device__ __forceinline__ double unit_roundoff();
+template <> __device__ __forceinline__ double unit_roundoff<float>() { return 5.9604644775390625e-8; }   // 2^-24
+template <> __device__ __forceinline__ double unit_roundoff<double>() { return 1.1102230246251565e-16; } // 2^-53
+
+// (value, index) lexicographic "less".
+template <typename F>
+__device__ __forceinline__ bool lex_less(F a, int ia, F b, int ib) {
+    return a < b || (a == b && ia < ib);
+}
+
+template <typename F>
+struct RowTop {
+    F b, s, t;   // best, second, third score
+    int ib, is;  // best / second cluster index
+};
+
+template <typename F>
+__device__ __forceinline__ void top_push(RowTop<F> &r, F v, int c) {
+    // Columns arrive in increasing order within a thread, so strict '<' keeps
+    // the lowest index on ties.
+    if (v < r.b) {
+        r.t = r.s;
+        r.s = r.b;
+        r.is = r.ib;
+        r.b = v;
+        r.ib = c;
+    } else if (v < r.s) {
+        r.t = r.s;
+        r.s = v;
+        r.is = c;
+    } else if (v < r.t) {
+        r.t = v;
+    }
+}
+
+template <typename F>
+__device__ __forceinline__ RowTop<F> top_merge(const RowTop<F> &x, const RowTop<F> &y) {
+    // Merge two sorted triples ((value, index) order); indices are kept for the
+    // first two places only. After o outputs a + b == o <= 2, so a, b < 3.
+    const F xv[3] = {x.b, x.s, x.t}, yv[3] = {y.b, y.s, y.t};
+    const int xi[3] = {x.ib, x.is, 0x7fffffff}, yi[3] = {y.ib, y.is, 0x7fffffff};
+    F ov[3];
+    int oi[3];
+    int a = 0, b = 0;
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {
+        if (lex_less(xv[a], xi[a], yv[b], yi[b])) {
+            ov[o] = xv[a];
+            oi[o] = xi[a];
+            ++a;
+        } else {
+            ov[o] = yv[b];
+            oi[o] = yi[b];
+            ++b;
+        }
+    }
+    RowTop<F> r;
+    r.b = ov[0];
+    r.ib = oi[0];
+    r.s = ov[1];
+    r.is = oi[1];
+    r.t = ov[2];
+    return r;
+}
+
+template <typename F>
+__device__ __forceinline__ RowTop<F> shfl_top(const RowTop<F> &x, int mask) {
+    RowTop<F> y;
+    y.b = __shfl_xor_sync(0xffffffffu, x.b, mask);
+    y.s = __shfl_xor_sync(0xffffffffu, x.s, mask);
+    y.t = __shfl_xor_sync(0xffffffffu, x.t, mask);
+    y.ib = __shfl_xor_sync(0xffffffffu, x.ib, mask);
+    y.is = __shfl_xor_sync(0xffffffffu, x.is, mask);
+    return y;
+}
+
+template <typename F, bool VEC>
+__global__ void __launch_bounds__(NT, 1)
+assign_plain_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restrict__ Ct, const F *__restrict__ h,
+                    int k, int kpad, const F *__restrict__ xnorm, const double *__restrict__ cnorm_max,
+                    int32_t *__restrict__ labels, F *__restrict__ d2, RecheckEntry *__restrict__ queue,
+                    LoopState *__restrict__ st) {
+    if (st && st->done) return;
+    using V4 = typename Vec4<F>::T;
+    __shared__ __align__(16) F Xs[2][BK][BM + PAD];
+    __shared__ __align__(16) F Cs[2][BK][BN + PAD];
+
+    const int tid = threadIdx.x;
+    const int ty = tid >> 4, tx = tid & 15;
+    const int64_t row0 = (int64_t)blockIdx.x * BM;
+
+    // Global-load mapping. X tile: 128 rows x 8 dims; thread -> row tid/2, dims (tid&1)*4..+3.
+    const int lr = tid >> 1, lk = (tid & 1) * 4;
+    const int64_t grow = row0 + lr;
+    const bool row_ok = grow < n;
+    const F *xrow = X + (row_ok ? grow : 0) * (int64_t)d;
+    // C tile: 8 dims x 128 clusters; thread -> dim tid/32, clusters (tid&31)*4..+3.
+    const int ck = tid >> 5, cn = (tid & 31) * 4;
+
+    const int nk = (d + BK - 1) / BK;
+    const int ntiles = kpad / BN;
+    const int steps = nk * ntiles;
+
+    F xr[4];
+    V4 cr;
+    auto gload = [&](int step) {
+        const int nt = step / nk, kc = step - nt * nk;
+        const int kb = kc * BK;
+        if (VEC) {
+            if (row_ok && kb + lk < d) {
+                V4 v = *reinterpret_cast<const V4 *>(xrow + kb + lk);
+                xr[0] = v.x; xr[1] = v.y; xr[2] = v.z; xr[3] = v.w;
+            } else {
+                xr[0] = xr[1] = xr[2] = xr[3] = F(0);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) xr[q] = (row_ok && kb + lk + q < d) ? xrow[kb + lk + q] : F(0);
+        }
+        // Ct has nk*BK rows (zero padded) and kpad columns.
+        cr = *reinterpret_cast<const V4 *>(Ct + (int64_t)(kb + ck) * kpad + nt * BN + cn);
+    };
+    auto sstore = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) Xs[buf][lk + q][lr] = xr[q];
+        *reinterpret_cast<V4 *>(&Cs[buf][ck][cn]) = cr;
+    };
+
+    RowTop<F> top[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        top[i].b = top[i].s = top[i].t = f_inf<F>();
+        top[i].ib = 0;
+        top[i].is = 0;
+    }
+    F acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = F(0);
+
+    gload(0);
+    sstore(0);
+    __syncthreads();
+
+    for (int step = 0; step < steps; ++step) {
+        const int buf = step & 1;
+        if (step + 1 < steps) gload(step + 1);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            F a[8], b[8];
+            V4 a0 = *reinterpret_cast<const V4 *>(&Xs[buf][kk][ty * 4]);
+            V4 a1 = *reinterpret_cast<const V4 *>(&Xs[buf][kk][64 + ty * 4]);
+            V4 b0 = *reinterpret_cast<const V4 *>(&Cs[buf][kk][tx * 4]);
+            V4 b1 = *reinterpret_cast<const V4 *>(&Cs[buf][kk][64 + tx * 4]);
+            a[0] = a0.x; a[1] = a0.y; a[2] = a0.z; a[3] = a0.w;
+            a[4] = a1.x; a[5] = a1.y; a[6] = a1.z; a[7] = a1.w;
+            b[0] = b0.x; b[1] = b0.y; b[2] = b0.z; b[3] = b0.w;
+            b[4] = b1.x; b[5] = b1.y; b[6] = b1.z; b[7] = b1.w;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        const int nt = step / nk;
+        if (step - nt * nk == nk - 1) {
+            // Epilogue of one N-tile: scores h_j - x.c_j into the running top-3.
+            const int cbase = nt * BN;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int col = cbase + (j < 4 ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+                const F hj = h[col];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    top_push(top[i], hj - acc[i][j], col);
+                    acc[i][j] = F(0);
+                }
+            }
+        }
+        if (step + 1 < steps) sstore(buf ^ 1);
+        __syncthreads();
+    }
+
+    // Reduce across the 16 lanes (tx) that share the same rows.
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+#pragma unroll
+        for (int m = 8; m >= 1; m >>= 1) top[i] = top_merge(top[i], shfl_top(top[i], m));
+    }
+    if (tx == 0) {
+        const double u = unit_roundoff<F>();
+        const double cmax = cnorm_max ? *cnorm_max : 0.0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int64_t r = row0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+            if (r >= n) continue;
+            const RowTop<F> &t = top[i];
+            labels[r] = t.ib;
+            const F xn = xnorm[r];
+            d2[r] = F(2) * t.b + xn;
+            if (queue) {
+                // |computed - exact| per score <= u*cmax^2 + (d+2)*u*||x||*cmax (+ slack);
+                // the order of two scores is certain when their gap exceeds twice that.
+                const double xl = sqrt(fmax((double)xn, 0.0));
+                const double e = 1.0625 * u * (cmax * cmax + (double)(d + 2) * xl * cmax);
+                const double band = 2.0 * e;
+                if ((double)t.s - (double)t.b <= band) {
+                    const int slot = atomicAdd(&st->n_recheck, 1);
+                    RecheckEntry q;
+                    q.row = (int)r;
+                    q.c1 = t.ib;
+                    q.c2 = t.is;
+                    q.full = ((double)t.t - (double)t.b <= band) ? 1 : 0;
+                    queue[slot] = q;
+                }
+            }
+        }
+    }
+}
+
+// Per-iteration centroid preparation: Ct (dpad x kpad, zero padded), h (kpad,
+// +inf padding), max ||c|| (double).
+template <typename F>
+__global__ void prep_centroids_kernel(const F *__restrict__ C, int k, int d, int dpad, int kpad, F *__restrict__ Ct,
+                                      F *__restrict__ h, double *__restrict__ cnorm_max, const LoopState *st) {
+    if (st && st->done) return;
+    __shared__ double red[32];
+    const int j = blockIdx.x;  // one block per (padded) cluster
+    double s = 0.0;
+    for (int t = threadIdx.x; t < dpad; t += blockDim.x) {
+        F v = (j < k && t < d) ? C[(int64_t)j * d + t] : F(0);
+        Ct[(int64_t)t * kpad + j] = v;
+        s += (double)v * (double)v;
+    }
+    for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+        h[j] = (j < k) ? F(0.5 * tot) : f_inf<F>();
+        if (j < k) {
+            // max of non-negative doubles via the ordered integer view
+            atomicMax(reinterpret_cast<unsigned long long *>(cnorm_max),
+                      (unsigned long long)__double_as_longlong(sqrt(tot)));
+        }
+    }
+}
+
+template <typename F>
+__global__ void row_norms_kernel(const F *__restrict__ X, int64_t n, int d, F *__restrict__ xnorm,
+                                 double *__restrict__ xnorm_max) {
+    // One warp per row.
+    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const F *x = X + row * d;
+    double s = 0.0;
+    for (int t = lane; t < d; t += 32) s += (double)x[t] * (double)x[t];
+    for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+    if (lane == 0) {
+        xnorm[row] = F(s);
+        if (xnorm_max) atomicMax(reinterpret_cast<unsigned long long *>(xnorm_max),
+                                 (unsigned long long)__double_as_longlong(sqrt(s)));
+    }
+}
+
+__global__ void reset_double_kernel(double *p, const LoopState *st) {
+    if (st && st->done) return;
+    *p = 0.0;
+}
+
+}  // namespace
+
+template <typename F>
+void launch_prep_centroids(const F *C, int64_t k, int64_t d, int64_t kpad, F *Ct, F *h, double *cnorm_max,
+                           const LoopState *st, cudaStream_t s) {
+    const int dpad = (int)((d + BK - 1) / BK * BK);
+    reset_double_kernel<<<1, 1, 0, s>>>(cnorm_max, st);
+    prep_centroids_kernel<F><<<(unsigned)kpad, 128, 0, s>>>(C, (int)k, (int)d, dpad, (int)kpad, Ct, h, cnorm_max, st);
+}
+
+template <typename F>
+void launch_row_norms(const F *X, int64_t n, int64_t d, F *xnorm, double *xnorm_max, cudaStream_t s) {
+    if (n == 0) return;
+    const int64_t blocks = (n * 32 + 255) / 256;
+    row_norms_kernel<F><<<(unsigned)blocks, 256, 0, s>>>(X, n, (int)d, xnorm, xnorm_max);
+}
+
+template <typename F>
+void launch_assign_plain(const F *X, int64_t n, int64_t d, const F *Ct, const F *h, int64_t k, int64_t kpad,
+                         const F *xnorm, const double *cnorm_max, int32_t *labels, F *d2, RecheckEntry *queue,
+                         LoopState *st, cudaStream_t s) {
+    if (n == 0) return;
+    const unsigned blocks = (unsigned)((n + BM - 1) / BM);
+    const bool vec = (d % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) % (4 * sizeof(F))) == 0);
+    if (vec)
+        assign_plain_kernel<F, true><<<blocks, NT, 0, s>>>(X, n, (int)d, Ct, h, (int)k, (int)kpad, xnorm, cnorm_max,
+                                                           labels, d2, queue, st);
+    else
+        assign_plain_kernel<F, false><<<blocks, NT, 0, s>>>(X, n, (int)d, Ct, h, (int)k, (int)kpad, xnorm, cnorm_max,
+                                                            labels, d2, queue, st);
+}
+
+#define KMB_INST(F)                                                                                                \
+    template void launch_prep_centroids<F>(const F *, int64_t, int64_t, int64_t, F *, F *, double *,            \
+                                           const LoopState *, cudaStream_t);                                     \
+    template void launch_row_norms<F>(const F *, int64_t, int64_t, F *, double *, cudaStream_t);                  \
+    template void launch_assign_plain<F>(const F *, int64_t, int64_t, const F *, const F *, int64_t, int64_t,    \
+                                         const F *, const double *, int32_t *, F *, RecheckEntry *, LoopState *, \
+                                         cudaStream_t);
+KMB_INST(float)
+KMB_INST(double)
+#undef KMB_INST
+
+}  // namespace kmb

@@ -1,0 +1,121 @@
+// Internal declarations shared by the k-means Lloyd kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/onedal_b200_kmeans.h"
+
+namespace kmb {
+
+// Device-resident loop state. Every per-iteration kernel reads `done` first and
+// returns at once when it is set, so the whole Lloyd loop is enqueued without a
+// host round trip per iteration (the reference's GPU loop synchronises on the
+// objective every iteration, cpp/oneapi/dal/algo/kmeans/backend/gpu/cluster_updater.hpp:135-136).
+struct LoopState {
+    int done;             // converged (shift <= eps) or failed
+    int error;            // kmb_status of a device-detected failure
+    int iterations;       // completed Lloyd updates
+    int n_empty;          // empty clusters in the current update
+    int n_recheck;        // rows queued for the FP64 recheck
+    int n_changed;        // rows whose label the recheck changed
+    long long empty_events;
+    long long rechecked_total;
+    double shift;         // sum ||c_old - c_new||^2 of the current update
+    double eps;
+};
+
+// Recheck queue entry written by the assignment kernels for near-tie rows.
+struct RecheckEntry {
+    int row;
+    int c1;    // approximate best cluster
+    int c2;    // approximate second-best cluster
+    int full;  // 1: more than two clusters lie inside the error band -> scan all k
+};
+
+// Per-call sizing of the update (counting sort + segmented FP64 sums).
+struct UpdatePlan {
+    int64_t n, k, d;
+    int64_t chunk_rows;   // rows per stable-scatter chunk
+    int64_t n_chunks;
+    int64_t piece_rows;   // rows per FP64 partial-sum piece
+    int64_t max_pieces;   // n / piece_rows + k (upper bound)
+};
+
+// Device scratch of one context. Buffers grow on demand and are reused across
+// calls; `bytes_*` track capacities.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct Workspace {
+    int device = 0;
+    DevBuf X, C0, Cout, labels, d2, xnorm, Ccur, Cnew, Ct, h, queue;
+    DevBuf H, Gs, counts, offsets, piece_base, perm, records, shift_part, empty_flag, empty_ids;
+    DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;
+    DevBuf Xhi, Xlo, Chi, Clo;
+    // Grows `b` to at least `bytes`; returns false on allocation failure.
+    bool ensure(DevBuf &b, size_t bytes);
+    void release();
+};
+
+// Scalars kept in device memory (one DevBuf "scalars").
+struct DevScalars {
+    double cnorm_max;
+    double xnorm_max;
+    double objective;
+    double pad;
+};
+
+// ---- assignment (plain FMA form) ------------------------------------------
+// Prepares per-iteration centroid data: transposed copy Ct (d x kpad), half
+// squared norms h (kpad, +inf padding) and max ||c|| for the error bound.
+template <typename F>
+void launch_prep_centroids(const F *C, int64_t k, int64_t d, int64_t kpad, F *Ct, F *h, double *cnorm_max,
+                           const LoopState *st, cudaStream_t s);
+
+// Row squared norms (once per call; X is constant across iterations).
+template <typename F>
+void launch_row_norms(const F *X, int64_t n, int64_t d, F *xnorm, double *xnorm_max, cudaStream_t s);
+
+// Fused distance + argmin over all clusters for every row.
+// Writes labels, d2 (squared distance to the winner, 2*best + ||x||^2, in F)
+// and, when `queue` is non-null, appends near-tie rows to the recheck queue.
+template <typename F>
+void launch_assign_plain(const F *X, int64_t n, int64_t d, const F *Ct, const F *h, int64_t k, int64_t kpad,
+                         const F *xnorm, const double *cnorm_max, int32_t *labels, F *d2, RecheckEntry *queue,
+                         LoopState *st, cudaStream_t s);
+
+// FP64 recheck of queued rows (exact expanded score in double, lowest index on ties).
+template <typename F>
+void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, const RecheckEntry *queue,
+                    int32_t *labels, F *d2, const F *xnorm, LoopState *st, cudaStream_t s);
+
+// ---- update ----------------------------------------------------------------
+UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d);
+// Sizes the update buffers of `ws` for plan `p` (false on allocation failure).
+bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize);
+
+// One Lloyd update: counting-sort the rows by label (stable, so each cluster's
+// rows are summed in row order), FP64 sums per fixed piece of rows, centroid =
+// sum / count rounded to F, empty clusters reseeded with the farthest rows,
+// centroid shift, convergence flag. C_old is overwritten by the new centroids
+// when `commit` (the loop path); otherwise they are left in C_new.
+template <typename F>
+void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *C_old, F *C_new,
+                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s);
+
+// Just the sums/counts half of the update (sharded training).
+template <typename F>
+void launch_partial_sums(const F *X, const UpdatePlan &p, const int32_t *labels, double *sums, int64_t *counts,
+                         Workspace &ws, cudaStream_t s);
+
+// Exact objective sum ||x - c_label||^2 in FP64, deterministic.
+template <typename F>
+void launch_objective(const F *X, int64_t n, int64_t d, const F *C, const int32_t *labels, double *partials,
+                      double *out, cudaStream_t s);
+
+}  // namespace kmb

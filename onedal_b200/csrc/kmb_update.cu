@@ -1,0 +1,759 @@
+// Lloyd update on the GPU: centroid sums, counts, empty-cluster reseeding,
+// centroid shift and the convergence test.
+//
+// Reference semantics (DAAL dense Lloyd):
+//  - per-cluster sums S1 and counts S0 over the rows' labels, reduced in double
+//      cpp/daal/src/algorithms/kmeans/kmeans_lloyd_impl.i:220-229, 363-411
+//  - c_j = S1_j / S0_j for non-empty clusters; empty clusters take, in ascending
+//    cluster order, the rows with the largest squared distance (descending)
+//      cpp/daal/src/algorithms/kmeans/kmeans_lloyd_batch_impl.i:153-188,
+//      kmeans_lloyd_impl.i:413-480
+//  - shift = sum_j ||c_old - c_new||^2 ; stop when shift <= eps
+//      kmeans_lloyd_batch_impl.i:189-212
+//
+// B200 design. The sums are FP64 and deterministic: rows are counting-sorted
+// by label with a stable scatter (per-chunk histograms, label-major scan,
+// warp-ranked scatter), then each cluster's rows are summed in row order in
+// fixed pieces of `piece_rows` rows and the pieces are added in order. Equal
+// labels therefore give bit-identical centroids run to run, which is what
+// makes the eps == 0 fixed-point stop (DAAL's "centroids unchanged") exact.
+// Every kernel returns at once when the device loop state says `done`.
+#include "kmb_internal.cuh"
+
+#include <algorithm>
+
+namespace kmb {
+namespace {
+
+constexpr int kSmemKMax = 8192;      // labels counted in shared memory up to this k
+constexpr int64_t kGroupChunks = 64; // chunks per scan group
+constexpr int64_t kPieceRows = 512;  // rows per FP64 partial sum
+
+__device__ __forceinline__ bool is_done(const LoopState *st) { return st && st->done; }
+
+// ---- counting sort ---------------------------------------------------------
+
+__global__ void hist_smem_kernel(const int32_t *__restrict__ labels, int64_t n, int k, int64_t R,
+                                 int32_t *__restrict__ H, const LoopState *st) {
+    if (is_done(st)) return;
+    extern __shared__ int sh[];
+    for (int j = threadIdx.x; j < k; j += blockDim.x) sh[j] = 0;
+    __syncthreads();
+    const int64_t c = blockIdx.x;
+    const int64_t b = c * R, e = min(n, b + R);
+    for (int64_t r = b + threadIdx.x; r < e; r += blockDim.x) atomicAdd(&sh[labels[r]], 1);
+    __syncthreads();
+    int32_t *Hc = H + c * (int64_t)k;
+    for (int j = threadIdx.x; j < k; j += blockDim.x) Hc[j] = sh[j];
+}
+
+__global__ void zero_i32_kernel(int32_t *__restrict__ p, int64_t count, const LoopState *st) {
+    if (is_done(st)) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = 0;
+}
+
+__global__ void hist_global_kernel(const int32_t *__restrict__ labels, int64_t n, int k, int64_t R,
+                                   int32_t *__restrict__ H, const LoopState *st) {
+    if (is_done(st)) return;
+    const int64_t c = blockIdx.x;
+    const int64_t b = c * R, e = min(n, b + R);
+    int32_t *Hc = H + c * (int64_t)k;
+    for (int64_t r = b + threadIdx.x; r < e; r += blockDim.x) atomicAdd(&Hc[labels[r]], 1);
+}
+
+// Gs[g][j] = sum of H[c][j] over the chunks c of group g.
+__global__ void scan_group_sum_kernel(const int32_t *__restrict__ H, int64_t n_chunks, int k,
+                                      int64_t *__restrict__ Gs, const LoopState *st) {
+    if (is_done(st)) return;
+    const int j = blockIdx.y * blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    const int64_t g = blockIdx.x;
+    const int64_t c0 = g * kGroupChunks, c1 = min(n_chunks, c0 + kGroupChunks);
+    int64_t s = 0;
+#pragma unroll 8
+    for (int64_t c = c0; c < c1; ++c) s += H[c * k + j];
+    Gs[g * k + j] = s;
+}
+
+// Exclusive scan of Gs over groups, per label; counts[j] = total rows of label j.
+__global__ void scan_groups_kernel(int64_t *__restrict__ Gs, int64_t n_groups, int k, int64_t *__restrict__ counts,
+                                   const LoopState *st) {
+    if (is_done(st)) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    int64_t run = 0;
+    for (int64_t g = 0; g < n_groups; ++g) {
+        const int64_t v = Gs[g * k + j];
+        Gs[g * k + j] = run;
+        run += v;
+    }
+    counts[j] = run;
+}
+
+// Single block: offsets = exclusive scan of counts (k+1 entries) and
+// piece_base = exclusive scan of ceil(counts / piece_rows) (k+1 entries).
+__global__ void offsets_kernel(const int64_t *__restrict__ counts, int k, int64_t piece_rows,
+                               int64_t *__restrict__ offsets, int64_t *__restrict__ piece_base, const LoopState *st) {
+    if (is_done(st)) return;
+    __shared__ int64_t s_rows[1024], s_pcs[1024];
+    const int T = blockDim.x;
+    const int per = (k + T - 1) / T;
+    const int j0 = threadIdx.x * per, j1 = min(k, j0 + per);
+    int64_t rows = 0, pcs = 0;
+    for (int j = j0; j < j1; ++j) {
+        rows += counts[j];
+        pcs += (counts[j] + piece_rows - 1) / piece_rows;
+    }
+    s_rows[threadIdx.x] = rows;
+    s_pcs[threadIdx.x] = pcs;
+    __syncthreads();
+    // Inclusive Hillis-Steele scan over the per-thread totals.
+    for (int off = 1; off < T; off <<= 1) {
+        int64_t a = 0, b = 0;
+        if ((int)threadIdx.x >= off) {
+            a = s_rows[threadIdx.x - off];
+            b = s_pcs[threadIdx.x - off];
+        }
+        __syncthreads();
+        s_rows[threadIdx.x] += a;
+        s_pcs[threadIdx.x] += b;
+        __syncthreads();
+    }
+    int64_t r = s_rows[threadIdx.x] - rows, p = s_pcs[threadIdx.x] - pcs;
+    for (int j = j0; j < j1; ++j) {
+        offsets[j] = r;
+        piece_base[j] = p;
+        r += counts[j];
+        p += (counts[j] + piece_rows - 1) / piece_rows;
+    }
+    if (threadIdx.x == T - 1) {
+        offsets[k] = s_rows[T - 1];
+        piece_base[k] = s_pcs[T - 1];
+    }
+}
+
+// H[c][j] <- first output position of chunk c's rows with label j.
+__global__ void scan_chunks_kernel(int32_t *__restrict__ H, int64_t n_chunks, int k, const int64_t *__restrict__ Gs,
+                                   const int64_t *__restrict__ offsets, const LoopState *st) {
+    if (is_done(st)) return;
+    const int j = blockIdx.y * blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    const int64_t g = blockIdx.x;
+    const int64_t c0 = g * kGroupChunks, c1 = min(n_chunks, c0 + kGroupChunks);
+    int64_t run = offsets[j] + Gs[g * k + j];
+    for (int64_t c = c0; c < c1; ++c) {
+        const int32_t v = H[c * k + j];
+        H[c * k + j] = (int32_t)run;
+        run += v;
+    }
+}
+
+// One warp per chunk: rows are visited in order 32 at a time; equal labels in a
+// group are ranked by lane, so the scatter is stable.
+template <bool SMEM>
+__global__ void scatter_kernel(const int32_t *__restrict__ labels, int64_t n, int k, int64_t R,
+                               int32_t *__restrict__ H, int32_t *__restrict__ perm, const LoopState *st) {
+    if (is_done(st)) return;
+    extern __shared__ int sh[];
+    const int lane = threadIdx.x;
+    const int64_t c = blockIdx.x;
+    int32_t *Hc = H + c * (int64_t)k;
+    int *cnt = SMEM ? sh : Hc;
+    if (SMEM) {
+        for (int j = lane; j < k; j += 32) sh[j] = Hc[j];
+        __syncwarp();
+    }
+    const int64_t b = c * R, e = min(n, b + R);
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t base = b; base < e; base += 32) {
+        const int64_t r = base + lane;
+        const bool valid = r < e;
+        const unsigned mask = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+            const int lab = labels[r];
+            const unsigned peers = __match_any_sync(mask, lab);
+            const int rank = __popc(peers & lt);
+            const int pos = cnt[lab] + rank;
+            perm[pos] = (int32_t)r;
+            __syncwarp(mask);
+            if (lane == __ffs(peers) - 1) cnt[lab] = pos - rank + __popc(peers);
+        }
+        __syncwarp();
+    }
+}
+
+// ---- FP64 sums ---------------------------------------------------------------
+
+// Thread layout for row-sum style kernels over d columns with NT threads:
+// dl columns lanes (power of two >= min(d, NT)), rp = NT / dl rows in parallel.
+__device__ __forceinline__ void row_layout(int d, int nt, int &dl, int &rp) {
+    dl = 32;
+    while (dl < d && dl < nt) dl <<= 1;
+    rp = nt / dl;
+}
+
+// Block p sums the rows of piece p (part of one cluster's segment of `perm`)
+// into records[p * d + t], in row order.
+template <typename F>
+__global__ void __launch_bounds__(128)
+segsum_kernel(const F *__restrict__ X, int d, int k, const int32_t *__restrict__ perm,
+              const int64_t *__restrict__ offsets, const int64_t *__restrict__ piece_base, int64_t piece_rows,
+              double *__restrict__ records, const LoopState *st) {
+    if (is_done(st)) return;
+    constexpr int NT = 128;
+    __shared__ int32_t rows[kPieceRows];
+    __shared__ double part[NT];
+    const int64_t p = blockIdx.x;
+    if (p >= piece_base[k]) return;
+    // cluster j: piece_base[j] <= p < piece_base[j + 1]
+    int lo = 0, hi = k;  // invariant: piece_base[lo] <= p < piece_base[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (piece_base[mid] <= p) lo = mid; else hi = mid;
+    }
+    const int j = lo;
+    const int64_t q = p - piece_base[j];
+    const int64_t s = offsets[j] + q * piece_rows;
+    const int64_t e = min(s + piece_rows, offsets[j + 1]);
+    const int cnt = (int)(e - s);
+    for (int i = threadIdx.x; i < cnt; i += NT) rows[i] = perm[s + i];
+    __syncthreads();
+
+    int dl, rp;
+    row_layout(d, NT, dl, rp);
+    const int t = threadIdx.x % dl, rr = threadIdx.x / dl;
+    for (int t0 = 0; t0 < d; t0 += dl) {
+        const int col = t0 + t;
+        double acc = 0.0;
+        if (col < d) {
+            int i = rr;
+            for (; i + 3 * rp < cnt; i += 4 * rp) {
+                const F v0 = X[(int64_t)rows[i] * d + col];
+                const F v1 = X[(int64_t)rows[i + rp] * d + col];
+                const F v2 = X[(int64_t)rows[i + 2 * rp] * d + col];
+                const F v3 = X[(int64_t)rows[i + 3 * rp] * d + col];
+                acc += (double)v0;
+                acc += (double)v1;
+                acc += (double)v2;
+                acc += (double)v3;
+            }
+            for (; i < cnt; i += rp) acc += (double)X[(int64_t)rows[i] * d + col];
+        }
+        part[threadIdx.x] = acc;
+        __syncthreads();
+        if (rr == 0 && col < d) {
+            double tot = part[t];
+            for (int r2 = 1; r2 < rp; ++r2) tot += part[r2 * dl + t];
+            records[p * d + col] = tot;
+        }
+        __syncthreads();
+    }
+}
+
+// Per cluster: S = sum of its pieces (in order); c = F(S / count); shift part.
+template <typename F>
+__global__ void finalize_kernel(const double *__restrict__ records, const int64_t *__restrict__ counts,
+                                const int64_t *__restrict__ piece_base, const F *__restrict__ C_old,
+                                F *__restrict__ C_new, int d, double *__restrict__ shift_part,
+                                int32_t *__restrict__ empty_flag, const LoopState *st) {
+    if (is_done(st)) return;
+    __shared__ double red[32];
+    const int j = blockIdx.x;
+    const int64_t cnt = counts[j];
+    const int64_t p0 = piece_base[j], p1 = piece_base[j + 1];
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < d; t += blockDim.x) {
+        const F old = C_old[(int64_t)j * d + t];
+        if (cnt > 0) {
+            double S = 0.0;
+            for (int64_t p = p0; p < p1; ++p) S += records[p * d + t];
+            const F c = F(S / (double)cnt);
+            const double df = (double)old - (double)c;
+            acc += df * df;
+            C_new[(int64_t)j * d + t] = c;
+        } else {
+            C_new[(int64_t)j * d + t] = old;
+        }
+    }
+    for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+        shift_part[j] = tot;
+        empty_flag[j] = cnt > 0 ? 0 : 1;
+    }
+}
+
+// Sums of the pieces without the division (sharded training).
+__global__ void sums_kernel(const double *__restrict__ records, const int64_t *__restrict__ counts_in,
+                            const int64_t *__restrict__ piece_base, int d, double *__restrict__ sums,
+                            int64_t *__restrict__ counts_out) {
+    const int j = blockIdx.x;
+    const int64_t p0 = piece_base[j], p1 = piece_base[j + 1];
+    for (int t = threadIdx.x; t < d; t += blockDim.x) {
+        double S = 0.0;
+        for (int64_t p = p0; p < p1; ++p) S += records[p * d + t];
+        sums[(int64_t)j * d + t] = S;
+    }
+    if (threadIdx.x == 0) counts_out[j] = counts_in[j];
+}
+
+// Single block: lists empty clusters in ascending order; when none, reduces the
+// shift in a fixed order.
+__global__ void empties_kernel(const int32_t *__restrict__ empty_flag, int k, int32_t *__restrict__ empty_ids,
+                               const double *__restrict__ shift_part, LoopState *st) {
+    if (is_done(st)) return;
+    __shared__ int s_cnt[1024];
+    __shared__ double s_sh[1024];
+    const int T = blockDim.x;
+    const int per = (k + T - 1) / T;
+    const int j0 = threadIdx.x * per, j1 = min(k, j0 + per);
+    int c = 0;
+    double sh = 0.0;
+    for (int j = j0; j < j1; ++j) {
+        c += empty_flag[j];
+        sh += shift_part[j];
+    }
+    s_cnt[threadIdx.x] = c;
+    s_sh[threadIdx.x] = sh;
+    __syncthreads();
+    for (int off = 1; off < T; off <<= 1) {
+        int a = 0;
+        if ((int)threadIdx.x >= off) a = s_cnt[threadIdx.x - off];
+        __syncthreads();
+        s_cnt[threadIdx.x] += a;
+        __syncthreads();
+    }
+    int pos = s_cnt[threadIdx.x] - c;
+    for (int j = j0; j < j1; ++j)
+        if (empty_flag[j]) empty_ids[pos++] = j;
+    if (threadIdx.x == 0) {
+        const int ne = s_cnt[T - 1];
+        st->n_empty = ne;
+        if (ne == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < T; ++w) tot += s_sh[w];
+            st->shift = tot;
+        }
+    }
+}
+
+// ---- empty-cluster reseeding: top-m rows by squared distance ---------------
+
+template <typename F> struct KeyOf;
+template <> struct KeyOf<float> {
+    using U = unsigned int;
+    static constexpr int BITS = 32;
+    __device__ static U key(float v) {
+        const U u = __float_as_uint(v);
+        return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    }
+};
+template <> struct KeyOf<double> {
+    using U = unsigned long long;
+    static constexpr int BITS = 64;
+    __device__ static U key(double v) {
+        const U u = (U)__double_as_longlong(v);
+        return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
+    }
+};
+
+struct SelState {
+    unsigned long long prefix;
+    unsigned long long mask;
+    long long need;       // rows still to take at or below the current prefix
+    long long above;      // rows strictly above the threshold
+    int active;
+};
+
+__global__ void sel_init_kernel(SelState *ss, unsigned int *hist, const LoopState *st) {
+    if (is_done(st) || st->n_empty == 0) return;
+    if (threadIdx.x == 0) {
+        ss->prefix = 0;
+        ss->mask = 0;
+        ss->need = st->n_empty;
+        ss->above = 0;
+        ss->active = 1;
+    }
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+}
+
+template <typename F>
+__global__ void sel_hist_kernel(const F *__restrict__ d2, int64_t n, int shift, const SelState *ss,
+                                unsigned int *__restrict__ hist, const LoopState *st) {
+    if (is_done(st) || st->n_empty == 0) return;
+    using K = KeyOf<F>;
+    __shared__ unsigned int sh[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const unsigned long long prefix = ss->prefix, mask = ss->mask;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long key = (unsigned long long)K::key(d2[i]);
+        if ((key & mask) == prefix) atomicAdd(&sh[(key >> shift) & 0xFFu], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+__global__ void sel_pick_kernel(SelState *ss, unsigned int *hist, int shift, const LoopState *st) {
+    if (is_done(st) || st->n_empty == 0) return;
+    if (threadIdx.x == 0) {
+        long long cum = 0;
+        int b = 255;
+        for (; b >= 0; --b) {
+            if (cum + (long long)hist[b] >= ss->need) break;
+            cum += hist[b];
+        }
+        if (b < 0) b = 0;  // not reachable when need <= rows matching the prefix
+        ss->need -= cum;
+        ss->above += cum;
+        ss->prefix |= ((unsigned long long)b) << shift;
+        ss->mask |= 0xFFull << shift;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) hist[i] = 0;
+}
+
+struct Cand {
+    unsigned long long key;
+    long long row;
+};
+
+// Single block: rows with key > T in row order, then the lowest rows with key == T.
+template <typename F>
+__global__ void sel_collect_kernel(const F *__restrict__ d2, int64_t n, const SelState *ss, Cand *__restrict__ cand,
+                                   int cap, const LoopState *st) {
+    if (is_done(st) || st->n_empty == 0) return;
+    using K = KeyOf<F>;
+    __shared__ int s_hi[1024], s_eq[1024];
+    __shared__ long long base_hi, base_eq;
+    const unsigned long long T = ss->prefix;
+    const long long n_hi = ss->above, n_eq = ss->need;
+    if (threadIdx.x == 0) {
+        base_hi = 0;
+        base_eq = 0;
+    }
+    __syncthreads();
+    for (int64_t b0 = 0; b0 < n; b0 += blockDim.x) {
+        if (base_hi >= n_hi && base_eq >= n_eq) break;
+        const int64_t i = b0 + threadIdx.x;
+        unsigned long long key = 0;
+        int is_hi = 0, is_eq = 0;
+        if (i < n) {
+            key = (unsigned long long)K::key(d2[i]);
+            is_hi = key > T;
+            is_eq = key == T;
+        }
+        s_hi[threadIdx.x] = is_hi;
+        s_eq[threadIdx.x] = is_eq;
+        __syncthreads();
+        for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+            int a = 0, c = 0;
+            if ((int)threadIdx.x >= off) {
+                a = s_hi[threadIdx.x - off];
+                c = s_eq[threadIdx.x - off];
+            }
+            __syncthreads();
+            s_hi[threadIdx.x] += a;
+            s_eq[threadIdx.x] += c;
+            __syncthreads();
+        }
+        const long long ph = base_hi + s_hi[threadIdx.x] - is_hi;
+        const long long pe = base_eq + s_eq[threadIdx.x] - is_eq;
+        if (is_hi && ph < n_hi && ph < cap) {
+            cand[ph].key = key;
+            cand[ph].row = i;
+        }
+        if (is_eq && pe < n_eq && n_hi + pe < cap) {
+            cand[n_hi + pe].key = key;
+            cand[n_hi + pe].row = i;
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) {
+            base_hi += s_hi[threadIdx.x];
+            base_eq += s_eq[threadIdx.x];
+        }
+        __syncthreads();
+    }
+}
+
+// Single block bitonic sort of the m = n_empty candidates by (key desc, row asc);
+// positions [m, P) hold sentinels that order last. The buffer holds
+// next_pow2(k) entries.
+__device__ __forceinline__ bool cand_before(const Cand &a, const Cand &b) {
+    return a.key > b.key || (a.key == b.key && a.row < b.row);
+}
+
+__global__ void sel_sort_kernel(Cand *__restrict__ cand, const LoopState *st) {
+    if (is_done(st) || st->n_empty == 0) return;
+    const long long m = st->n_empty;
+    if (m <= 1) return;
+    long long P = 1;
+    while (P < m) P <<= 1;
+    for (long long i = m + threadIdx.x; i < P; i += blockDim.x) {
+        cand[i].key = 0ull;
+        cand[i].row = 0x7fffffffffffffffll;
+    }
+    __syncthreads();
+    for (long long size = 2; size <= P; size <<= 1) {
+        for (long long stride = size >> 1; stride > 0; stride >>= 1) {
+            for (long long i = threadIdx.x; i < P; i += blockDim.x) {
+                const long long j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const Cand a = cand[i], b = cand[j];
+                    const bool swap = up ? cand_before(b, a) : cand_before(a, b);
+                    if (swap) {
+                        cand[i] = b;
+                        cand[j] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Empty cluster e (ascending id) takes candidate e; shift part = ||c_old - x||^2.
+template <typename F>
+__global__ void reseed_apply_kernel(const F *__restrict__ X, int d, const Cand *__restrict__ cand,
+                                    const int32_t *__restrict__ empty_ids, const F *__restrict__ C_old,
+                                    F *__restrict__ C_new, double *__restrict__ shift_part, LoopState *st) {
+    if (is_done(st)) return;
+    const int ne = st->n_empty;
+    __shared__ double red[32];
+    for (int e = blockIdx.x; e < ne; e += gridDim.x) {
+        const int id = empty_ids[e];
+        const long long row = cand[e].row;
+        double acc = 0.0;
+        for (int t = threadIdx.x; t < d; t += blockDim.x) {
+            const F x = X[row * d + t];
+            const double df = (double)C_old[(int64_t)id * d + t] - (double)x;
+            acc += df * df;
+            C_new[(int64_t)id * d + t] = x;
+        }
+        for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+            shift_part[id] = tot;
+        }
+        __syncthreads();
+    }
+}
+
+// After reseeding: shift = sum of all parts in a fixed order (single block).
+__global__ void shift_total_kernel(const double *__restrict__ shift_part, int k, LoopState *st) {
+    if (is_done(st) || st->n_empty == 0) return;
+    __shared__ double s[1024];
+    const int T = blockDim.x;
+    const int per = (k + T - 1) / T;
+    const int j0 = threadIdx.x * per, j1 = min(k, j0 + per);
+    double a = 0.0;
+    for (int j = j0; j < j1; ++j) a += shift_part[j];
+    s[threadIdx.x] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < T; ++w) tot += s[w];
+        st->shift = tot;
+        st->empty_events += st->n_empty;
+    }
+}
+
+template <typename F>
+__global__ void commit_copy_kernel(const F *__restrict__ src, F *__restrict__ dst, int64_t count, const LoopState *st) {
+    if (is_done(st)) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+__global__ void decide_kernel(LoopState *st) {
+    if (st->done) return;
+    st->iterations += 1;
+    if (st->shift <= st->eps) st->done = 1;
+}
+
+// ---- objective -------------------------------------------------------------
+
+template <typename F>
+__global__ void __launch_bounds__(256)
+objective_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restrict__ C, const int32_t *__restrict__ labels,
+                 double *__restrict__ partials) {
+    constexpr int NT = 256;
+    __shared__ double part[NT];
+    int dl, rp;
+    row_layout(d, NT, dl, rp);
+    const int t = threadIdx.x % dl, rr = threadIdx.x / dl;
+    const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t b = (int64_t)blockIdx.x * per, e = min(n, b + per);
+    double acc = 0.0;
+    for (int t0 = 0; t0 < d; t0 += dl) {
+        const int col = t0 + t;
+        if (col >= d) continue;
+        for (int64_t i = b + rr; i < e; i += rp) {
+            const double df = (double)X[i * d + col] - (double)C[(int64_t)labels[i] * d + col];
+            acc += df * df;
+        }
+    }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = NT / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = part[0];
+}
+
+__global__ void sum_partials_kernel(const double *__restrict__ partials, int count, double *__restrict__ out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < count; ++i) s += partials[i];
+        *out = s;
+    }
+}
+
+}  // namespace
+
+constexpr int kObjectiveBlocks = 148 * 8;
+
+UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d) {
+    UpdatePlan p;
+    p.n = n;
+    p.k = k;
+    p.d = d;
+    // Chunk histograms are n_chunks x k int32: keep them under 2^25 entries.
+    int64_t R = 2048;
+    const double need = (double)n * (double)k / (double)(1ll << 25);
+    while ((double)R < need) R <<= 1;
+    p.chunk_rows = R;
+    p.n_chunks = n > 0 ? (n + R - 1) / R : 0;
+    p.piece_rows = kPieceRows;
+    p.max_pieces = (n + kPieceRows - 1) / kPieceRows + k;
+    return p;
+}
+
+bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize) {
+    const int64_t n_groups = (p.n_chunks + kGroupChunks - 1) / kGroupChunks;
+    bool ok = true;
+    ok &= ws.ensure(ws.H, sizeof(int32_t) * std::max<int64_t>(1, p.n_chunks * p.k));
+    ok &= ws.ensure(ws.Gs, sizeof(int64_t) * std::max<int64_t>(1, n_groups * p.k));
+    ok &= ws.ensure(ws.counts, sizeof(int64_t) * (p.k + 1));
+    ok &= ws.ensure(ws.offsets, sizeof(int64_t) * (p.k + 1));
+    ok &= ws.ensure(ws.piece_base, sizeof(int64_t) * (p.k + 1));
+    ok &= ws.ensure(ws.perm, sizeof(int32_t) * std::max<int64_t>(1, p.n));
+    ok &= ws.ensure(ws.records, sizeof(double) * p.max_pieces * p.d);
+    ok &= ws.ensure(ws.shift_part, sizeof(double) * p.k);
+    ok &= ws.ensure(ws.empty_flag, sizeof(int32_t) * p.k);
+    ok &= ws.ensure(ws.empty_ids, sizeof(int32_t) * p.k);
+    ok &= ws.ensure(ws.sel_hist, sizeof(unsigned int) * 256);
+    ok &= ws.ensure(ws.sel_state, sizeof(SelState));
+    int64_t pk = 1;
+    while (pk < p.k) pk <<= 1;
+    ok &= ws.ensure(ws.cand, sizeof(Cand) * pk);
+    ok &= ws.ensure(ws.obj_part, sizeof(double) * kObjectiveBlocks);
+    (void)fsize;
+    return ok;
+}
+
+// Stable counting sort of rows by label + FP64 piece sums (records).
+static void sort_and_sum_pieces(const void *Xv, size_t fsize, const UpdatePlan &p, const int32_t *labels,
+                                Workspace &ws, const LoopState *st, cudaStream_t s) {
+    const int k = (int)p.k;
+    const int64_t n_groups = (p.n_chunks + kGroupChunks - 1) / kGroupChunks;
+    int32_t *H = (int32_t *)ws.H.ptr;
+    int64_t *Gs = (int64_t *)ws.Gs.ptr;
+    int64_t *counts = (int64_t *)ws.counts.ptr;
+    int64_t *offsets = (int64_t *)ws.offsets.ptr;
+    int64_t *piece_base = (int64_t *)ws.piece_base.ptr;
+    int32_t *perm = (int32_t *)ws.perm.ptr;
+    const bool smem = k <= kSmemKMax;
+    if (smem) {
+        hist_smem_kernel<<<(unsigned)p.n_chunks, 256, sizeof(int) * k, s>>>(labels, p.n, k, p.chunk_rows, H, st);
+    } else {
+        zero_i32_kernel<<<1184, 256, 0, s>>>(H, p.n_chunks * p.k, st);
+        hist_global_kernel<<<(unsigned)p.n_chunks, 256, 0, s>>>(labels, p.n, k, p.chunk_rows, H, st);
+    }
+    const dim3 g2((unsigned)n_groups, (unsigned)((k + 255) / 256));
+    scan_group_sum_kernel<<<g2, 256, 0, s>>>(H, p.n_chunks, k, Gs, st);
+    scan_groups_kernel<<<(unsigned)((k + 255) / 256), 256, 0, s>>>(Gs, n_groups, k, counts, st);
+    offsets_kernel<<<1, 1024, 0, s>>>(counts, k, p.piece_rows, offsets, piece_base, st);
+    scan_chunks_kernel<<<g2, 256, 0, s>>>(H, p.n_chunks, k, Gs, offsets, st);
+    if (smem)
+        scatter_kernel<true><<<(unsigned)p.n_chunks, 32, sizeof(int) * k, s>>>(labels, p.n, k, p.chunk_rows, H, perm, st);
+    else
+        scatter_kernel<false><<<(unsigned)p.n_chunks, 32, 0, s>>>(labels, p.n, k, p.chunk_rows, H, perm, st);
+    double *records = (double *)ws.records.ptr;
+    if (fsize == sizeof(float))
+        segsum_kernel<float><<<(unsigned)p.max_pieces, 128, 0, s>>>((const float *)Xv, (int)p.d, k, perm, offsets,
+                                                                    piece_base, p.piece_rows, records, st);
+    else
+        segsum_kernel<double><<<(unsigned)p.max_pieces, 128, 0, s>>>((const double *)Xv, (int)p.d, k, perm, offsets,
+                                                                     piece_base, p.piece_rows, records, st);
+}
+
+template <typename F>
+void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *C_old, F *C_new,
+                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s) {
+    const int k = (int)p.k, d = (int)p.d;
+    sort_and_sum_pieces(X, sizeof(F), p, labels, ws, st, s);
+    double *shift_part = (double *)ws.shift_part.ptr;
+    int32_t *empty_flag = (int32_t *)ws.empty_flag.ptr;
+    int32_t *empty_ids = (int32_t *)ws.empty_ids.ptr;
+    finalize_kernel<F><<<k, 128, 0, s>>>((const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr,
+                                         (const int64_t *)ws.piece_base.ptr, C_old, C_new, d, shift_part,
+                                         empty_flag, st);
+    empties_kernel<<<1, 1024, 0, s>>>(empty_flag, k, empty_ids, shift_part, st);
+    // Reseeding: every kernel below returns at once unless some cluster is empty.
+    SelState *ss = (SelState *)ws.sel_state.ptr;
+    unsigned int *hist = (unsigned int *)ws.sel_hist.ptr;
+    Cand *cand = (Cand *)ws.cand.ptr;
+    sel_init_kernel<<<1, 256, 0, s>>>(ss, hist, st);
+    for (int shift = KeyOf<F>::BITS - 8; shift >= 0; shift -= 8) {
+        sel_hist_kernel<F><<<592, 256, 0, s>>>(d2, p.n, shift, ss, hist, st);
+        sel_pick_kernel<<<1, 256, 0, s>>>(ss, hist, shift, st);
+    }
+    sel_collect_kernel<F><<<1, 1024, 0, s>>>(d2, p.n, ss, cand, k, st);
+    sel_sort_kernel<<<1, 1024, 0, s>>>(cand, st);
+    reseed_apply_kernel<F><<<std::min(k, 1024), 128, 0, s>>>(X, d, cand, empty_ids, C_old, C_new, shift_part, st);
+    shift_total_kernel<<<1, 1024, 0, s>>>(shift_part, k, st);
+    if (commit) {
+        commit_copy_kernel<F><<<std::max<int64_t>(1, std::min<int64_t>(1184, (p.k * p.d + 255) / 256)), 256, 0, s>>>(
+            C_new, C_old, p.k * p.d, st);
+        decide_kernel<<<1, 1, 0, s>>>(st);
+    }
+}
+
+template <typename F>
+void launch_partial_sums(const F *X, const UpdatePlan &p, const int32_t *labels, double *sums, int64_t *counts,
+                         Workspace &ws, cudaStream_t s) {
+    sort_and_sum_pieces(X, sizeof(F), p, labels, ws, nullptr, s);
+    sums_kernel<<<(unsigned)p.k, 128, 0, s>>>((const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr,
+                                             (const int64_t *)ws.piece_base.ptr, (int)p.d, sums, counts);
+}
+
+template <typename F>
+void launch_objective(const F *X, int64_t n, int64_t d, const F *C, const int32_t *labels, double *partials,
+                      double *out, cudaStream_t s) {
+    objective_kernel<F><<<kObjectiveBlocks, 256, 0, s>>>(X, n, (int)d, C, labels, partials);
+    sum_partials_kernel<<<1, 32, 0, s>>>(partials, kObjectiveBlocks, out);
+}
+
+#define KMB_INST(F)                                                                                                 \
+    template void launch_update<F>(const F *, const UpdatePlan &, const int32_t *, const F *, F *, F *, Workspace &, \
+                                   LoopState *, bool, cudaStream_t);                                               \
+    template void launch_partial_sums<F>(const F *, const UpdatePlan &, const int32_t *, double *, int64_t *,       \
+                                         Workspace &, cudaStream_t);                                               \
+    template void launch_objective<F>(const F *, int64_t, int64_t, const F *, const int32_t *, double *, double *, \
+                                      cudaStream_t);
+KMB_INST(float)
+KMB_INST(double)
+#undef KMB_INST
+
+}  // namespace kmb

@@ -1,0 +1,139 @@
+"""CPU tests: the oracle is pinned against the reference's golden vectors and
+against the reference's own DAAL kernel compiled from source."""
+import numpy as np
+import pytest
+
+from helpers import centroid_rel_err, find_match_centroids, load_json, rel_close
+from oracle import daal_ref, restated
+
+DTYPES = [np.float64, np.float32]
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+def test_gold_known_answer(dt):
+    """cpp/oneapi/dal/algo/kmeans/test/fixture.hpp:156-203 with data.hpp:26-184."""
+    g = load_json("gold.json")
+    X = np.array(g["data"], dt).reshape(100, 3)
+    C0 = np.array(g["initial_centroids"], dt).reshape(3, 3)
+    C, lab, obj, it = restated.train(X, C0, g["max_iteration_count"], g["accuracy_threshold"])
+    exp = np.array(g["expected_centroids"]).reshape(3, 3)
+    m = find_match_centroids(exp, C)
+    tol = 1e-7 if dt == np.float64 else 1e-6
+    assert centroid_rel_err(exp, C, m) < tol
+    assert rel_close(obj, g["expected_objective"], tol)
+    # responses under the centroid permutation (fixture.hpp:191-193)
+    assert (m[lab] == np.array(g["expected_responses"])).all()
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+def test_empty_clusters_known_answer(dt):
+    """'kmeans empty clusters test', fixture.hpp:205-219: reseed order and responses."""
+    e = load_json("empty_clusters.json")
+    X = np.array(e["data"], dt).reshape(10, 1)
+    C0 = np.array(e["initial_centroids"], dt).reshape(3, 1)
+    C, lab, obj, it = restated.train(X, C0, 1, 0.0)
+    np.testing.assert_allclose(C.ravel(), e["expected_centroids"], rtol=5 * np.finfo(dt).eps * 100)
+    assert lab.tolist() == e["expected_responses"]
+    assert it == 1
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+def test_smoke_infer_known_answer(dt):
+    """Infer half of the smoke test, fixture.hpp:221-252: objective 4."""
+    s = load_json("smoke_infer.json")
+    X = np.array(s["data"], dt).reshape(8, 2)
+    C = np.array(s["centroids"], dt).reshape(2, 2)
+    lab, obj = restated.infer(X, C, True)
+    assert lab.tolist() == s["expected_responses"]
+    assert rel_close(obj, s["expected_objective"], s["rel_tol"])
+
+
+@pytest.mark.parametrize("tag,dt", [("f64", np.float64), ("f32", np.float32)])
+def test_example_dataset_matches_reference_kernel(tag, dt):
+    """The k-means example's data (data/kmeans_dense_train_*.csv, k=20, 5 iterations,
+    eps 0.001) against outputs of the reference kernel recorded in the fixture."""
+    z = np.load(__import__("os").path.join(__import__("helpers").GOLDEN, "example_dense.npz"))
+    C, lab, obj, it = restated.train(z["X"].astype(dt), z["C0"].astype(dt), 5, 0.001)
+    assert it == int(z[f"iters_{tag}"])
+    assert (lab == z[f"labels_{tag}"]).all()
+    assert centroid_rel_err(z[f"C_{tag}"], C) < (1e-13 if dt == np.float64 else 1e-6)
+    assert rel_close(obj, float(z[f"obj_{tag}"]), 1e-12 if dt == np.float64 else 1e-6)
+
+
+@pytest.mark.parametrize("tag,dt", [("f64", np.float64), ("f32", np.float32)])
+def test_blob_workload_matches_reference_kernel(tag, dt):
+    """Reduced plain-CPU-shaped workload (d=20, k=20, init = first rows, eps 0, 50 max
+    iterations) against recorded reference-kernel outputs."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import blobs_c1
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "daal_ref_c1.npz"))
+    X = blobs_c1(int(z["n"]), int(z["seed"])).astype(dt)
+    C, lab, obj, it = restated.train(X, X[:20].copy(), 50, 0.0)
+    assert it == int(z[f"iters_{tag}"])
+    assert (lab == z[f"labels_{tag}"]).all()
+    assert centroid_rel_err(z[f"C_{tag}"], C) < (1e-13 if dt == np.float64 else 1e-6)
+    assert rel_close(obj, float(z[f"obj_{tag}"]), 1e-12 if dt == np.float64 else 1e-6)
+
+
+needs_ref = pytest.mark.skipif(not daal_ref.available(), reason="reference kernel not built (make -C oracle/ref)")
+
+
+@needs_ref
+@pytest.mark.parametrize("seed", [0, 1, 2])
+@pytest.mark.parametrize("n,d,k", [(257, 3, 5), (1000, 7, 31), (513, 33, 130), (64, 2, 64)])
+def test_restated_equals_reference_kernel_f64(seed, n, d, k):
+    """Live comparison with the reference DAAL kernel (single thread), ragged shapes,
+    including k == n (every row its own cluster) and empty-cluster reseeding."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, d)) * rng.uniform(0.5, 3.0, d)
+    C0 = X[rng.choice(n, k, replace=False)].copy() if seed != 2 else np.repeat(X[:1], k, axis=0) + 1e-3 * np.arange(k)[:, None]
+    daal_ref.set_threads(1)
+    r = daal_ref.train(X, C0, 30, 0.0)
+    s = restated.train(X, C0, 30, 0.0)
+    assert s[3] == r[3]
+    assert (s[1] == r[1]).all()
+    assert centroid_rel_err(r[0], s[0]) < 1e-12
+    assert rel_close(s[2], r[2], 1e-12)
+
+
+@needs_ref
+def test_reference_kernel_thread_count_does_not_change_f64_labels():
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((5000, 8))
+    C0 = X[:16].copy()
+    daal_ref.set_threads(1)
+    a = daal_ref.train(X, C0, 10, 0.0)
+    daal_ref.set_threads(4)
+    b = daal_ref.train(X, C0, 10, 0.0)
+    daal_ref.set_threads(1)
+    assert (a[1] == b[1]).all() and a[3] == b[3]
+    assert centroid_rel_err(a[0], b[0]) < 1e-12
+
+
+def test_step_matches_train_first_iteration():
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((600, 5))
+    C0 = X[:7].copy()
+    C1, lab, shift, ne, goal = restated.step(X, C0)
+    C, _, _, it = restated.train(X, C0, 1, 0.0)
+    assert it == 1
+    np.testing.assert_array_equal(C, C1)
+    assert shift > 0 and ne == 0
+
+
+def test_planted_label_flip_is_detected():
+    """A mistake planted in the oracle's output (one flipped label, one perturbed
+    centroid) must fail the same checks the GPU parity tests apply."""
+    g = load_json("gold.json")
+    X = np.array(g["data"]).reshape(100, 3)
+    C0 = np.array(g["initial_centroids"]).reshape(3, 3)
+    C, lab, obj, it = restated.train(X, C0, 100, 0.0)
+    bad = lab.copy()
+    bad[17] = (bad[17] + 1) % 3
+    m = find_match_centroids(np.array(g["expected_centroids"]).reshape(3, 3), C)
+    assert not (m[bad] == np.array(g["expected_responses"])).all()
+    Cb = C.copy()
+    Cb[1, 2] *= 1 + 1e-5
+    assert centroid_rel_err(C, Cb) > 1e-7
