@@ -25,6 +25,7 @@ struct kmb_context {
     kmb::Workspace ws;
     std::string last_error;
     kmb::LoopState *h_state = nullptr;  // pinned mirror of the device states
+    int num_sms = 148;
     // kernel timing (kmb_context_set_kernel_timing)
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -137,10 +138,18 @@ int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 // Buffers shared by train/infer/step. Returns KMB_OK or KMB_ENOMEM.
 template <typename F>
-int ensure_common(kmb_context *ctx, int64_t n, int64_t d, int64_t k, bool recheck) {
+int ensure_common(kmb_context *ctx, int64_t n, int64_t d, int64_t k, bool recheck, bool tc = false) {
     kmb::Workspace &ws = ctx->ws;
     const int64_t kpad = round_up(k, kBN), dpad = round_up(d, kBK);
     bool ok = true;
+    if (tc) {
+        const int64_t tdp = kmb::tc_dpad(d), tkp = kmb::tc_kpad(k);
+        ok &= ws.ensure(ws.Xhi, sizeof(uint16_t) * n * tdp);
+        ok &= ws.ensure(ws.Xlo, sizeof(uint16_t) * n * tdp);
+        ok &= ws.ensure(ws.Chi, sizeof(uint16_t) * tkp * tdp);
+        ok &= ws.ensure(ws.Clo, sizeof(uint16_t) * tkp * tdp);
+        ok &= ws.ensure(ws.h, sizeof(float) * tkp);
+    }
     ok &= ws.ensure(ws.labels, sizeof(int32_t) * n);
     ok &= ws.ensure(ws.d2, sizeof(F) * n);
     ok &= ws.ensure(ws.xnorm, sizeof(F) * n);
@@ -169,8 +178,37 @@ __global__ void account_recheck_kernel(LoopState *st) {
 
 // One assignment pass of the plain form (+ optional FP64 recheck) under C.
 template <typename F>
-void assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, int64_t k, bool recheck,
-                 int32_t *labels, F *d2, LoopState *st) {
+int assign_pass_tc(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, int64_t k, int32_t *labels,
+                   F *d2, LoopState *st) {
+    return KMB_EUNSUPPORTED;  // float64 data has no tensor-core form
+}
+
+template <>
+int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d, const float *C, int64_t k,
+                          int32_t *labels, float *d2, LoopState *st) {
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    reset_iteration_kernel<<<1, 1, 0, s>>>(st);
+    kmb::launch_prep_centroids_tc(C, k, d, ws.Chi.ptr, ws.Clo.ptr, (float *)ws.h.ptr, &sc->cnorm_max, st, s);
+    int rc;
+    {
+        KernelTimer timer(ctx, 1);
+        rc = kmb::launch_assign_tc(ws.Xhi.ptr, ws.Xlo.ptr, n, d, ws.Chi.ptr, ws.Clo.ptr, (const float *)ws.h.ptr, k,
+                                   (const float *)ws.xnorm.ptr, &sc->cnorm_max, labels, d2,
+                                   (RecheckEntry *)ws.queue.ptr, st, ctx->num_sms, s);
+    }
+    if (rc != KMB_OK) return fail(ctx, rc, "tensor-core assignment launch failed (d=%lld)", (long long)d);
+    kmb::launch_recheck<float>(X, n, d, C, k, (const RecheckEntry *)ws.queue.ptr, labels, d2,
+                               (const float *)ws.xnorm.ptr, st, s);
+    account_recheck_kernel<<<1, 1, 0, s>>>(st);
+    return KMB_OK;
+}
+
+template <typename F>
+int assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, int64_t k, bool recheck,
+                int32_t *labels, F *d2, LoopState *st, bool tc = false) {
+    if (tc) return assign_pass_tc<F>(ctx, X, n, d, C, k, labels, d2, st);
     kmb::Workspace &ws = ctx->ws;
     cudaStream_t s = ctx->stream;
     const int64_t kpad = round_up(k, kBN);
@@ -188,6 +226,15 @@ void assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C,
                                (const F *)ws.xnorm.ptr, st, s);
         account_recheck_kernel<<<1, 1, 0, s>>>(st);
     }
+    return KMB_OK;
+}
+
+// Splits X into the BF16 hi/lo panels the tensor-core form reads (once per call).
+template <typename F>
+void split_rows(kmb_context *ctx, const F *X, int64_t n, int64_t d) {}
+template <>
+void split_rows<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d) {
+    kmb::launch_split_rows(X, n, d, ctx->ws.Xhi.ptr, ctx->ws.Xlo.ptr, ctx->stream);
 }
 
 template <typename F>
@@ -226,13 +273,16 @@ int run_loop(kmb_context *ctx, const F *X, int64_t n, int64_t d, F *C, const kmb
     KMB_CUDA(cudaMemcpyAsync(st, ctx->h_state, sizeof(LoopState), cudaMemcpyHostToDevice, s));
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
     kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
+    const bool tc = p->form == KMB_FORM_BF16X3;
+    if (tc) split_rows<F>(ctx, X, n, d);
     const int64_t T = p->max_iteration_count;
     int64_t enq = 0;
     int64_t batch = 2;
     while (enq < T) {
         const int64_t upto = std::min(T, enq + batch);
         for (; enq < upto; ++enq) {
-            assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, d2, st);
+            int rc = assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, d2, st, tc);
+            if (rc) return rc;
             KernelTimer timer(ctx, 2);
             kmb::launch_update<F>(X, plan, labels, d2, C, Cnew, ws, st, /*commit=*/true, s);
         }
@@ -251,9 +301,10 @@ template <typename F>
 int iterate_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, void *Cv, const kmb_params *p,
                  int32_t *labels, int64_t *iteration_count, kmb_stats *stats) {
     const int64_t k = p->cluster_count;
-    if (p->form == KMB_FORM_BF16X3) return fail(ctx, KMB_EUNSUPPORTED, "BF16x3 form is not built in this library");
-    const bool recheck = p->recheck != 0;
-    int rc = ensure_common<F>(ctx, n, d, k, recheck);
+    const bool tc = p->form == KMB_FORM_BF16X3;
+    if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
+    const bool recheck = p->recheck != 0 || tc;
+    int rc = ensure_common<F>(ctx, n, d, k, recheck, tc);
     if (rc) return rc;
     kmb::UpdatePlan plan = kmb::make_update_plan(n, k, d);
     if (!kmb::ensure_update_buffers(ctx->ws, plan, sizeof(F))) return fail(ctx, KMB_ENOMEM, "update buffers");
@@ -279,9 +330,9 @@ int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
                kmb_stats *stats) {
     const int64_t k = p->cluster_count;
     const bool tc = p->form == KMB_FORM_BF16X3;
-    if (tc) return fail(ctx, KMB_EUNSUPPORTED, "BF16x3 form is not built in this library");
+    if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
     const bool recheck = p->recheck != 0 || tc;
-    int rc = ensure_common<F>(ctx, n, d, k, recheck);
+    int rc = ensure_common<F>(ctx, n, d, k, recheck, tc);
     if (rc) return rc;
     kmb::UpdatePlan plan = kmb::make_update_plan(n, k, d);
     if (!kmb::ensure_update_buffers(ctx->ws, plan, sizeof(F))) return fail(ctx, KMB_ENOMEM, "update buffers");
@@ -306,7 +357,7 @@ int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     KMB_CUDA(cudaMemcpyAsync(Ccur, C0, sizeof(F) * k * d, cudaMemcpyDeviceToDevice, s));
     if ((rc = run_loop<F>(ctx, X, n, d, Ccur, p, plan, labels, recheck))) return rc;
     // Responses against the final centroids, then the exact objective.
-    assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, d2, st_final);
+    if ((rc = assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, d2, st_final, tc))) return rc;
     double *obj_dev = &sc->objective;
     kmb::launch_objective<F>(X, n, d, Ccur, labels, (double *)ws.obj_part.ptr, obj_dev, s);
     KMB_CUDA(cudaGetLastError());
@@ -336,9 +387,9 @@ template <typename F>
 int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t d, const void *Cv, int64_t k,
                int32_t form, int32_t compute_objective, int32_t *responses, double *objective, kmb_stats *stats) {
     const bool tc = form == KMB_FORM_BF16X3;
-    if (tc) return fail(ctx, KMB_EUNSUPPORTED, "BF16x3 form is not built in this library");
+    if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
     const bool recheck = tc;
-    int rc = ensure_common<F>(ctx, n, d, k, recheck);
+    int rc = ensure_common<F>(ctx, n, d, k, recheck, tc);
     if (rc) return rc;
     if (!ctx->ws.ensure(ctx->ws.obj_part, sizeof(double) * 148 * 8)) return fail(ctx, KMB_ENOMEM, "objective");
     kmb::Workspace &ws = ctx->ws;
@@ -356,7 +407,8 @@ int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     KMB_CUDA(cudaMemcpyAsync(st, &ctx->h_state[1], sizeof(LoopState), cudaMemcpyHostToDevice, s));
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
     kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
-    assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, (F *)ws.d2.ptr, st);
+    if (tc) split_rows<F>(ctx, X, n, d);
+    if ((rc = assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, (F *)ws.d2.ptr, st, tc))) return rc;
     if (compute_objective)
         kmb::launch_objective<F>(X, n, d, C, labels, (double *)ws.obj_part.ptr, &sc->objective, s);
     KMB_CUDA(cudaGetLastError());
@@ -381,9 +433,9 @@ template <typename F>
 int step_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, const void *Cin, int64_t k, int32_t form,
               int32_t recheck_flag, void *C_out, int32_t *labels, double *shift, int64_t *n_empty) {
     const bool tc = form == KMB_FORM_BF16X3;
-    if (tc) return fail(ctx, KMB_EUNSUPPORTED, "BF16x3 form is not built in this library");
+    if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
     const bool recheck = recheck_flag != 0 || tc;
-    int rc = ensure_common<F>(ctx, n, d, k, recheck);
+    int rc = ensure_common<F>(ctx, n, d, k, recheck, tc);
     if (rc) return rc;
     kmb::UpdatePlan plan = kmb::make_update_plan(n, k, d);
     if (!kmb::ensure_update_buffers(ctx->ws, plan, sizeof(F))) return fail(ctx, KMB_ENOMEM, "update buffers");
@@ -398,7 +450,8 @@ int step_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, const void
     KMB_CUDA(cudaMemcpyAsync(Ccur, Cin, sizeof(F) * k * d, cudaMemcpyDeviceToDevice, s));
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
     kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
-    assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, (F *)ws.d2.ptr, st);
+    if (tc) split_rows<F>(ctx, X, n, d);
+    if ((rc = assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, (F *)ws.d2.ptr, st, tc))) return rc;
     kmb::launch_update<F>(X, plan, labels, (const F *)ws.d2.ptr, Ccur, (F *)C_out, ws, st, /*commit=*/false, s);
     KMB_CUDA(cudaGetLastError());
     KMB_CUDA(cudaMemcpyAsync(ctx->h_state, st, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
@@ -460,6 +513,7 @@ int kmb_context_create(int device, kmb_context **out) {
         return KMB_ECUDA;
     }
     ctx->own_stream = true;
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     *out = ctx;
     return KMB_OK;
 }

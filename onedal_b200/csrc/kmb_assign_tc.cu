@@ -1,0 +1,532 @@
+// Tensor-core assignment (KMB_FORM_BF16X3): split-BF16 x.c on tcgen05 with FP32
+// accumulation in TMEM, fused per-row argmin, near-tie queue for the FP64 recheck.
+//
+// Same contract as the plain kernel (scores h_j - x.c_j, lowest index on ties,
+// DAAL's kmeans_lloyd_impl.i:185-216 / kmeans_lloyd_postprocessing.h:95-130),
+// different arithmetic: x = xh + xl and c = ch + cl with xh = bf16(x),
+// xl = bf16(x - xh) (same for c), and
+//     x.c ~= xh.ch + xh.cl + xl.ch
+// as three tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulate) per 16-wide
+// k-step into one TMEM accumulator.
+//
+// Per-score error bound (u_b = 2^-8 bf16 unit roundoff, u = 2^-24 FP32):
+//   |dropped terms| <= 3.03 u_b^2 sum_t |x_t c_t|                (split)
+//   |accumulation|  <= 2 * 3 dpad * 2u * sum_t |x_t c_t|         (FP32 adds in the
+//                      tensor core, truncation allowed, factor 2 margin)
+//   |h rounding + final subtraction| <= 2u (h + ||x|| ||c||)
+// with sum_t |x_t c_t| <= ||x|| ||c|| <= ||x|| cmax. Two scores whose computed
+// gap exceeds twice the bound are ordered as the exact ones; every other row
+// is queued with its two best clusters (or flagged for a full rescan when a
+// third cluster is inside the band) and re-scored in FP64 by the recheck kernel.
+//
+// Kernel structure (one CTA per SM, persistent over 128-row tiles, 6 warps):
+//   warp 0   TMA producer: A = the tile's Xhi/Xlo panels (128 rows x 64 bf16,
+//            SWIZZLE_128B), B = Chi/Clo panels of 128 clusters, ring of stages
+//   warp 1   TMEM allocation + single-thread tcgen05.mma issue; commits free
+//            B stages, publish accumulators and release A tiles
+//   warps 2-5 epilogue: tcgen05.ld of the 128x128 FP32 accumulator (one TMEM
+//            lane = one row per thread), running top-3 per row, outputs
+// Accumulators are double-buffered in TMEM so the epilogue of cluster tile j
+// overlaps the MMAs of tile j+1. Every mbarrier wait is bounded; on timeout the
+// CTA records KMB_ETIMEDOUT in the loop state, drains its own TMA loads and
+// MMAs with bounded waits, frees TMEM and returns.
+#include "kmb_internal.cuh"
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+namespace kmb {
+namespace tc {
+
+constexpr int BM = 128;                 // rows per tile (UMMA M)
+constexpr int BN = 128;                 // clusters per tile (UMMA N)
+constexpr int KP = 64;                  // bf16 per panel row (128 bytes, SWIZZLE_128B)
+constexpr int PANEL = 128 * 128;        // bytes per 128-row panel
+constexpr int NACC = 2;                 // TMEM accumulator buffers
+constexpr int TMEM_COLS = NACC * BN;    // 256
+constexpr int MAX_B_STAGES = 8;
+constexpr long long kTimeoutCycles = 4000000000ll;  // ~2 s at 1.9 GHz
+
+struct Params {
+    int64_t n;
+    int d, dpad, k, kpad;
+    int n_tiles, kpanels, ntiles_n;
+    int a_stages, b_stages;
+    const float *h;
+    const float *xnorm;
+    const double *cnorm_max;
+    int32_t *labels;
+    float *d2;
+    RecheckEntry *queue;
+    LoopState *st;
+};
+
+struct Barriers {
+    uint64_t a_full[2], a_empty[2];
+    uint64_t b_full[MAX_B_STAGES], b_empty[MAX_B_STAGES];
+    uint64_t acc_full[NACC], acc_empty[NACC];
+    uint64_t mma_done;
+    uint32_t tmem_base;
+    int abort;
+};
+
+__device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false on abort (set by any role) or timeout (which sets abort).
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort) {
+    if (mbar_test(b, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_test(b, parity)) {
+        if (*abort) return false;
+        if (clock64() - t0 > kTimeoutCycles) {
+            *abort = 1;
+            return false;
+        }
+    }
+    return true;
+}
+// Drain wait used on the abort path: ignores the abort flag, still bounded.
+__device__ __forceinline__ void mbar_drain(uint64_t *b, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_test(b, parity)) {
+        if (clock64() - t0 > kTimeoutCycles) return;
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, uint64_t *bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            su32(dst)),
+        "l"(tm), "r"(su32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major SWIZZLE_128B operand descriptor (sm100 format: version 1, LBO 16 B
+// (unused for swizzled K-major), SBO 1024 B between 8-row groups, layout 2).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+    d |= (uint64_t)1 << 16;          // LBO
+    d |= (uint64_t)(1024 >> 4) << 32; // SBO
+    d |= (uint64_t)1 << 46;          // version
+    d |= (uint64_t)2 << 61;          // SWIZZLE_128B
+    return d;
+}
+
+// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=BN.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+struct Top3 {
+    float b, s, t;
+    int ib, is;
+};
+
+__global__ void __launch_bounds__(192, 1)
+assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant__ CUtensorMap tmXl,
+                 const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl, Params p) {
+    // One read of the loop flag for the whole CTA, so every thread takes the same path.
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) s_skip = p.st->done;
+    __syncthreads();
+    if (s_skip) return;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int a_stage_bytes = 2 * p.kpanels * PANEL;  // hi + lo panels
+    uint8_t *A = smem;
+    uint8_t *B = A + (size_t)p.a_stages * a_stage_bytes;
+    Barriers *bar = (Barriers *)(B + (size_t)p.b_stages * 2 * PANEL);
+    volatile int *abort = &bar->abort;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&bar->a_full[i], 1);
+            mbar_init(&bar->a_empty[i], 1);
+        }
+        for (int i = 0; i < p.b_stages; ++i) {
+            mbar_init(&bar->b_full[i], 1);
+            mbar_init(&bar->b_empty[i], 1);
+        }
+        for (int i = 0; i < NACC; ++i) {
+            mbar_init(&bar->acc_full[i], 1);
+            mbar_init(&bar->acc_empty[i], 4);
+        }
+        mbar_init(&bar->mma_done, 1);
+        bar->abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&bar->tmem_base)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = bar->tmem_base;
+
+    const int my_tiles = (p.n_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            int a_issued[2] = {0, 0};
+            int b_issued[MAX_B_STAGES];
+            for (int i = 0; i < MAX_B_STAGES; ++i) b_issued[i] = 0;
+            long long bcount = 0;
+            bool ok = true;
+            for (int lt = 0; lt < my_tiles && ok; ++lt) {
+                const int tile = blockIdx.x + lt * gridDim.x;
+                const int as = p.a_stages == 2 ? (lt & 1) : 0;
+                const int ause = p.a_stages == 2 ? (lt >> 1) : lt;
+                if (!mbar_wait(&bar->a_empty[as], (ause & 1) ^ 1, abort)) { ok = false; break; }
+                mbar_expect_tx(&bar->a_full[as], (uint32_t)a_stage_bytes);
+                uint8_t *Ab = A + (size_t)as * a_stage_bytes;
+                for (int kp = 0; kp < p.kpanels; ++kp) {
+                    tma_load_2d(Ab + (size_t)kp * PANEL, &tmXh, &bar->a_full[as], kp * KP, tile * BM);
+                    tma_load_2d(Ab + (size_t)(p.kpanels + kp) * PANEL, &tmXl, &bar->a_full[as], kp * KP, tile * BM);
+                }
+                a_issued[as]++;
+                for (int j = 0; j < p.ntiles_n && ok; ++j) {
+                    for (int kp = 0; kp < p.kpanels; ++kp, ++bcount) {
+                        const int bs = (int)(bcount % p.b_stages);
+                        const int buse = (int)(bcount / p.b_stages);
+                        if (!mbar_wait(&bar->b_empty[bs], (buse & 1) ^ 1, abort)) { ok = false; break; }
+                        mbar_expect_tx(&bar->b_full[bs], 2 * PANEL);
+                        uint8_t *Bb = B + (size_t)bs * 2 * PANEL;
+                        tma_load_2d(Bb, &tmCh, &bar->b_full[bs], kp * KP, j * BN);
+                        tma_load_2d(Bb + PANEL, &tmCl, &bar->b_full[bs], kp * KP, j * BN);
+                        b_issued[bs]++;
+                    }
+                }
+            }
+            if (!ok) {
+                // Do not leave while our own bulk copies may still land in shared memory.
+                for (int i = 0; i < 2; ++i)
+                    if (a_issued[i]) mbar_drain(&bar->a_full[i], (a_issued[i] - 1) & 1);
+                for (int i = 0; i < p.b_stages; ++i)
+                    if (b_issued[i]) mbar_drain(&bar->b_full[i], (b_issued[i] - 1) & 1);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            long long bcount = 0, acount = 0;
+            bool ok = true;
+            for (int lt = 0; lt < my_tiles && ok; ++lt) {
+                const int as = p.a_stages == 2 ? (lt & 1) : 0;
+                const int ause = p.a_stages == 2 ? (lt >> 1) : lt;
+                if (!mbar_wait(&bar->a_full[as], ause & 1, abort)) { ok = false; break; }
+                tc_fence_after();
+                const uint32_t a_base = su32(A + (size_t)as * a_stage_bytes);
+                for (int j = 0; j < p.ntiles_n && ok; ++j, ++acount) {
+                    const int slot = (int)(acount % NACC);
+                    const int use = (int)(acount / NACC);
+                    if (!mbar_wait(&bar->acc_empty[slot], (use & 1) ^ 1, abort)) { ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t tmem_d = tmem_base + (uint32_t)(slot * BN);
+                    for (int kp = 0; kp < p.kpanels; ++kp, ++bcount) {
+                        const int bs = (int)(bcount % p.b_stages);
+                        const int buse = (int)(bcount / p.b_stages);
+                        if (!mbar_wait(&bar->b_full[bs], buse & 1, abort)) { ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t ah = a_base + kp * PANEL, al = a_base + (p.kpanels + kp) * PANEL;
+                        const uint32_t bh = su32(B + (size_t)bs * 2 * PANEL), bl = bh + PANEL;
+#pragma unroll
+                        for (int ks = 0; ks < KP / 16; ++ks) {
+                            const uint32_t off = ks * 32;  // 16 bf16 = 32 bytes along the swizzled row
+                            const uint32_t acc = (kp | ks) ? 1u : 0u;
+                            mma_bf16(tmem_d, sw128_desc(ah + off), sw128_desc(bh + off), acc);
+                            mma_bf16(tmem_d, sw128_desc(ah + off), sw128_desc(bl + off), 1u);
+                            mma_bf16(tmem_d, sw128_desc(al + off), sw128_desc(bh + off), 1u);
+                        }
+                        mma_commit(&bar->b_empty[bs]);  // frees the B stage once these MMAs finish
+                    }
+                    if (ok) mma_commit(&bar->acc_full[slot]);
+                }
+                if (ok) mma_commit(&bar->a_empty[as]);
+            }
+            // All issued MMAs complete before TMEM is released.
+            mma_commit(&bar->mma_done);
+            mbar_drain(&bar->mma_done, 0);
+        }
+    } else {
+        // ---------------- epilogue (warps 2..5) ----------------
+        const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
+        const int row_in_tile = quarter * 32 + lane;
+        const double u = 5.9604644775390625e-8;  // 2^-24
+        const double ub2 = 1.52587890625e-5;      // 2^-16
+        const double cmax = *p.cnorm_max;
+        long long acount = 0;
+        bool ok = true;
+        for (int lt = 0; lt < my_tiles && ok; ++lt) {
+            const int tile = blockIdx.x + lt * gridDim.x;
+            Top3 r;
+            r.b = r.s = r.t = __int_as_float(0x7f800000);
+            r.ib = r.is = 0;
+            for (int j = 0; j < p.ntiles_n; ++j, ++acount) {
+                const int slot = (int)(acount % NACC);
+                const int use = (int)(acount / NACC);
+                if (!mbar_wait(&bar->acc_full[slot], use & 1, abort)) { ok = false; break; }
+                tc_fence_after();
+                const float *hj = p.h + j * BN;
+#pragma unroll 1
+                for (int c0 = 0; c0 < BN; c0 += 32) {
+                    float v[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(slot * BN + c0), v);
+#pragma unroll
+                    for (int i = 0; i < 32; i += 4) {
+                        const float4 h4 = __ldg(reinterpret_cast<const float4 *>(hj + c0 + i));
+                        const float sc[4] = {h4.x - v[i], h4.y - v[i + 1], h4.z - v[i + 2], h4.w - v[i + 3]};
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float x = sc[q];
+                            if (x < r.t) {
+                                const int col = j * BN + c0 + i + q;
+                                if (x < r.b) {
+                                    r.t = r.s;
+                                    r.s = r.b;
+                                    r.is = r.ib;
+                                    r.b = x;
+                                    r.ib = col;
+                                } else if (x < r.s) {
+                                    r.t = r.s;
+                                    r.s = x;
+                                    r.is = col;
+                                } else {
+                                    r.t = x;
+                                }
+                            }
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar->acc_empty[slot]);
+            }
+            if (!ok) break;
+            const int64_t row = (int64_t)tile * BM + row_in_tile;
+            if (row < p.n) {
+                p.labels[row] = r.ib;
+                const float xn = p.xnorm[row];
+                p.d2[row] = 2.0f * r.b + xn;
+                if (p.queue) {
+                    const double xl = sqrt(fmax((double)xn, 0.0));
+                    const double xc = xl * cmax;
+                    const double e = 1.0625 * ((3.03 * ub2 + 2.0 * 3.0 * p.dpad * 2.0 * u) * xc +
+                                               2.0 * u * (0.5 * cmax * cmax + xc));
+                    const double band = 2.0 * e;
+                    if ((double)r.s - (double)r.b <= band) {
+                        const int qslot = atomicAdd(&p.st->n_recheck, 1);
+                        RecheckEntry q;
+                        q.row = (int)row;
+                        q.c1 = r.ib;
+                        q.c2 = r.is;
+                        q.full = ((double)r.t - (double)r.b <= band) ? 1 : 0;
+                        p.queue[qslot] = q;
+                    }
+                }
+            }
+        }
+    }
+
+    __syncwarp();
+    tc_fence_before();
+    __syncthreads();
+    if (bar->abort && threadIdx.x == 0) {
+        p.st->error = KMB_ETIMEDOUT;
+        p.st->done = 1;
+    }
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// x -> (bf16(x), bf16(x - bf16(x))) into [rows][dpad] panels, zero padding.
+__global__ void split_rows_kernel(const float *__restrict__ src, int64_t rows, int d, int dpad,
+                                  __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
+    const int64_t total = rows * (int64_t)dpad;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / dpad;
+        const int t = (int)(i - r * dpad);
+        const float x = t < d ? src[r * d + t] : 0.0f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        hi[i] = h;
+        lo[i] = __float2bfloat16_rn(x - __bfloat162float(h));
+    }
+}
+
+// Per-iteration centroid prep for the tensor-core form: Chi/Clo [kpad][dpad],
+// h = 0.5||c||^2 (FP32 from a double sum, +inf padding), max ||c||.
+__global__ void prep_centroids_tc_kernel(const float *__restrict__ C, int k, int d, int dpad, int kpad,
+                                         __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
+                                         float *__restrict__ h, double *__restrict__ cnorm_max, const LoopState *st) {
+    if (st && st->done) return;
+    __shared__ double red[32];
+    const int j = blockIdx.x;
+    double s = 0.0;
+    for (int t = threadIdx.x; t < dpad; t += blockDim.x) {
+        const float x = (j < k && t < d) ? C[(int64_t)j * d + t] : 0.0f;
+        const __nv_bfloat16 b = __float2bfloat16_rn(x);
+        hi[(int64_t)j * dpad + t] = b;
+        lo[(int64_t)j * dpad + t] = __float2bfloat16_rn(x - __bfloat162float(b));
+        s += (double)x * (double)x;
+    }
+    for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+        h[j] = (j < k) ? (float)(0.5 * tot) : __int_as_float(0x7f800000);
+        if (j < k)
+            atomicMax(reinterpret_cast<unsigned long long *>(cnorm_max),
+                      (unsigned long long)__double_as_longlong(sqrt(tot)));
+    }
+}
+
+__global__ void reset_cmax_kernel(double *p, const LoopState *st) {
+    if (st && st->done) return;
+    *p = 0.0;
+}
+
+}  // namespace tc
+
+int64_t tc_dpad(int64_t d) { return (d + tc::KP - 1) / tc::KP * tc::KP; }
+int64_t tc_kpad(int64_t k) { return (k + tc::BN - 1) / tc::BN * tc::BN; }
+bool tc_supported(int64_t d) { return tc_dpad(d) <= 256; }
+
+void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, cudaStream_t s) {
+    const int64_t dpad = tc_dpad(d);
+    const int64_t total = rows * dpad;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+    tc::split_rows_kernel<<<blocks, 256, 0, s>>>(X, rows, (int)d, (int)dpad, (__nv_bfloat16 *)hi, (__nv_bfloat16 *)lo);
+}
+
+void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, void *Clo, float *h, double *cnorm_max,
+                              const LoopState *st, cudaStream_t s) {
+    const int64_t dpad = tc_dpad(d), kpad = tc_kpad(k);
+    tc::reset_cmax_kernel<<<1, 1, 0, s>>>(cnorm_max, st);
+    tc::prep_centroids_tc_kernel<<<(unsigned)kpad, 128, 0, s>>>(C, (int)k, (int)d, (int)dpad, (int)kpad,
+                                                                 (__nv_bfloat16 *)Chi, (__nv_bfloat16 *)Clo, h,
+                                                                 cnorm_max, st);
+}
+
+static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t dpad) {
+    const cuuint64_t dims[2] = {(cuuint64_t)dpad, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)dpad * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)tc::KP, 128u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    return cuTensorMapEncodeTiled(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
+                                  estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Launches the tensor-core assignment. Returns KMB_OK, or an error status when
+// the shape is outside the kernel's limits or tensor maps cannot be encoded.
+int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
+                     const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
+                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, cudaStream_t s) {
+    const int64_t dpad = tc_dpad(d), kpad = tc_kpad(k);
+    if (dpad > 256) return KMB_EUNSUPPORTED;
+    if (n == 0) return KMB_OK;
+    // Shared memory plan: A stages (hi+lo panels of the row tile), B ring.
+    int optin = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int kpanels = (int)(dpad / tc::KP);
+    const int a_stage = 2 * kpanels * tc::PANEL;
+    const int fixed = 1024 + (int)sizeof(tc::Barriers) + 64;
+    int a_stages = (2 * a_stage + 3 * 2 * tc::PANEL + fixed <= optin) ? 2 : 1;
+    int b_stages = (optin - fixed - a_stages * a_stage) / (2 * tc::PANEL);
+    b_stages = std::min(b_stages, tc::MAX_B_STAGES);
+    if (b_stages < 2) return KMB_EUNSUPPORTED;
+    const size_t smem = (size_t)a_stages * a_stage + (size_t)b_stages * 2 * tc::PANEL + fixed;
+
+    CUtensorMap mXh, mXl, mCh, mCl;
+    if (!encode_map(&mXh, Xhi, n, dpad) || !encode_map(&mXl, Xlo, n, dpad) || !encode_map(&mCh, Chi, kpad, dpad) ||
+        !encode_map(&mCl, Clo, kpad, dpad))
+        return KMB_ECUDA;
+    tc::Params p;
+    p.n = n;
+    p.d = (int)d;
+    p.dpad = (int)dpad;
+    p.k = (int)k;
+    p.kpad = (int)kpad;
+    p.n_tiles = (int)((n + tc::BM - 1) / tc::BM);
+    p.kpanels = kpanels;
+    p.ntiles_n = (int)(kpad / tc::BN);
+    p.a_stages = a_stages;
+    p.b_stages = b_stages;
+    p.h = h;
+    p.xnorm = xnorm;
+    p.cnorm_max = cnorm_max;
+    p.labels = labels;
+    p.d2 = d2;
+    p.queue = queue;
+    p.st = st;
+    if (cudaFuncSetAttribute(tc::assign_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return KMB_ECUDA;
+    const int grid = (int)std::min<int64_t>(num_sms, p.n_tiles);
+    tc::assign_tc_kernel<<<grid, 192, smem, s>>>(mXh, mXl, mCh, mCl, p);
+    return cudaGetLastError() == cudaSuccess ? KMB_OK : KMB_ECUDA;
+}
+
+}  // namespace kmb

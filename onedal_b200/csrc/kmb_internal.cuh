@@ -94,6 +94,19 @@ template <typename F>
 void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, const RecheckEntry *queue,
                     int32_t *labels, F *d2, const F *xnorm, LoopState *st, cudaStream_t s);
 
+// ---- assignment (tensor-core BF16x3 form, float32 data) ----------------------
+int64_t tc_dpad(int64_t d);   // d rounded up to the 64-wide K panel
+int64_t tc_kpad(int64_t k);   // k rounded up to the 128-wide cluster tile
+bool tc_supported(int64_t d); // dpad <= 256
+// X (rows x d, FP32) -> hi/lo BF16 [rows][dpad], zero padded.
+void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, cudaStream_t s);
+// C -> Chi/Clo [kpad][dpad], h (kpad, +inf padding), max ||c||.
+void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, void *Clo, float *h,
+                              double *cnorm_max, const LoopState *st, cudaStream_t s);
+int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
+                     const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
+                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, cudaStream_t s);
+
 // ---- update ----------------------------------------------------------------
 UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d);
 // Sizes the update buffers of `ws` for plan `p` (false on allocation failure).

@@ -94,18 +94,32 @@ def test_example_dataset(tag, dt):
 
 @pytest.mark.parametrize("tag,dt", [("f64", np.float64), ("f32", np.float32)])
 def test_blob_workload_end_to_end(tag, dt):
-    """Reduced plain-CPU-shaped workload (d=20, k=20, eps 0, 50 max iterations): iteration
-    count, responses, centroids and objective vs the recorded reference-kernel run."""
+    """Reduced plain-CPU-shaped workload (d=20, k=20, eps 0, 50 max iterations) vs the
+    recorded reference-kernel run. float64: iteration count, responses, centroids and
+    objective as the reference's. float32: the reference's own FP32 labels differ from
+    any other FP32 summation order on near-ties, so responses are checked against the FP64
+    oracle under the returned centroids (exact outside the rounding band) and against the
+    reference's FP32 labels up to 0.1% of rows."""
     sys.path.insert(0, GOLDEN)
     from make_golden import blobs_c1
     z = np.load(os.path.join(GOLDEN, "daal_ref_c1.npz"))
     X = blobs_c1(int(z["n"]), int(z["seed"])).astype(dt)
     r = kmeans.train(desc(dt, 20, 50, 0.0), X, X[:20].copy())
+    C = r.get_model().get_centroids()
+    lab = r.get_responses().ravel()
     assert r.get_iteration_count() == int(z[f"iters_{tag}"])
-    assert (r.get_responses().ravel() == z[f"labels_{tag}"]).all()
-    ref64 = restated.train(X.astype(np.float64), X[:20].astype(np.float64), 50, 0.0)
-    assert centroid_rel_err(ref64[0], r.get_model().get_centroids()) < CENTROID_TOL[dt]
-    assert rel_close(r.get_objective_function_value(), ref64[2], OBJ_TOL)
+    if dt == np.float64:
+        assert (lab == z[f"labels_{tag}"]).all()
+        ref64 = restated.train(X, X[:20].copy(), 50, 0.0)
+        assert centroid_rel_err(ref64[0], C) < CENTROID_TOL[dt]
+        assert rel_close(r.get_objective_function_value(), ref64[2], OBJ_TOL)
+    else:
+        assert (lab != z[f"labels_{tag}"]).mean() < 1e-3
+        lab64, near = _fp64_gap_bound(X, C, dt)
+        assert ((lab == lab64) | near).all()
+        obj64 = restated.objective(X.astype(np.float64), C.astype(np.float64), lab)
+        assert rel_close(r.get_objective_function_value(), obj64, OBJ_TOL)
+        assert rel_close(r.get_objective_function_value(), float(z["obj_f64"]), 1e-5)
 
 
 def _fp64_gap_bound(X, C, dt):
