@@ -53,7 +53,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     if failed:
         raise RuntimeError(f"nvcc failed for: {failed}")
     if _needs(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs
         subprocess.check_call(cmd)
     return LIB
 

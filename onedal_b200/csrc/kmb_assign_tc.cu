@@ -468,12 +468,32 @@ void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, v
                                                                  cnorm_max, st);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point, so the library
+// does not link libcuda directly (it loads on hosts without a driver).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
 static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t dpad) {
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)dpad, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)dpad * 2};
     const cuuint32_t box[2] = {(cuuint32_t)tc::KP, 128u};
     const cuuint32_t estr[2] = {1u, 1u};
-    return cuTensorMapEncodeTiled(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
                                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
