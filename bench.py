@@ -216,6 +216,9 @@ def run_b200(args):
     ut = ctypes.c_double()
     ul = ctypes.c_int64()
     ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 2, ctypes.byref(ut), ctypes.byref(ul)))
+    ll = ctypes.c_int64()
+    ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 3, None, ctypes.byref(ll)))
+    gpu_launches = int(ll.value)
     ctx.check(ctx.lib.kmb_context_set_kernel_timing(ctx.handle, 0))
     if dist:
         t = torch.tensor([ms], device="cuda")
@@ -296,7 +299,7 @@ def run_b200(args):
                        "form": args.form, "iterations_completed": iters_done,
                        "l2": "inputs (10.24 GB) larger than L2; no flush"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": None, "clocks": clocks,
+            "gpu_launches": gpu_launches, "clocks": clocks,
             "plain_fp32_value": plain_value,
             "bf16_over_plain": (value / plain_value) if plain_value else None,
             "recheck_rows_last_iteration": st.rechecked_rows,

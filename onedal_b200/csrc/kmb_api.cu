@@ -28,6 +28,7 @@ struct kmb_context {
     int num_sms = 148;
     // kernel timing (kmb_context_set_kernel_timing)
     bool timing = false;
+    int64_t launches_at_enable = 0;
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used[3];
 
@@ -73,6 +74,11 @@ struct KernelTimer {
 };
 
 namespace kmb {
+
+int64_t &launch_count() {
+    static thread_local int64_t count = 0;
+    return count;
+}
 
 bool Workspace::ensure(DevBuf &b, size_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -190,6 +196,7 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
     cudaStream_t s = ctx->stream;
     kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
     reset_iteration_kernel<<<1, 1, 0, s>>>(st);
+    KMB_LAUNCHED();
     kmb::launch_prep_centroids_tc(C, k, d, ws.Chi.ptr, ws.Clo.ptr, (float *)ws.h.ptr, &sc->cnorm_max, st, s);
     int rc;
     {
@@ -202,6 +209,7 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
     kmb::launch_recheck<float>(X, n, d, C, k, (const RecheckEntry *)ws.queue.ptr, labels, d2,
                                (const float *)ws.xnorm.ptr, st, s);
     account_recheck_kernel<<<1, 1, 0, s>>>(st);
+    KMB_LAUNCHED();
     return KMB_OK;
 }
 
@@ -214,6 +222,7 @@ int assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, 
     const int64_t kpad = round_up(k, kBN);
     kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
     reset_iteration_kernel<<<1, 1, 0, s>>>(st);
+    KMB_LAUNCHED();
     kmb::launch_prep_centroids<F>(C, k, d, kpad, (F *)ws.Ct.ptr, (F *)ws.h.ptr, &sc->cnorm_max, st, s);
     {
         KernelTimer timer(ctx, 0);
@@ -225,6 +234,7 @@ int assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, 
         kmb::launch_recheck<F>(X, n, d, C, k, (const RecheckEntry *)ws.queue.ptr, labels, d2,
                                (const F *)ws.xnorm.ptr, st, s);
         account_recheck_kernel<<<1, 1, 0, s>>>(st);
+        KMB_LAUNCHED();
     }
     return KMB_OK;
 }
@@ -618,11 +628,18 @@ int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled) {
     cudaStreamSynchronize(ctx->stream);
     ctx->recycle_events();
     ctx->timing = enabled != 0;
+    ctx->launches_at_enable = kmb::launch_count();
     return KMB_OK;
 }
 
 int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int64_t *launches) {
-    if (!ctx || kernel < 0 || kernel > 2) return KMB_EINVAL;
+    if (!ctx || kernel < 0 || kernel > 3) return KMB_EINVAL;
+    if (kernel == 3) {
+        // every kernel launched by this thread since timing was enabled
+        if (total_ms) *total_ms = 0.0;
+        if (launches) *launches = kmb::launch_count() - ctx->launches_at_enable;
+        return KMB_OK;
+    }
     double tot = 0.0;
     for (auto &pr : ctx->ev_used[kernel]) {
         if (cudaEventSynchronize(pr.second) != cudaSuccess) return cuda_fail(ctx, cudaGetLastError(), "event");

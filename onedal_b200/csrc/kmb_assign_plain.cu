@@ -312,7 +312,9 @@ void launch_prep_centroids(const F *C, int64_t k, int64_t d, int64_t kpad, F *Ct
                            const LoopState *st, cudaStream_t s) {
     const int dpad = (int)((d + BK - 1) / BK * BK);
     reset_double_kernel<<<1, 1, 0, s>>>(cnorm_max, st);
+    KMB_LAUNCHED();
     prep_centroids_kernel<F><<<(unsigned)kpad, 128, 0, s>>>(C, (int)k, (int)d, dpad, (int)kpad, Ct, h, cnorm_max, st);
+    KMB_LAUNCHED();
 }
 
 template <typename F>
@@ -320,6 +322,7 @@ void launch_row_norms(const F *X, int64_t n, int64_t d, F *xnorm, double *xnorm_
     if (n == 0) return;
     const int64_t blocks = (n * 32 + 255) / 256;
     row_norms_kernel<F><<<(unsigned)blocks, 256, 0, s>>>(X, n, (int)d, xnorm, xnorm_max);
+    KMB_LAUNCHED();
 }
 
 template <typename F>
@@ -329,12 +332,15 @@ void launch_assign_plain(const F *X, int64_t n, int64_t d, const F *Ct, const F 
     if (n == 0) return;
     const unsigned blocks = (unsigned)((n + BM - 1) / BM);
     const bool vec = (d % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) % (4 * sizeof(F))) == 0);
-    if (vec)
+    if (vec) {
         assign_plain_kernel<F, true><<<blocks, NT, 0, s>>>(X, n, (int)d, Ct, h, (int)k, (int)kpad, xnorm, cnorm_max,
-                                                           labels, d2, queue, st);
-    else
+            labels, d2, queue, st);
+        KMB_LAUNCHED();
+    } else {
         assign_plain_kernel<F, false><<<blocks, NT, 0, s>>>(X, n, (int)d, Ct, h, (int)k, (int)kpad, xnorm, cnorm_max,
-                                                            labels, d2, queue, st);
+            labels, d2, queue, st);
+        KMB_LAUNCHED();
+    }
 }
 
 #define KMB_INST(F)                                                                                                \

@@ -457,15 +457,18 @@ void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *
     const int64_t total = rows * dpad;
     const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
     tc::split_rows_kernel<<<blocks, 256, 0, s>>>(X, rows, (int)d, (int)dpad, (__nv_bfloat16 *)hi, (__nv_bfloat16 *)lo);
+    KMB_LAUNCHED();
 }
 
 void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, void *Clo, float *h, double *cnorm_max,
                               const LoopState *st, cudaStream_t s) {
     const int64_t dpad = tc_dpad(d), kpad = tc_kpad(k);
     tc::reset_cmax_kernel<<<1, 1, 0, s>>>(cnorm_max, st);
+    KMB_LAUNCHED();
     tc::prep_centroids_tc_kernel<<<(unsigned)kpad, 128, 0, s>>>(C, (int)k, (int)d, (int)dpad, (int)kpad,
                                                                  (__nv_bfloat16 *)Chi, (__nv_bfloat16 *)Clo, h,
                                                                  cnorm_max, st);
+    KMB_LAUNCHED();
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point, so the library
@@ -546,6 +549,7 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
         return KMB_ECUDA;
     const int grid = (int)std::min<int64_t>(num_sms, p.n_tiles);
     tc::assign_tc_kernel<<<grid, 192, smem, s>>>(mXh, mXl, mCh, mCl, p);
+    KMB_LAUNCHED();
     return cudaGetLastError() == cudaSuccess ? KMB_OK : KMB_ECUDA;
 }
 

@@ -10,6 +10,11 @@
 
 namespace kmb {
 
+// Number of kernels this host thread has launched through the library (read by
+// kmb_context_kernel_time(ctx, 3, ...) for the launch count of a timed region).
+int64_t &launch_count();
+#define KMB_LAUNCHED() (++::kmb::launch_count())
+
 // Device-resident loop state. Every per-iteration kernel reads `done` first and
 // returns at once when it is set, so the whole Lloyd loop is enqueued without a
 // host round trip per iteration (the reference's GPU loop synchronises on the

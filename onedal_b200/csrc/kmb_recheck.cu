@@ -78,6 +78,7 @@ void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, con
                     int32_t *labels, F *d2, const F *xnorm, LoopState *st, cudaStream_t s) {
     (void)n;
     recheck_kernel<F><<<148 * 4, 256, 0, s>>>(X, (int)d, C, (int)k, queue, labels, d2, xnorm, st);
+    KMB_LAUNCHED();
 }
 
 template void launch_recheck<float>(const float *, int64_t, int64_t, const float *, int64_t, const RecheckEntry *,

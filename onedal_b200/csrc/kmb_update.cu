@@ -676,26 +676,39 @@ static void sort_and_sum_pieces(const void *Xv, size_t fsize, const UpdatePlan &
     const bool smem = k <= kSmemKMax;
     if (smem) {
         hist_smem_kernel<<<(unsigned)p.n_chunks, 256, sizeof(int) * k, s>>>(labels, p.n, k, p.chunk_rows, H, st);
+        KMB_LAUNCHED();
     } else {
         zero_i32_kernel<<<1184, 256, 0, s>>>(H, p.n_chunks * p.k, st);
+        KMB_LAUNCHED();
         hist_global_kernel<<<(unsigned)p.n_chunks, 256, 0, s>>>(labels, p.n, k, p.chunk_rows, H, st);
+        KMB_LAUNCHED();
     }
     const dim3 g2((unsigned)n_groups, (unsigned)((k + 255) / 256));
     scan_group_sum_kernel<<<g2, 256, 0, s>>>(H, p.n_chunks, k, Gs, st);
+    KMB_LAUNCHED();
     scan_groups_kernel<<<(unsigned)((k + 255) / 256), 256, 0, s>>>(Gs, n_groups, k, counts, st);
+    KMB_LAUNCHED();
     offsets_kernel<<<1, 1024, 0, s>>>(counts, k, p.piece_rows, offsets, piece_base, st);
+    KMB_LAUNCHED();
     scan_chunks_kernel<<<g2, 256, 0, s>>>(H, p.n_chunks, k, Gs, offsets, st);
-    if (smem)
+    KMB_LAUNCHED();
+    if (smem) {
         scatter_kernel<true><<<(unsigned)p.n_chunks, 32, sizeof(int) * k, s>>>(labels, p.n, k, p.chunk_rows, H, perm, st);
-    else
+        KMB_LAUNCHED();
+    } else {
         scatter_kernel<false><<<(unsigned)p.n_chunks, 32, 0, s>>>(labels, p.n, k, p.chunk_rows, H, perm, st);
+        KMB_LAUNCHED();
+    }
     double *records = (double *)ws.records.ptr;
-    if (fsize == sizeof(float))
+    if (fsize == sizeof(float)) {
         segsum_kernel<float><<<(unsigned)p.max_pieces, 128, 0, s>>>((const float *)Xv, (int)p.d, k, perm, offsets,
-                                                                    piece_base, p.piece_rows, records, st);
-    else
+            piece_base, p.piece_rows, records, st);
+        KMB_LAUNCHED();
+    } else {
         segsum_kernel<double><<<(unsigned)p.max_pieces, 128, 0, s>>>((const double *)Xv, (int)p.d, k, perm, offsets,
-                                                                     piece_base, p.piece_rows, records, st);
+            piece_base, p.piece_rows, records, st);
+        KMB_LAUNCHED();
+    }
 }
 
 template <typename F>
@@ -709,24 +722,35 @@ void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const
     finalize_kernel<F><<<k, 128, 0, s>>>((const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr,
                                          (const int64_t *)ws.piece_base.ptr, C_old, C_new, d, shift_part,
                                          empty_flag, st);
+    KMB_LAUNCHED();
     empties_kernel<<<1, 1024, 0, s>>>(empty_flag, k, empty_ids, shift_part, st);
+    KMB_LAUNCHED();
     // Reseeding: every kernel below returns at once unless some cluster is empty.
     SelState *ss = (SelState *)ws.sel_state.ptr;
     unsigned int *hist = (unsigned int *)ws.sel_hist.ptr;
     Cand *cand = (Cand *)ws.cand.ptr;
     sel_init_kernel<<<1, 256, 0, s>>>(ss, hist, st);
+    KMB_LAUNCHED();
     for (int shift = KeyOf<F>::BITS - 8; shift >= 0; shift -= 8) {
         sel_hist_kernel<F><<<592, 256, 0, s>>>(d2, p.n, shift, ss, hist, st);
+        KMB_LAUNCHED();
         sel_pick_kernel<<<1, 256, 0, s>>>(ss, hist, shift, st);
+        KMB_LAUNCHED();
     }
     sel_collect_kernel<F><<<1, 1024, 0, s>>>(d2, p.n, ss, cand, k, st);
+    KMB_LAUNCHED();
     sel_sort_kernel<<<1, 1024, 0, s>>>(cand, st);
+    KMB_LAUNCHED();
     reseed_apply_kernel<F><<<std::min(k, 1024), 128, 0, s>>>(X, d, cand, empty_ids, C_old, C_new, shift_part, st);
+    KMB_LAUNCHED();
     shift_total_kernel<<<1, 1024, 0, s>>>(shift_part, k, st);
+    KMB_LAUNCHED();
     if (commit) {
         commit_copy_kernel<F><<<std::max<int64_t>(1, std::min<int64_t>(1184, (p.k * p.d + 255) / 256)), 256, 0, s>>>(
             C_new, C_old, p.k * p.d, st);
+        KMB_LAUNCHED();
         decide_kernel<<<1, 1, 0, s>>>(st);
+        KMB_LAUNCHED();
     }
 }
 
@@ -736,13 +760,16 @@ void launch_partial_sums(const F *X, const UpdatePlan &p, const int32_t *labels,
     sort_and_sum_pieces(X, sizeof(F), p, labels, ws, nullptr, s);
     sums_kernel<<<(unsigned)p.k, 128, 0, s>>>((const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr,
                                              (const int64_t *)ws.piece_base.ptr, (int)p.d, sums, counts);
+    KMB_LAUNCHED();
 }
 
 template <typename F>
 void launch_objective(const F *X, int64_t n, int64_t d, const F *C, const int32_t *labels, double *partials,
                       double *out, cudaStream_t s) {
     objective_kernel<F><<<kObjectiveBlocks, 256, 0, s>>>(X, n, (int)d, C, labels, partials);
+    KMB_LAUNCHED();
     sum_partials_kernel<<<1, 32, 0, s>>>(partials, kObjectiveBlocks, out);
+    KMB_LAUNCHED();
 }
 
 #define KMB_INST(F)                                                                                                 \
