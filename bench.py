@@ -171,7 +171,7 @@ def run_b200(args):
     w = workloads.PRECISION
     form = _native.KMB_FORM_BF16X3 if args.form == "bf16x3" else _native.KMB_FORM_PLAIN
 
-    X, C0 = make_workload("cuda")
+    X, C0 = make_workload("cuda", n=args.rows)
     n, d = X.shape
     k = C0.shape[0]
     ctx = _native.context(local)
@@ -320,6 +320,8 @@ def main():
     ap.add_argument("--cpu-sample-rows", type=int, default=200_000)
     ap.add_argument("--traffic-bytes", type=float, default=None)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--rows", type=int, default=None,
+                    help="fewer rows of the same workload (profiling captures); default: the full 20M")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
