@@ -160,6 +160,27 @@ KMB_API int kmb_lloyd_iterate(kmb_context *ctx, int dtype, const void *X, int64_
 KMB_API int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled);
 KMB_API int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int64_t *launches);
 
+/* Responses (and, when objective != NULL, the exact objective) of n rows X
+ * against k centroids C, like kmb_infer with the plain form, for callers that
+ * cannot allocate device memory -- e.g. a plugin inside a framework that owns
+ * every device allocation, or a latency-bound loop that cannot pay for
+ * cudaMalloc/cudaFree. This entry point has no counterpart in the reference.
+ * Everything is device memory: X (n x d), C (k x d), responses (n int32),
+ * objective (one double). Kernels are enqueued on cuda_stream (a cudaStream_t,
+ * NULL = legacy default stream) and the call returns without waiting.
+ * It allocates nothing: its scratch is one fixed 24 MiB device array that the
+ * library holds on every GPU that loads it until the process exits. A call
+ * needs 2*n*sizeof(F) + kpad*dpad*sizeof(F) + kpad*sizeof(F) + 9728 bytes
+ * (kpad = k rounded up to 128, dpad = d rounded up to 8, each part rounded up
+ * to 256 bytes); bigger problems return KMB_EINVAL with a message on stderr.
+ * All calls on a device share the array, which keeps the last call's
+ * contents; calls that overlap on the GPU (other streams or host threads)
+ * race, so issue them on one stream. The first call on each device looks up
+ * the array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture on the device. */
+KMB_API int kmb_infer_noalloc(int dtype, const void *X, int64_t n, int64_t d, const void *C, int64_t k,
+                              int32_t *responses, double *objective, void *cuda_stream);
+
 /* Library version string. */
 KMB_API const char *kmb_version(void);
 

@@ -20,7 +20,7 @@ EXPORTED = (
     "kmb_context_create", "kmb_context_destroy", "kmb_context_set_stream", "kmb_context_last_error",
     "kmb_status_string", "kmb_context_release_workspace", "kmb_train", "kmb_infer", "kmb_lloyd_step",
     "kmb_partial_sums", "kmb_finalize_centroids", "kmb_version", "kmb_lloyd_iterate",
-    "kmb_context_set_kernel_timing", "kmb_context_kernel_time",
+    "kmb_context_set_kernel_timing", "kmb_context_kernel_time", "kmb_infer_noalloc",
 )
 
 
@@ -76,6 +76,7 @@ def load_library(path: str = LIB_PATH):
                                               ctypes.POINTER(I64), ctypes.POINTER(kmb_stats)]
             lib.kmb_context_set_kernel_timing.argtypes = [P, ctypes.c_int]
             lib.kmb_context_kernel_time.argtypes = [P, ctypes.c_int, ctypes.POINTER(D), ctypes.POINTER(I64)]
+            lib.kmb_infer_noalloc.argtypes = [ctypes.c_int, P, I64, I64, P, I64, P, P, P]
             _lib = lib
     return _lib
 

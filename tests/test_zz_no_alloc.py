@@ -1,0 +1,73 @@
+"""GPU test of kmb_infer_noalloc, the entry point for callers that cannot
+allocate device memory (a plugin whose host framework owns every device
+allocation, or a latency-bound loop that cannot pay for cudaMalloc/cudaFree).
+
+It is called through the C ABI twice in a row and must match kmb_infer (the
+allocating entry point) each time: responses exactly, the objective within the
+1e-6 relative tolerance the parity tests use. The file sorts last so that a run
+stopping at the first failure has already run every other test; it also passes
+on its own in a fresh process.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from onedal_b200 import _native
+
+pytestmark = pytest.mark.gpu
+
+OBJ_TOL = 1e-6
+
+
+def _infer_allocating(ctx, dtype, X, C):
+    n, d = X.shape
+    k = C.shape[0]
+    lab = torch.empty(n, dtype=torch.int32, device="cuda")
+    obj = ctypes.c_double()
+    ctx.check(ctx.lib.kmb_infer(ctx.handle, dtype, _native.KMB_MEM_DEVICE, X.data_ptr(), n, d, C.data_ptr(), k,
+                                _native.KMB_FORM_PLAIN, 1, lab.data_ptr(), ctypes.byref(obj), None))
+    return lab.cpu().numpy(), obj.value
+
+
+def _infer_noalloc(lib, dtype, X, C, stream):
+    n, d = X.shape
+    k = C.shape[0]
+    lab = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    obj = torch.zeros(1, dtype=torch.float64, device="cuda")
+    rc = lib.kmb_infer_noalloc(dtype, ctypes.c_void_p(X.data_ptr()), n, d, ctypes.c_void_p(C.data_ptr()), k,
+                               ctypes.c_void_p(lab.data_ptr()), ctypes.c_void_p(obj.data_ptr()),
+                               ctypes.c_void_p(stream.cuda_stream))
+    assert rc == _native.KMB_OK
+    stream.synchronize()
+    return lab.cpu().numpy(), float(obj.item())
+
+
+@pytest.mark.parametrize("torch_dtype,dtype", [(torch.float32, _native.KMB_F32), (torch.float64, _native.KMB_F64)])
+def test_noalloc_matches_allocating_infer_twice(torch_dtype, dtype):
+    g = torch.Generator(device="cpu").manual_seed(7)
+    n, d, k = 50_000, 40, 300
+    centres = torch.rand(k, d, generator=g, dtype=torch.float64) * 20 - 10
+    X = (centres[torch.randint(0, k, (n,), generator=g)] + torch.randn(n, d, generator=g, dtype=torch.float64))
+    X = X.to(torch_dtype).cuda()
+    C = X[:k].clone() + 0.25
+    ctx = _native.context(0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ref_lab, ref_obj = _infer_allocating(ctx, dtype, X, C)
+    lib = _native.load_library()
+    for _ in range(2):
+        lab, obj = _infer_noalloc(lib, dtype, X, C, stream)
+        np.testing.assert_array_equal(lab, ref_lab)
+        assert abs(obj - ref_obj) <= OBJ_TOL * abs(ref_obj)
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    lib = _native.load_library()
+    n, d, k = 4_000_000, 8, 16  # 2 * 4M * 4 bytes of row scratch alone exceeds the 24 MiB array
+    X = torch.zeros(1, dtype=torch.float32, device="cuda")  # never read: the size check comes first
+    lab = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = lib.kmb_infer_noalloc(_native.KMB_F32, ctypes.c_void_p(X.data_ptr()), n, d, ctypes.c_void_p(X.data_ptr()),
+                               k, ctypes.c_void_p(lab.data_ptr()), None, None)
+    assert rc == _native.KMB_EINVAL
