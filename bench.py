@@ -216,6 +216,9 @@ def run_b200(args):
     ut = ctypes.c_double()
     ul = ctypes.c_int64()
     ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 2, ctypes.byref(ut), ctypes.byref(ul)))
+    rt = ctypes.c_double()
+    rl = ctypes.c_int64()
+    ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 4, ctypes.byref(rt), ctypes.byref(rl)))
     ll = ctypes.c_int64()
     ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 3, None, ctypes.byref(ll)))
     gpu_launches = int(ll.value)
@@ -255,7 +258,8 @@ def run_b200(args):
                 "peak": peak, "unit": "TFLOP/s", "frac": (achieved_tflops / peak) if achieved_tflops else None,
                 "traffic": args.traffic_bytes, "peak_source": peak_note,
                 "kernel_ms_avg": avg_kernel_s * 1e3, "kernel_launches": kl.value,
-                "update_ms_avg": (ut.value / max(ul.value, 1)), "algorithmic_flops_per_launch": flops_per_launch,
+                "update_ms_avg": (ut.value / max(ul.value, 1)),
+                "recheck_ms_avg": (rt.value / max(rl.value, 1)) if rl.value else None, "algorithmic_flops_per_launch": flops_per_launch,
                 "algorithmic_bytes_per_launch": n * d * 4 + 4 * n}
 
     # e2e through the public API with pinned host buffers.

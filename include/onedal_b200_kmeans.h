@@ -154,9 +154,9 @@ KMB_API int kmb_lloyd_iterate(kmb_context *ctx, int dtype, const void *X, int64_
 /* Kernel timing: when enabled, CUDA events are recorded on the launching
  * stream around every launch of the dominant assignment kernel; the totals are
  * read (synchronising) with kmb_context_kernel_time and cleared by enabling
- * again. kernel: 0 = plain assignment, 1 = tensor-core assignment, 2 = update;
- * kernel 3 returns in *launches every kernel this host thread launched since
- * timing was enabled (total_ms = 0). */
+ * again. kernel: 0 = plain assignment, 1 = tensor-core assignment, 2 = update,
+ * 4 = FP64 near-tie recheck; kernel 3 returns in *launches every kernel this
+ * host thread launched since timing was enabled (total_ms = 0). */
 KMB_API int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled);
 KMB_API int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int64_t *launches);
 

@@ -30,7 +30,7 @@ struct kmb_context {
     bool timing = false;
     int64_t launches_at_enable = 0;
     std::vector<cudaEvent_t> ev_pool;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used[3];
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_used[5];
 
     cudaEvent_t take_event() {
         if (!ev_pool.empty()) {
@@ -206,8 +206,11 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
                                    (RecheckEntry *)ws.queue.ptr, st, ctx->num_sms, s);
     }
     if (rc != KMB_OK) return fail(ctx, rc, "tensor-core assignment launch failed (d=%lld)", (long long)d);
-    kmb::launch_recheck<float>(X, n, d, C, k, (const RecheckEntry *)ws.queue.ptr, labels, d2,
-                               (const float *)ws.xnorm.ptr, st, s);
+    {
+        KernelTimer timer(ctx, 4);
+        kmb::launch_recheck<float>(X, n, d, C, k, (const RecheckEntry *)ws.queue.ptr, labels, d2,
+                                   (const float *)ws.xnorm.ptr, st, s);
+    }
     account_recheck_kernel<<<1, 1, 0, s>>>(st);
     KMB_LAUNCHED();
     return KMB_OK;
@@ -231,6 +234,7 @@ int assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, 
                                     recheck ? (RecheckEntry *)ws.queue.ptr : nullptr, st, s);
     }
     if (recheck) {
+        KernelTimer timer(ctx, 4);
         kmb::launch_recheck<F>(X, n, d, C, k, (const RecheckEntry *)ws.queue.ptr, labels, d2,
                                (const F *)ws.xnorm.ptr, st, s);
         account_recheck_kernel<<<1, 1, 0, s>>>(st);
@@ -633,7 +637,7 @@ int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled) {
 }
 
 int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int64_t *launches) {
-    if (!ctx || kernel < 0 || kernel > 3) return KMB_EINVAL;
+    if (!ctx || kernel < 0 || kernel > 4) return KMB_EINVAL;
     if (kernel == 3) {
         // every kernel launched by this thread since timing was enabled
         if (total_ms) *total_ms = 0.0;

@@ -24,10 +24,16 @@
 //            SWIZZLE_128B), B = Chi/Clo panels of 128 clusters, ring of stages
 //   warp 1   TMEM allocation + single-thread tcgen05.mma issue; commits free
 //            B stages, publish accumulators and release A tiles
-//   warps 2-5 epilogue: tcgen05.ld of the 128x128 FP32 accumulator (one TMEM
-//            lane = one row per thread), running top-3 per row, outputs
-// Accumulators are double-buffered in TMEM so the epilogue of cluster tile j
-// overlaps the MMAs of tile j+1. Every mbarrier wait is bounded; on timeout the
+//   warps 2-9 epilogue, two groups of 4 warps: group g takes the cluster tiles
+//            whose running index is g mod 2, reads the 128x128 FP32 accumulator
+//            with tcgen05.ld (one TMEM lane = one row per thread), and keeps a
+//            running top-3 per row. Each 32-column chunk is first reduced to
+//            its minimum (branch-free, 3-input min); only chunks that beat the
+//            row's third-best score take the exact insertion path. At the end
+//            of a row tile group 1 hands its top-3 to group 0 through TMEM
+//            (columns 256..263), group 0 merges and writes the row's outputs.
+// The two accumulators alternate between the groups, so both epilogue groups
+// and the MMAs of the next cluster tile run concurrently. Every mbarrier wait is bounded; on timeout the
 // CTA records KMB_ETIMEDOUT in the loop state, drains its own TMA loads and
 // MMAs with bounded waits, frees TMEM and returns.
 #include "kmb_internal.cuh"
@@ -44,8 +50,10 @@ constexpr int BM = 128;                 // rows per tile (UMMA M)
 constexpr int BN = 128;                 // clusters per tile (UMMA N)
 constexpr int KP = 64;                  // bf16 per panel row (128 bytes, SWIZZLE_128B)
 constexpr int PANEL = 128 * 128;        // bytes per 128-row panel
-constexpr int NACC = 2;                 // TMEM accumulator buffers
-constexpr int TMEM_COLS = NACC * BN;    // 256
+constexpr int NACC = 2;                 // TMEM accumulator buffers (one per epilogue group)
+constexpr int TMEM_COLS = 512;          // 2 x 128 accumulator columns + the groups' exchange area
+constexpr int XCHG_COL = NACC * BN;     // 256: per-row top-3 handed from group 1 to group 0
+constexpr int NTHREADS = 320;           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two groups of 4)
 constexpr int MAX_B_STAGES = 8;
 constexpr long long kTimeoutCycles = 4000000000ll;  // ~2 s at 1.9 GHz
 
@@ -174,7 +182,71 @@ struct Top3 {
     int ib, is;
 };
 
-__global__ void __launch_bounds__(192, 1)
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+__device__ __forceinline__ void named_bar_sync(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// (value, index) order; indices kept for the first two places.
+__device__ __forceinline__ bool lex_lt(float a, int ia, float b, int ib) { return a < b || (a == b && ia < ib); }
+
+__device__ __forceinline__ Top3 top3_merge(const Top3 &x, const Top3 &y) {
+    const float xv[3] = {x.b, x.s, x.t}, yv[3] = {y.b, y.s, y.t};
+    const int xi[3] = {x.ib, x.is, 0x7fffffff}, yi[3] = {y.ib, y.is, 0x7fffffff};
+    float ov[3];
+    int oi[3];
+    int a = 0, b = 0;
+#pragma unroll
+    for (int o = 0; o < 3; ++o) {  // a + b == o <= 2, so a, b < 3
+        if (lex_lt(xv[a], xi[a], yv[b], yi[b])) {
+            ov[o] = xv[a];
+            oi[o] = xi[a];
+            ++a;
+        } else {
+            ov[o] = yv[b];
+            oi[o] = yi[b];
+            ++b;
+        }
+    }
+    Top3 r;
+    r.b = ov[0];
+    r.s = ov[1];
+    r.t = ov[2];
+    r.ib = oi[0];
+    r.is = oi[1];
+    return r;
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const Top3 &r) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+        "r"(__float_as_uint(r.b)), "r"(__float_as_uint(r.s)), "r"(__float_as_uint(r.t)), "r"((uint32_t)r.ib),
+        "r"((uint32_t)r.is), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ Top3 tmem_ld8(uint32_t taddr) {
+    uint32_t q[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    Top3 r;
+    r.b = __uint_as_float(q[0]);
+    r.s = __uint_as_float(q[1]);
+    r.t = __uint_as_float(q[2]);
+    r.ib = (int)q[3];
+    r.is = (int)q[4];
+    return r;
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1)
 assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant__ CUtensorMap tmXl,
                  const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl, Params p) {
     // One read of the loop flag for the whole CTA, so every thread takes the same path.
@@ -305,48 +377,68 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             mbar_drain(&bar->mma_done, 0);
         }
     } else {
-        // ---------------- epilogue (warps 2..5) ----------------
-        const int quarter = warp & 3;  // TMEM lanes 32*quarter .. +31
+        // ---------------- epilogue (warps 2..9, two groups) ----------------
+        const int quarter = warp & 3;          // TMEM lanes 32*quarter .. +31
+        const int group = (warp - 2) >> 2;     // 0: warps 2-5, 1: warps 6-9
         const int row_in_tile = quarter * 32 + lane;
+        const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
         const double u = 5.9604644775390625e-8;  // 2^-24
         const double ub2 = 1.52587890625e-5;      // 2^-16
         const double cmax = *p.cnorm_max;
         long long acount = 0;
         bool ok = true;
-        for (int lt = 0; lt < my_tiles && ok; ++lt) {
+        // Both groups pass the same number of named barriers (one per row tile),
+        // also after an abort, so neither can be left waiting on the other.
+        for (int lt = 0; lt < my_tiles; ++lt) {
             const int tile = blockIdx.x + lt * gridDim.x;
             Top3 r;
             r.b = r.s = r.t = __int_as_float(0x7f800000);
             r.ib = r.is = 0;
             for (int j = 0; j < p.ntiles_n; ++j, ++acount) {
-                const int slot = (int)(acount % NACC);
-                const int use = (int)(acount / NACC);
-                if (!mbar_wait(&bar->acc_full[slot], use & 1, abort)) { ok = false; break; }
+                if ((int)(acount & 1) != group || !ok) continue;
+                const int slot = group;
+                const int use = (int)(acount >> 1);
+                // every lane waits; the warp proceeds only if all lanes saw completion
+                if (!__all_sync(0xffffffffu, mbar_wait(&bar->acc_full[slot], use & 1, abort))) {
+                    ok = false;
+                    continue;
+                }
                 tc_fence_after();
                 const float *hj = p.h + j * BN;
 #pragma unroll 1
                 for (int c0 = 0; c0 < BN; c0 += 32) {
                     float v[32];
-                    tmem_ld32(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(slot * BN + c0), v);
+                    tmem_ld32(lane_base + (uint32_t)(slot * BN + c0), v);
 #pragma unroll
                     for (int i = 0; i < 32; i += 4) {
                         const float4 h4 = __ldg(reinterpret_cast<const float4 *>(hj + c0 + i));
-                        const float sc[4] = {h4.x - v[i], h4.y - v[i + 1], h4.z - v[i + 2], h4.w - v[i + 3]};
+                        v[i] = h4.x - v[i];
+                        v[i + 1] = h4.y - v[i + 1];
+                        v[i + 2] = h4.z - v[i + 2];
+                        v[i + 3] = h4.w - v[i + 3];
+                    }
+                    float m[11];
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const float x = sc[q];
+                    for (int i = 0; i < 10; ++i) m[i] = min3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+                    m[10] = fminf(v[30], v[31]);
+                    const float m1 = min3f(min3f(m[0], m[1], m[2]), min3f(m[3], m[4], m[5]),
+                                           min3f(m[6], m[7], min3f(m[8], m[9], m[10])));
+                    if (m1 < r.t) {
+                        const int colbase = j * BN + c0;
+#pragma unroll
+                        for (int i = 0; i < 32; ++i) {
+                            const float x = v[i];
                             if (x < r.t) {
-                                const int col = j * BN + c0 + i + q;
                                 if (x < r.b) {
                                     r.t = r.s;
                                     r.s = r.b;
                                     r.is = r.ib;
                                     r.b = x;
-                                    r.ib = col;
+                                    r.ib = colbase + i;
                                 } else if (x < r.s) {
                                     r.t = r.s;
                                     r.s = x;
-                                    r.is = col;
+                                    r.is = colbase + i;
                                 } else {
                                     r.t = x;
                                 }
@@ -358,7 +450,18 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&bar->acc_empty[slot]);
             }
-            if (!ok) break;
+            // Group 1 hands its top-3 to group 0 through TMEM columns XCHG_COL..+7 of
+            // the same lanes (alternating by row-tile parity), then group 0 merges.
+            const uint32_t xaddr = lane_base + (uint32_t)(XCHG_COL + 8 * (lt & 1));
+            if (group == 1) {
+                tmem_st8(xaddr, r);
+                tc_fence_before();
+            }
+            named_bar_sync(1 + quarter, 64);
+            if (group == 1 || !ok) continue;
+            tc_fence_after();
+            const Top3 o = tmem_ld8(xaddr);
+            r = top3_merge(r, o);
             const int64_t row = (int64_t)tile * BM + row_in_tile;
             if (row < p.n) {
                 p.labels[row] = r.ib;
@@ -548,7 +651,7 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
         cudaSuccess)
         return KMB_ECUDA;
     const int grid = (int)std::min<int64_t>(num_sms, p.n_tiles);
-    tc::assign_tc_kernel<<<grid, 192, smem, s>>>(mXh, mXl, mCh, mCl, p);
+    tc::assign_tc_kernel<<<grid, tc::NTHREADS, smem, s>>>(mXh, mXl, mCh, mCl, p);
     KMB_LAUNCHED();
     return cudaGetLastError() == cudaSuccess ? KMB_OK : KMB_ECUDA;
 }

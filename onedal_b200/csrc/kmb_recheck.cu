@@ -77,7 +77,7 @@ template <typename F>
 void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, const RecheckEntry *queue,
                     int32_t *labels, F *d2, const F *xnorm, LoopState *st, cudaStream_t s) {
     (void)n;
-    recheck_kernel<F><<<148 * 4, 256, 0, s>>>(X, (int)d, C, (int)k, queue, labels, d2, xnorm, st);
+    recheck_kernel<F><<<148 * 8, 256, 0, s>>>(X, (int)d, C, (int)k, queue, labels, d2, xnorm, st);
     KMB_LAUNCHED();
 }
 
