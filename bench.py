@@ -150,6 +150,112 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def run_serving(args, device=0):
+    """Serving form: 64 resident centroid sets, a Poisson stream of infer (90%) and small
+    train (10%) requests; saturation throughput, then p50/p99 latency at fractions of it."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    from onedal_b200.serving import KMeansServer
+
+    rng = np.random.default_rng(1005)
+    n_models = 64
+    ks = np.exp(rng.uniform(np.log(16), np.log(4096), n_models)).astype(int)
+    ds = rng.choice([32, 64, 128, 256], n_models)
+    models = [rng.uniform(-1, 1, (int(k), int(d))).astype(np.float32) for k, d in zip(ks, ds)]
+    pool_rows = 1 << 20
+    pools = {}
+    for dd in (32, 64, 128, 256):  # pinned N(0,1) rows per width; request rows are contiguous slices
+        t = torch.empty((pool_rows, dd), dtype=torch.float32, pin_memory=True)
+        t.normal_(generator=torch.Generator().manual_seed(dd))
+        pools[dd] = (t, t.numpy())
+    # small-train datasets (Gaussian mixtures), reused by the train requests
+    trains = []
+    for i in range(8):
+        k = int(rng.integers(2, 65))
+        d = int(rng.choice([32, 64, 128, 256]))
+        n = int(rng.integers(max(k, 5000), 50_001))
+        c = rng.uniform(-10, 10, (k, d))
+        X = (c[rng.integers(0, k, n)] + rng.standard_normal((n, d))).astype(np.float32)
+        trains.append((X, X[:k].copy()))
+
+    def make_requests(count, seed):
+        g = np.random.default_rng(seed)
+        out = []
+        for _ in range(count):
+            if g.random() < 0.9:
+                m = int(g.integers(0, n_models))
+                n = int(min(1_000_000, max(1, round(g.lognormal(np.log(4096), 1.5)))))
+                d = models[m].shape[1]
+                off = int(g.integers(0, pool_rows - n + 1))
+                out.append(("infer", m, pools[d][1][off:off + n]))
+            else:
+                out.append(("train", int(g.integers(0, len(trains))), None))
+        return out
+
+    def submit(srv, ids, req):
+        kind, m, X = req
+        if kind == "infer":
+            return srv.submit_infer(ids[m], X)
+        Xt, C0 = trains[m]
+        return srv.submit_train(Xt, C0, 15)
+
+    def run_point(srv, ids, reqs, rate):
+        """rate=None: everything at t=0 (saturation); else Poisson arrivals at `rate` per s."""
+        g = np.random.default_rng(77)
+        handles = [None] * len(reqs)
+        lat = {}
+        done = threading.Event()
+
+        def collector():
+            for i in range(len(reqs)):
+                while handles[i] is None:
+                    time.sleep(0.0001)
+                _, l = srv.wait(handles[i], timeout=600)
+                lat[i] = l
+            done.set()
+
+        prepared = reqs
+        th = threading.Thread(target=collector)
+        th.start()
+        t0 = time.perf_counter()
+        t_next = t0
+        for i, req in enumerate(prepared):
+            if rate:
+                t_next += g.exponential(1.0 / rate)
+                while time.perf_counter() < t_next:
+                    pass
+            handles[i] = submit(srv, ids, req)
+        done.wait()
+        t1 = time.perf_counter()
+        th.join()
+        inf = [lat[i] for i, r in enumerate(reqs) if r[0] == "infer"]
+        return {"requests": len(reqs), "seconds": t1 - t0, "throughput_rps": len(reqs) / (t1 - t0),
+                "p50_ms": float(np.percentile(inf, 50) * 1e3), "p99_ms": float(np.percentile(inf, 99) * 1e3),
+                "train_p50_ms": float(np.percentile([lat[i] for i, r in enumerate(reqs) if r[0] == "train"] or [0],
+                                                    50) * 1e3)}
+
+    with KMeansServer(device=device, hbm_budget_bytes=60 << 30, lanes=4, trainers=6) as srv:
+        ids = [srv.add_model(C) for C in models]
+        run_point(srv, ids, make_requests(200, 1), None)  # warm-up
+        sat = run_point(srv, ids, make_requests(args.serving_requests, 2), None)
+        points = []
+        for frac in (0.5, 0.8):
+            rate = frac * sat["throughput_rps"]
+            pt = run_point(srv, ids, make_requests(args.serving_requests, 3 + int(frac * 10)), rate)
+            pt["offered_rps"] = rate
+            pt["fraction_of_saturation"] = frac
+            points.append(pt)
+        st = srv.stats()
+    return {"saturation_rps": sat["throughput_rps"], "saturation_p99_ms": sat["p99_ms"], "points": points,
+            "models": n_models, "budget_bytes": 60 << 30, "lanes": 4, "trainers": 6,
+            "mean_requests_per_batch": st["batched_requests"] / max(st["batches"], 1),
+            "peak_in_use_bytes": st["peak_in_use_bytes"],
+            "note": "p50/p99 = host submit->completion of infer requests; rows from a pinned pool"}
+
+
 def run_b200(args):
     import ctypes
 
@@ -292,6 +398,12 @@ def run_b200(args):
                    "sample": f"first {ns} of {n} rows, {it} Lloyd iterations of the reference DAAL kernel "
                              f"(OpenBLAS sgemm, std::thread shim), per-iteration time scaled by rows"}
 
+    serving = None
+    if rank == 0 and world == 1 and args.serving_requests > 0:
+        del X
+        torch.cuda.empty_cache()
+        serving = run_serving(args, local)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value * (world if False else 1), "unit": UNIT, "n_gpus": world,
@@ -307,6 +419,7 @@ def run_b200(args):
             "plain_fp32_value": plain_value,
             "bf16_over_plain": (value / plain_value) if plain_value else None,
             "recheck_rows_last_iteration": st.rechecked_rows,
+            "serving": serving,
         }
         print(json.dumps(line))
     if dist:
@@ -324,6 +437,8 @@ def main():
     ap.add_argument("--cpu-sample-rows", type=int, default=200_000)
     ap.add_argument("--traffic-bytes", type=float, default=None)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--serving-requests", type=int, default=3000,
+                    help="requests per serving load point (0 skips the serving measurement)")
     ap.add_argument("--rows", type=int, default=None,
                     help="fewer rows of the same workload (profiling captures); default: the full 20M")
     args = ap.parse_args()

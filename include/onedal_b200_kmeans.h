@@ -181,6 +181,44 @@ KMB_API int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_
 KMB_API int kmb_infer_noalloc(int dtype, const void *X, int64_t n, int64_t d, const void *C, int64_t k,
                               int32_t *responses, double *objective, void *cuda_stream);
 
+/* ---- Serving loop ---------------------------------------------------------
+ * No counterpart in the reference (its API is one synchronous call per
+ * train/infer). A server keeps fitted centroid sets resident on one GPU, admits
+ * requests under an HBM byte budget, and batches every admissible pending
+ * infer request into one grouped launch per free lane (CUDA stream), so
+ * requests that arrive while others run are picked up by the next free lane and
+ * their work overlaps on the device. Small train requests run on trainer
+ * threads, each with its own context. Responses are identical to kmb_infer /
+ * kmb_train (plain form) on the same inputs. Host buffers passed to submit_*
+ * must stay valid until the request is waited for; pinned host memory gives
+ * the lowest latency. Thread-safe. */
+typedef struct kmb_server_stats {
+    int64_t completed;
+    int64_t failed;
+    int64_t batches;          /* grouped infer launches */
+    int64_t batched_requests; /* infer requests over all batches */
+    int64_t pending;
+    int64_t in_use_bytes;
+    int64_t peak_in_use_bytes;
+    int64_t budget_bytes;
+} kmb_server_stats;
+
+KMB_API int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32_t trainers, void **server);
+/* Waits for all admitted work, then releases everything. */
+KMB_API int kmb_server_destroy(void *server);
+/* Makes a fitted centroid set (k x d float32, host) resident; returns its id. */
+KMB_API int kmb_server_add_model(void *server, const float *C, int64_t k, int64_t d, int32_t *model_id);
+/* Responses of n rows (n x d float32, host) against a resident model. */
+KMB_API int kmb_server_submit_infer(void *server, int32_t model_id, const float *X, int64_t n, int64_t d,
+                                    int32_t *responses, int64_t *request_id);
+/* A small train (plain form, eps 0, exactly up to `iterations` Lloyd updates). */
+KMB_API int kmb_server_submit_train(void *server, const float *X, int64_t n, int64_t d, const float *C0, int64_t k,
+                                    int64_t iterations, float *C_out, int32_t *responses, int64_t *request_id);
+/* Waits up to timeout_s (< 0: no limit) for a request; returns its status or
+ * KMB_ETIMEDOUT; latency_s = submit -> completion on the host clock. */
+KMB_API int kmb_server_wait(void *server, int64_t request_id, double timeout_s, double *latency_s);
+KMB_API int kmb_server_get_stats(void *server, kmb_server_stats *stats);
+
 /* Library version string. */
 KMB_API const char *kmb_version(void);
 

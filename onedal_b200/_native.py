@@ -21,7 +21,15 @@ EXPORTED = (
     "kmb_status_string", "kmb_context_release_workspace", "kmb_train", "kmb_infer", "kmb_lloyd_step",
     "kmb_partial_sums", "kmb_finalize_centroids", "kmb_version", "kmb_lloyd_iterate",
     "kmb_context_set_kernel_timing", "kmb_context_kernel_time", "kmb_infer_noalloc",
+    "kmb_server_create", "kmb_server_destroy", "kmb_server_add_model", "kmb_server_submit_infer",
+    "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats",
 )
+
+
+class kmb_server_stats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("batches", ctypes.c_int64),
+                ("batched_requests", ctypes.c_int64), ("pending", ctypes.c_int64), ("in_use_bytes", ctypes.c_int64),
+                ("peak_in_use_bytes", ctypes.c_int64), ("budget_bytes", ctypes.c_int64)]
 
 
 class kmb_params(ctypes.Structure):
@@ -77,6 +85,13 @@ def load_library(path: str = LIB_PATH):
             lib.kmb_context_set_kernel_timing.argtypes = [P, ctypes.c_int]
             lib.kmb_context_kernel_time.argtypes = [P, ctypes.c_int, ctypes.POINTER(D), ctypes.POINTER(I64)]
             lib.kmb_infer_noalloc.argtypes = [ctypes.c_int, P, I64, I64, P, I64, P, P, P]
+            lib.kmb_server_create.argtypes = [ctypes.c_int, I64, I32, I32, ctypes.POINTER(P)]
+            lib.kmb_server_destroy.argtypes = [P]
+            lib.kmb_server_add_model.argtypes = [P, P, I64, I64, ctypes.POINTER(I32)]
+            lib.kmb_server_submit_infer.argtypes = [P, I32, P, I64, I64, P, ctypes.POINTER(I64)]
+            lib.kmb_server_submit_train.argtypes = [P, P, I64, I64, P, I64, I64, P, P, ctypes.POINTER(I64)]
+            lib.kmb_server_wait.argtypes = [P, I64, D, ctypes.POINTER(D)]
+            lib.kmb_server_get_stats.argtypes = [P, ctypes.c_void_p]
             _lib = lib
     return _lib
 

@@ -408,6 +408,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
 #pragma unroll 1
                 for (int c0 = 0; c0 < BN; c0 += 32) {
                     float v[32];
+                    __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the filtered path
                     tmem_ld32(lane_base + (uint32_t)(slot * BN + c0), v);
 #pragma unroll
                     for (int i = 0; i < 32; i += 4) {
@@ -453,6 +454,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             // Group 1 hands its top-3 to group 0 through TMEM columns XCHG_COL..+7 of
             // the same lanes (alternating by row-tile parity), then group 0 merges.
             const uint32_t xaddr = lane_base + (uint32_t)(XCHG_COL + 8 * (lt & 1));
+            __syncwarp();
             if (group == 1) {
                 tmem_st8(xaddr, r);
                 tc_fence_before();

@@ -1,0 +1,494 @@
+// Serving loop: fitted centroid sets stay resident in HBM; infer and small
+// train requests of different n, k and d are admitted under an HBM budget and
+// batched, as they arrive, into shared launches on several streams.
+//
+// Structure (host, C++):
+//  * models   -- centroids plus their prepared transposed copy and half norms,
+//                kept on the device for the server's lifetime;
+//  * admission -- a request is admitted when its device bytes fit in the budget
+//                next to everything in flight; otherwise it waits, in FIFO
+//                order, until completions free memory;
+//  * lanes    -- L CUDA streams. The scheduler thread fills a free lane with
+//                every admissible pending infer request (continuous batching:
+//                requests that arrived while earlier batches run are picked up
+//                by the next free lane), uploads their rows, runs one grouped
+//                assignment launch over all of them (kmb_serve_kernels.cu) and
+//                copies the labels back; a host callback on the stream marks the
+//                batch complete and returns its memory to the budget. Batches on
+//                different lanes overlap on the device;
+//  * trainers -- small train requests run on worker threads, each with its own
+//                kmb_context (stream + workspace), concurrently with the lanes.
+// Latency is measured on the host from submit to completion (steady_clock).
+#include "kmb_internal.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <new>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace kmb {
+void launch_grouped_infer(const void *reqs_dev, int nreq, long long n_items, long long total_rows, cudaStream_t s);
+size_t grouped_desc_bytes();
+int grouped_chunk_clusters();
+namespace serve {
+struct ReqDesc {
+    const float *X;
+    const float *Ct;
+    const float *h;
+    unsigned long long *key;
+    int32_t *labels;
+    long long n;
+    int d, k, kpad, chunks;
+    long long item_begin;
+    long long row_begin;
+};
+}  // namespace serve
+}  // namespace kmb
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+enum ReqState { PENDING = 0, RUNNING = 1, DONE = 2, FAILED = 3 };
+enum ReqKind { INFER = 0, TRAIN = 1 };
+
+struct Model {
+    int64_t k, d, kpad, dpad;
+    float *C = nullptr, *Ct = nullptr, *h = nullptr;
+};
+
+struct Request {
+    int64_t id;
+    int kind;
+    int model;
+    int64_t n, d, k, iters;
+    const float *X;
+    const float *C0;
+    int32_t *labels_out;
+    float *C_out;
+    size_t bytes;
+    int state = PENDING;
+    int rc = KMB_OK;
+    Clock::time_point t_submit, t_done;
+    // device buffers while running (infer)
+    float *dX = nullptr;
+    unsigned long long *dkey = nullptr;
+    int32_t *dlab = nullptr;
+};
+
+struct Lane;
+
+struct Server {
+    int device = 0;
+    size_t budget = 0;
+    size_t in_use = 0, peak_in_use = 0;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Request *> pending;      // infer, FIFO
+    std::deque<Request *> train_queue;  // train, FIFO
+    std::unordered_map<int64_t, Request *> all;
+    std::vector<Model> models;
+    std::vector<Lane *> lanes;
+    std::vector<std::thread> threads;
+    bool stop = false;
+    int64_t next_id = 1;
+    int64_t batches = 0, batched_requests = 0, completed = 0, failed = 0;
+    int64_t max_batch_rows = 1 << 22;
+    Clock::time_point t0 = Clock::now();
+};
+
+struct Lane {
+    Server *srv;
+    cudaStream_t stream = nullptr;
+    bool busy = false;
+    std::vector<Request *> batch;
+    kmb::serve::ReqDesc *h_desc = nullptr;  // pinned
+    void *d_desc = nullptr;
+    int cap = 0;
+};
+
+size_t infer_bytes(int64_t n, int64_t d) { return (size_t)n * d * 4 + (size_t)n * 8 + (size_t)n * 4 + 4096; }
+size_t train_bytes(int64_t n, int64_t d, int64_t k) {
+    // rows + the context workspace of a small train (labels, sort buffers, records)
+    return (size_t)n * d * 4 + (size_t)n * 40 + (size_t)k * d * 64 + (size_t)(n / 512 + k) * d * 8 + (8u << 20);
+}
+
+void CUDART_CB batch_done(void *arg) {
+    Lane *lane = (Lane *)arg;
+    Server *srv = lane->srv;
+    const auto now = Clock::now();
+    std::lock_guard<std::mutex> lock(srv->mu);
+    for (Request *r : lane->batch) {
+        r->t_done = now;
+        r->state = r->rc == KMB_OK ? DONE : FAILED;
+        srv->in_use -= r->bytes;
+        srv->completed += 1;
+        if (r->rc != KMB_OK) srv->failed += 1;
+    }
+    lane->batch.clear();
+    lane->busy = false;
+    srv->cv.notify_all();
+}
+
+// Runs on the scheduler thread with the server lock released.
+int launch_batch(Server *srv, Lane *lane) {
+    cudaStream_t s = lane->stream;
+    const int nreq = (int)lane->batch.size();
+    if (nreq > lane->cap) {
+        if (lane->h_desc) cudaFreeHost(lane->h_desc);
+        if (lane->d_desc) cudaFree(lane->d_desc);
+        lane->cap = std::max(nreq, 2 * lane->cap);
+        lane->h_desc = nullptr;
+        lane->d_desc = nullptr;
+        if (cudaMallocHost(&lane->h_desc, sizeof(kmb::serve::ReqDesc) * lane->cap) != cudaSuccess ||
+            cudaMalloc(&lane->d_desc, sizeof(kmb::serve::ReqDesc) * lane->cap) != cudaSuccess) {
+            cudaGetLastError();
+            lane->cap = 0;
+            return KMB_ENOMEM;
+        }
+    }
+    const int chunk = kmb::grouped_chunk_clusters();
+    long long items = 0, rows = 0;
+    for (int i = 0; i < nreq; ++i) {
+        Request *r = lane->batch[i];
+        const Model &m = srv->models[r->model];
+        if (cudaMallocAsync((void **)&r->dX, sizeof(float) * r->n * r->d, s) != cudaSuccess ||
+            cudaMallocAsync((void **)&r->dkey, sizeof(unsigned long long) * r->n, s) != cudaSuccess ||
+            cudaMallocAsync((void **)&r->dlab, sizeof(int32_t) * r->n, s) != cudaSuccess) {
+            cudaGetLastError();
+            return KMB_ENOMEM;
+        }
+        cudaMemcpyAsync(r->dX, r->X, sizeof(float) * r->n * r->d, cudaMemcpyHostToDevice, s);
+        kmb::serve::ReqDesc &q = lane->h_desc[i];
+        q.X = r->dX;
+        q.Ct = m.Ct;
+        q.h = m.h;
+        q.key = r->dkey;
+        q.labels = r->dlab;
+        q.n = r->n;
+        q.d = (int)r->d;
+        q.k = (int)m.k;
+        q.kpad = (int)m.kpad;
+        q.chunks = (int)((m.kpad + chunk - 1) / chunk);
+        q.item_begin = items;
+        q.row_begin = rows;
+        items += ((r->n + 127) / 128) * q.chunks;
+        rows += r->n;
+    }
+    cudaMemcpyAsync(lane->d_desc, lane->h_desc, sizeof(kmb::serve::ReqDesc) * nreq, cudaMemcpyHostToDevice, s);
+    kmb::launch_grouped_infer(lane->d_desc, nreq, items, rows, s);
+    for (Request *r : lane->batch) {
+        cudaMemcpyAsync(r->labels_out, r->dlab, sizeof(int32_t) * r->n, cudaMemcpyDeviceToHost, s);
+        cudaFreeAsync(r->dX, s);
+        cudaFreeAsync(r->dkey, s);
+        cudaFreeAsync(r->dlab, s);
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        for (Request *r : lane->batch) r->rc = KMB_ECUDA;
+    }
+    cudaLaunchHostFunc(s, batch_done, lane);
+    return KMB_OK;
+}
+
+void scheduler_loop(Server *srv) {
+    cudaSetDevice(srv->device);
+    std::unique_lock<std::mutex> lock(srv->mu);
+    while (true) {
+        Lane *lane = nullptr;
+        srv->cv.wait(lock, [&] {
+            if (srv->stop) return true;
+            if (srv->pending.empty()) return false;
+            for (Lane *l : srv->lanes)
+                if (!l->busy) {
+                    lane = l;
+                    break;
+                }
+            if (!lane) return false;
+            // admission of at least the head request
+            return srv->in_use + srv->pending.front()->bytes <= srv->budget || srv->in_use == 0;
+        });
+        if (srv->stop) break;
+        // Continuous batching: take every admissible pending request (FIFO).
+        int64_t rows = 0;
+        while (!srv->pending.empty()) {
+            Request *r = srv->pending.front();
+            if (srv->in_use + r->bytes > srv->budget && !(srv->in_use == 0 && lane->batch.empty())) break;
+            if (!lane->batch.empty() && rows + r->n > srv->max_batch_rows) break;
+            srv->pending.pop_front();
+            r->state = RUNNING;
+            srv->in_use += r->bytes;
+            srv->peak_in_use = std::max(srv->peak_in_use, srv->in_use);
+            rows += r->n;
+            lane->batch.push_back(r);
+        }
+        if (lane->batch.empty()) continue;
+        lane->busy = true;
+        srv->batches += 1;
+        srv->batched_requests += (int64_t)lane->batch.size();
+        lock.unlock();
+        const int rc = launch_batch(srv, lane);
+        if (rc != KMB_OK) {
+            // Release what was allocated and complete the batch as failed, in stream order.
+            for (Request *r : lane->batch) {
+                r->rc = rc;
+                if (r->dX) cudaFreeAsync(r->dX, lane->stream);
+                if (r->dkey) cudaFreeAsync(r->dkey, lane->stream);
+                if (r->dlab) cudaFreeAsync(r->dlab, lane->stream);
+            }
+            cudaLaunchHostFunc(lane->stream, batch_done, lane);
+        }
+        lock.lock();
+    }
+}
+
+void trainer_loop(Server *srv) {
+    cudaSetDevice(srv->device);
+    kmb_context *ctx = nullptr;
+    if (kmb_context_create(srv->device, &ctx) != KMB_OK) ctx = nullptr;
+    std::unique_lock<std::mutex> lock(srv->mu);
+    while (true) {
+        srv->cv.wait(lock, [&] {
+            if (srv->stop) return true;
+            if (srv->train_queue.empty()) return false;
+            return srv->in_use + srv->train_queue.front()->bytes <= srv->budget || srv->in_use == 0;
+        });
+        if (srv->stop) break;
+        Request *r = srv->train_queue.front();
+        srv->train_queue.pop_front();
+        r->state = RUNNING;
+        srv->in_use += r->bytes;
+        srv->peak_in_use = std::max(srv->peak_in_use, srv->in_use);
+        lock.unlock();
+        int rc = KMB_ECUDA;
+        if (ctx) {
+            kmb_params p{r->k, r->iters, 0.0, KMB_FORM_PLAIN, 0};
+            double obj = 0.0;
+            int64_t it = 0;
+            rc = kmb_train(ctx, KMB_F32, KMB_MEM_HOST, r->X, r->n, r->d, r->C0, &p, r->C_out, r->labels_out, &obj,
+                           &it, nullptr);
+        }
+        lock.lock();
+        r->rc = rc;
+        r->t_done = Clock::now();
+        r->state = rc == KMB_OK ? DONE : FAILED;
+        srv->in_use -= r->bytes;
+        srv->completed += 1;
+        if (rc != KMB_OK) srv->failed += 1;
+        srv->cv.notify_all();
+    }
+    lock.unlock();
+    if (ctx) kmb_context_destroy(ctx);
+}
+
+__global__ void prep_model_kernel(const float *__restrict__ C, int k, int d, int dpad, int kpad, float *__restrict__ Ct,
+                                  float *__restrict__ h) {
+    const int j = blockIdx.x;
+    double s = 0.0;
+    for (int t = 0; t < dpad; ++t) {
+        const float v = (j < k && t < d) ? C[(int64_t)j * d + t] : 0.f;
+        Ct[(int64_t)t * kpad + j] = v;
+        s += (double)v * (double)v;
+    }
+    h[j] = j < k ? (float)(0.5 * s) : __int_as_float(0x7f800000);
+}
+
+}  // namespace
+
+extern "C" {
+
+int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32_t trainers, void **out) {
+    if (!out || hbm_budget_bytes <= 0 || lanes <= 0 || trainers < 0) return KMB_EINVAL;
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return KMB_ECUDA;
+    Server *srv = new (std::nothrow) Server;
+    if (!srv) return KMB_ENOMEM;
+    srv->device = device;
+    srv->budget = (size_t)hbm_budget_bytes;
+    // Keep freed request memory in the stream-ordered pool instead of returning it to the driver.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = (uint64_t)hbm_budget_bytes;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    for (int i = 0; i < lanes; ++i) {
+        Lane *l = new Lane;
+        l->srv = srv;
+        if (cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete l;
+            return KMB_ECUDA;
+        }
+        srv->lanes.push_back(l);
+    }
+    srv->threads.emplace_back(scheduler_loop, srv);
+    for (int i = 0; i < trainers; ++i) srv->threads.emplace_back(trainer_loop, srv);
+    *out = srv;
+    return KMB_OK;
+}
+
+int kmb_server_destroy(void *handle) {
+    Server *srv = (Server *)handle;
+    if (!srv) return KMB_EINVAL;
+    {
+        std::unique_lock<std::mutex> lock(srv->mu);
+        // wait for in-flight work
+        srv->cv.wait(lock, [&] {
+            for (Lane *l : srv->lanes)
+                if (l->busy) return false;
+            return srv->pending.empty() && srv->train_queue.empty() && srv->in_use == 0;
+        });
+        srv->stop = true;
+    }
+    srv->cv.notify_all();
+    for (auto &t : srv->threads) t.join();
+    cudaSetDevice(srv->device);
+    for (Lane *l : srv->lanes) {
+        cudaStreamSynchronize(l->stream);
+        cudaStreamDestroy(l->stream);
+        if (l->h_desc) cudaFreeHost(l->h_desc);
+        if (l->d_desc) cudaFree(l->d_desc);
+        delete l;
+    }
+    for (Model &m : srv->models) {
+        cudaFree(m.C);
+        cudaFree(m.Ct);
+        cudaFree(m.h);
+    }
+    for (auto &kv : srv->all) delete kv.second;
+    delete srv;
+    return KMB_OK;
+}
+
+int kmb_server_add_model(void *handle, const float *C_host, int64_t k, int64_t d, int32_t *model_id) {
+    Server *srv = (Server *)handle;
+    if (!srv || !C_host || k <= 0 || d <= 0 || k > INT32_MAX || !model_id) return KMB_EINVAL;
+    cudaSetDevice(srv->device);
+    Model m;
+    m.k = k;
+    m.d = d;
+    m.kpad = (k + 127) / 128 * 128;
+    m.dpad = (d + 7) / 8 * 8;
+    if (cudaMalloc(&m.C, sizeof(float) * k * d) != cudaSuccess ||
+        cudaMalloc(&m.Ct, sizeof(float) * m.kpad * m.dpad) != cudaSuccess ||
+        cudaMalloc(&m.h, sizeof(float) * m.kpad) != cudaSuccess)
+        return KMB_ENOMEM;
+    cudaMemcpy(m.C, C_host, sizeof(float) * k * d, cudaMemcpyHostToDevice);
+    prep_model_kernel<<<(unsigned)m.kpad, 1>>>(m.C, (int)k, (int)d, (int)m.dpad, (int)m.kpad, m.Ct, m.h);
+    KMB_LAUNCHED();
+    if (cudaDeviceSynchronize() != cudaSuccess) return KMB_ECUDA;
+    std::lock_guard<std::mutex> lock(srv->mu);
+    srv->models.push_back(m);
+    *model_id = (int32_t)srv->models.size() - 1;
+    return KMB_OK;
+}
+
+int kmb_server_submit_infer(void *handle, int32_t model_id, const float *X_host, int64_t n, int64_t d,
+                            int32_t *labels_host, int64_t *request_id) {
+    Server *srv = (Server *)handle;
+    if (!srv || !X_host || !labels_host || n <= 0 || !request_id) return KMB_EINVAL;
+    Request *r = new (std::nothrow) Request;
+    if (!r) return KMB_ENOMEM;
+    {
+        std::lock_guard<std::mutex> lock(srv->mu);
+        if (model_id < 0 || model_id >= (int32_t)srv->models.size() || srv->models[model_id].d != d) {
+            delete r;
+            return KMB_EINVAL;
+        }
+        r->id = srv->next_id++;
+        r->kind = INFER;
+        r->model = model_id;
+        r->n = n;
+        r->d = d;
+        r->k = srv->models[model_id].k;
+        r->iters = 0;
+        r->X = X_host;
+        r->C0 = nullptr;
+        r->labels_out = labels_host;
+        r->C_out = nullptr;
+        r->bytes = infer_bytes(n, d);
+        r->t_submit = Clock::now();
+        srv->all[r->id] = r;
+        srv->pending.push_back(r);
+        *request_id = r->id;
+    }
+    srv->cv.notify_all();
+    return KMB_OK;
+}
+
+int kmb_server_submit_train(void *handle, const float *X_host, int64_t n, int64_t d, const float *C0_host, int64_t k,
+                            int64_t iterations, float *C_out_host, int32_t *labels_host, int64_t *request_id) {
+    Server *srv = (Server *)handle;
+    if (!srv || !X_host || !C0_host || !C_out_host || !labels_host || n <= 0 || d <= 0 || k <= 0 || k > n ||
+        iterations < 0 || !request_id)
+        return KMB_EINVAL;
+    Request *r = new (std::nothrow) Request;
+    if (!r) return KMB_ENOMEM;
+    {
+        std::lock_guard<std::mutex> lock(srv->mu);
+        r->id = srv->next_id++;
+        r->kind = TRAIN;
+        r->model = -1;
+        r->n = n;
+        r->d = d;
+        r->k = k;
+        r->iters = iterations;
+        r->X = X_host;
+        r->C0 = C0_host;
+        r->labels_out = labels_host;
+        r->C_out = C_out_host;
+        r->bytes = train_bytes(n, d, k);
+        r->t_submit = Clock::now();
+        srv->all[r->id] = r;
+        srv->train_queue.push_back(r);
+        *request_id = r->id;
+    }
+    srv->cv.notify_all();
+    return KMB_OK;
+}
+
+// Waits (up to timeout_s; < 0 = no limit) for a request; returns its status
+// (KMB_OK when done) or KMB_ETIMEDOUT. latency_s receives submit -> done.
+// A finished request is forgotten after a successful wait.
+int kmb_server_wait(void *handle, int64_t request_id, double timeout_s, double *latency_s) {
+    Server *srv = (Server *)handle;
+    if (!srv) return KMB_EINVAL;
+    std::unique_lock<std::mutex> lock(srv->mu);
+    auto it = srv->all.find(request_id);
+    if (it == srv->all.end()) return KMB_EINVAL;
+    Request *r = it->second;
+    auto done = [&] { return r->state == DONE || r->state == FAILED; };
+    if (timeout_s < 0) {
+        srv->cv.wait(lock, done);
+    } else if (!srv->cv.wait_for(lock, std::chrono::duration<double>(timeout_s), done)) {
+        return KMB_ETIMEDOUT;
+    }
+    if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+    const int rc = r->rc;
+    srv->all.erase(it);
+    delete r;
+    return rc;
+}
+
+int kmb_server_get_stats(void *handle, kmb_server_stats *out) {
+    Server *srv = (Server *)handle;
+    if (!srv || !out) return KMB_EINVAL;
+    std::lock_guard<std::mutex> lock(srv->mu);
+    out->completed = srv->completed;
+    out->failed = srv->failed;
+    out->batches = srv->batches;
+    out->batched_requests = srv->batched_requests;
+    out->pending = (int64_t)(srv->pending.size() + srv->train_queue.size());
+    out->in_use_bytes = (int64_t)srv->in_use;
+    out->peak_in_use_bytes = (int64_t)srv->peak_in_use;
+    out->budget_bytes = (int64_t)srv->budget;
+    return KMB_OK;
+}
+
+}  // extern "C"
