@@ -256,6 +256,55 @@ def run_serving(args, device=0):
             "note": "p50/p99 = host submit->completion of infer requests; rows from a pinned pool"}
 
 
+def run_sharded(args, dist, world, rank, local, form):
+    """N > 1: weak scaling. Each rank holds its own 20M-row shard of an N x 20M-row
+    problem (same generator, seed + rank) and the ranks run Lloyd iterations with one
+    FP64 all-reduce of [sums | counts] per iteration (onedal_b200.spmd). value =
+    shards x iterations / s (iterations/s of 20M-row shards processed by the job)."""
+    import torch
+
+    from onedal_b200 import spmd, workloads
+
+    w = workloads.PRECISION
+    n = args.rows or w.n
+    X, _ = workloads.make(workloads.Workload(w.name, n, w.d, w.k, w.iterations, w.eps, w.seed + rank), "cuda", n=n)
+    C0 = workloads.make(w, "cpu", n=max(w.k, 100_000))[1].cuda()  # same initial centroids on every rank
+    ops = spmd.DeviceShardOps(X, form)
+
+    def iterate(C, T):
+        for _ in range(T):
+            st = ops.partial(C)
+            dist.all_reduce(st.sums)
+            dist.all_reduce(st.counts)
+            C, shift, empty = ops.finalize(st.sums, st.counts, C)
+        return C
+
+    iterate(C0.clone(), args.warmup)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    iterate(C0.clone(), args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms = float(ms.item())
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"precision, {n} rows per rank (seed + rank), d={w.d}, k={w.k}, float32",
+                       "n_per_rank": n, "d": w.d, "k": w.k, "form": args.form,
+                       "exchange": "NCCL all-reduce of FP64 sums (k*d) and int64 counts (k) per iteration",
+                       "value_unit": "20M-row shard iterations per second, summed over ranks"},
+        }
+        print(json.dumps(line))
+    dist.destroy_process_group()
+
+
 def run_b200(args):
     import ctypes
 
@@ -276,6 +325,8 @@ def run_b200(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     w = workloads.PRECISION
     form = _native.KMB_FORM_BF16X3 if args.form == "bf16x3" else _native.KMB_FORM_PLAIN
+    if world > 1:
+        return run_sharded(args, dist, world, rank, local, form)
 
     X, C0 = make_workload("cuda", n=args.rows)
     n, d = X.shape

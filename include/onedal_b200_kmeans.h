@@ -126,18 +126,23 @@ KMB_API int kmb_lloyd_step(kmb_context *ctx, int dtype, const void *X, int64_t n
 
 /* Partial statistics for row-sharded (SPMD) training, device memory only:
  * labels of this shard's rows under C (k x d), FP64 per-cluster sums
- * sums (k x d), counts (k, int64) and the shard's sum of squared distances.
- * The caller all-reduces sums/counts across shards, then calls
- * kmb_finalize_centroids. The reference's SPMD path performs the same
- * exchange (cpp/oneapi/dal/algo/kmeans/backend/gpu/cluster_updater.hpp:117-153). */
+ * sums (k x d), counts (k, int64), the shard's sum of squared distances
+ * (*sq_distances, one device double; may be NULL) and, when row_sq_distance
+ * is not NULL, each row's squared distance to its centroid (n values of the
+ * data type; used to pick empty-cluster candidates). Sums are added in row
+ * order, so equal labels give bit-identical sums. The caller all-reduces
+ * sums/counts across shards, then calls kmb_finalize_centroids. The
+ * reference's SPMD path performs the same exchange
+ * (cpp/oneapi/dal/algo/kmeans/backend/gpu/cluster_updater.hpp:117-153). */
 KMB_API int kmb_partial_sums(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, const void *C,
                              int64_t k, int32_t form, int32_t *labels, double *sums, int64_t *counts,
-                             double *sq_distances, float *row_sq_distance);
+                             double *sq_distances, void *row_sq_distance);
 
 /* Centroids from all-reduced sums/counts (device memory): c_j = sums_j / counts_j
  * rounded to F; clusters with count 0 keep C_in and are listed (ascending) in
- * empty_ids (k int32, device) with *n_empty set; shift = sum over non-empty
- * clusters of ||c_old - c_new||^2. */
+ * empty_ids (k int32, device) with *n_empty (host) set; *shift (host) = sum over
+ * non-empty clusters of ||c_old - c_new||^2. The caller reseeds the listed
+ * clusters (kmeans_lloyd_batch_impl.i:167-186) and adds their shift. */
 KMB_API int kmb_finalize_centroids(kmb_context *ctx, int dtype, const double *sums, const int64_t *counts,
                                    const void *C_in, int64_t k, int64_t d, void *C_out, double *shift,
                                    int32_t *empty_ids, int64_t *n_empty);

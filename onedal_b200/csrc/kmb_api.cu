@@ -476,6 +476,36 @@ int step_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, const void
     return KMB_OK;
 }
 
+// One shard's statistics under C: labels, FP64 sums/counts, sum of squared
+// distances, optional per-row squared distances (for candidate selection).
+template <typename F>
+int partial_impl(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, int64_t k, int32_t form,
+                 int32_t *labels, double *sums, int64_t *counts, double *sq_distances, F *row_sq) {
+    const bool tc = form == KMB_FORM_BF16X3;
+    if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
+    int rc = ensure_common<F>(ctx, n, d, k, tc, tc);
+    if (rc) return rc;
+    kmb::UpdatePlan plan = kmb::make_update_plan(n, k, d);
+    if (!kmb::ensure_update_buffers(ctx->ws, plan, sizeof(F))) return fail(ctx, KMB_ENOMEM, "update buffers");
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    LoopState *st = (LoopState *)ws.state.ptr + 1;
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    init_state(ctx->h_state[1], 0.0);
+    KMB_CUDA(cudaMemcpyAsync(st, &ctx->h_state[1], sizeof(LoopState), cudaMemcpyHostToDevice, s));
+    KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
+    kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
+    if (tc) split_rows<F>(ctx, X, n, d);
+    if ((rc = assign_pass<F>(ctx, X, n, d, C, k, tc, labels, (F *)ws.d2.ptr, st, tc))) return rc;
+    kmb::launch_partial_sums<F>(X, plan, labels, sums, counts, ws, s);
+    if (sq_distances)
+        kmb::launch_sum_values<F>((const F *)ws.d2.ptr, n, (double *)ws.obj_part.ptr, sq_distances, s);
+    if (row_sq) KMB_CUDA(cudaMemcpyAsync(row_sq, ws.d2.ptr, sizeof(F) * n, cudaMemcpyDeviceToDevice, s));
+    KMB_CUDA(cudaGetLastError());
+    KMB_CUDA(cudaStreamSynchronize(s));
+    return KMB_OK;
+}
+
 int validate_shapes(kmb_context *ctx, int dtype, int64_t n, int64_t d, int64_t k) {
     if (!ctx) return KMB_EINVAL;
     if (dtype != KMB_F32 && dtype != KMB_F64) return fail(ctx, KMB_EINVAL, "unknown dtype %d", dtype);
@@ -658,17 +688,52 @@ int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int6
 
 int kmb_partial_sums(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, const void *C, int64_t k,
                      int32_t form, int32_t *labels, double *sums, int64_t *counts, double *sq_distances,
-                     float *row_sq_distance) {
-    (void)ctx; (void)dtype; (void)X; (void)n; (void)d; (void)C; (void)k; (void)form; (void)labels; (void)sums;
-    (void)counts; (void)sq_distances; (void)row_sq_distance;
-    return KMB_EUNSUPPORTED;
+                     void *row_sq_distance) {
+    if (!ctx) return KMB_EINVAL;
+    ctx->last_error.clear();
+    if (dtype != KMB_F32 && dtype != KMB_F64) return fail(ctx, KMB_EINVAL, "unknown dtype %d", dtype);
+    if (n <= 0 || n > INT32_MAX || d <= 0 || k <= 0 || k > INT32_MAX) return fail(ctx, KMB_EINVAL, "bad shape");
+    int rc = check_form(ctx, dtype, form);
+    if (rc) return rc;
+    if (!X || !C || !labels || !sums || !counts) return fail(ctx, KMB_EINVAL, "null device pointer");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    if (dtype == KMB_F32)
+        return partial_impl<float>(ctx, (const float *)X, n, d, (const float *)C, k, form, labels, sums, counts,
+                                   sq_distances, (float *)row_sq_distance);
+    return partial_impl<double>(ctx, (const double *)X, n, d, (const double *)C, k, form, labels, sums, counts,
+                                sq_distances, (double *)row_sq_distance);
 }
 
 int kmb_finalize_centroids(kmb_context *ctx, int dtype, const double *sums, const int64_t *counts, const void *C_in,
                            int64_t k, int64_t d, void *C_out, double *shift, int32_t *empty_ids, int64_t *n_empty) {
-    (void)ctx; (void)dtype; (void)sums; (void)counts; (void)C_in; (void)k; (void)d; (void)C_out; (void)shift;
-    (void)empty_ids; (void)n_empty;
-    return KMB_EUNSUPPORTED;
+    if (!ctx) return KMB_EINVAL;
+    ctx->last_error.clear();
+    if (dtype != KMB_F32 && dtype != KMB_F64) return fail(ctx, KMB_EINVAL, "unknown dtype %d", dtype);
+    if (k <= 0 || d <= 0 || !sums || !counts || !C_in || !C_out || !empty_ids)
+        return fail(ctx, KMB_EINVAL, "bad arguments");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    kmb::Workspace &ws = ctx->ws;
+    if (!ws.ensure(ws.shift_part, sizeof(double) * k) || !ws.ensure(ws.empty_flag, sizeof(int32_t) * k) ||
+        !ws.ensure(ws.scalars, sizeof(kmb::DevScalars)))
+        return fail(ctx, KMB_ENOMEM, "finalize buffers");
+    cudaStream_t s = ctx->stream;
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    double *shift_dev = &sc->objective;
+    long long *ne_dev = (long long *)&sc->pad;
+    if (dtype == KMB_F32)
+        kmb::launch_finalize_from_sums<float>(sums, counts, (const float *)C_in, (float *)C_out, k, d, ws, shift_dev,
+                                              empty_ids, ne_dev, s);
+    else
+        kmb::launch_finalize_from_sums<double>(sums, counts, (const double *)C_in, (double *)C_out, k, d, ws,
+                                               shift_dev, empty_ids, ne_dev, s);
+    double hv[2];
+    KMB_CUDA(cudaMemcpyAsync(hv, shift_dev, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaStreamSynchronize(s));
+    if (shift) *shift = hv[0];
+    long long ne = 0;
+    std::memcpy(&ne, &hv[1], sizeof(ne));
+    if (n_empty) *n_empty = ne;
+    return KMB_OK;
 }
 
 }  // extern "C"

@@ -131,6 +131,16 @@ template <typename F>
 void launch_partial_sums(const F *X, const UpdatePlan &p, const int32_t *labels, double *sums, int64_t *counts,
                          Workspace &ws, cudaStream_t s);
 
+// Sharded helpers: centroids from all-reduced sums/counts (shift over the
+// non-empty clusters, ascending list of empty clusters), and a deterministic
+// FP64 sum of n values.
+template <typename F>
+void launch_finalize_from_sums(const double *sums, const int64_t *counts, const F *C_old, F *C_new, int64_t k,
+                               int64_t d, Workspace &ws, double *shift_out, int32_t *empty_ids, long long *n_empty,
+                               cudaStream_t s);
+template <typename F>
+void launch_sum_values(const F *v, int64_t n, double *partials, double *out, cudaStream_t s);
+
 // Exact objective sum ||x - c_label||^2 in FP64, deterministic.
 template <typename F>
 void launch_objective(const F *X, int64_t n, int64_t d, const F *C, const int32_t *labels, double *partials,

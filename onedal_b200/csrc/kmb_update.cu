@@ -619,6 +619,97 @@ __global__ void sum_partials_kernel(const double *__restrict__ partials, int cou
     }
 }
 
+// ---- sharded (SPMD) helpers ---------------------------------------------------
+
+// Centroids from all-reduced FP64 sums and counts: c = F(S / count); empty
+// clusters keep C_in (the caller reseeds them) and are flagged.
+template <typename F>
+__global__ void finalize_from_sums_kernel(const double *__restrict__ sums, const int64_t *__restrict__ counts,
+                                          const F *__restrict__ C_old, F *__restrict__ C_new, int d,
+                                          double *__restrict__ shift_part, int32_t *__restrict__ empty_flag) {
+    __shared__ double red[32];
+    const int j = blockIdx.x;
+    const int64_t cnt = counts[j];
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < d; t += blockDim.x) {
+        const F old = C_old[(int64_t)j * d + t];
+        if (cnt > 0) {
+            const F c = F(sums[(int64_t)j * d + t] / (double)cnt);
+            const double df = (double)old - (double)c;
+            acc += df * df;
+            C_new[(int64_t)j * d + t] = c;
+        } else {
+            C_new[(int64_t)j * d + t] = old;
+        }
+    }
+    for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+        shift_part[j] = tot;
+        empty_flag[j] = cnt > 0 ? 0 : 1;
+    }
+}
+
+// Fixed-order sum of k doubles (single block).
+__global__ void sum_doubles_kernel(const double *__restrict__ v, int k, double *__restrict__ out) {
+    __shared__ double s[1024];
+    const int T = blockDim.x;
+    const int per = (k + T - 1) / T;
+    const int j0 = threadIdx.x * per, j1 = min(k, j0 + per);
+    double a = 0.0;
+    for (int j = j0; j < j1; ++j) a += v[j];
+    s[threadIdx.x] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < T; ++w) tot += s[w];
+        *out = tot;
+    }
+}
+
+// Deterministic FP64 sum of n values of F (per-block partials, then one block).
+template <typename F>
+__global__ void sum_values_kernel(const F *__restrict__ v, int64_t n, double *__restrict__ partials) {
+    __shared__ double s[256];
+    const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t b = (int64_t)blockIdx.x * per, e = min(n, b + per);
+    double a = 0.0;
+    for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) a += (double)v[i];
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if ((int)threadIdx.x < st) s[threadIdx.x] += s[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = s[0];
+}
+
+__global__ void list_empties_kernel(const int32_t *__restrict__ empty_flag, int k, int32_t *__restrict__ empty_ids,
+                                    long long *__restrict__ n_empty) {
+    __shared__ int s_cnt[1024];
+    const int T = blockDim.x;
+    const int per = (k + T - 1) / T;
+    const int j0 = threadIdx.x * per, j1 = min(k, j0 + per);
+    int c = 0;
+    for (int j = j0; j < j1; ++j) c += empty_flag[j];
+    s_cnt[threadIdx.x] = c;
+    __syncthreads();
+    for (int off = 1; off < T; off <<= 1) {
+        int a = 0;
+        if ((int)threadIdx.x >= off) a = s_cnt[threadIdx.x - off];
+        __syncthreads();
+        s_cnt[threadIdx.x] += a;
+        __syncthreads();
+    }
+    int pos = s_cnt[threadIdx.x] - c;
+    for (int j = j0; j < j1; ++j)
+        if (empty_flag[j]) empty_ids[pos++] = j;
+    if (threadIdx.x == 0) *n_empty = s_cnt[T - 1];
+}
+
 }  // namespace
 
 constexpr int kObjectiveBlocks = 148 * 8;
@@ -771,6 +862,37 @@ void launch_objective(const F *X, int64_t n, int64_t d, const F *C, const int32_
     sum_partials_kernel<<<1, 32, 0, s>>>(partials, kObjectiveBlocks, out);
     KMB_LAUNCHED();
 }
+
+template <typename F>
+void launch_finalize_from_sums(const double *sums, const int64_t *counts, const F *C_old, F *C_new, int64_t k,
+                               int64_t d, Workspace &ws, double *shift_out, int32_t *empty_ids, long long *n_empty,
+                               cudaStream_t s) {
+    double *shift_part = (double *)ws.shift_part.ptr;
+    int32_t *empty_flag = (int32_t *)ws.empty_flag.ptr;
+    finalize_from_sums_kernel<F><<<(unsigned)k, 128, 0, s>>>(sums, counts, C_old, C_new, (int)d, shift_part,
+                                                             empty_flag);
+    KMB_LAUNCHED();
+    sum_doubles_kernel<<<1, 1024, 0, s>>>(shift_part, (int)k, shift_out);
+    KMB_LAUNCHED();
+    list_empties_kernel<<<1, 1024, 0, s>>>(empty_flag, (int)k, empty_ids, n_empty);
+    KMB_LAUNCHED();
+}
+
+template <typename F>
+void launch_sum_values(const F *v, int64_t n, double *partials, double *out, cudaStream_t s) {
+    sum_values_kernel<F><<<kObjectiveBlocks, 256, 0, s>>>(v, n, partials);
+    KMB_LAUNCHED();
+    sum_partials_kernel<<<1, 32, 0, s>>>(partials, kObjectiveBlocks, out);
+    KMB_LAUNCHED();
+}
+
+template void launch_finalize_from_sums<float>(const double *, const int64_t *, const float *, float *, int64_t,
+                                               int64_t, Workspace &, double *, int32_t *, long long *, cudaStream_t);
+template void launch_finalize_from_sums<double>(const double *, const int64_t *, const double *, double *, int64_t,
+                                                int64_t, Workspace &, double *, int32_t *, long long *,
+                                                cudaStream_t);
+template void launch_sum_values<float>(const float *, int64_t, double *, double *, cudaStream_t);
+template void launch_sum_values<double>(const double *, int64_t, double *, double *, cudaStream_t);
 
 #define KMB_INST(F)                                                                                                 \
     template void launch_update<F>(const F *, const UpdatePlan &, const int32_t *, const F *, F *, F *, Workspace &, \
