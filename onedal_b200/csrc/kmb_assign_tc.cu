@@ -24,14 +24,17 @@
 //            SWIZZLE_128B), B = Chi/Clo panels of 128 clusters, ring of stages
 //   warp 1   TMEM allocation + single-thread tcgen05.mma issue; commits free
 //            B stages, publish accumulators and release A tiles
-//   warps 2-9 epilogue, two groups of 4 warps: group g takes the cluster tiles
-//            whose running index is g mod 2, reads the 128x128 FP32 accumulator
-//            with tcgen05.ld (one TMEM lane = one row per thread), and keeps a
-//            running top-3 per row. Each 32-column chunk is first reduced to
-//            its minimum (branch-free, 3-input min); only chunks that beat the
-//            row's third-best score take the exact insertion path. At the end
-//            of a row tile group 1 hands its top-3 to group 0 through TMEM
-//            (columns 256..263), group 0 merges and writes the row's outputs.
+//   warps 2-9 epilogue, two groups of 4 warps: group g owns TMEM accumulator g
+//            and the cluster tiles whose running index is g mod 2. Before the
+//            MMAs of a tile start, the group writes -h_j into every lane of the
+//            accumulator (tcgen05.st), so the MMAs leave y = x.c - h = -score
+//            there and no per-score subtraction is needed. The group reads y
+//            with tcgen05.ld (one TMEM lane = one row per thread) and keeps a
+//            running top-3 per row: each 32-column chunk is first reduced to
+//            its maximum (branch-free, 3-input max); only chunks that beat the
+//            row's third-best take the exact insertion path. At the end of a
+//            row tile group 1 hands its top-3 to group 0 through TMEM (columns
+//            256..263); group 0 merges and writes the row's outputs.
 // The two accumulators alternate between the groups, so both epilogue groups
 // and the MMAs of the next cluster tile run concurrently. Every mbarrier wait is bounded; on timeout the
 // CTA records KMB_ETIMEDOUT in the loop state, drains its own TMA loads and
@@ -62,7 +65,7 @@ struct Params {
     int d, dpad, k, kpad;
     int n_tiles, kpanels, ntiles_n;
     int a_stages, b_stages;
-    const float *h;
+    const float *h;  // -0.5||c_j||^2 per cluster, -inf padding
     const float *xnorm;
     const double *cnorm_max;
     int32_t *labels;
@@ -187,6 +190,37 @@ __device__ __forceinline__ float min3f(float a, float b, float c) {
     asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
     return r;
 }
+
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Stores 32 consecutive floats of global memory (the same for every lane) into
+// this warp's 32 TMEM lanes, 32 columns starting at taddr.
+__device__ __forceinline__ void tmem_st32_from(uint32_t taddr, const float *src) {
+    uint32_t r[32];
+#pragma unroll
+    for (int i = 0; i < 32; i += 4) {
+        const float4 q = __ldg(reinterpret_cast<const float4 *>(src + i));
+        r[i] = __float_as_uint(q.x);
+        r[i + 1] = __float_as_uint(q.y);
+        r[i + 2] = __float_as_uint(q.z);
+        r[i + 3] = __float_as_uint(q.w);
+    }
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]),
+        "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]),
+        "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void named_bar_sync(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
@@ -348,7 +382,8 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 for (int j = 0; j < p.ntiles_n && ok; ++j, ++acount) {
                     const int slot = (int)(acount % NACC);
                     const int use = (int)(acount / NACC);
-                    if (!mbar_wait(&bar->acc_empty[slot], (use & 1) ^ 1, abort)) { ok = false; break; }
+                    // the epilogue has written -h into this accumulator (first use included)
+                    if (!mbar_wait(&bar->acc_empty[slot], use & 1, abort)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t tmem_d = tmem_base + (uint32_t)(slot * BN);
                     for (int kp = 0; kp < p.kpanels; ++kp, ++bcount) {
@@ -361,8 +396,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
 #pragma unroll
                         for (int ks = 0; ks < KP / 16; ++ks) {
                             const uint32_t off = ks * 32;  // 16 bf16 = 32 bytes along the swizzled row
-                            const uint32_t acc = (kp | ks) ? 1u : 0u;
-                            mma_bf16(tmem_d, sw128_desc(ah + off), sw128_desc(bh + off), acc);
+                            mma_bf16(tmem_d, sw128_desc(ah + off), sw128_desc(bh + off), 1u);
                             mma_bf16(tmem_d, sw128_desc(ah + off), sw128_desc(bl + off), 1u);
                             mma_bf16(tmem_d, sw128_desc(al + off), sw128_desc(bh + off), 1u);
                         }
@@ -387,12 +421,26 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
         const double cmax = *p.cnorm_max;
         long long acount = 0;
         bool ok = true;
+        // Accumulators start from -h (written here, one row per lane), so after the
+        // MMAs they hold y = x.c - h = -score and the argmin becomes a max over y.
+        {
+            const float *hn = p.h + (size_t)(group % p.ntiles_n) * BN;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                __syncwarp();
+                tmem_st32_from(lane_base + (uint32_t)(group * BN + c0), hn + c0);
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar->acc_empty[group]);
+        }
         // Both groups pass the same number of named barriers (one per row tile),
         // also after an abort, so neither can be left waiting on the other.
         for (int lt = 0; lt < my_tiles; ++lt) {
             const int tile = blockIdx.x + lt * gridDim.x;
-            Top3 r;
-            r.b = r.s = r.t = __int_as_float(0x7f800000);
+            Top3 r;  // in y = -score space: b >= s >= t
+            r.b = r.s = r.t = __int_as_float(0xff800000);
             r.ib = r.is = 0;
             for (int j = 0; j < p.ntiles_n; ++j, ++acount) {
                 if ((int)(acount & 1) != group || !ok) continue;
@@ -404,39 +452,34 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                     continue;
                 }
                 tc_fence_after();
-                const float *hj = p.h + j * BN;
+                // -h of the cluster tile this accumulator holds next
+                const float *hn = p.h + (size_t)((acount + NACC) % p.ntiles_n) * BN;
 #pragma unroll 1
                 for (int c0 = 0; c0 < BN; c0 += 32) {
                     float v[32];
-                    __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the filtered path
-                    tmem_ld32(lane_base + (uint32_t)(slot * BN + c0), v);
-#pragma unroll
-                    for (int i = 0; i < 32; i += 4) {
-                        const float4 h4 = __ldg(reinterpret_cast<const float4 *>(hj + c0 + i));
-                        v[i] = h4.x - v[i];
-                        v[i + 1] = h4.y - v[i + 1];
-                        v[i + 2] = h4.z - v[i + 2];
-                        v[i + 3] = h4.w - v[i + 3];
-                    }
+                    __syncwarp();  // tcgen05.ld/st are warp-collective: reconverge after the filtered path
+                    const uint32_t taddr = lane_base + (uint32_t)(slot * BN + c0);
+                    tmem_ld32(taddr, v);
+                    tmem_st32_from(taddr, hn + c0);
                     float m[11];
 #pragma unroll
-                    for (int i = 0; i < 10; ++i) m[i] = min3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
-                    m[10] = fminf(v[30], v[31]);
-                    const float m1 = min3f(min3f(m[0], m[1], m[2]), min3f(m[3], m[4], m[5]),
-                                           min3f(m[6], m[7], min3f(m[8], m[9], m[10])));
-                    if (m1 < r.t) {
+                    for (int i = 0; i < 10; ++i) m[i] = max3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+                    m[10] = fmaxf(v[30], v[31]);
+                    const float m1 = max3f(max3f(m[0], m[1], m[2]), max3f(m[3], m[4], m[5]),
+                                           max3f(m[6], m[7], max3f(m[8], m[9], m[10])));
+                    if (m1 > r.t) {
                         const int colbase = j * BN + c0;
 #pragma unroll
                         for (int i = 0; i < 32; ++i) {
                             const float x = v[i];
-                            if (x < r.t) {
-                                if (x < r.b) {
+                            if (x > r.t) {  // columns increase: strict '>' keeps the lowest index on ties
+                                if (x > r.b) {
                                     r.t = r.s;
                                     r.s = r.b;
                                     r.is = r.ib;
                                     r.b = x;
                                     r.ib = colbase + i;
-                                } else if (x < r.s) {
+                                } else if (x > r.s) {
                                     r.t = r.s;
                                     r.s = x;
                                     r.is = colbase + i;
@@ -447,10 +490,15 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                         }
                     }
                 }
+                tmem_wait_st();
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&bar->acc_empty[slot]);
             }
+            // back to score space (score = -y) for the merge and the outputs
+            r.b = -r.b;
+            r.s = -r.s;
+            r.t = -r.t;
             // Group 1 hands its top-3 to group 0 through TMEM columns XCHG_COL..+7 of
             // the same lanes (alternating by row-tile parity), then group 0 merges.
             const uint32_t xaddr = lane_base + (uint32_t)(XCHG_COL + 8 * (lt & 1));
@@ -518,7 +566,7 @@ __global__ void split_rows_kernel(const float *__restrict__ src, int64_t rows, i
 }
 
 // Per-iteration centroid prep for the tensor-core form: Chi/Clo [kpad][dpad],
-// h = 0.5||c||^2 (FP32 from a double sum, +inf padding), max ||c||.
+// -h = -0.5||c||^2 (FP32 from a double sum, -inf padding), max ||c||.
 __global__ void prep_centroids_tc_kernel(const float *__restrict__ C, int k, int d, int dpad, int kpad,
                                          __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
                                          float *__restrict__ h, double *__restrict__ cnorm_max, const LoopState *st) {
@@ -539,7 +587,7 @@ __global__ void prep_centroids_tc_kernel(const float *__restrict__ C, int k, int
     if (threadIdx.x == 0) {
         double tot = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
-        h[j] = (j < k) ? (float)(0.5 * tot) : __int_as_float(0x7f800000);
+        h[j] = (j < k) ? (float)(-0.5 * tot) : __int_as_float(0xff800000);  // -h, -inf padding
         if (j < k)
             atomicMax(reinterpret_cast<unsigned long long *>(cnorm_max),
                       (unsigned long long)__double_as_longlong(sqrt(tot)));

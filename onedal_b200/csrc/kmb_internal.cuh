@@ -105,7 +105,7 @@ int64_t tc_kpad(int64_t k);   // k rounded up to the 128-wide cluster tile
 bool tc_supported(int64_t d); // dpad <= 256
 // X (rows x d, FP32) -> hi/lo BF16 [rows][dpad], zero padded.
 void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, cudaStream_t s);
-// C -> Chi/Clo [kpad][dpad], h (kpad, +inf padding), max ||c||.
+// C -> Chi/Clo [kpad][dpad], -h = -0.5||c||^2 (kpad, -inf padding), max ||c||.
 void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, void *Clo, float *h,
                               double *cnorm_max, const LoopState *st, cudaStream_t s);
 int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
