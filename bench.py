@@ -305,6 +305,51 @@ def run_sharded(args, dist, world, rank, local, form):
     dist.destroy_process_group()
 
 
+def run_batched(args):
+    """Batched form: `args.batched_problems` independent problems (n log-uniform in
+    [1e3, 2e5], d in {8,16,32,64}, k log-uniform int in [4,128], Gaussian mixtures of
+    k blobs, std 1, centres U[-10,10]^d), 30 iterations each, one graph-replayed
+    sequence of grouped launches per iteration."""
+    import numpy as np
+    import torch
+
+    from onedal_b200.batched import batched_train
+
+    g = np.random.default_rng(1004)
+    tg = torch.Generator(device="cuda")
+    tg.manual_seed(1004)
+    probs = []
+    flops = 0.0
+    rows = 0
+    for _ in range(args.batched_problems):
+        n = int(np.exp(g.uniform(np.log(1e3), np.log(2e5))))
+        d = int(g.choice([8, 16, 32, 64]))
+        k = int(round(np.exp(g.uniform(np.log(4), np.log(128)))))
+        centres = (torch.rand(k, d, generator=tg, device="cuda") * 20 - 10)
+        lab = torch.randint(0, k, (n,), generator=tg, device="cuda")
+        X = centres[lab] + torch.randn(n, d, generator=tg, device="cuda")
+        C0 = X[torch.randperm(n, generator=tg, device="cuda")[:k]].clone()
+        probs.append((X, C0))
+        flops += 2.0 * n * k * d
+        rows += n
+    T = 30
+    batched_train(probs[: min(64, len(probs))], 2)  # autotune + warm-up on the classes present
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res, info = batched_train(probs, T, use_graph=True)
+    e1.record()
+    torch.cuda.synchronize()
+    s = e0.elapsed_time(e1) / 1e3
+    iters = sum(r[2] for r in res)
+    return {"problems": len(probs), "iterations_each_max": T, "total_problem_iterations": iters,
+            "seconds": s, "problem_iterations_per_s": iters / s, "rows": rows,
+            "row_iterations_per_s": sum(p[0].shape[0] * r[2] for p, r in zip(probs, res)) / s,
+            "algorithmic_tflops": flops * (iters / len(probs)) / s / 1e12, "variants": info["variants"],
+            "note": "includes per-call setup (arena, row norms, fixed-point scales, graph capture)"}
+
+
 def run_b200(args):
     import ctypes
 
@@ -449,6 +494,9 @@ def run_b200(args):
                    "sample": f"first {ns} of {n} rows, {it} Lloyd iterations of the reference DAAL kernel "
                              f"(OpenBLAS sgemm, std::thread shim), per-iteration time scaled by rows"}
 
+    batched = None
+    if rank == 0 and world == 1 and args.batched_problems > 0:
+        batched = run_batched(args)
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
         del X
@@ -471,6 +519,7 @@ def run_b200(args):
             "bf16_over_plain": (value / plain_value) if plain_value else None,
             "recheck_rows_last_iteration": st.rechecked_rows,
             "serving": serving,
+            "batched": batched,
         }
         print(json.dumps(line))
     if dist:
@@ -488,6 +537,8 @@ def main():
     ap.add_argument("--cpu-sample-rows", type=int, default=200_000)
     ap.add_argument("--traffic-bytes", type=float, default=None)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--batched-problems", type=int, default=4096,
+                    help="problems in the batched-form measurement (0 skips it)")
     ap.add_argument("--serving-requests", type=int, default=3000,
                     help="requests per serving load point (0 skips the serving measurement)")
     ap.add_argument("--rows", type=int, default=None,

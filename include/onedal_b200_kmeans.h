@@ -186,6 +186,39 @@ KMB_API int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_
 KMB_API int kmb_infer_noalloc(int dtype, const void *X, int64_t n, int64_t d, const void *C, int64_t k,
                               int32_t *responses, double *objective, void *cuda_stream);
 
+/* ---- Batched form ---------------------------------------------------------
+ * Many independent float32 problems (each its own X, n, d, k) train together:
+ * every Lloyd iteration is one fixed sequence of grouped launches over all
+ * problems (optionally captured once into a CUDA graph and replayed), with
+ * per-problem convergence flags on the device. Per problem the semantics are
+ * those of kmb_lloyd_iterate (plain form): up to max_iteration_count updates,
+ * stop when the shift <= accuracy_threshold; C (k x d) is updated in place and
+ * labels hold the assignment of the last completed update. Sums are 64-bit
+ * fixed point with a per-problem scale (exact on that grid, independent of
+ * scheduling). Limits: k <= 256 and (k*d + k) * 8 <= 200 KiB per problem. The
+ * assignment tile per (d, k) class is chosen by a built-in autotuner the first
+ * time the class is seen on a device. No counterpart in the reference. */
+typedef struct kmb_batched_problem {
+    const void *X;      /* device, n x d */
+    int64_t n, d;
+    void *C;            /* device, k x d, in/out */
+    int64_t k;
+    int32_t *labels;    /* device, n */
+    int64_t iterations; /* out */
+    double last_shift;  /* out */
+} kmb_batched_problem;
+
+typedef struct kmb_batched_info {
+    int64_t problems;
+    int32_t variants;         /* assignment tile variants launched per iteration */
+    int64_t total_iterations; /* summed over problems */
+    int64_t graph_launches;
+} kmb_batched_info;
+
+KMB_API int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64_t count, int64_t max_iteration_count,
+                              double accuracy_threshold, int32_t use_graph, void *cuda_stream,
+                              kmb_batched_info *info);
+
 /* ---- Serving loop ---------------------------------------------------------
  * No counterpart in the reference (its API is one synchronous call per
  * train/infer). A server keeps fitted centroid sets resident on one GPU, admits

@@ -1,0 +1,67 @@
+// A oneDAL client written only against the unchanged oneDAL public headers
+// (oneapi/dal/algo/kmeans.hpp, oneapi/dal/table/homogen.hpp): dal::train and
+// dal::infer on the gold known-answer data of the reference test suite
+// (cpp/oneapi/dal/algo/kmeans/test/data.hpp), read from a text file. Linked
+// against the B200 dispatchers, every call below runs on the GPU.
+//
+//   kmeans_client <gold.txt> <float|double>
+// prints: iterations, objective, centroids, responses, infer objective.
+#include "oneapi/dal/algo/kmeans.hpp"
+#include "oneapi/dal/table/homogen.hpp"
+#include "oneapi/dal/table/row_accessor.hpp"
+
+#include <cstdio>
+#include <fstream>
+#include <string>
+#include <vector>
+
+namespace dal = oneapi::dal;
+
+template <typename F>
+int run(const std::vector<double> &xs, std::int64_t n, std::int64_t d, const std::vector<double> &cs,
+        std::int64_t k) {
+    std::vector<F> x(xs.begin(), xs.end()), c(cs.begin(), cs.end());
+    const auto data = dal::homogen_table::wrap(x.data(), n, d);
+    const auto init = dal::homogen_table::wrap(c.data(), k, d);
+    const auto desc = dal::kmeans::descriptor<F>().set_cluster_count(k).set_max_iteration_count(100).set_accuracy_threshold(0.0);
+    const auto result = dal::train(desc, data, init);
+    std::printf("iterations %lld\n", (long long)result.get_iteration_count());
+    std::printf("objective %.10g\n", result.get_objective_function_value());
+    const auto cen = dal::row_accessor<const F>(result.get_model().get_centroids()).pull({ 0, -1 });
+    std::printf("centroids");
+    for (std::int64_t i = 0; i < cen.get_count(); ++i) std::printf(" %.9g", (double)cen[i]);
+    std::printf("\n");
+    const auto desc_inf = dal::kmeans::descriptor<F>().set_cluster_count(k).set_result_options(
+        dal::kmeans::result_options::compute_exact_objective_function);
+    const auto inf = dal::infer(desc_inf, result.get_model(), data);
+    const auto lab = dal::row_accessor<const std::int32_t>(inf.get_responses()).pull({ 0, -1 });
+    std::printf("responses");
+    for (std::int64_t i = 0; i < lab.get_count(); ++i) std::printf(" %d", lab[i]);
+    std::printf("\n");
+    std::printf("infer_objective %.10g\n", inf.get_objective_function_value());
+    // a precondition the reference checks before dispatch (detail/train_ops.hpp:50-52)
+    try {
+        dal::train(dal::kmeans::descriptor<F>().set_cluster_count(n + 1), data, dal::homogen_table{});
+        std::printf("precondition not enforced\n");
+    } catch (const dal::invalid_argument &) {
+        std::printf("invalid_argument ok\n");
+    }
+    return 0;
+}
+
+int main(int argc, char **argv) {
+    if (argc < 3) return 2;
+    std::ifstream f(argv[1]);
+    std::int64_t n, d, k;
+    f >> n >> d >> k;
+    std::vector<double> x(n * d), c(k * d);
+    for (auto &v : x) f >> v;
+    for (auto &v : c) f >> v;
+    const std::string t = argv[2];
+    try {
+        return t == "double" ? run<double>(x, n, d, c, k) : run<float>(x, n, d, c, k);
+    } catch (const std::exception &e) {
+        std::printf("exception: %s\n", e.what());
+        return 1;
+    }
+}

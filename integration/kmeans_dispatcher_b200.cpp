@@ -1,0 +1,126 @@
+// oneDAL host-policy dispatchers for k-means Lloyd (dense) backed by the B200
+// library (include/onedal_b200_kmeans.h). Compiled against the unchanged
+// oneDAL headers in place of the reference's host-policy instantiations of
+// cpp/oneapi/dal/algo/kmeans/detail/train_ops.cpp:35-42 and
+// detail/infer_ops.cpp:37-43; everything above them (descriptor, tables,
+// pre/post-condition checks of detail/train_ops.hpp:40-84) stays oneDAL's.
+#include "oneapi/dal/algo/kmeans/detail/infer_ops.hpp"
+#include "oneapi/dal/algo/kmeans/detail/train_ops.hpp"
+#include "oneapi/dal/detail/common.hpp"
+#include "oneapi/dal/detail/policy.hpp"
+#include "oneapi/dal/exceptions.hpp"
+#include "oneapi/dal/table/homogen.hpp"
+#include "oneapi/dal/table/row_accessor.hpp"
+
+#include "onedal_b200_kmeans.h"
+
+#include <type_traits>
+
+namespace oneapi::dal::kmeans::detail::v1 {
+
+namespace {
+
+// One context (CUDA stream + workspace) per host thread; the C ABI context is
+// not thread-safe.
+kmb_context *thread_context() {
+    thread_local struct Holder {
+        kmb_context *ctx = nullptr;
+        ~Holder() {
+            if (ctx) kmb_context_destroy(ctx);
+        }
+    } holder;
+    if (!holder.ctx) {
+        const int rc = kmb_context_create(0, &holder.ctx);
+        if (rc != KMB_OK) {
+            holder.ctx = nullptr;
+            throw internal_error(kmb_status_string(rc));
+        }
+    }
+    return holder.ctx;
+}
+
+// kmb_status -> the exception types oneDAL raises for the same failures
+// (cpp/oneapi/dal/backend/interop/error_converter.cpp:136-254).
+void check(kmb_context *ctx, int status) {
+    switch (status) {
+        case KMB_OK: return;
+        case KMB_EINVAL: throw invalid_argument(kmb_context_last_error(ctx));
+        case KMB_ENOMEM: throw host_bad_alloc();
+        case KMB_ETOO_MANY_EMPTY: throw domain_error(kmb_status_string(status));
+        default: throw internal_error(kmb_context_last_error(ctx));
+    }
+}
+
+template <typename F>
+constexpr int dtype_of = std::is_same_v<F, float> ? KMB_F32 : KMB_F64;
+
+}  // namespace
+
+template <typename F>
+struct train_ops_dispatcher<dal::detail::host_policy, F, method::lloyd_dense, task::clustering> {
+    train_result<task::clustering> operator()(const dal::detail::host_policy &,
+                                              const descriptor_base<task::clustering> &desc,
+                                              const train_input<task::clustering> &input) const {
+        const table &data = input.get_data();
+        const std::int64_t n = data.get_row_count();
+        const std::int64_t d = data.get_column_count();
+        const std::int64_t k = desc.get_cluster_count();
+        if (!input.get_initial_centroids().has_data()) {
+            throw unimplemented(dal::detail::error_messages::method_not_implemented());
+        }
+        const auto x = row_accessor<const F>(data).pull({ 0, -1 });
+        const auto c0 = row_accessor<const F>(input.get_initial_centroids()).pull({ 0, -1 });
+        auto centroids = array<F>::empty(k * d);
+        auto responses = array<std::int32_t>::empty(n);
+        kmb_params p{ k, desc.get_max_iteration_count(), desc.get_accuracy_threshold(), KMB_FORM_PLAIN, 0 };
+        double objective = 0.0;
+        std::int64_t iterations = 0;
+        kmb_context *ctx = thread_context();
+        check(ctx, kmb_train(ctx, dtype_of<F>, KMB_MEM_HOST, x.get_data(), n, d, c0.get_data(), &p,
+                             centroids.get_mutable_data(), responses.get_mutable_data(), &objective, &iterations,
+                             nullptr));
+        return train_result<task::clustering>{}
+            .set_model(model<task::clustering>{}.set_centroids(
+                dal::detail::homogen_table_builder{}.reset(centroids, k, d).build()))
+            .set_responses(dal::detail::homogen_table_builder{}.reset(responses, n, 1).build())
+            .set_iteration_count(iterations)
+            .set_objective_function_value(objective);
+    }
+};
+
+template <typename F>
+struct infer_ops_dispatcher<dal::detail::host_policy, F, method::lloyd_dense, task::clustering> {
+    infer_result<task::clustering> operator()(const dal::detail::host_policy &,
+                                              const descriptor_base<task::clustering> &desc,
+                                              const infer_input<task::clustering> &input) const {
+        const table &data = input.get_data();
+        const table &c = input.get_model().get_centroids();
+        const std::int64_t n = data.get_row_count();
+        const std::int64_t d = data.get_column_count();
+        const std::int64_t k = c.get_row_count();
+        const auto x = row_accessor<const F>(data).pull({ 0, -1 });
+        const auto cc = row_accessor<const F>(c).pull({ 0, -1 });
+        const bool want_obj =
+            desc.get_result_options().test(result_options::compute_exact_objective_function);
+        auto responses = array<std::int32_t>::empty(n);
+        double objective = 0.0;
+        kmb_context *ctx = thread_context();
+        check(ctx, kmb_infer(ctx, dtype_of<F>, KMB_MEM_HOST, x.get_data(), n, d, cc.get_data(), k, KMB_FORM_PLAIN,
+                             want_obj ? 1 : 0, responses.get_mutable_data(), &objective, nullptr));
+        auto result = infer_result<task::clustering>{}.set_result_options(desc.get_result_options());
+        result.set_responses(dal::detail::homogen_table_builder{}.reset(responses, n, 1).build());
+        if (want_obj) result.set_objective_function_value(objective);
+        return result;
+    }
+};
+
+template struct ONEDAL_EXPORT
+    train_ops_dispatcher<dal::detail::host_policy, float, method::lloyd_dense, task::clustering>;
+template struct ONEDAL_EXPORT
+    train_ops_dispatcher<dal::detail::host_policy, double, method::lloyd_dense, task::clustering>;
+template struct ONEDAL_EXPORT
+    infer_ops_dispatcher<dal::detail::host_policy, float, method::lloyd_dense, task::clustering>;
+template struct ONEDAL_EXPORT
+    infer_ops_dispatcher<dal::detail::host_policy, double, method::lloyd_dense, task::clustering>;
+
+}  // namespace oneapi::dal::kmeans::detail::v1

@@ -22,8 +22,19 @@ EXPORTED = (
     "kmb_partial_sums", "kmb_finalize_centroids", "kmb_version", "kmb_lloyd_iterate",
     "kmb_context_set_kernel_timing", "kmb_context_kernel_time", "kmb_infer_noalloc",
     "kmb_server_create", "kmb_server_destroy", "kmb_server_add_model", "kmb_server_submit_infer",
-    "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats",
+    "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats", "kmb_batched_train",
 )
+
+
+class kmb_batched_problem(ctypes.Structure):
+    _fields_ = [("X", ctypes.c_void_p), ("n", ctypes.c_int64), ("d", ctypes.c_int64), ("C", ctypes.c_void_p),
+                ("k", ctypes.c_int64), ("labels", ctypes.c_void_p), ("iterations", ctypes.c_int64),
+                ("last_shift", ctypes.c_double)]
+
+
+class kmb_batched_info(ctypes.Structure):
+    _fields_ = [("problems", ctypes.c_int64), ("variants", ctypes.c_int32), ("total_iterations", ctypes.c_int64),
+                ("graph_launches", ctypes.c_int64)]
 
 
 class kmb_server_stats(ctypes.Structure):
@@ -92,6 +103,7 @@ def load_library(path: str = LIB_PATH):
             lib.kmb_server_submit_train.argtypes = [P, P, I64, I64, P, I64, I64, P, P, ctypes.POINTER(I64)]
             lib.kmb_server_wait.argtypes = [P, I64, D, ctypes.POINTER(D)]
             lib.kmb_server_get_stats.argtypes = [P, ctypes.c_void_p]
+            lib.kmb_batched_train.argtypes = [ctypes.c_int, P, I64, I64, D, I32, P, P]
             _lib = lib
     return _lib
 

@@ -100,7 +100,7 @@ bool Workspace::ensure(DevBuf &b, size_t bytes) {
 void Workspace::release() {
     DevBuf *all[] = {&X, &C0, &Cout, &labels, &d2, &xnorm, &Ccur, &Cnew, &Ct, &h, &queue, &H, &Gs,
                      &counts, &offsets, &piece_base, &perm, &records, &shift_part, &empty_flag, &empty_ids,
-                     &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo};
+                     &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx};
     for (DevBuf *b : all) {
         if (b->ptr) cudaFree(b->ptr);
         b->ptr = nullptr;
@@ -155,6 +155,7 @@ int ensure_common(kmb_context *ctx, int64_t n, int64_t d, int64_t k, bool rechec
         ok &= ws.ensure(ws.Chi, sizeof(uint16_t) * tkp * tdp);
         ok &= ws.ensure(ws.Clo, sizeof(uint16_t) * tkp * tdp);
         ok &= ws.ensure(ws.h, sizeof(float) * tkp);
+        ok &= ws.ensure(ws.tcx, kmb::tc_xchg_bytes(ctx->num_sms));
     }
     ok &= ws.ensure(ws.labels, sizeof(int32_t) * n);
     ok &= ws.ensure(ws.d2, sizeof(F) * n);
@@ -203,7 +204,7 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
         KernelTimer timer(ctx, 1);
         rc = kmb::launch_assign_tc(ws.Xhi.ptr, ws.Xlo.ptr, n, d, ws.Chi.ptr, ws.Clo.ptr, (const float *)ws.h.ptr, k,
                                    (const float *)ws.xnorm.ptr, &sc->cnorm_max, labels, d2,
-                                   (RecheckEntry *)ws.queue.ptr, st, ctx->num_sms, s);
+                                   (RecheckEntry *)ws.queue.ptr, st, ctx->num_sms, ws.tcx.ptr, s);
     }
     if (rc != KMB_OK) return fail(ctx, rc, "tensor-core assignment launch failed (d=%lld)", (long long)d);
     {

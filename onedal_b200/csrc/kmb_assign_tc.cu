@@ -33,10 +33,12 @@
 //            running top-3 per row: each 32-column chunk is first reduced to
 //            its maximum (branch-free, 3-input max); only chunks that beat the
 //            row's third-best take the exact insertion path. At the end of a
-//            row tile group 1 hands its top-3 to group 0 through TMEM (columns
-//            256..263); group 0 merges and writes the row's outputs.
-// The two accumulators alternate between the groups, so both epilogue groups
-// and the MMAs of the next cluster tile run concurrently. Every mbarrier wait is bounded; on timeout the
+//            row tile group 1 hands its top-3 to group 0 through a small global
+//            scratch (per CTA, by row-tile parity) and a named barrier; group 0
+//            merges and writes the row's outputs.
+// Four accumulators (all 512 TMEM columns) alternate between the groups, two
+// per group, so each group reads one accumulator while the MMAs fill its other
+// one, and both groups run concurrently with the MMAs. Every mbarrier wait is bounded; on timeout the
 // CTA records KMB_ETIMEDOUT in the loop state, drains its own TMA loads and
 // MMAs with bounded waits, frees TMEM and returns.
 #include "kmb_internal.cuh"
@@ -53,12 +55,18 @@ constexpr int BM = 128;                 // rows per tile (UMMA M)
 constexpr int BN = 128;                 // clusters per tile (UMMA N)
 constexpr int KP = 64;                  // bf16 per panel row (128 bytes, SWIZZLE_128B)
 constexpr int PANEL = 128 * 128;        // bytes per 128-row panel
-constexpr int NACC = 2;                 // TMEM accumulator buffers (one per epilogue group)
-constexpr int TMEM_COLS = 512;          // 2 x 128 accumulator columns + the groups' exchange area
-constexpr int XCHG_COL = NACC * BN;     // 256: per-row top-3 handed from group 1 to group 0
+constexpr int NACC = 4;                 // TMEM accumulators: two per epilogue group (double-buffered)
+constexpr int TMEM_COLS = NACC * BN;    // 512 = all of TMEM
 constexpr int NTHREADS = 320;           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two groups of 4)
 constexpr int MAX_B_STAGES = 8;
 constexpr long long kTimeoutCycles = 4000000000ll;  // ~2 s at 1.9 GHz
+
+// One row's running top-3 (score space) as handed between the epilogue groups.
+struct Top3x {
+    float b, s, t;
+    int ib, is;
+    int pad[3];
+};
 
 struct Params {
     int64_t n;
@@ -72,6 +80,7 @@ struct Params {
     float *d2;
     RecheckEntry *queue;
     LoopState *st;
+    Top3x *xchg;  // per CTA: 2 x 128 rows of group 1's top-3 (row-tile parity)
 };
 
 struct Barriers {
@@ -256,29 +265,6 @@ __device__ __forceinline__ Top3 top3_merge(const Top3 &x, const Top3 &y) {
     return r;
 }
 
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const Top3 &r) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-        "r"(__float_as_uint(r.b)), "r"(__float_as_uint(r.s)), "r"(__float_as_uint(r.t)), "r"((uint32_t)r.ib),
-        "r"((uint32_t)r.is), "r"(0u), "r"(0u), "r"(0u)
-        : "memory");
-    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ Top3 tmem_ld8(uint32_t taddr) {
-    uint32_t q[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7])
-                 : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    Top3 r;
-    r.b = __uint_as_float(q[0]);
-    r.s = __uint_as_float(q[1]);
-    r.t = __uint_as_float(q[2]);
-    r.ib = (int)q[3];
-    r.is = (int)q[4];
-    return r;
-}
 
 __global__ void __launch_bounds__(NTHREADS, 1)
 assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant__ CUtensorMap tmXl,
@@ -423,17 +409,17 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
         bool ok = true;
         // Accumulators start from -h (written here, one row per lane), so after the
         // MMAs they hold y = x.c - h = -score and the argmin becomes a max over y.
-        {
-            const float *hn = p.h + (size_t)(group % p.ntiles_n) * BN;
+        for (int a0 = group; a0 < NACC; a0 += 2) {  // this group's accumulators: running tiles a0, a0 + 4, ...
+            const float *hn = p.h + (size_t)(a0 % p.ntiles_n) * BN;
 #pragma unroll 1
             for (int c0 = 0; c0 < BN; c0 += 32) {
                 __syncwarp();
-                tmem_st32_from(lane_base + (uint32_t)(group * BN + c0), hn + c0);
+                tmem_st32_from(lane_base + (uint32_t)(a0 * BN + c0), hn + c0);
             }
             tmem_wait_st();
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bar->acc_empty[group]);
+            if (lane == 0) mbar_arrive(&bar->acc_empty[a0]);
         }
         // Both groups pass the same number of named barriers (one per row tile),
         // also after an abort, so neither can be left waiting on the other.
@@ -444,8 +430,8 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             r.ib = r.is = 0;
             for (int j = 0; j < p.ntiles_n; ++j, ++acount) {
                 if ((int)(acount & 1) != group || !ok) continue;
-                const int slot = group;
-                const int use = (int)(acount >> 1);
+                const int slot = (int)(acount % NACC);
+                const int use = (int)(acount / NACC);
                 // every lane waits; the warp proceeds only if all lanes saw completion
                 if (!__all_sync(0xffffffffu, mbar_wait(&bar->acc_full[slot], use & 1, abort))) {
                     ok = false;
@@ -499,18 +485,28 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             r.b = -r.b;
             r.s = -r.s;
             r.t = -r.t;
-            // Group 1 hands its top-3 to group 0 through TMEM columns XCHG_COL..+7 of
-            // the same lanes (alternating by row-tile parity), then group 0 merges.
-            const uint32_t xaddr = lane_base + (uint32_t)(XCHG_COL + 8 * (lt & 1));
-            __syncwarp();
+            // Group 1 hands its top-3 to group 0 (same rows) through the CTA's
+            // scratch slot for this row-tile parity, then group 0 merges.
+            Top3x *xs = p.xchg + ((size_t)blockIdx.x * 2 + (lt & 1)) * BM + row_in_tile;
             if (group == 1) {
-                tmem_st8(xaddr, r);
-                tc_fence_before();
+                Top3x q;
+                q.b = r.b;
+                q.s = r.s;
+                q.t = r.t;
+                q.ib = r.ib;
+                q.is = r.is;
+                *xs = q;
+                __threadfence_block();
             }
             named_bar_sync(1 + quarter, 64);
             if (group == 1 || !ok) continue;
-            tc_fence_after();
-            const Top3 o = tmem_ld8(xaddr);
+            const Top3x q = *xs;
+            Top3 o;
+            o.b = q.b;
+            o.s = q.s;
+            o.t = q.t;
+            o.ib = q.ib;
+            o.is = q.is;
             r = top3_merge(r, o);
             const int64_t row = (int64_t)tile * BM + row_in_tile;
             if (row < p.n) {
@@ -601,6 +597,8 @@ __global__ void reset_cmax_kernel(double *p, const LoopState *st) {
 
 }  // namespace tc
 
+size_t tc_xchg_bytes(int num_sms) { return (size_t)num_sms * 2 * tc::BM * sizeof(tc::Top3x); }
+
 int64_t tc_dpad(int64_t d) { return (d + tc::KP - 1) / tc::KP * tc::KP; }
 int64_t tc_kpad(int64_t k) { return (k + tc::BN - 1) / tc::BN * tc::BN; }
 bool tc_supported(int64_t d) { return tc_dpad(d) <= 256; }
@@ -658,7 +656,7 @@ static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t d
 // the shape is outside the kernel's limits or tensor maps cannot be encoded.
 int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
                      const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
-                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, cudaStream_t s) {
+                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, cudaStream_t s) {
     const int64_t dpad = tc_dpad(d), kpad = tc_kpad(k);
     if (dpad > 256) return KMB_EUNSUPPORTED;
     if (n == 0) return KMB_OK;
@@ -697,6 +695,7 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     p.d2 = d2;
     p.queue = queue;
     p.st = st;
+    p.xchg = (tc::Top3x *)xchg;
     if (cudaFuncSetAttribute(tc::assign_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return KMB_ECUDA;

@@ -61,7 +61,7 @@ struct Workspace {
     DevBuf X, C0, Cout, labels, d2, xnorm, Ccur, Cnew, Ct, h, queue;
     DevBuf H, Gs, counts, offsets, piece_base, perm, records, shift_part, empty_flag, empty_ids;
     DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;
-    DevBuf Xhi, Xlo, Chi, Clo;
+    DevBuf Xhi, Xlo, Chi, Clo, tcx;
     // Grows `b` to at least `bytes`; returns false on allocation failure.
     bool ensure(DevBuf &b, size_t bytes);
     void release();
@@ -108,9 +108,11 @@ void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *
 // C -> Chi/Clo [kpad][dpad], -h = -0.5||c||^2 (kpad, -inf padding), max ||c||.
 void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, void *Clo, float *h,
                               double *cnorm_max, const LoopState *st, cudaStream_t s);
+// xchg: tc_xchg_bytes(num_sms) bytes of device scratch (epilogue hand-off).
 int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
                      const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
-                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, cudaStream_t s);
+                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, cudaStream_t s);
+size_t tc_xchg_bytes(int num_sms);
 
 // ---- update ----------------------------------------------------------------
 UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d);

@@ -1,0 +1,71 @@
+"""The drop-in proof: a oneDAL client compiled against the unchanged oneDAL
+headers and runtime sources (integration/Makefile), whose host-policy k-means
+dispatchers are integration/kmeans_dispatcher_b200.cpp. On a GPU it must
+reproduce the reference's gold known-answer case (cpp/oneapi/dal/algo/kmeans/
+test/fixture.hpp:156-203 with test/data.hpp) through dal::train / dal::infer;
+without a GPU the dispatcher must surface the library's failure as a oneDAL
+exception. The client is built only where the reference tree is present; the
+built binary travels with the tree."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLIENT = os.path.join(ROOT, "integration", "_build", "kmeans_client")
+
+needs_client = pytest.mark.skipif(not os.path.exists(CLIENT), reason="integration client not built")
+
+
+def _gold_file(tmp_path):
+    g = json.load(open(os.path.join(ROOT, "tests", "golden", "gold.json")))
+    X = np.asarray(g["data"], np.float64).ravel()
+    C = np.asarray(g["initial_centroids"], np.float64).ravel()
+    p = tmp_path / "gold.txt"
+    p.write_text("%d %d %d\n%s\n%s\n" % (g["row_count"], g["column_count"], g["cluster_count"],
+                                          " ".join(repr(float(v)) for v in X), " ".join(repr(float(v)) for v in C)))
+    return g, str(p)
+
+
+def _parse(out):
+    res = {}
+    for line in out.splitlines():
+        key, _, rest = line.partition(" ")
+        res[key] = rest
+    return res
+
+
+@needs_client
+def test_client_links_b200_library():
+    deps = subprocess.run(["ldd", CLIENT], capture_output=True, text=True).stdout
+    assert "libonedal_b200_kmeans.so" in deps and "not found" not in deps
+
+
+@needs_client
+def test_client_reports_library_failure_as_onedal_exception(tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the GPU test covers the success path")
+    _, path = _gold_file(tmp_path)
+    r = subprocess.run([CLIENT, path, "double"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 1
+    assert r.stdout.startswith("exception: ")
+
+
+@pytest.mark.gpu
+@needs_client
+@pytest.mark.parametrize("dtype,rtol", [("double", 1e-7), ("float", 1e-4)])
+def test_client_gold_through_dal_train_infer(tmp_path, dtype, rtol):
+    g, path = _gold_file(tmp_path)
+    r = subprocess.run([CLIENT, path, dtype], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = _parse(r.stdout)
+    cen = np.array(out["centroids"].split(), np.float64).reshape(g["cluster_count"], g["column_count"])
+    np.testing.assert_allclose(cen, np.asarray(g["expected_centroids"]).reshape(cen.shape), rtol=rtol, atol=rtol)
+    resp = np.array(out["responses"].split(), np.int64)
+    assert (resp == np.asarray(g["expected_responses"]).ravel()).all()
+    assert abs(float(out["objective"]) - g["expected_objective"]) <= rtol * g["expected_objective"]
+    assert abs(float(out["infer_objective"]) - g["expected_objective"]) <= rtol * g["expected_objective"]
+    assert out.get("invalid_argument") == "ok"
