@@ -28,6 +28,8 @@ import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# (525.47 MB read + 11.61 MB written) / 1,000,000 rows, assign_tc_kernel at d=128, k=1024
+TC_DRAM_BYTES_PER_ROW = 537.08
 sys.path.insert(0, ROOT)
 
 METRIC = "Lloyd iter/s n=20M,d=128,k=1024 BF16-TC vs FP32 plain; p50/p99 infer latency"
@@ -456,13 +458,24 @@ def run_b200(args):
         # FP32 FFMA issue peak: 148 SMs x 128 lanes x 2 flop x max SM clock (no measured figure exists).
         peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
         peak_note = "fp32 FFMA issue peak at max SM clock (148x128x2xclock)"
+    dpad = (d + 63) // 64 * 64
+    if form == _native.KMB_FORM_BF16X3:
+        algo_bytes = 4 * n * dpad + 8 * n  # Xhi + Xlo read once, labels + d2 written
+        # DRAM read+write bytes per row from the ncu capture summarised in
+        # profiles/assign_tc_kernel_precision_n1M.txt (scaled by rows).
+        traffic = args.traffic_bytes if args.traffic_bytes is not None else TC_DRAM_BYTES_PER_ROW * n
+        traffic_src = "ncu dram__bytes_read+write per row of a 1M-row capture, x rows"
+    else:
+        algo_bytes = 4 * n * d + 8 * n
+        traffic = args.traffic_bytes
+        traffic_src = None
     roofline = {"bound": "tensor" if form == _native.KMB_FORM_BF16X3 else "fp32_fma", "achieved": achieved_tflops,
                 "peak": peak, "unit": "TFLOP/s", "frac": (achieved_tflops / peak) if achieved_tflops else None,
-                "traffic": args.traffic_bytes, "peak_source": peak_note,
+                "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_note,
                 "kernel_ms_avg": avg_kernel_s * 1e3, "kernel_launches": kl.value,
                 "update_ms_avg": (ut.value / max(ul.value, 1)),
                 "recheck_ms_avg": (rt.value / max(rl.value, 1)) if rl.value else None, "algorithmic_flops_per_launch": flops_per_launch,
-                "algorithmic_bytes_per_launch": n * d * 4 + 4 * n}
+                "algorithmic_bytes_per_launch": algo_bytes}
 
     # e2e through the public API with pinned host buffers.
     e2e = None
@@ -505,19 +518,20 @@ def run_b200(args):
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value * (world if False else 1), "unit": UNIT, "n_gpus": world,
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / max(iters_done, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "precision n=20000000 d=128 k=1024 float32, 1024 blobs std 1 in U[-5,5]^128, "
+            "config": {"workload": f"precision n={n} d={d} k={k} float32, {k} blobs std 1 in U[-5,5]^{d}, "
                                    "10% bisector near-ties", "n": n, "d": d, "k": k,
                        "form": args.form, "iterations_completed": iters_done,
-                       "l2": "inputs (10.24 GB) larger than L2; no flush"},
+                       "l2": f"inputs ({n * d * 4 / 1e9:.2f} GB) larger than L2; no flush"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": gpu_launches, "clocks": clocks,
             "plain_fp32_value": plain_value,
             "bf16_over_plain": (value / plain_value) if plain_value else None,
-            "recheck_rows_last_iteration": st.rechecked_rows,
+            "recheck_rows_per_iteration": st.rechecked_rows / max(iters_done, 1),
+            "full_rescans_per_iteration": st.full_rescans / max(iters_done, 1),
             "serving": serving,
             "batched": batched,
         }
@@ -532,7 +546,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--form", default="plain", choices=["bf16x3", "plain"])
+    ap.add_argument("--form", default="bf16x3", choices=["bf16x3", "plain"])
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--cpu-sample-rows", type=int, default=200_000)
     ap.add_argument("--traffic-bytes", type=float, default=None)

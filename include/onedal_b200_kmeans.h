@@ -79,10 +79,12 @@ typedef struct kmb_params {
 
 /* Per-call diagnostics (optional output of the train/infer calls). */
 typedef struct kmb_stats {
-    int64_t rechecked_rows;   /* rows re-scored in FP64 in the last assignment  */
+    int64_t rechecked_rows;   /* rows re-scored in FP64 in the last assignment
+                                 (kmb_lloyd_iterate: summed over its assignments) */
     int64_t changed_by_recheck;
     int64_t empty_cluster_events; /* clusters reseeded over the whole train  */
     double last_shift;        /* sum ||c_old - c_new||^2 of the last update     */
+    int64_t full_rescans;     /* of those, rows re-scored against all k clusters */
 } kmb_stats;
 
 /* Context: one CUDA device, one stream, a workspace that grows on demand.

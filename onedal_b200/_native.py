@@ -50,7 +50,8 @@ class kmb_params(ctypes.Structure):
 
 class kmb_stats(ctypes.Structure):
     _fields_ = [("rechecked_rows", ctypes.c_int64), ("changed_by_recheck", ctypes.c_int64),
-                ("empty_cluster_events", ctypes.c_int64), ("last_shift", ctypes.c_double)]
+                ("empty_cluster_events", ctypes.c_int64), ("last_shift", ctypes.c_double),
+                ("full_rescans", ctypes.c_int64)]
 
 
 class NativeError(RuntimeError):

@@ -176,35 +176,39 @@ __global__ void reset_iteration_kernel(LoopState *st) {
     if (st->done) return;
     st->n_recheck = 0;
     st->n_changed = 0;
+    st->n_full = 0;
 }
 
 __global__ void account_recheck_kernel(LoopState *st) {
     if (st->done) return;
     st->rechecked_total += st->n_recheck;
+    st->full_total += st->n_full;
 }
 
 // One assignment pass of the plain form (+ optional FP64 recheck) under C.
 template <typename F>
 int assign_pass_tc(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, int64_t k, int32_t *labels,
-                   F *d2, LoopState *st) {
+                   F *d2, LoopState *st, bool prior) {
     return KMB_EUNSUPPORTED;  // float64 data has no tensor-core form
 }
 
 template <>
 int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d, const float *C, int64_t k,
-                          int32_t *labels, float *d2, LoopState *st) {
+                          int32_t *labels, float *d2, LoopState *st, bool prior) {
     kmb::Workspace &ws = ctx->ws;
     cudaStream_t s = ctx->stream;
     kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
     reset_iteration_kernel<<<1, 1, 0, s>>>(st);
     KMB_LAUNCHED();
-    kmb::launch_prep_centroids_tc(C, k, d, ws.Chi.ptr, ws.Clo.ptr, (float *)ws.h.ptr, &sc->cnorm_max, st, s);
+    kmb::launch_prep_centroids_tc(C, k, d, ws.Chi.ptr, ws.Clo.ptr, (float *)ws.h.ptr, &sc->cnorm_max,
+                                  &sc->cnorm_max_prev, st, s);
     int rc;
     {
         KernelTimer timer(ctx, 1);
         rc = kmb::launch_assign_tc(ws.Xhi.ptr, ws.Xlo.ptr, n, d, ws.Chi.ptr, ws.Clo.ptr, (const float *)ws.h.ptr, k,
                                    (const float *)ws.xnorm.ptr, &sc->cnorm_max, labels, d2,
-                                   (RecheckEntry *)ws.queue.ptr, st, ctx->num_sms, ws.tcx.ptr, s);
+                                   (RecheckEntry *)ws.queue.ptr, st, ctx->num_sms, ws.tcx.ptr, prior,
+                                   (const double *)ws.shift_part.ptr, &sc->cnorm_max_prev, s);
     }
     if (rc != KMB_OK) return fail(ctx, rc, "tensor-core assignment launch failed (d=%lld)", (long long)d);
     {
@@ -219,8 +223,8 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
 
 template <typename F>
 int assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, int64_t k, bool recheck,
-                int32_t *labels, F *d2, LoopState *st, bool tc = false) {
-    if (tc) return assign_pass_tc<F>(ctx, X, n, d, C, k, labels, d2, st);
+                int32_t *labels, F *d2, LoopState *st, bool tc = false, bool prior = false) {
+    if (tc) return assign_pass_tc<F>(ctx, X, n, d, C, k, labels, d2, st, prior);
     kmb::Workspace &ws = ctx->ws;
     cudaStream_t s = ctx->stream;
     const int64_t kpad = round_up(k, kBN);
@@ -244,12 +248,18 @@ int assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, 
     return KMB_OK;
 }
 
-// Splits X into the BF16 hi/lo panels the tensor-core form reads (once per call).
+// Row norms for the pass, plus -- for the tensor-core form -- the BF16 hi/lo
+// panels it reads, both from one read of X (once per call).
 template <typename F>
-void split_rows(kmb_context *ctx, const F *X, int64_t n, int64_t d) {}
+void prepare_rows(kmb_context *ctx, const F *X, int64_t n, int64_t d, bool tc) {
+    kmb::launch_row_norms<F>(X, n, d, (F *)ctx->ws.xnorm.ptr, ctx->stream);
+}
 template <>
-void split_rows<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d) {
-    kmb::launch_split_rows(X, n, d, ctx->ws.Xhi.ptr, ctx->ws.Xlo.ptr, ctx->stream);
+void prepare_rows<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d, bool tc) {
+    if (tc)
+        kmb::launch_split_rows(X, n, d, ctx->ws.Xhi.ptr, ctx->ws.Xlo.ptr, (float *)ctx->ws.xnorm.ptr, ctx->stream);
+    else
+        kmb::launch_row_norms<float>(X, n, d, (float *)ctx->ws.xnorm.ptr, ctx->stream);
 }
 
 template <typename F>
@@ -287,16 +297,16 @@ int run_loop(kmb_context *ctx, const F *X, int64_t n, int64_t d, F *C, const kmb
     init_state(ctx->h_state[0], p->accuracy_threshold);
     KMB_CUDA(cudaMemcpyAsync(st, ctx->h_state, sizeof(LoopState), cudaMemcpyHostToDevice, s));
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
-    kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
     const bool tc = p->form == KMB_FORM_BF16X3;
-    if (tc) split_rows<F>(ctx, X, n, d);
+    prepare_rows<F>(ctx, X, n, d, tc);
     const int64_t T = p->max_iteration_count;
     int64_t enq = 0;
     int64_t batch = 2;
     while (enq < T) {
         const int64_t upto = std::min(T, enq + batch);
         for (; enq < upto; ++enq) {
-            int rc = assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, d2, st, tc);
+            // from the second iteration on, labels/d2/shift_part describe the previous pass
+            int rc = assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, d2, st, tc, /*prior=*/enq > 0);
             if (rc) return rc;
             KernelTimer timer(ctx, 2);
             kmb::launch_update<F>(X, plan, labels, d2, C, Cnew, ws, st, /*commit=*/true, s);
@@ -332,6 +342,7 @@ int iterate_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, void *C
     if (iteration_count) *iteration_count = hs.iterations;
     if (stats) {
         stats->rechecked_rows = hs.rechecked_total;
+        stats->full_rescans = hs.full_total;
         stats->changed_by_recheck = hs.n_changed;
         stats->empty_cluster_events = hs.empty_events;
         stats->last_shift = hs.shift;
@@ -372,7 +383,10 @@ int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     KMB_CUDA(cudaMemcpyAsync(Ccur, C0, sizeof(F) * k * d, cudaMemcpyDeviceToDevice, s));
     if ((rc = run_loop<F>(ctx, X, n, d, Ccur, p, plan, labels, recheck))) return rc;
     // Responses against the final centroids, then the exact objective.
-    if ((rc = assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, d2, st_final, tc))) return rc;
+    // (after at least one iteration, the last assignment + update seed the prior bound)
+    if ((rc = assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, d2, st_final, tc,
+                             /*prior=*/p->max_iteration_count > 0)))
+        return rc;
     double *obj_dev = &sc->objective;
     kmb::launch_objective<F>(X, n, d, Ccur, labels, (double *)ws.obj_part.ptr, obj_dev, s);
     KMB_CUDA(cudaGetLastError());
@@ -391,6 +405,7 @@ int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     if (iteration_count) *iteration_count = hs.iterations;
     if (stats) {
         stats->rechecked_rows = ctx->h_state[1].n_recheck;
+        stats->full_rescans = ctx->h_state[1].n_full;
         stats->changed_by_recheck = ctx->h_state[1].n_changed;
         stats->empty_cluster_events = hs.empty_events;
         stats->last_shift = hs.shift;
@@ -421,8 +436,7 @@ int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     init_state(ctx->h_state[1], 0.0);
     KMB_CUDA(cudaMemcpyAsync(st, &ctx->h_state[1], sizeof(LoopState), cudaMemcpyHostToDevice, s));
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
-    kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
-    if (tc) split_rows<F>(ctx, X, n, d);
+    prepare_rows<F>(ctx, X, n, d, tc);
     if ((rc = assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, (F *)ws.d2.ptr, st, tc))) return rc;
     if (compute_objective)
         kmb::launch_objective<F>(X, n, d, C, labels, (double *)ws.obj_part.ptr, &sc->objective, s);
@@ -437,6 +451,7 @@ int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     if (compute_objective && objective) *objective = obj_h;
     if (stats) {
         stats->rechecked_rows = ctx->h_state[1].n_recheck;
+        stats->full_rescans = ctx->h_state[1].n_full;
         stats->changed_by_recheck = ctx->h_state[1].n_changed;
         stats->empty_cluster_events = 0;
         stats->last_shift = 0.0;
@@ -464,8 +479,7 @@ int step_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, const void
     KMB_CUDA(cudaMemcpyAsync(st, ctx->h_state, sizeof(LoopState), cudaMemcpyHostToDevice, s));
     KMB_CUDA(cudaMemcpyAsync(Ccur, Cin, sizeof(F) * k * d, cudaMemcpyDeviceToDevice, s));
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
-    kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
-    if (tc) split_rows<F>(ctx, X, n, d);
+    prepare_rows<F>(ctx, X, n, d, tc);
     if ((rc = assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, (F *)ws.d2.ptr, st, tc))) return rc;
     kmb::launch_update<F>(X, plan, labels, (const F *)ws.d2.ptr, Ccur, (F *)C_out, ws, st, /*commit=*/false, s);
     KMB_CUDA(cudaGetLastError());
@@ -495,8 +509,7 @@ int partial_impl(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C,
     init_state(ctx->h_state[1], 0.0);
     KMB_CUDA(cudaMemcpyAsync(st, &ctx->h_state[1], sizeof(LoopState), cudaMemcpyHostToDevice, s));
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
-    kmb::launch_row_norms<F>(X, n, d, (F *)ws.xnorm.ptr, &sc->xnorm_max, s);
-    if (tc) split_rows<F>(ctx, X, n, d);
+    prepare_rows<F>(ctx, X, n, d, tc);
     if ((rc = assign_pass<F>(ctx, X, n, d, C, k, tc, labels, (F *)ws.d2.ptr, st, tc))) return rc;
     kmb::launch_partial_sums<F>(X, plan, labels, sums, counts, ws, s);
     if (sq_distances)

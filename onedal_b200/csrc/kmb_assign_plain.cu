@@ -282,21 +282,18 @@ __global__ void prep_centroids_kernel(const F *__restrict__ C, int k, int d, int
     }
 }
 
+// ||x||^2 per row: FP64 sum of squares (lane t, t+32, ...; then a butterfly),
+// rounded to F. One warp per row, grid-stride over rows.
 template <typename F>
-__global__ void row_norms_kernel(const F *__restrict__ X, int64_t n, int d, F *__restrict__ xnorm,
-                                 double *__restrict__ xnorm_max) {
-    // One warp per row.
-    const int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__global__ void row_norms_kernel(const F *__restrict__ X, int64_t n, int d, F *__restrict__ xnorm) {
     const int lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const F *x = X + row * d;
-    double s = 0.0;
-    for (int t = lane; t < d; t += 32) s += (double)x[t] * (double)x[t];
-    for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
-    if (lane == 0) {
-        xnorm[row] = F(s);
-        if (xnorm_max) atomicMax(reinterpret_cast<unsigned long long *>(xnorm_max),
-                                 (unsigned long long)__double_as_longlong(sqrt(s)));
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < n; row += warps) {
+        const F *x = X + row * d;
+        double s = 0.0;
+        for (int t = lane; t < d; t += 32) s += (double)x[t] * (double)x[t];
+        for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+        if (lane == 0) xnorm[row] = F(s);
     }
 }
 
@@ -318,10 +315,10 @@ void launch_prep_centroids(const F *C, int64_t k, int64_t d, int64_t kpad, F *Ct
 }
 
 template <typename F>
-void launch_row_norms(const F *X, int64_t n, int64_t d, F *xnorm, double *xnorm_max, cudaStream_t s) {
+void launch_row_norms(const F *X, int64_t n, int64_t d, F *xnorm, cudaStream_t s) {
     if (n == 0) return;
-    const int64_t blocks = (n * 32 + 255) / 256;
-    row_norms_kernel<F><<<(unsigned)blocks, 256, 0, s>>>(X, n, (int)d, xnorm, xnorm_max);
+    const int64_t blocks = std::min<int64_t>((n * 32 + 255) / 256, 148 * 16);
+    row_norms_kernel<F><<<(unsigned)blocks, 256, 0, s>>>(X, n, (int)d, xnorm);
     KMB_LAUNCHED();
 }
 
@@ -346,7 +343,7 @@ void launch_assign_plain(const F *X, int64_t n, int64_t d, const F *Ct, const F 
 #define KMB_INST(F)                                                                                                \
     template void launch_prep_centroids<F>(const F *, int64_t, int64_t, int64_t, F *, F *, double *,            \
                                            const LoopState *, cudaStream_t);                                     \
-    template void launch_row_norms<F>(const F *, int64_t, int64_t, F *, double *, cudaStream_t);                  \
+    template void launch_row_norms<F>(const F *, int64_t, int64_t, F *, cudaStream_t);                                            \
     template void launch_assign_plain<F>(const F *, int64_t, int64_t, const F *, const F *, int64_t, int64_t,    \
                                          const F *, const double *, int32_t *, F *, RecheckEntry *, LoopState *, \
                                          cudaStream_t);

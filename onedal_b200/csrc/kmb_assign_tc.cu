@@ -76,6 +76,12 @@ struct Params {
     const float *h;  // -0.5||c_j||^2 per cluster, -inf padding
     const float *xnorm;
     const double *cnorm_max;
+    // Prior bound (valid only when `prior`): labels / d2 of the previous pass
+    // (read before this pass overwrites them), per-cluster squared shifts of the
+    // update in between, and max ||c|| of the previous centroids.
+    int prior;
+    const double *shift_part;
+    const double *cnorm_max_prev;
     int32_t *labels;
     float *d2;
     RecheckEntry *queue;
@@ -185,6 +191,22 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// tcgen05.ld of 32 columns without the wait (the caller issues wait::ld).
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, float *v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
@@ -423,11 +445,43 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
         }
         // Both groups pass the same number of named barriers (one per row tile),
         // also after an abort, so neither can be left waiting on the other.
+        const double cmax_prev = p.prior ? *p.cnorm_max_prev : 0.0;
         for (int lt = 0; lt < my_tiles; ++lt) {
             const int tile = blockIdx.x + lt * gridDim.x;
+            const int64_t row = (int64_t)tile * BM + row_in_tile;
+            const float xn = row < p.n ? p.xnorm[row] : 0.0f;
+            // Per-score error bound e of this row (see the header); band = 2e.
+            const double xl = sqrt(fmax((double)xn, 0.0));
+            const double xc = xl * cmax;
+            const double e = 1.0625 * ((3.03 * ub2 + 2.0 * 3.0 * p.dpad * 2.0 * u) * xc +
+                                       2.0 * u * (0.5 * cmax * cmax + xc));
+            const double band = 2.0 * e;
+            const float band_up = __double2float_ru(band);
+            // Prior lower bound on the row's final best y (y = -score). With l the
+            // previous label and D_old^2 <= d2_prev + (its rounding bound), the
+            // triangle inequality gives ||x - c_new[l]|| <= D_old + ||c_new[l] -
+            // c_old[l]||, hence best y >= 0.5 (||x||^2 - (D_old + delta_l)^2) - e.
+            // Any cluster that can be the best or lie inside the band of the
+            // best has y >= that bound - band, so lower values are skipped.
+            float thr0 = __int_as_float(0xff800000);
+            const int lprev = (p.prior && row < p.n) ? p.labels[row] : -1;
+            if (lprev >= 0 && lprev < p.k) {
+                const int l = lprev;
+                const double d2p = (double)p.d2[row];
+                const double xcp = xl * cmax_prev;
+                const double e_prev = 1.0625 * ((3.03 * ub2 + 2.0 * 3.0 * p.dpad * 2.0 * u) * xcp +
+                                                2.0 * u * (0.5 * cmax_prev * cmax_prev + xcp));
+                const double dsq = fmax(d2p, 0.0) + 2.0 * e_prev + 2.0 * u * (fabs(d2p) + (double)xn);
+                const double rad = sqrt(dsq) + sqrt(p.shift_part[l]) * (1.0 + 1e-12);
+                const double r2 = rad * rad;
+                const double lb = 0.5 * ((double)xn * (1.0 - 2.0 * u) - r2) - 3.0 * e -
+                                  9.5367431640625e-7 * ((double)xn + r2);  // 2^-20 slack for this arithmetic
+                if (lb >= -3.0e38) thr0 = __double2float_rd(lb);  // also rejects NaN
+            }
             Top3 r;  // in y = -score space: b >= s >= t
             r.b = r.s = r.t = __int_as_float(0xff800000);
             r.ib = r.is = 0;
+            float thr = thr0;  // values below thr cannot change the outputs
             for (int j = 0; j < p.ntiles_n; ++j, ++acount) {
                 if ((int)(acount & 1) != group || !ok) continue;
                 const int slot = (int)(acount % NACC);
@@ -441,36 +495,68 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 // -h of the cluster tile this accumulator holds next
                 const float *hn = p.h + (size_t)((acount + NACC) % p.ntiles_n) * BN;
 #pragma unroll 1
-                for (int c0 = 0; c0 < BN; c0 += 32) {
-                    float v[32];
+                for (int c0 = 0; c0 < BN; c0 += 64) {
+                    float v[64];
                     __syncwarp();  // tcgen05.ld/st are warp-collective: reconverge after the filtered path
                     const uint32_t taddr = lane_base + (uint32_t)(slot * BN + c0);
-                    tmem_ld32(taddr, v);
+                    tmem_ld32_nowait(taddr, v);
+                    tmem_ld32_nowait(taddr + 32, v + 32);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                     tmem_st32_from(taddr, hn + c0);
-                    float m[11];
+                    tmem_st32_from(taddr + 32, hn + c0 + 32);
 #pragma unroll
-                    for (int i = 0; i < 10; ++i) m[i] = max3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
-                    m[10] = fmaxf(v[30], v[31]);
-                    const float m1 = max3f(max3f(m[0], m[1], m[2]), max3f(m[3], m[4], m[5]),
-                                           max3f(m[6], m[7], max3f(m[8], m[9], m[10])));
-                    if (m1 > r.t) {
-                        const int colbase = j * BN + c0;
+                    for (int half = 0; half < 2; ++half) {
+                        const float *w = v + 32 * half;
+                        float m[11];
 #pragma unroll
-                        for (int i = 0; i < 32; ++i) {
-                            const float x = v[i];
-                            if (x > r.t) {  // columns increase: strict '>' keeps the lowest index on ties
-                                if (x > r.b) {
-                                    r.t = r.s;
-                                    r.s = r.b;
-                                    r.is = r.ib;
-                                    r.b = x;
-                                    r.ib = colbase + i;
-                                } else if (x > r.s) {
-                                    r.t = r.s;
-                                    r.s = x;
-                                    r.is = colbase + i;
-                                } else {
-                                    r.t = x;
+                        for (int i = 0; i < 10; ++i) m[i] = max3f(w[3 * i], w[3 * i + 1], w[3 * i + 2]);
+                        m[10] = fmaxf(w[30], w[31]);
+                        const float m1 = max3f(max3f(m[0], m[1], m[2]), max3f(m[3], m[4], m[5]),
+                                               max3f(m[6], m[7], max3f(m[8], m[9], m[10])));
+                        // Rare path (a lane's chunk holds a value >= thr): the triples
+                        // holding such values are visited in column order, each one
+                        // extracted with a branch-free select chain; the code stays
+                        // small so the warps' instruction fetch is not disturbed.
+                        if (__any_sync(0xffffffffu, m1 >= thr)) {
+                            unsigned tm = 0;
+#pragma unroll
+                            for (int g = 0; g < 11; ++g) tm |= (m[g] >= thr ? 1u : 0u) << g;
+                            const int colbase = j * BN + c0 + 32 * half;
+                            while (__any_sync(0xffffffffu, tm != 0)) {
+                                const bool act = tm != 0;
+                                const int g = act ? __ffs(tm) - 1 : 0;
+                                tm &= tm - 1;
+                                float e3[3] = {w[0], w[1], w[2]};
+#pragma unroll
+                                for (int gg = 1; gg < 11; ++gg) {
+                                    const bool sel = gg == g;
+                                    e3[0] = sel ? w[3 * gg] : e3[0];
+                                    e3[1] = sel ? w[3 * gg + 1] : e3[1];
+                                    e3[2] = sel ? (gg < 10 ? w[3 * gg + 2] : __int_as_float(0xff800000)) : e3[2];
+                                }
+                                if (act) {
+#pragma unroll
+                                    for (int i = 0; i < 3; ++i) {
+                                        const float x = e3[i];
+                                        // columns increase: strict '>' keeps the lowest index on ties
+                                        if (x >= thr && x > r.t) {
+                                            const int col = colbase + 3 * g + i;
+                                            if (x > r.b) {
+                                                r.t = r.s;
+                                                r.s = r.b;
+                                                r.is = r.ib;
+                                                r.b = x;
+                                                r.ib = col;
+                                            } else if (x > r.s) {
+                                                r.t = r.s;
+                                                r.s = x;
+                                                r.is = col;
+                                            } else {
+                                                r.t = x;
+                                            }
+                                            thr = fmaxf(fmaxf(thr0, r.t), __fsub_rd(r.b, band_up));
+                                        }
+                                    }
                                 }
                             }
                         }
@@ -508,24 +594,19 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             o.ib = q.ib;
             o.is = q.is;
             r = top3_merge(r, o);
-            const int64_t row = (int64_t)tile * BM + row_in_tile;
             if (row < p.n) {
                 p.labels[row] = r.ib;
-                const float xn = p.xnorm[row];
                 p.d2[row] = 2.0f * r.b + xn;
                 if (p.queue) {
-                    const double xl = sqrt(fmax((double)xn, 0.0));
-                    const double xc = xl * cmax;
-                    const double e = 1.0625 * ((3.03 * ub2 + 2.0 * 3.0 * p.dpad * 2.0 * u) * xc +
-                                               2.0 * u * (0.5 * cmax * cmax + xc));
-                    const double band = 2.0 * e;
-                    if ((double)r.s - (double)r.b <= band) {
+                    // (a row for which no cluster passed the filters -- impossible while
+                    // the prior bound holds -- goes to the full FP64 rescan)
+                    if ((double)r.s - (double)r.b <= band || !(r.b < __int_as_float(0x7f800000))) {
                         const int qslot = atomicAdd(&p.st->n_recheck, 1);
                         RecheckEntry q;
                         q.row = (int)row;
                         q.c1 = r.ib;
                         q.c2 = r.is;
-                        q.full = ((double)r.t - (double)r.b <= band) ? 1 : 0;
+                        q.full = ((double)r.t - (double)r.b <= band || !(r.b < __int_as_float(0x7f800000))) ? 1 : 0;
                         p.queue[qslot] = q;
                     }
                 }
@@ -547,17 +628,26 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
     }
 }
 
-// x -> (bf16(x), bf16(x - bf16(x))) into [rows][dpad] panels, zero padding.
+// x -> (bf16(x), bf16(x - bf16(x))) into [rows][dpad] panels, zero padding,
+// and ||x||^2 with the summation order of row_norms_kernel. One warp per row,
+// grid-stride over rows; every element of X is read once.
 __global__ void split_rows_kernel(const float *__restrict__ src, int64_t rows, int d, int dpad,
-                                  __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo) {
-    const int64_t total = rows * (int64_t)dpad;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = i / dpad;
-        const int t = (int)(i - r * dpad);
-        const float x = t < d ? src[r * d + t] : 0.0f;
-        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        hi[i] = h;
-        lo[i] = __float2bfloat16_rn(x - __bfloat162float(h));
+                                  __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
+                                  float *__restrict__ xnorm) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
+        const float *x = src + r * d;
+        double s = 0.0;
+        for (int t = lane; t < dpad; t += 32) {
+            const float v = t < d ? x[t] : 0.0f;
+            if (t < d) s += (double)v * (double)v;
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            hi[r * dpad + t] = h;
+            lo[r * dpad + t] = __float2bfloat16_rn(v - __bfloat162float(h));
+        }
+        for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+        if (lane == 0) xnorm[r] = (float)s;
     }
 }
 
@@ -590,8 +680,9 @@ __global__ void prep_centroids_tc_kernel(const float *__restrict__ C, int k, int
     }
 }
 
-__global__ void reset_cmax_kernel(double *p, const LoopState *st) {
+__global__ void reset_cmax_kernel(double *p, double *prev, const LoopState *st) {
     if (st && st->done) return;
+    *prev = *p;
     *p = 0.0;
 }
 
@@ -603,18 +694,19 @@ int64_t tc_dpad(int64_t d) { return (d + tc::KP - 1) / tc::KP * tc::KP; }
 int64_t tc_kpad(int64_t k) { return (k + tc::BN - 1) / tc::BN * tc::BN; }
 bool tc_supported(int64_t d) { return tc_dpad(d) <= 256; }
 
-void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, cudaStream_t s) {
+void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, float *xnorm, cudaStream_t s) {
+    if (rows == 0) return;
     const int64_t dpad = tc_dpad(d);
-    const int64_t total = rows * dpad;
-    const int blocks = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
-    tc::split_rows_kernel<<<blocks, 256, 0, s>>>(X, rows, (int)d, (int)dpad, (__nv_bfloat16 *)hi, (__nv_bfloat16 *)lo);
+    const int blocks = (int)std::min<int64_t>((rows * 32 + 255) / 256, 148 * 16);
+    tc::split_rows_kernel<<<blocks, 256, 0, s>>>(X, rows, (int)d, (int)dpad, (__nv_bfloat16 *)hi, (__nv_bfloat16 *)lo,
+                                                 xnorm);
     KMB_LAUNCHED();
 }
 
 void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, void *Clo, float *h, double *cnorm_max,
-                              const LoopState *st, cudaStream_t s) {
+                              double *cnorm_max_prev, const LoopState *st, cudaStream_t s) {
     const int64_t dpad = tc_dpad(d), kpad = tc_kpad(k);
-    tc::reset_cmax_kernel<<<1, 1, 0, s>>>(cnorm_max, st);
+    tc::reset_cmax_kernel<<<1, 1, 0, s>>>(cnorm_max, cnorm_max_prev, st);
     KMB_LAUNCHED();
     tc::prep_centroids_tc_kernel<<<(unsigned)kpad, 128, 0, s>>>(C, (int)k, (int)d, (int)dpad, (int)kpad,
                                                                  (__nv_bfloat16 *)Chi, (__nv_bfloat16 *)Clo, h,
@@ -656,8 +748,10 @@ static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t d
 // the shape is outside the kernel's limits or tensor maps cannot be encoded.
 int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
                      const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
-                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, cudaStream_t s) {
+                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, bool prior,
+                     const double *shift_part, const double *cnorm_max_prev, cudaStream_t s) {
     const int64_t dpad = tc_dpad(d), kpad = tc_kpad(k);
+    if (prior && (!shift_part || !cnorm_max_prev)) return KMB_EINVAL;
     if (dpad > 256) return KMB_EUNSUPPORTED;
     if (n == 0) return KMB_OK;
     // Shared memory plan: A stages (hi+lo panels of the row tile), B ring.
@@ -691,6 +785,9 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     p.h = h;
     p.xnorm = xnorm;
     p.cnorm_max = cnorm_max;
+    p.prior = prior ? 1 : 0;
+    p.shift_part = shift_part;
+    p.cnorm_max_prev = cnorm_max_prev;
     p.labels = labels;
     p.d2 = d2;
     p.queue = queue;

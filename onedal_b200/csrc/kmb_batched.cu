@@ -555,13 +555,21 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
     if (use_graph && max_iteration_count > 0) {
-        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = KMB_ECUDA;
+        // Capture on a private stream (the caller's may be the legacy default
+        // stream, which cannot be captured); the graph is then launched on the
+        // caller's stream, after the setup work above.
+        cudaStream_t cap = nullptr;
+        if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            rc = KMB_ECUDA;
         if (rc == KMB_OK) {
-            enqueue_iteration(s);
-            if (cudaStreamEndCapture(s, &graph) != cudaSuccess ||
+            enqueue_iteration(cap);
+            if (cudaStreamEndCapture(cap, &graph) != cudaSuccess ||
                 cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
                 rc = KMB_ECUDA;
         }
+        if (cap) cudaStreamDestroy(cap);
+        if (rc != KMB_OK) cudaGetLastError();
         for (int64_t it = 0; rc == KMB_OK && it < max_iteration_count; ++it) {
             if (cudaGraphLaunch(exec, s) != cudaSuccess) rc = KMB_ECUDA;
             launch_count() += per_iter;

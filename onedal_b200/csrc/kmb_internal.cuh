@@ -30,6 +30,9 @@ struct LoopState {
     long long rechecked_total;
     double shift;         // sum ||c_old - c_new||^2 of the current update
     double eps;
+    int n_full;           // queued rows that needed the full k rescan (this pass)
+    int pad_;
+    long long full_total;
 };
 
 // Recheck queue entry written by the assignment kernels for near-tie rows.
@@ -73,6 +76,7 @@ struct DevScalars {
     double xnorm_max;
     double objective;
     double pad;
+    double cnorm_max_prev;  // max ||c|| of the previous tensor-core pass's centroids
 };
 
 // ---- assignment (plain FMA form) ------------------------------------------
@@ -84,7 +88,7 @@ void launch_prep_centroids(const F *C, int64_t k, int64_t d, int64_t kpad, F *Ct
 
 // Row squared norms (once per call; X is constant across iterations).
 template <typename F>
-void launch_row_norms(const F *X, int64_t n, int64_t d, F *xnorm, double *xnorm_max, cudaStream_t s);
+void launch_row_norms(const F *X, int64_t n, int64_t d, F *xnorm, cudaStream_t s);
 
 // Fused distance + argmin over all clusters for every row.
 // Writes labels, d2 (squared distance to the winner, 2*best + ||x||^2, in F)
@@ -104,14 +108,20 @@ int64_t tc_dpad(int64_t d);   // d rounded up to the 64-wide K panel
 int64_t tc_kpad(int64_t k);   // k rounded up to the 128-wide cluster tile
 bool tc_supported(int64_t d); // dpad <= 256
 // X (rows x d, FP32) -> hi/lo BF16 [rows][dpad], zero padded.
-void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, cudaStream_t s);
+// x -> BF16 hi/lo panels [rows][dpad] and ||x||^2 (the same value launch_row_norms gives).
+void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, float *xnorm, cudaStream_t s);
 // C -> Chi/Clo [kpad][dpad], -h = -0.5||c||^2 (kpad, -inf padding), max ||c||.
+// Also moves the previous max ||c|| into *cnorm_max_prev before recomputing it.
 void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, void *Clo, float *h,
-                              double *cnorm_max, const LoopState *st, cudaStream_t s);
+                              double *cnorm_max, double *cnorm_max_prev, const LoopState *st, cudaStream_t s);
 // xchg: tc_xchg_bytes(num_sms) bytes of device scratch (epilogue hand-off).
+// prior: labels/d2 hold the previous pass's results under the centroids that
+// the update in between moved by sqrt(shift_part[j]); they seed a lower bound
+// on each row's best score that lets the epilogue skip hopeless clusters.
 int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
                      const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
-                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, cudaStream_t s);
+                     float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, bool prior,
+                     const double *shift_part, const double *cnorm_max_prev, cudaStream_t s);
 size_t tc_xchg_bytes(int num_sms);
 
 // ---- update ----------------------------------------------------------------

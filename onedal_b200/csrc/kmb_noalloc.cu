@@ -94,7 +94,7 @@ int infer_noalloc(const F *X, int64_t n, int64_t d, const F *C, int64_t k, int32
     p += align256(sizeof(double) * kObjectivePartials);
     double *cnorm_max = (double *)p;  // zeroed by the centroid preparation on every call
 
-    launch_row_norms<F>(X, n, d, xnorm, nullptr, s);
+    launch_row_norms<F>(X, n, d, xnorm, s);
     launch_prep_centroids<F>(C, k, d, kpad, Ct, h, cnorm_max, nullptr, s);
     launch_assign_plain<F>(X, n, d, Ct, h, k, kpad, xnorm, cnorm_max, labels, d2, nullptr, nullptr, s);
     if (objective) launch_objective<F>(X, n, d, C, labels, partials, objective, s);

@@ -7,26 +7,11 @@
 // F inputs, with the reference's score 0.5||c||^2 - x.c and its lowest-index
 // tie rule (cpp/daal/src/algorithms/kmeans/kmeans_lloyd_impl.i:197-216), so the
 // final labels equal the FP64 oracle's. Two-candidate entries (nearly all of
-// them) take two threads each; entries flagged for a full scan take a warp.
+// them) take two threads each; entries flagged for a full scan take a warp (32 clusters per step).
 #include "kmb_internal.cuh"
 
 namespace kmb {
 namespace {
-
-template <typename F>
-__device__ __forceinline__ double warp_score(const F *__restrict__ x, const F *__restrict__ c, int d, int lane) {
-    double cc = 0.0, xc = 0.0;
-    for (int t = lane; t < d; t += 32) {
-        const double cv = (double)c[t];
-        cc = fma(cv, cv, cc);
-        xc = fma((double)x[t], cv, xc);
-    }
-    for (int m = 16; m >= 1; m >>= 1) {
-        cc += __shfl_xor_sync(0xffffffffu, cc, m);
-        xc += __shfl_xor_sync(0xffffffffu, xc, m);
-    }
-    return 0.5 * cc - xc;
-}
 
 // Two-candidate entries: two threads per entry (one candidate each, a
 // sequential FP64 dot product over d), decided with one shuffle.
@@ -79,27 +64,82 @@ __global__ void recheck_pairs_kernel(const F *__restrict__ X, int d, const F *__
     if (lane == 0 && changed) atomicAdd(&st->n_changed, changed);
 }
 
-// Entries with a third cluster inside the band: a warp scans all k clusters.
+// Butterfly reduce-scatter over the warp: on entry lane L holds 32 partial sums
+// a[0..31] (one per cluster of a group of 32); on exit a[0] on lane L is the
+// total for cluster L. Every cluster's total has the same association, so equal
+// inputs give equal sums.
+template <int H>
+__device__ __forceinline__ void reduce_scatter_step(double (&a)[32], int lane) {
+    const bool upper = (lane & H) != 0;
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        const double send = upper ? a[i] : a[i + H];
+        const double keep = upper ? a[i + H] : a[i];
+        a[i] = keep + __shfl_xor_sync(0xffffffffu, send, H);
+    }
+}
+__device__ __forceinline__ void reduce_scatter32(double (&a)[32], int lane) {
+    reduce_scatter_step<16>(a, lane);
+    reduce_scatter_step<8>(a, lane);
+    reduce_scatter_step<4>(a, lane);
+    reduce_scatter_step<2>(a, lane);
+    reduce_scatter_step<1>(a, lane);
+}
+
+// Entries with a third cluster inside the band: a warp re-scores all k
+// clusters, 32 at a time. Lane L accumulates its coordinates' (t = L, L+32,
+// ...) contributions to ||c||^2 and x.c for the 32 clusters (coalesced loads of
+// each centroid row), then one reduce-scatter per quantity leaves cluster
+// j0 + L's sums on lane L. Lanes keep a running best in ascending cluster
+// order; the warp argmin breaks ties to the lowest index.
 template <typename F>
-__global__ void recheck_full_kernel(const F *__restrict__ X, int d, const F *__restrict__ C, int k,
-                                    const RecheckEntry *__restrict__ queue, int32_t *__restrict__ labels,
-                                    F *__restrict__ d2, const F *__restrict__ xnorm, LoopState *st) {
+__global__ void __launch_bounds__(256) recheck_full_kernel(const F *__restrict__ X, int d, const F *__restrict__ C,
+                                                           int k, const RecheckEntry *__restrict__ queue,
+                                                           int32_t *__restrict__ labels, F *__restrict__ d2,
+                                                           const F *__restrict__ xnorm, LoopState *st) {
     if (st->done) return;
     const int count = st->n_recheck;
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
-    int changed = 0;
+    int changed = 0, fulls = 0;
     for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += warps) {
         const RecheckEntry q = queue[w];
         if (!q.full) continue;
+        ++fulls;
         const F *x = X + (int64_t)q.row * d;
-        double best = warp_score(x, C, d, lane);
-        int bi = 0;
-        for (int j = 1; j < k; ++j) {
-            const double v = warp_score(x, C + (int64_t)j * d, d, lane);
-            if (v < best) {  // ascending j: lowest index on ties
-                best = v;
-                bi = j;
+        double best = 0.0;
+        int bi = 0x7fffffff;
+        for (int j0 = 0; j0 < k; j0 += 32) {
+            double xc[32], cc[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) xc[i] = cc[i] = 0.0;
+            for (int t = lane; t < d; t += 32) {
+                const double xv = (double)x[t];
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const int j = min(j0 + i, k - 1);  // rows past k are read but not used
+                    const double cv = (double)C[(int64_t)j * d + t];
+                    cc[i] = fma(cv, cv, cc[i]);
+                    xc[i] = fma(xv, cv, xc[i]);
+                }
+            }
+            reduce_scatter32(cc, lane);
+            reduce_scatter32(xc, lane);
+            const int j = j0 + lane;
+            if (j < k) {
+                const double sc = 0.5 * cc[0] - xc[0];
+                if (bi == 0x7fffffff || sc < best) {  // ascending j per lane: lowest index on ties
+                    best = sc;
+                    bi = j;
+                }
+            }
+        }
+        for (int m = 16; m >= 1; m >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, m);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, m);
+            if (oi != 0x7fffffff && (bi == 0x7fffffff || ob < best || (ob == best && oi < bi))) {
+                best = ob;
+                bi = oi;
             }
         }
         if (lane == 0) {
@@ -109,6 +149,7 @@ __global__ void recheck_full_kernel(const F *__restrict__ X, int d, const F *__r
         }
     }
     if (lane == 0 && changed) atomicAdd(&st->n_changed, changed);
+    if (lane == 0 && fulls) atomicAdd(&st->n_full, fulls);
 }
 
 }  // namespace

@@ -112,3 +112,34 @@ def test_gold_data_tensor_core_form():
     assert centroid_rel_err(exp, r.get_model().get_centroids(), m) < 1e-6
     assert rel_close(r.get_objective_function_value(), g["expected_objective"], 1e-6)
     assert (m[r.get_responses().ravel()] == np.array(g["expected_responses"])).all()
+
+
+@pytest.mark.parametrize("n,d,k,T", [(40000, 128, 512, 6), (30000, 96, 300, 10)])
+def test_train_multi_iteration_equals_plain_form(n, d, k, T):
+    """From the second iteration on, the tensor-core epilogue skips clusters below a
+    lower bound built from the previous labels, distances and centroid shifts; whole
+    trainings must still equal the plain form with recheck bit for bit."""
+    X, C0 = workloads.make(workloads.Workload("precision", n, d, k, T, 0.0, 23 + d), "cpu", n)
+    X, C0 = X.numpy(), C0.numpy()
+    a = kmeans.train(tc_desc(k, T), X, C0)
+    p = kmeans.descriptor(np.float32).set_cluster_count(k).set_max_iteration_count(T).set_recheck(True)
+    b = kmeans.train(p, X, C0)
+    assert a.get_iteration_count() == b.get_iteration_count()
+    np.testing.assert_array_equal(a.get_responses(), b.get_responses())
+    np.testing.assert_array_equal(a.get_model().get_centroids(), b.get_model().get_centroids())
+    assert a.get_objective_function_value() == b.get_objective_function_value()
+
+
+def test_train_with_reseeds_equals_plain_form():
+    """Duplicate initial centroids empty clusters in the first iterations; reseeded
+    clusters move far, which the prior bound must absorb."""
+    rng = np.random.default_rng(24)
+    centres = rng.uniform(-5, 5, (64, 48))
+    X = (centres[rng.integers(0, 64, 20000)] + rng.standard_normal((20000, 48))).astype(np.float32)
+    C0 = np.repeat(X[:16], 4, axis=0).copy()
+    a = kmeans.train(tc_desc(64, 12), X, C0)
+    p = kmeans.descriptor(np.float32).set_cluster_count(64).set_max_iteration_count(12).set_recheck(True)
+    b = kmeans.train(p, X, C0)
+    assert a.get_iteration_count() == b.get_iteration_count()
+    np.testing.assert_array_equal(a.get_responses(), b.get_responses())
+    np.testing.assert_array_equal(a.get_model().get_centroids(), b.get_model().get_centroids())
