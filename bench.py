@@ -28,8 +28,8 @@ import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-# (525.47 MB read + 11.61 MB written) / 1,000,000 rows, assign_tc_kernel at d=128, k=1024
-TC_DRAM_BYTES_PER_ROW = 537.08
+# (525.38 MB read + 11.13 MB written) / 1,000,000 rows, assign_tc_kernel at d=128, k=1024
+TC_DRAM_BYTES_PER_ROW = 536.51
 sys.path.insert(0, ROOT)
 
 METRIC = "Lloyd iter/s n=20M,d=128,k=1024 BF16-TC vs FP32 plain; p50/p99 infer latency"
@@ -160,6 +160,7 @@ def run_serving(args, device=0):
     import numpy as np
     import torch
 
+    from onedal_b200 import _native
     from onedal_b200.serving import KMeansServer
 
     rng = np.random.default_rng(1005)
@@ -209,14 +210,16 @@ def run_serving(args, device=0):
         g = np.random.default_rng(77)
         handles = [None] * len(reqs)
         lat = {}
+        queued = {}
         done = threading.Event()
 
         def collector():
             for i in range(len(reqs)):
                 while handles[i] is None:
                     time.sleep(0.0001)
-                _, l = srv.wait(handles[i], timeout=600)
+                _, (l, qd) = srv.wait(handles[i], timeout=600, detail=True)
                 lat[i] = l
+                queued[i] = qd
             done.set()
 
         prepared = reqs
@@ -234,8 +237,20 @@ def run_serving(args, device=0):
         t1 = time.perf_counter()
         th.join()
         inf = [lat[i] for i, r in enumerate(reqs) if r[0] == "infer"]
+        tc_form = _native.KMB_FORM_BF16X3
+        forms = [srv.infer_form(ids[r[1]], r[2].shape[0]) if r[0] == "infer" else None for r in reqs]
+        by = {f: [lat[i] for i, r in enumerate(reqs) if r[0] == "infer" and forms[i] == f]
+              for f in (_native.KMB_FORM_PLAIN, tc_form)}
+        byq = {f: [queued[i] for i, r in enumerate(reqs) if r[0] == "infer" and forms[i] == f]
+               for f in (_native.KMB_FORM_PLAIN, tc_form)}
+        cls = {name: {"requests": len(by[f]), "p50_ms": float(np.percentile(by[f], 50) * 1e3) if by[f] else None,
+                      "p99_ms": float(np.percentile(by[f], 99) * 1e3) if by[f] else None,
+                      "queued_p50_ms": float(np.percentile(byq[f], 50) * 1e3) if byq[f] else None,
+                      "queued_p99_ms": float(np.percentile(byq[f], 99) * 1e3) if byq[f] else None}
+               for name, f in (("grouped_plain", _native.KMB_FORM_PLAIN), ("tensor_core", tc_form))}
         return {"requests": len(reqs), "seconds": t1 - t0, "throughput_rps": len(reqs) / (t1 - t0),
                 "p50_ms": float(np.percentile(inf, 50) * 1e3), "p99_ms": float(np.percentile(inf, 99) * 1e3),
+                "by_form": cls,
                 "train_p50_ms": float(np.percentile([lat[i] for i, r in enumerate(reqs) if r[0] == "train"] or [0],
                                                     50) * 1e3)}
 

@@ -165,6 +165,10 @@ KMB_API int kmb_lloyd_iterate(kmb_context *ctx, int dtype, const void *X, int64_
  * 4 = FP64 near-tie recheck; kernel 3 returns in *launches every kernel this
  * host thread launched since timing was enabled (total_ms = 0). */
 KMB_API int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled);
+/* Caps the CTAs of the persistent tensor-core assignment at max_sms (one per SM;
+ * 0 restores all SMs), leaving the remaining SMs to other streams' work -- the
+ * serving loop uses it so that small requests never wait for a whole launch. */
+KMB_API int kmb_context_set_max_sms(kmb_context *ctx, int max_sms);
 KMB_API int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int64_t *launches);
 
 /* Responses (and, when objective != NULL, the exact objective) of n rows X
@@ -228,10 +232,17 @@ KMB_API int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64_t 
  * infer request into one grouped launch per free lane (CUDA stream), so
  * requests that arrive while others run are picked up by the next free lane and
  * their work overlaps on the device. Small train requests run on trainer
- * threads, each with its own context. Responses are identical to kmb_infer /
- * kmb_train (plain form) on the same inputs. Host buffers passed to submit_*
- * must stay valid until the request is waited for; pinned host memory gives
- * the lowest latency. Thread-safe. */
+ * threads, each with its own context. Large infer requests (d <= 256 and
+ * n * kpad * dpad >= KMB_SERVER_TC_MACS, kpad = k rounded up to 128, dpad = d
+ * rounded up to 64) run on tensor-core workers instead (BF16x3 form with the
+ * FP64 recheck, in row chunks, on a low-priority stream, so small batches keep
+ * the SMs they need). Every response equals kmb_infer's on the same inputs in
+ * the form kmb_server_infer_form reports (plain form: bit-identical to the
+ * grouped launch; BF16x3: the FP64 oracle's labels), and kmb_train's (plain
+ * form) for trains. Host buffers passed to submit_* must stay valid until the
+ * request is waited for; pinned host memory gives the lowest latency.
+ * Thread-safe. */
+#define KMB_SERVER_TC_MACS (1LL << 33)
 typedef struct kmb_server_stats {
     int64_t completed;
     int64_t failed;
@@ -241,6 +252,7 @@ typedef struct kmb_server_stats {
     int64_t in_use_bytes;
     int64_t peak_in_use_bytes;
     int64_t budget_bytes;
+    int64_t tensor_core_requests; /* infer requests served by the tensor-core worker */
 } kmb_server_stats;
 
 KMB_API int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32_t trainers, void **server);
@@ -257,6 +269,12 @@ KMB_API int kmb_server_submit_train(void *server, const float *X, int64_t n, int
 /* Waits up to timeout_s (< 0: no limit) for a request; returns its status or
  * KMB_ETIMEDOUT; latency_s = submit -> completion on the host clock. */
 KMB_API int kmb_server_wait(void *server, int64_t request_id, double timeout_s, double *latency_s);
+/* kmb_server_wait plus queued_s = submit -> dispatch (admitted onto a lane or worker). */
+KMB_API int kmb_server_wait_detail(void *server, int64_t request_id, double timeout_s, double *latency_s,
+                                   double *queued_s);
+/* The form (KMB_FORM_PLAIN or KMB_FORM_BF16X3) an infer of n rows against
+ * model_id is served in. */
+KMB_API int kmb_server_infer_form(void *server, int32_t model_id, int64_t n, int32_t *form);
 KMB_API int kmb_server_get_stats(void *server, kmb_server_stats *stats);
 
 /* Library version string. */

@@ -22,7 +22,7 @@ EXPORTED = (
     "kmb_partial_sums", "kmb_finalize_centroids", "kmb_version", "kmb_lloyd_iterate",
     "kmb_context_set_kernel_timing", "kmb_context_kernel_time", "kmb_infer_noalloc",
     "kmb_server_create", "kmb_server_destroy", "kmb_server_add_model", "kmb_server_submit_infer",
-    "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats", "kmb_batched_train",
+    "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats", "kmb_server_infer_form", "kmb_server_wait_detail", "kmb_context_set_max_sms", "kmb_batched_train",
 )
 
 
@@ -40,7 +40,8 @@ class kmb_batched_info(ctypes.Structure):
 class kmb_server_stats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("batches", ctypes.c_int64),
                 ("batched_requests", ctypes.c_int64), ("pending", ctypes.c_int64), ("in_use_bytes", ctypes.c_int64),
-                ("peak_in_use_bytes", ctypes.c_int64), ("budget_bytes", ctypes.c_int64)]
+                ("peak_in_use_bytes", ctypes.c_int64), ("budget_bytes", ctypes.c_int64),
+                ("tensor_core_requests", ctypes.c_int64)]
 
 
 class kmb_params(ctypes.Structure):
@@ -103,7 +104,9 @@ def load_library(path: str = LIB_PATH):
             lib.kmb_server_submit_infer.argtypes = [P, I32, P, I64, I64, P, ctypes.POINTER(I64)]
             lib.kmb_server_submit_train.argtypes = [P, P, I64, I64, P, I64, I64, P, P, ctypes.POINTER(I64)]
             lib.kmb_server_wait.argtypes = [P, I64, D, ctypes.POINTER(D)]
+            lib.kmb_server_wait_detail.argtypes = [P, I64, D, ctypes.POINTER(D), ctypes.POINTER(D)]
             lib.kmb_server_get_stats.argtypes = [P, ctypes.c_void_p]
+            lib.kmb_server_infer_form.argtypes = [P, I32, I64, ctypes.POINTER(I32)]
             lib.kmb_batched_train.argtypes = [ctypes.c_int, P, I64, I64, D, I32, P, P]
             _lib = lib
     return _lib

@@ -83,12 +83,12 @@ int64_t &launch_count() {
 bool Workspace::ensure(DevBuf &b, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (b.bytes >= bytes) return true;
-    if (b.ptr) cudaFree(b.ptr);
+    if (b.ptr) cudaFreeAsync(b.ptr, stream);
     b.ptr = nullptr;
     b.bytes = 0;
     // round up to 2 MiB to limit reallocations
     const size_t rounded = (bytes + (size_t(2) << 20) - 1) / (size_t(2) << 20) * (size_t(2) << 20);
-    if (cudaMalloc(&b.ptr, rounded) != cudaSuccess) {
+    if (cudaMallocAsync(&b.ptr, rounded, stream) != cudaSuccess) {
         cudaGetLastError();
         b.ptr = nullptr;
         return false;
@@ -102,7 +102,7 @@ void Workspace::release() {
                      &counts, &offsets, &piece_base, &perm, &records, &shift_part, &empty_flag, &empty_ids,
                      &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx};
     for (DevBuf *b : all) {
-        if (b->ptr) cudaFree(b->ptr);
+        if (b->ptr) cudaFreeAsync(b->ptr, stream);
         b->ptr = nullptr;
         b->bytes = 0;
     }
@@ -181,7 +181,7 @@ __global__ void reset_iteration_kernel(LoopState *st) {
 
 __global__ void account_recheck_kernel(LoopState *st) {
     if (st->done) return;
-    st->rechecked_total += st->n_recheck;
+    st->rechecked_total += st->n_recheck + st->n_full;
     st->full_total += st->n_full;
 }
 
@@ -404,7 +404,7 @@ int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     if (objective) *objective = obj_h;
     if (iteration_count) *iteration_count = hs.iterations;
     if (stats) {
-        stats->rechecked_rows = ctx->h_state[1].n_recheck;
+        stats->rechecked_rows = ctx->h_state[1].n_recheck + ctx->h_state[1].n_full;
         stats->full_rescans = ctx->h_state[1].n_full;
         stats->changed_by_recheck = ctx->h_state[1].n_changed;
         stats->empty_cluster_events = hs.empty_events;
@@ -450,7 +450,7 @@ int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     KMB_CUDA(cudaStreamSynchronize(s));
     if (compute_objective && objective) *objective = obj_h;
     if (stats) {
-        stats->rechecked_rows = ctx->h_state[1].n_recheck;
+        stats->rechecked_rows = ctx->h_state[1].n_recheck + ctx->h_state[1].n_full;
         stats->full_rescans = ctx->h_state[1].n_full;
         stats->changed_by_recheck = ctx->h_state[1].n_changed;
         stats->empty_cluster_events = 0;
@@ -571,6 +571,7 @@ int kmb_context_create(int device, kmb_context **out) {
         return KMB_ECUDA;
     }
     ctx->own_stream = true;
+    ctx->ws.stream = ctx->stream;
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     *out = ctx;
     return KMB_OK;
@@ -581,6 +582,7 @@ int kmb_context_destroy(kmb_context *ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->ws.release();
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->recycle_events();
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -591,8 +593,11 @@ int kmb_context_destroy(kmb_context *ctx) {
 
 int kmb_context_set_stream(kmb_context *ctx, void *cuda_stream) {
     if (!ctx) return KMB_EINVAL;
+    // workspace buffers were allocated in the old stream's order
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     ctx->stream = (cudaStream_t)cuda_stream;
+    ctx->ws.stream = ctx->stream;
     ctx->own_stream = false;
     return KMB_OK;
 }
@@ -604,6 +609,7 @@ int kmb_context_release_workspace(kmb_context *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     ctx->ws.release();
+    cudaStreamSynchronize(ctx->stream);
     return KMB_OK;
 }
 
@@ -669,6 +675,14 @@ int kmb_lloyd_iterate(kmb_context *ctx, int dtype, const void *X, int64_t n, int
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
     if (dtype == KMB_F32) return iterate_impl<float>(ctx, X, n, d, C, params, labels, iteration_count, stats);
     return iterate_impl<double>(ctx, X, n, d, C, params, labels, iteration_count, stats);
+}
+
+int kmb_context_set_max_sms(kmb_context *ctx, int max_sms) {
+    if (!ctx || max_sms < 0) return KMB_EINVAL;
+    int all = 148;
+    cudaDeviceGetAttribute(&all, cudaDevAttrMultiProcessorCount, ctx->device);
+    ctx->num_sms = (max_sms == 0 || max_sms > all) ? all : max_sms;
+    return KMB_OK;
 }
 
 int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled) {

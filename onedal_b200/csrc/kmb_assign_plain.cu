@@ -239,15 +239,8 @@ assign_plain_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restri
                 const double xl = sqrt(fmax((double)xn, 0.0));
                 const double e = 1.0625 * u * (cmax * cmax + (double)(d + 2) * xl * cmax);
                 const double band = 2.0 * e;
-                if ((double)t.s - (double)t.b <= band) {
-                    const int slot = atomicAdd(&st->n_recheck, 1);
-                    RecheckEntry q;
-                    q.row = (int)r;
-                    q.c1 = t.ib;
-                    q.c2 = t.is;
-                    q.full = ((double)t.t - (double)t.b <= band) ? 1 : 0;
-                    queue[slot] = q;
-                }
+                if ((double)t.s - (double)t.b <= band)
+                    enqueue_recheck(queue, n, st, (int)r, t.ib, t.is, (double)t.t - (double)t.b <= band);
             }
         }
     }

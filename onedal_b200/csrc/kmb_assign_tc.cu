@@ -600,15 +600,10 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 if (p.queue) {
                     // (a row for which no cluster passed the filters -- impossible while
                     // the prior bound holds -- goes to the full FP64 rescan)
-                    if ((double)r.s - (double)r.b <= band || !(r.b < __int_as_float(0x7f800000))) {
-                        const int qslot = atomicAdd(&p.st->n_recheck, 1);
-                        RecheckEntry q;
-                        q.row = (int)row;
-                        q.c1 = r.ib;
-                        q.c2 = r.is;
-                        q.full = ((double)r.t - (double)r.b <= band || !(r.b < __int_as_float(0x7f800000))) ? 1 : 0;
-                        p.queue[qslot] = q;
-                    }
+                    const bool none = !(r.b < __int_as_float(0x7f800000));
+                    if ((double)r.s - (double)r.b <= band || none)
+                        enqueue_recheck(p.queue, p.n, p.st, (int)row, r.ib, r.is,
+                                        (double)r.t - (double)r.b <= band || none);
                 }
             }
         }

@@ -43,6 +43,22 @@ struct RecheckEntry {
     int full;  // 1: more than two clusters lie inside the error band -> scan all k
 };
 
+// Queues a near-tie row for the FP64 recheck. Two-candidate entries fill the
+// queue from the front (count st->n_recheck), full-rescan entries from the back
+// (count st->n_full); the capacity is the row count, and a row is queued once.
+__device__ __forceinline__ void enqueue_recheck(RecheckEntry *queue, int64_t cap, LoopState *st, int row, int c1,
+                                                int c2, bool full) {
+    RecheckEntry q;
+    q.row = row;
+    q.c1 = c1;
+    q.c2 = c2;
+    q.full = full ? 1 : 0;
+    if (full)
+        queue[cap - 1 - atomicAdd(&st->n_full, 1)] = q;
+    else
+        queue[atomicAdd(&st->n_recheck, 1)] = q;
+}
+
 // Per-call sizing of the update (counting sort + segmented FP64 sums).
 struct UpdatePlan {
     int64_t n, k, d;
@@ -61,6 +77,11 @@ struct DevBuf {
 
 struct Workspace {
     int device = 0;
+    // Buffers are stream-ordered allocations on the context's stream: growing
+    // one never synchronises the device (a plain cudaFree would stall every
+    // other stream's host thread, e.g. a serving loop's lanes, until the device
+    // drains).
+    cudaStream_t stream = nullptr;
     DevBuf X, C0, Cout, labels, d2, xnorm, Ccur, Cnew, Ct, h, queue;
     DevBuf H, Gs, counts, offsets, piece_base, perm, records, shift_part, empty_flag, empty_ids;
     DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;

@@ -7,54 +7,65 @@
 // F inputs, with the reference's score 0.5||c||^2 - x.c and its lowest-index
 // tie rule (cpp/daal/src/algorithms/kmeans/kmeans_lloyd_impl.i:197-216), so the
 // final labels equal the FP64 oracle's. Two-candidate entries (nearly all of
-// them) take two threads each; entries flagged for a full scan take a warp (32 clusters per step).
+// them; the front of the queue) take eight lanes each; entries flagged for a
+// full scan (the back of the queue) take a warp, 32 clusters per step.
 #include "kmb_internal.cuh"
 
 namespace kmb {
 namespace {
 
-// Two-candidate entries: two threads per entry (one candidate each, a
-// sequential FP64 dot product over d), decided with one shuffle.
+// Two-candidate entries (the front of the queue): eight lanes per entry, four
+// entries per warp. Lane l of a group accumulates coordinates t = l, l+8, ...
+// of ||c||^2 and x.c for both candidates in double (consecutive lanes read
+// consecutive floats of the row and of each centroid), then three butterfly
+// steps give the group's totals; both candidates' sums have the same
+// association, so equal centroids give equal scores.
 template <typename F>
-__global__ void recheck_pairs_kernel(const F *__restrict__ X, int d, const F *__restrict__ C,
-                                     const RecheckEntry *__restrict__ queue, int32_t *__restrict__ labels,
-                                     F *__restrict__ d2, const F *__restrict__ xnorm, LoopState *st) {
+__global__ void __launch_bounds__(256) recheck_pairs_kernel(const F *__restrict__ X, int d, const F *__restrict__ C,
+                                                            const RecheckEntry *__restrict__ queue,
+                                                            int32_t *__restrict__ labels, F *__restrict__ d2,
+                                                            const F *__restrict__ xnorm, LoopState *st) {
     if (st->done) return;
     const int count = st->n_recheck;
     const int lane = threadIdx.x & 31;
-    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int sub = lane & 7;
+    const long long groups = ((long long)gridDim.x * blockDim.x) >> 3;
     int changed = 0;
-    // each warp takes 16 entries per step; the loop bound is uniform across the warp
-    for (long long base = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 16; base < count;
-         base += warps * 16) {
-        const long long e = base + (lane >> 1);
+    // the loop bound is uniform across the warp (four groups step together)
+    for (long long base = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 4; base < count;
+         base += groups) {
+        const long long e = base + (lane >> 3);
         const bool valid = e < count;
         RecheckEntry q;
         q.row = 0;
         q.c1 = q.c2 = 0;
-        q.full = 1;
         if (valid) q = queue[e];
-        const bool active = valid && !q.full;
         const int a = min(q.c1, q.c2), b = max(q.c1, q.c2);
-        const int cand = (lane & 1) ? b : a;
-        double score = 0.0;
-        if (active) {
+        double cca = 0.0, xca = 0.0, ccb = 0.0, xcb = 0.0;
+        if (valid) {
             const F *x = X + (int64_t)q.row * d;
-            const F *c = C + (int64_t)cand * d;
-            double cc = 0.0, xc = 0.0;
-            for (int t = 0; t < d; ++t) {
-                const double cv = (double)c[t];
-                cc = fma(cv, cv, cc);
-                xc = fma((double)x[t], cv, xc);
+            const F *ca = C + (int64_t)a * d;
+            const F *cb = C + (int64_t)b * d;
+            for (int t = sub; t < d; t += 8) {
+                const double xv = (double)x[t], va = (double)ca[t], vb = (double)cb[t];
+                cca = fma(va, va, cca);
+                xca = fma(xv, va, xca);
+                ccb = fma(vb, vb, ccb);
+                xcb = fma(xv, vb, xcb);
             }
-            score = 0.5 * cc - xc;
         }
-        const double other = __shfl_xor_sync(0xffffffffu, score, 1);
-        if (active && (lane & 1) == 0) {
-            // lane holds the lower index a; b wins only when strictly better
-            const bool take_b = other < score;
+#pragma unroll
+        for (int m = 4; m >= 1; m >>= 1) {
+            cca += __shfl_xor_sync(0xffffffffu, cca, m);
+            xca += __shfl_xor_sync(0xffffffffu, xca, m);
+            ccb += __shfl_xor_sync(0xffffffffu, ccb, m);
+            xcb += __shfl_xor_sync(0xffffffffu, xcb, m);
+        }
+        if (valid && sub == 0) {
+            const double sa = 0.5 * cca - xca, sb = 0.5 * ccb - xcb;
+            const bool take_b = sb < sa;  // the lower index a wins ties
             const int bi = take_b ? b : a;
-            const double best = take_b ? other : score;
+            const double best = take_b ? sb : sa;
             if (labels[q.row] != bi) ++changed;
             labels[q.row] = bi;
             d2[q.row] = F(2.0 * best + (double)xnorm[q.row]);
@@ -94,18 +105,16 @@ __device__ __forceinline__ void reduce_scatter32(double (&a)[32], int lane) {
 // order; the warp argmin breaks ties to the lowest index.
 template <typename F>
 __global__ void __launch_bounds__(256) recheck_full_kernel(const F *__restrict__ X, int d, const F *__restrict__ C,
-                                                           int k, const RecheckEntry *__restrict__ queue,
+                                                           int k, const RecheckEntry *__restrict__ queue, int64_t cap,
                                                            int32_t *__restrict__ labels, F *__restrict__ d2,
                                                            const F *__restrict__ xnorm, LoopState *st) {
     if (st->done) return;
-    const int count = st->n_recheck;
+    const int count = st->n_full;  // entries queue[cap - 1], queue[cap - 2], ...
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
-    int changed = 0, fulls = 0;
+    int changed = 0;
     for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += warps) {
-        const RecheckEntry q = queue[w];
-        if (!q.full) continue;
-        ++fulls;
+        const RecheckEntry q = queue[cap - 1 - w];
         const F *x = X + (int64_t)q.row * d;
         double best = 0.0;
         int bi = 0x7fffffff;
@@ -149,7 +158,6 @@ __global__ void __launch_bounds__(256) recheck_full_kernel(const F *__restrict__
         }
     }
     if (lane == 0 && changed) atomicAdd(&st->n_changed, changed);
-    if (lane == 0 && fulls) atomicAdd(&st->n_full, fulls);
 }
 
 }  // namespace
@@ -157,10 +165,10 @@ __global__ void __launch_bounds__(256) recheck_full_kernel(const F *__restrict__
 template <typename F>
 void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, const RecheckEntry *queue,
                     int32_t *labels, F *d2, const F *xnorm, LoopState *st, cudaStream_t s) {
-    (void)n;
     recheck_pairs_kernel<F><<<148 * 8, 256, 0, s>>>(X, (int)d, C, queue, labels, d2, xnorm, st);
     KMB_LAUNCHED();
-    recheck_full_kernel<F><<<148 * 4, 256, 0, s>>>(X, (int)d, C, (int)k, queue, labels, d2, xnorm, st);
+    // one wave: the kernel keeps 254 registers per thread, one 256-thread block per SM
+    recheck_full_kernel<F><<<148, 256, 0, s>>>(X, (int)d, C, (int)k, queue, n, labels, d2, xnorm, st);
     KMB_LAUNCHED();
 }
 

@@ -13,18 +13,34 @@
 //                requests that arrived while earlier batches run are picked up
 //                by the next free lane), uploads their rows, runs one grouped
 //                assignment launch over all of them (kmb_serve_kernels.cu) and
-//                copies the labels back; a host callback on the stream marks the
-//                batch complete and returns its memory to the budget. Batches on
-//                different lanes overlap on the device;
+//                copies the labels back, then records an event; the lane's
+//                completion thread sleeps on that event (blocking sync), marks
+//                the batch complete and returns its memory to the budget.
+//                Batches on different lanes overlap on the device;
+//  * tensor-core worker -- infer requests large enough for the tensor cores
+//                (d <= 256, n * kpad * dpad >= KMB_SERVER_TC_MACS) skip the
+//                grouped lanes and run on kTcWorkers worker threads, each with its own
+//                context: BF16x3 form with the FP64 recheck, in row chunks of at
+//                most kTcChunkRows, on a low-priority stream. A large request
+//                therefore never holds a batch of small ones, and the small
+//                lanes (high-priority streams) get SMs as soon as a chunk's
+//                CTAs retire. The worker's workspace is reserved in the budget
+//                once, at creation;
 //  * trainers -- small train requests run on worker threads, each with its own
-//                kmb_context (stream + workspace), concurrently with the lanes.
+//                kmb_context (workspace) on a low-priority stream, concurrently
+//                with the lanes.
 // Latency is measured on the host from submit to completion (steady_clock).
+// With KMB_SERVE_TRACE=<file> in the environment, the server appends one line
+// per finished request (R ...) and per lane batch (B ...) to that file, times
+// in microseconds since the server was created.
 #include "kmb_internal.cuh"
 
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <mutex>
@@ -64,9 +80,16 @@ struct Model {
     float *C = nullptr, *Ct = nullptr, *h = nullptr;
 };
 
+constexpr int64_t kTcChunkRows = 1 << 18;
+constexpr size_t kTcReserveBytes = (size_t)448 << 20;  // one worker's workspace at kTcChunkRows rows, d <= 256
+constexpr int kTcWorkers = 2;
+constexpr int kTcMaxSms = 100;                   // SMs a tensor-core launch may hold; the rest stay with the lanes
+constexpr double kBatchMacs = 4294967296.0;      // cap on a lane batch's n * kpad * dpad (one large request may exceed it alone)
+
 struct Request {
     int64_t id;
     int kind;
+    int form = KMB_FORM_PLAIN;
     int model;
     int64_t n, d, k, iters;
     const float *X;
@@ -76,11 +99,12 @@ struct Request {
     size_t bytes;
     int state = PENDING;
     int rc = KMB_OK;
-    Clock::time_point t_submit, t_done;
+    Clock::time_point t_submit, t_start, t_done;  // t_start: admitted and dispatched
     // device buffers while running (infer)
     float *dX = nullptr;
     unsigned long long *dkey = nullptr;
     int32_t *dlab = nullptr;
+    int64_t lab_off = 0;  // offset in the lane's pinned label staging
 };
 
 struct Lane;
@@ -93,6 +117,12 @@ struct Server {
     std::condition_variable cv;
     std::deque<Request *> pending;      // infer, FIFO
     std::deque<Request *> train_queue;  // train, FIFO
+    std::deque<Request *> tc_queue;     // large infer, FIFO (tensor-core worker)
+    bool tc_enabled = false;
+    int tc_busy = 0;                    // tensor-core workers running a request
+    size_t base_use = 0;                // permanent reservation (tensor-core worker workspaces)
+    int prio_low = 0, prio_high = 0;
+    int64_t tc_requests = 0;
     std::unordered_map<int64_t, Request *> all;
     std::vector<Model> models;
     std::vector<Lane *> lanes;
@@ -102,6 +132,8 @@ struct Server {
     int64_t batches = 0, batched_requests = 0, completed = 0, failed = 0;
     int64_t max_batch_rows = 1 << 22;
     Clock::time_point t0 = Clock::now();
+    FILE *trace = nullptr;  // KMB_SERVE_TRACE
+    double us(Clock::time_point t) const { return std::chrono::duration<double, std::micro>(t - t0).count(); }
 };
 
 struct Lane {
@@ -112,7 +144,25 @@ struct Lane {
     kmb::serve::ReqDesc *h_desc = nullptr;  // pinned
     void *d_desc = nullptr;
     int cap = 0;
+    // Pinned staging for the batch's labels: the device->host copy stays
+    // asynchronous (a copy into pageable memory would block the scheduler
+    // thread until the batch finished), and the completion callback moves
+    // each request's labels into the caller's buffer.
+    int32_t *h_lab = nullptr;
+    int64_t h_lab_cap = 0;
+    int index = 0;
+    cudaEvent_t done_ev = nullptr;  // recorded after the batch's last copy
+    bool in_flight = false;         // a launched batch awaits its completion thread
+    std::thread completer;
+    Clock::time_point t_launch, t_launched;  // host time around launch_batch
+    double us_alloc = 0, us_h2d = 0, us_kernel = 0, us_tail = 0, us_d2h = 0, us_free = 0;  // host time inside launch_batch
 };
+
+int serve_form(const Server *srv, const Model &m, int64_t n) {
+    if (!srv->tc_enabled || m.d > 256) return KMB_FORM_PLAIN;
+    const int64_t kpad = (m.k + 127) / 128 * 128, dpad = (m.d + 63) / 64 * 64;
+    return (double)n * (double)kpad * (double)dpad >= (double)KMB_SERVER_TC_MACS ? KMB_FORM_BF16X3 : KMB_FORM_PLAIN;
+}
 
 size_t infer_bytes(int64_t n, int64_t d) { return (size_t)n * d * 4 + (size_t)n * 8 + (size_t)n * 4 + 4096; }
 size_t train_bytes(int64_t n, int64_t d, int64_t k) {
@@ -120,11 +170,12 @@ size_t train_bytes(int64_t n, int64_t d, int64_t k) {
     return (size_t)n * d * 4 + (size_t)n * 40 + (size_t)k * d * 64 + (size_t)(n / 512 + k) * d * 8 + (8u << 20);
 }
 
-void CUDART_CB batch_done(void *arg) {
-    Lane *lane = (Lane *)arg;
+void batch_done(Lane *lane) {
     Server *srv = lane->srv;
-    const auto now = Clock::now();
+    for (Request *r : lane->batch)
+        if (r->rc == KMB_OK) std::memcpy(r->labels_out, lane->h_lab + r->lab_off, sizeof(int32_t) * r->n);
     std::lock_guard<std::mutex> lock(srv->mu);
+    const auto now = Clock::now();
     for (Request *r : lane->batch) {
         r->t_done = now;
         r->state = r->rc == KMB_OK ? DONE : FAILED;
@@ -132,9 +183,35 @@ void CUDART_CB batch_done(void *arg) {
         srv->completed += 1;
         if (r->rc != KMB_OK) srv->failed += 1;
     }
+    if (srv->trace) {
+        int64_t rows = 0;
+        for (Request *r : lane->batch) rows += r->n;
+        std::fprintf(srv->trace,
+                     "B lane=%d nreq=%zu rows=%lld launch=%.1f launched=%.1f done=%.1f alloc=%.1f h2d=%.1f kern=%.1f "
+                     "tail=%.1f d2h=%.1f free=%.1f\n",
+                     lane->index, lane->batch.size(), (long long)rows, srv->us(lane->t_launch),
+                     srv->us(lane->t_launched), srv->us(now), lane->us_alloc, lane->us_h2d, lane->us_kernel,
+                     lane->us_tail, lane->us_d2h, lane->us_free);
+    }
     lane->batch.clear();
     lane->busy = false;
+    lane->in_flight = false;
     srv->cv.notify_all();
+}
+
+// One per lane: waits (sleeping, not spinning) for the lane's batch event.
+void completer_loop(Lane *lane) {
+    Server *srv = lane->srv;
+    cudaSetDevice(srv->device);
+    std::unique_lock<std::mutex> lock(srv->mu);
+    while (true) {
+        srv->cv.wait(lock, [&] { return srv->stop || lane->in_flight; });
+        if (!lane->in_flight) break;  // stop with nothing in flight
+        lock.unlock();
+        cudaEventSynchronize(lane->done_ev);
+        batch_done(lane);
+        lock.lock();
+    }
 }
 
 // Runs on the scheduler thread with the server lock released.
@@ -154,18 +231,36 @@ int launch_batch(Server *srv, Lane *lane) {
             return KMB_ENOMEM;
         }
     }
+    int64_t batch_rows = 0;
+    for (Request *r : lane->batch) batch_rows += r->n;
+    if (batch_rows > lane->h_lab_cap) {
+        if (lane->h_lab) cudaFreeHost(lane->h_lab);
+        lane->h_lab = nullptr;
+        lane->h_lab_cap = 0;
+        const int64_t cap = std::max<int64_t>(batch_rows, srv->max_batch_rows);
+        if (cudaMallocHost(&lane->h_lab, sizeof(int32_t) * cap) != cudaSuccess) {
+            cudaGetLastError();
+            return KMB_ENOMEM;
+        }
+        lane->h_lab_cap = cap;
+    }
     const int chunk = kmb::grouped_chunk_clusters();
     long long items = 0, rows = 0;
     for (int i = 0; i < nreq; ++i) {
         Request *r = lane->batch[i];
         const Model &m = srv->models[r->model];
+        const auto ta = Clock::now();
         if (cudaMallocAsync((void **)&r->dX, sizeof(float) * r->n * r->d, s) != cudaSuccess ||
             cudaMallocAsync((void **)&r->dkey, sizeof(unsigned long long) * r->n, s) != cudaSuccess ||
             cudaMallocAsync((void **)&r->dlab, sizeof(int32_t) * r->n, s) != cudaSuccess) {
             cudaGetLastError();
             return KMB_ENOMEM;
         }
+        const auto tb = Clock::now();
         cudaMemcpyAsync(r->dX, r->X, sizeof(float) * r->n * r->d, cudaMemcpyHostToDevice, s);
+        const auto tc = Clock::now();
+        lane->us_alloc += std::chrono::duration<double, std::micro>(tb - ta).count();
+        lane->us_h2d += std::chrono::duration<double, std::micro>(tc - tb).count();
         kmb::serve::ReqDesc &q = lane->h_desc[i];
         q.X = r->dX;
         q.Ct = m.Ct;
@@ -179,22 +274,31 @@ int launch_batch(Server *srv, Lane *lane) {
         q.chunks = (int)((m.kpad + chunk - 1) / chunk);
         q.item_begin = items;
         q.row_begin = rows;
+        r->lab_off = rows;
         items += ((r->n + 127) / 128) * q.chunks;
         rows += r->n;
     }
+    const auto tk0 = Clock::now();
     cudaMemcpyAsync(lane->d_desc, lane->h_desc, sizeof(kmb::serve::ReqDesc) * nreq, cudaMemcpyHostToDevice, s);
     kmb::launch_grouped_infer(lane->d_desc, nreq, items, rows, s);
+    const auto tk1 = Clock::now();
+    lane->us_kernel += std::chrono::duration<double, std::micro>(tk1 - tk0).count();
     for (Request *r : lane->batch) {
-        cudaMemcpyAsync(r->labels_out, r->dlab, sizeof(int32_t) * r->n, cudaMemcpyDeviceToHost, s);
+        const auto t0 = Clock::now();
+        cudaMemcpyAsync(lane->h_lab + r->lab_off, r->dlab, sizeof(int32_t) * r->n, cudaMemcpyDeviceToHost, s);
+        const auto t1 = Clock::now();
         cudaFreeAsync(r->dX, s);
         cudaFreeAsync(r->dkey, s);
         cudaFreeAsync(r->dlab, s);
+        lane->us_d2h += std::chrono::duration<double, std::micro>(t1 - t0).count();
+        lane->us_free += std::chrono::duration<double, std::micro>(Clock::now() - t1).count();
     }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         for (Request *r : lane->batch) r->rc = KMB_ECUDA;
     }
-    cudaLaunchHostFunc(s, batch_done, lane);
+    cudaEventRecord(lane->done_ev, s);
+    lane->us_tail += std::chrono::duration<double, std::micro>(Clock::now() - tk1).count();
     return KMB_OK;
 }
 
@@ -213,17 +317,24 @@ void scheduler_loop(Server *srv) {
                 }
             if (!lane) return false;
             // admission of at least the head request
-            return srv->in_use + srv->pending.front()->bytes <= srv->budget || srv->in_use == 0;
+            return srv->in_use + srv->pending.front()->bytes <= srv->budget || srv->in_use == srv->base_use;
         });
         if (srv->stop) break;
         // Continuous batching: take every admissible pending request (FIFO).
         int64_t rows = 0;
+        double macs = 0.0;
         while (!srv->pending.empty()) {
             Request *r = srv->pending.front();
-            if (srv->in_use + r->bytes > srv->budget && !(srv->in_use == 0 && lane->batch.empty())) break;
-            if (!lane->batch.empty() && rows + r->n > srv->max_batch_rows) break;
+            if (srv->in_use + r->bytes > srv->budget && !(srv->in_use == srv->base_use && lane->batch.empty())) break;
+            const Model &m = srv->models[r->model];
+            const double w = (double)r->n * (double)((m.k + 127) / 128 * 128) * (double)((m.d + 7) / 8 * 8);
+            // a batch ends when it is large enough: small requests behind it go to the next free lane
+            if (!lane->batch.empty() && (rows + r->n > srv->max_batch_rows || macs + w > kBatchMacs)) break;
+            macs += w;
             srv->pending.pop_front();
             r->state = RUNNING;
+            r->t_start = Clock::now();
+        r->t_start = Clock::now();
             srv->in_use += r->bytes;
             srv->peak_in_use = std::max(srv->peak_in_use, srv->in_use);
             rows += r->n;
@@ -234,7 +345,10 @@ void scheduler_loop(Server *srv) {
         srv->batches += 1;
         srv->batched_requests += (int64_t)lane->batch.size();
         lock.unlock();
+        lane->us_alloc = lane->us_h2d = lane->us_kernel = lane->us_tail = lane->us_d2h = lane->us_free = 0;
+        lane->t_launch = Clock::now();
         const int rc = launch_batch(srv, lane);
+        lane->t_launched = Clock::now();
         if (rc != KMB_OK) {
             // Release what was allocated and complete the batch as failed, in stream order.
             for (Request *r : lane->batch) {
@@ -243,27 +357,108 @@ void scheduler_loop(Server *srv) {
                 if (r->dkey) cudaFreeAsync(r->dkey, lane->stream);
                 if (r->dlab) cudaFreeAsync(r->dlab, lane->stream);
             }
-            cudaLaunchHostFunc(lane->stream, batch_done, lane);
+            cudaEventRecord(lane->done_ev, lane->stream);
         }
         lock.lock();
+        lane->in_flight = true;
+        srv->cv.notify_all();
     }
+}
+
+// Large infer request on the tensor-core worker: rows uploaded once, then
+// kmb_infer (BF16x3, FP64 recheck) over row chunks on the worker's stream.
+int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r) {
+    float *dX = nullptr;
+    int32_t *dlab = nullptr;
+    if (cudaMallocAsync((void **)&dX, sizeof(float) * r->n * r->d, s) != cudaSuccess ||
+        cudaMallocAsync((void **)&dlab, sizeof(int32_t) * r->n, s) != cudaSuccess) {
+        cudaGetLastError();
+        if (dX) cudaFreeAsync(dX, s);
+        cudaStreamSynchronize(s);
+        return KMB_ENOMEM;
+    }
+    int rc = KMB_OK;
+    if (cudaMemcpyAsync(dX, r->X, sizeof(float) * r->n * r->d, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        rc = KMB_ECUDA;
+    for (int64_t off = 0; rc == KMB_OK && off < r->n; off += kTcChunkRows) {
+        const int64_t rows = std::min<int64_t>(kTcChunkRows, r->n - off);
+        rc = kmb_infer(ctx, KMB_F32, KMB_MEM_DEVICE, dX + off * r->d, rows, r->d, m.C, m.k, KMB_FORM_BF16X3, 0,
+                       dlab + off, nullptr, nullptr);
+    }
+    if (rc == KMB_OK &&
+        cudaMemcpyAsync(r->labels_out, dlab, sizeof(int32_t) * r->n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        rc = KMB_ECUDA;
+    cudaFreeAsync(dX, s);
+    cudaFreeAsync(dlab, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess && rc == KMB_OK) rc = KMB_ECUDA;
+    return rc;
+}
+
+void tc_worker_loop(Server *srv) {
+    cudaSetDevice(srv->device);
+    kmb_context *ctx = nullptr;
+    cudaStream_t ts = nullptr;
+    if (kmb_context_create(srv->device, &ctx) != KMB_OK) ctx = nullptr;
+    if (ctx && cudaStreamCreateWithPriority(&ts, cudaStreamNonBlocking, srv->prio_low) == cudaSuccess) {
+        kmb_context_set_stream(ctx, ts);
+        kmb_context_set_max_sms(ctx, kTcMaxSms);
+    } else if (ctx) {
+        kmb_context_destroy(ctx);
+        ctx = nullptr;
+    }
+    std::unique_lock<std::mutex> lock(srv->mu);
+    while (true) {
+        srv->cv.wait(lock, [&] {
+            if (srv->stop) return true;
+            if (srv->tc_queue.empty()) return false;
+            return srv->in_use + srv->tc_queue.front()->bytes <= srv->budget || srv->in_use == srv->base_use;
+        });
+        if (srv->stop) break;
+        Request *r = srv->tc_queue.front();
+        srv->tc_queue.pop_front();
+        r->state = RUNNING;
+        r->t_start = Clock::now();
+        srv->in_use += r->bytes;
+        srv->peak_in_use = std::max(srv->peak_in_use, srv->in_use);
+        srv->tc_busy += 1;
+        const Model m = srv->models[r->model];
+        lock.unlock();
+        const int rc = ctx ? run_tc_request(ctx, ts, m, r) : KMB_ECUDA;
+        lock.lock();
+        r->rc = rc;
+        r->t_done = Clock::now();
+        r->state = rc == KMB_OK ? DONE : FAILED;
+        srv->in_use -= r->bytes;
+        srv->completed += 1;
+        srv->tc_requests += 1;
+        if (rc != KMB_OK) srv->failed += 1;
+        srv->tc_busy -= 1;
+        srv->cv.notify_all();
+    }
+    lock.unlock();
+    if (ctx) kmb_context_destroy(ctx);
+    if (ts) cudaStreamDestroy(ts);
 }
 
 void trainer_loop(Server *srv) {
     cudaSetDevice(srv->device);
     kmb_context *ctx = nullptr;
+    cudaStream_t ts = nullptr;
     if (kmb_context_create(srv->device, &ctx) != KMB_OK) ctx = nullptr;
+    if (ctx && cudaStreamCreateWithPriority(&ts, cudaStreamNonBlocking, srv->prio_low) == cudaSuccess)
+        kmb_context_set_stream(ctx, ts);
     std::unique_lock<std::mutex> lock(srv->mu);
     while (true) {
         srv->cv.wait(lock, [&] {
             if (srv->stop) return true;
             if (srv->train_queue.empty()) return false;
-            return srv->in_use + srv->train_queue.front()->bytes <= srv->budget || srv->in_use == 0;
+            return srv->in_use + srv->train_queue.front()->bytes <= srv->budget || srv->in_use == srv->base_use;
         });
         if (srv->stop) break;
         Request *r = srv->train_queue.front();
         srv->train_queue.pop_front();
         r->state = RUNNING;
+        r->t_start = Clock::now();
         srv->in_use += r->bytes;
         srv->peak_in_use = std::max(srv->peak_in_use, srv->in_use);
         lock.unlock();
@@ -286,6 +481,7 @@ void trainer_loop(Server *srv) {
     }
     lock.unlock();
     if (ctx) kmb_context_destroy(ctx);
+    if (ts) cudaStreamDestroy(ts);
 }
 
 __global__ void prep_model_kernel(const float *__restrict__ C, int k, int d, int dpad, int kpad, float *__restrict__ Ct,
@@ -312,22 +508,48 @@ int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32
     if (!srv) return KMB_ENOMEM;
     srv->device = device;
     srv->budget = (size_t)hbm_budget_bytes;
+    if (const char *path = std::getenv("KMB_SERVE_TRACE")) srv->trace = std::fopen(path, "a");
     // Keep freed request memory in the stream-ordered pool instead of returning it to the driver.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
         uint64_t thr = (uint64_t)hbm_budget_bytes;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
+    cudaDeviceGetStreamPriorityRange(&srv->prio_low, &srv->prio_high);
     for (int i = 0; i < lanes; ++i) {
         Lane *l = new Lane;
         l->srv = srv;
-        if (cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        l->index = i;
+        // descriptor and label staging sized up front: growing them later
+        // (cudaFree / cudaFreeHost) would synchronise the device mid-stream
+        l->cap = 256;
+        l->h_lab_cap = srv->max_batch_rows;
+        if (cudaMallocHost(&l->h_desc, sizeof(kmb::serve::ReqDesc) * l->cap) != cudaSuccess ||
+            cudaMalloc(&l->d_desc, sizeof(kmb::serve::ReqDesc) * l->cap) != cudaSuccess ||
+            cudaMallocHost(&l->h_lab, sizeof(int32_t) * l->h_lab_cap) != cudaSuccess ||
+            cudaEventCreateWithFlags(&l->done_ev, cudaEventBlockingSync | cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            if (l->h_desc) cudaFreeHost(l->h_desc);
+            if (l->d_desc) cudaFree(l->d_desc);
+            delete l;
+            return KMB_ENOMEM;
+        }
+        if (cudaStreamCreateWithPriority(&l->stream, cudaStreamNonBlocking, srv->prio_high) != cudaSuccess) {
             delete l;
             return KMB_ECUDA;
         }
         srv->lanes.push_back(l);
     }
+    // The tensor-core worker needs its workspace reserved; small budgets serve everything on the lanes.
+    if (srv->budget >= 4 * kTcWorkers * kTcReserveBytes) {
+        srv->tc_enabled = true;
+        srv->base_use = kTcWorkers * kTcReserveBytes;
+        srv->in_use = srv->peak_in_use = srv->base_use;
+    }
     srv->threads.emplace_back(scheduler_loop, srv);
+    for (Lane *l : srv->lanes) l->completer = std::thread(completer_loop, l);
+    if (srv->tc_enabled)
+        for (int i = 0; i < kTcWorkers; ++i) srv->threads.emplace_back(tc_worker_loop, srv);
     for (int i = 0; i < trainers; ++i) srv->threads.emplace_back(trainer_loop, srv);
     *out = srv;
     return KMB_OK;
@@ -342,17 +564,22 @@ int kmb_server_destroy(void *handle) {
         srv->cv.wait(lock, [&] {
             for (Lane *l : srv->lanes)
                 if (l->busy) return false;
-            return srv->pending.empty() && srv->train_queue.empty() && srv->in_use == 0;
+            return srv->pending.empty() && srv->train_queue.empty() && srv->tc_queue.empty() && srv->tc_busy == 0 &&
+                   srv->in_use == srv->base_use;
         });
         srv->stop = true;
     }
     srv->cv.notify_all();
     for (auto &t : srv->threads) t.join();
+    for (Lane *l : srv->lanes)
+        if (l->completer.joinable()) l->completer.join();
     cudaSetDevice(srv->device);
     for (Lane *l : srv->lanes) {
         cudaStreamSynchronize(l->stream);
         cudaStreamDestroy(l->stream);
         if (l->h_desc) cudaFreeHost(l->h_desc);
+        if (l->h_lab) cudaFreeHost(l->h_lab);
+        if (l->done_ev) cudaEventDestroy(l->done_ev);
         if (l->d_desc) cudaFree(l->d_desc);
         delete l;
     }
@@ -362,6 +589,7 @@ int kmb_server_destroy(void *handle) {
         cudaFree(m.h);
     }
     for (auto &kv : srv->all) delete kv.second;
+    if (srv->trace) std::fclose(srv->trace);
     delete srv;
     return KMB_OK;
 }
@@ -412,10 +640,14 @@ int kmb_server_submit_infer(void *handle, int32_t model_id, const float *X_host,
         r->C0 = nullptr;
         r->labels_out = labels_host;
         r->C_out = nullptr;
-        r->bytes = infer_bytes(n, d);
+        r->form = serve_form(srv, srv->models[model_id], n);
+        r->bytes = r->form == KMB_FORM_BF16X3 ? (size_t)n * d * 4 + (size_t)n * 4 + 4096 : infer_bytes(n, d);
         r->t_submit = Clock::now();
         srv->all[r->id] = r;
-        srv->pending.push_back(r);
+        if (r->form == KMB_FORM_BF16X3)
+            srv->tc_queue.push_back(r);
+        else
+            srv->pending.push_back(r);
         *request_id = r->id;
     }
     srv->cv.notify_all();
@@ -454,9 +686,10 @@ int kmb_server_submit_train(void *handle, const float *X_host, int64_t n, int64_
 }
 
 // Waits (up to timeout_s; < 0 = no limit) for a request; returns its status
-// (KMB_OK when done) or KMB_ETIMEDOUT. latency_s receives submit -> done.
-// A finished request is forgotten after a successful wait.
-int kmb_server_wait(void *handle, int64_t request_id, double timeout_s, double *latency_s) {
+// (KMB_OK when done) or KMB_ETIMEDOUT. latency_s receives submit -> done,
+// queued_s submit -> dispatch. A finished request is forgotten after a
+// successful wait.
+int kmb_server_wait_detail(void *handle, int64_t request_id, double timeout_s, double *latency_s, double *queued_s) {
     Server *srv = (Server *)handle;
     if (!srv) return KMB_EINVAL;
     std::unique_lock<std::mutex> lock(srv->mu);
@@ -470,10 +703,28 @@ int kmb_server_wait(void *handle, int64_t request_id, double timeout_s, double *
         return KMB_ETIMEDOUT;
     }
     if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+    if (queued_s) *queued_s = std::chrono::duration<double>(r->t_start - r->t_submit).count();
+    if (srv->trace)
+        std::fprintf(srv->trace, "R id=%lld kind=%d form=%d n=%lld k=%lld d=%lld submit=%.1f start=%.1f done=%.1f\n",
+                     (long long)r->id, r->kind, r->form, (long long)r->n, (long long)r->k, (long long)r->d,
+                     srv->us(r->t_submit), srv->us(r->t_start), srv->us(r->t_done));
     const int rc = r->rc;
     srv->all.erase(it);
     delete r;
     return rc;
+}
+
+int kmb_server_wait(void *handle, int64_t request_id, double timeout_s, double *latency_s) {
+    return kmb_server_wait_detail(handle, request_id, timeout_s, latency_s, nullptr);
+}
+
+int kmb_server_infer_form(void *handle, int32_t model_id, int64_t n, int32_t *form) {
+    Server *srv = (Server *)handle;
+    if (!srv || !form || n <= 0) return KMB_EINVAL;
+    std::lock_guard<std::mutex> lock(srv->mu);
+    if (model_id < 0 || model_id >= (int32_t)srv->models.size()) return KMB_EINVAL;
+    *form = serve_form(srv, srv->models[model_id], n);
+    return KMB_OK;
 }
 
 int kmb_server_get_stats(void *handle, kmb_server_stats *out) {
@@ -484,7 +735,8 @@ int kmb_server_get_stats(void *handle, kmb_server_stats *out) {
     out->failed = srv->failed;
     out->batches = srv->batches;
     out->batched_requests = srv->batched_requests;
-    out->pending = (int64_t)(srv->pending.size() + srv->train_queue.size());
+    out->pending = (int64_t)(srv->pending.size() + srv->train_queue.size() + srv->tc_queue.size());
+    out->tensor_core_requests = srv->tc_requests;
     out->in_use_bytes = (int64_t)srv->in_use;
     out->peak_in_use_bytes = (int64_t)srv->peak_in_use;
     out->budget_bytes = (int64_t)srv->budget;

@@ -3,8 +3,11 @@
 Fitted centroid sets stay resident in HBM; infer and small-train requests of
 different n, k and d are admitted under an HBM byte budget and batched, as they
 arrive, into shared grouped launches on several CUDA streams (continuous
-batching). Responses equal those of ``kmeans.infer`` / ``kmeans.train`` (plain
-form) on the same inputs.
+batching). Infer requests large enough for the tensor cores (d <= 256 and
+n * kpad * dpad >= 2^33) run on a tensor-core worker in the BF16x3 form with the
+FP64 recheck; ``infer_form`` tells which form a request gets. Responses equal
+those of ``kmeans.infer`` in that form (and of ``kmeans.train``, plain form, for
+trains) on the same inputs.
 
     srv = KMeansServer(hbm_budget_bytes=60 << 30)
     mid = srv.add_model(centroids)              # float32 (k, d)
@@ -80,18 +83,31 @@ class KMeansServer:
             raise ServingError(f"submit_train failed ({rc})")
         return Request(rid.value, "train", (X, C0), labels, C)
 
-    def wait(self, req: Request, timeout: float = -1.0):
-        """Returns (labels, latency_s) for infer, ((centroids, labels), latency_s) for train."""
+    def wait(self, req: Request, timeout: float = -1.0, detail: bool = False):
+        """Returns (labels, latency_s) for infer, ((centroids, labels), latency_s) for train;
+        with detail=True the latency is a (latency_s, queued_s) pair, queued_s being the
+        time from submit to dispatch."""
         lat = ctypes.c_double()
-        rc = self.lib.kmb_server_wait(self.handle, req.id, float(timeout), ctypes.byref(lat))
+        q = ctypes.c_double()
+        rc = self.lib.kmb_server_wait_detail(self.handle, req.id, float(timeout), ctypes.byref(lat), ctypes.byref(q))
         if rc == _native.KMB_ETIMEDOUT:
             raise TimeoutError(f"request {req.id} not done after {timeout} s")
         if rc != _native.KMB_OK:
             raise ServingError(f"request {req.id} failed: {self.lib.kmb_status_string(rc).decode()}")
         req.keep = None
+        t = (lat.value, q.value) if detail else lat.value
         if req.kind == "train":
-            return (req.centroids, req.labels), lat.value
-        return req.labels, lat.value
+            return (req.centroids, req.labels), t
+        return req.labels, t
+
+    def infer_form(self, model_id: int, n: int) -> int:
+        """_native.KMB_FORM_PLAIN or KMB_FORM_BF16X3: the form an infer of n rows against
+        model_id is served in."""
+        f = ctypes.c_int32()
+        rc = self.lib.kmb_server_infer_form(self.handle, int(model_id), int(n), ctypes.byref(f))
+        if rc != _native.KMB_OK:
+            raise ServingError(f"infer_form failed ({rc})")
+        return f.value
 
     def stats(self) -> dict:
         s = _native.kmb_server_stats()
