@@ -165,9 +165,12 @@ KMB_API int kmb_lloyd_iterate(kmb_context *ctx, int dtype, const void *X, int64_
  * 4 = FP64 near-tie recheck; kernel 3 returns in *launches every kernel this
  * host thread launched since timing was enabled (total_ms = 0). */
 KMB_API int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled);
-/* Caps the CTAs of the persistent tensor-core assignment at max_sms (one per SM;
- * 0 restores all SMs), leaving the remaining SMs to other streams' work -- the
- * serving loop uses it so that small requests never wait for a whole launch. */
+/* Grid of the persistent launches (tensor-core assignment, row splitting,
+ * recheck): at most max_sms SMs (0: all), leaving the rest to other streams'
+ * work. max_sms = -1 instead launches the tensor-core assignment as one short
+ * CTA per 128-row tile, which other streams' launches interleave with at tile
+ * granularity -- the serving loop uses it so that neither side waits for a
+ * whole launch of the other. */
 KMB_API int kmb_context_set_max_sms(kmb_context *ctx, int max_sms);
 KMB_API int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int64_t *launches);
 
@@ -235,8 +238,8 @@ KMB_API int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64_t 
  * threads, each with its own context. Large infer requests (d <= 256 and
  * n * kpad * dpad >= KMB_SERVER_TC_MACS, kpad = k rounded up to 128, dpad = d
  * rounded up to 64) run on tensor-core workers instead (BF16x3 form with the
- * FP64 recheck, in row chunks, on a low-priority stream, so small batches keep
- * the SMs they need). Every response equals kmb_infer's on the same inputs in
+ * FP64 recheck, in row chunks, launched as one short CTA per row tile, so that
+ * small batches interleave with them). Every response equals kmb_infer's on the same inputs in
  * the form kmb_server_infer_form reports (plain form: bit-identical to the
  * grouped launch; BF16x3: the FP64 oracle's labels), and kmb_train's (plain
  * form) for trains. Host buffers passed to submit_* must stay valid until the

@@ -26,6 +26,7 @@ struct kmb_context {
     std::string last_error;
     kmb::LoopState *h_state = nullptr;  // pinned mirror of the device states
     int num_sms = 148;
+    bool tc_per_tile = false;  // tensor-core assignment: one CTA per row tile instead of persistent CTAs
     // kernel timing (kmb_context_set_kernel_timing)
     bool timing = false;
     int64_t launches_at_enable = 0;
@@ -155,7 +156,7 @@ int ensure_common(kmb_context *ctx, int64_t n, int64_t d, int64_t k, bool rechec
         ok &= ws.ensure(ws.Chi, sizeof(uint16_t) * tkp * tdp);
         ok &= ws.ensure(ws.Clo, sizeof(uint16_t) * tkp * tdp);
         ok &= ws.ensure(ws.h, sizeof(float) * tkp);
-        ok &= ws.ensure(ws.tcx, kmb::tc_xchg_bytes(ctx->num_sms));
+        ok &= ws.ensure(ws.tcx, kmb::tc_xchg_bytes());
     }
     ok &= ws.ensure(ws.labels, sizeof(int32_t) * n);
     ok &= ws.ensure(ws.d2, sizeof(F) * n);
@@ -207,14 +208,15 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
         KernelTimer timer(ctx, 1);
         rc = kmb::launch_assign_tc(ws.Xhi.ptr, ws.Xlo.ptr, n, d, ws.Chi.ptr, ws.Clo.ptr, (const float *)ws.h.ptr, k,
                                    (const float *)ws.xnorm.ptr, &sc->cnorm_max, labels, d2,
-                                   (RecheckEntry *)ws.queue.ptr, st, ctx->num_sms, ws.tcx.ptr, prior,
+                                   (RecheckEntry *)ws.queue.ptr, st, ctx->tc_per_tile ? -1 : ctx->num_sms,
+                                   ws.tcx.ptr, prior,
                                    (const double *)ws.shift_part.ptr, &sc->cnorm_max_prev, s);
     }
     if (rc != KMB_OK) return fail(ctx, rc, "tensor-core assignment launch failed (d=%lld)", (long long)d);
     {
         KernelTimer timer(ctx, 4);
         kmb::launch_recheck<float>(X, n, d, C, k, (const RecheckEntry *)ws.queue.ptr, labels, d2,
-                                   (const float *)ws.xnorm.ptr, st, s);
+                                   (const float *)ws.xnorm.ptr, st, ctx->num_sms, s);
     }
     account_recheck_kernel<<<1, 1, 0, s>>>(st);
     KMB_LAUNCHED();
@@ -241,7 +243,7 @@ int assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, 
     if (recheck) {
         KernelTimer timer(ctx, 4);
         kmb::launch_recheck<F>(X, n, d, C, k, (const RecheckEntry *)ws.queue.ptr, labels, d2,
-                               (const F *)ws.xnorm.ptr, st, s);
+                               (const F *)ws.xnorm.ptr, st, ctx->num_sms, s);
         account_recheck_kernel<<<1, 1, 0, s>>>(st);
         KMB_LAUNCHED();
     }
@@ -257,7 +259,8 @@ void prepare_rows(kmb_context *ctx, const F *X, int64_t n, int64_t d, bool tc) {
 template <>
 void prepare_rows<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d, bool tc) {
     if (tc)
-        kmb::launch_split_rows(X, n, d, ctx->ws.Xhi.ptr, ctx->ws.Xlo.ptr, (float *)ctx->ws.xnorm.ptr, ctx->stream);
+        kmb::launch_split_rows(X, n, d, ctx->ws.Xhi.ptr, ctx->ws.Xlo.ptr, (float *)ctx->ws.xnorm.ptr, ctx->num_sms,
+                               ctx->stream);
     else
         kmb::launch_row_norms<float>(X, n, d, (float *)ctx->ws.xnorm.ptr, ctx->stream);
 }
@@ -678,10 +681,11 @@ int kmb_lloyd_iterate(kmb_context *ctx, int dtype, const void *X, int64_t n, int
 }
 
 int kmb_context_set_max_sms(kmb_context *ctx, int max_sms) {
-    if (!ctx || max_sms < 0) return KMB_EINVAL;
+    if (!ctx || max_sms < -1) return KMB_EINVAL;
     int all = 148;
     cudaDeviceGetAttribute(&all, cudaDevAttrMultiProcessorCount, ctx->device);
-    ctx->num_sms = (max_sms == 0 || max_sms > all) ? all : max_sms;
+    ctx->tc_per_tile = max_sms == -1;
+    ctx->num_sms = (max_sms <= 0 || max_sms > all) ? all : max_sms;
     return KMB_OK;
 }
 

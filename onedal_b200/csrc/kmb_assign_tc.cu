@@ -59,6 +59,7 @@ constexpr int NACC = 4;                 // TMEM accumulators: two per epilogue g
 constexpr int TMEM_COLS = NACC * BN;    // 512 = all of TMEM
 constexpr int NTHREADS = 320;           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two groups of 4)
 constexpr int MAX_B_STAGES = 8;
+constexpr int kMaxSmid = 1024;
 constexpr long long kTimeoutCycles = 4000000000ll;  // ~2 s at 1.9 GHz
 
 // One row's running top-3 (score space) as handed between the epilogue groups.
@@ -86,7 +87,7 @@ struct Params {
     float *d2;
     RecheckEntry *queue;
     LoopState *st;
-    Top3x *xchg;  // per CTA: 2 x 128 rows of group 1's top-3 (row-tile parity)
+    Top3x *xchg;  // per SM (one CTA fits an SM): 2 x 128 rows of group 1's top-3 (row-tile parity)
 };
 
 struct Barriers {
@@ -334,6 +335,9 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
     const uint32_t tmem_base = bar->tmem_base;
 
     const int my_tiles = (p.n_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    uint32_t smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    if (smid >= (uint32_t)kMaxSmid) smid = 0;  // (cannot happen on sm_100: ids stay below the SM count)
 
     if (warp == 0) {
         if (lane == 0) {
@@ -573,7 +577,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             r.t = -r.t;
             // Group 1 hands its top-3 to group 0 (same rows) through the CTA's
             // scratch slot for this row-tile parity, then group 0 merges.
-            Top3x *xs = p.xchg + ((size_t)blockIdx.x * 2 + (lt & 1)) * BM + row_in_tile;
+            Top3x *xs = p.xchg + ((size_t)smid * 2 + (lt & 1)) * BM + row_in_tile;
             if (group == 1) {
                 Top3x q;
                 q.b = r.b;
@@ -683,16 +687,19 @@ __global__ void reset_cmax_kernel(double *p, double *prev, const LoopState *st) 
 
 }  // namespace tc
 
-size_t tc_xchg_bytes(int num_sms) { return (size_t)num_sms * 2 * tc::BM * sizeof(tc::Top3x); }
+// Hand-off slots are indexed by %smid (a CTA needs a whole SM's shared memory,
+// so no two CTAs of this kernel share an SM at a time); ids are below kMaxSmid.
+size_t tc_xchg_bytes() { return (size_t)tc::kMaxSmid * 2 * tc::BM * sizeof(tc::Top3x); }
 
 int64_t tc_dpad(int64_t d) { return (d + tc::KP - 1) / tc::KP * tc::KP; }
 int64_t tc_kpad(int64_t k) { return (k + tc::BN - 1) / tc::BN * tc::BN; }
 bool tc_supported(int64_t d) { return tc_dpad(d) <= 256; }
 
-void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, float *xnorm, cudaStream_t s) {
+void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, float *xnorm, int num_sms,
+                       cudaStream_t s) {
     if (rows == 0) return;
     const int64_t dpad = tc_dpad(d);
-    const int blocks = (int)std::min<int64_t>((rows * 32 + 255) / 256, 148 * 16);
+    const int blocks = (int)std::min<int64_t>((rows * 32 + 255) / 256, (int64_t)num_sms * 16);
     tc::split_rows_kernel<<<blocks, 256, 0, s>>>(X, rows, (int)d, (int)dpad, (__nv_bfloat16 *)hi, (__nv_bfloat16 *)lo,
                                                  xnorm);
     KMB_LAUNCHED();
@@ -760,7 +767,10 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     int b_stages = (optin - fixed - a_stages * a_stage) / (2 * tc::PANEL);
     b_stages = std::min(b_stages, tc::MAX_B_STAGES);
     if (b_stages < 2) return KMB_EUNSUPPORTED;
-    const size_t smem = (size_t)a_stages * a_stage + (size_t)b_stages * 2 * tc::PANEL + fixed;
+    // More than half of an SM's shared memory: one CTA per SM, which the
+    // %smid-indexed hand-off slots rely on.
+    const size_t smem = std::max<size_t>((size_t)a_stages * a_stage + (size_t)b_stages * 2 * tc::PANEL + fixed,
+                                         (size_t)optin / 2 + 4096);
 
     CUtensorMap mXh, mXl, mCh, mCl;
     if (!encode_map(&mXh, Xhi, n, dpad) || !encode_map(&mXl, Xlo, n, dpad) || !encode_map(&mCh, Chi, kpad, dpad) ||
@@ -791,7 +801,9 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     if (cudaFuncSetAttribute(tc::assign_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return KMB_ECUDA;
-    const int grid = (int)std::min<int64_t>(num_sms, p.n_tiles);
+    // num_sms < 0: one CTA per 128-row tile (no persistence), so that other
+    // streams' launches interleave with this one at tile granularity
+    const int grid = num_sms < 0 ? p.n_tiles : (int)std::min<int64_t>(num_sms, p.n_tiles);
     tc::assign_tc_kernel<<<grid, tc::NTHREADS, smem, s>>>(mXh, mXl, mCh, mCl, p);
     KMB_LAUNCHED();
     return cudaGetLastError() == cudaSuccess ? KMB_OK : KMB_ECUDA;

@@ -122,7 +122,7 @@ void launch_assign_plain(const F *X, int64_t n, int64_t d, const F *Ct, const F 
 // FP64 recheck of queued rows (exact expanded score in double, lowest index on ties).
 template <typename F>
 void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, const RecheckEntry *queue,
-                    int32_t *labels, F *d2, const F *xnorm, LoopState *st, cudaStream_t s);
+                    int32_t *labels, F *d2, const F *xnorm, LoopState *st, int num_sms, cudaStream_t s);
 
 // ---- assignment (tensor-core BF16x3 form, float32 data) ----------------------
 int64_t tc_dpad(int64_t d);   // d rounded up to the 64-wide K panel
@@ -130,7 +130,8 @@ int64_t tc_kpad(int64_t k);   // k rounded up to the 128-wide cluster tile
 bool tc_supported(int64_t d); // dpad <= 256
 // X (rows x d, FP32) -> hi/lo BF16 [rows][dpad], zero padded.
 // x -> BF16 hi/lo panels [rows][dpad] and ||x||^2 (the same value launch_row_norms gives).
-void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, float *xnorm, cudaStream_t s);
+void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, float *xnorm, int num_sms,
+                       cudaStream_t s);
 // C -> Chi/Clo [kpad][dpad], -h = -0.5||c||^2 (kpad, -inf padding), max ||c||.
 // Also moves the previous max ||c|| into *cnorm_max_prev before recomputing it.
 void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, void *Clo, float *h,
@@ -143,7 +144,7 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
                      const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
                      float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, bool prior,
                      const double *shift_part, const double *cnorm_max_prev, cudaStream_t s);
-size_t tc_xchg_bytes(int num_sms);
+size_t tc_xchg_bytes();
 
 // ---- update ----------------------------------------------------------------
 UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d);

@@ -8,7 +8,7 @@
 // tie rule (cpp/daal/src/algorithms/kmeans/kmeans_lloyd_impl.i:197-216), so the
 // final labels equal the FP64 oracle's. Two-candidate entries (nearly all of
 // them; the front of the queue) take eight lanes each; entries flagged for a
-// full scan (the back of the queue) take a warp, 32 clusters per step.
+// full scan (the back of the queue) take a block, 8 warps x 32 clusters per step.
 #include "kmb_internal.cuh"
 
 namespace kmb {
@@ -97,28 +97,30 @@ __device__ __forceinline__ void reduce_scatter32(double (&a)[32], int lane) {
     reduce_scatter_step<1>(a, lane);
 }
 
-// Entries with a third cluster inside the band: a warp re-scores all k
-// clusters, 32 at a time. Lane L accumulates its coordinates' (t = L, L+32,
-// ...) contributions to ||c||^2 and x.c for the 32 clusters (coalesced loads of
-// each centroid row), then one reduce-scatter per quantity leaves cluster
-// j0 + L's sums on lane L. Lanes keep a running best in ascending cluster
-// order; the warp argmin breaks ties to the lowest index.
+// Entries with a third cluster inside the band (the back of the queue): a block
+// re-scores all k clusters of one row. Its 8 warps take interleaved groups of
+// 32 clusters; lane L accumulates its coordinates' (t = L, L+32, ...)
+// contributions to ||c||^2 and x.c for the group's 32 clusters (coalesced loads
+// of each centroid row), then one reduce-scatter per quantity leaves cluster
+// j0 + L's sums on lane L. Every lane keeps a running best in ascending cluster
+// order; the warp and then the block reduce with ties to the lowest index.
 template <typename F>
 __global__ void __launch_bounds__(256) recheck_full_kernel(const F *__restrict__ X, int d, const F *__restrict__ C,
                                                            int k, const RecheckEntry *__restrict__ queue, int64_t cap,
                                                            int32_t *__restrict__ labels, F *__restrict__ d2,
                                                            const F *__restrict__ xnorm, LoopState *st) {
     if (st->done) return;
+    __shared__ double s_best[8];
+    __shared__ int s_idx[8];
     const int count = st->n_full;  // entries queue[cap - 1], queue[cap - 2], ...
-    const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int changed = 0;
-    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += warps) {
-        const RecheckEntry q = queue[cap - 1 - w];
+    for (int e = blockIdx.x; e < count; e += gridDim.x) {
+        const RecheckEntry q = queue[cap - 1 - e];
         const F *x = X + (int64_t)q.row * d;
         double best = 0.0;
         int bi = 0x7fffffff;
-        for (int j0 = 0; j0 < k; j0 += 32) {
+        for (int j0 = 32 * warp; j0 < k; j0 += 256) {
             double xc[32], cc[32];
 #pragma unroll
             for (int i = 0; i < 32; ++i) xc[i] = cc[i] = 0.0;
@@ -152,29 +154,43 @@ __global__ void __launch_bounds__(256) recheck_full_kernel(const F *__restrict__
             }
         }
         if (lane == 0) {
+            s_best[warp] = best;
+            s_idx[warp] = bi;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < 8; ++w) {
+                const double ob = s_best[w];
+                const int oi = s_idx[w];
+                if (oi != 0x7fffffff && (bi == 0x7fffffff || ob < best || (ob == best && oi < bi))) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
             if (labels[q.row] != bi) ++changed;
             labels[q.row] = bi;
             d2[q.row] = F(2.0 * best + (double)xnorm[q.row]);
         }
+        __syncthreads();
     }
-    if (lane == 0 && changed) atomicAdd(&st->n_changed, changed);
+    if (threadIdx.x == 0 && changed) atomicAdd(&st->n_changed, changed);
 }
 
 }  // namespace
 
 template <typename F>
 void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, const RecheckEntry *queue,
-                    int32_t *labels, F *d2, const F *xnorm, LoopState *st, cudaStream_t s) {
-    recheck_pairs_kernel<F><<<148 * 8, 256, 0, s>>>(X, (int)d, C, queue, labels, d2, xnorm, st);
+                    int32_t *labels, F *d2, const F *xnorm, LoopState *st, int num_sms, cudaStream_t s) {
+    recheck_pairs_kernel<F><<<num_sms * 8, 256, 0, s>>>(X, (int)d, C, queue, labels, d2, xnorm, st);
     KMB_LAUNCHED();
-    // one wave: the kernel keeps 254 registers per thread, one 256-thread block per SM
-    recheck_full_kernel<F><<<148, 256, 0, s>>>(X, (int)d, C, (int)k, queue, n, labels, d2, xnorm, st);
+    // one wave (254 registers per thread: one 256-thread block per SM), a block per entry
+    recheck_full_kernel<F><<<num_sms, 256, 0, s>>>(X, (int)d, C, (int)k, queue, n, labels, d2, xnorm, st);
     KMB_LAUNCHED();
 }
 
 template void launch_recheck<float>(const float *, int64_t, int64_t, const float *, int64_t, const RecheckEntry *,
-                                    int32_t *, float *, const float *, LoopState *, cudaStream_t);
+                                    int32_t *, float *, const float *, LoopState *, int, cudaStream_t);
 template void launch_recheck<double>(const double *, int64_t, int64_t, const double *, int64_t, const RecheckEntry *,
-                                     int32_t *, double *, const double *, LoopState *, cudaStream_t);
+                                     int32_t *, double *, const double *, LoopState *, int, cudaStream_t);
 
 }  // namespace kmb

@@ -21,11 +21,11 @@
 //                (d <= 256, n * kpad * dpad >= KMB_SERVER_TC_MACS) skip the
 //                grouped lanes and run on kTcWorkers worker threads, each with its own
 //                context: BF16x3 form with the FP64 recheck, in row chunks of at
-//                most kTcChunkRows, on a low-priority stream. A large request
-//                therefore never holds a batch of small ones, and the small
-//                lanes (high-priority streams) get SMs as soon as a chunk's
-//                CTAs retire. The worker's workspace is reserved in the budget
-//                once, at creation;
+//                most kTcChunkRows, its assignment launched as one short CTA
+//                per 128-row tile (kmb_context_set_max_sms(-1)). A large
+//                request therefore never holds a batch of small ones, and lane
+//                launches interleave with it at tile granularity. The workers'
+//                workspaces are reserved in the budget once, at creation;
 //  * trainers -- small train requests run on worker threads, each with its own
 //                kmb_context (workspace) on a low-priority stream, concurrently
 //                with the lanes.
@@ -83,13 +83,13 @@ struct Model {
 constexpr int64_t kTcChunkRows = 1 << 18;
 constexpr size_t kTcReserveBytes = (size_t)448 << 20;  // one worker's workspace at kTcChunkRows rows, d <= 256
 constexpr int kTcWorkers = 2;
-constexpr int kTcMaxSms = 100;                   // SMs a tensor-core launch may hold; the rest stay with the lanes
 constexpr double kBatchMacs = 4294967296.0;      // cap on a lane batch's n * kpad * dpad (one large request may exceed it alone)
 
 struct Request {
     int64_t id;
     int kind;
     int form = KMB_FORM_PLAIN;
+    bool srv_trace = false;  // the server traces: time the tensor-core phases
     int model;
     int64_t n, d, k, iters;
     const float *X;
@@ -105,6 +105,8 @@ struct Request {
     unsigned long long *dkey = nullptr;
     int32_t *dlab = nullptr;
     int64_t lab_off = 0;  // offset in the lane's pinned label staging
+    double us_h2d = 0, us_compute = 0, us_d2h = 0;  // tensor-core worker phases (trace)
+    double ms_tc = 0, ms_recheck = 0;                // device time of the assignment / recheck kernels (trace)
 };
 
 struct Lane;
@@ -378,16 +380,35 @@ int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r)
         return KMB_ENOMEM;
     }
     int rc = KMB_OK;
+    const auto t0 = Clock::now();
     if (cudaMemcpyAsync(dX, r->X, sizeof(float) * r->n * r->d, cudaMemcpyHostToDevice, s) != cudaSuccess)
         rc = KMB_ECUDA;
+    const bool timed = r->srv_trace;
+    if (timed) {
+        cudaStreamSynchronize(s);
+        kmb_context_set_kernel_timing(ctx, 1);
+    }
+    const auto t1 = Clock::now();
     for (int64_t off = 0; rc == KMB_OK && off < r->n; off += kTcChunkRows) {
         const int64_t rows = std::min<int64_t>(kTcChunkRows, r->n - off);
         rc = kmb_infer(ctx, KMB_F32, KMB_MEM_DEVICE, dX + off * r->d, rows, r->d, m.C, m.k, KMB_FORM_BF16X3, 0,
                        dlab + off, nullptr, nullptr);
     }
+    const auto t2 = Clock::now();
     if (rc == KMB_OK &&
         cudaMemcpyAsync(r->labels_out, dlab, sizeof(int32_t) * r->n, cudaMemcpyDeviceToHost, s) != cudaSuccess)
         rc = KMB_ECUDA;
+    if (timed) {
+        cudaStreamSynchronize(s);
+        const auto t3 = Clock::now();
+        r->us_h2d = std::chrono::duration<double, std::micro>(t1 - t0).count();
+        r->us_compute = std::chrono::duration<double, std::micro>(t2 - t1).count();
+        r->us_d2h = std::chrono::duration<double, std::micro>(t3 - t2).count();
+        int64_t nl = 0;
+        kmb_context_kernel_time(ctx, 1, &r->ms_tc, &nl);
+        kmb_context_kernel_time(ctx, 4, &r->ms_recheck, &nl);
+        kmb_context_set_kernel_timing(ctx, 0);
+    }
     cudaFreeAsync(dX, s);
     cudaFreeAsync(dlab, s);
     if (cudaStreamSynchronize(s) != cudaSuccess && rc == KMB_OK) rc = KMB_ECUDA;
@@ -399,9 +420,11 @@ void tc_worker_loop(Server *srv) {
     kmb_context *ctx = nullptr;
     cudaStream_t ts = nullptr;
     if (kmb_context_create(srv->device, &ctx) != KMB_OK) ctx = nullptr;
-    if (ctx && cudaStreamCreateWithPriority(&ts, cudaStreamNonBlocking, srv->prio_low) == cudaSuccess) {
+    // Same priority as the lanes: a lower one let a stream of small launches
+    // starve the persistent CTAs (which need whole SMs) for tens of ms.
+    if (ctx && cudaStreamCreateWithPriority(&ts, cudaStreamNonBlocking, srv->prio_high) == cudaSuccess) {
         kmb_context_set_stream(ctx, ts);
-        kmb_context_set_max_sms(ctx, kTcMaxSms);
+        kmb_context_set_max_sms(ctx, -1);
     } else if (ctx) {
         kmb_context_destroy(ctx);
         ctx = nullptr;
@@ -447,6 +470,24 @@ void trainer_loop(Server *srv) {
     if (kmb_context_create(srv->device, &ctx) != KMB_OK) ctx = nullptr;
     if (ctx && cudaStreamCreateWithPriority(&ts, cudaStreamNonBlocking, srv->prio_low) == cudaSuccess)
         kmb_context_set_stream(ctx, ts);
+    // Pinned staging of a train's inputs and outputs: the caller's buffers may
+    // be pageable, and a pageable copy goes through the driver's own staging,
+    // holding a copy engine far longer than the DMA of a pinned buffer.
+    float *stage = nullptr;
+    size_t stage_bytes = 0;
+    auto stage_for = [&](size_t bytes) -> bool {
+        if (bytes <= stage_bytes) return true;
+        if (stage) cudaFreeHost(stage);
+        stage = nullptr;
+        stage_bytes = 0;
+        if (cudaMallocHost(&stage, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        stage_bytes = bytes;
+        return true;
+    };
+    stage_for((size_t)96 << 20);
     std::unique_lock<std::mutex> lock(srv->mu);
     while (true) {
         srv->cv.wait(lock, [&] {
@@ -467,8 +508,21 @@ void trainer_loop(Server *srv) {
             kmb_params p{r->k, r->iters, 0.0, KMB_FORM_PLAIN, 0};
             double obj = 0.0;
             int64_t it = 0;
-            rc = kmb_train(ctx, KMB_F32, KMB_MEM_HOST, r->X, r->n, r->d, r->C0, &p, r->C_out, r->labels_out, &obj,
-                           &it, nullptr);
+            const size_t nx = (size_t)r->n * r->d, nc = (size_t)r->k * r->d;
+            if (stage_for(sizeof(float) * (nx + 2 * nc + r->n))) {
+                float *sX = stage, *sC0 = stage + nx, *sC = sC0 + nc;
+                int32_t *slab = (int32_t *)(sC + nc);
+                std::memcpy(sX, r->X, sizeof(float) * nx);
+                std::memcpy(sC0, r->C0, sizeof(float) * nc);
+                rc = kmb_train(ctx, KMB_F32, KMB_MEM_HOST, sX, r->n, r->d, sC0, &p, sC, slab, &obj, &it, nullptr);
+                if (rc == KMB_OK) {
+                    std::memcpy(r->C_out, sC, sizeof(float) * nc);
+                    std::memcpy(r->labels_out, slab, sizeof(int32_t) * r->n);
+                }
+            } else {
+                rc = kmb_train(ctx, KMB_F32, KMB_MEM_HOST, r->X, r->n, r->d, r->C0, &p, r->C_out, r->labels_out,
+                               &obj, &it, nullptr);
+            }
         }
         lock.lock();
         r->rc = rc;
@@ -482,6 +536,7 @@ void trainer_loop(Server *srv) {
     lock.unlock();
     if (ctx) kmb_context_destroy(ctx);
     if (ts) cudaStreamDestroy(ts);
+    if (stage) cudaFreeHost(stage);
 }
 
 __global__ void prep_model_kernel(const float *__restrict__ C, int k, int d, int dpad, int kpad, float *__restrict__ Ct,
@@ -641,6 +696,7 @@ int kmb_server_submit_infer(void *handle, int32_t model_id, const float *X_host,
         r->labels_out = labels_host;
         r->C_out = nullptr;
         r->form = serve_form(srv, srv->models[model_id], n);
+        r->srv_trace = srv->trace != nullptr;
         r->bytes = r->form == KMB_FORM_BF16X3 ? (size_t)n * d * 4 + (size_t)n * 4 + 4096 : infer_bytes(n, d);
         r->t_submit = Clock::now();
         srv->all[r->id] = r;
@@ -705,9 +761,12 @@ int kmb_server_wait_detail(void *handle, int64_t request_id, double timeout_s, d
     if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
     if (queued_s) *queued_s = std::chrono::duration<double>(r->t_start - r->t_submit).count();
     if (srv->trace)
-        std::fprintf(srv->trace, "R id=%lld kind=%d form=%d n=%lld k=%lld d=%lld submit=%.1f start=%.1f done=%.1f\n",
+        std::fprintf(srv->trace,
+                     "R id=%lld kind=%d form=%d n=%lld k=%lld d=%lld submit=%.1f start=%.1f done=%.1f h2d=%.1f "
+                     "compute=%.1f d2h=%.1f tc_ms=%.3f recheck_ms=%.3f\n",
                      (long long)r->id, r->kind, r->form, (long long)r->n, (long long)r->k, (long long)r->d,
-                     srv->us(r->t_submit), srv->us(r->t_start), srv->us(r->t_done));
+                     srv->us(r->t_submit), srv->us(r->t_start), srv->us(r->t_done), r->us_h2d, r->us_compute,
+                     r->us_d2h, r->ms_tc, r->ms_recheck);
     const int rc = r->rc;
     srv->all.erase(it);
     delete r;
