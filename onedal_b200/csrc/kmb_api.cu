@@ -101,7 +101,7 @@ bool Workspace::ensure(DevBuf &b, size_t bytes) {
 void Workspace::release() {
     DevBuf *all[] = {&X, &C0, &Cout, &labels, &d2, &xnorm, &Ccur, &Cnew, &Ct, &h, &queue, &H, &Gs,
                      &counts, &offsets, &piece_base, &perm, &records, &shift_part, &empty_flag, &empty_ids,
-                     &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx};
+                     &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx, &rowb};
     for (DevBuf *b : all) {
         if (b->ptr) cudaFreeAsync(b->ptr, stream);
         b->ptr = nullptr;
@@ -157,6 +157,7 @@ int ensure_common(kmb_context *ctx, int64_t n, int64_t d, int64_t k, bool rechec
         ok &= ws.ensure(ws.Clo, sizeof(uint16_t) * tkp * tdp);
         ok &= ws.ensure(ws.h, sizeof(float) * tkp);
         ok &= ws.ensure(ws.tcx, kmb::tc_xchg_bytes());
+        ok &= ws.ensure(ws.rowb, sizeof(float) * 2 * n);
     }
     ok &= ws.ensure(ws.labels, sizeof(int32_t) * n);
     ok &= ws.ensure(ws.d2, sizeof(F) * n);
@@ -210,7 +211,7 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
                                    (const float *)ws.xnorm.ptr, &sc->cnorm_max, labels, d2,
                                    (RecheckEntry *)ws.queue.ptr, st, ctx->tc_per_tile ? -1 : ctx->num_sms,
                                    ws.tcx.ptr, prior,
-                                   (const double *)ws.shift_part.ptr, &sc->cnorm_max_prev, s);
+                                   (const double *)ws.shift_part.ptr, &sc->cnorm_max_prev, ws.rowb.ptr, s);
     }
     if (rc != KMB_OK) return fail(ctx, rc, "tensor-core assignment launch failed (d=%lld)", (long long)d);
     {

@@ -76,13 +76,7 @@ struct Params {
     int a_stages, b_stages;
     const float *h;  // -0.5||c_j||^2 per cluster, -inf padding
     const float *xnorm;
-    const double *cnorm_max;
-    // Prior bound (valid only when `prior`): labels / d2 of the previous pass
-    // (read before this pass overwrites them), per-cluster squared shifts of the
-    // update in between, and max ||c|| of the previous centroids.
-    int prior;
-    const double *shift_part;
-    const double *cnorm_max_prev;
+    const float2 *rowb;  // per row: {prior threshold, band}, from row_bounds_kernel
     int32_t *labels;
     float *d2;
     RecheckEntry *queue;
@@ -428,9 +422,6 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
         const int group = (warp - 2) >> 2;     // 0: warps 2-5, 1: warps 6-9
         const int row_in_tile = quarter * 32 + lane;
         const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
-        const double u = 5.9604644775390625e-8;  // 2^-24
-        const double ub2 = 1.52587890625e-5;      // 2^-16
-        const double cmax = *p.cnorm_max;
         long long acount = 0;
         bool ok = true;
         // Accumulators start from -h (written here, one row per lane), so after the
@@ -449,38 +440,26 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
         }
         // Both groups pass the same number of named barriers (one per row tile),
         // also after an abort, so neither can be left waiting on the other.
-        const double cmax_prev = p.prior ? *p.cnorm_max_prev : 0.0;
+        // Per-row inputs (band, prior threshold, ||x||^2) come from the row-bounds
+        // pass and are loaded one row tile ahead, so no latency sits between two
+        // accumulator drains.
+        auto row_of = [&](int lt_) { return (int64_t)(blockIdx.x + lt_ * gridDim.x) * BM + row_in_tile; };
+        float2 nb = make_float2(__int_as_float(0xff800000), 0.0f);
+        float nxn = 0.0f;
+        if (my_tiles > 0 && row_of(0) < p.n) {
+            nb = p.rowb[row_of(0)];
+            nxn = p.xnorm[row_of(0)];
+        }
         for (int lt = 0; lt < my_tiles; ++lt) {
             const int tile = blockIdx.x + lt * gridDim.x;
             const int64_t row = (int64_t)tile * BM + row_in_tile;
-            const float xn = row < p.n ? p.xnorm[row] : 0.0f;
-            // Per-score error bound e of this row (see the header); band = 2e.
-            const double xl = sqrt(fmax((double)xn, 0.0));
-            const double xc = xl * cmax;
-            const double e = 1.0625 * ((3.03 * ub2 + 2.0 * 3.0 * p.dpad * 2.0 * u) * xc +
-                                       2.0 * u * (0.5 * cmax * cmax + xc));
-            const double band = 2.0 * e;
-            const float band_up = __double2float_ru(band);
-            // Prior lower bound on the row's final best y (y = -score). With l the
-            // previous label and D_old^2 <= d2_prev + (its rounding bound), the
-            // triangle inequality gives ||x - c_new[l]|| <= D_old + ||c_new[l] -
-            // c_old[l]||, hence best y >= 0.5 (||x||^2 - (D_old + delta_l)^2) - e.
-            // Any cluster that can be the best or lie inside the band of the
-            // best has y >= that bound - band, so lower values are skipped.
-            float thr0 = __int_as_float(0xff800000);
-            const int lprev = (p.prior && row < p.n) ? p.labels[row] : -1;
-            if (lprev >= 0 && lprev < p.k) {
-                const int l = lprev;
-                const double d2p = (double)p.d2[row];
-                const double xcp = xl * cmax_prev;
-                const double e_prev = 1.0625 * ((3.03 * ub2 + 2.0 * 3.0 * p.dpad * 2.0 * u) * xcp +
-                                                2.0 * u * (0.5 * cmax_prev * cmax_prev + xcp));
-                const double dsq = fmax(d2p, 0.0) + 2.0 * e_prev + 2.0 * u * (fabs(d2p) + (double)xn);
-                const double rad = sqrt(dsq) + sqrt(p.shift_part[l]) * (1.0 + 1e-12);
-                const double r2 = rad * rad;
-                const double lb = 0.5 * ((double)xn * (1.0 - 2.0 * u) - r2) - 3.0 * e -
-                                  9.5367431640625e-7 * ((double)xn + r2);  // 2^-20 slack for this arithmetic
-                if (lb >= -3.0e38) thr0 = __double2float_rd(lb);  // also rejects NaN
+            const float thr0 = nb.x;     // prior lower bound minus the band (-inf without a prior)
+            const float band_up = nb.y;  // 2e rounded up
+            const double band = (double)band_up;
+            const float xn = nxn;
+            if (lt + 1 < my_tiles && row_of(lt + 1) < p.n) {
+                nb = p.rowb[row_of(lt + 1)];
+                nxn = p.xnorm[row_of(lt + 1)];
             }
             Top3 r;  // in y = -score space: b >= s >= t
             r.b = r.s = r.t = __int_as_float(0xff800000);
@@ -627,6 +606,50 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
     }
 }
 
+// Per row, ahead of the tensor-core pass (after the centroid prep has computed
+// max ||c||): the recheck band 2e rounded up, and the prior threshold.
+//   e = 1.0625 ((3.03 u_b^2 + 2 * 3 dpad * 2u) ||x|| cmax + 2u (cmax^2 / 2 + ||x|| cmax))
+// (the per-score bound of the kernel header). The prior: with l the previous
+// label and D_old^2 <= d2_prev + (its rounding bound, e of the previous
+// centroids), the triangle inequality gives ||x - c_new[l]|| <= D_old +
+// ||c_new[l] - c_old[l]||, hence the row's computed best y (= -score) is at
+// least 0.5 (||x||^2 - (D_old + delta_l)^2) - e. Any cluster that can be the
+// best or lie inside the band of the best has y >= that bound - 2e, so the
+// epilogue skips values below thr0 = bound - 2e (rounded down). Without a prior,
+// or for a row without a valid previous label, thr0 = -inf.
+__global__ void row_bounds_kernel(int64_t n, const float *__restrict__ xnorm, const int32_t *__restrict__ labels,
+                                  const float *__restrict__ d2, const double *__restrict__ shift_part,
+                                  const double *__restrict__ cnorm_max, const double *__restrict__ cnorm_max_prev,
+                                  int dpad, int k, int prior, float2 *__restrict__ out, const LoopState *st) {
+    if (st && st->done) return;
+    const double u = 5.9604644775390625e-8;  // 2^-24
+    const double ub2 = 1.52587890625e-5;      // 2^-16
+    const double cmax = *cnorm_max;
+    const double cmax_prev = prior ? *cnorm_max_prev : 0.0;
+    const double acc = 3.03 * ub2 + 2.0 * 3.0 * dpad * 2.0 * u;
+    for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < n;
+         row += (int64_t)gridDim.x * blockDim.x) {
+        const float xn = xnorm[row];
+        const double xl = sqrt(fmax((double)xn, 0.0));
+        const double xc = xl * cmax;
+        const double e = 1.0625 * (acc * xc + 2.0 * u * (0.5 * cmax * cmax + xc));
+        float thr0 = __int_as_float(0xff800000);
+        const int l = prior ? labels[row] : -1;
+        if (l >= 0 && l < k) {
+            const double d2p = (double)d2[row];
+            const double xcp = xl * cmax_prev;
+            const double e_prev = 1.0625 * (acc * xcp + 2.0 * u * (0.5 * cmax_prev * cmax_prev + xcp));
+            const double dsq = fmax(d2p, 0.0) + 2.0 * e_prev + 2.0 * u * (fabs(d2p) + (double)xn);
+            const double rad = sqrt(dsq) + sqrt(shift_part[l]) * (1.0 + 1e-12);
+            const double r2 = rad * rad;
+            const double lb = 0.5 * ((double)xn * (1.0 - 2.0 * u) - r2) - 3.0 * e -
+                              9.5367431640625e-7 * ((double)xn + r2);  // 2^-20 slack for this arithmetic
+            if (lb >= -3.0e38) thr0 = __double2float_rd(lb);          // also rejects NaN
+        }
+        out[row] = make_float2(thr0, __double2float_ru(2.0 * e));
+    }
+}
+
 // x -> (bf16(x), bf16(x - bf16(x))) into [rows][dpad] panels, zero padding,
 // and ||x||^2 with the summation order of row_norms_kernel. One warp per row,
 // grid-stride over rows; every element of X is read once.
@@ -751,9 +774,9 @@ static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t d
 int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
                      const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
                      float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, bool prior,
-                     const double *shift_part, const double *cnorm_max_prev, cudaStream_t s) {
+                     const double *shift_part, const double *cnorm_max_prev, void *rowb, cudaStream_t s) {
     const int64_t dpad = tc_dpad(d), kpad = tc_kpad(k);
-    if (prior && (!shift_part || !cnorm_max_prev)) return KMB_EINVAL;
+    if ((prior && (!shift_part || !cnorm_max_prev)) || !rowb) return KMB_EINVAL;
     if (dpad > 256) return KMB_EUNSUPPORTED;
     if (n == 0) return KMB_OK;
     // Shared memory plan: A stages (hi+lo panels of the row tile), B ring.
@@ -789,15 +812,18 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     p.b_stages = b_stages;
     p.h = h;
     p.xnorm = xnorm;
-    p.cnorm_max = cnorm_max;
-    p.prior = prior ? 1 : 0;
-    p.shift_part = shift_part;
-    p.cnorm_max_prev = cnorm_max_prev;
+    p.rowb = (const float2 *)rowb;
     p.labels = labels;
     p.d2 = d2;
     p.queue = queue;
     p.st = st;
     p.xchg = (tc::Top3x *)xchg;
+    {
+        const int bs = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+        tc::row_bounds_kernel<<<bs, 256, 0, s>>>(n, xnorm, labels, d2, shift_part, cnorm_max, cnorm_max_prev, (int)dpad,
+                                                 (int)k, prior ? 1 : 0, (float2 *)rowb, st);
+        KMB_LAUNCHED();
+    }
     if (cudaFuncSetAttribute(tc::assign_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return KMB_ECUDA;

@@ -85,7 +85,7 @@ struct Workspace {
     DevBuf X, C0, Cout, labels, d2, xnorm, Ccur, Cnew, Ct, h, queue;
     DevBuf H, Gs, counts, offsets, piece_base, perm, records, shift_part, empty_flag, empty_ids;
     DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;
-    DevBuf Xhi, Xlo, Chi, Clo, tcx;
+    DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb;
     // Grows `b` to at least `bytes`; returns false on allocation failure.
     bool ensure(DevBuf &b, size_t bytes);
     void release();
@@ -143,7 +143,7 @@ void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, v
 int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
                      const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
                      float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, bool prior,
-                     const double *shift_part, const double *cnorm_max_prev, cudaStream_t s);
+                     const double *shift_part, const double *cnorm_max_prev, void *rowb, cudaStream_t s);
 size_t tc_xchg_bytes();
 
 // ---- update ----------------------------------------------------------------
