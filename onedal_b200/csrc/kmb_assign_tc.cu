@@ -159,12 +159,16 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
 // kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=BN.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+// The three split-BF16 products of one k-step (xh.ch, xh.cl, xl.ch) into one
+// accumulator; descriptors are passed precomputed.
+__device__ __forceinline__ void mma_bf16x3(uint32_t tmem_d, uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+        "setp.ne.b32 p, 1, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %3, %5, p;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %4, %5, p;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %2, %3, %5, p;\n\t}" ::"r"(tmem_d),
+        "l"(ah), "l"(al), "l"(bh), "l"(bl), "r"(kIdesc)
         : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -339,7 +343,8 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             int a_issued[2] = {0, 0};
             int b_issued[MAX_B_STAGES];
             for (int i = 0; i < MAX_B_STAGES; ++i) b_issued[i] = 0;
-            long long bcount = 0;
+            int bs = 0;
+            uint32_t bphase = 0;  // B ring position and the parity of its current lap
             bool ok = true;
             for (int lt = 0; lt < my_tiles && ok; ++lt) {
                 const int tile = blockIdx.x + lt * gridDim.x;
@@ -354,15 +359,17 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 }
                 a_issued[as]++;
                 for (int j = 0; j < p.ntiles_n && ok; ++j) {
-                    for (int kp = 0; kp < p.kpanels; ++kp, ++bcount) {
-                        const int bs = (int)(bcount % p.b_stages);
-                        const int buse = (int)(bcount / p.b_stages);
-                        if (!mbar_wait(&bar->b_empty[bs], (buse & 1) ^ 1, abort)) { ok = false; break; }
+                    for (int kp = 0; kp < p.kpanels; ++kp) {
+                        if (!mbar_wait(&bar->b_empty[bs], bphase ^ 1, abort)) { ok = false; break; }
                         mbar_expect_tx(&bar->b_full[bs], 2 * PANEL);
                         uint8_t *Bb = B + (size_t)bs * 2 * PANEL;
                         tma_load_2d(Bb, &tmCh, &bar->b_full[bs], kp * KP, j * BN);
                         tma_load_2d(Bb + PANEL, &tmCl, &bar->b_full[bs], kp * KP, j * BN);
                         b_issued[bs]++;
+                        if (++bs == p.b_stages) {
+                            bs = 0;
+                            bphase ^= 1;
+                        }
                     }
                 }
             }
@@ -377,7 +384,9 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
     } else if (warp == 1) {
         if (lane == 0) {
             // ---------------- MMA issuer ----------------
-            long long bcount = 0, acount = 0;
+            long long acount = 0;
+            int bs = 0;
+            uint32_t bphase = 0;  // B ring position and the parity of its current lap
             bool ok = true;
             for (int lt = 0; lt < my_tiles && ok; ++lt) {
                 const int as = p.a_stages == 2 ? (lt & 1) : 0;
@@ -392,21 +401,22 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                     if (!mbar_wait(&bar->acc_empty[slot], use & 1, abort)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t tmem_d = tmem_base + (uint32_t)(slot * BN);
-                    for (int kp = 0; kp < p.kpanels; ++kp, ++bcount) {
-                        const int bs = (int)(bcount % p.b_stages);
-                        const int buse = (int)(bcount / p.b_stages);
-                        if (!mbar_wait(&bar->b_full[bs], buse & 1, abort)) { ok = false; break; }
+                    for (int kp = 0; kp < p.kpanels; ++kp) {
+                        if (!mbar_wait(&bar->b_full[bs], bphase, abort)) { ok = false; break; }
                         tc_fence_after();
-                        const uint32_t ah = a_base + kp * PANEL, al = a_base + (p.kpanels + kp) * PANEL;
-                        const uint32_t bh = su32(B + (size_t)bs * 2 * PANEL), bl = bh + PANEL;
+                        const uint64_t ah = sw128_desc(a_base + kp * PANEL);
+                        const uint64_t al = sw128_desc(a_base + (p.kpanels + kp) * PANEL);
+                        const uint64_t bh = sw128_desc(su32(B + (size_t)bs * 2 * PANEL));
+                        const uint64_t bl = sw128_desc(su32(B + (size_t)bs * 2 * PANEL + PANEL));
+                        // 16 bf16 = 32 bytes along the swizzled row = 2 in the descriptor's address field
 #pragma unroll
-                        for (int ks = 0; ks < KP / 16; ++ks) {
-                            const uint32_t off = ks * 32;  // 16 bf16 = 32 bytes along the swizzled row
-                            mma_bf16(tmem_d, sw128_desc(ah + off), sw128_desc(bh + off), 1u);
-                            mma_bf16(tmem_d, sw128_desc(ah + off), sw128_desc(bl + off), 1u);
-                            mma_bf16(tmem_d, sw128_desc(al + off), sw128_desc(bh + off), 1u);
-                        }
+                        for (int ks = 0; ks < KP / 16; ++ks)
+                            mma_bf16x3(tmem_d, ah + 2 * ks, al + 2 * ks, bh + 2 * ks, bl + 2 * ks);
                         mma_commit(&bar->b_empty[bs]);  // frees the B stage once these MMAs finish
+                        if (++bs == p.b_stages) {
+                            bs = 0;
+                            bphase ^= 1;
+                        }
                     }
                     if (ok) mma_commit(&bar->acc_full[slot]);
                 }
