@@ -19,26 +19,27 @@
 // is queued with its two best clusters (or flagged for a full rescan when a
 // third cluster is inside the band) and re-scored in FP64 by the recheck kernel.
 //
-// Kernel structure (one CTA per SM, persistent over 128-row tiles, 6 warps):
+// Kernel structure (one CTA per SM, persistent over 128-row tiles, 14 warps):
 //   warp 0   TMA producer: A = the tile's Xhi/Xlo panels (128 rows x 64 bf16,
 //            SWIZZLE_128B), B = Chi/Clo panels of 128 clusters, ring of stages
 //   warp 1   TMEM allocation + single-thread tcgen05.mma issue; commits free
 //            B stages, publish accumulators and release A tiles
-//   warps 2-9 epilogue, two groups of 4 warps: group g owns TMEM accumulator g
-//            and the cluster tiles whose running index is g mod 2. Before the
-//            MMAs of a tile start, the group writes -h_j into every lane of the
-//            accumulator (tcgen05.st), so the MMAs leave y = x.c - h = -score
-//            there and no per-score subtraction is needed. The group reads y
-//            with tcgen05.ld (one TMEM lane = one row per thread) and keeps a
-//            running top-3 per row: each 32-column chunk is first reduced to
-//            its maximum (branch-free, 3-input max); only chunks that beat the
-//            row's third-best take the exact insertion path. At the end of a
-//            row tile group 1 hands its top-3 to group 0 through a small global
-//            scratch (per CTA, by row-tile parity) and a named barrier; group 0
-//            merges and writes the row's outputs.
-// Four accumulators (all 512 TMEM columns) alternate between the groups, two
-// per group, so each group reads one accumulator while the MMAs fill its other
-// one, and both groups run concurrently with the MMAs. Every mbarrier wait is bounded; on timeout the
+//   warps 2-13 epilogue, three groups of 4 warps (one per TMEM lane quarter):
+//            the running cluster tiles go round the groups. Before the MMAs of
+//            a tile start, the group that drained the accumulator last writes
+//            -h_j into every lane of it (tcgen05.st), so the MMAs leave
+//            y = x.c - h = -score there and no per-score subtraction is needed.
+//            A group reads y with tcgen05.ld (one TMEM lane = one row per
+//            thread) and keeps a running top-3 per row: each 32-column chunk
+//            is first reduced to its maximum (branch-free, 3-input max); only
+//            chunks holding a value at or above the row's threshold take the
+//            exact insertion path. At the end of a row tile groups 1 and 2 hand
+//            their top-3 to group 0 through a small global scratch (per SM, by
+//            row-tile parity) and a named barrier; group 0 merges and writes
+//            the row's outputs.
+// Four accumulators (all 512 TMEM columns) rotate through the groups, so
+// while one group drains an accumulator the MMAs fill the others. Every mbarrier
+// wait is bounded; on timeout the
 // CTA records KMB_ETIMEDOUT in the loop state, drains its own TMA loads and
 // MMAs with bounded waits, frees TMEM and returns.
 #include "kmb_internal.cuh"
@@ -57,7 +58,8 @@ constexpr int KP = 64;                  // bf16 per panel row (128 bytes, SWIZZL
 constexpr int PANEL = 128 * 128;        // bytes per 128-row panel
 constexpr int NACC = 4;                 // TMEM accumulators: two per epilogue group (double-buffered)
 constexpr int TMEM_COLS = NACC * BN;    // 512 = all of TMEM
-constexpr int NTHREADS = 320;           // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue (two groups of 4)
+constexpr int NGROUPS = 3;              // epilogue groups of 4 warps (one warp per TMEM lane quarter)
+constexpr int NTHREADS = 64 + NGROUPS * 128;  // warp 0 TMA, warp 1 MMA, warps 2.. epilogue
 constexpr int MAX_B_STAGES = 8;
 constexpr int kMaxSmid = 1024;
 constexpr long long kTimeoutCycles = 4000000000ll;  // ~2 s at 1.9 GHz
@@ -81,7 +83,7 @@ struct Params {
     float *d2;
     RecheckEntry *queue;
     LoopState *st;
-    Top3x *xchg;  // per SM (one CTA fits an SM): 2 x 128 rows of group 1's top-3 (row-tile parity)
+    Top3x *xchg;  // per SM (one CTA fits an SM): 2 (row-tile parity) x (NGROUPS-1) x 128 rows of top-3
 };
 
 struct Barriers {
@@ -427,16 +429,17 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             mbar_drain(&bar->mma_done, 0);
         }
     } else {
-        // ---------------- epilogue (warps 2..9, two groups) ----------------
+        // ---------------- epilogue (warps 2.., NGROUPS groups of 4) ----------------
         const int quarter = warp & 3;          // TMEM lanes 32*quarter .. +31
-        const int group = (warp - 2) >> 2;     // 0: warps 2-5, 1: warps 6-9
+        const int group = (warp - 2) >> 2;     // 0: warps 2-5, 1: warps 6-9, ...
         const int row_in_tile = quarter * 32 + lane;
         const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
         long long acount = 0;
+        int arot = 0;  // acount % NGROUPS
         bool ok = true;
         // Accumulators start from -h (written here, one row per lane), so after the
         // MMAs they hold y = x.c - h = -score and the argmin becomes a max over y.
-        for (int a0 = group; a0 < NACC; a0 += 2) {  // this group's accumulators: running tiles a0, a0 + 4, ...
+        for (int a0 = group; a0 < NACC; a0 += NGROUPS) {  // first uses of the accumulators, spread over the groups
             const float *hn = p.h + (size_t)(a0 % p.ntiles_n) * BN;
 #pragma unroll 1
             for (int c0 = 0; c0 < BN; c0 += 32) {
@@ -475,8 +478,8 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             r.b = r.s = r.t = __int_as_float(0xff800000);
             r.ib = r.is = 0;
             float thr = thr0;  // values below thr cannot change the outputs
-            for (int j = 0; j < p.ntiles_n; ++j, ++acount) {
-                if ((int)(acount & 1) != group || !ok) continue;
+            for (int j = 0; j < p.ntiles_n; ++j, ++acount, arot = (arot + 1 == NGROUPS) ? 0 : arot + 1) {
+                if (arot != group || !ok) continue;  // running cluster tiles go round the groups
                 const int slot = (int)(acount % NACC);
                 const int use = (int)(acount / NACC);
                 // every lane waits; the warp proceeds only if all lanes saw completion
@@ -488,18 +491,16 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 // -h of the cluster tile this accumulator holds next
                 const float *hn = p.h + (size_t)((acount + NACC) % p.ntiles_n) * BN;
 #pragma unroll 1
-                for (int c0 = 0; c0 < BN; c0 += 64) {
-                    float v[64];
+                for (int c0 = 0; c0 < BN; c0 += 32) {
+                    float v[32];
                     __syncwarp();  // tcgen05.ld/st are warp-collective: reconverge after the filtered path
                     const uint32_t taddr = lane_base + (uint32_t)(slot * BN + c0);
                     tmem_ld32_nowait(taddr, v);
-                    tmem_ld32_nowait(taddr + 32, v + 32);
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                     tmem_st32_from(taddr, hn + c0);
-                    tmem_st32_from(taddr + 32, hn + c0 + 32);
-#pragma unroll
-                    for (int half = 0; half < 2; ++half) {
-                        const float *w = v + 32 * half;
+                    {
+                        const float *w = v;
+                        constexpr int half = 0;
                         float m[11];
 #pragma unroll
                         for (int i = 0; i < 10; ++i) m[i] = max3f(w[3 * i], w[3 * i + 1], w[3 * i + 2]);
@@ -564,29 +565,32 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             r.b = -r.b;
             r.s = -r.s;
             r.t = -r.t;
-            // Group 1 hands its top-3 to group 0 (same rows) through the CTA's
-            // scratch slot for this row-tile parity, then group 0 merges.
-            Top3x *xs = p.xchg + ((size_t)smid * 2 + (lt & 1)) * BM + row_in_tile;
-            if (group == 1) {
+            // Groups 1.. hand their top-3 to group 0 (same rows) through the SM's
+            // scratch slots for this row-tile parity, then group 0 merges.
+            Top3x *xs = p.xchg + ((size_t)smid * 2 + (lt & 1)) * (NGROUPS - 1) * BM + row_in_tile;
+            if (group > 0) {
                 Top3x q;
                 q.b = r.b;
                 q.s = r.s;
                 q.t = r.t;
                 q.ib = r.ib;
                 q.is = r.is;
-                *xs = q;
+                xs[(group - 1) * BM] = q;
                 __threadfence_block();
             }
-            named_bar_sync(1 + quarter, 64);
-            if (group == 1 || !ok) continue;
-            const Top3x q = *xs;
-            Top3 o;
-            o.b = q.b;
-            o.s = q.s;
-            o.t = q.t;
-            o.ib = q.ib;
-            o.is = q.is;
-            r = top3_merge(r, o);
+            named_bar_sync(1 + quarter, 32 * NGROUPS);
+            if (group > 0 || !ok) continue;
+#pragma unroll
+            for (int g = 1; g < NGROUPS; ++g) {
+                const Top3x q = xs[(g - 1) * BM];
+                Top3 o;
+                o.b = q.b;
+                o.s = q.s;
+                o.t = q.t;
+                o.ib = q.ib;
+                o.is = q.is;
+                r = top3_merge(r, o);
+            }
             if (row < p.n) {
                 p.labels[row] = r.ib;
                 p.d2[row] = 2.0f * r.b + xn;
@@ -722,7 +726,7 @@ __global__ void reset_cmax_kernel(double *p, double *prev, const LoopState *st) 
 
 // Hand-off slots are indexed by %smid (a CTA needs a whole SM's shared memory,
 // so no two CTAs of this kernel share an SM at a time); ids are below kMaxSmid.
-size_t tc_xchg_bytes() { return (size_t)tc::kMaxSmid * 2 * tc::BM * sizeof(tc::Top3x); }
+size_t tc_xchg_bytes() { return (size_t)tc::kMaxSmid * 2 * (tc::NGROUPS - 1) * tc::BM * sizeof(tc::Top3x); }
 
 int64_t tc_dpad(int64_t d) { return (d + tc::KP - 1) / tc::KP * tc::KP; }
 int64_t tc_kpad(int64_t k) { return (k + tc::BN - 1) / tc::BN * tc::BN; }
