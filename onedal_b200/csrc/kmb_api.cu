@@ -269,7 +269,11 @@ void prepare_rows<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d,
 template <typename F>
 int upload(kmb_context *ctx, kmb::DevBuf &buf, const void *src, size_t bytes, const F **out) {
     if (!ctx->ws.ensure(buf, bytes)) return fail(ctx, KMB_ENOMEM, "device allocation of %zu bytes failed", bytes);
-    KMB_CUDA(cudaMemcpyAsync(buf.ptr, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    // in pieces, so that other streams' small copies interleave with a large upload
+    const size_t piece = (size_t)8 << 20;
+    for (size_t off = 0; off < bytes; off += piece)
+        KMB_CUDA(cudaMemcpyAsync((char *)buf.ptr + off, (const char *)src + off, std::min(piece, bytes - off),
+                                 cudaMemcpyHostToDevice, ctx->stream));
     *out = (const F *)buf.ptr;
     return KMB_OK;
 }

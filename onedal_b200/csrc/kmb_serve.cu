@@ -367,6 +367,19 @@ void scheduler_loop(Server *srv) {
     }
 }
 
+// Host<->device copy in pieces of at most 8 MiB: a copy engine works through a
+// stream's copies in order, so a 300 MB upload in one piece held a small
+// request's 100 KB upload on another stream for milliseconds.
+cudaError_t copy_in_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+    const size_t piece = (size_t)8 << 20;
+    for (size_t off = 0; off < bytes; off += piece) {
+        const cudaError_t e = cudaMemcpyAsync((char *)dst + off, (const char *)src + off, std::min(piece, bytes - off),
+                                              kind, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 // Large infer request on the tensor-core worker: rows uploaded once, then
 // kmb_infer (BF16x3, FP64 recheck) over row chunks on the worker's stream.
 int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r) {
@@ -381,7 +394,7 @@ int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r)
     }
     int rc = KMB_OK;
     const auto t0 = Clock::now();
-    if (cudaMemcpyAsync(dX, r->X, sizeof(float) * r->n * r->d, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    if (copy_in_pieces(dX, r->X, sizeof(float) * r->n * r->d, cudaMemcpyHostToDevice, s) != cudaSuccess)
         rc = KMB_ECUDA;
     const bool timed = r->srv_trace;
     if (timed) {
