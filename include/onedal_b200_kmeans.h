@@ -101,14 +101,28 @@ KMB_API int kmb_context_release_workspace(kmb_context *ctx);
 /* Train: replaces train_ops_dispatcher<host_policy, F, lloyd_dense, clustering>
  * (cpp/oneapi/dal/algo/kmeans/detail/train_ops.cpp:24-42 ->
  *  backend/cpu/train_kernel_lloyd.cpp:84-144).
- * X: n x d, C0: k x d initial centroids (required; k-means++ init is not on
- * this path). Outputs: C_out k x d, responses n (int32, against the final
+ * X: n x d, C0: k x d initial centroids (required here; a dispatcher given
+ * none first calls kmb_init_plusplus, as oneDAL's train() does). Outputs: C_out k x d, responses n (int32, against the final
  * centroids), objective = exact sum ||x - c_label||^2 (FP64 accumulation),
  * iteration_count. Pointers are host or device memory per `memory`.
  * stats may be NULL. */
 KMB_API int kmb_train(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, const void *C0,
                       const kmb_params *params, void *C_out, int32_t *responses, double *objective,
                       int64_t *iteration_count, kmb_stats *stats);
+
+/* k-means++ initial centroids: replaces the default initialisation that
+ * oneDAL's train() runs when no initial centroids are given
+ * (cpp/oneapi/dal/algo/kmeans/detail/train_init_centroids.hpp:47-74 ->
+ *  DAAL KMeansInitKernel<plusPlusDense>, kmeans_plusplus_init_impl.i:538-673,
+ *  one trial). With seed = 777777 (the reference's default,
+ * kmeans_init_parameter_types.cpp:41-48) the chosen rows equal the
+ * reference's: the same generator, draw order, block sums and sampling walk.
+ * C_out: k x d, host or device per `memory`. KMB_EINVAL for k > n, and when
+ * every remaining distance is zero (fewer distinct rows than k) or the total
+ * is not finite: the reference's resampling would never end there. */
+KMB_API int kmb_init_plusplus(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, int64_t k,
+                              uint32_t seed, void *C_out);
+#define KMB_PLUSPLUS_DEFAULT_SEED 777777u
 
 /* Infer: replaces infer_ops_dispatcher<host_policy, F, lloyd_dense, clustering>
  * (cpp/oneapi/dal/algo/kmeans/detail/infer_ops.cpp:26-43 ->

@@ -5,7 +5,9 @@
 // against the B200 dispatchers, every call below runs on the GPU.
 //
 //   kmeans_client <gold.txt> <float|double>
-// prints: iterations, objective, centroids, responses, infer objective.
+// prints: iterations, objective, centroids, responses, infer objective, then the
+// smoke case of the reference suite (fixture.hpp:221-252) trained WITHOUT initial
+// centroids (oneDAL's default k-means++ init): smoke_centroids, smoke_responses.
 #include "oneapi/dal/algo/kmeans.hpp"
 #include "oneapi/dal/table/homogen.hpp"
 #include "oneapi/dal/table/row_accessor.hpp"
@@ -46,6 +48,19 @@ int run(const std::vector<double> &xs, std::int64_t n, std::int64_t d, const std
     } catch (const dal::invalid_argument &) {
         std::printf("invalid_argument ok\n");
     }
+    const F smoke[] = { 1, 1, 2, 2, 1, 2, 2, 1, -1, -1, -1, -2, -2, -1, -2, -2 };
+    const auto smoke_data = dal::homogen_table::wrap(smoke, 8, 2);
+    const auto smoke_res = dal::train(
+        dal::kmeans::descriptor<F>().set_cluster_count(2).set_max_iteration_count(4).set_accuracy_threshold(0.001),
+        smoke_data);
+    const auto sc = dal::row_accessor<const F>(smoke_res.get_model().get_centroids()).pull({ 0, -1 });
+    std::printf("smoke_centroids");
+    for (std::int64_t i = 0; i < sc.get_count(); ++i) std::printf(" %.9g", (double)sc[i]);
+    std::printf("\n");
+    const auto sr = dal::row_accessor<const std::int32_t>(smoke_res.get_responses()).pull({ 0, -1 });
+    std::printf("smoke_responses");
+    for (std::int64_t i = 0; i < sr.get_count(); ++i) std::printf(" %d", sr[i]);
+    std::printf("\n");
     return 0;
 }
 

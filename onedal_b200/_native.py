@@ -22,7 +22,7 @@ EXPORTED = (
     "kmb_partial_sums", "kmb_finalize_centroids", "kmb_version", "kmb_lloyd_iterate",
     "kmb_context_set_kernel_timing", "kmb_context_kernel_time", "kmb_infer_noalloc",
     "kmb_server_create", "kmb_server_destroy", "kmb_server_add_model", "kmb_server_submit_infer",
-    "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats", "kmb_server_infer_form", "kmb_server_wait_detail", "kmb_context_set_max_sms", "kmb_batched_train",
+    "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats", "kmb_server_infer_form", "kmb_server_wait_detail", "kmb_context_set_max_sms", "kmb_init_plusplus", "kmb_batched_train",
 )
 
 
@@ -84,6 +84,8 @@ def load_library(path: str = LIB_PATH):
             lib.kmb_status_string.restype = ctypes.c_char_p
             lib.kmb_context_release_workspace.argtypes = [P]
             lib.kmb_version.restype = ctypes.c_char_p
+            lib.kmb_init_plusplus.argtypes = [P, ctypes.c_int, ctypes.c_int, P, I64, I64, I64, ctypes.c_uint32, P]
+            lib.kmb_context_set_max_sms.argtypes = [P, ctypes.c_int]
             lib.kmb_train.argtypes = [P, ctypes.c_int, ctypes.c_int, P, I64, I64, P, ctypes.POINTER(kmb_params), P, P,
                                       ctypes.POINTER(D), ctypes.POINTER(I64), ctypes.POINTER(kmb_stats)]
             lib.kmb_infer.argtypes = [P, ctypes.c_int, ctypes.c_int, P, I64, I64, P, I64, I32, I32, P,

@@ -13,8 +13,10 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -101,7 +103,8 @@ bool Workspace::ensure(DevBuf &b, size_t bytes) {
 void Workspace::release() {
     DevBuf *all[] = {&X, &C0, &Cout, &labels, &d2, &xnorm, &Ccur, &Cnew, &Ct, &h, &queue, &H, &Gs,
                      &counts, &offsets, &piece_base, &perm, &records, &shift_part, &empty_flag, &empty_ids,
-                     &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx, &rowb};
+                     &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx, &rowb, &pp_acc, &pp_rand,
+                     &pp_state};
     for (DevBuf *b : all) {
         if (b->ptr) cudaFreeAsync(b->ptr, stream);
         b->ptr = nullptr;
@@ -541,6 +544,79 @@ int validate_shapes(kmb_context *ctx, int dtype, int64_t n, int64_t d, int64_t k
 
 }  // namespace
 
+// k-means++ initialisation (kmb_init.cu has the device side). The host draws
+// the uniforms exactly as the reference's generator does and hands them to
+// the device in order: k center probabilities, then a pool of resample draws
+// (refilled, continuing the same sequence, when a round runs out of them).
+template <typename F>
+int init_plusplus_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t d, int64_t k, uint32_t seed,
+                       void *C_out) {
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    const F *X = (const F *)Xv;
+    if (memory == KMB_MEM_HOST) {
+        int rc = upload<F>(ctx, ws.X, Xv, sizeof(F) * n * d, &X);
+        if (rc) return rc;
+    }
+    // KMB_PLUSPLUS_POOL (1..2^20) shrinks the resample pool so tests can drive the refill path
+    int pool_n = 4096;
+    if (const char *e = getenv("KMB_PLUSPLUS_POOL")) pool_n = (int)std::min(std::max(atol(e), 1L), 1L << 20);
+    const int64_t nb = (n + 511) / 512;
+    bool ok = ws.ensure(ws.d2, sizeof(F) * n) && ws.ensure(ws.pp_acc, sizeof(F) * nb) &&
+              ws.ensure(ws.pp_rand, sizeof(F) * (k + pool_n)) && ws.ensure(ws.pp_state, sizeof(kmb::PPState)) &&
+              ws.ensure(ws.Cout, sizeof(F) * k * d);
+    if (!ok) return fail(ctx, KMB_ENOMEM, "device allocation failed (k-means++ init, n=%lld)", (long long)n);
+    F *md = (F *)ws.d2.ptr, *acc = (F *)ws.pp_acc.ptr, *rnd = (F *)ws.pp_rand.ptr;
+    kmb::PPState *st = (kmb::PPState *)ws.pp_state.ptr;
+    F *C = memory == KMB_MEM_DEVICE ? (F *)C_out : (F *)ws.Cout.ptr;
+
+    std::mt19937 gen(seed);
+    std::uniform_real_distribution<F> uni(F(0), F(1));
+    std::vector<F> host((size_t)(k + pool_n));
+    for (int64_t i = 0; i < k; ++i) host[(size_t)i] = uni(gen);
+    for (int i = 0; i < pool_n; ++i) host[(size_t)(k + i)] = uni(gen);
+    KMB_CUDA(cudaMemcpyAsync(rnd, host.data(), sizeof(F) * (k + pool_n), cudaMemcpyHostToDevice, s));
+    kmb::PPState hs{};
+    KMB_CUDA(cudaMemcpyAsync(st, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+    int64_t row0 = (int64_t)(size_t)(host[0] * F(n));
+    if (row0 == n) --row0;
+    kmb::launch_pp_fill<F>(md, n, s);
+    kmb::launch_pp_first<F>(X, d, row0, C, s);
+    int64_t c_begin = 1;
+    bool update_first = true;
+    int64_t round_draws = 0;  // resample draws spent on the round that stopped
+    for (;;) {
+        kmb::launch_pp_rounds<F>(X, n, d, k, c_begin, update_first, md, acc, rnd, rnd + k, pool_n, C, st, s);
+        KMB_CUDA(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        KMB_CUDA(cudaStreamSynchronize(s));
+        if (!hs.stopped) break;
+        if (hs.stopped == 2)
+            return fail(ctx, KMB_EINVAL,
+                        "k-means++ init: no row left to sample for center %lld (fewer than k distinct rows, or "
+                        "non-finite distances)",
+                        (long long)hs.stop_round);
+        // the reference keeps drawing until a row with a positive distance is hit; with a
+        // positive finite total at least 90% of the mass lies on such rows, so this bound
+        // is only reached on broken arithmetic
+        round_draws = hs.stop_round == c_begin && !update_first ? round_draws + hs.pool_used : hs.pool_used;
+        if (round_draws > (int64_t)1 << 24)
+            return fail(ctx, KMB_EINVAL, "k-means++ init: no row with a positive distance found for center %lld",
+                        (long long)hs.stop_round);
+        for (int i = 0; i < pool_n; ++i) host[(size_t)(k + i)] = uni(gen);
+        KMB_CUDA(cudaMemcpyAsync(rnd + k, host.data() + k, sizeof(F) * pool_n, cudaMemcpyHostToDevice, s));
+        c_begin = hs.stop_round;
+        update_first = false;
+        hs.stopped = 0;
+        hs.pool_used = 0;
+        KMB_CUDA(cudaMemcpyAsync(st, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+    }
+    if (memory == KMB_MEM_HOST) {
+        KMB_CUDA(cudaMemcpyAsync(C_out, C, sizeof(F) * k * d, cudaMemcpyDeviceToHost, s));
+        KMB_CUDA(cudaStreamSynchronize(s));
+    }
+    return KMB_OK;
+}
+
 extern "C" {
 
 const char *kmb_version(void) { return "onedal_b200 kmeans 0.1 (sm_100a)"; }
@@ -637,6 +713,19 @@ int kmb_train(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n,
     if (dtype == KMB_F32)
         return train_impl<float>(ctx, memory, X, n, d, C0, params, C_out, responses, objective, iteration_count, stats);
     return train_impl<double>(ctx, memory, X, n, d, C0, params, C_out, responses, objective, iteration_count, stats);
+}
+
+int kmb_init_plusplus(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, int64_t k,
+                      uint32_t seed, void *C_out) {
+    if (!ctx) return KMB_EINVAL;
+    ctx->last_error.clear();
+    cudaSetDevice(ctx->device);
+    if (!X || !C_out || n <= 0 || d <= 0 || k <= 0) return fail(ctx, KMB_EINVAL, "bad argument");
+    if (k > n) return fail(ctx, KMB_EINVAL, "cluster_count %lld exceeds the row count %lld", (long long)k, (long long)n);
+    if (memory != KMB_MEM_HOST && memory != KMB_MEM_DEVICE) return fail(ctx, KMB_EINVAL, "unknown memory kind");
+    if (dtype == KMB_F32) return init_plusplus_impl<float>(ctx, memory, X, n, d, k, seed, C_out);
+    if (dtype == KMB_F64) return init_plusplus_impl<double>(ctx, memory, X, n, d, k, seed, C_out);
+    return fail(ctx, KMB_EINVAL, "unknown dtype");
 }
 
 int kmb_infer(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, const void *C, int64_t k,

@@ -43,6 +43,22 @@ struct RecheckEntry {
     int full;  // 1: more than two clusters lie inside the error band -> scan all k
 };
 
+// Device state of the k-means++ initialisation (kmb_init.cu).
+struct PPState {
+    int stopped;          // the select step ran out of uniforms (stop_round is to be redone)
+    int pool_used;        // resample draws consumed from the current pool
+    long long stop_round;
+    long long rows_chosen;
+};
+
+template <typename F>
+void launch_pp_fill(F *md, int64_t n, cudaStream_t s);
+template <typename F>
+void launch_pp_first(const F *X, int64_t d, int64_t row, F *C, cudaStream_t s);
+template <typename F>
+void launch_pp_rounds(const F *X, int64_t n, int64_t d, int64_t k, int64_t c_begin, bool update_first, F *md, F *acc,
+                      const F *probs, const F *pool, int pool_n, F *C, PPState *st, cudaStream_t s);
+
 // Queues a near-tie row for the FP64 recheck. Two-candidate entries fill the
 // queue from the front (count st->n_recheck), full-rescan entries from the back
 // (count st->n_full); the capacity is the row count, and a row is queued once.
@@ -85,7 +101,7 @@ struct Workspace {
     DevBuf X, C0, Cout, labels, d2, xnorm, Ccur, Cnew, Ct, h, queue;
     DevBuf H, Gs, counts, offsets, piece_base, perm, records, shift_part, empty_flag, empty_ids;
     DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;
-    DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb;
+    DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb, pp_acc, pp_rand, pp_state;
     // Grows `b` to at least `bytes`; returns false on allocation failure.
     bool ensure(DevBuf &b, size_t bytes);
     void release();

@@ -318,20 +318,49 @@ def _device_of(t):
     return t.device.index if t.device.index is not None else 0
 
 
+def init_plusplus(data, cluster_count: int, float_type=np.float32, seed: int = 777777, ctx=None):
+    """k-means++ initial centroids (k x d) as oneDAL's train() computes them when no
+    initial centroids are given: DAAL's dense plusPlus init with one trial
+    (kmeans_plusplus_init_impl.i:538-673), seed 777777 by default. Same memory
+    space as `data` (numpy array or CUDA tensor)."""
+    X, dev = _as_table(data, float_type)
+    n, d = X.shape
+    k = int(cluster_count)
+    if ctx is None:
+        ctx = _native.context(_device_of(X) if dev else 0)
+    if dev:
+        import torch
+        C = torch.empty((k, d), dtype=X.dtype, device=X.device)
+        ctx.set_stream(torch.cuda.current_stream(X.device).cuda_stream)
+    else:
+        C = np.empty((k, d), dtype=float_type)
+    dtype = _native.KMB_F32 if float_type == np.float32 else _native.KMB_F64
+    mem = _native.KMB_MEM_DEVICE if dev else _native.KMB_MEM_HOST
+    try:
+        ctx.check(ctx.lib.kmb_init_plusplus(ctx.handle, dtype, mem, _ptr(X, dev), n, d, k, ctypes.c_uint32(seed),
+                                            _ptr(C, dev)))
+    except _native.NativeError as e:
+        _raise_native(e)
+    return C
+
+
 def train(desc: descriptor, data, initial_centroids=None) -> train_result:
     """dal::train(desc, data, initial_centroids) for method lloyd_dense (train.hpp:26-29)."""
     if desc.method != method.lloyd_dense:
         raise invalid_argument("only method::lloyd_dense is implemented on this path")
     _check_train_preconditions(desc, data, initial_centroids)
-    if not _has_data(initial_centroids):
-        raise invalid_argument("initial_centroids are required: k-means++ initialisation is not on this path")
     X, dev = _as_table(data, desc.float_type)
-    C0, dev_c = _as_table(initial_centroids, desc.float_type)
-    if dev != dev_c:
-        raise invalid_argument("data and initial centroids must live in the same memory space")
     n, d = X.shape
     k = desc.get_cluster_count()
     ctx = _native.context(_device_of(X) if dev else 0)
+    if _has_data(initial_centroids):
+        C0, dev_c = _as_table(initial_centroids, desc.float_type)
+        if dev != dev_c:
+            raise invalid_argument("data and initial centroids must live in the same memory space")
+    else:
+        # the reference's default: k-means++ with one trial and seed 777777
+        # (detail/train_init_centroids.hpp:47-74), computed on the GPU
+        C0 = init_plusplus(X, k, desc.float_type, ctx=ctx)
     if dev:
         import torch
         C = torch.empty_like(C0)

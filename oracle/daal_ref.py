@@ -47,6 +47,8 @@ def _load():
             getattr(_lib, f"daalref_train_{sfx}").argtypes = [P, I64, I64, P, I64, I64, D, P, P, P, P, P]
             getattr(_lib, f"daalref_infer_{sfx}").argtypes = [P, I64, I64, P, I64, ctypes.c_int, P, P, P]
         _lib.daalref_set_threads.argtypes = [ctypes.c_int]
+        for sfx in ("f64", "f32"):
+            getattr(_lib, f"daalref_init_plusplus_{sfx}").argtypes = [P, I64, I64, I64, ctypes.c_uint32, P]
     return _lib
 
 
@@ -96,3 +98,18 @@ def infer(X, C, compute_objective=True):
     if rc != 0:
         raise ReferenceError_(int(code[0]))
     return lab, (float(obj[0]) if compute_objective else None)
+
+
+def init_plusplus(X, k, seed=777777):
+    """The reference's KMeansInitKernel<plusPlusDense, F, avx2> with one trial and an
+    mt19937 engine seeded with `seed`, as oneDAL's train() uses it without initial
+    centroids (cpp/oneapi/dal/algo/kmeans/detail/train_init_centroids.hpp:47-74)."""
+    X = np.ascontiguousarray(X)
+    lib = _load()
+    n, d = X.shape
+    C = np.empty((k, d), X.dtype)
+    sfx = "f64" if X.dtype == np.float64 else "f32"
+    rc = getattr(lib, f"daalref_init_plusplus_{sfx}")(_p(X), n, d, int(k), int(seed), _p(C))
+    if rc != 0:
+        raise ReferenceError_(rc)
+    return C

@@ -1,0 +1,112 @@
+/*
+ * ORACLE -- test infrastructure only (tests/, the smoke check and bench.py's
+ * CPU-baseline leg use it; the product never does). CPU restatement of DAAL's
+ * dense k-means++ initialisation with one trial, the path oneDAL's train()
+ * takes without initial centroids
+ * (cpp/oneapi/dal/algo/kmeans/detail/train_init_centroids.hpp:47-74):
+ *
+ *   engine         std::mt19937 seeded with 777777, uniform draws from
+ *                  std::uniform_real_distribution<F>(0, 1) -- the reference's
+ *                  own RNG backend (cpp/daal/src/externals/service_rng_ref.h:
+ *                  109-117, 190-199) and default seed
+ *                  (cpp/daal/src/algorithms/kmeans/kmeans_init_parameter_types.cpp:41-48)
+ *   probabilities  k draws up front (kmeans_plusplus_init_impl.i:551, 403-407)
+ *   first center   row = size_t(p0 * F(n)), n - 1 on round-off (:573-585)
+ *   min distances  per 512-row block: d2 = sum_i (x_i - c_i)^2 in F in
+ *                  coordinate order (contracted to an FMA as the avx2 build
+ *                  does), min(best, d2) keeping best on ties, block sum in
+ *                  row order, overall = block sums in block order (:215-246, 637-656)
+ *   next centers   sample = overall * p; walk block sums, then the block's rows,
+ *                  subtracting while sample >= value (:588-611); a row whose
+ *                  distance is <= eps = 0.1 * overall / n is resampled with a
+ *                  fresh draw, the chosen row's distance is zeroed (:613-635);
+ *                  no update after the last center (:669-673).
+ *   no candidate   when the overall distance is zero (fewer than k distinct rows)
+ *                  or not finite, no draw can succeed and the reference's loop
+ *                  never ends; this restatement returns 4 instead.
+ */
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <random>
+#include <vector>
+
+namespace {
+
+template <typename F>
+int init_plusplus(const F *X, int64_t n, int64_t d, int64_t k, uint32_t seed, int fused, F *C, int64_t *rows_out) {
+    if (!X || !C || n <= 0 || d <= 0 || k <= 0 || k > n) return 2;
+    std::mt19937 gen(seed);
+    std::uniform_real_distribution<F> uni(F(0), F(1));
+    std::vector<F> prob((size_t)k);
+    for (int64_t i = 0; i < k; ++i) prob[(size_t)i] = uni(gen);
+    const int64_t B = 512, nb = (n + B - 1) / B;
+    std::vector<F> md((size_t)n, std::numeric_limits<F>::max()), acc((size_t)nb);
+    F overall = F(0);
+    auto update = [&](const F *c) {
+        for (int64_t b = 0; b < nb; ++b) {
+            const int64_t r0 = b * B, r1 = std::min(n, r0 + B);
+            F sum = F(0);
+            for (int64_t r = r0; r < r1; ++r) {
+                const F *x = X + r * d;
+                F d2 = F(0);
+                for (int64_t i = 0; i < d; ++i) {
+                    const F t = x[i] - c[i];
+                    d2 = fused ? std::fma(t, t, d2) : d2 + t * t;
+                }
+                md[(size_t)r] = !(d2 < md[(size_t)r]) ? md[(size_t)r] : d2;
+                sum += md[(size_t)r];
+            }
+            acc[(size_t)b] = sum;
+        }
+        overall = acc[0];
+        for (int64_t b = 1; b < nb; ++b) overall += acc[(size_t)b];
+    };
+    auto find = [&](F sample) -> int64_t {
+        int64_t b = 0;
+        for (; b + 1 < nb && sample >= acc[(size_t)b]; ++b) sample -= acc[(size_t)b];
+        const int64_t r0 = b * B, cnt = (b == nb - 1) ? n - r0 : B;
+        int64_t r = 0;
+        for (; r + 1 < cnt && sample >= md[(size_t)(r0 + r)]; ++r) sample -= md[(size_t)(r0 + r)];
+        return r0 + r;
+    };
+    int64_t row = (int64_t)(size_t)(prob[0] * F(n));
+    if (row == n) --row;
+    std::memcpy(C, X + row * d, sizeof(F) * (size_t)d);
+    if (rows_out) rows_out[0] = row;
+    update(C);
+    for (int64_t c = 1; c < k; ++c) {
+        F p = prob[(size_t)c];
+        if (!(overall > F(0)) || !(overall <= std::numeric_limits<F>::max())) return 4;
+        const F eps = F(0.1) * overall / F(n);
+        int64_t tries = 0;
+        for (;;) {
+            row = find(overall * p);
+            if (md[(size_t)row] > eps) {
+                md[(size_t)row] = F(0);
+                break;
+            }
+            if (++tries > 10000000) return 3;  // the reference would retry forever
+            p = uni(gen);
+        }
+        std::memcpy(C + c * d, X + row * d, sizeof(F) * (size_t)d);
+        if (rows_out) rows_out[c] = row;
+        if (c == k - 1) break;
+        update(C + c * d);
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+int kmo_init_plusplus_f64(const double *X, int64_t n, int64_t d, int64_t k, uint32_t seed, int fused, double *C,
+                          int64_t *rows) {
+    return init_plusplus<double>(X, n, d, k, seed, fused, C, rows);
+}
+int kmo_init_plusplus_f32(const float *X, int64_t n, int64_t d, int64_t k, uint32_t seed, int fused, float *C,
+                          int64_t *rows) {
+    return init_plusplus<float>(X, n, d, k, seed, fused, C, rows);
+}
+}

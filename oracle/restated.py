@@ -22,6 +22,10 @@ class OracleError(RuntimeError):
     pass
 
 
+class NoCandidateRows(OracleError):
+    """k-means++ found no row with a positive distance to the chosen centers."""
+
+
 class TooManyEmptyClusters(OracleError):
     """DAAL's ErrorKMeansNumberOfClustersIsTooLarge (kmeans_lloyd_batch_impl.i:171)."""
 
@@ -43,6 +47,8 @@ def _load():
         _lib.kmo_objective_f64.restype = ctypes.c_double
         _lib.kmo_objective_f32.restype = ctypes.c_float
         _lib.kmo_assign_f32_in_f64.argtypes = [P, I64, I64, P, I64, P, P, P]
+        for sfx in ("f64", "f32"):
+            getattr(_lib, f"kmo_init_plusplus_{sfx}").argtypes = [P, I64, I64, I64, ctypes.c_uint32, ctypes.c_int, P, P]
     return _lib
 
 
@@ -146,3 +152,20 @@ def objective(X, C, labels):
     labels = np.ascontiguousarray(labels, dtype=np.int32)
     n, d = X.shape
     return float(getattr(lib, f"kmo_objective_{_sfx(X.dtype)}")(_p(X), n, d, _p(C), C.shape[0], _p(labels)))
+
+
+def init_plusplus(X, k, seed=777777, fused=True):
+    """DAAL's dense k-means++ initialisation with one trial (kmeans_init_oracle.cpp).
+    `fused` computes the squared distances with fused multiply-adds (as the reference's
+    vectorised loop and the CUDA kernel do); False rounds every product.
+    Returns (centroids k x d, chosen row indices)."""
+    X = np.ascontiguousarray(X)
+    lib = _load()
+    n, d = X.shape
+    C = np.empty((k, d), X.dtype)
+    rows = np.empty(k, np.int64)
+    rc = getattr(lib, f"kmo_init_plusplus_{_sfx(X.dtype)}")(_p(X), n, d, int(k), int(seed), int(bool(fused)), _p(C), _p(rows))
+    if rc == 4:
+        raise NoCandidateRows("fewer than k distinct rows (no row left to sample)")
+    _check(rc)
+    return C, rows

@@ -24,6 +24,11 @@ Sources (paths inside the reference project):
   Gaussian-blob workload shaped like the plain CPU configuration (d=20, k=20,
   init = first k rows, eps 0), float64 and float32, so the restated oracle can
   be re-checked where the reference tree is absent.
+* daal_ref_plusplus.npz -- the centers chosen by the reference's dense k-means++
+  initialisation (DAAL KMeansInitKernel<plusPlusDense>, one trial, mt19937 seeded
+  777777: the default of cpp/oneapi/dal/algo/kmeans/detail/train_init_centroids.hpp)
+  built from source, float64 and float32, on the seeded inputs of plusplus_cases()
+  and on the example data with k=20.
 """
 import argparse
 import json
@@ -109,6 +114,26 @@ def blobs_c1(n, seed):
     return centres[lab] + rng.standard_normal((n, d))
 
 
+def plusplus_cases():
+    """Seeded inputs of the k-means++ fixtures: (name, X float64, k). Rounded data has
+    many duplicate rows, which exercises the reference's resampling."""
+    out = []
+    for name, n, d, k, seed, kind in (("normal_5k", 5000, 7, 16, 2001, "normal"),
+                                      ("blobs_20k", 20000, 20, 20, 2002, "blobs"),
+                                      ("ragged_3001", 3001, 33, 100, 2003, "normal"),
+                                      ("wide_1500", 1500, 64, 300, 2004, "normal"),
+                                      ("dups_4096", 4096, 3, 50, 2005, "rounded")):
+        rng = np.random.default_rng(seed)
+        if kind == "blobs":
+            X = blobs_c1(n, seed)
+        else:
+            X = 3.0 * rng.standard_normal((n, d))
+            if kind == "rounded":
+                X = np.round(X)
+        out.append((name, X, k))
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -138,6 +163,15 @@ def main():
         C, lab, obj, it = daal_ref.train(Xd, Xd[:20].copy(), 50, 0.0)
         out.update({f"C_{tag}": C, f"labels_{tag}": lab.astype(np.uint8), f"obj_{tag}": obj, f"iters_{tag}": it})
     np.savez_compressed(os.path.join(HERE, "daal_ref_c1.npz"), **out)
+
+    # k-means++ (train() without initial centroids): the reference's chosen centers
+    out = {}
+    cases = plusplus_cases() + [("example", np.loadtxt(os.path.join(ref, "data/kmeans_dense_train_data.csv"),
+                                                       delimiter=",", dtype=np.float64), 20)]
+    for name, X, k in cases:
+        for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+            out[f"C_{name}_{tag}"] = daal_ref.init_plusplus(X.astype(dt), k)
+    np.savez_compressed(os.path.join(HERE, "daal_ref_plusplus.npz"), **out)
     print("golden fixtures written to", HERE)
 
 

@@ -2,7 +2,9 @@
 headers and runtime sources (integration/Makefile), whose host-policy k-means
 dispatchers are integration/kmeans_dispatcher_b200.cpp. On a GPU it must
 reproduce the reference's gold known-answer case (cpp/oneapi/dal/algo/kmeans/
-test/fixture.hpp:156-203 with test/data.hpp) through dal::train / dal::infer;
+test/fixture.hpp:156-203 with test/data.hpp) through dal::train / dal::infer,
+and its smoke case (fixture.hpp:221-252) through train() without initial
+centroids (the default k-means++ init);
 without a GPU the dispatcher must surface the library's failure as a oneDAL
 exception. The client is built only where the reference tree is present; the
 built binary travels with the tree."""
@@ -76,3 +78,7 @@ def test_client_gold_through_dal_train_infer(tmp_path, dtype, rtol):
     assert rel_close(float(out["objective"]), g["expected_objective"], rtol)
     assert rel_close(float(out["infer_objective"]), g["expected_objective"], rtol)
     assert out.get("invalid_argument") == "ok"
+    # fixture.hpp:221-252 without initial centroids: compared WITHOUT a match map
+    sc = np.array(out["smoke_centroids"].split(), np.float64).reshape(2, 2)
+    assert centroid_rel_err(np.array([[-1.5, -1.5], [1.5, 1.5]]), sc) < rtol
+    assert out["smoke_responses"].split() == ["1", "1", "1", "1", "0", "0", "0", "0"]

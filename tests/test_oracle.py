@@ -137,3 +137,76 @@ def test_planted_label_flip_is_detected():
     Cb = C.copy()
     Cb[1, 2] *= 1 + 1e-5
     assert centroid_rel_err(C, Cb) > 1e-7
+
+
+def _plusplus_inputs():
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import plusplus_cases
+    from helpers import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "example_dense.npz"))
+    return plusplus_cases() + [("example", z["X"], 20)]
+
+
+@pytest.mark.parametrize("tag,dt", [("f64", np.float64), ("f32", np.float32)])
+def test_plusplus_matches_reference_fixtures(tag, dt):
+    """The restated k-means++ picks exactly the reference's centers (bit-identical rows of
+    X), duplicate-heavy data included, in both precisions."""
+    import os
+    from helpers import GOLDEN
+    z = np.load(os.path.join(GOLDEN, "daal_ref_plusplus.npz"))
+    for name, X, k in _plusplus_inputs():
+        X = X.astype(dt)
+        C, rows = restated.init_plusplus(X, k)
+        assert C.dtype == dt
+        assert np.array_equal(C, z[f"C_{name}_{tag}"]), name
+        assert np.array_equal(C, X[rows]), name
+        assert (rows >= 0).all() and (rows < len(X)).all()
+
+
+def test_plusplus_fused_and_unfused_distance_agree_on_fixtures():
+    """The oracle's distance loop with and without FMA contraction picks the same rows on
+    the fixture data (the reference build is compiled with contraction)."""
+    for name, X, k in _plusplus_inputs()[:3]:
+        a = restated.init_plusplus(X, k)[1]
+        b = restated.init_plusplus(X, k, fused=False)[1]
+        assert (a == b).all(), name
+
+
+@needs_ref
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("n,d,k,seed", [(1, 1, 1, 0), (7, 2, 7, 1), (513, 5, 40, 2), (1025, 9, 3, 3), (2000, 1, 3, 4),
+                                         (3000, 2, 9, 5)])
+def test_plusplus_restated_equals_reference_live(dt, n, d, k, seed):
+    """Live comparison with the reference build on ragged shapes: n not a multiple of the
+    512-row block, k == n, d == 1, and tiny integer grids with exactly k distinct rows
+    (many duplicates, so the reference resamples candidates within its epsilon)."""
+    rng = np.random.default_rng(seed)
+    X = rng.integers(0, 3, (n, d)).astype(dt) if seed >= 4 else rng.standard_normal((n, d)).astype(dt)
+    for s in (777777, 12345):
+        assert np.array_equal(restated.init_plusplus(X, k, s)[0], daal_ref.init_plusplus(X, k, s))
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+def test_plusplus_fewer_distinct_rows_than_k_is_an_error(dt):
+    """With fewer than k distinct rows every distance becomes zero and the reference's
+    resampling loop (kmeans_plusplus_init_impl.i:613-635) never ends; the restatement
+    reports it instead (the reference build is not run on this input)."""
+    X = np.repeat(np.arange(3, dtype=dt)[:, None], 100, axis=0)
+    assert len(restated.init_plusplus(X, 3)[1]) == 3
+    with pytest.raises(restated.NoCandidateRows):
+        restated.init_plusplus(X, 4)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+def test_plusplus_smoke_known_answer(dt):
+    """fixture.hpp:221-252 trains the 8-point smoke data without initial centroids and
+    compares centroids and responses without a centroid match: the k-means++ rows picked
+    with seed 777777 fix the order (-1.5, -1.5), (1.5, 1.5) and responses 1,1,1,1,0,0,0,0."""
+    X = np.array([1, 1, 2, 2, 1, 2, 2, 1, -1, -1, -1, -2, -2, -1, -2, -2], dt).reshape(8, 2)
+    C0, rows = restated.init_plusplus(X, 2)
+    C, lab, obj, it = restated.train(X, C0, 4, 0.001)
+    assert centroid_rel_err(np.array([[-1.5, -1.5], [1.5, 1.5]]), C) < 5 * np.finfo(dt).eps * it * 100
+    assert lab.tolist() == [1, 1, 1, 1, 0, 0, 0, 0]
+    assert rel_close(obj, 4.0, 1e-6)
