@@ -13,9 +13,15 @@
  *   probabilities  k draws up front (kmeans_plusplus_init_impl.i:551, 403-407)
  *   first center   row = size_t(p0 * F(n)), n - 1 on round-off (:573-585)
  *   min distances  per 512-row block: d2 = sum_i (x_i - c_i)^2 in F in
- *                  coordinate order (contracted to an FMA as the avx2 build
- *                  does), min(best, d2) keeping best on ties, block sum in
- *                  row order, overall = block sums in block order (:215-246, 637-656)
+ *                  coordinate order, each step an FMA, min(best, d2) keeping
+ *                  best on ties, block sum in row order, overall = block sums
+ *                  in block order (:191-216, 637-656). The reference marks the
+ *                  d2 loop `omp simd reduction(+)` (:201), so its own order is
+ *                  the compiler's vector-lane split; that changes d2 by a few
+ *                  ulps and the chosen row only when a sample lands within
+ *                  rounding of a boundary. The reference built with its GNU
+ *                  flags (-fopenmp-simd, avx2) picks the same rows as this
+ *                  restatement on every recorded fixture.
  *   next centers   sample = overall * p; walk block sums, then the block's rows,
  *                  subtracting while sample >= value (:588-611); a row whose
  *                  distance is <= eps = 0.1 * overall / n is resampled with a

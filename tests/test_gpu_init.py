@@ -40,10 +40,12 @@ def test_plusplus_matches_reference_fixtures(tag, dt):
 
 @pytest.mark.parametrize("dt", DTYPES)
 @pytest.mark.parametrize("n,d,k,seed", [(1, 1, 1, 1), (511, 3, 511, 2), (513, 17, 40, 3), (5000, 130, 257, 4),
-                                         (70001, 9, 64, 5), (300000, 32, 16, 6)])
+                                         (70001, 9, 64, 5), (300000, 32, 16, 6), (300007, 40, 8, 7),
+                                         (2500001, 4, 12, 8)])
 def test_plusplus_matches_oracle(dt, n, d, k, seed):
-    """Ragged block counts (n around the 512-row block), k == n, d above one tile of
-    the distance kernel, and a few hundred thousand rows."""
+    """Ragged block counts (n around the 512-row block), k == n, rows narrower and wider
+    than one 128-byte segment of the distance kernel, and 2.5M rows (more block sums than
+    one shared-memory chunk of the selection kernel holds)."""
     rng = np.random.default_rng(seed)
     X = (rng.standard_normal((n, d)) * rng.uniform(0.1, 4.0, d)).astype(dt)
     for s in (777777, seed):
