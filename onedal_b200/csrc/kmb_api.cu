@@ -104,7 +104,7 @@ void Workspace::release() {
     DevBuf *all[] = {&X, &C0, &Cout, &labels, &d2, &xnorm, &Ccur, &Cnew, &Ct, &h, &queue, &H, &Gs,
                      &counts, &offsets, &piece_base, &perm, &records, &shift_part, &empty_flag, &empty_ids,
                      &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx, &rowb, &pp_acc, &pp_rand,
-                     &pp_state};
+                     &pp_state, &pp_flags};
     for (DevBuf *b : all) {
         if (b->ptr) cudaFreeAsync(b->ptr, stream);
         b->ptr = nullptr;
@@ -564,6 +564,7 @@ int init_plusplus_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, 
     const int64_t nb = (n + 511) / 512;
     bool ok = ws.ensure(ws.d2, sizeof(F) * n) && ws.ensure(ws.pp_acc, sizeof(F) * nb) &&
               ws.ensure(ws.pp_rand, sizeof(F) * (k + pool_n)) && ws.ensure(ws.pp_state, sizeof(kmb::PPState)) &&
+              ws.ensure(ws.pp_flags, sizeof(unsigned) * nb) &&
               ws.ensure(ws.Cout, sizeof(F) * k * d);
     if (!ok) return fail(ctx, KMB_ENOMEM, "device allocation failed (k-means++ init, n=%lld)", (long long)n);
     F *md = (F *)ws.d2.ptr, *acc = (F *)ws.pp_acc.ptr, *rnd = (F *)ws.pp_rand.ptr;
@@ -578,6 +579,8 @@ int init_plusplus_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, 
     KMB_CUDA(cudaMemcpyAsync(rnd, host.data(), sizeof(F) * (k + pool_n), cudaMemcpyHostToDevice, s));
     kmb::PPState hs{};
     KMB_CUDA(cudaMemcpyAsync(st, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+    // block-sum publication flags: round c publishes c, so zero means "none yet"
+    KMB_CUDA(cudaMemsetAsync(ws.pp_flags.ptr, 0, sizeof(unsigned) * nb, s));
     int64_t row0 = (int64_t)(size_t)(host[0] * F(n));
     if (row0 == n) --row0;
     kmb::launch_pp_fill<F>(md, n, s);
@@ -586,10 +589,14 @@ int init_plusplus_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, 
     bool update_first = true;
     int64_t round_draws = 0;  // resample draws spent on the round that stopped
     for (;;) {
-        kmb::launch_pp_rounds<F>(X, n, d, k, c_begin, update_first, md, acc, rnd, rnd + k, pool_n, C, st, s);
+        kmb::launch_pp_rounds<F>(X, n, d, k, c_begin, update_first, md, acc, (unsigned *)ws.pp_flags.ptr, rnd,
+                                 rnd + k, pool_n, C, st, s);
         KMB_CUDA(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
         KMB_CUDA(cudaStreamSynchronize(s));
         if (!hs.stopped) break;
+        if (hs.stopped == 3)
+            return fail(ctx, KMB_ETIMEDOUT, "k-means++ init: overall-sum fold timed out in round %lld",
+                        (long long)hs.stop_round);
         if (hs.stopped == 2)
             return fail(ctx, KMB_EINVAL,
                         "k-means++ init: no row left to sample for center %lld (fewer than k distinct rows, or "

@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <type_traits>
 
 namespace kmb {
 namespace {
@@ -43,101 +44,394 @@ __global__ void pp_fill_kernel(F *__restrict__ md, int64_t n) {
         md[i] = f_max<F>();
 }
 
-// One CTA per 512-row block, 16 warps x 32 rows, each lane owning one row's
-// distance. Rows are staged through shared memory one 128-byte segment per row
-// at a time (W columns; a warp load instruction covers 32/W rows, fully
-// coalesced), and the next segment's loads are in flight while the current one
-// is folded, so each warp keeps 4 KB of loads outstanding. Each lane folds its
-// row's columns in coordinate order; thread 0 then sums the block's minima in
-// row order. Rows narrower than one segment are read directly (the warp's 32
-// rows are one contiguous range, so the lanes' reads share cache lines).
+constexpr int kUpdWarps = 4;  // warps per CTA of the distance update
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ unsigned load_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void store_release(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// A block's sum is published: acc[b] first, then flags[b] = epoch (release).
 template <typename F>
-__global__ void __launch_bounds__(kPPBlock, 2) pp_update_kernel(const F *__restrict__ X, int64_t n, int d,
-                                                                const F *__restrict__ center, F *__restrict__ md,
-                                                                F *__restrict__ acc, const PPState *st) {
+__device__ __forceinline__ void publish_block_sum(F *acc, unsigned *flags, int64_t b, F sum, unsigned epoch) {
+    acc[b] = sum;
+    store_release(flags + b, epoch);
+}
+
+// The overall sum acc[0] + acc[1] + ... in block order, folded by the update
+// grid's leading CTA while the other CTAs still produce block sums: each lane
+// waits for eight consecutive blocks' flags (acquire loads issued together),
+// reads their sums past L1, and every lane folds the 256 values in order
+// through shuffles. Blocks are produced in
+// roughly increasing order, so the fold trails the update by about one wave of
+// warps and the round's sequential part shrinks to the sampling walk. Producers
+// never wait, so the wait always ends; it is still bounded (10 s), after which
+// the round is marked timed out. Result: st->overall.
+template <typename F>
+__device__ void fold_overall(const F *acc, const unsigned *flags, int64_t nb, unsigned epoch, PPState *st) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long deadline = global_ns() + 10000000000ull;
+    F overall = F(0);
+    bool ok = true;
+    constexpr int PER = 8;  // blocks per lane per batch
+    for (int64_t b0 = 0; b0 < nb && ok; b0 += 32 * PER) {
+        const int64_t mine = b0 + lane * PER;  // this lane's first block
+        const int have = (int)max((int64_t)0, min((int64_t)PER, nb - mine));
+        for (;;) {  // wait until all of this lane's flags carry the epoch
+            bool ready = true;
+#pragma unroll
+            for (int i = 0; i < PER; ++i)
+                if (i < have && load_acquire(flags + mine + i) != epoch) ready = false;
+            if (ready) break;
+            if (global_ns() > deadline) {
+                ok = false;
+                break;
+            }
+            __nanosleep(200);
+        }
+        F v[PER];
+#pragma unroll
+        for (int i = 0; i < PER; ++i) v[i] = (ok && i < have) ? __ldcg(acc + mine + i) : F(0);
+        ok = __all_sync(0xffffffffu, ok);
+        const int64_t cnt = min((int64_t)32 * PER, nb - b0);
+#pragma unroll 2
+        for (int src = 0; src < 32; ++src) {
+#pragma unroll
+            for (int i = 0; i < PER; ++i) {
+                const F x = __shfl_sync(0xffffffffu, v[i], src);
+                if (src * PER + i < cnt) overall += x;
+            }
+        }
+    }
+    if (lane == 0) {
+        if (ok) {
+            st->overall = (double)overall;
+        } else {
+            st->stopped = 3;
+            st->stop_round = (long long)epoch;
+        }
+    }
+}
+
+// One warp per 512-row block: the block's rows go 32 at a time (a group), one
+// row per lane. A group's rows are staged through shared memory one 128-byte
+// segment per row at a time (W columns; one warp load instruction covers 32/W
+// rows, fully coalesced), and the next segment's loads are in flight while the
+// current one is folded (4 KB outstanding per warp). Each lane folds its row's
+// columns in coordinate order, reading the row and the center 16 bytes at a
+// time (row pitch W + 16/sizeof(F): conflict-free for 16-byte reads). After
+// the last group, lane 0 sums the block's 512 new minima in row order. Rows
+// narrower than one segment are read directly (the group's 32 rows are one
+// contiguous range, so the lanes' reads share cache lines). Warps never wait
+// for one another.
+template <typename F>
+__global__ void __launch_bounds__(kUpdWarps * 32, 8)
+    pp_update_kernel(const F *__restrict__ X, int64_t n, int d, int64_t nb, const F *__restrict__ center,
+                     F *__restrict__ md, F *__restrict__ acc, unsigned *__restrict__ flags, unsigned epoch,
+                     PPState *st) {
     constexpr int W = 128 / (int)sizeof(F);  // columns per segment
+    constexpr int V = 16 / (int)sizeof(F);   // elements per 16-byte read
+    constexpr int P = W + V;                 // tile row pitch
     constexpr int RPI = 32 / W;              // rows per warp load instruction
-    constexpr int NLD = 32 / RPI;            // load instructions per 32-row segment
+    constexpr int NLD = 32 / RPI;            // load instructions per segment
+    using Vec = typename std::conditional<sizeof(F) == 4, float4, double2>::type;
+    __shared__ __align__(16) F tile[kUpdWarps][32][P];
+    __shared__ __align__(16) F cseg[kUpdWarps][W];
+    __shared__ __align__(16) F s_md[kUpdWarps][kPPBlock];
     if (st->stopped) return;
-    extern __shared__ __align__(16) unsigned char pp_smem[];
-    F(*tile)[32][W + 1] = reinterpret_cast<F(*)[32][W + 1]>(pp_smem);  // [16 warps][32 rows][W + pad]
-    F *s_md = reinterpret_cast<F *>(pp_smem) + 16 * 32 * (W + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t r0 = (int64_t)blockIdx.x * kPPBlock + warp * 32;
-    const int64_t row = r0 + lane;
-    F d2 = F(0);
+    if (blockIdx.x == 0) {  // the leading CTA folds the overall sum
+        if (warp == 0) fold_overall(acc, flags, nb, epoch, st);
+        return;
+    }
+    const int64_t b = (int64_t)(blockIdx.x - 1) * kUpdWarps + warp;
+    if (b >= nb) return;  // warp-uniform; no CTA-wide barrier below
+    const int64_t base = b * kPPBlock;
+    const int cnt = (int)min((int64_t)kPPBlock, n - base);
+    const int ngroups = (cnt + 31) / 32;
     if (d < W) {
-        if (row < n) {
-            const F *x = X + row * d;
-            for (int i = 0; i < d; ++i) {
-                const F t = x[i] - center[i];
-                d2 = fma(t, t, d2);
+        for (int g = 0; g < ngroups; ++g) {
+            const int r = g * 32 + lane;
+            if (r < cnt) {
+                const F *x = X + (base + r) * d;
+                F d2 = F(0);
+                for (int i = 0; i < d; ++i) {
+                    const F t = x[i] - center[i];
+                    d2 = fma(t, t, d2);
+                }
+                const F old = md[base + r];
+                const F m = !(d2 < old) ? old : d2;  // the reference's min(best, d2)
+                md[base + r] = m;
+                s_md[warp][r] = m;
             }
         }
     } else {
         const int sub = lane / W, col = lane % W;
+        const int nseg = (d + W - 1) / W;
         F v[NLD];
-        auto load_segment = [&](int c0) {
+        auto load_segment = [&](int g, int c0) {
             const int c = c0 + col;
 #pragma unroll
             for (int j = 0; j < NLD; ++j) {
-                const int64_t r = r0 + j * RPI + sub;
-                v[j] = (r < n && c < d) ? X[r * d + c] : F(0);
+                const int r = g * 32 + j * RPI + sub;
+                v[j] = (r < cnt && c < d) ? X[(base + r) * d + c] : F(0);
             }
         };
-        load_segment(0);
-        for (int c0 = 0; c0 < d; c0 += W) {
+        load_segment(0, 0);
+        F d2 = F(0), old = F(0);
+        int g = 0, sg = 0;
+        for (;;) {
+            const int c0 = sg * W;
+            if (sg == 0 && g * 32 + lane < cnt) old = md[base + g * 32 + lane];
 #pragma unroll
             for (int j = 0; j < NLD; ++j) tile[warp][j * RPI + sub][col] = v[j];
+            if (sub == 0) cseg[warp][col] = c0 + col < d ? center[c0 + col] : F(0);
             __syncwarp();
-            if (c0 + W < d) load_segment(c0 + W);
-            const F cv = c0 + col < d ? center[c0 + col] : F(0);
-            const int cols = min(W, d - c0);
-            for (int i = 0; i < cols; ++i) {
-                const F t = tile[warp][lane][i] - __shfl_sync(0xffffffffu, cv, i);
-                d2 = fma(t, t, d2);
+            // next segment (of this group, else the next group's first)
+            int ng = g, nsg = sg + 1;
+            if (nsg == nseg) {
+                nsg = 0;
+                ++ng;
+            }
+            if (ng < ngroups) load_segment(ng, nsg * W);
+            const F *xr = &tile[warp][lane][0];
+            const F *cr = &cseg[warp][0];
+            if (c0 + W <= d) {
+#pragma unroll
+                for (int i = 0; i < W; i += V) {
+                    const Vec xv = *reinterpret_cast<const Vec *>(xr + i);
+                    const Vec cv = *reinterpret_cast<const Vec *>(cr + i);
+                    const F *xe = reinterpret_cast<const F *>(&xv), *ce = reinterpret_cast<const F *>(&cv);
+#pragma unroll
+                    for (int u = 0; u < V; ++u) {
+                        const F t = xe[u] - ce[u];
+                        d2 = fma(t, t, d2);
+                    }
+                }
+            } else {
+                for (int i = 0; i < d - c0; ++i) {
+                    const F t = xr[i] - cr[i];
+                    d2 = fma(t, t, d2);
+                }
             }
             __syncwarp();
+            if (nsg == 0) {  // the group's rows are complete
+                const int r = g * 32 + lane;
+                if (r < cnt) {
+                    const F m = !(d2 < old) ? old : d2;  // the reference's min(best, d2)
+                    md[base + r] = m;
+                    s_md[warp][r] = m;
+                }
+                d2 = F(0);
+            }
+            if (ng >= ngroups) break;
+            g = ng;
+            sg = nsg;
         }
     }
-    F m = F(0);
-    if (row < n) {
-        const F old = md[row];
-        m = !(d2 < old) ? old : d2;  // the reference's min(best, d2)
-        md[row] = m;
-    }
-    s_md[threadIdx.x] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int64_t b0 = (int64_t)blockIdx.x * kPPBlock;
-        const int cnt = (int)((n - b0) < (int64_t)kPPBlock ? (n - b0) : (int64_t)kPPBlock);
+    __syncwarp();
+    if (lane == 0) {
+        const F *m = s_md[warp];
         F sum = F(0);
-        for (int i = 0; i < cnt; ++i) sum += s_md[i];
-        acc[blockIdx.x] = sum;
+        int i = 0;
+        for (; i + V <= cnt; i += V) {
+            const Vec x = *reinterpret_cast<const Vec *>(m + i);
+            const F *e = reinterpret_cast<const F *>(&x);
+#pragma unroll
+            for (int u = 0; u < V; ++u) sum += e[u];
+        }
+        for (; i < cnt; ++i) sum += m[i];
+        publish_block_sum(acc, flags, b, sum, epoch);
     }
 }
 
-constexpr int kSelThreads = 1024;
+// 16-byte global -> shared copies that bypass registers (zero-filled past
+// `src_bytes`), grouped per pipeline stage.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+constexpr int kAsyncStages = 4;
+
+template <typename F>
+__host__ __device__ constexpr int async_warp_smem() {  // bytes per warp: stages of (32 row segments + center segment) + minima
+    return kAsyncStages * (32 * (128 + 16) + 128) + kPPBlock * (int)sizeof(F);
+}
+
+// The distance update for rows of 16-byte multiple length at a 16-byte aligned
+// base: the same one-warp-per-block fold as pp_update_kernel, but each 4 KB
+// group segment (32 row pieces of 128 bytes, plus the center's piece) goes
+// global -> shared with cp.async in a 4-stage ring per warp, so three segments
+// stay in flight while one is folded, no registers hold loads and a lane issues
+// eight 16-byte copies per segment. Columns past d and rows past the block are
+// zero-filled; they add (0 - 0)^2 = +0 to a non-negative sum, which leaves it
+// unchanged, so every segment is folded whole.
+template <typename F>
+__global__ void __launch_bounds__(kUpdWarps * 32)
+    pp_update_async_kernel(const F *__restrict__ X, int64_t n, int d, int64_t nb, const F *__restrict__ center,
+                           F *__restrict__ md, F *__restrict__ acc, unsigned *__restrict__ flags, unsigned epoch,
+                           PPState *st) {
+    constexpr int W = 128 / (int)sizeof(F);  // columns per segment
+    constexpr int V = 16 / (int)sizeof(F);   // columns per 16-byte piece
+    constexpr int P = W + V;                 // tile row pitch (144 bytes)
+    using Vec = typename std::conditional<sizeof(F) == 4, float4, double2>::type;
+    extern __shared__ __align__(16) unsigned char pp_async_smem[];
+    if (st->stopped) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (blockIdx.x == 0) {  // the leading CTA folds the overall sum
+        if (warp == 0) fold_overall(acc, flags, nb, epoch, st);
+        return;
+    }
+    const int64_t b = (int64_t)(blockIdx.x - 1) * kUpdWarps + warp;
+    if (b >= nb) return;  // warp-uniform; no CTA-wide barrier below
+    unsigned char *ws = pp_async_smem + (size_t)warp * async_warp_smem<F>();
+    F(*tile)[32][P] = reinterpret_cast<F(*)[32][P]>(ws);                            // [stage][row][P]
+    F(*cst)[W] = reinterpret_cast<F(*)[W]>(ws + kAsyncStages * 32 * P * sizeof(F));  // [stage][W]
+    F *s_md = reinterpret_cast<F *>(ws + kAsyncStages * (32 * P + W) * sizeof(F));
+    const int64_t base = b * kPPBlock;
+    const int cnt = (int)min((int64_t)kPPBlock, n - base);
+    const int ngroups = (cnt + 31) / 32;
+    const int nseg = (d + W - 1) / W;
+    const int total = ngroups * nseg;
+    // this lane's copies: piece q of rows (lane >> 3) + 4 k, k = 0..7
+    const int q = lane & 7, rl = lane >> 3;
+    const F *src0 = X + (base + rl) * (int64_t)d + q * V;
+    int ig = 0, isg = 0;  // next (group, segment) to issue
+    auto issue = [&](int stage) {
+        const int c = isg * W + q * V;
+        const bool col_ok = c < d;
+        const F *p = src0 + (int64_t)ig * 32 * d + isg * W;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int r = ig * 32 + rl + 4 * k;
+            const bool ok = col_ok && r < cnt;
+            cp_async16(&tile[stage][rl + 4 * k][q * V], ok ? (const void *)(p + (int64_t)4 * k * d) : (const void *)X,
+                       ok ? 16 : 0);
+        }
+        if (lane < 8) cp_async16(&cst[stage][q * V], col_ok ? (const void *)(center + c) : (const void *)center,
+                                 col_ok ? 16 : 0);
+        if (++isg == nseg) {
+            isg = 0;
+            ++ig;
+        }
+    };
+#pragma unroll
+    for (int t = 0; t < kAsyncStages - 1; ++t) {
+        if (t < total) issue(t);
+        cp_async_commit();
+    }
+    F d2 = F(0), old = F(0);
+    int g = 0, sg = 0;
+    for (int t = 0; t < total; ++t) {
+        if (t + kAsyncStages - 1 < total) issue((t + kAsyncStages - 1) % kAsyncStages);
+        cp_async_commit();
+        if (sg == 0 && g * 32 + lane < cnt) old = md[base + g * 32 + lane];
+        cp_async_wait<kAsyncStages - 1>();
+        __syncwarp();
+        const int stage = t % kAsyncStages;
+        const F *xr = &tile[stage][lane][0];
+        const F *cr = &cst[stage][0];
+#pragma unroll
+        for (int i = 0; i < W; i += V) {
+            const Vec xv = *reinterpret_cast<const Vec *>(xr + i);
+            const Vec cv = *reinterpret_cast<const Vec *>(cr + i);
+            const F *xe = reinterpret_cast<const F *>(&xv), *ce = reinterpret_cast<const F *>(&cv);
+#pragma unroll
+            for (int u = 0; u < V; ++u) {
+                const F e = xe[u] - ce[u];
+                d2 = fma(e, e, d2);
+            }
+        }
+        __syncwarp();
+        if (++sg == nseg) {  // the group's rows are complete
+            const int r = g * 32 + lane;
+            if (r < cnt) {
+                const F m = !(d2 < old) ? old : d2;  // the reference's min(best, d2)
+                md[base + r] = m;
+                s_md[r] = m;
+            }
+            d2 = F(0);
+            sg = 0;
+            ++g;
+        }
+    }
+    cp_async_wait<0>();
+    __syncwarp();
+    if (lane == 0) {
+        F sum = F(0);
+        int i = 0;
+        for (; i + V <= cnt; i += V) {
+            const Vec x = *reinterpret_cast<const Vec *>(s_md + i);
+            const F *e = reinterpret_cast<const F *>(&x);
+#pragma unroll
+            for (int u = 0; u < V; ++u) sum += e[u];
+        }
+        for (; i < cnt; ++i) sum += s_md[i];
+        publish_block_sum(acc, flags, b, sum, epoch);
+    }
+}
+
+constexpr int kSelThreads = 256;
+
+// Eight consecutive values from 16-byte aligned shared memory in 16-byte loads.
+__device__ __forceinline__ void load8(const float *p, float (&o)[8]) {
+    const float4 a = reinterpret_cast<const float4 *>(p)[0], b = reinterpret_cast<const float4 *>(p)[1];
+    o[0] = a.x, o[1] = a.y, o[2] = a.z, o[3] = a.w, o[4] = b.x, o[5] = b.y, o[6] = b.z, o[7] = b.w;
+}
+__device__ __forceinline__ void load8(const double *p, double (&o)[8]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const double2 a = reinterpret_cast<const double2 *>(p)[q];
+        o[2 * q] = a.x, o[2 * q + 1] = a.y;
+    }
+}
 
 // Sequential walk of the block sums for thread 0 over a[lo, hi): advances while
 // s >= a[j], subtracting, exactly as the scalar loop would; eight steps at a
 // time are computed speculatively and kept when all eight pass.
+// `a` is 16-byte aligned; the next eight values load while the current eight
+// are folded.
 template <typename F>
-__device__ __forceinline__ int64_t walk_span(const F *a, int64_t lo, int64_t hi, F &s) {
-    int64_t j = lo;
+__device__ __forceinline__ int walk_span(const F *a, int hi, F &s) {
+    int j = 0;
     F t = s;
-    while (j + 8 <= hi) {
-        F u[9];
-        u[0] = t;
-        bool all = true;
+    if (hi >= 8) {
+        F v[8];
+        load8(a, v);
+        for (;;) {
+            F w[8];
+            const bool more = j + 16 <= hi;
+            if (more) load8(a + j + 8, w);
+            F u[9];
+            u[0] = t;
+            bool all = true;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            all = all & (u[q] >= a[j + q]);
-            u[q + 1] = u[q] - a[j + q];
+            for (int q = 0; q < 8; ++q) {
+                all = all & (u[q] >= v[q]);
+                u[q + 1] = u[q] - v[q];
+            }
+            if (!all) break;
+            t = u[8];
+            j += 8;
+            if (!more) break;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = w[q];
         }
-        if (!all) break;
-        t = u[8];
-        j += 8;
     }
     while (j < hi && t >= a[j]) {
         t -= a[j];
@@ -147,10 +441,10 @@ __device__ __forceinline__ int64_t walk_span(const F *a, int64_t lo, int64_t hi,
     return j;
 }
 
-// Round c's sequential part in one CTA: the overall sum of the block sums, the
-// sampling walk (block sums, then the chosen block's rows) with resampling,
-// and the new center. The block sums stream through two shared-memory chunks:
-// warps 1.. load chunk q + 1 while thread 0 folds chunk q.
+// Round c's sequential part in one CTA: the sampling walk (block sums, then the
+// chosen block's rows) with resampling, and the new center. The block sums
+// stream through two shared-memory chunks: warps 1.. load chunk q + 1 while
+// thread 0 walks chunk q.
 template <typename F>
 __global__ void __launch_bounds__(kSelThreads) pp_select_kernel(const F *__restrict__ X, int64_t n, int d, int64_t nb,
                                                                 const F *__restrict__ acc, F *__restrict__ md,
@@ -160,7 +454,7 @@ __global__ void __launch_bounds__(kSelThreads) pp_select_kernel(const F *__restr
     constexpr int CH = 16384 / (int)sizeof(F);  // elements per chunk
     __shared__ __align__(16) F buf[2][CH];
     __shared__ __align__(16) F rows[kPPBlock];
-    __shared__ F s_val;          // overall sum, then the walk's remainder
+    __shared__ F s_val;          // the walk's remainder, then a resample draw
     __shared__ long long s_pos;  // chosen block, then chosen row (-1: give up)
     __shared__ int s_flag;
     const int tid = threadIdx.x;
@@ -170,30 +464,8 @@ __global__ void __launch_bounds__(kSelThreads) pp_select_kernel(const F *__restr
         const int64_t lo = q * CH, cnt = min((int64_t)CH, nb - lo);
         for (int64_t i = t0; i < cnt; i += nt) buf[q & 1][i] = acc[lo + i];
     };
-    // overall = acc[0] + acc[1] + ... in block order
-    load_chunk(0, tid, kSelThreads);
-    __syncthreads();
-    F overall = F(0);
-    for (int64_t q = 0; q < nchunks; ++q) {
-        if (tid >= 32 && q + 1 < nchunks) load_chunk(q + 1, tid - 32, kSelThreads - 32);
-        if (tid == 0) {
-            const int64_t cnt = min((int64_t)CH, nb - q * CH);
-            const F *a = buf[q & 1];
-            int64_t i = 0;
-            for (; i + 8 <= cnt; i += 8) {
-#pragma unroll
-                for (int u = 0; u < 8; ++u) overall += a[i + u];
-            }
-            for (; i < cnt; ++i) overall += a[i];
-        }
-        __syncthreads();
-    }
-    if (tid == 0) {
-        s_val = overall;
-        s_flag = 0;
-    }
-    __syncthreads();
-    overall = s_val;
+    // the overall sum, folded in block order by the update grid's leading CTA
+    const F overall = (F)st->overall;
     if (!(overall > F(0)) || !(overall <= f_max<F>())) {
         // every remaining distance is zero (fewer than k distinct rows) or the sum is not
         // finite: no draw can ever succeed, the reference would sample forever
@@ -206,6 +478,7 @@ __global__ void __launch_bounds__(kSelThreads) pp_select_kernel(const F *__restr
     const F eps = F(0.1) * overall / F(n);
     F p = probs[c];
     int used = st->pool_used;
+    if (tid == 0) s_flag = 0;
     __syncthreads();  // every thread has read pool_used before thread 0 may change it
     for (;;) {
         // walk the block sums: advance while b + 1 < nb and sample >= acc[b]
@@ -217,7 +490,7 @@ __global__ void __launch_bounds__(kSelThreads) pp_select_kernel(const F *__restr
             if (tid >= 32 && q + 1 < nchunks) load_chunk(q + 1, tid - 32, kSelThreads - 32);
             if (tid == 0) {
                 const int64_t lo = q * CH, hi = min(lo + CH, nb - 1);
-                const int64_t j = lo < hi ? lo + walk_span(buf[q & 1], 0, hi - lo, s) : lo;
+                const int64_t j = lo < hi ? lo + walk_span(buf[q & 1], (int)(hi - lo), s) : lo;
                 if (j < hi || hi == nb - 1) {
                     s_pos = j;
                     s_val = s;
@@ -233,7 +506,7 @@ __global__ void __launch_bounds__(kSelThreads) pp_select_kernel(const F *__restr
         __syncthreads();
         if (tid == 0) {
             F r_s = s_val;
-            const int64_t r = walk_span(rows, 0, cnt - 1, r_s);
+            const int64_t r = walk_span(rows, (int)cnt - 1, r_s);
             if (rows[r] > eps) {
                 s_pos = s0 + r;
                 s_flag = 2;
@@ -287,13 +560,22 @@ void launch_pp_first(const F *X, int64_t d, int64_t row, F *C, cudaStream_t s) {
 // include center c_begin - 1 (a resumed round).
 template <typename F>
 void launch_pp_rounds(const F *X, int64_t n, int64_t d, int64_t k, int64_t c_begin, bool update_first, F *md, F *acc,
-                      const F *probs, const F *pool, int pool_n, F *C, PPState *st, cudaStream_t s) {
+                      unsigned *flags, const F *probs, const F *pool, int pool_n, F *C, PPState *st, cudaStream_t s) {
     const int64_t nb = (n + kPPBlock - 1) / kPPBlock;
-    const size_t smem = sizeof(F) * (16 * 32 * (128 / sizeof(F) + 1) + kPPBlock);
-    cudaFuncSetAttribute(pp_update_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const unsigned grid = 1 + (unsigned)((nb + kUpdWarps - 1) / kUpdWarps);  // + the overall-sum CTA
+    // 16-byte copies need 16-byte aligned rows; narrower rows take the register path
+    const bool async = ((uintptr_t)X % 16) == 0 && ((uintptr_t)C % 16) == 0 && (d * sizeof(F)) % 16 == 0 &&
+                       d >= 128 / (int64_t)sizeof(F);
+    const int async_smem = kUpdWarps * async_warp_smem<F>();
+    if (async) cudaFuncSetAttribute(pp_update_async_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, async_smem);
     for (int64_t c = c_begin; c < k; ++c) {
         if (c > c_begin || update_first) {
-            pp_update_kernel<F><<<(unsigned)nb, kPPBlock, smem, s>>>(X, n, (int)d, C + (c - 1) * d, md, acc, st);
+            if (async)
+                pp_update_async_kernel<F><<<grid, kUpdWarps * 32, async_smem, s>>>(
+                    X, n, (int)d, nb, C + (c - 1) * d, md, acc, flags, (unsigned)c, st);
+            else
+                pp_update_kernel<F><<<grid, kUpdWarps * 32, 0, s>>>(X, n, (int)d, nb, C + (c - 1) * d, md, acc, flags,
+                                                                    (unsigned)c, st);
             KMB_LAUNCHED();
         }
         pp_select_kernel<F><<<1, kSelThreads, 0, s>>>(X, n, (int)d, nb, acc, md, probs, pool, pool_n, c, C, st);
@@ -304,8 +586,8 @@ void launch_pp_rounds(const F *X, int64_t n, int64_t d, int64_t k, int64_t c_beg
 #define KMB_PP_INST(F)                                                                                               \
     template void launch_pp_fill<F>(F *, int64_t, cudaStream_t);                                                    \
     template void launch_pp_first<F>(const F *, int64_t, int64_t, F *, cudaStream_t);                               \
-    template void launch_pp_rounds<F>(const F *, int64_t, int64_t, int64_t, int64_t, bool, F *, F *, const F *,     \
-                                      const F *, int, F *, PPState *, cudaStream_t);
+    template void launch_pp_rounds<F>(const F *, int64_t, int64_t, int64_t, int64_t, bool, F *, F *, unsigned *,    \
+                                      const F *, const F *, int, F *, PPState *, cudaStream_t);
 KMB_PP_INST(float)
 KMB_PP_INST(double)
 #undef KMB_PP_INST

@@ -45,10 +45,12 @@ struct RecheckEntry {
 
 // Device state of the k-means++ initialisation (kmb_init.cu).
 struct PPState {
-    int stopped;          // the select step ran out of uniforms (stop_round is to be redone)
+    int stopped;          // 1: out of uniforms (stop_round is to be redone); 2: no row can be drawn;
+                          // 3: the overall-sum fold timed out waiting for a block sum
     int pool_used;        // resample draws consumed from the current pool
     long long stop_round;
     long long rows_chosen;
+    double overall;       // the current round's overall distance sum (computed in F)
 };
 
 template <typename F>
@@ -57,7 +59,7 @@ template <typename F>
 void launch_pp_first(const F *X, int64_t d, int64_t row, F *C, cudaStream_t s);
 template <typename F>
 void launch_pp_rounds(const F *X, int64_t n, int64_t d, int64_t k, int64_t c_begin, bool update_first, F *md, F *acc,
-                      const F *probs, const F *pool, int pool_n, F *C, PPState *st, cudaStream_t s);
+                      unsigned *flags, const F *probs, const F *pool, int pool_n, F *C, PPState *st, cudaStream_t s);
 
 // Queues a near-tie row for the FP64 recheck. Two-candidate entries fill the
 // queue from the front (count st->n_recheck), full-rescan entries from the back
@@ -101,7 +103,7 @@ struct Workspace {
     DevBuf X, C0, Cout, labels, d2, xnorm, Ccur, Cnew, Ct, h, queue;
     DevBuf H, Gs, counts, offsets, piece_base, perm, records, shift_part, empty_flag, empty_ids;
     DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;
-    DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb, pp_acc, pp_rand, pp_state;
+    DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb, pp_acc, pp_rand, pp_state, pp_flags;
     // Grows `b` to at least `bytes`; returns false on allocation failure.
     bool ensure(DevBuf &b, size_t bytes);
     void release();

@@ -91,6 +91,23 @@ def test_plusplus_device_memory(dt):
 
 
 @pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("d", [32, 64])
+def test_plusplus_unaligned_device_rows(dt, d):
+    """Rows whose start is not 16-byte aligned take the register-staged distance kernel;
+    aligned rows take the asynchronous-copy one. Both pick the oracle's rows."""
+    rng = np.random.default_rng(41 + d)
+    n = 40000
+    X = rng.standard_normal((n, d)).astype(dt)
+    flat = torch.empty(n * d + 1, dtype=torch.float32 if dt == np.float32 else torch.float64, device="cuda")
+    Xd = flat[1:].view(n, d)
+    Xd.copy_(torch.from_numpy(X))
+    assert Xd.data_ptr() % 16 != 0
+    ref = restated.init_plusplus(X, 33)[0]
+    assert np.array_equal(kmeans.init_plusplus(Xd, 33, dt).cpu().numpy(), ref)
+    assert np.array_equal(kmeans.init_plusplus(torch.from_numpy(X).cuda(), 33, dt).cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
 def test_train_without_initial_centroids_smoke(dt):
     """The smoke test, fixture.hpp:221-252: train() with the default k-means++ init on 8
     points, 4 iterations, eps 0.001. The reference compares centroids and responses
