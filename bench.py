@@ -108,6 +108,52 @@ def cpu_reference_iters_per_s(X_host, C0_host, n_full, iters, threads):
     return 1.0 / (per_iter * scale), per_iter, it
 
 
+def run_plusplus(args, X, ctx):
+    """k-means++ initialisation (the default init of train() without initial centroids)
+    over the resident rows: centers/s, with each round's pass over X against the HBM
+    roofline, and the reference kernel's rounds on a row sample on the host cores."""
+    import numpy as np
+    import torch
+
+    from onedal_b200 import kmeans
+    n, d = X.shape
+    k = args.plusplus_k
+    stream = torch.cuda.current_stream()
+    kmeans.init_plusplus(X, min(k, 8), np.float32, ctx=ctx)  # warm-up (allocations, module load)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    kmeans.init_plusplus(X, k, np.float32, ctx=ctx)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    s = e0.elapsed_time(e1) / 1e3
+    peaks, src = load_peaks()
+    bytes_per_round = n * d * 4 + 2 * n * 4  # rows read, running minima read + written
+    achieved = bytes_per_round * (k - 1) / s / 1e9
+    out = {"metric": "k-means++ centers/s", "value": (k - 1) / s, "unit": "centers/s", "k": k, "seconds": s,
+           "ms_per_center": s / (k - 1) * 1e3,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": achieved / peaks["hbm_gbs"], "peak_source": src,
+                        "algorithmic_bytes_per_round": bytes_per_round,
+                        "note": "whole rounds (distance update + sampling walk) against the rows' bytes"}}
+    if args.cpu_sample_rows > 0:
+        from oracle import daal_ref
+        if daal_ref.available():
+            ns = min(args.cpu_sample_rows, n)
+            kc = 64
+            Xs = X[:ns].cpu().numpy()
+            daal_ref.set_threads(os.cpu_count() or 1)
+            t0 = time.perf_counter()
+            daal_ref.init_plusplus(Xs, kc)
+            per_round = (time.perf_counter() - t0) / (kc - 1) * (n / ns)
+            out["cpu_baseline"] = {"value": 1.0 / per_round, "unit": "centers/s", "cores": os.cpu_count(),
+                                   "kind": "reference",
+                                   "sample": f"reference plusPlus init kernel, first {ns} of {n} rows, {kc} centers, "
+                                             f"per-center time scaled by rows"}
+    return out
+
+
 def make_workload(device, n=None):
     import torch
     from onedal_b200 import workloads
@@ -522,6 +568,10 @@ def run_b200(args):
                    "sample": f"first {ns} of {n} rows, {it} Lloyd iterations of the reference DAAL kernel "
                              f"(OpenBLAS sgemm, std::thread shim), per-iteration time scaled by rows"}
 
+    plusplus = None
+    if rank == 0 and world == 1 and args.plusplus_k > 1:
+        plusplus = run_plusplus(args, X, ctx)
+
     batched = None
     if rank == 0 and world == 1 and args.batched_problems > 0:
         batched = run_batched(args)
@@ -549,6 +599,7 @@ def run_b200(args):
             "full_rescans_per_iteration": st.full_rescans / max(iters_done, 1),
             "serving": serving,
             "batched": batched,
+            "plusplus": plusplus,
         }
         print(json.dumps(line))
     if dist:
@@ -570,6 +621,8 @@ def main():
                     help="problems in the batched-form measurement (0 skips it)")
     ap.add_argument("--serving-requests", type=int, default=3000,
                     help="requests per serving load point (0 skips the serving measurement)")
+    ap.add_argument("--plusplus-k", type=int, default=1024,
+                    help="centers of the k-means++ initialisation measurement (0 skips it)")
     ap.add_argument("--rows", type=int, default=None,
                     help="fewer rows of the same workload (profiling captures); default: the full 20M")
     args = ap.parse_args()
