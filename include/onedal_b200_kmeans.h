@@ -124,6 +124,25 @@ KMB_API int kmb_init_plusplus(kmb_context *ctx, int dtype, int memory, const voi
                               uint32_t seed, void *C_out);
 #define KMB_PLUSPLUS_DEFAULT_SEED 777777u
 
+/* Model serialisation in oneDAL's binary archive format: the bytes of
+ * detail::serialize(kmeans::model<task::clustering>, binary_output_archive)
+ * (cpp/oneapi/dal/algo/kmeans/common.cpp:44-56,144-156 with
+ * cpp/oneapi/dal/detail/archives.hpp:24-78), so archives move between oneDAL
+ * and this library in both directions. Context-free; no GPU is needed for host
+ * memory.
+ * kmb_model_serialize: C is k x d (row-major, host or device per `memory`; k = 0
+ *   writes a model without centroids). buf = NULL only reports *size; otherwise
+ *   capacity must be >= *size.
+ * kmb_model_deserialize: reports the stored dtype (KMB_F32 / KMB_F64) and shape;
+ *   with C_out != NULL also copies the centroids (row-major, host or device) when
+ *   capacity_bytes suffices. Malformed or mismatched archives (bad magic, ids,
+ *   element types, sizes, truncation) return KMB_EINVAL, where oneDAL throws
+ *   invalid_argument("Archive content does not match requested type"). */
+KMB_API int kmb_model_serialize(int dtype, int memory, const void *C, int64_t k, int64_t d, void *buf,
+                                int64_t capacity, int64_t *size);
+KMB_API int kmb_model_deserialize(const void *buf, int64_t size, int *dtype, int64_t *k, int64_t *d, int memory,
+                                  void *C_out, int64_t capacity_bytes);
+
 /* Infer: replaces infer_ops_dispatcher<host_policy, F, lloyd_dense, clustering>
  * (cpp/oneapi/dal/algo/kmeans/detail/infer_ops.cpp:26-43 ->
  *  backend/cpu/infer_kernel.cpp:52-116). responses against C (k x d);
@@ -277,6 +296,9 @@ KMB_API int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lane
 KMB_API int kmb_server_destroy(void *server);
 /* Makes a fitted centroid set (k x d float32, host) resident; returns its id. */
 KMB_API int kmb_server_add_model(void *server, const float *C, int64_t k, int64_t d, int32_t *model_id);
+/* The same from a oneDAL model archive (kmb_model_deserialize's format); double
+ * centroids are rounded to float, the serving engine's working type. */
+KMB_API int kmb_server_add_model_serialized(void *server, const void *buf, int64_t size, int32_t *model_id);
 /* Responses of n rows (n x d float32, host) against a resident model. */
 KMB_API int kmb_server_submit_infer(void *server, int32_t model_id, const float *X, int64_t n, int64_t d,
                                     int32_t *responses, int64_t *request_id);

@@ -8,12 +8,24 @@
 // prints: iterations, objective, centroids, responses, infer objective, then the
 // smoke case of the reference suite (fixture.hpp:221-252) trained WITHOUT initial
 // centroids (oneDAL's default k-means++ init): smoke_centroids, smoke_responses.
+//
+//   kmeans_client serialize <centroids.txt> <float|double> <out.bin>
+// builds kmeans::model from "k d v..." (k = 0: a default model without centroids)
+// and writes oneDAL's binary archive of it (detail::serialize into
+// binary_output_archive, cpp/oneapi/dal/detail/archives.hpp). No GPU is used.
+//
+//   kmeans_client deserialize <in.bin> <float|double>
+// reads such an archive with oneDAL's binary_input_archive + detail::deserialize
+// and prints: cluster_count, centroids (or "exception: <what>").
 #include "oneapi/dal/algo/kmeans.hpp"
+#include "oneapi/dal/detail/archives.hpp"
+#include "oneapi/dal/detail/serialization.hpp"
 #include "oneapi/dal/table/homogen.hpp"
 #include "oneapi/dal/table/row_accessor.hpp"
 
 #include <cstdio>
 #include <fstream>
+#include <iterator>
 #include <string>
 #include <vector>
 
@@ -64,7 +76,67 @@ int run(const std::vector<double> &xs, std::int64_t n, std::int64_t d, const std
     return 0;
 }
 
+template <typename F>
+int serialize_model(const char *in, const char *out) {
+    std::ifstream f(in);
+    std::int64_t k, d;
+    f >> k >> d;
+    std::vector<F> c(k * d);
+    for (auto &v : c) {
+        double x;
+        f >> x;
+        v = F(x);
+    }
+    dal::kmeans::model<> m;
+    if (k > 0) m.set_centroids(dal::homogen_table::wrap(c.data(), k, d));
+    dal::detail::binary_output_archive ar;
+    dal::detail::serialize(m, ar);
+    const auto bytes = ar.to_array();
+    std::FILE *o = std::fopen(out, "wb");
+    if (!o) return 1;
+    std::fwrite(bytes.get_data(), 1, bytes.get_count(), o);
+    std::fclose(o);
+    std::printf("bytes %lld\n", (long long)bytes.get_count());
+    return 0;
+}
+
+template <typename F>
+int deserialize_model(const char *in) {
+    std::ifstream f(in, std::ios::binary);
+    const std::vector<char> raw((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    dal::detail::binary_input_archive ar(reinterpret_cast<const dal::byte_t *>(raw.data()),
+                                         (std::int64_t)raw.size());
+    dal::kmeans::model<> m;
+    dal::detail::deserialize(m, ar);
+    std::printf("cluster_count %lld\n", (long long)m.get_cluster_count());
+    std::printf("centroids");
+    if (m.get_cluster_count() > 0) {
+        const auto c = dal::row_accessor<const F>(m.get_centroids()).pull({ 0, -1 });
+        for (std::int64_t i = 0; i < c.get_count(); ++i) std::printf(" %.17g", (double)c[i]);
+    }
+    std::printf("\n");
+    return 0;
+}
+
 int main(int argc, char **argv) {
+    if (argc >= 5 && std::string(argv[1]) == "serialize") {
+        try {
+            return std::string(argv[3]) == "double" ? serialize_model<double>(argv[2], argv[4])
+                                                    : serialize_model<float>(argv[2], argv[4]);
+        } catch (const std::exception &e) {
+            std::printf("exception: %s\n", e.what());
+            return 1;
+        }
+    }
+    if (argc >= 4 && std::string(argv[1]) == "deserialize") {
+        try {
+            return std::string(argv[3]) == "double" ? deserialize_model<double>(argv[2])
+                                                    : deserialize_model<float>(argv[2]);
+        } catch (const std::exception &e) {
+            std::printf("exception: %s\n", e.what());
+            return 1;
+        }
+    }
     if (argc < 3) return 2;
     std::ifstream f(argv[1]);
     std::int64_t n, d, k;

@@ -23,6 +23,7 @@ EXPORTED = (
     "kmb_context_set_kernel_timing", "kmb_context_kernel_time", "kmb_infer_noalloc",
     "kmb_server_create", "kmb_server_destroy", "kmb_server_add_model", "kmb_server_submit_infer",
     "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats", "kmb_server_infer_form", "kmb_server_wait_detail", "kmb_context_set_max_sms", "kmb_init_plusplus", "kmb_batched_train",
+    "kmb_model_serialize", "kmb_model_deserialize", "kmb_server_add_model_serialized",
 )
 
 
@@ -110,6 +111,10 @@ def load_library(path: str = LIB_PATH):
             lib.kmb_server_get_stats.argtypes = [P, ctypes.c_void_p]
             lib.kmb_server_infer_form.argtypes = [P, I32, I64, ctypes.POINTER(I32)]
             lib.kmb_batched_train.argtypes = [ctypes.c_int, P, I64, I64, D, I32, P, P]
+            lib.kmb_model_serialize.argtypes = [ctypes.c_int, ctypes.c_int, P, I64, I64, P, I64, ctypes.POINTER(I64)]
+            lib.kmb_model_deserialize.argtypes = [P, I64, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(I64),
+                                                  ctypes.POINTER(I64), ctypes.c_int, P, I64]
+            lib.kmb_server_add_model_serialized.argtypes = [P, P, I64, ctypes.POINTER(I32)]
             _lib = lib
     return _lib
 

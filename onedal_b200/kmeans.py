@@ -68,6 +68,7 @@ class _msg:
     model_cc_neq_data_cc = "Input model centroids column count is not equal to input data column count"
     objective_lt_zero = "Objective function value is lower than zero"
     too_many_empty = "Number of clusters exceeds the number of points"
+    archive_content_does_not_match_type = "Archive content does not match requested type"
 
 
 class method:
@@ -194,6 +195,74 @@ class model:
 
     def has_centroids(self):
         return _has_data(self._centroids)
+
+    def serialize(self) -> bytes:
+        """oneDAL's binary archive of this model (the bytes detail::serialize writes into
+        binary_output_archive; algo/kmeans/common.cpp:44-56,144-156), via
+        kmb_model_serialize. Device-resident centroids are read back by the library."""
+        lib = _native.load_library()
+        C = self._centroids
+        k = 0 if C is None else int(C.shape[0])
+        d = 0 if C is None else int(C.shape[1])
+        dev = _is_torch_cuda(C) if C is not None else False
+        if C is not None:
+            if dev:
+                C = C.contiguous()
+                dtype = _native.KMB_F64 if str(C.dtype) == "torch.float64" else _native.KMB_F32
+            else:
+                C = np.ascontiguousarray(C)
+                if C.dtype not in (np.float32, np.float64):
+                    C = C.astype(np.float64)
+                dtype = _native.KMB_F64 if C.dtype == np.float64 else _native.KMB_F32
+        else:
+            dtype = _native.KMB_F32
+        size = ctypes.c_int64()
+        mem = _native.KMB_MEM_DEVICE if dev else _native.KMB_MEM_HOST
+        ptr = None if C is None else _ptr(C, dev)
+        rc = lib.kmb_model_serialize(dtype, mem, ptr, k, d, None, 0, ctypes.byref(size))
+        if rc != _native.KMB_OK:
+            raise invalid_argument(lib.kmb_status_string(rc).decode())
+        buf = ctypes.create_string_buffer(size.value)
+        rc = lib.kmb_model_serialize(dtype, mem, ptr, k, d, buf, size.value, ctypes.byref(size))
+        if rc != _native.KMB_OK:
+            raise internal_error(lib.kmb_status_string(rc).decode())
+        return buf.raw[:size.value]
+
+    @classmethod
+    def deserialize(cls, data: bytes, device=None) -> "model":
+        """A model from oneDAL's binary archive (detail::deserialize from
+        binary_input_archive). Centroids keep the archive's float type; with `device`
+        (a torch device) they are copied straight into device memory. Malformed archives
+        raise invalid_argument with oneDAL's message."""
+        lib = _native.load_library()
+        raw = bytes(data)
+        dt, k, d = ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64()
+        rc = lib.kmb_model_deserialize(raw, len(raw), ctypes.byref(dt), ctypes.byref(k), ctypes.byref(d),
+                                       _native.KMB_MEM_HOST, None, 0)
+        if rc != _native.KMB_OK:
+            raise invalid_argument(_msg.archive_content_does_not_match_type)
+        if k.value == 0:
+            return cls()
+        npdt = np.float64 if dt.value == _native.KMB_F64 else np.float32
+        if device is not None:
+            import torch
+            C = torch.empty((k.value, d.value), dtype=torch.float64 if npdt == np.float64 else torch.float32,
+                            device=device)
+            mem, ptr, nbytes = _native.KMB_MEM_DEVICE, C.data_ptr(), C.numel() * C.element_size()
+        else:
+            C = np.empty((k.value, d.value), npdt)
+            mem, ptr, nbytes = _native.KMB_MEM_HOST, C.ctypes.data, C.nbytes
+        rc = lib.kmb_model_deserialize(raw, len(raw), ctypes.byref(dt), ctypes.byref(k), ctypes.byref(d), mem,
+                                       ptr, nbytes)
+        if rc != _native.KMB_OK:
+            raise invalid_argument(_msg.archive_content_does_not_match_type)
+        return cls(C)
+
+    def __getstate__(self):
+        return {"archive": self.serialize()}
+
+    def __setstate__(self, state):
+        self._centroids = model.deserialize(state["archive"])._centroids
 
 
 class train_result:

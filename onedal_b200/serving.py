@@ -60,6 +60,16 @@ class KMeansServer:
             raise ServingError(f"add_model failed ({rc})")
         return mid.value
 
+    def add_model_serialized(self, archive: bytes) -> int:
+        """Makes a model resident from oneDAL's binary model archive
+        (kmeans.model.serialize(), or oneDAL's own detail::serialize)."""
+        raw = bytes(archive)
+        mid = ctypes.c_int32()
+        rc = self.lib.kmb_server_add_model_serialized(self.handle, raw, len(raw), ctypes.byref(mid))
+        if rc != _native.KMB_OK:
+            raise ServingError(f"add_model_serialized failed ({rc})")
+        return mid.value
+
     def submit_infer(self, model_id: int, rows) -> Request:
         X = self._f32(rows)
         labels = np.empty(X.shape[0], np.int32)

@@ -29,6 +29,13 @@ Sources (paths inside the reference project):
   777777: the default of cpp/oneapi/dal/algo/kmeans/detail/train_init_centroids.hpp)
   built from source, float64 and float32, on the seeded inputs of plusplus_cases()
   and on the example data with k=20.
+* model_archives.npz -- oneDAL binary archives of k-means models written by
+  oneDAL's own serialisation code (detail::serialize into binary_output_archive,
+  compiled from the reference sources into integration/_build/kmeans_client):
+  the model of the serialisation test (cpp/oneapi/dal/algo/kmeans/test/
+  serialization.cpp:39-123; trained by the reference kernel with the default
+  descriptor and k-means++ init) in float and double with the test rows'
+  responses, a 7x3 double model and a model without centroids.
 """
 import argparse
 import json
@@ -105,6 +112,31 @@ def smoke_infer(ref):
     }
 
 
+def serialization_case(ref):
+    """Train/test rows of the model serialisation test
+    (cpp/oneapi/dal/algo/kmeans/test/serialization.cpp:39-72)."""
+    src = open(os.path.join(ref, "cpp/oneapi/dal/algo/kmeans/test/serialization.cpp")).read()
+    x_test, p = _array_after(src, "x_test[]")
+    x_train, p = _array_after(src, "x_train[]", p)
+    assert len(x_test) == 20 and len(x_train) == 48
+    return np.array(x_train, np.float64).reshape(12, 4), np.array(x_test, np.float64).reshape(5, 4)
+
+
+def onedal_archive(client, centroids, tag, workdir):
+    """oneDAL's own binary archive of a k-means model with `centroids` (k x d; k = 0 for
+    a model without centroids), written by the integration client, which runs
+    detail::serialize into binary_output_archive compiled from the reference sources."""
+    import subprocess
+    src = os.path.join(workdir, f"c_{tag}.txt")
+    out = os.path.join(workdir, f"m_{tag}.bin")
+    k, d = centroids.shape
+    with open(src, "w") as f:
+        f.write(f"{k} {d}\n" + " ".join(repr(float(v)) for v in centroids.ravel()) + "\n")
+    subprocess.run([client, "serialize", src, "double" if centroids.dtype == np.float64 else "float", out],
+                   check=True, capture_output=True)
+    return np.frombuffer(open(out, "rb").read(), np.uint8)
+
+
 def blobs_c1(n, seed):
     """Seeded mixture of 20 isotropic Gaussian blobs (std 1) in d=20, centres U[-10,10]."""
     rng = np.random.default_rng(seed)
@@ -172,6 +204,32 @@ def main():
         for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
             out[f"C_{name}_{tag}"] = daal_ref.init_plusplus(X.astype(dt), k)
     np.savez_compressed(os.path.join(HERE, "daal_ref_plusplus.npz"), **out)
+
+    # model archives: the serialisation test's model (default descriptor: k = 2, 100
+    # iterations, eps 0, k-means++ init) trained by the reference kernel, archived by
+    # oneDAL's own serialisation code (integration client), plus the test rows' responses
+    client = os.path.join(os.path.dirname(os.path.dirname(HERE)), "integration", "_build", "kmeans_client")
+    if os.path.exists(client):
+        import tempfile
+        x_train, x_test = serialization_case(ref)
+        out = {"x_train": x_train, "x_test": x_test}
+        with tempfile.TemporaryDirectory() as tmp:
+            for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+                X = x_train.astype(dt)
+                C0 = daal_ref.init_plusplus(X, 2)
+                C, _, _, _ = daal_ref.train(X, C0, 100, 0.0)
+                lab, _ = daal_ref.infer(x_test.astype(dt), C, False)
+                out[f"C_{tag}"] = C
+                out[f"responses_{tag}"] = lab
+                out[f"archive_{tag}"] = onedal_archive(client, C, tag, tmp)
+            rng = np.random.default_rng(2024)
+            W = rng.standard_normal((7, 3))
+            out["C_wide_f64"] = W
+            out["archive_wide_f64"] = onedal_archive(client, W, "wide", tmp)
+            out["archive_empty"] = onedal_archive(client, np.zeros((0, 0)), "empty", tmp)
+        np.savez_compressed(os.path.join(HERE, "model_archives.npz"), **out)
+    else:
+        print("integration client not built: model_archives.npz left as is")
     print("golden fixtures written to", HERE)
 
 
