@@ -124,6 +124,25 @@ KMB_API int kmb_init_plusplus(kmb_context *ctx, int dtype, int memory, const voi
                               uint32_t seed, void *C_out);
 #define KMB_PLUSPLUS_DEFAULT_SEED 777777u
 
+/* CSR rows (kmeans::method::lloyd_csr): replaces the lloyd_csr instantiations of
+ * the same dispatchers (detail/train_ops.cpp:41-42, detail/infer_ops.cpp:42-43 ->
+ * DAAL KMeansBatchKernel<lloydCSR>, kmeans_lloyd_impl.i:248-344,
+ * kmeans_lloyd_postprocessing.h:186-350). Rows are given as csr_table holds them
+ * (csr_table::wrap(values, column_indices, row_offsets, row_count, column_count,
+ * indexing)): values (nnz, dtype), column_indices (nnz int64), row_offsets
+ * (n + 1 int64), indexing 0 = zero_based, 1 = one_based; column indices must
+ * increase strictly within each row. Centroids are dense (k x d). Scores are the
+ * sparse product over the stored entries; the objective is the reference's CSR
+ * form (per row: sum over stored entries of x^2 - 2xc, plus ||c||^2, clipped at
+ * zero). Train takes the plain form only and requires initial centroids. */
+KMB_API int kmb_train_csr(kmb_context *ctx, int dtype, int memory, const void *values, const int64_t *col_indices,
+                          const int64_t *row_offsets, int64_t n, int64_t d, int32_t indexing, const void *C0,
+                          const kmb_params *params, void *C_out, int32_t *responses, double *objective,
+                          int64_t *iteration_count, kmb_stats *stats);
+KMB_API int kmb_infer_csr(kmb_context *ctx, int dtype, int memory, const void *values, const int64_t *col_indices,
+                          const int64_t *row_offsets, int64_t n, int64_t d, int32_t indexing, const void *C, int64_t k,
+                          int32_t compute_objective, int32_t *responses, double *objective);
+
 /* Model serialisation in oneDAL's binary archive format: the bytes of
  * detail::serialize(kmeans::model<task::clustering>, binary_output_archive)
  * (cpp/oneapi/dal/algo/kmeans/common.cpp:44-56,144-156 with

@@ -104,7 +104,8 @@ void Workspace::release() {
     DevBuf *all[] = {&X, &C0, &Cout, &labels, &d2, &xnorm, &Ccur, &Cnew, &Ct, &h, &queue, &H, &Gs,
                      &counts, &offsets, &piece_base, &perm, &records, &shift_part, &empty_flag, &empty_ids,
                      &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx, &rowb, &pp_acc, &pp_rand,
-                     &pp_state, &pp_flags};
+                     &pp_state, &pp_flags, &csr_vals, &csr_cols64, &csr_rowptr64, &csr_cols, &csr_rowptr,
+                     &csr_bad, &csr_cnorm};
     for (DevBuf *b : all) {
         if (b->ptr) cudaFreeAsync(b->ptr, stream);
         b->ptr = nullptr;
@@ -542,6 +543,184 @@ int validate_shapes(kmb_context *ctx, int dtype, int64_t n, int64_t d, int64_t k
     return KMB_OK;
 }
 
+// ---- CSR rows (kmeans::method::lloyd_csr) ----------------------------------
+
+// Brings caller CSR arrays (host or device; indices int64 with base 0 or 1) into
+// the device form of kmb::CsrRows and checks them.
+template <typename F>
+int prepare_csr(kmb_context *ctx, int memory, const void *vals, const int64_t *cols, const int64_t *rowptr, int64_t n,
+                int64_t d, int base, kmb::CsrRows *out) {
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    int64_t ends[2];
+    if (memory == KMB_MEM_HOST) {
+        ends[0] = rowptr[0];
+        ends[1] = rowptr[n];
+    } else {
+        KMB_CUDA(cudaMemcpyAsync(&ends[0], rowptr, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        KMB_CUDA(cudaMemcpyAsync(&ends[1], rowptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        KMB_CUDA(cudaStreamSynchronize(s));
+    }
+    if (ends[0] != base) return fail(ctx, KMB_EINVAL, "CSR row offsets must start at the index base (%d)", base);
+    const int64_t nnz = ends[1] - base;
+    if (nnz < 0) return fail(ctx, KMB_EINVAL, "CSR row offsets are decreasing");
+    bool ok = ws.ensure(ws.csr_cols, sizeof(int32_t) * std::max<int64_t>(1, nnz)) &&
+              ws.ensure(ws.csr_rowptr, sizeof(int64_t) * (n + 1)) && ws.ensure(ws.csr_bad, sizeof(int));
+    const F *v = (const F *)vals;
+    const int64_t *c64 = cols, *r64 = rowptr;
+    if (ok && memory == KMB_MEM_HOST) {
+        ok = ws.ensure(ws.csr_cols64, sizeof(int64_t) * std::max<int64_t>(1, nnz)) &&
+             ws.ensure(ws.csr_rowptr64, sizeof(int64_t) * (n + 1));
+        if (ok) {
+            int rc = upload<F>(ctx, ws.csr_vals, vals, sizeof(F) * std::max<int64_t>(1, nnz), &v);
+            if (rc) return rc;
+            KMB_CUDA(cudaMemcpyAsync(ws.csr_cols64.ptr, cols, sizeof(int64_t) * nnz, cudaMemcpyHostToDevice, s));
+            KMB_CUDA(cudaMemcpyAsync(ws.csr_rowptr64.ptr, rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s));
+            c64 = (const int64_t *)ws.csr_cols64.ptr;
+            r64 = (const int64_t *)ws.csr_rowptr64.ptr;
+        }
+    }
+    if (!ok) return fail(ctx, KMB_ENOMEM, "device allocation failed (CSR rows, nnz=%lld)", (long long)nnz);
+    KMB_CUDA(cudaMemsetAsync(ws.csr_bad.ptr, 0, sizeof(int), s));
+    kmb::launch_csr_prepare(c64, r64, n, d, nnz, base, (int32_t *)ws.csr_cols.ptr, (int64_t *)ws.csr_rowptr.ptr,
+                            (int *)ws.csr_bad.ptr, s);
+    int bad = 0;
+    KMB_CUDA(cudaMemcpyAsync(&bad, ws.csr_bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaStreamSynchronize(s));
+    if (bad & 1) return fail(ctx, KMB_EINVAL, "CSR row offsets are out of order or out of range");
+    if (bad & 2)
+        return fail(ctx, KMB_EINVAL,
+                    "CSR column indices must lie in [0, column_count) and increase strictly within each row");
+    *out = kmb::CsrRows{v, (const int32_t *)ws.csr_cols.ptr, (const int64_t *)ws.csr_rowptr.ptr, n, d, nnz};
+    return KMB_OK;
+}
+
+template <typename F>
+void csr_assign_pass(kmb_context *ctx, const kmb::CsrRows &X, const F *C, int64_t k, int32_t *labels, F *d2,
+                     LoopState *st) {
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    const int64_t kpad = round_up(k, kBN);
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    reset_iteration_kernel<<<1, 1, 0, s>>>(st);
+    KMB_LAUNCHED();
+    kmb::launch_prep_centroids<F>(C, k, X.d, kpad, (F *)ws.Ct.ptr, (F *)ws.h.ptr, &sc->cnorm_max, st, s);
+    KernelTimer timer(ctx, 0);
+    kmb::launch_csr_assign<F>(X, (const F *)ws.Ct.ptr, (const F *)ws.h.ptr, k, kpad, labels, d2, st, s);
+}
+
+template <typename F>
+int train_csr_impl(kmb_context *ctx, int memory, const void *vals, const int64_t *cols, const int64_t *rowptr,
+                   int64_t n, int64_t d, int base, const void *C0v, const kmb_params *p, void *C_out,
+                   int32_t *responses, double *objective, int64_t *iteration_count, kmb_stats *stats) {
+    const int64_t k = p->cluster_count;
+    int rc = ensure_common<F>(ctx, n, d, k, false, false);
+    if (rc) return rc;
+    kmb::UpdatePlan plan = kmb::make_update_plan(n, k, d);
+    if (!kmb::ensure_update_buffers(ctx->ws, plan, sizeof(F)) || !ctx->ws.ensure(ctx->ws.csr_cnorm, sizeof(double) * k))
+        return fail(ctx, KMB_ENOMEM, "update buffers");
+    kmb::CsrRows X;
+    if ((rc = prepare_csr<F>(ctx, memory, vals, cols, rowptr, n, d, base, &X))) return rc;
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    const F *C0 = (const F *)C0v;
+    if (memory == KMB_MEM_HOST && (rc = upload<F>(ctx, ws.C0, C0v, sizeof(F) * k * d, &C0))) return rc;
+    int32_t *labels = (memory == KMB_MEM_DEVICE && responses) ? responses : (int32_t *)ws.labels.ptr;
+    F *Ccur = (F *)ws.Ccur.ptr, *Cnew = (F *)ws.Cnew.ptr, *d2 = (F *)ws.d2.ptr;
+    LoopState *st = (LoopState *)ws.state.ptr;
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    init_state(ctx->h_state[0], p->accuracy_threshold);
+    init_state(ctx->h_state[1], 0.0);
+    KMB_CUDA(cudaMemcpyAsync(st, ctx->h_state, sizeof(LoopState) * 2, cudaMemcpyHostToDevice, s));
+    KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
+    KMB_CUDA(cudaMemcpyAsync(Ccur, C0, sizeof(F) * k * d, cudaMemcpyDeviceToDevice, s));
+    const int64_t T = p->max_iteration_count;
+    int64_t enq = 0, batch = 2;
+    while (enq < T) {
+        const int64_t upto = std::min(T, enq + batch);
+        for (; enq < upto; ++enq) {
+            csr_assign_pass<F>(ctx, X, Ccur, k, labels, d2, st);
+            KernelTimer timer(ctx, 2);
+            kmb::launch_update<F>(nullptr, plan, labels, d2, Ccur, Cnew, ws, st, /*commit=*/true, s, &X);
+        }
+        KMB_CUDA(cudaGetLastError());
+        if (enq < T) {
+            KMB_CUDA(cudaMemcpyAsync(ctx->h_state, st, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaStreamSynchronize(s));
+            if (ctx->h_state[0].done) break;
+            batch = std::min<int64_t>(batch * 2, 8);
+        }
+    }
+    // responses against the final centroids, then the exact objective
+    csr_assign_pass<F>(ctx, X, Ccur, k, labels, d2, st + 1);
+    kmb::launch_csr_objective<F>(X, Ccur, k, labels, (double *)ws.csr_cnorm.ptr, (double *)ws.obj_part.ptr,
+                                 &sc->objective, s);
+    KMB_CUDA(cudaGetLastError());
+    const cudaMemcpyKind out_kind = memory == KMB_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (C_out) KMB_CUDA(cudaMemcpyAsync(C_out, Ccur, sizeof(F) * k * d, out_kind, s));
+    if (responses && labels != responses)
+        KMB_CUDA(cudaMemcpyAsync(responses, labels, sizeof(int32_t) * n, out_kind, s));
+    double obj_h = 0.0;
+    KMB_CUDA(cudaMemcpyAsync(&obj_h, &sc->objective, sizeof(double), cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaMemcpyAsync(ctx->h_state, st, sizeof(LoopState) * 2, cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaStreamSynchronize(s));
+    const LoopState &hs = ctx->h_state[0];
+    if (hs.error) return fail(ctx, hs.error, "device loop failed (status %d)", hs.error);
+    if (objective) *objective = obj_h;
+    if (iteration_count) *iteration_count = hs.iterations;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->empty_cluster_events = hs.empty_events;
+        stats->last_shift = hs.shift;
+    }
+    return KMB_OK;
+}
+
+template <typename F>
+int infer_csr_impl(kmb_context *ctx, int memory, const void *vals, const int64_t *cols, const int64_t *rowptr,
+                   int64_t n, int64_t d, int base, const void *Cv, int64_t k, int32_t compute_objective,
+                   int32_t *responses, double *objective) {
+    int rc = ensure_common<F>(ctx, n, d, k, false, false);
+    if (rc) return rc;
+    kmb::Workspace &ws = ctx->ws;
+    if (!ws.ensure(ws.obj_part, sizeof(double) * 148 * 8) || !ws.ensure(ws.csr_cnorm, sizeof(double) * k))
+        return fail(ctx, KMB_ENOMEM, "objective");
+    kmb::CsrRows X;
+    if ((rc = prepare_csr<F>(ctx, memory, vals, cols, rowptr, n, d, base, &X))) return rc;
+    cudaStream_t s = ctx->stream;
+    const F *C = (const F *)Cv;
+    if (memory == KMB_MEM_HOST && (rc = upload<F>(ctx, ws.C0, Cv, sizeof(F) * k * d, &C))) return rc;
+    int32_t *labels = (memory == KMB_MEM_DEVICE && responses) ? responses : (int32_t *)ws.labels.ptr;
+    LoopState *st = (LoopState *)ws.state.ptr + 1;
+    kmb::DevScalars *sc = (kmb::DevScalars *)ws.scalars.ptr;
+    init_state(ctx->h_state[1], 0.0);
+    KMB_CUDA(cudaMemcpyAsync(st, &ctx->h_state[1], sizeof(LoopState), cudaMemcpyHostToDevice, s));
+    KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
+    csr_assign_pass<F>(ctx, X, C, k, labels, (F *)ws.d2.ptr, st);
+    if (compute_objective)
+        kmb::launch_csr_objective<F>(X, C, k, labels, (double *)ws.csr_cnorm.ptr, (double *)ws.obj_part.ptr,
+                                     &sc->objective, s);
+    KMB_CUDA(cudaGetLastError());
+    const cudaMemcpyKind out_kind = memory == KMB_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (responses && labels != responses)
+        KMB_CUDA(cudaMemcpyAsync(responses, labels, sizeof(int32_t) * n, out_kind, s));
+    double obj_h = 0.0;
+    KMB_CUDA(cudaMemcpyAsync(&obj_h, &sc->objective, sizeof(double), cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaStreamSynchronize(s));
+    if (compute_objective && objective) *objective = obj_h;
+    return KMB_OK;
+}
+
+int validate_csr_call(kmb_context *ctx, int dtype, int memory, const void *vals, const int64_t *cols,
+                      const int64_t *rowptr, int32_t indexing) {
+    if (dtype != KMB_F32 && dtype != KMB_F64) return fail(ctx, KMB_EINVAL, "unknown dtype %d", dtype);
+    if (memory != KMB_MEM_HOST && memory != KMB_MEM_DEVICE) return fail(ctx, KMB_EINVAL, "unknown memory kind");
+    if (indexing != 0 && indexing != 1) return fail(ctx, KMB_EINVAL, "indexing must be 0 (zero-based) or 1 (one-based)");
+    if (!vals || !cols || !rowptr) return fail(ctx, KMB_EINVAL, "CSR values, column indices and row offsets are required");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    return KMB_OK;
+}
+
 }  // namespace
 
 // k-means++ initialisation (kmb_init.cu has the device side). The host draws
@@ -720,6 +899,44 @@ int kmb_train(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n,
     if (dtype == KMB_F32)
         return train_impl<float>(ctx, memory, X, n, d, C0, params, C_out, responses, objective, iteration_count, stats);
     return train_impl<double>(ctx, memory, X, n, d, C0, params, C_out, responses, objective, iteration_count, stats);
+}
+
+int kmb_train_csr(kmb_context *ctx, int dtype, int memory, const void *values, const int64_t *col_indices,
+                  const int64_t *row_offsets, int64_t n, int64_t d, int32_t indexing, const void *C0,
+                  const kmb_params *params, void *C_out, int32_t *responses, double *objective,
+                  int64_t *iteration_count, kmb_stats *stats) {
+    if (!ctx || !params) return KMB_EINVAL;
+    ctx->last_error.clear();
+    int rc = validate_shapes(ctx, dtype, n, d, params->cluster_count);
+    if (rc) return rc;
+    if (params->max_iteration_count < 0) return fail(ctx, KMB_EINVAL, "max_iteration_count must be >= 0");
+    if (!(params->accuracy_threshold >= 0.0)) return fail(ctx, KMB_EINVAL, "accuracy_threshold must be >= 0");
+    if (params->form != KMB_FORM_PLAIN) return fail(ctx, KMB_EINVAL, "CSR rows take the plain form");
+    if (!C0) return fail(ctx, KMB_EINVAL, "initial centroids are required");
+    if ((rc = validate_csr_call(ctx, dtype, memory, values, col_indices, row_offsets, indexing))) return rc;
+    if (dtype == KMB_F32)
+        return train_csr_impl<float>(ctx, memory, values, col_indices, row_offsets, n, d, indexing, C0, params, C_out,
+                                     responses, objective, iteration_count, stats);
+    return train_csr_impl<double>(ctx, memory, values, col_indices, row_offsets, n, d, indexing, C0, params, C_out,
+                                  responses, objective, iteration_count, stats);
+}
+
+int kmb_infer_csr(kmb_context *ctx, int dtype, int memory, const void *values, const int64_t *col_indices,
+                  const int64_t *row_offsets, int64_t n, int64_t d, int32_t indexing, const void *C, int64_t k,
+                  int32_t compute_objective, int32_t *responses, double *objective) {
+    if (!ctx) return KMB_EINVAL;
+    ctx->last_error.clear();
+    if (n <= 0) return fail(ctx, KMB_EINVAL, "input data is empty");
+    if (n > INT32_MAX) return fail(ctx, KMB_EINVAL, "row count exceeds INT32_MAX");
+    if (d <= 0 || k <= 0 || k > INT32_MAX) return fail(ctx, KMB_EINVAL, "bad centroid shape");
+    if (!C) return fail(ctx, KMB_EINVAL, "centroids are required");
+    int rc = validate_csr_call(ctx, dtype, memory, values, col_indices, row_offsets, indexing);
+    if (rc) return rc;
+    if (dtype == KMB_F32)
+        return infer_csr_impl<float>(ctx, memory, values, col_indices, row_offsets, n, d, indexing, C, k,
+                                     compute_objective, responses, objective);
+    return infer_csr_impl<double>(ctx, memory, values, col_indices, row_offsets, n, d, indexing, C, k,
+                                  compute_objective, responses, objective);
 }
 
 int kmb_init_plusplus(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, int64_t k,

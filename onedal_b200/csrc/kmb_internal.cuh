@@ -104,6 +104,7 @@ struct Workspace {
     DevBuf H, Gs, counts, offsets, piece_base, perm, records, shift_part, empty_flag, empty_ids;
     DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;
     DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb, pp_acc, pp_rand, pp_state, pp_flags;
+    DevBuf csr_vals, csr_cols64, csr_rowptr64, csr_cols, csr_rowptr, csr_bad, csr_cnorm;
     // Grows `b` to at least `bytes`; returns false on allocation failure.
     bool ensure(DevBuf &b, size_t bytes);
     void release();
@@ -164,6 +165,35 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
                      const double *shift_part, const double *cnorm_max_prev, void *rowb, cudaStream_t s);
 size_t tc_xchg_bytes();
 
+// ---- CSR rows (kmeans::method::lloyd_csr) ------------------------------------
+// Zero-based, device-resident CSR rows: values (nnz, F), column indices (int32,
+// strictly increasing within a row, in [0, d)) and row offsets (n + 1, int64,
+// rowptr[0] == 0).
+struct CsrRows {
+    const void *vals;
+    const int32_t *cols;
+    const int64_t *rowptr;
+    int64_t n, d, nnz;
+};
+
+// Converts caller indices (int64, `base` 0 or 1) into CsrRows' form and checks
+// them; *bad (device int) becomes nonzero when an offset is out of order or a
+// column index is out of range or not strictly increasing within its row.
+void launch_csr_prepare(const int64_t *cols_in, const int64_t *rowptr_in, int64_t n, int64_t d, int64_t nnz, int base,
+                        int32_t *cols_out, int64_t *rowptr_out, int *bad, cudaStream_t s);
+
+// Labels and squared distances (2*best + sum of the row's v^2, in F) of CSR rows
+// against centroids prepared by launch_prep_centroids (Ct d x kpad, h kpad).
+template <typename F>
+void launch_csr_assign(const CsrRows &X, const F *Ct, const F *h, int64_t k, int64_t kpad, int32_t *labels, F *d2,
+                       const LoopState *st, cudaStream_t s);
+
+// Exact objective of CSR rows: per row sum over stored entries of (x^2 - 2xc) +
+// ||c||^2, clipped at zero, in FP64, deterministic. cnorm2: k doubles of scratch.
+template <typename F>
+void launch_csr_objective(const CsrRows &X, const F *C, int64_t k, const int32_t *labels, double *cnorm2,
+                          double *partials, double *out, cudaStream_t s);
+
 // ---- update ----------------------------------------------------------------
 UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d);
 // Sizes the update buffers of `ws` for plan `p` (false on allocation failure).
@@ -174,9 +204,11 @@ bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize);
 // sum / count rounded to F, empty clusters reseeded with the farthest rows,
 // centroid shift, convergence flag. C_old is overwritten by the new centroids
 // when `commit` (the loop path); otherwise they are left in C_new.
+// With `csr`, the rows are CSR (X is unused): piece sums scatter the stored
+// entries and a reseeded cluster takes its candidate row expanded to dense.
 template <typename F>
 void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *C_old, F *C_new,
-                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s);
+                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr = nullptr);
 
 // Just the sums/counts half of the update (sharded training).
 template <typename F>

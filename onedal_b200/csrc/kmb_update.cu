@@ -251,6 +251,38 @@ segsum_kernel(const F *__restrict__ X, int d, int k, const int32_t *__restrict__
     }
 }
 
+// CSR form of segsum_kernel: one warp per piece. The piece's record is zeroed,
+// then its rows' stored entries are added in row order (a row's columns are
+// distinct, so its lanes never collide; __syncwarp orders consecutive rows).
+template <typename F>
+__global__ void __launch_bounds__(128)
+csr_segsum_kernel(const F *__restrict__ vals, const int32_t *__restrict__ cols, const int64_t *__restrict__ rowptr,
+                  int d, int k, const int32_t *__restrict__ perm, const int64_t *__restrict__ offsets,
+                  const int64_t *__restrict__ piece_base, int64_t piece_rows, int64_t max_pieces,
+                  double *__restrict__ records, const LoopState *st) {
+    if (is_done(st)) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t p = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (p >= max_pieces || p >= piece_base[k]) return;
+    int lo = 0, hi = k;  // invariant: piece_base[lo] <= p < piece_base[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (piece_base[mid] <= p) lo = mid; else hi = mid;
+    }
+    const int j = lo;
+    const int64_t q = p - piece_base[j];
+    const int64_t s = offsets[j] + q * piece_rows;
+    const int64_t e = min(s + piece_rows, offsets[j + 1]);
+    double *rec = records + p * (int64_t)d;
+    for (int t = lane; t < d; t += 32) rec[t] = 0.0;
+    __syncwarp();
+    for (int64_t i = s; i < e; ++i) {
+        const int64_t r = perm[i];
+        for (int64_t x = rowptr[r] + lane; x < rowptr[r + 1]; x += 32) rec[cols[x]] += (double)vals[x];
+        __syncwarp();
+    }
+}
+
 // Per cluster: S = sum of its pieces (in order); c = F(S / count); shift part.
 template <typename F>
 __global__ void finalize_kernel(const double *__restrict__ records, const int64_t *__restrict__ counts,
@@ -548,6 +580,40 @@ __global__ void reseed_apply_kernel(const F *__restrict__ X, int d, const Cand *
     }
 }
 
+// CSR form of reseed_apply_kernel: the candidate row expanded to dense.
+template <typename F>
+__global__ void csr_reseed_apply_kernel(const F *__restrict__ vals, const int32_t *__restrict__ cols,
+                                        const int64_t *__restrict__ rowptr, int d, const Cand *__restrict__ cand,
+                                        const int32_t *__restrict__ empty_ids, const F *__restrict__ C_old,
+                                        F *__restrict__ C_new, double *__restrict__ shift_part, LoopState *st) {
+    if (is_done(st)) return;
+    const int ne = st->n_empty;
+    __shared__ double red[32];
+    for (int e = blockIdx.x; e < ne; e += gridDim.x) {
+        const int id = empty_ids[e];
+        const long long row = cand[e].row;
+        F *c = C_new + (int64_t)id * d;
+        for (int t = threadIdx.x; t < d; t += blockDim.x) c[t] = F(0);
+        __syncthreads();
+        for (int64_t x = rowptr[row] + threadIdx.x; x < rowptr[row + 1]; x += blockDim.x) c[cols[x]] = vals[x];
+        __syncthreads();
+        double acc = 0.0;
+        for (int t = threadIdx.x; t < d; t += blockDim.x) {
+            const double df = (double)C_old[(int64_t)id * d + t] - (double)c[t];
+            acc += df * df;
+        }
+        for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+            shift_part[id] = tot;
+        }
+        __syncthreads();
+    }
+}
+
 // After reseeding: shift = sum of all parts in a fixed order (single block).
 __global__ void shift_total_kernel(const double *__restrict__ shift_part, int k, LoopState *st) {
     if (is_done(st) || st->n_empty == 0) return;
@@ -755,7 +821,7 @@ bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize) {
 
 // Stable counting sort of rows by label + FP64 piece sums (records).
 static void sort_and_sum_pieces(const void *Xv, size_t fsize, const UpdatePlan &p, const int32_t *labels,
-                                Workspace &ws, const LoopState *st, cudaStream_t s) {
+                                Workspace &ws, const LoopState *st, cudaStream_t s, const CsrRows *csr = nullptr) {
     const int k = (int)p.k;
     const int64_t n_groups = (p.n_chunks + kGroupChunks - 1) / kGroupChunks;
     int32_t *H = (int32_t *)ws.H.ptr;
@@ -791,7 +857,18 @@ static void sort_and_sum_pieces(const void *Xv, size_t fsize, const UpdatePlan &
         KMB_LAUNCHED();
     }
     double *records = (double *)ws.records.ptr;
-    if (fsize == sizeof(float)) {
+    if (csr) {
+        const unsigned grid = (unsigned)((p.max_pieces + 3) / 4);
+        if (fsize == sizeof(float))
+            csr_segsum_kernel<float><<<grid, 128, 0, s>>>((const float *)csr->vals, csr->cols, csr->rowptr, (int)p.d,
+                                                          k, perm, offsets, piece_base, p.piece_rows, p.max_pieces,
+                                                          records, st);
+        else
+            csr_segsum_kernel<double><<<grid, 128, 0, s>>>((const double *)csr->vals, csr->cols, csr->rowptr,
+                                                           (int)p.d, k, perm, offsets, piece_base, p.piece_rows,
+                                                           p.max_pieces, records, st);
+        KMB_LAUNCHED();
+    } else if (fsize == sizeof(float)) {
         segsum_kernel<float><<<(unsigned)p.max_pieces, 128, 0, s>>>((const float *)Xv, (int)p.d, k, perm, offsets,
             piece_base, p.piece_rows, records, st);
         KMB_LAUNCHED();
@@ -804,9 +881,9 @@ static void sort_and_sum_pieces(const void *Xv, size_t fsize, const UpdatePlan &
 
 template <typename F>
 void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *C_old, F *C_new,
-                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s) {
+                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr) {
     const int k = (int)p.k, d = (int)p.d;
-    sort_and_sum_pieces(X, sizeof(F), p, labels, ws, st, s);
+    sort_and_sum_pieces(X, sizeof(F), p, labels, ws, st, s, csr);
     double *shift_part = (double *)ws.shift_part.ptr;
     int32_t *empty_flag = (int32_t *)ws.empty_flag.ptr;
     int32_t *empty_ids = (int32_t *)ws.empty_ids.ptr;
@@ -832,7 +909,11 @@ void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const
     KMB_LAUNCHED();
     sel_sort_kernel<<<1, 1024, 0, s>>>(cand, st);
     KMB_LAUNCHED();
-    reseed_apply_kernel<F><<<std::min(k, 1024), 128, 0, s>>>(X, d, cand, empty_ids, C_old, C_new, shift_part, st);
+    if (csr)
+        csr_reseed_apply_kernel<F><<<std::min(k, 1024), 128, 0, s>>>((const F *)csr->vals, csr->cols, csr->rowptr, d,
+                                                                     cand, empty_ids, C_old, C_new, shift_part, st);
+    else
+        reseed_apply_kernel<F><<<std::min(k, 1024), 128, 0, s>>>(X, d, cand, empty_ids, C_old, C_new, shift_part, st);
     KMB_LAUNCHED();
     shift_total_kernel<<<1, 1024, 0, s>>>(shift_part, k, st);
     KMB_LAUNCHED();
@@ -896,7 +977,7 @@ template void launch_sum_values<double>(const double *, int64_t, double *, doubl
 
 #define KMB_INST(F)                                                                                                 \
     template void launch_update<F>(const F *, const UpdatePlan &, const int32_t *, const F *, F *, F *, Workspace &, \
-                                   LoopState *, bool, cudaStream_t);                                               \
+                                   LoopState *, bool, cudaStream_t, const CsrRows *);                              \
     template void launch_partial_sums<F>(const F *, const UpdatePlan &, const int32_t *, double *, int64_t *,       \
                                          Workspace &, cudaStream_t);                                               \
     template void launch_objective<F>(const F *, int64_t, int64_t, const F *, const int32_t *, double *, double *, \

@@ -177,6 +177,86 @@ class descriptor:
         return self
 
 
+class sparse_indexing:
+    """oneapi::dal::sparse_indexing (table/common.hpp:37)."""
+    zero_based = 0
+    one_based = 1
+
+
+class csr_table:
+    """oneapi::dal::csr_table (table/csr.hpp:55-70): values, column_indices, row_offsets
+    (row_count + 1 entries), row_count, column_count and the index base (one_based by
+    default, as csr_table::wrap). Arrays are numpy (host) or torch CUDA tensors
+    (device); indices are int64. Column indices must increase strictly within a row."""
+
+    def __init__(self, data, column_indices, row_offsets, row_count, column_count,
+                 indexing=sparse_indexing.one_based):
+        self.data = data
+        self.column_indices = column_indices
+        self.row_offsets = row_offsets
+        self.row_count = int(row_count)
+        self.column_count = int(column_count)
+        self.indexing = int(indexing)
+        if self.indexing not in (sparse_indexing.zero_based, sparse_indexing.one_based):
+            raise invalid_argument("unknown sparse indexing")
+
+    @classmethod
+    def from_scipy(cls, m):
+        """From a scipy.sparse matrix (canonical CSR: sorted, no duplicates), zero-based."""
+        m = m.tocsr()
+        m.sum_duplicates()
+        m.sort_indices()
+        return cls(m.data, m.indices.astype(np.int64), m.indptr.astype(np.int64), m.shape[0], m.shape[1],
+                   sparse_indexing.zero_based)
+
+    @property
+    def shape(self):
+        return (self.row_count, self.column_count)
+
+    def to_dense(self):
+        """Dense row-major copy (host numpy)."""
+        base = self.indexing
+        v = _to_numpy(self.data)
+        c = _to_numpy(self.column_indices).astype(np.int64) - base
+        r = _to_numpy(self.row_offsets).astype(np.int64) - base
+        out = np.zeros((self.row_count, self.column_count), v.dtype)
+        for i in range(self.row_count):
+            out[i, c[r[i]:r[i + 1]]] = v[r[i]:r[i + 1]]
+        return out
+
+
+def _to_numpy(a):
+    if _is_torch_cuda(a):
+        return a.cpu().numpy()
+    return np.asarray(a)
+
+
+def _as_csr(t, dtype):
+    """(values, column_indices, row_offsets, on_device) of a csr_table in the descriptor's type."""
+    if not isinstance(t, csr_table):
+        try:
+            import scipy.sparse as sp
+            if sp.issparse(t):
+                t = csr_table.from_scipy(t)
+        except ImportError:
+            pass
+    if not isinstance(t, csr_table):
+        raise invalid_argument("method::lloyd_csr takes a csr_table")
+    if _is_torch_cuda(t.data):
+        import torch
+        tdt = torch.float32 if dtype == np.float32 else torch.float64
+        vals = t.data.to(tdt).contiguous()
+        cols = t.column_indices.to(torch.int64).contiguous()
+        offs = t.row_offsets.to(torch.int64).contiguous()
+        return t, vals, cols, offs, True
+    vals = np.ascontiguousarray(t.data, dtype=dtype)
+    cols = np.ascontiguousarray(t.column_indices, dtype=np.int64)
+    offs = np.ascontiguousarray(t.row_offsets, dtype=np.int64)
+    if len(offs) != t.row_count + 1:
+        raise invalid_argument("row_offsets must hold row_count + 1 entries")
+    return t, vals, cols, offs, False
+
+
 class model:
     """kmeans::model (common.hpp:244-278)."""
 
@@ -413,10 +493,96 @@ def init_plusplus(data, cluster_count: int, float_type=np.float32, seed: int = 7
     return C
 
 
+def _train_csr(desc, data, initial_centroids):
+    """method::lloyd_csr (kmb_train_csr): CSR rows, dense centroids."""
+    t, vals, cols, offs, dev = _as_csr(data, desc.float_type)
+    n, d = t.shape
+    k = desc.get_cluster_count()
+    if n <= 0 or d <= 0:
+        raise invalid_argument(_msg.input_data_is_empty)
+    if k > n:
+        raise invalid_argument(_msg.cluster_count_exceeds_data_row_count)
+    if not _has_data(initial_centroids):
+        raise invalid_argument("method::lloyd_csr on this path requires initial centroids")
+    C0, dev_c = _as_table(initial_centroids, desc.float_type)
+    if dev != dev_c:
+        raise invalid_argument("data and initial centroids must live in the same memory space")
+    if C0.shape[0] != k:
+        raise invalid_argument(_msg.init_rc_neq_cluster_count)
+    if C0.shape[1] != d:
+        raise invalid_argument(_msg.init_cc_neq_data_cc)
+    ctx = _native.context(_device_of(vals) if dev else 0)
+    if dev:
+        import torch
+        C = torch.empty_like(C0)
+        labels = torch.empty(n, dtype=torch.int32, device=vals.device)
+        ctx.set_stream(torch.cuda.current_stream(vals.device).cuda_stream)
+    else:
+        C = np.empty_like(C0)
+        labels = np.empty(n, np.int32)
+    params = _native.kmb_params(k, desc.get_max_iteration_count(), desc.get_accuracy_threshold(),
+                                _native.KMB_FORM_PLAIN, 0)
+    obj, it, stats = ctypes.c_double(0.0), ctypes.c_int64(0), _native.kmb_stats()
+    dtype = _native.KMB_F32 if desc.float_type == np.float32 else _native.KMB_F64
+    mem = _native.KMB_MEM_DEVICE if dev else _native.KMB_MEM_HOST
+    try:
+        ctx.check(ctx.lib.kmb_train_csr(ctx.handle, dtype, mem, _ptr(vals, dev), _ptr(cols, dev), _ptr(offs, dev),
+                                        n, d, t.indexing, _ptr(C0, dev), ctypes.byref(params), _ptr(C, dev),
+                                        _ptr(labels, dev), ctypes.byref(obj), ctypes.byref(it), ctypes.byref(stats)))
+    except _native.NativeError as e:
+        _raise_native(e)
+    r = train_result()
+    r._model = model(C)
+    r._responses = labels.reshape(n, 1)
+    r._iteration_count = int(it.value)
+    r._objective = float(obj.value)
+    r.stats = stats
+    return r
+
+
+def _infer_csr(desc, mdl, data):
+    t, vals, cols, offs, dev = _as_csr(data, desc.float_type)
+    n, d = t.shape
+    if not mdl.has_centroids():
+        raise invalid_argument(_msg.model_centroids_are_empty)
+    C, dev_c = _as_table(mdl.get_centroids(), desc.float_type)
+    if dev != dev_c:
+        raise invalid_argument("data and model centroids must live in the same memory space")
+    if C.shape[0] != desc.get_cluster_count():
+        raise invalid_argument(_msg.model_rc_neq_cluster_count)
+    if C.shape[1] != d:
+        raise invalid_argument(_msg.model_cc_neq_data_cc)
+    k = C.shape[0]
+    want_obj = desc.get_result_options().test(result_options.compute_exact_objective_function)
+    ctx = _native.context(_device_of(vals) if dev else 0)
+    if dev:
+        import torch
+        labels = torch.empty(n, dtype=torch.int32, device=vals.device)
+        ctx.set_stream(torch.cuda.current_stream(vals.device).cuda_stream)
+    else:
+        labels = np.empty(n, np.int32)
+    obj = ctypes.c_double(0.0)
+    dtype = _native.KMB_F32 if desc.float_type == np.float32 else _native.KMB_F64
+    mem = _native.KMB_MEM_DEVICE if dev else _native.KMB_MEM_HOST
+    try:
+        ctx.check(ctx.lib.kmb_infer_csr(ctx.handle, dtype, mem, _ptr(vals, dev), _ptr(cols, dev), _ptr(offs, dev), n,
+                                        d, t.indexing, _ptr(C, dev), k, int(want_obj), _ptr(labels, dev),
+                                        ctypes.byref(obj)))
+    except _native.NativeError as e:
+        _raise_native(e)
+    r = infer_result(desc.get_result_options())
+    r._responses = labels.reshape(n, 1)
+    if want_obj:
+        r._set_objective(float(obj.value))
+    return r
+
+
 def train(desc: descriptor, data, initial_centroids=None) -> train_result:
-    """dal::train(desc, data, initial_centroids) for method lloyd_dense (train.hpp:26-29)."""
+    """dal::train(desc, data, initial_centroids) for method lloyd_dense and lloyd_csr (train.hpp:26-29)."""
+    if desc.method == method.lloyd_csr:
+        return _train_csr(desc, data, initial_centroids)
     if desc.method != method.lloyd_dense:
-        raise invalid_argument("only method::lloyd_dense is implemented on this path")
+        raise invalid_argument("unknown method")
     _check_train_preconditions(desc, data, initial_centroids)
     X, dev = _as_table(data, desc.float_type)
     n, d = X.shape
@@ -463,9 +629,11 @@ def train(desc: descriptor, data, initial_centroids=None) -> train_result:
 
 
 def infer(desc: descriptor, mdl: model, data) -> infer_result:
-    """dal::infer(desc, model, data) for method lloyd_dense (infer.hpp)."""
+    """dal::infer(desc, model, data) for method lloyd_dense and lloyd_csr (infer.hpp)."""
+    if desc.method == method.lloyd_csr:
+        return _infer_csr(desc, mdl, data)
     if desc.method != method.lloyd_dense:
-        raise invalid_argument("only method::lloyd_dense is implemented on this path")
+        raise invalid_argument("unknown method")
     _check_infer_preconditions(desc, mdl, data)
     X, dev = _as_table(data, desc.float_type)
     C, dev_c = _as_table(mdl.get_centroids(), desc.float_type)

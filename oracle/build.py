@@ -1,7 +1,7 @@
 """ORACLE -- test infrastructure only. Builds the oracle libraries.
 
-* oracle/_build/libkmeans_oracle.so from oracle/kmeans_oracle.c and
-  oracle/kmeans_init_oracle.cpp (always);
+* oracle/_build/libkmeans_oracle.so from oracle/kmeans_oracle.c,
+  oracle/kmeans_csr_oracle.c and oracle/kmeans_init_oracle.cpp (always);
 * oracle/_ref/libkmeans_daal_ref.so from the reference tree via
   oracle/ref/Makefile, when that tree is present (it is absent on GPU hosts,
   which use the prebuilt library that travels with the working tree).
@@ -17,17 +17,20 @@ REFERENCE_TREE = os.environ.get("ONEDAL_REFERENCE_TREE", "/root/reference")
 
 def build_restated(force: bool = False) -> str:
     src = os.path.join(HERE, "kmeans_oracle.c")
+    src_csr = os.path.join(HERE, "kmeans_csr_oracle.c")
     src_init = os.path.join(HERE, "kmeans_init_oracle.cpp")
-    newest = max(os.path.getmtime(src), os.path.getmtime(src_init))
+    newest = max(os.path.getmtime(src), os.path.getmtime(src_csr), os.path.getmtime(src_init))
     if force or not os.path.exists(RESTATED_LIB) or os.path.getmtime(RESTATED_LIB) < newest:
         out = os.path.dirname(RESTATED_LIB)
         os.makedirs(out, exist_ok=True)
         obj_c, obj_cpp = os.path.join(out, "kmeans_oracle.o"), os.path.join(out, "kmeans_init_oracle.o")
+        obj_csr = os.path.join(out, "kmeans_csr_oracle.o")
         subprocess.check_call(["gcc", "-O2", "-fopenmp", "-fPIC", "-std=c11", "-c", "-o", obj_c, src])
+        subprocess.check_call(["gcc", "-O2", "-fopenmp", "-fPIC", "-std=c11", "-c", "-o", obj_csr, src_csr])
         # strict IEEE arithmetic; the FMA the restatement needs is written explicitly
         subprocess.check_call(["g++", "-O2", "-fPIC", "-std=c++17", "-ffp-contract=off", "-c", "-o", obj_cpp,
                                src_init])
-        subprocess.check_call(["g++", "-fopenmp", "-shared", "-o", RESTATED_LIB, obj_c, obj_cpp])
+        subprocess.check_call(["g++", "-fopenmp", "-shared", "-o", RESTATED_LIB, obj_c, obj_csr, obj_cpp])
     return RESTATED_LIB
 
 

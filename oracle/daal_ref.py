@@ -49,6 +49,8 @@ def _load():
         _lib.daalref_set_threads.argtypes = [ctypes.c_int]
         for sfx in ("f64", "f32"):
             getattr(_lib, f"daalref_init_plusplus_{sfx}").argtypes = [P, I64, I64, I64, ctypes.c_uint32, P]
+            getattr(_lib, f"daalref_train_csr_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, I64, D, P, P, P, P, P]
+            getattr(_lib, f"daalref_infer_csr_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, ctypes.c_int, P, P, P]
     return _lib
 
 
@@ -113,3 +115,44 @@ def init_plusplus(X, k, seed=777777):
     if rc != 0:
         raise ReferenceError_(rc)
     return C
+
+
+def _csr(vals, cols, rowptr, dtype):
+    return (np.ascontiguousarray(vals, dtype=dtype), np.ascontiguousarray(cols, dtype=np.int64),
+            np.ascontiguousarray(rowptr, dtype=np.int64))
+
+
+def train_csr(vals, cols, rowptr, d, C0, max_iteration_count=100, accuracy_threshold=0.0):
+    """The reference's KMeansBatchKernel<lloydCSR> on zero-based CSR rows.
+    Returns (centroids, responses int32, objective, iteration_count)."""
+    lib = _load()
+    C0 = np.ascontiguousarray(C0)
+    v, c, r = _csr(vals, cols, rowptr, C0.dtype)
+    n, k = len(r) - 1, C0.shape[0]
+    C = np.empty_like(C0)
+    lab = np.empty(n, np.int32)
+    obj = np.zeros(1, C0.dtype)
+    it = np.zeros(1, np.int64)
+    code = np.zeros(1, np.int32)
+    rc = getattr(lib, f"daalref_train_csr_{_sfx(C0.dtype)}")(_p(v), _p(c), _p(r), n, int(d), _p(C0), k,
+                                                             int(max_iteration_count), float(accuracy_threshold), _p(C),
+                                                             _p(lab), _p(obj), _p(it), _p(code))
+    if rc != 0:
+        raise ReferenceError_(int(code[0]))
+    return C, lab, float(obj[0]), int(it[0])
+
+
+def infer_csr(vals, cols, rowptr, d, C, compute_objective=True):
+    """Returns (responses int32, objective or None) from the reference CSR kernel."""
+    lib = _load()
+    C = np.ascontiguousarray(C)
+    v, c, r = _csr(vals, cols, rowptr, C.dtype)
+    n = len(r) - 1
+    lab = np.empty(n, np.int32)
+    obj = np.zeros(1, C.dtype)
+    code = np.zeros(1, np.int32)
+    rc = getattr(lib, f"daalref_infer_csr_{_sfx(C.dtype)}")(_p(v), _p(c), _p(r), n, int(d), _p(C), C.shape[0],
+                                                             int(bool(compute_objective)), _p(lab), _p(obj), _p(code))
+    if rc != 0:
+        raise ReferenceError_(int(code[0]))
+    return lab, (float(obj[0]) if compute_objective else None)

@@ -49,6 +49,10 @@ def _load():
         _lib.kmo_assign_f32_in_f64.argtypes = [P, I64, I64, P, I64, P, P, P]
         for sfx in ("f64", "f32"):
             getattr(_lib, f"kmo_init_plusplus_{sfx}").argtypes = [P, I64, I64, I64, ctypes.c_uint32, ctypes.c_int, P, P]
+            getattr(_lib, f"kmoc_train_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, I64, D, P, P, P, P]
+            getattr(_lib, f"kmoc_infer_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, ctypes.c_int, P, P]
+            getattr(_lib, f"kmoc_step_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, P, P, P, P]
+            getattr(_lib, f"kmoc_assign_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, P, P]
     return _lib
 
 
@@ -169,3 +173,51 @@ def init_plusplus(X, k, seed=777777, fused=True):
         raise NoCandidateRows("fewer than k distinct rows (no row left to sample)")
     _check(rc)
     return C, rows
+
+
+def _csr(vals, cols, rowptr, dtype):
+    return (np.ascontiguousarray(vals, dtype=dtype), np.ascontiguousarray(cols, dtype=np.int64),
+            np.ascontiguousarray(rowptr, dtype=np.int64))
+
+
+def train_csr(vals, cols, rowptr, d, C0, max_iteration_count, accuracy_threshold):
+    """CSR Lloyd (kmeans_csr_oracle.c): zero-based CSR rows (values, column indices,
+    n + 1 row offsets) with d columns. Returns (centroids, responses, objective, iterations)."""
+    C0 = np.ascontiguousarray(C0)
+    v, c, r = _csr(vals, cols, rowptr, C0.dtype)
+    n, k = len(r) - 1, C0.shape[0]
+    C = np.empty_like(C0)
+    lab = np.empty(n, np.int32)
+    obj = np.zeros(1, C0.dtype)
+    it = np.zeros(1, np.int64)
+    lib = _load()
+    _check(getattr(lib, f"kmoc_train_{_sfx(C0.dtype)}")(_p(v), _p(c), _p(r), n, int(d), _p(C0), k,
+                                                       int(max_iteration_count), float(accuracy_threshold), _p(C),
+                                                       _p(lab), _p(obj), _p(it)))
+    return C, lab, float(obj[0]), int(it[0])
+
+
+def infer_csr(vals, cols, rowptr, d, C, compute_objective=True):
+    """Returns (responses int32, objective or None) for CSR rows."""
+    C = np.ascontiguousarray(C)
+    v, c, r = _csr(vals, cols, rowptr, C.dtype)
+    n = len(r) - 1
+    lab = np.empty(n, np.int32)
+    obj = np.zeros(1, C.dtype)
+    _check(getattr(_load(), f"kmoc_infer_{_sfx(C.dtype)}")(_p(v), _p(c), _p(r), n, int(d), _p(C), C.shape[0],
+                                                          int(bool(compute_objective)), _p(lab), _p(obj)))
+    return lab, (float(obj[0]) if compute_objective else None)
+
+
+def step_csr(vals, cols, rowptr, d, C_in):
+    """One CSR Lloyd update: (C_out, labels under C_in, shift, empty count)."""
+    C_in = np.ascontiguousarray(C_in)
+    v, c, r = _csr(vals, cols, rowptr, C_in.dtype)
+    n = len(r) - 1
+    C = np.empty_like(C_in)
+    lab = np.empty(n, np.int32)
+    shift = np.zeros(1, C_in.dtype)
+    ne = np.zeros(1, np.int64)
+    _check(getattr(_load(), f"kmoc_step_{_sfx(C_in.dtype)}")(_p(v), _p(c), _p(r), n, int(d), _p(C_in), C_in.shape[0],
+                                                            _p(C), _p(lab), _p(shift), _p(ne)))
+    return C, lab, float(shift[0]), int(ne[0])

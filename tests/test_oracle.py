@@ -210,3 +210,64 @@ def test_plusplus_smoke_known_answer(dt):
     assert centroid_rel_err(np.array([[-1.5, -1.5], [1.5, 1.5]]), C) < 5 * np.finfo(dt).eps * it * 100
     assert lab.tolist() == [1, 1, 1, 1, 0, 0, 0, 0]
     assert rel_close(obj, 4.0, 1e-6)
+
+
+def _sparse_case(seed, n, d, k, density, dt):
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    M = sp.random(n, d, density=density, format="csr", random_state=seed, dtype=np.float64)
+    M.data = rng.standard_normal(M.nnz) * 3
+    M.sort_indices()
+    C0 = M[rng.choice(n, k, replace=False)].toarray()
+    return M.data.astype(dt), M.indices.astype(np.int64), M.indptr.astype(np.int64), C0.astype(dt)
+
+
+def test_csr_exact_objective_known_answer():
+    """'KMeans CSR exact objective accounts for unstored features' (test/batch.cpp:406-480):
+    3 rows with one stored value each, 2 centroids, 1 iteration: the CSR objective equals
+    the dense one (100), the responses and centroids too."""
+    v = np.array([10, 10, 20.0])
+    c = np.array([0, 1, 2])
+    r = np.array([0, 1, 2, 3])
+    C0 = np.array([[5, 5, 0], [0, 0, 20.0]])
+    dense = np.array([[10, 0, 0], [0, 10, 0], [0, 0, 20.0]])
+    for dt in DTYPES:
+        Cs, ls, os_, its = restated.train_csr(v.astype(dt), c, r, 3, C0.astype(dt), 1, 0.0)
+        Cd, ld, od, itd = restated.train(dense.astype(dt), C0.astype(dt), 1, 0.0)
+        assert (ls == ld).all() and its == itd == 1
+        assert centroid_rel_err(Cd, Cs) < (1e-10 if dt == np.float64 else 1e-5)
+        assert rel_close(os_, 100.0, 1e-6) and rel_close(od, 100.0, 1e-6)
+
+
+@needs_ref
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("seed", range(6))
+def test_csr_restated_equals_reference_kernel(seed, dt):
+    """Live comparison with the reference KMeansBatchKernel<lloydCSR> (single thread):
+    responses and iteration count exact, centroids and objective to rounding."""
+    rng = np.random.default_rng(100 + seed)
+    n, d, k = int(rng.integers(30, 700)), int(rng.integers(4, 150)), int(rng.integers(2, 30))
+    v, c, r, C0 = _sparse_case(seed, n, d, k, float(rng.uniform(0.03, 0.3)), dt)
+    daal_ref.set_threads(1)
+    a = restated.train_csr(v, c, r, d, C0, 25, 0.0)
+    b = daal_ref.train_csr(v, c, r, d, C0, 25, 0.0)
+    assert (a[1] == b[1]).all() and a[3] == b[3]
+    tol = 1e-12 if dt == np.float64 else 1e-5
+    assert centroid_rel_err(b[0], a[0]) < tol
+    assert rel_close(a[2], b[2], tol)
+    la, oa = restated.infer_csr(v, c, r, d, a[0], True)
+    lb, ob = daal_ref.infer_csr(v, c, r, d, a[0], True)
+    assert (la == lb).all() and rel_close(oa, ob, tol)
+
+
+@needs_ref
+def test_csr_reference_reseeds_empty_clusters_like_restatement():
+    """Duplicate initial centroids force empty clusters; the reseeded centers (farthest
+    rows expanded to dense) agree."""
+    v, c, r, C0 = _sparse_case(42, 300, 40, 12, 0.1, np.float64)
+    C0[5:] = C0[0]
+    daal_ref.set_threads(1)
+    a = restated.train_csr(v, c, r, 40, C0, 10, 0.0)
+    b = daal_ref.train_csr(v, c, r, 40, C0, 10, 0.0)
+    assert (a[1] == b[1]).all() and a[3] == b[3]
+    assert centroid_rel_err(b[0], a[0]) < 1e-12
