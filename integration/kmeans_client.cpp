@@ -20,6 +20,7 @@
 #include "oneapi/dal/algo/kmeans.hpp"
 #include "oneapi/dal/detail/archives.hpp"
 #include "oneapi/dal/detail/serialization.hpp"
+#include "oneapi/dal/table/csr.hpp"
 #include "oneapi/dal/table/homogen.hpp"
 #include "oneapi/dal/table/row_accessor.hpp"
 
@@ -73,6 +74,25 @@ int run(const std::vector<double> &xs, std::int64_t n, std::int64_t d, const std
     std::printf("smoke_responses");
     for (std::int64_t i = 0; i < sr.get_count(); ++i) std::printf(" %d", sr[i]);
     std::printf("\n");
+    // 'KMeans CSR exact objective accounts for unstored features' (test/batch.cpp:406-480)
+    // through dal::train / dal::infer on a one-based csr_table
+    const F cv[] = { 10, 10, 20 };
+    const std::int64_t ci[] = { 1, 2, 3 }, ro[] = { 1, 2, 3, 4 };
+    const F cinit[] = { 5, 5, 0, 0, 0, 20 };
+    const auto csr = dal::csr_table::wrap(cv, ci, ro, 3, 3, dal::sparse_indexing::one_based);
+    const auto csr_desc = dal::kmeans::descriptor<F, dal::kmeans::method::lloyd_csr>()
+                              .set_cluster_count(2)
+                              .set_max_iteration_count(1)
+                              .set_accuracy_threshold(0.0)
+                              .set_result_options(dal::kmeans::result_options::compute_exact_objective_function);
+    const auto csr_res = dal::train(csr_desc, csr, dal::homogen_table::wrap(cinit, 2, 3));
+    const auto crr = dal::row_accessor<const std::int32_t>(csr_res.get_responses()).pull({ 0, -1 });
+    std::printf("csr_responses");
+    for (std::int64_t i = 0; i < crr.get_count(); ++i) std::printf(" %d", crr[i]);
+    std::printf("\n");
+    std::printf("csr_objective %.10g\n", csr_res.get_objective_function_value());
+    const auto csr_inf = dal::infer(csr_desc, csr_res.get_model(), csr);
+    std::printf("csr_infer_objective %.10g\n", csr_inf.get_objective_function_value());
     return 0;
 }
 

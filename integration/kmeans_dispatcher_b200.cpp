@@ -9,6 +9,7 @@
 #include "oneapi/dal/detail/common.hpp"
 #include "oneapi/dal/detail/policy.hpp"
 #include "oneapi/dal/exceptions.hpp"
+#include "oneapi/dal/table/csr_accessor.hpp"
 #include "oneapi/dal/table/homogen.hpp"
 #include "oneapi/dal/table/row_accessor.hpp"
 
@@ -120,6 +121,80 @@ struct infer_ops_dispatcher<dal::detail::host_policy, F, method::lloyd_dense, ta
         return result;
     }
 };
+
+// method::lloyd_csr: the data table is a csr_table, pulled zero-based; centroids
+// stay dense (detail/train_ops.cpp:41-42, detail/infer_ops.cpp:42-43).
+template <typename F>
+struct train_ops_dispatcher<dal::detail::host_policy, F, method::lloyd_csr, task::clustering> {
+    train_result<task::clustering> operator()(const dal::detail::host_policy &,
+                                              const descriptor_base<task::clustering> &desc,
+                                              const train_input<task::clustering> &input) const {
+        const table &data = input.get_data();
+        const std::int64_t n = data.get_row_count();
+        const std::int64_t d = data.get_column_count();
+        const std::int64_t k = desc.get_cluster_count();
+        if (!input.get_initial_centroids().has_data()) {
+            // the CSR k-means++ initialisation is not on this path
+            throw unimplemented(dal::detail::error_messages::method_not_implemented());
+        }
+        if (data.get_kind() != csr_table::kind()) throw invalid_argument("method::lloyd_csr takes a csr_table");
+        const auto [vals, cols, offs] =
+            csr_accessor<const F>(static_cast<const csr_table &>(data)).pull({ 0, -1 }, sparse_indexing::zero_based);
+        const auto c0 = row_accessor<const F>(input.get_initial_centroids()).pull({ 0, -1 });
+        auto centroids = array<F>::empty(k * d);
+        auto responses = array<std::int32_t>::empty(n);
+        kmb_params p{ k, desc.get_max_iteration_count(), desc.get_accuracy_threshold(), KMB_FORM_PLAIN, 0 };
+        double objective = 0.0;
+        std::int64_t iterations = 0;
+        kmb_context *ctx = thread_context();
+        check(ctx, kmb_train_csr(ctx, dtype_of<F>, KMB_MEM_HOST, vals.get_data(), cols.get_data(), offs.get_data(),
+                                 n, d, 0, c0.get_data(), &p, centroids.get_mutable_data(),
+                                 responses.get_mutable_data(), &objective, &iterations, nullptr));
+        return train_result<task::clustering>{}
+            .set_model(model<task::clustering>{}.set_centroids(
+                dal::detail::homogen_table_builder{}.reset(centroids, k, d).build()))
+            .set_responses(dal::detail::homogen_table_builder{}.reset(responses, n, 1).build())
+            .set_iteration_count(iterations)
+            .set_objective_function_value(objective);
+    }
+};
+
+template <typename F>
+struct infer_ops_dispatcher<dal::detail::host_policy, F, method::lloyd_csr, task::clustering> {
+    infer_result<task::clustering> operator()(const dal::detail::host_policy &,
+                                              const descriptor_base<task::clustering> &desc,
+                                              const infer_input<task::clustering> &input) const {
+        const table &data = input.get_data();
+        const table &c = input.get_model().get_centroids();
+        const std::int64_t n = data.get_row_count();
+        const std::int64_t d = data.get_column_count();
+        const std::int64_t k = c.get_row_count();
+        if (data.get_kind() != csr_table::kind()) throw invalid_argument("method::lloyd_csr takes a csr_table");
+        const auto [vals, cols, offs] =
+            csr_accessor<const F>(static_cast<const csr_table &>(data)).pull({ 0, -1 }, sparse_indexing::zero_based);
+        const auto cc = row_accessor<const F>(c).pull({ 0, -1 });
+        const bool want_obj =
+            desc.get_result_options().test(result_options::compute_exact_objective_function);
+        auto responses = array<std::int32_t>::empty(n);
+        double objective = 0.0;
+        kmb_context *ctx = thread_context();
+        check(ctx, kmb_infer_csr(ctx, dtype_of<F>, KMB_MEM_HOST, vals.get_data(), cols.get_data(), offs.get_data(), n,
+                                 d, 0, cc.get_data(), k, want_obj ? 1 : 0, responses.get_mutable_data(), &objective));
+        auto result = infer_result<task::clustering>{}.set_result_options(desc.get_result_options());
+        result.set_responses(dal::detail::homogen_table_builder{}.reset(responses, n, 1).build());
+        if (want_obj) result.set_objective_function_value(objective);
+        return result;
+    }
+};
+
+template struct ONEDAL_EXPORT
+    train_ops_dispatcher<dal::detail::host_policy, float, method::lloyd_csr, task::clustering>;
+template struct ONEDAL_EXPORT
+    train_ops_dispatcher<dal::detail::host_policy, double, method::lloyd_csr, task::clustering>;
+template struct ONEDAL_EXPORT
+    infer_ops_dispatcher<dal::detail::host_policy, float, method::lloyd_csr, task::clustering>;
+template struct ONEDAL_EXPORT
+    infer_ops_dispatcher<dal::detail::host_policy, double, method::lloyd_csr, task::clustering>;
 
 template struct ONEDAL_EXPORT
     train_ops_dispatcher<dal::detail::host_policy, float, method::lloyd_dense, task::clustering>;

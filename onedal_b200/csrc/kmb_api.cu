@@ -102,7 +102,8 @@ bool Workspace::ensure(DevBuf &b, size_t bytes) {
 
 void Workspace::release() {
     DevBuf *all[] = {&X, &C0, &Cout, &labels, &d2, &xnorm, &Ccur, &Cnew, &Ct, &h, &queue, &H, &Gs,
-                     &counts, &offsets, &piece_base, &perm, &records, &shift_part, &empty_flag, &empty_ids,
+                     &counts, &offsets, &piece_base, &perm, &records, &shift_part, &shift_tiles, &empty_flag,
+                     &empty_ids,
                      &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx, &rowb, &pp_acc, &pp_rand,
                      &pp_state, &pp_flags, &csr_vals, &csr_cols64, &csr_rowptr64, &csr_cols, &csr_rowptr,
                      &csr_bad, &csr_cnorm};

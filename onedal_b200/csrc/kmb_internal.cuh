@@ -101,7 +101,7 @@ struct Workspace {
     // drains).
     cudaStream_t stream = nullptr;
     DevBuf X, C0, Cout, labels, d2, xnorm, Ccur, Cnew, Ct, h, queue;
-    DevBuf H, Gs, counts, offsets, piece_base, perm, records, shift_part, empty_flag, empty_ids;
+    DevBuf H, Gs, counts, offsets, piece_base, perm, records, shift_part, shift_tiles, empty_flag, empty_ids;
     DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;
     DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb, pp_acc, pp_rand, pp_state, pp_flags;
     DevBuf csr_vals, csr_cols64, csr_rowptr64, csr_cols, csr_rowptr, csr_bad, csr_cnorm;

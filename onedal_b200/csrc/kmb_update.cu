@@ -283,26 +283,46 @@ csr_segsum_kernel(const F *__restrict__ vals, const int32_t *__restrict__ cols, 
     }
 }
 
-// Per cluster: S = sum of its pieces (in order); c = F(S / count); shift part.
+// S[t] = sum over pieces p0..p1-1 of records[p * d + t], added in piece order
+// (four loads in flight per step; the additions stay sequential).
+__device__ __forceinline__ double piece_sum(const double *__restrict__ records, int64_t p0, int64_t p1, int64_t d,
+                                            int t) {
+    double S = 0.0;
+    int64_t p = p0;
+    for (; p + 4 <= p1; p += 4) {
+        const double a = records[p * d + t], b = records[(p + 1) * d + t];
+        const double c = records[(p + 2) * d + t], e = records[(p + 3) * d + t];
+        S += a;
+        S += b;
+        S += c;
+        S += e;
+    }
+    for (; p < p1; ++p) S += records[p * d + t];
+    return S;
+}
+
+constexpr int kFinalizeCols = 128;  // columns per finalize block (one per thread)
+
+// Block (j, tile): S = sum of cluster j's pieces (in order) for the tile's
+// columns; c = F(S / count); the tile's shift part. One large cluster thus
+// spreads over d / 128 blocks instead of serialising on one.
 template <typename F>
-__global__ void finalize_kernel(const double *__restrict__ records, const int64_t *__restrict__ counts,
-                                const int64_t *__restrict__ piece_base, const F *__restrict__ C_old,
-                                F *__restrict__ C_new, int d, double *__restrict__ shift_part,
-                                int32_t *__restrict__ empty_flag, const LoopState *st) {
+__global__ void __launch_bounds__(kFinalizeCols)
+finalize_kernel(const double *__restrict__ records, const int64_t *__restrict__ counts,
+                const int64_t *__restrict__ piece_base, const F *__restrict__ C_old, F *__restrict__ C_new, int d,
+                double *__restrict__ shift_tiles, int32_t *__restrict__ empty_flag, const LoopState *st) {
     if (is_done(st)) return;
-    __shared__ double red[32];
+    __shared__ double red[kFinalizeCols / 32];
     const int j = blockIdx.x;
+    const int t = blockIdx.y * kFinalizeCols + threadIdx.x;
     const int64_t cnt = counts[j];
-    const int64_t p0 = piece_base[j], p1 = piece_base[j + 1];
     double acc = 0.0;
-    for (int t = threadIdx.x; t < d; t += blockDim.x) {
+    if (t < d) {
         const F old = C_old[(int64_t)j * d + t];
         if (cnt > 0) {
-            double S = 0.0;
-            for (int64_t p = p0; p < p1; ++p) S += records[p * d + t];
-            const F c = F(S / (double)cnt);
+            const F c = F(piece_sum(records, piece_base[j], piece_base[j + 1], d, t) / (double)cnt);
             const double df = (double)old - (double)c;
-            acc += df * df;
+            acc = df * df;
             C_new[(int64_t)j * d + t] = c;
         } else {
             C_new[(int64_t)j * d + t] = old;
@@ -313,24 +333,31 @@ __global__ void finalize_kernel(const double *__restrict__ records, const int64_
     __syncthreads();
     if (threadIdx.x == 0) {
         double tot = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
-        shift_part[j] = tot;
-        empty_flag[j] = cnt > 0 ? 0 : 1;
+        for (int w = 0; w < kFinalizeCols / 32; ++w) tot += red[w];
+        shift_tiles[(int64_t)j * gridDim.y + blockIdx.y] = tot;
+        if (blockIdx.y == 0) empty_flag[j] = cnt > 0 ? 0 : 1;
     }
 }
 
-// Sums of the pieces without the division (sharded training).
+// shift_part[j] = the tiles' parts of cluster j, in tile order.
+__global__ void shift_tiles_kernel(const double *__restrict__ shift_tiles, int k, int tiles,
+                                   double *__restrict__ shift_part, const LoopState *st) {
+    if (is_done(st)) return;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int y = 0; y < tiles; ++y) s += shift_tiles[(int64_t)j * tiles + y];
+        shift_part[j] = s;
+    }
+}
+
+// Sums of the pieces without the division (sharded training); block (j, tile).
 __global__ void sums_kernel(const double *__restrict__ records, const int64_t *__restrict__ counts_in,
                             const int64_t *__restrict__ piece_base, int d, double *__restrict__ sums,
                             int64_t *__restrict__ counts_out) {
     const int j = blockIdx.x;
-    const int64_t p0 = piece_base[j], p1 = piece_base[j + 1];
-    for (int t = threadIdx.x; t < d; t += blockDim.x) {
-        double S = 0.0;
-        for (int64_t p = p0; p < p1; ++p) S += records[p * d + t];
-        sums[(int64_t)j * d + t] = S;
-    }
-    if (threadIdx.x == 0) counts_out[j] = counts_in[j];
+    const int t = blockIdx.y * kFinalizeCols + threadIdx.x;
+    if (t < d) sums[(int64_t)j * d + t] = piece_sum(records, piece_base[j], piece_base[j + 1], d, t);
+    if (threadIdx.x == 0 && blockIdx.y == 0) counts_out[j] = counts_in[j];
 }
 
 // Single block: lists empty clusters in ascending order; when none, reduces the
@@ -807,6 +834,7 @@ bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize) {
     ok &= ws.ensure(ws.perm, sizeof(int32_t) * std::max<int64_t>(1, p.n));
     ok &= ws.ensure(ws.records, sizeof(double) * p.max_pieces * p.d);
     ok &= ws.ensure(ws.shift_part, sizeof(double) * p.k);
+    ok &= ws.ensure(ws.shift_tiles, sizeof(double) * p.k * ((p.d + kFinalizeCols - 1) / kFinalizeCols));
     ok &= ws.ensure(ws.empty_flag, sizeof(int32_t) * p.k);
     ok &= ws.ensure(ws.empty_ids, sizeof(int32_t) * p.k);
     ok &= ws.ensure(ws.sel_hist, sizeof(unsigned int) * 256);
@@ -887,9 +915,13 @@ void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const
     double *shift_part = (double *)ws.shift_part.ptr;
     int32_t *empty_flag = (int32_t *)ws.empty_flag.ptr;
     int32_t *empty_ids = (int32_t *)ws.empty_ids.ptr;
-    finalize_kernel<F><<<k, 128, 0, s>>>((const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr,
-                                         (const int64_t *)ws.piece_base.ptr, C_old, C_new, d, shift_part,
-                                         empty_flag, st);
+    const int tiles = (d + kFinalizeCols - 1) / kFinalizeCols;
+    finalize_kernel<F><<<dim3((unsigned)k, (unsigned)tiles), kFinalizeCols, 0, s>>>(
+        (const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr, (const int64_t *)ws.piece_base.ptr, C_old,
+        C_new, d, (double *)ws.shift_tiles.ptr, empty_flag, st);
+    KMB_LAUNCHED();
+    shift_tiles_kernel<<<(unsigned)std::min(148, (k + 255) / 256), 256, 0, s>>>((const double *)ws.shift_tiles.ptr, k,
+                                                                              tiles, shift_part, st);
     KMB_LAUNCHED();
     empties_kernel<<<1, 1024, 0, s>>>(empty_flag, k, empty_ids, shift_part, st);
     KMB_LAUNCHED();
@@ -930,7 +962,8 @@ template <typename F>
 void launch_partial_sums(const F *X, const UpdatePlan &p, const int32_t *labels, double *sums, int64_t *counts,
                          Workspace &ws, cudaStream_t s) {
     sort_and_sum_pieces(X, sizeof(F), p, labels, ws, nullptr, s);
-    sums_kernel<<<(unsigned)p.k, 128, 0, s>>>((const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr,
+    sums_kernel<<<dim3((unsigned)p.k, (unsigned)((p.d + kFinalizeCols - 1) / kFinalizeCols)), kFinalizeCols, 0, s>>>(
+        (const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr,
                                              (const int64_t *)ws.piece_base.ptr, (int)p.d, sums, counts);
     KMB_LAUNCHED();
 }

@@ -82,3 +82,7 @@ def test_client_gold_through_dal_train_infer(tmp_path, dtype, rtol):
     sc = np.array(out["smoke_centroids"].split(), np.float64).reshape(2, 2)
     assert centroid_rel_err(np.array([[-1.5, -1.5], [1.5, 1.5]]), sc) < rtol
     assert out["smoke_responses"].split() == ["1", "1", "1", "1", "0", "0", "0", "0"]
+    # method::lloyd_csr on a one-based csr_table (test/batch.cpp:406-480): objective 100
+    assert out["csr_responses"].split() == ["0", "0", "1"]
+    assert rel_close(float(out["csr_objective"]), 100.0, rtol)
+    assert rel_close(float(out["csr_infer_objective"]), 100.0, rtol)
