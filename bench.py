@@ -154,6 +154,74 @@ def run_plusplus(args, X, ctx):
     return out
 
 
+def run_csr(args, ctx):
+    """method::lloyd_csr on a synthetic sparse workload held in HBM: n = 2M rows,
+    d = 20,000 columns, 64 stored entries per row (uniform columns, one per
+    312-column stripe, N(0, 1) values), k = 256 centroids started from k rows,
+    float32, 10 iterations (eps 0). Reports Lloyd iterations/s of the whole train
+    call (the final responses pass and objective included), the assignment
+    kernel's FLOP rate and its centroid-gather bytes, and the CSR oracle port on a
+    20,000-row sample on the host cores, scaled by rows."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from onedal_b200 import _native, kmeans
+    n, d, per, k, T = args.csr_rows, 20000, 64, 256, 10
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    stripe = d // per
+    cols = (torch.randint(0, stripe, (n, per), device="cuda", generator=g)
+            + torch.arange(per, device="cuda") * stripe).to(torch.int64).reshape(-1)
+    vals = torch.randn(n * per, device="cuda", generator=g, dtype=torch.float32)
+    offs = torch.arange(0, n * per + 1, per, device="cuda", dtype=torch.int64)
+    table = kmeans.csr_table(vals, cols, offs, n, d, kmeans.sparse_indexing.zero_based)
+    pick = torch.randperm(n, device="cuda", generator=g)[:k]
+    C0 = torch.zeros((k, d), device="cuda")
+    rows_idx = (pick[:, None] * per + torch.arange(per, device="cuda")[None, :]).reshape(-1)
+    C0[torch.arange(k, device="cuda").repeat_interleave(per), cols[rows_idx]] = vals[rows_idx]
+    desc = kmeans.descriptor(np.float32, kmeans.method.lloyd_csr).set_cluster_count(k).set_max_iteration_count(T)
+    kmeans.train(desc.set_max_iteration_count(1), table, C0)  # warm-up
+    desc.set_max_iteration_count(T)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.check(ctx.lib.kmb_context_set_kernel_timing(ctx.handle, 1))
+    e0.record(stream)
+    r = kmeans.train(desc, table, C0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    kt, kl = ctypes.c_double(), ctypes.c_int64()
+    ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 0, ctypes.byref(kt), ctypes.byref(kl)))
+    ut, ul = ctypes.c_double(), ctypes.c_int64()
+    ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 2, ctypes.byref(ut), ctypes.byref(ul)))
+    ctx.check(ctx.lib.kmb_context_set_kernel_timing(ctx.handle, 0))
+    s = e0.elapsed_time(e1) / 1e3
+    it = r.get_iteration_count()
+    assign_ms = kt.value / max(kl.value, 1)
+    nnz = n * per
+    out = {"metric": "CSR Lloyd iter/s", "value": it / s, "unit": "iter/s", "iterations": it, "seconds": s,
+           "config": {"workload": f"synthetic CSR n={n} d={d} {per} stored entries per row, k={k}, float32",
+                      "nnz": nnz},
+           "assign_ms_avg": assign_ms, "update_ms_avg": ut.value / max(ul.value, 1),
+           "assign_tflops": 2.0 * nnz * k / (assign_ms / 1e3) / 1e12,
+           "assign_centroid_gather_gbs": nnz * k * 4 / (assign_ms / 1e3) / 1e9}
+    if args.cpu_sample_rows > 0:
+        from oracle import restated
+        ns = 20000
+        v = vals[:ns * per].cpu().numpy()
+        c = cols[:ns * per].cpu().numpy()
+        o = offs[:ns + 1].cpu().numpy()
+        t0 = time.perf_counter()
+        _, _, _, itc = restated.train_csr(v, c, o, d, C0.cpu().numpy(), 2, 0.0)
+        per_iter = (time.perf_counter() - t0) / 3 * (n / ns)  # 2 updates + the final pass
+        out["cpu_baseline"] = {"value": 1.0 / per_iter, "unit": "iter/s", "cores": os.cpu_count(), "kind": "port",
+                               "sample": f"CSR oracle (OpenMP) on the first {ns} of {n} rows, 2 iterations + final "
+                                         f"pass, per-pass time scaled by rows"}
+    return out
+
+
 def make_workload(device, n=None):
     import torch
     from onedal_b200 import workloads
@@ -571,6 +639,9 @@ def run_b200(args):
     plusplus = None
     if rank == 0 and world == 1 and args.plusplus_k > 1:
         plusplus = run_plusplus(args, X, ctx)
+    csr = None
+    if rank == 0 and world == 1 and args.csr_rows > 0:
+        csr = run_csr(args, ctx)
 
     batched = None
     if rank == 0 and world == 1 and args.batched_problems > 0:
@@ -600,6 +671,7 @@ def run_b200(args):
             "serving": serving,
             "batched": batched,
             "plusplus": plusplus,
+            "csr": csr,
         }
         print(json.dumps(line))
     if dist:
@@ -621,6 +693,8 @@ def main():
                     help="problems in the batched-form measurement (0 skips it)")
     ap.add_argument("--serving-requests", type=int, default=3000,
                     help="requests per serving load point (0 skips the serving measurement)")
+    ap.add_argument("--csr-rows", type=int, default=2_000_000,
+                    help="rows of the CSR (lloyd_csr) measurement (0 skips it)")
     ap.add_argument("--plusplus-k", type=int, default=1024,
                     help="centers of the k-means++ initialisation measurement (0 skips it)")
     ap.add_argument("--rows", type=int, default=None,

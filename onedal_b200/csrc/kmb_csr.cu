@@ -49,7 +49,9 @@ __global__ void csr_prepare_kernel(const int64_t *__restrict__ cols_in, const in
     }
 }
 
-template <typename F, int T>
+// G entries are gathered before any of them is folded, so G * T loads per lane
+// are in flight (the folds stay in entry order per accumulator).
+template <typename F, int T, int G>
 __global__ void __launch_bounds__(256) csr_assign_kernel(const F *__restrict__ vals, const int32_t *__restrict__ cols,
                                                          const int64_t *__restrict__ rowptr, int64_t n,
                                                          const F *__restrict__ Ct, const F *__restrict__ h, int kpad,
@@ -71,13 +73,23 @@ __global__ void __launch_bounds__(256) csr_assign_kernel(const F *__restrict__ v
                 const F v = e < re ? vals[e] : F(0);
                 const int col = e < re ? cols[e] : 0;
                 const int cnt = (int)min((int64_t)32, re - e0);
-                for (int q = 0; q < cnt; ++q) {
-                    const F vq = __shfl_sync(0xffffffffu, v, q);
-                    const int cq = __shfl_sync(0xffffffffu, col, q);
-                    const F *crow = Ct + (int64_t)cq * kpad + c0 + lane;
+                for (int q = 0; q < cnt; q += G) {
+                    F vq[G], x[G][T];
 #pragma unroll
-                    for (int t = 0; t < T; ++t)
-                        if (c0 + 32 * t < kpad) acc[t] = fma(vq, crow[32 * t], acc[t]);
+                    for (int g = 0; g < G; ++g) {
+                        // entries past the row's end fold 0 * (a valid centroid value): no change
+                        const int qq = (q + g) & 31;
+                        const F vg = __shfl_sync(0xffffffffu, v, qq);
+                        const int cg = __shfl_sync(0xffffffffu, col, qq);
+                        vq[g] = q + g < cnt ? vg : F(0);
+                        const F *crow = Ct + (int64_t)(q + g < cnt ? cg : 0) * kpad + c0 + lane;
+#pragma unroll
+                        for (int t = 0; t < T; ++t) x[g][t] = c0 + 32 * t < kpad ? crow[32 * t] : F(0);
+                    }
+#pragma unroll
+                    for (int g = 0; g < G; ++g)
+#pragma unroll
+                        for (int t = 0; t < T; ++t) acc[t] = fma(vq[g], x[g][t], acc[t]);
                 }
             }
 #pragma unroll
@@ -172,8 +184,9 @@ __global__ void csr_sum_partials_kernel(const double *__restrict__ partials, int
 template <typename F, int T>
 void assign_t(const CsrRows &X, const F *Ct, const F *h, int64_t kpad, int32_t *labels, F *d2, const LoopState *st,
               cudaStream_t s) {
+    constexpr int G = T <= 8 ? 4 : (T <= 16 ? 2 : 1);
     const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((X.n + 7) / 8, 148 * 8));
-    csr_assign_kernel<F, T><<<(unsigned)blocks, 256, 0, s>>>((const F *)X.vals, X.cols, X.rowptr, X.n, Ct, h,
+    csr_assign_kernel<F, T, G><<<(unsigned)blocks, 256, 0, s>>>((const F *)X.vals, X.cols, X.rowptr, X.n, Ct, h,
                                                              (int)kpad, labels, d2, st);
     KMB_LAUNCHED();
 }
