@@ -134,7 +134,8 @@ KMB_API int kmb_init_plusplus(kmb_context *ctx, int dtype, int memory, const voi
  * increase strictly within each row. Centroids are dense (k x d). Scores are the
  * sparse product over the stored entries; the objective is the reference's CSR
  * form (per row: sum over stored entries of x^2 - 2xc, plus ||c||^2, clipped at
- * zero). Train takes the plain form only and requires initial centroids. */
+ * zero). Train takes the plain form only and requires initial centroids (a caller
+ * without them first runs kmb_init_plusplus_csr, as oneDAL's train() does). */
 KMB_API int kmb_train_csr(kmb_context *ctx, int dtype, int memory, const void *values, const int64_t *col_indices,
                           const int64_t *row_offsets, int64_t n, int64_t d, int32_t indexing, const void *C0,
                           const kmb_params *params, void *C_out, int32_t *responses, double *objective,
@@ -142,6 +143,14 @@ KMB_API int kmb_train_csr(kmb_context *ctx, int dtype, int memory, const void *v
 KMB_API int kmb_infer_csr(kmb_context *ctx, int dtype, int memory, const void *values, const int64_t *col_indices,
                           const int64_t *row_offsets, int64_t n, int64_t d, int32_t indexing, const void *C, int64_t k,
                           int32_t compute_objective, int32_t *responses, double *objective);
+/* The default initialisation of train() with method::lloyd_csr and no initial
+ * centroids: DAAL plusPlusCSR, one trial (detail/train_init_centroids.hpp:39-74,
+ * kmeans_plusplus_init_impl.i:244-316): the sampling of kmb_init_plusplus with the
+ * CSR distance ||c||^2 + sum over stored entries of (x*x - 2*x*c), each operation
+ * rounded as written. C_out: k x d dense centers, host or device per `memory`. */
+KMB_API int kmb_init_plusplus_csr(kmb_context *ctx, int dtype, int memory, const void *values,
+                                  const int64_t *col_indices, const int64_t *row_offsets, int64_t n, int64_t d,
+                                  int32_t indexing, int64_t k, uint32_t seed, void *C_out);
 
 /* Model serialisation in oneDAL's binary archive format: the bytes of
  * detail::serialize(kmeans::model<task::clustering>, binary_output_archive)

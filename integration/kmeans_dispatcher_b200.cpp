@@ -133,20 +133,27 @@ struct train_ops_dispatcher<dal::detail::host_policy, F, method::lloyd_csr, task
         const std::int64_t n = data.get_row_count();
         const std::int64_t d = data.get_column_count();
         const std::int64_t k = desc.get_cluster_count();
-        if (!input.get_initial_centroids().has_data()) {
-            // the CSR k-means++ initialisation is not on this path
-            throw unimplemented(dal::detail::error_messages::method_not_implemented());
-        }
         if (data.get_kind() != csr_table::kind()) throw invalid_argument("method::lloyd_csr takes a csr_table");
         const auto [vals, cols, offs] =
             csr_accessor<const F>(static_cast<const csr_table &>(data)).pull({ 0, -1 }, sparse_indexing::zero_based);
-        const auto c0 = row_accessor<const F>(input.get_initial_centroids()).pull({ 0, -1 });
+        kmb_context *ctx = thread_context();
+        array<F> c0;
+        if (input.get_initial_centroids().has_data()) {
+            c0 = row_accessor<const F>(input.get_initial_centroids()).pull({ 0, -1 });
+        }
+        else {
+            // the default for lloyd_csr: plusPlusCSR, one trial, seed 777777
+            // (detail/train_init_centroids.hpp:39-74)
+            c0 = array<F>::empty(k * d);
+            check(ctx, kmb_init_plusplus_csr(ctx, dtype_of<F>, KMB_MEM_HOST, vals.get_data(), cols.get_data(),
+                                             offs.get_data(), n, d, 0, k, KMB_PLUSPLUS_DEFAULT_SEED,
+                                             c0.get_mutable_data()));
+        }
         auto centroids = array<F>::empty(k * d);
         auto responses = array<std::int32_t>::empty(n);
         kmb_params p{ k, desc.get_max_iteration_count(), desc.get_accuracy_threshold(), KMB_FORM_PLAIN, 0 };
         double objective = 0.0;
         std::int64_t iterations = 0;
-        kmb_context *ctx = thread_context();
         check(ctx, kmb_train_csr(ctx, dtype_of<F>, KMB_MEM_HOST, vals.get_data(), cols.get_data(), offs.get_data(),
                                  n, d, 0, c0.get_data(), &p, centroids.get_mutable_data(),
                                  responses.get_mutable_data(), &objective, &iterations, nullptr));

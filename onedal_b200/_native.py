@@ -24,7 +24,7 @@ EXPORTED = (
     "kmb_server_create", "kmb_server_destroy", "kmb_server_add_model", "kmb_server_submit_infer",
     "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats", "kmb_server_infer_form", "kmb_server_wait_detail", "kmb_context_set_max_sms", "kmb_init_plusplus", "kmb_batched_train",
     "kmb_model_serialize", "kmb_model_deserialize", "kmb_server_add_model_serialized",
-    "kmb_train_csr", "kmb_infer_csr",
+    "kmb_train_csr", "kmb_infer_csr", "kmb_init_plusplus_csr",
 )
 
 
@@ -119,6 +119,8 @@ def load_library(path: str = LIB_PATH):
             lib.kmb_train_csr.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, I64, I64, I32, P,
                                           ctypes.POINTER(kmb_params), P, P, ctypes.POINTER(D), ctypes.POINTER(I64),
                                           ctypes.POINTER(kmb_stats)]
+            lib.kmb_init_plusplus_csr.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, I64, I64, I32, I64,
+                                                  ctypes.c_uint32, P]
             lib.kmb_infer_csr.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, I64, I64, I32, P, I64, I32, P,
                                           ctypes.POINTER(D)]
             _lib = lib

@@ -729,15 +729,10 @@ int validate_csr_call(kmb_context *ctx, int dtype, int memory, const void *vals,
 // the device in order: k center probabilities, then a pool of resample draws
 // (refilled, continuing the same sequence, when a round runs out of them).
 template <typename F>
-int init_plusplus_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t d, int64_t k, uint32_t seed,
-                       void *C_out) {
+int init_plusplus_core(kmb_context *ctx, int memory, const F *X, const kmb::CsrRows *csr, int64_t n, int64_t d,
+                       int64_t k, uint32_t seed, void *C_out) {
     kmb::Workspace &ws = ctx->ws;
     cudaStream_t s = ctx->stream;
-    const F *X = (const F *)Xv;
-    if (memory == KMB_MEM_HOST) {
-        int rc = upload<F>(ctx, ws.X, Xv, sizeof(F) * n * d, &X);
-        if (rc) return rc;
-    }
     // KMB_PLUSPLUS_POOL (1..2^20) shrinks the resample pool so tests can drive the refill path
     int pool_n = 4096;
     if (const char *e = getenv("KMB_PLUSPLUS_POOL")) pool_n = (int)std::min(std::max(atol(e), 1L), 1L << 20);
@@ -764,13 +759,20 @@ int init_plusplus_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, 
     int64_t row0 = (int64_t)(size_t)(host[0] * F(n));
     if (row0 == n) --row0;
     kmb::launch_pp_fill<F>(md, n, s);
-    kmb::launch_pp_first<F>(X, d, row0, C, s);
+    if (csr)
+        kmb::launch_pp_first_csr<F>(*csr, row0, C, st, s);
+    else
+        kmb::launch_pp_first<F>(X, d, row0, C, s);
     int64_t c_begin = 1;
     bool update_first = true;
     int64_t round_draws = 0;  // resample draws spent on the round that stopped
     for (;;) {
-        kmb::launch_pp_rounds<F>(X, n, d, k, c_begin, update_first, md, acc, (unsigned *)ws.pp_flags.ptr, rnd,
-                                 rnd + k, pool_n, C, st, s);
+        if (csr)
+            kmb::launch_pp_rounds_csr<F>(*csr, k, c_begin, update_first, md, acc, (unsigned *)ws.pp_flags.ptr, rnd,
+                                         rnd + k, pool_n, C, st, s);
+        else
+            kmb::launch_pp_rounds<F>(X, n, d, k, c_begin, update_first, md, acc, (unsigned *)ws.pp_flags.ptr, rnd,
+                                     rnd + k, pool_n, C, st, s);
         KMB_CUDA(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
         KMB_CUDA(cudaStreamSynchronize(s));
         if (!hs.stopped) break;
@@ -802,6 +804,26 @@ int init_plusplus_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, 
         KMB_CUDA(cudaStreamSynchronize(s));
     }
     return KMB_OK;
+}
+
+template <typename F>
+int init_plusplus_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t d, int64_t k, uint32_t seed,
+                       void *C_out) {
+    const F *X = (const F *)Xv;
+    if (memory == KMB_MEM_HOST) {
+        int rc = upload<F>(ctx, ctx->ws.X, Xv, sizeof(F) * n * d, &X);
+        if (rc) return rc;
+    }
+    return init_plusplus_core<F>(ctx, memory, X, nullptr, n, d, k, seed, C_out);
+}
+
+template <typename F>
+int init_plusplus_csr_impl(kmb_context *ctx, int memory, const void *vals, const int64_t *cols, const int64_t *rowptr,
+                           int64_t n, int64_t d, int base, int64_t k, uint32_t seed, void *C_out) {
+    kmb::CsrRows X;
+    int rc = prepare_csr<F>(ctx, memory, vals, cols, rowptr, n, d, base, &X);
+    if (rc) return rc;
+    return init_plusplus_core<F>(ctx, memory, nullptr, &X, n, d, k, seed, C_out);
 }
 
 extern "C" {
@@ -951,6 +973,21 @@ int kmb_init_plusplus(kmb_context *ctx, int dtype, int memory, const void *X, in
     if (dtype == KMB_F32) return init_plusplus_impl<float>(ctx, memory, X, n, d, k, seed, C_out);
     if (dtype == KMB_F64) return init_plusplus_impl<double>(ctx, memory, X, n, d, k, seed, C_out);
     return fail(ctx, KMB_EINVAL, "unknown dtype");
+}
+
+int kmb_init_plusplus_csr(kmb_context *ctx, int dtype, int memory, const void *values, const int64_t *col_indices,
+                          const int64_t *row_offsets, int64_t n, int64_t d, int32_t indexing, int64_t k, uint32_t seed,
+                          void *C_out) {
+    if (!ctx) return KMB_EINVAL;
+    ctx->last_error.clear();
+    if (!C_out || n <= 0 || d <= 0 || k <= 0) return fail(ctx, KMB_EINVAL, "bad argument");
+    if (k > n) return fail(ctx, KMB_EINVAL, "cluster_count %lld exceeds the row count %lld", (long long)k, (long long)n);
+    int rc = validate_csr_call(ctx, dtype, memory, values, col_indices, row_offsets, indexing);
+    if (rc) return rc;
+    if (dtype == KMB_F32)
+        return init_plusplus_csr_impl<float>(ctx, memory, values, col_indices, row_offsets, n, d, indexing, k, seed,
+                                             C_out);
+    return init_plusplus_csr_impl<double>(ctx, memory, values, col_indices, row_offsets, n, d, indexing, k, seed, C_out);
 }
 
 int kmb_infer(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n, int64_t d, const void *C, int64_t k,

@@ -529,11 +529,83 @@ __global__ void __launch_bounds__(kSelThreads) pp_select_kernel(const F *__restr
         __syncthreads();  // s_val / s_flag are rewritten by the next attempt
     }
     const int64_t row = s_pos;
-    for (int i = tid; i < d; i += kSelThreads) C[c * d + i] = X[row * d + i];
+    if (X)  // dense rows; CSR rows are expanded by pp_csr_emit_kernel
+        for (int i = tid; i < d; i += kSelThreads) C[c * d + i] = X[row * d + i];
     if (tid == 0) {
         md[row] = F(0);
         st->pool_used = used;
         st->rows_chosen += 1;
+        st->last_row = row;
+    }
+}
+
+// ---- CSR rows (plusPlusCSR, DataHelperCSR of kmeans_plusplus_init_impl.i:244-316) ----
+
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+// Center c = row (st->last_row, or `row` when >= 0) expanded to dense, and its
+// squared norm in F summed in column order (the unstored zeros add nothing).
+template <typename F>
+__global__ void pp_csr_emit_kernel(const F *__restrict__ vals, const int32_t *__restrict__ cols,
+                                   const int64_t *__restrict__ rowptr, int d, int64_t c, int64_t row, F *__restrict__ C,
+                                   PPState *st) {
+    if (st->stopped) return;
+    const int64_t r = row >= 0 ? row : st->last_row;
+    F *out = C + c * d;
+    for (int i = threadIdx.x; i < d; i += blockDim.x) out[i] = F(0);
+    __syncthreads();
+    for (int64_t e = rowptr[r] + threadIdx.x; e < rowptr[r + 1]; e += blockDim.x) out[cols[e]] = vals[e];
+    if (threadIdx.x == 0) {
+        F s = F(0);
+        for (int64_t e = rowptr[r]; e < rowptr[r + 1]; ++e) s = add_rn(s, mul_rn(vals[e], vals[e]));
+        st->cnorm = (double)s;
+    }
+}
+
+// d2 = ||c||^2, then per stored entry in order d2 += x*x - (2x)*c_col, every
+// operation rounded as written (no contraction). One warp per 512-row block, one
+// lane per row; lane 0 sums the block's minima in row order and publishes them
+// for the leading CTA's overall-sum fold.
+template <typename F>
+__global__ void __launch_bounds__(kUpdWarps * 32)
+    pp_update_csr_kernel(const F *__restrict__ vals, const int32_t *__restrict__ cols,
+                         const int64_t *__restrict__ rowptr, int64_t n, int64_t nb, const F *__restrict__ center,
+                         F *__restrict__ md, F *__restrict__ acc, unsigned *__restrict__ flags, unsigned epoch,
+                         PPState *st) {
+    __shared__ F s_md[kUpdWarps][kPPBlock];
+    if (st->stopped) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (blockIdx.x == 0) {
+        if (warp == 0) fold_overall(acc, flags, nb, epoch, st);
+        return;
+    }
+    const int64_t b = (int64_t)(blockIdx.x - 1) * kUpdWarps + warp;
+    if (b >= nb) return;
+    const int64_t base = b * kPPBlock;
+    const int cnt = (int)min((int64_t)kPPBlock, n - base);
+    const F cn = (F)st->cnorm;
+    for (int r = lane; r < cnt; r += 32) {
+        const int64_t row = base + r;
+        F d2 = cn;
+        for (int64_t e = rowptr[row]; e < rowptr[row + 1]; ++e) {
+            const F x = vals[e];
+            d2 = add_rn(d2, sub_rn(mul_rn(x, x), mul_rn(mul_rn(F(2), x), center[cols[e]])));
+        }
+        const F old = md[row];
+        const F m = !(d2 < old) ? old : d2;  // the reference's min(best, d2)
+        md[row] = m;
+        s_md[warp][r] = m;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        F sum = F(0);
+        for (int i = 0; i < cnt; ++i) sum += s_md[warp][i];
+        publish_block_sum(acc, flags, b, sum, epoch);
     }
 }
 
@@ -583,7 +655,35 @@ void launch_pp_rounds(const F *X, int64_t n, int64_t d, int64_t k, int64_t c_beg
     }
 }
 
+template <typename F>
+void launch_pp_first_csr(const CsrRows &X, int64_t row, F *C, PPState *st, cudaStream_t s) {
+    pp_csr_emit_kernel<F><<<1, 256, 0, s>>>((const F *)X.vals, X.cols, X.rowptr, (int)X.d, 0, row, C, st);
+    KMB_LAUNCHED();
+}
+
+template <typename F>
+void launch_pp_rounds_csr(const CsrRows &X, int64_t k, int64_t c_begin, bool update_first, F *md, F *acc,
+                          unsigned *flags, const F *probs, const F *pool, int pool_n, F *C, PPState *st, cudaStream_t s) {
+    const int64_t n = X.n, d = X.d;
+    const int64_t nb = (n + kPPBlock - 1) / kPPBlock;
+    const unsigned grid = 1 + (unsigned)((nb + kUpdWarps - 1) / kUpdWarps);  // + the overall-sum CTA
+    for (int64_t c = c_begin; c < k; ++c) {
+        if (c > c_begin || update_first) {
+            pp_update_csr_kernel<F><<<grid, kUpdWarps * 32, 0, s>>>((const F *)X.vals, X.cols, X.rowptr, n, nb,
+                                                                    C + (c - 1) * d, md, acc, flags, (unsigned)c, st);
+            KMB_LAUNCHED();
+        }
+        pp_select_kernel<F><<<1, kSelThreads, 0, s>>>(nullptr, n, (int)d, nb, acc, md, probs, pool, pool_n, c, C, st);
+        KMB_LAUNCHED();
+        pp_csr_emit_kernel<F><<<1, 256, 0, s>>>((const F *)X.vals, X.cols, X.rowptr, (int)d, c, -1, C, st);
+        KMB_LAUNCHED();
+    }
+}
+
 #define KMB_PP_INST(F)                                                                                               \
+    template void launch_pp_first_csr<F>(const CsrRows &, int64_t, F *, PPState *, cudaStream_t);                  \
+    template void launch_pp_rounds_csr<F>(const CsrRows &, int64_t, int64_t, bool, F *, F *, unsigned *, const F *, \
+                                          const F *, int, F *, PPState *, cudaStream_t);                           \
     template void launch_pp_fill<F>(F *, int64_t, cudaStream_t);                                                    \
     template void launch_pp_first<F>(const F *, int64_t, int64_t, F *, cudaStream_t);                               \
     template void launch_pp_rounds<F>(const F *, int64_t, int64_t, int64_t, int64_t, bool, F *, F *, unsigned *,    \

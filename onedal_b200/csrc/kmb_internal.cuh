@@ -51,6 +51,8 @@ struct PPState {
     long long stop_round;
     long long rows_chosen;
     double overall;       // the current round's overall distance sum (computed in F)
+    long long last_row;   // the row chosen by the last selection
+    double cnorm;         // CSR rows: ||c||^2 of the last center (computed in F)
 };
 
 template <typename F>
@@ -60,6 +62,14 @@ void launch_pp_first(const F *X, int64_t d, int64_t row, F *C, cudaStream_t s);
 template <typename F>
 void launch_pp_rounds(const F *X, int64_t n, int64_t d, int64_t k, int64_t c_begin, bool update_first, F *md, F *acc,
                       unsigned *flags, const F *probs, const F *pool, int pool_n, F *C, PPState *st, cudaStream_t s);
+// The same for CSR rows (plusPlusCSR): center c = row `row` expanded to dense,
+// with ||c||^2 in st->cnorm; launch_pp_first_csr places center 0.
+struct CsrRows;
+template <typename F>
+void launch_pp_first_csr(const CsrRows &X, int64_t row, F *C, PPState *st, cudaStream_t s);
+template <typename F>
+void launch_pp_rounds_csr(const CsrRows &X, int64_t k, int64_t c_begin, bool update_first, F *md, F *acc,
+                          unsigned *flags, const F *probs, const F *pool, int pool_n, F *C, PPState *st, cudaStream_t s);
 
 // Queues a near-tie row for the FP64 recheck. Two-candidate entries fill the
 // queue from the front (count st->n_recheck), full-rescan entries from the back

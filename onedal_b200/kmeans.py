@@ -502,11 +502,13 @@ def _train_csr(desc, data, initial_centroids):
         raise invalid_argument(_msg.input_data_is_empty)
     if k > n:
         raise invalid_argument(_msg.cluster_count_exceeds_data_row_count)
-    if not _has_data(initial_centroids):
-        raise invalid_argument("method::lloyd_csr on this path requires initial centroids")
-    C0, dev_c = _as_table(initial_centroids, desc.float_type)
-    if dev != dev_c:
-        raise invalid_argument("data and initial centroids must live in the same memory space")
+    if _has_data(initial_centroids):
+        C0, dev_c = _as_table(initial_centroids, desc.float_type)
+        if dev != dev_c:
+            raise invalid_argument("data and initial centroids must live in the same memory space")
+    else:
+        # the reference's default for lloyd_csr: plusPlusCSR, one trial, seed 777777
+        C0 = init_plusplus_csr(t, k, desc.float_type)
     if C0.shape[0] != k:
         raise invalid_argument(_msg.init_rc_neq_cluster_count)
     if C0.shape[1] != d:
@@ -575,6 +577,32 @@ def _infer_csr(desc, mdl, data):
     if want_obj:
         r._set_objective(float(obj.value))
     return r
+
+
+def init_plusplus_csr(data, cluster_count: int, float_type=np.float32, seed: int = 777777, ctx=None):
+    """k-means++ centers of CSR rows as oneDAL's train() computes them for method::lloyd_csr
+    without initial centroids (DAAL plusPlusCSR, one trial; kmb_init_plusplus_csr). Dense
+    k x d centers in the rows' memory space."""
+    t, vals, cols, offs, dev = _as_csr(data, float_type)
+    n, d = t.shape
+    k = int(cluster_count)
+    if ctx is None:
+        ctx = _native.context(_device_of(vals) if dev else 0)
+    if dev:
+        import torch
+        C = torch.empty((k, d), dtype=vals.dtype, device=vals.device)
+        ctx.set_stream(torch.cuda.current_stream(vals.device).cuda_stream)
+    else:
+        C = np.empty((k, d), dtype=float_type)
+    dtype = _native.KMB_F32 if np.dtype(float_type) == np.float32 else _native.KMB_F64
+    mem = _native.KMB_MEM_DEVICE if dev else _native.KMB_MEM_HOST
+    try:
+        ctx.check(ctx.lib.kmb_init_plusplus_csr(ctx.handle, dtype, mem, _ptr(vals, dev), _ptr(cols, dev),
+                                                _ptr(offs, dev), n, d, t.indexing, k, ctypes.c_uint32(seed),
+                                                _ptr(C, dev)))
+    except _native.NativeError as e:
+        _raise_native(e)
+    return C
 
 
 def train(desc: descriptor, data, initial_centroids=None) -> train_result:

@@ -49,6 +49,7 @@ def _load():
         _lib.daalref_set_threads.argtypes = [ctypes.c_int]
         for sfx in ("f64", "f32"):
             getattr(_lib, f"daalref_init_plusplus_{sfx}").argtypes = [P, I64, I64, I64, ctypes.c_uint32, P]
+            getattr(_lib, f"daalref_init_plusplus_csr_{sfx}").argtypes = [P, P, P, I64, I64, I64, ctypes.c_uint32, P]
             getattr(_lib, f"daalref_train_csr_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, I64, D, P, P, P, P, P]
             getattr(_lib, f"daalref_infer_csr_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, ctypes.c_int, P, P, P]
     return _lib
@@ -156,3 +157,18 @@ def infer_csr(vals, cols, rowptr, d, C, compute_objective=True):
     if rc != 0:
         raise ReferenceError_(int(code[0]))
     return lab, (float(obj[0]) if compute_objective else None)
+
+
+def init_plusplus_csr(vals, cols, rowptr, d, k, seed=777777, dtype=None):
+    """The reference's KMeansInitKernel<plusPlusCSR> (one trial, mt19937 seeded `seed`)
+    on zero-based CSR rows; returns the dense centers."""
+    lib = _load()
+    dtype = np.asarray(vals).dtype if dtype is None else dtype
+    v, c, r = _csr(vals, cols, rowptr, dtype)
+    n = len(r) - 1
+    C = np.empty((k, d), v.dtype)
+    rc = getattr(lib, f"daalref_init_plusplus_csr_{_sfx(v.dtype)}")(_p(v), _p(c), _p(r), n, int(d), int(k), int(seed),
+                                                                    _p(C))
+    if rc != 0:
+        raise ReferenceError_(rc)
+    return C

@@ -27,6 +27,12 @@
  *                  distance is <= eps = 0.1 * overall / n is resampled with a
  *                  fresh draw, the chosen row's distance is zeroed (:613-635);
  *                  no update after the last center (:669-673).
+ *   CSR rows       plusPlusCSR (the default init of method::lloyd_csr) differs only
+ *                  in the distance (DataHelperCSR, :244-316): d2 = ||c||^2 (the
+ *                  sum of c_i^2 over all columns in order, i.e. over the center
+ *                  row's stored entries) then, per stored entry in order,
+ *                  d2 += x*x - 2*x*c_col, every operation rounded; the first and
+ *                  the chosen centers are their rows expanded to dense.
  *   no candidate   when the overall distance is zero (fewer than k distinct rows)
  *                  or not finite, no draw can succeed and the reference's loop
  *                  never ends; this restatement returns 4 instead.
@@ -40,9 +46,55 @@
 
 namespace {
 
+// Dense rows: d2 = sum_i (x_i - c_i)^2 in coordinate order.
 template <typename F>
-int init_plusplus(const F *X, int64_t n, int64_t d, int64_t k, uint32_t seed, int fused, F *C, int64_t *rows_out) {
-    if (!X || !C || n <= 0 || d <= 0 || k <= 0 || k > n) return 2;
+struct DenseRows {
+    const F *X;
+    int64_t d;
+    int fused;
+    F dist(int64_t r, const F *c, F) const {
+        const F *x = X + r * d;
+        F d2 = F(0);
+        for (int64_t i = 0; i < d; ++i) {
+            const F t = x[i] - c[i];
+            d2 = fused ? std::fma(t, t, d2) : d2 + t * t;
+        }
+        return d2;
+    }
+    F center_norm(const F *) const { return F(0); }
+    void copy_row(int64_t r, F *dst) const { std::memcpy(dst, X + r * d, sizeof(F) * (size_t)d); }
+};
+
+// CSR rows (zero-based): d2 = ||c||^2, then d2 += x*x - 2*x*c per stored entry.
+template <typename F>
+struct CsrRowsOracle {
+    const F *v;
+    const int64_t *col, *rowptr;
+    int64_t d;
+    F dist(int64_t r, const F *c, F cnorm) const {
+        F d2 = cnorm;
+        for (int64_t e = rowptr[r]; e < rowptr[r + 1]; ++e) {
+            const F x = v[e];
+            const F a = x * x;
+            const F b = (F(2) * x) * c[col[e]];
+            d2 = d2 + (a - b);
+        }
+        return d2;
+    }
+    F center_norm(const F *c) const {
+        F s = F(0);
+        for (int64_t i = 0; i < d; ++i) s = s + c[i] * c[i];
+        return s;
+    }
+    void copy_row(int64_t r, F *dst) const {
+        for (int64_t i = 0; i < d; ++i) dst[i] = F(0);
+        for (int64_t e = rowptr[r]; e < rowptr[r + 1]; ++e) dst[col[e]] = v[e];
+    }
+};
+
+template <typename F, typename Rows>
+int init_plusplus_rows(const Rows &rows, int64_t n, int64_t d, int64_t k, uint32_t seed, F *C, int64_t *rows_out) {
+    if (!C || n <= 0 || d <= 0 || k <= 0 || k > n) return 2;
     std::mt19937 gen(seed);
     std::uniform_real_distribution<F> uni(F(0), F(1));
     std::vector<F> prob((size_t)k);
@@ -51,16 +103,12 @@ int init_plusplus(const F *X, int64_t n, int64_t d, int64_t k, uint32_t seed, in
     std::vector<F> md((size_t)n, std::numeric_limits<F>::max()), acc((size_t)nb);
     F overall = F(0);
     auto update = [&](const F *c) {
+        const F cnorm = rows.center_norm(c);
         for (int64_t b = 0; b < nb; ++b) {
             const int64_t r0 = b * B, r1 = std::min(n, r0 + B);
             F sum = F(0);
             for (int64_t r = r0; r < r1; ++r) {
-                const F *x = X + r * d;
-                F d2 = F(0);
-                for (int64_t i = 0; i < d; ++i) {
-                    const F t = x[i] - c[i];
-                    d2 = fused ? std::fma(t, t, d2) : d2 + t * t;
-                }
+                const F d2 = rows.dist(r, c, cnorm);
                 md[(size_t)r] = !(d2 < md[(size_t)r]) ? md[(size_t)r] : d2;
                 sum += md[(size_t)r];
             }
@@ -79,7 +127,7 @@ int init_plusplus(const F *X, int64_t n, int64_t d, int64_t k, uint32_t seed, in
     };
     int64_t row = (int64_t)(size_t)(prob[0] * F(n));
     if (row == n) --row;
-    std::memcpy(C, X + row * d, sizeof(F) * (size_t)d);
+    rows.copy_row(row, C);
     if (rows_out) rows_out[0] = row;
     update(C);
     for (int64_t c = 1; c < k; ++c) {
@@ -96,12 +144,25 @@ int init_plusplus(const F *X, int64_t n, int64_t d, int64_t k, uint32_t seed, in
             if (++tries > 10000000) return 3;  // the reference would retry forever
             p = uni(gen);
         }
-        std::memcpy(C + c * d, X + row * d, sizeof(F) * (size_t)d);
+        rows.copy_row(row, C + c * d);
         if (rows_out) rows_out[c] = row;
         if (c == k - 1) break;
         update(C + c * d);
     }
     return 0;
+}
+
+template <typename F>
+int init_plusplus(const F *X, int64_t n, int64_t d, int64_t k, uint32_t seed, int fused, F *C, int64_t *rows_out) {
+    if (!X) return 2;
+    return init_plusplus_rows<F>(DenseRows<F>{X, d, fused}, n, d, k, seed, C, rows_out);
+}
+
+template <typename F>
+int init_plusplus_csr(const F *v, const int64_t *col, const int64_t *rowptr, int64_t n, int64_t d, int64_t k,
+                      uint32_t seed, F *C, int64_t *rows_out) {
+    if (!v || !col || !rowptr || n <= 0 || rowptr[0] != 0) return 2;
+    return init_plusplus_rows<F>(CsrRowsOracle<F>{v, col, rowptr, d}, n, d, k, seed, C, rows_out);
 }
 
 }  // namespace
@@ -114,5 +175,13 @@ int kmo_init_plusplus_f64(const double *X, int64_t n, int64_t d, int64_t k, uint
 int kmo_init_plusplus_f32(const float *X, int64_t n, int64_t d, int64_t k, uint32_t seed, int fused, float *C,
                           int64_t *rows) {
     return init_plusplus<float>(X, n, d, k, seed, fused, C, rows);
+}
+int kmo_init_plusplus_csr_f64(const double *v, const int64_t *col, const int64_t *rowptr, int64_t n, int64_t d,
+                              int64_t k, uint32_t seed, double *C, int64_t *rows) {
+    return init_plusplus_csr<double>(v, col, rowptr, n, d, k, seed, C, rows);
+}
+int kmo_init_plusplus_csr_f32(const float *v, const int64_t *col, const int64_t *rowptr, int64_t n, int64_t d,
+                              int64_t k, uint32_t seed, float *C, int64_t *rows) {
+    return init_plusplus_csr<float>(v, col, rowptr, n, d, k, seed, C, rows);
 }
 }

@@ -19,12 +19,16 @@
 #include "src/algorithms/distributions/uniform/uniform_kernel.h"
 #include "src/algorithms/distributions/uniform/uniform_impl.i"
 #include "data_management/data/homogen_numeric_table.h"
+#include "data_management/data/csr_numeric_table.h"
 
 #include <cstdint>
+#include <vector>
 
 namespace daal { namespace algorithms { namespace kmeans { namespace init { namespace internal {
 template class KMeansInitKernel<plusPlusDense, double, daal::internal::avx2>;
 template class KMeansInitKernel<plusPlusDense, float, daal::internal::avx2>;
+template class KMeansInitKernel<plusPlusCSR, double, daal::internal::avx2>;
+template class KMeansInitKernel<plusPlusCSR, float, daal::internal::avx2>;
 }}}}}
 
 namespace daal { namespace algorithms { namespace distributions { namespace uniform { namespace internal {
@@ -52,9 +56,43 @@ int run_init(const F * X, int64_t n, int64_t d, int64_t k, uint32_t seed, F * C_
     services::Status s = kernel.compute(1, in, 1, out, &par, engine);
     return s.ok() ? 0 : 1;
 }
+// plusPlusCSR (the default init of train() with method::lloyd_csr,
+// cpp/oneapi/dal/algo/kmeans/detail/train_init_centroids.hpp:39-42) on zero-based
+// CSR arrays, given to DAAL one-based.
+template <typename F>
+int run_init_csr(const F * vals, const int64_t * cols, const int64_t * rowptr, int64_t n, int64_t d, int64_t k, uint32_t seed,
+                 F * C_out)
+{
+    if (n <= 0 || d <= 0 || k <= 0 || k > n || rowptr[0] != 0) return 2;
+    const int64_t nnz = rowptr[n];
+    std::vector<F> v(vals, vals + nnz);
+    std::vector<size_t> c((size_t)nnz), r((size_t)n + 1);
+    for (int64_t e = 0; e < nnz; ++e) c[(size_t)e] = (size_t)cols[e] + 1;
+    for (int64_t i = 0; i <= n; ++i) r[(size_t)i] = (size_t)rowptr[i] + 1;
+    services::Status st;
+    auto tX = CSRNumericTable::create<F>(v.data(), c.data(), r.data(), (size_t)d, (size_t)n, CSRNumericTableIface::oneBased, &st);
+    auto tC = HomogenNumericTable<F>::create(C_out, (size_t)d, (size_t)k, &st);
+    kinit::Parameter par((size_t)k, 0, seed);
+    daal::algorithms::engines::mt19937::internal::BatchImpl<daal::internal::avx2, F> engine(seed);
+    const NumericTable * in[1] = { tX.get() };
+    const NumericTable * out[1] = { tC.get() };
+    kinit::internal::KMeansInitKernel<kinit::plusPlusCSR, F, daal::internal::avx2> kernel;
+    services::Status s = kernel.compute(1, in, 1, out, &par, engine);
+    return s.ok() ? 0 : 1;
+}
 } // namespace
 
 extern "C" {
+int daalref_init_plusplus_csr_f64(const double * v, const int64_t * c, const int64_t * r, int64_t n, int64_t d, int64_t k, uint32_t seed,
+                                  double * C_out)
+{
+    return run_init_csr<double>(v, c, r, n, d, k, seed, C_out);
+}
+int daalref_init_plusplus_csr_f32(const float * v, const int64_t * c, const int64_t * r, int64_t n, int64_t d, int64_t k, uint32_t seed,
+                                  float * C_out)
+{
+    return run_init_csr<float>(v, c, r, n, d, k, seed, C_out);
+}
 int daalref_init_plusplus_f64(const double * X, int64_t n, int64_t d, int64_t k, uint32_t seed, double * C_out)
 {
     return run_init<double>(X, n, d, k, seed, C_out);

@@ -49,6 +49,7 @@ def _load():
         _lib.kmo_assign_f32_in_f64.argtypes = [P, I64, I64, P, I64, P, P, P]
         for sfx in ("f64", "f32"):
             getattr(_lib, f"kmo_init_plusplus_{sfx}").argtypes = [P, I64, I64, I64, ctypes.c_uint32, ctypes.c_int, P, P]
+            getattr(_lib, f"kmo_init_plusplus_csr_{sfx}").argtypes = [P, P, P, I64, I64, I64, ctypes.c_uint32, P, P]
             getattr(_lib, f"kmoc_train_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, I64, D, P, P, P, P]
             getattr(_lib, f"kmoc_infer_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, ctypes.c_int, P, P]
             getattr(_lib, f"kmoc_step_{sfx}").argtypes = [P, P, P, I64, I64, P, I64, P, P, P, P]
@@ -221,3 +222,19 @@ def step_csr(vals, cols, rowptr, d, C_in):
     _check(getattr(_load(), f"kmoc_step_{_sfx(C_in.dtype)}")(_p(v), _p(c), _p(r), n, int(d), _p(C_in), C_in.shape[0],
                                                             _p(C), _p(lab), _p(shift), _p(ne)))
     return C, lab, float(shift[0]), int(ne[0])
+
+
+def init_plusplus_csr(vals, cols, rowptr, d, k, seed=777777, dtype=None):
+    """DAAL's plusPlusCSR with one trial (kmeans_init_oracle.cpp) on zero-based CSR rows.
+    Returns (centroids k x d dense, chosen row indices)."""
+    dtype = np.asarray(vals).dtype if dtype is None else dtype
+    v, c, r = _csr(vals, cols, rowptr, dtype)
+    n = len(r) - 1
+    C = np.empty((k, d), v.dtype)
+    rows = np.empty(k, np.int64)
+    rc = getattr(_load(), f"kmo_init_plusplus_csr_{_sfx(v.dtype)}")(_p(v), _p(c), _p(r), n, int(d), int(k), int(seed),
+                                                                    _p(C), _p(rows))
+    if rc == 4:
+        raise NoCandidateRows("fewer than k distinct rows (no row left to sample)")
+    _check(rc)
+    return C, rows

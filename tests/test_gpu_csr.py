@@ -190,3 +190,47 @@ def test_csr_malformed_input_is_invalid_argument():
         t = kmeans.csr_table(good_v, c, r, 2, 3, kmeans.sparse_indexing.zero_based)
         with pytest.raises(kmeans.invalid_argument):
             kmeans.train(_desc(np.float64, 1, 2), t, C0)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("n,d,k,density", [(1, 4, 1, 0.5), (513, 40, 17, 0.1), (5000, 300, 64, 0.03),
+                                           (70001, 2000, 40, 0.005)])
+def test_csr_plusplus_matches_oracle(dt, n, d, k, density):
+    """plusPlusCSR on the GPU picks the oracle's rows exactly (the oracle is pinned to the
+    reference build): ragged block counts, empty rows, wide sparse rows."""
+    M, _ = _case(n + k, n, d, 1, density)
+    M = M.astype(dt)
+    C = kmeans.init_plusplus_csr(kmeans.csr_table.from_scipy(M), k, dt)
+    Co, rows = restated.init_plusplus_csr(M.data, M.indices.astype(np.int64), M.indptr.astype(np.int64), d, k)
+    assert np.array_equal(C, Co)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+def test_csr_plusplus_device_rows_and_pool_refill(dt, monkeypatch):
+    M, _ = _case(17, 4000, 150, 1, 0.05)
+    M = M.astype(dt)
+    M.data = np.round(M.data).astype(dt) + dt(0.5)  # duplicate-heavy: resampling happens
+    ref = restated.init_plusplus_csr(M.data, M.indices.astype(np.int64), M.indptr.astype(np.int64), 150, 30)[0]
+    monkeypatch.setenv("KMB_PLUSPLUS_POOL", "1")
+    assert np.array_equal(kmeans.init_plusplus_csr(kmeans.csr_table.from_scipy(M), 30, dt), ref)
+    t = kmeans.csr_table(torch.from_numpy(M.data).cuda(), torch.from_numpy(M.indices.astype(np.int64) + 1).cuda(),
+                         torch.from_numpy(M.indptr.astype(np.int64) + 1).cuda(), 4000, 150,
+                         kmeans.sparse_indexing.one_based)
+    assert np.array_equal(kmeans.init_plusplus_csr(t, 30, dt).cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("k,n,d", [(5, 50, 20), (16, 200, 100), (32, 10000, 512)])
+def test_csr_sparse_blobs_without_initial_centroids(dt, k, n, d):
+    """test/batch.cpp:276-351 without initial centroids: the default plusPlusCSR init.
+    The responses are the oracle's from the oracle's k-means++ centers (the same rows the
+    reference build picks); with float32 draws on the (16, 200, 100) case the reference
+    itself places two centers in one generating cluster, so the recovered partition is
+    checked against the oracle rather than the generator."""
+    M, truth = _sparse_blobs(n, d, k, 5 + k, dt)
+    r = kmeans.train(_desc(dt, k, 30, 0.01), kmeans.csr_table.from_scipy(M))
+    C0 = restated.init_plusplus_csr(M.data, M.indices.astype(np.int64), M.indptr.astype(np.int64), d, k)[0]
+    r2 = kmeans.train(_desc(dt, k, 30, 0.01), kmeans.csr_table.from_scipy(M), C0)
+    assert np.array_equal(r.get_model().get_centroids(), r2.get_model().get_centroids())
+    _, lo, _, ito = restated.train_csr(M.data, M.indices, M.indptr, d, C0, 30, 0.01)
+    assert (r.get_responses().ravel() == lo).all() and r.get_iteration_count() == ito

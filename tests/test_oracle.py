@@ -271,3 +271,25 @@ def test_csr_reference_reseeds_empty_clusters_like_restatement():
     b = daal_ref.train_csr(v, c, r, 40, C0, 10, 0.0)
     assert (a[1] == b[1]).all() and a[3] == b[3]
     assert centroid_rel_err(b[0], a[0]) < 1e-12
+
+
+@needs_ref
+@pytest.mark.parametrize("dt", DTYPES)
+@pytest.mark.parametrize("seed", range(8))
+def test_plusplus_csr_restated_equals_reference_live(seed, dt):
+    """plusPlusCSR (the lloyd_csr default init): the restatement picks the reference
+    build's centers exactly, including rounded values (duplicate rows) and empty rows."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(300 + seed)
+    n, d = int(rng.integers(10, 2500)), int(rng.integers(3, 250))
+    k = min(int(rng.integers(1, 50)), n)
+    M = sp.random(n, d, density=float(rng.uniform(0.02, 0.4)), format="csr", random_state=seed)
+    M.data = rng.standard_normal(M.nnz) * 2
+    if seed % 3 == 0:
+        M.data = np.round(M.data) + 0.5
+    M.sort_indices()
+    v = M.data.astype(dt)
+    a, rows = restated.init_plusplus_csr(v, M.indices, M.indptr, d, k)
+    b = daal_ref.init_plusplus_csr(v, M.indices, M.indptr, d, k)
+    assert np.array_equal(a, b)
+    assert np.array_equal(a, M[rows].toarray().astype(dt))
