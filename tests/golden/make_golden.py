@@ -29,6 +29,9 @@ Sources (paths inside the reference project):
   777777: the default of cpp/oneapi/dal/algo/kmeans/detail/train_init_centroids.hpp)
   built from source, float64 and float32, on the seeded inputs of plusplus_cases()
   and on the example data with k=20.
+* daal_ref_csr.npz -- outputs of the reference CSR kernels built from source
+  (KMeansBatchKernel<lloydCSR>: 25 iterations, eps 0; KMeansInitKernel<plusPlusCSR>)
+  on the seeded CSR inputs of csr_cases(), float64 and float32.
 * model_archives.npz -- oneDAL binary archives of k-means models written by
   oneDAL's own serialisation code (detail::serialize into binary_output_archive,
   compiled from the reference sources into integration/_build/kmeans_client):
@@ -137,6 +140,22 @@ def onedal_archive(client, centroids, tag, workdir):
     return np.frombuffer(open(out, "rb").read(), np.uint8)
 
 
+def csr_cases():
+    """Seeded CSR inputs of daal_ref_csr.npz: (name, values, columns, row offsets, d, k,
+    initial centroids) -- zero-based, sorted columns, float64."""
+    import scipy.sparse as sp
+    out = []
+    for name, n, d, k, density, seed in (("small", 300, 40, 6, 0.15, 401), ("wide", 2000, 500, 32, 0.02, 402),
+                                         ("dense_ish", 800, 24, 12, 0.5, 403)):
+        rng = np.random.default_rng(seed)
+        M = sp.random(n, d, density=density, format="csr", random_state=seed, dtype=np.float64)
+        M.data = rng.standard_normal(M.nnz) * 3
+        M.sort_indices()
+        C0 = M[rng.choice(n, k, replace=False)].toarray()
+        out.append((name, M.data, M.indices.astype(np.int64), M.indptr.astype(np.int64), d, k, C0))
+    return out
+
+
 def blobs_c1(n, seed):
     """Seeded mixture of 20 isotropic Gaussian blobs (std 1) in d=20, centres U[-10,10]."""
     rng = np.random.default_rng(seed)
@@ -204,6 +223,17 @@ def main():
         for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
             out[f"C_{name}_{tag}"] = daal_ref.init_plusplus(X.astype(dt), k)
     np.savez_compressed(os.path.join(HERE, "daal_ref_plusplus.npz"), **out)
+
+    # CSR Lloyd and plusPlusCSR: outputs of the reference kernels on seeded CSR inputs
+    out = {}
+    for name, v, c, r, d, k, C0 in csr_cases():
+        for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+            daal_ref.set_threads(1)
+            C, lab, obj, it = daal_ref.train_csr(v.astype(dt), c, r, d, C0.astype(dt), 25, 0.0)
+            out[f"C_{name}_{tag}"], out[f"labels_{name}_{tag}"] = C, lab
+            out[f"obj_{name}_{tag}"], out[f"iters_{name}_{tag}"] = obj, it
+            out[f"pp_{name}_{tag}"] = daal_ref.init_plusplus_csr(v.astype(dt), c, r, d, k)
+    np.savez_compressed(os.path.join(HERE, "daal_ref_csr.npz"), **out)
 
     # model archives: the serialisation test's model (default descriptor: k = 2, 100
     # iterations, eps 0, k-means++ init) trained by the reference kernel, archived by

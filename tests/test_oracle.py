@@ -293,3 +293,22 @@ def test_plusplus_csr_restated_equals_reference_live(seed, dt):
     b = daal_ref.init_plusplus_csr(v, M.indices, M.indptr, d, k)
     assert np.array_equal(a, b)
     assert np.array_equal(a, M[rows].toarray().astype(dt))
+
+
+@pytest.mark.parametrize("tag,dt", [("f64", np.float64), ("f32", np.float32)])
+def test_csr_restated_matches_reference_fixtures(tag, dt):
+    """The CSR restatement against the reference CSR kernels' recorded outputs
+    (tests/golden/daal_ref_csr.npz), usable where the reference build is absent."""
+    import os
+    import sys
+    from helpers import GOLDEN
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from make_golden import csr_cases
+    z = np.load(os.path.join(GOLDEN, "daal_ref_csr.npz"))
+    for name, v, c, r, d, k, C0 in csr_cases():
+        C, lab, obj, it = restated.train_csr(v.astype(dt), c, r, d, C0.astype(dt), 25, 0.0)
+        assert (lab == z[f"labels_{name}_{tag}"]).all() and it == int(z[f"iters_{name}_{tag}"]), name
+        tol = 1e-12 if dt == np.float64 else 1e-5
+        assert centroid_rel_err(z[f"C_{name}_{tag}"], C) < tol, name
+        assert rel_close(obj, float(z[f"obj_{name}_{tag}"]), tol), name
+        assert np.array_equal(restated.init_plusplus_csr(v.astype(dt), c, r, d, k)[0], z[f"pp_{name}_{tag}"]), name
