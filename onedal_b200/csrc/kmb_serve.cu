@@ -113,6 +113,7 @@ struct Lane;
 
 struct Server {
     int device = 0;
+    int64_t tc_chunk_rows = kTcChunkRows;  // KMB_SERVER_TC_CHUNK_ROWS (4096 .. kTcChunkRows)
     size_t budget = 0;
     size_t in_use = 0, peak_in_use = 0;
     std::mutex mu;
@@ -382,7 +383,7 @@ cudaError_t copy_in_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyK
 
 // Large infer request on the tensor-core worker: rows uploaded once, then
 // kmb_infer (BF16x3, FP64 recheck) over row chunks on the worker's stream.
-int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r) {
+int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r, int64_t chunk_rows) {
     float *dX = nullptr;
     int32_t *dlab = nullptr;
     if (cudaMallocAsync((void **)&dX, sizeof(float) * r->n * r->d, s) != cudaSuccess ||
@@ -402,8 +403,8 @@ int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r)
         kmb_context_set_kernel_timing(ctx, 1);
     }
     const auto t1 = Clock::now();
-    for (int64_t off = 0; rc == KMB_OK && off < r->n; off += kTcChunkRows) {
-        const int64_t rows = std::min<int64_t>(kTcChunkRows, r->n - off);
+    for (int64_t off = 0; rc == KMB_OK && off < r->n; off += chunk_rows) {
+        const int64_t rows = std::min<int64_t>(chunk_rows, r->n - off);
         rc = kmb_infer(ctx, KMB_F32, KMB_MEM_DEVICE, dX + off * r->d, rows, r->d, m.C, m.k, KMB_FORM_BF16X3, 0,
                        dlab + off, nullptr, nullptr);
     }
@@ -459,7 +460,7 @@ void tc_worker_loop(Server *srv) {
         srv->tc_busy += 1;
         const Model m = srv->models[r->model];
         lock.unlock();
-        const int rc = ctx ? run_tc_request(ctx, ts, m, r) : KMB_ECUDA;
+        const int rc = ctx ? run_tc_request(ctx, ts, m, r, srv->tc_chunk_rows) : KMB_ECUDA;
         lock.lock();
         r->rc = rc;
         r->t_done = Clock::now();
@@ -577,6 +578,10 @@ int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32
     srv->device = device;
     srv->budget = (size_t)hbm_budget_bytes;
     if (const char *path = std::getenv("KMB_SERVE_TRACE")) srv->trace = std::fopen(path, "a");
+    // smaller assignment launches let lane kernels queued behind a large request's
+    // CTAs start sooner (at a per-launch cost)
+    if (const char *e = std::getenv("KMB_SERVER_TC_CHUNK_ROWS"))
+        srv->tc_chunk_rows = std::min<int64_t>(std::max<int64_t>(atoll(e), 4096), kTcChunkRows);
     // Keep freed request memory in the stream-ordered pool instead of returning it to the driver.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
