@@ -62,8 +62,12 @@ typedef enum kmb_memory { KMB_MEM_HOST = 0, KMB_MEM_DEVICE = 1 } kmb_memory;
  *                  tensor-core contraction with FP32 accumulation in TMEM; every
  *                  row whose top-2 gap is inside the derived error bound is
  *                  rechecked exactly in FP64, so responses equal the FP64
- *                  oracle's. */
-typedef enum kmb_form { KMB_FORM_PLAIN = 0, KMB_FORM_BF16X3 = 1 } kmb_form;
+ *                  oracle's.
+ * KMB_FORM_AUTO  : BF16X3 for FP32 data with d <= 256 once the contraction is
+ *                  dense enough to pay for the tensor cores (n * kpad * dpad >=
+ *                  KMB_AUTO_TC_MACS), the plain form otherwise. */
+typedef enum kmb_form { KMB_FORM_PLAIN = 0, KMB_FORM_BF16X3 = 1, KMB_FORM_AUTO = 2 } kmb_form;
+#define KMB_AUTO_TC_MACS (1LL << 30)
 
 typedef struct kmb_context kmb_context;
 

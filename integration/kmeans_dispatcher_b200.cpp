@@ -81,7 +81,7 @@ struct train_ops_dispatcher<dal::detail::host_policy, F, method::lloyd_dense, ta
         }
         auto centroids = array<F>::empty(k * d);
         auto responses = array<std::int32_t>::empty(n);
-        kmb_params p{ k, desc.get_max_iteration_count(), desc.get_accuracy_threshold(), KMB_FORM_PLAIN, 0 };
+        kmb_params p{ k, desc.get_max_iteration_count(), desc.get_accuracy_threshold(), KMB_FORM_AUTO, 0 };
         double objective = 0.0;
         std::int64_t iterations = 0;
         check(ctx, kmb_train(ctx, dtype_of<F>, KMB_MEM_HOST, x.get_data(), n, d, c0.get_data(), &p,
@@ -113,7 +113,7 @@ struct infer_ops_dispatcher<dal::detail::host_policy, F, method::lloyd_dense, ta
         auto responses = array<std::int32_t>::empty(n);
         double objective = 0.0;
         kmb_context *ctx = thread_context();
-        check(ctx, kmb_infer(ctx, dtype_of<F>, KMB_MEM_HOST, x.get_data(), n, d, cc.get_data(), k, KMB_FORM_PLAIN,
+        check(ctx, kmb_infer(ctx, dtype_of<F>, KMB_MEM_HOST, x.get_data(), n, d, cc.get_data(), k, KMB_FORM_AUTO,
                              want_obj ? 1 : 0, responses.get_mutable_data(), &objective, nullptr));
         auto result = infer_result<task::clustering>{}.set_result_options(desc.get_result_options());
         result.set_responses(dal::detail::homogen_table_builder{}.reset(responses, n, 1).build());

@@ -284,10 +284,19 @@ int upload(kmb_context *ctx, kmb::DevBuf &buf, const void *src, size_t bytes, co
 }
 
 int check_form(kmb_context *ctx, int dtype, int form) {
-    if (form != KMB_FORM_PLAIN && form != KMB_FORM_BF16X3) return fail(ctx, KMB_EINVAL, "unknown form %d", form);
+    if (form != KMB_FORM_PLAIN && form != KMB_FORM_BF16X3 && form != KMB_FORM_AUTO)
+        return fail(ctx, KMB_EINVAL, "unknown form %d", form);
     if (form == KMB_FORM_BF16X3 && dtype != KMB_F32)
         return fail(ctx, KMB_EINVAL, "the BF16x3 tensor-core form takes float32 data");
     return KMB_OK;
+}
+
+// KMB_FORM_AUTO -> the concrete form for this shape.
+int resolve_form(int dtype, int form, int64_t n, int64_t k, int64_t d) {
+    if (form != KMB_FORM_AUTO) return form;
+    if (dtype != KMB_F32 || !kmb::tc_supported(d)) return KMB_FORM_PLAIN;
+    const double macs = (double)n * (double)kmb::tc_kpad(k) * (double)kmb::tc_dpad(d);
+    return macs >= (double)KMB_AUTO_TC_MACS ? KMB_FORM_BF16X3 : KMB_FORM_PLAIN;
 }
 
 void init_state(LoopState &h, double eps) {
@@ -919,9 +928,11 @@ int kmb_train(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n,
     if (!X || !C0) return fail(ctx, KMB_EINVAL, "data and initial centroids are required");
     if (memory != KMB_MEM_HOST && memory != KMB_MEM_DEVICE) return fail(ctx, KMB_EINVAL, "unknown memory kind");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    kmb_params p = *params;
+    p.form = resolve_form(dtype, p.form, n, p.cluster_count, d);
     if (dtype == KMB_F32)
-        return train_impl<float>(ctx, memory, X, n, d, C0, params, C_out, responses, objective, iteration_count, stats);
-    return train_impl<double>(ctx, memory, X, n, d, C0, params, C_out, responses, objective, iteration_count, stats);
+        return train_impl<float>(ctx, memory, X, n, d, C0, &p, C_out, responses, objective, iteration_count, stats);
+    return train_impl<double>(ctx, memory, X, n, d, C0, &p, C_out, responses, objective, iteration_count, stats);
 }
 
 int kmb_train_csr(kmb_context *ctx, int dtype, int memory, const void *values, const int64_t *col_indices,
@@ -1003,6 +1014,7 @@ int kmb_infer(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n,
     if (!X || !C) return fail(ctx, KMB_EINVAL, "data and centroids are required");
     if (memory != KMB_MEM_HOST && memory != KMB_MEM_DEVICE) return fail(ctx, KMB_EINVAL, "unknown memory kind");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    form = resolve_form(dtype, form, n, k, d);
     if (dtype == KMB_F32)
         return infer_impl<float>(ctx, memory, X, n, d, C, k, form, compute_objective, responses, objective, stats);
     return infer_impl<double>(ctx, memory, X, n, d, C, k, form, compute_objective, responses, objective, stats);
@@ -1017,6 +1029,7 @@ int kmb_lloyd_step(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_
     if ((rc = check_form(ctx, dtype, form))) return rc;
     if (!X || !C_in || !C_out || !labels) return fail(ctx, KMB_EINVAL, "null device pointer");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    form = resolve_form(dtype, form, n, k, d);
     if (dtype == KMB_F32) return step_impl<float>(ctx, X, n, d, C_in, k, form, recheck, C_out, labels, shift, n_empty);
     return step_impl<double>(ctx, X, n, d, C_in, k, form, recheck, C_out, labels, shift, n_empty);
 }
@@ -1032,8 +1045,10 @@ int kmb_lloyd_iterate(kmb_context *ctx, int dtype, const void *X, int64_t n, int
     if ((rc = check_form(ctx, dtype, params->form))) return rc;
     if (!X || !C) return fail(ctx, KMB_EINVAL, "null device pointer");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
-    if (dtype == KMB_F32) return iterate_impl<float>(ctx, X, n, d, C, params, labels, iteration_count, stats);
-    return iterate_impl<double>(ctx, X, n, d, C, params, labels, iteration_count, stats);
+    kmb_params p = *params;
+    p.form = resolve_form(dtype, p.form, n, p.cluster_count, d);
+    if (dtype == KMB_F32) return iterate_impl<float>(ctx, X, n, d, C, &p, labels, iteration_count, stats);
+    return iterate_impl<double>(ctx, X, n, d, C, &p, labels, iteration_count, stats);
 }
 
 int kmb_context_set_max_sms(kmb_context *ctx, int max_sms) {
@@ -1085,6 +1100,7 @@ int kmb_partial_sums(kmb_context *ctx, int dtype, const void *X, int64_t n, int6
     if (rc) return rc;
     if (!X || !C || !labels || !sums || !counts) return fail(ctx, KMB_EINVAL, "null device pointer");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    form = resolve_form(dtype, form, n, k, d);
     if (dtype == KMB_F32)
         return partial_impl<float>(ctx, (const float *)X, n, d, (const float *)C, k, form, labels, sums, counts,
                                    sq_distances, (float *)row_sq_distance);

@@ -93,14 +93,19 @@ class result_options:
 
 
 class compute_form:
-    """How x.c is contracted on the GPU (the kmb_form of the C ABI)."""
+    """How x.c is contracted on the GPU (the kmb_form of the C ABI). `auto` (the
+    default) takes the BF16x3 tensor-core form with its exact FP64 recheck for float32
+    data with d <= 256 once n * k * d is large enough, and the plain FMA form otherwise."""
     plain = _native.KMB_FORM_PLAIN
     bf16x3 = _native.KMB_FORM_BF16X3
+    auto = _native.KMB_FORM_AUTO
 
 
 def _default_form():
-    v = os.environ.get("ONEDAL_B200_KMEANS_FORM", "plain").lower()
-    return compute_form.bf16x3 if v in ("bf16x3", "bf16", "tc") else compute_form.plain
+    v = os.environ.get("ONEDAL_B200_KMEANS_FORM", "auto").lower()
+    if v in ("bf16x3", "bf16", "tc"):
+        return compute_form.bf16x3
+    return compute_form.plain if v == "plain" else compute_form.auto
 
 
 class descriptor:
@@ -163,7 +168,7 @@ class descriptor:
 
     # B200-specific knobs (not part of the reference descriptor).
     def set_compute_form(self, form):
-        if form not in (compute_form.plain, compute_form.bf16x3):
+        if form not in (compute_form.plain, compute_form.bf16x3, compute_form.auto):
             raise domain_error("unknown compute form")
         self._form = form
         return self

@@ -22,9 +22,11 @@ def _models(rng, count=6):
 
 
 def _alone_infer(C, X, form=_native.KMB_FORM_PLAIN):
+    """The same infer alone, through kmeans.infer in the given form (explicit: the mirror's
+    default form is auto)."""
     d = kmeans.descriptor(np.float32).set_cluster_count(C.shape[0])
-    if form == _native.KMB_FORM_BF16X3:
-        d = d.set_compute_form(kmeans.compute_form.bf16x3)
+    d = d.set_compute_form(kmeans.compute_form.bf16x3 if form == _native.KMB_FORM_BF16X3
+                           else kmeans.compute_form.plain)
     return kmeans.infer(d, kmeans.model(C), X).get_responses().ravel()
 
 
