@@ -11,7 +11,8 @@
 //
 // B200 design. One warp per row: the row's entries are read 32 at a time and
 // broadcast by shuffles; lane l owns clusters c0 + l + 32t (t < T) of a chunk of
-// 32T clusters, so each entry costs T coalesced 128-byte reads of the
+// 32T clusters (T <= 16; wider k takes several passes over the row's entries),
+// so each entry costs T coalesced 128-byte reads of the
 // transposed centroids (d x kpad, L2-resident for moderate d*k) and T FMAs per
 // lane. The running minimum is lane-local in ascending cluster order, then a
 // warp reduction breaks ties by the lower index. The objective is FP64 with a
@@ -210,8 +211,7 @@ void launch_csr_assign(const CsrRows &X, const F *Ct, const F *h, int64_t k, int
     else if (per_lane <= 2) assign_t<F, 2>(X, Ct, h, kpad, labels, d2, st, s);
     else if (per_lane <= 4) assign_t<F, 4>(X, Ct, h, kpad, labels, d2, st, s);
     else if (per_lane <= 8) assign_t<F, 8>(X, Ct, h, kpad, labels, d2, st, s);
-    else if (per_lane <= 16) assign_t<F, 16>(X, Ct, h, kpad, labels, d2, st, s);
-    else assign_t<F, 32>(X, Ct, h, kpad, labels, d2, st, s);
+    else assign_t<F, 16>(X, Ct, h, kpad, labels, d2, st, s);  // wider k: 512-cluster passes (two CTAs per SM fit)
 }
 
 template <typename F>
