@@ -109,11 +109,14 @@ __device__ __forceinline__ RowTop<F> shfl_top(const RowTop<F> &x, int mask) {
     return y;
 }
 
-// Two CTAs per SM (16 warps): the register cap of 128 costs a few spilled
+// float: two CTAs per SM (16 warps): the register cap of 128 costs a few spilled
 // epilogue values but doubles the warps that hide the FMA and shared-memory
 // latencies (10 % faster at d=128, k=1024 and 32 % at d=64, k=256).
+// double: one CTA per SM. The 8 x 8 FP64 accumulators alone take 128 registers;
+// under the 128 cap they spilled 3.5 KB per thread and ran at 2.9 TFLOP/s, with
+// 254 registers the same launch runs at 15.4 TFLOP/s (d=128, k=1024).
 template <typename F, bool VEC>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, sizeof(F) == 4 ? 2 : 1)
 assign_plain_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restrict__ Ct, const F *__restrict__ h,
                     int k, int kpad, const F *__restrict__ xnorm, const double *__restrict__ cnorm_max,
                     int32_t *__restrict__ labels, F *__restrict__ d2, RecheckEntry *__restrict__ queue,
