@@ -301,6 +301,64 @@ __global__ void reset_double_kernel(double *p, const LoopState *st) {
     *p = 0.0;
 }
 
+constexpr int kSmallK = 32;        // clusters handled by assign_small_kernel
+constexpr int kSmallThreads = 128;
+
+// Few clusters (k <= 32, d <= 64): one row per thread, its d values in registers,
+// all centroids in shared memory (read as broadcasts). The contraction of row and
+// cluster accumulates x_t * c_t in ascending t, as the tiled kernel does, so the
+// scores -- and the labels, distances and recheck entries -- are the same; only
+// the 128-cluster tile padding and the tile epilogue are gone.
+template <typename F, int DMAX>
+__global__ void __launch_bounds__(kSmallThreads)
+assign_small_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restrict__ Ct, const F *__restrict__ h,
+                    int k, int kpad, const F *__restrict__ xnorm, const double *__restrict__ cnorm_max,
+                    int32_t *__restrict__ labels, F *__restrict__ d2, RecheckEntry *__restrict__ queue,
+                    LoopState *__restrict__ st) {
+    if (st && st->done) return;
+    __shared__ __align__(16) F Cs[kSmallK][DMAX];
+    __shared__ F hs[kSmallK];
+    for (int i = threadIdx.x; i < kSmallK * DMAX; i += blockDim.x) {
+        const int j = i / DMAX, t = i % DMAX;
+        Cs[j][t] = (j < k && t < d) ? Ct[(int64_t)t * kpad + j] : F(0);
+    }
+    for (int j = threadIdx.x; j < kSmallK; j += blockDim.x) hs[j] = j < k ? h[j] : f_inf<F>();
+    __syncthreads();
+    const double u = unit_roundoff<F>();
+    const double cmax = cnorm_max ? *cnorm_max : 0.0;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        F x[DMAX];
+        const F *xr = X + r * (int64_t)d;
+#pragma unroll
+        for (int t = 0; t < DMAX; ++t) x[t] = t < d ? xr[t] : F(0);
+        RowTop<F> top;
+        top.b = top.s = top.t = f_inf<F>();
+        top.ib = top.is = 0;
+        for (int j = 0; j < k; ++j) {
+            F dot = F(0);
+#pragma unroll
+            for (int t = 0; t < DMAX; t += 4) {
+                const typename Vec4<F>::T c = *reinterpret_cast<const typename Vec4<F>::T *>(&Cs[j][t]);
+                dot = fma(x[t], c.x, dot);
+                dot = fma(x[t + 1], c.y, dot);
+                dot = fma(x[t + 2], c.z, dot);
+                dot = fma(x[t + 3], c.w, dot);
+            }
+            top_push(top, hs[j] - dot, j);
+        }
+        labels[r] = top.ib;
+        const F xn = xnorm[r];
+        d2[r] = F(2) * top.b + xn;
+        if (queue) {
+            const double xl = sqrt(fmax((double)xn, 0.0));
+            const double e = 1.0625 * u * (cmax * cmax + (double)(d + 2) * xl * cmax);
+            const double band = 2.0 * e;
+            if ((double)top.s - (double)top.b <= band)
+                enqueue_recheck(queue, n, st, (int)r, top.ib, top.is, (double)top.t - (double)top.b <= band);
+        }
+    }
+}
+
 }  // namespace
 
 template <typename F>
@@ -321,11 +379,27 @@ void launch_row_norms(const F *X, int64_t n, int64_t d, F *xnorm, cudaStream_t s
     KMB_LAUNCHED();
 }
 
+template <typename F, int DMAX>
+void launch_small(const F *X, int64_t n, int64_t d, const F *Ct, const F *h, int64_t k, int64_t kpad, const F *xnorm,
+                  const double *cnorm_max, int32_t *labels, F *d2, RecheckEntry *queue, LoopState *st,
+                  cudaStream_t s) {
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((n + kSmallThreads - 1) / kSmallThreads, 148 * 16));
+    assign_small_kernel<F, DMAX><<<(unsigned)blocks, kSmallThreads, 0, s>>>(X, n, (int)d, Ct, h, (int)k, (int)kpad,
+                                                                           xnorm, cnorm_max, labels, d2, queue, st);
+    KMB_LAUNCHED();
+}
+
 template <typename F>
 void launch_assign_plain(const F *X, int64_t n, int64_t d, const F *Ct, const F *h, int64_t k, int64_t kpad,
                          const F *xnorm, const double *cnorm_max, int32_t *labels, F *d2, RecheckEntry *queue,
                          LoopState *st, cudaStream_t s) {
     if (n == 0) return;
+    if (k <= kSmallK && d <= 64) {  // few clusters: row per thread, centroids in shared memory
+        if (d <= 16) launch_small<F, 16>(X, n, d, Ct, h, k, kpad, xnorm, cnorm_max, labels, d2, queue, st, s);
+        else if (d <= 32) launch_small<F, 32>(X, n, d, Ct, h, k, kpad, xnorm, cnorm_max, labels, d2, queue, st, s);
+        else launch_small<F, 64>(X, n, d, Ct, h, k, kpad, xnorm, cnorm_max, labels, d2, queue, st, s);
+        return;
+    }
     const unsigned blocks = (unsigned)((n + BM - 1) / BM);
     const bool vec = (d % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) % (4 * sizeof(F))) == 0);
     if (vec) {
