@@ -1,0 +1,107 @@
+"""GPU side of the row-sharded Lloyd path (onedal_b200.spmd.DeviceShardOps over
+kmb_partial_sums / kmb_finalize_centroids), in one process on one GPU:
+
+- shards of one matrix give per-shard FP64 sums and counts whose sum, finalized on
+  the device, is the FP64 oracle's single-process update (responses, centroids,
+  shift, empty clusters), with widths that take several 128-column tiles;
+- train_spmd over a one-rank NCCL group equals the oracle's training run
+  (responses, iteration count, centroids, objective), an emptied cluster included.
+
+The exchange itself with two and three ranks is covered on the CPU (gloo) with the
+same train_spmd code."""
+import datetime
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+
+from helpers import centroid_rel_err, rel_close
+from onedal_b200 import _native
+from onedal_b200.spmd import DeviceShardOps, train_spmd
+from oracle import restated
+
+pytestmark = pytest.mark.gpu
+
+CENTROID_TOL = {np.float32: 1e-6, np.float64: 1e-12}
+
+
+def _blobs(n, d, k, dt, seed, far_centroid=False):
+    rng = np.random.default_rng(seed)
+    centers = rng.uniform(-20, 20, (k, d))
+    lab = rng.integers(0, k, n)
+    X = (centers[lab] + rng.standard_normal((n, d))).astype(dt)
+    # one start near each blob's center: no row lies near a bisector, so float32
+    # responses equal the FP64 oracle's
+    C0 = (centers + 0.1 * rng.standard_normal((k, d))).astype(dt)
+    if far_centroid:
+        C0[k // 2] = 1e4  # nearest to no row: its cluster is empty after the first assignment
+    return X, C0
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("d,k,far", [(300, 37, False), (130, 129, True), (20, 5, False)])
+def test_shard_sums_match_single_update(dt, d, k, far):
+    n = 20000
+    X, C0 = _blobs(n, d, k, dt, seed=d + k, far_centroid=far)
+    Cd = torch.from_numpy(C0).cuda()
+    cuts = [0, 7001, 12000, n]
+    sums = torch.zeros((k, d), dtype=torch.float64, device="cuda")
+    counts = torch.zeros(k, dtype=torch.int64, device="cuda")
+    labels = []
+    sq = 0.0
+    ops = None
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        ops = DeviceShardOps(torch.from_numpy(X[a:b]).cuda())
+        st = ops.partial(Cd)
+        sums += st.sums
+        counts += st.counts
+        labels.append(st.labels.cpu().numpy())
+        sq += st.sq_total
+    C_new, shift, empty = ops.finalize(sums, counts, Cd)
+    torch.cuda.synchronize()
+
+    C64, lab64, shift64, ne64, _ = restated.step(X.astype(np.float64), C0.astype(np.float64))
+    g_lab = np.concatenate(labels)
+    assert (g_lab == lab64).all()
+    assert np.array_equal(counts.cpu().numpy(), np.bincount(lab64, minlength=k))
+    assert len(empty) == ne64 == (1 if far else 0)
+    if far:
+        assert empty == [k // 2]
+    # finalize leaves an empty cluster's centroid as it was; the oracle reseeds it
+    keep = np.ones(k, bool)
+    keep[empty] = False
+    g_C = C_new.cpu().numpy()
+    assert centroid_rel_err(C64[keep], g_C[keep]) < CENTROID_TOL[dt]
+    assert np.array_equal(g_C[~keep], C0[~keep])
+    if not far:
+        assert rel_close(shift, shift64, 1e-6)
+    obj = restated.objective(X.astype(np.float64), C0.astype(np.float64), lab64)
+    assert rel_close(sq, obj, 1e-4 if dt == np.float32 else 1e-10)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+@pytest.mark.parametrize("far", [False, True])
+def test_train_spmd_one_rank_nccl(far):
+    X, C0 = _blobs(30000, 160, 48, np.float64, seed=77, far_centroid=far)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60), device_id=torch.device("cuda", 0))
+    try:
+        ops = DeviceShardOps(torch.from_numpy(X).cuda(), _native.KMB_FORM_PLAIN)
+        C, lab, it, obj = train_spmd(ops, torch.from_numpy(C0).cuda(), 25, 0.0)
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+    Cr, labr, objr, itr = restated.train(X, C0, 25, 0.0)
+    assert it == itr
+    assert (lab.cpu().numpy() == labr).all()
+    assert centroid_rel_err(Cr, C.cpu().numpy()) < 1e-12
+    assert rel_close(obj, objr, 1e-10)
