@@ -295,7 +295,8 @@ int check_form(kmb_context *ctx, int dtype, int form) {
 int resolve_form(int dtype, int form, int64_t n, int64_t k, int64_t d) {
     if (form != KMB_FORM_AUTO) return form;
     if (dtype != KMB_F32 || !kmb::tc_supported(d)) return KMB_FORM_PLAIN;
-    const double macs = (double)n * (double)kmb::tc_kpad(k) * (double)kmb::tc_dpad(d);
+    // kpad: k rounded up to 128 clusters, dpad: d rounded up to 64 features
+    const double macs = (double)n * (double)round_up(k, 128) * (double)kmb::tc_dpad(d);
     return macs >= (double)KMB_AUTO_TC_MACS ? KMB_FORM_BF16X3 : KMB_FORM_PLAIN;
 }
 

@@ -21,13 +21,15 @@
 //
 // Kernel structure (one CTA per SM, persistent over 128-row tiles, 14 warps):
 //   warp 0   TMA producer: A = the tile's Xhi/Xlo panels (128 rows x 64 bf16,
-//            SWIZZLE_128B), B = Chi/Clo panels of 128 clusters, ring of stages
-//   warp 1   TMEM allocation + single-thread tcgen05.mma issue; commits free
-//            B stages, publish accumulators and release A tiles
+//            SWIZZLE_128B), B = Chi/Clo panels of 256 clusters x 32 bf16
+//            (SWIZZLE_64B), ring of stages
+//   warp 1   TMEM allocation + single-thread tcgen05.mma issue (M=128, N=256,
+//            K=16); commits free B stages, publish accumulators and release A tiles
 //   warps 2-13 epilogue, three groups of 4 warps (one per TMEM lane quarter):
-//            the running cluster tiles go round the groups. Before the MMAs of
-//            a tile start, the group that drained the accumulator last writes
-//            -h_j into every lane of it (tcgen05.st), so the MMAs leave
+//            group g drains the 32-column chunks g, g+3, g+6 of every
+//            accumulator. Before the MMAs of a tile start, the drain of the
+//            accumulator's previous tile writes -h_j into every lane of it
+//            (tcgen05.st), so the MMAs leave
 //            y = x.c - h = -score there and no per-score subtraction is needed.
 //            A group reads y with tcgen05.ld (one TMEM lane = one row per
 //            thread) and keeps a running top-3 per row: each 32-column chunk
@@ -37,8 +39,10 @@
 //            their top-3 to group 0 through a small global scratch (per SM, by
 //            row-tile parity) and a named barrier; group 0 merges and writes
 //            the row's outputs.
-// Four accumulators (all 512 TMEM columns) rotate through the groups, so
-// while one group drains an accumulator the MMAs fill the others. Every mbarrier
+// Two accumulators of 256 columns (all 512 TMEM columns): while the groups drain
+// one, the MMAs fill the other. The 256-wide tile halves the shared-memory reads
+// of the A panels per MMA; at N=128 the operand reads plus the B panel writes
+// exceeded the shared-memory bandwidth at full tensor rate. Every mbarrier
 // wait is bounded; on timeout the
 // CTA records KMB_ETIMEDOUT in the loop state, drains its own TMA loads and
 // MMAs with bounded waits, frees TMEM and returns.
@@ -53,10 +57,15 @@ namespace kmb {
 namespace tc {
 
 constexpr int BM = 128;                 // rows per tile (UMMA M)
-constexpr int BN = 128;                 // clusters per tile (UMMA N)
-constexpr int KP = 64;                  // bf16 per panel row (128 bytes, SWIZZLE_128B)
-constexpr int PANEL = 128 * 128;        // bytes per 128-row panel
-constexpr int NACC = 4;                 // TMEM accumulators: two per epilogue group (double-buffered)
+constexpr int BN = 256;                 // clusters per tile (UMMA N)
+constexpr int KP = 64;                  // bf16 per A panel row (128 bytes, SWIZZLE_128B)
+#ifndef KMB_TC_KPB
+#define KMB_TC_KPB 32
+#endif
+constexpr int KPB = KMB_TC_KPB;         // bf16 per B panel row (64 bytes, SWIZZLE_64B)
+constexpr int PANEL = 128 * 128;        // bytes per A panel (128 rows x 128 B)
+constexpr int PANEL_B = BN * KPB * 2;   // bytes per B panel (256 rows x 64 B)
+constexpr int NACC = 2;                 // TMEM accumulators (double-buffered)
 constexpr int TMEM_COLS = NACC * BN;    // 512 = all of TMEM
 constexpr int NGROUPS = 3;              // epilogue groups of 4 warps (one warp per TMEM lane quarter)
 constexpr int NTHREADS = 64 + NGROUPS * 128;  // warp 0 TMA, warp 1 MMA, warps 2.. epilogue
@@ -155,6 +164,18 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     d |= (uint64_t)(1024 >> 4) << 32; // SBO
     d |= (uint64_t)1 << 46;          // version
     d |= (uint64_t)2 << 61;          // SWIZZLE_128B
+    return d;
+}
+
+// K-major B panel descriptor: rows of KPB bf16 (64 B: SWIZZLE_64B, layout 4;
+// 32 B: SWIZZLE_32B, layout 6), SBO = 8 rows between 8-row groups.
+__device__ __forceinline__ uint64_t swb_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+    d |= (uint64_t)1 << 16;                       // LBO
+    d |= (uint64_t)((8 * KPB * 2) >> 4) << 32;    // SBO
+    d |= (uint64_t)1 << 46;                       // version
+    d |= (uint64_t)(KPB == 32 ? 4 : 6) << 61;     // SWIZZLE_64B / SWIZZLE_32B
     return d;
 }
 
@@ -302,7 +323,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
     const int a_stage_bytes = 2 * p.kpanels * PANEL;  // hi + lo panels
     uint8_t *A = smem;
     uint8_t *B = A + (size_t)p.a_stages * a_stage_bytes;
-    Barriers *bar = (Barriers *)(B + (size_t)p.b_stages * 2 * PANEL);
+    Barriers *bar = (Barriers *)(B + (size_t)p.b_stages * 2 * PANEL_B);
     volatile int *abort = &bar->abort;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -317,7 +338,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
         }
         for (int i = 0; i < NACC; ++i) {
             mbar_init(&bar->acc_full[i], 1);
-            mbar_init(&bar->acc_empty[i], 4);
+            mbar_init(&bar->acc_empty[i], 4 * NGROUPS);
         }
         mbar_init(&bar->mma_done, 1);
         bar->abort = 0;
@@ -361,12 +382,12 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 }
                 a_issued[as]++;
                 for (int j = 0; j < p.ntiles_n && ok; ++j) {
-                    for (int kp = 0; kp < p.kpanels; ++kp) {
+                    for (int kb = 0; kb < p.kpanels * (KP / KPB); ++kb) {
                         if (!mbar_wait(&bar->b_empty[bs], bphase ^ 1, abort)) { ok = false; break; }
-                        mbar_expect_tx(&bar->b_full[bs], 2 * PANEL);
-                        uint8_t *Bb = B + (size_t)bs * 2 * PANEL;
-                        tma_load_2d(Bb, &tmCh, &bar->b_full[bs], kp * KP, j * BN);
-                        tma_load_2d(Bb + PANEL, &tmCl, &bar->b_full[bs], kp * KP, j * BN);
+                        mbar_expect_tx(&bar->b_full[bs], 2 * PANEL_B);
+                        uint8_t *Bb = B + (size_t)bs * 2 * PANEL_B;
+                        tma_load_2d(Bb, &tmCh, &bar->b_full[bs], kb * KPB, j * BN);
+                        tma_load_2d(Bb + PANEL_B, &tmCl, &bar->b_full[bs], kb * KPB, j * BN);
                         b_issued[bs]++;
                         if (++bs == p.b_stages) {
                             bs = 0;
@@ -403,16 +424,18 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                     if (!mbar_wait(&bar->acc_empty[slot], use & 1, abort)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t tmem_d = tmem_base + (uint32_t)(slot * BN);
-                    for (int kp = 0; kp < p.kpanels; ++kp) {
+                    for (int kb = 0; kb < p.kpanels * (KP / KPB); ++kb) {
                         if (!mbar_wait(&bar->b_full[bs], bphase, abort)) { ok = false; break; }
                         tc_fence_after();
-                        const uint64_t ah = sw128_desc(a_base + kp * PANEL);
-                        const uint64_t al = sw128_desc(a_base + (p.kpanels + kp) * PANEL);
-                        const uint64_t bh = sw128_desc(su32(B + (size_t)bs * 2 * PANEL));
-                        const uint64_t bl = sw128_desc(su32(B + (size_t)bs * 2 * PANEL + PANEL));
+                        // A: the 64-wide panel holding this 32-wide slice, advanced to the slice
+                        const int kp = kb / (KP / KPB), ka = (kb % (KP / KPB)) * (KPB * 2 / 16);
+                        const uint64_t ah = sw128_desc(a_base + kp * PANEL) + ka;
+                        const uint64_t al = sw128_desc(a_base + (p.kpanels + kp) * PANEL) + ka;
+                        const uint64_t bh = swb_desc(su32(B + (size_t)bs * 2 * PANEL_B));
+                        const uint64_t bl = swb_desc(su32(B + (size_t)bs * 2 * PANEL_B + PANEL_B));
                         // 16 bf16 = 32 bytes along the swizzled row = 2 in the descriptor's address field
 #pragma unroll
-                        for (int ks = 0; ks < KP / 16; ++ks)
+                        for (int ks = 0; ks < KPB / 16; ++ks)
                             mma_bf16x3(tmem_d, ah + 2 * ks, al + 2 * ks, bh + 2 * ks, bl + 2 * ks);
                         mma_commit(&bar->b_empty[bs]);  // frees the B stage once these MMAs finish
                         if (++bs == p.b_stages) {
@@ -435,14 +458,15 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
         const int row_in_tile = quarter * 32 + lane;
         const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
         long long acount = 0;
-        int arot = 0;  // acount % NGROUPS
         bool ok = true;
         // Accumulators start from -h (written here, one row per lane), so after the
         // MMAs they hold y = x.c - h = -score and the argmin becomes a max over y.
-        for (int a0 = group; a0 < NACC; a0 += NGROUPS) {  // first uses of the accumulators, spread over the groups
+        // Every group drains the 32-column chunks group, group + NGROUPS, ... of each
+        // accumulator (ascending columns within a group).
+        for (int a0 = 0; a0 < NACC; ++a0) {  // first uses of the accumulators
             const float *hn = p.h + (size_t)(a0 % p.ntiles_n) * BN;
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 32) {
+            for (int c0 = 32 * group; c0 < BN; c0 += 32 * NGROUPS) {
                 __syncwarp();
                 tmem_st32_from(lane_base + (uint32_t)(a0 * BN + c0), hn + c0);
             }
@@ -478,8 +502,8 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             r.b = r.s = r.t = __int_as_float(0xff800000);
             r.ib = r.is = 0;
             float thr = thr0;  // values below thr cannot change the outputs
-            for (int j = 0; j < p.ntiles_n; ++j, ++acount, arot = (arot + 1 == NGROUPS) ? 0 : arot + 1) {
-                if (arot != group || !ok) continue;  // running cluster tiles go round the groups
+            for (int j = 0; j < p.ntiles_n; ++j, ++acount) {
+                if (!ok) continue;
                 const int slot = (int)(acount % NACC);
                 const int use = (int)(acount / NACC);
                 // every lane waits; the warp proceeds only if all lanes saw completion
@@ -491,7 +515,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 // -h of the cluster tile this accumulator holds next
                 const float *hn = p.h + (size_t)((acount + NACC) % p.ntiles_n) * BN;
 #pragma unroll 1
-                for (int c0 = 0; c0 < BN; c0 += 32) {
+                for (int c0 = 32 * group; c0 < BN; c0 += 32 * NGROUPS) {
                     float v[32];
                     __syncwarp();  // tcgen05.ld/st are warp-collective: reconverge after the filtered path
                     const uint32_t taddr = lane_base + (uint32_t)(slot * BN + c0);
@@ -771,15 +795,20 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
-static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t dpad) {
+// Row panels: the split rows (128 rows x 64 bf16, SWIZZLE_128B) or the split
+// centroids (256 clusters x 32 bf16, SWIZZLE_64B).
+static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t dpad, bool centroids) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)dpad, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)dpad * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)tc::KP, 128u};
+    const cuuint32_t box[2] = {centroids ? (cuuint32_t)tc::KPB : (cuuint32_t)tc::KP,
+                               centroids ? (cuuint32_t)tc::BN : (cuuint32_t)tc::BM};
     const cuuint32_t estr[2] = {1u, 1u};
-    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
-                                  estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE,
+               centroids ? (tc::KPB == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B)
+                         : CU_TENSOR_MAP_SWIZZLE_128B,
                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -801,17 +830,17 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     const int a_stage = 2 * kpanels * tc::PANEL;
     const int fixed = 1024 + (int)sizeof(tc::Barriers) + 64;
     int a_stages = (2 * a_stage + 3 * 2 * tc::PANEL + fixed <= optin) ? 2 : 1;
-    int b_stages = (optin - fixed - a_stages * a_stage) / (2 * tc::PANEL);
+    int b_stages = (optin - fixed - a_stages * a_stage) / (2 * tc::PANEL_B);
     b_stages = std::min(b_stages, tc::MAX_B_STAGES);
     if (b_stages < 2) return KMB_EUNSUPPORTED;
     // More than half of an SM's shared memory: one CTA per SM, which the
     // %smid-indexed hand-off slots rely on.
-    const size_t smem = std::max<size_t>((size_t)a_stages * a_stage + (size_t)b_stages * 2 * tc::PANEL + fixed,
+    const size_t smem = std::max<size_t>((size_t)a_stages * a_stage + (size_t)b_stages * 2 * tc::PANEL_B + fixed,
                                          (size_t)optin / 2 + 4096);
 
     CUtensorMap mXh, mXl, mCh, mCl;
-    if (!encode_map(&mXh, Xhi, n, dpad) || !encode_map(&mXl, Xlo, n, dpad) || !encode_map(&mCh, Chi, kpad, dpad) ||
-        !encode_map(&mCl, Clo, kpad, dpad))
+    if (!encode_map(&mXh, Xhi, n, dpad, false) || !encode_map(&mXl, Xlo, n, dpad, false) ||
+        !encode_map(&mCh, Chi, kpad, dpad, true) || !encode_map(&mCl, Clo, kpad, dpad, true))
         return KMB_ECUDA;
     tc::Params p;
     p.n = n;
