@@ -28,8 +28,8 @@ import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-# (526.82 MB read + 10.67 MB written) / 1,000,000 rows, assign_tc_kernel at d=128, k=1024
-TC_DRAM_BYTES_PER_ROW = 537.49
+# (526.31 MB read + 10.91 MB written) / 1,000,000 rows, assign_tc_kernel at d=128, k=1024
+TC_DRAM_BYTES_PER_ROW = 537.21
 sys.path.insert(0, ROOT)
 
 METRIC = "Lloyd iter/s n=20M,d=128,k=1024 BF16-TC vs FP32 plain; p50/p99 infer latency"
