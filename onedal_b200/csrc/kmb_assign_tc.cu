@@ -21,12 +21,13 @@
 //
 // Kernel structure (one CTA per SM, persistent over 128-row tiles, 14 warps):
 //   warp 0   TMA producer: A = the tile's Xhi/Xlo panels (128 rows x 64 bf16,
-//            SWIZZLE_128B), B = Chi/Clo panels of 256 clusters x 32 bf16
-//            (SWIZZLE_64B), ring of stages
-//   warp 1   TMEM allocation + single-thread tcgen05.mma issue (M=128, N=256,
+//            SWIZZLE_128B), B = Chi/Clo panels of BN clusters (BN = 256: 32 bf16,
+//            SWIZZLE_64B; BN = 128 where padding k to 256 would cost more than
+//            the wider tile gains: 64 bf16, SWIZZLE_128B), ring of 32 KB stages
+//   warp 1   TMEM allocation + single-thread tcgen05.mma issue (M=128, N=BN,
 //            K=16); commits free B stages, publish accumulators and release A tiles
 //   warps 2-13 epilogue, three groups of 4 warps (one per TMEM lane quarter):
-//            group g drains the 32-column chunks g, g+3, g+6 of every
+//            group g drains the 32-column chunks g, g+3, g+6, ... of every
 //            accumulator. Before the MMAs of a tile start, the drain of the
 //            accumulator's previous tile writes -h_j into every lane of it
 //            (tcgen05.st), so the MMAs leave
@@ -39,8 +40,8 @@
 //            their top-3 to group 0 through a small global scratch (per SM, by
 //            row-tile parity) and a named barrier; group 0 merges and writes
 //            the row's outputs.
-// Two accumulators of 256 columns (all 512 TMEM columns): while the groups drain
-// one, the MMAs fill the other. The 256-wide tile halves the shared-memory reads
+// 512 / BN accumulators of BN columns (all 512 TMEM columns): while the groups
+// drain one, the MMAs fill the others. The 256-wide tile halves the shared-memory reads
 // of the A panels per MMA; at N=128 the operand reads plus the B panel writes
 // exceeded the shared-memory bandwidth at full tensor rate. Every mbarrier
 // wait is bounded; on timeout the
@@ -57,14 +58,17 @@ namespace kmb {
 namespace tc {
 
 constexpr int BM = 128;                 // rows per tile (UMMA M)
-constexpr int BN = 256;                 // clusters per tile (UMMA N)
+// Clusters per tile (UMMA N) is the kernel's template parameter BN: 256 when
+// the padded cluster count (a multiple of 128) divides by 256, else 128.
 constexpr int KP = 64;                  // bf16 per A panel row (128 bytes, SWIZZLE_128B)
-constexpr int KPB = 32;                 // bf16 per B panel row (64 bytes, SWIZZLE_64B; 16-wide
-                                        // panels in six stages measured 11 % slower)
+// bf16 per B panel row: 32 (64 B, SWIZZLE_64B) for 256-cluster tiles, 64 (128 B,
+// SWIZZLE_128B) for 128-cluster tiles, so a B stage (hi + lo panels) is 32 KB
+// either way; 16-wide panels in six stages measured 11 % slower.
+__host__ __device__ constexpr int kpb_of(int bn) { return bn == 256 ? 32 : 64; }
 constexpr int PANEL = 128 * 128;        // bytes per A panel (128 rows x 128 B)
-constexpr int PANEL_B = BN * KPB * 2;   // bytes per B panel (256 rows x 64 B)
-constexpr int NACC = 2;                 // TMEM accumulators (double-buffered)
-constexpr int TMEM_COLS = NACC * BN;    // 512 = all of TMEM
+constexpr int TMEM_COLS = 512;          // all of TMEM: 512 / BN accumulators of BN columns
+constexpr int kMaxAcc = 4;
+__host__ __device__ constexpr int panel_b_bytes(int bn) { return bn * kpb_of(bn) * 2; }  // one B panel (16 KB)
 constexpr int NGROUPS = 3;              // epilogue groups of 4 warps (one warp per TMEM lane quarter)
 constexpr int NTHREADS = 64 + NGROUPS * 128;  // warp 0 TMA, warp 1 MMA, warps 2.. epilogue
 constexpr int MAX_B_STAGES = 8;
@@ -96,7 +100,7 @@ struct Params {
 struct Barriers {
     uint64_t a_full[2], a_empty[2];
     uint64_t b_full[MAX_B_STAGES], b_empty[MAX_B_STAGES];
-    uint64_t acc_full[NACC], acc_empty[NACC];
+    uint64_t acc_full[kMaxAcc], acc_empty[kMaxAcc];
     uint64_t mma_done;
     uint32_t tmem_base;
     int abort;
@@ -165,31 +169,36 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     return d;
 }
 
-// K-major B panel descriptor: rows of KPB bf16 (64 B: SWIZZLE_64B, layout 4;
-// 32 B: SWIZZLE_32B, layout 6), SBO = 8 rows between 8-row groups.
+// K-major B panel descriptor: rows of KPB bf16 (128 B: SWIZZLE_128B, layout 2;
+// 64 B: SWIZZLE_64B, layout 4), SBO = 8 rows between 8-row groups.
+template <int KPB>
 __device__ __forceinline__ uint64_t swb_desc(uint32_t saddr) {
+    static_assert(KPB == 32 || KPB == 64, "B panel width");
     uint64_t d = 0;
     d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
     d |= (uint64_t)1 << 16;                       // LBO
     d |= (uint64_t)((8 * KPB * 2) >> 4) << 32;    // SBO
     d |= (uint64_t)1 << 46;                       // version
-    d |= (uint64_t)(KPB == 32 ? 4 : 6) << 61;     // SWIZZLE_64B / SWIZZLE_32B
+    d |= (uint64_t)(KPB == 32 ? 4 : 2) << 61;     // SWIZZLE_64B / SWIZZLE_128B
     return d;
 }
 
-// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=BN.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=bn.
+__host__ __device__ constexpr uint32_t make_idesc(int bn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
 
 // The three split-BF16 products of one k-step (xh.ch, xh.cl, xl.ch) into one
 // accumulator; descriptors are passed precomputed.
-__device__ __forceinline__ void mma_bf16x3(uint32_t tmem_d, uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl) {
+__device__ __forceinline__ void mma_bf16x3(uint32_t tmem_d, uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl,
+                                           uint32_t idesc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, 1, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %3, %5, p;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %4, %5, p;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %2, %3, %5, p;\n\t}" ::"r"(tmem_d),
-        "l"(ah), "l"(al), "l"(bh), "l"(bl), "r"(kIdesc)
+        "l"(ah), "l"(al), "l"(bh), "l"(bl), "r"(idesc)
         : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -308,9 +317,15 @@ __device__ __forceinline__ Top3 top3_merge(const Top3 &x, const Top3 &y) {
 }
 
 
+template <int BN>
 __global__ void __launch_bounds__(NTHREADS, 1)
 assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant__ CUtensorMap tmXl,
                  const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl, Params p) {
+    constexpr int NACC = TMEM_COLS / BN;  // TMEM accumulators (double-buffered or more)
+    constexpr int PANEL_B = panel_b_bytes(BN);
+    constexpr int KPB = kpb_of(BN);
+    constexpr uint32_t kIdesc = make_idesc(BN);
+    static_assert(NACC >= 2 && NACC <= kMaxAcc, "accumulator count");
     // One read of the loop flag for the whole CTA, so every thread takes the same path.
     __shared__ int s_skip;
     if (threadIdx.x == 0) s_skip = p.st->done;
@@ -429,12 +444,12 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                         const int kp = kb / (KP / KPB), ka = (kb % (KP / KPB)) * (KPB * 2 / 16);
                         const uint64_t ah = sw128_desc(a_base + kp * PANEL) + ka;
                         const uint64_t al = sw128_desc(a_base + (p.kpanels + kp) * PANEL) + ka;
-                        const uint64_t bh = swb_desc(su32(B + (size_t)bs * 2 * PANEL_B));
-                        const uint64_t bl = swb_desc(su32(B + (size_t)bs * 2 * PANEL_B + PANEL_B));
+                        const uint64_t bh = swb_desc<KPB>(su32(B + (size_t)bs * 2 * PANEL_B));
+                        const uint64_t bl = swb_desc<KPB>(su32(B + (size_t)bs * 2 * PANEL_B + PANEL_B));
                         // 16 bf16 = 32 bytes along the swizzled row = 2 in the descriptor's address field
 #pragma unroll
                         for (int ks = 0; ks < KPB / 16; ++ks)
-                            mma_bf16x3(tmem_d, ah + 2 * ks, al + 2 * ks, bh + 2 * ks, bl + 2 * ks);
+                            mma_bf16x3(tmem_d, ah + 2 * ks, al + 2 * ks, bh + 2 * ks, bl + 2 * ks, kIdesc);
                         mma_commit(&bar->b_empty[bs]);  // frees the B stage once these MMAs finish
                         if (++bs == p.b_stages) {
                             bs = 0;
@@ -751,7 +766,18 @@ __global__ void reset_cmax_kernel(double *p, double *prev, const LoopState *st) 
 size_t tc_xchg_bytes() { return (size_t)tc::kMaxSmid * 2 * (tc::NGROUPS - 1) * tc::BM * sizeof(tc::Top3x); }
 
 int64_t tc_dpad(int64_t d) { return (d + tc::KP - 1) / tc::KP * tc::KP; }
-int64_t tc_kpad(int64_t k) { return (k + tc::BN - 1) / tc::BN * tc::BN; }
+// Cluster tile (UMMA N) for k clusters: 256 unless its padding costs more than
+// the wider tile gains. Per padded column the 256-wide tile ran 1.16x faster than
+// the 128-wide one (20M x 128, k = 1152: 17.25 ms padded to 1280 against 17.86 ms
+// at 1152), so 128 is kept where padding to 256 adds more than 16 %.
+int tc_tile_n(int64_t k) {
+    const int64_t k128 = (k + 127) / 128 * 128, k256 = (k + 255) / 256 * 256;
+    return k256 * 100 <= k128 * 116 ? 256 : 128;
+}
+int64_t tc_kpad(int64_t k) {
+    const int64_t bn = tc_tile_n(k);
+    return (k + bn - 1) / bn * bn;
+}
 bool tc_supported(int64_t d) { return tc_dpad(d) <= 256; }
 
 void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, float *xnorm, int num_sms,
@@ -795,18 +821,17 @@ static EncodeTiledFn encode_fn() {
 
 // Row panels: the split rows (128 rows x 64 bf16, SWIZZLE_128B) or the split
 // centroids (256 clusters x 32 bf16, SWIZZLE_64B).
-static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t dpad, bool centroids) {
+static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t dpad, bool centroids, int bn = 0) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)dpad, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)dpad * 2};
-    const cuuint32_t box[2] = {centroids ? (cuuint32_t)tc::KPB : (cuuint32_t)tc::KP,
-                               centroids ? (cuuint32_t)tc::BN : (cuuint32_t)tc::BM};
+    const cuuint32_t box[2] = {centroids ? (cuuint32_t)tc::kpb_of(bn) : (cuuint32_t)tc::KP,
+                               centroids ? (cuuint32_t)bn : (cuuint32_t)tc::BM};
     const cuuint32_t estr[2] = {1u, 1u};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE,
-               centroids ? (tc::KPB == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B)
-                         : CU_TENSOR_MAP_SWIZZLE_128B,
+               (centroids && tc::kpb_of(bn) == 32) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -827,18 +852,20 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     const int kpanels = (int)(dpad / tc::KP);
     const int a_stage = 2 * kpanels * tc::PANEL;
     const int fixed = 1024 + (int)sizeof(tc::Barriers) + 64;
-    int a_stages = (2 * a_stage + 3 * 2 * tc::PANEL + fixed <= optin) ? 2 : 1;
-    int b_stages = (optin - fixed - a_stages * a_stage) / (2 * tc::PANEL_B);
+    const int bn = tc_tile_n(k);  // cluster tile (UMMA N); kpad is a multiple of it
+    const int panel_b = tc::panel_b_bytes(bn);
+    int a_stages = (2 * a_stage + 3 * 2 * panel_b + fixed <= optin) ? 2 : 1;
+    int b_stages = (optin - fixed - a_stages * a_stage) / (2 * panel_b);
     b_stages = std::min(b_stages, tc::MAX_B_STAGES);
     if (b_stages < 2) return KMB_EUNSUPPORTED;
     // More than half of an SM's shared memory: one CTA per SM, which the
     // %smid-indexed hand-off slots rely on.
-    const size_t smem = std::max<size_t>((size_t)a_stages * a_stage + (size_t)b_stages * 2 * tc::PANEL_B + fixed,
+    const size_t smem = std::max<size_t>((size_t)a_stages * a_stage + (size_t)b_stages * 2 * panel_b + fixed,
                                          (size_t)optin / 2 + 4096);
 
     CUtensorMap mXh, mXl, mCh, mCl;
     if (!encode_map(&mXh, Xhi, n, dpad, false) || !encode_map(&mXl, Xlo, n, dpad, false) ||
-        !encode_map(&mCh, Chi, kpad, dpad, true) || !encode_map(&mCl, Clo, kpad, dpad, true))
+        !encode_map(&mCh, Chi, kpad, dpad, true, bn) || !encode_map(&mCl, Clo, kpad, dpad, true, bn))
         return KMB_ECUDA;
     tc::Params p;
     p.n = n;
@@ -848,7 +875,7 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     p.kpad = (int)kpad;
     p.n_tiles = (int)((n + tc::BM - 1) / tc::BM);
     p.kpanels = kpanels;
-    p.ntiles_n = (int)(kpad / tc::BN);
+    p.ntiles_n = (int)(kpad / bn);
     p.a_stages = a_stages;
     p.b_stages = b_stages;
     p.h = h;
@@ -865,13 +892,13 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
                                                  (int)k, prior ? 1 : 0, (float2 *)rowb, st);
         KMB_LAUNCHED();
     }
-    if (cudaFuncSetAttribute(tc::assign_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
+    auto kern = bn == 256 ? tc::assign_tc_kernel<256> : tc::assign_tc_kernel<128>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return KMB_ECUDA;
     // num_sms < 0: one CTA per 128-row tile (no persistence), so that other
     // streams' launches interleave with this one at tile granularity
     const int grid = num_sms < 0 ? p.n_tiles : (int)std::min<int64_t>(num_sms, p.n_tiles);
-    tc::assign_tc_kernel<<<grid, tc::NTHREADS, smem, s>>>(mXh, mXl, mCh, mCl, p);
+    kern<<<grid, tc::NTHREADS, smem, s>>>(mXh, mXl, mCh, mCl, p);
     KMB_LAUNCHED();
     return cudaGetLastError() == cudaSuccess ? KMB_OK : KMB_ECUDA;
 }

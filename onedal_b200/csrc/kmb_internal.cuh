@@ -155,7 +155,8 @@ void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, con
 
 // ---- assignment (tensor-core BF16x3 form, float32 data) ----------------------
 int64_t tc_dpad(int64_t d);   // d rounded up to the 64-wide K panel
-int64_t tc_kpad(int64_t k);   // k rounded up to the 256-wide cluster tile
+int tc_tile_n(int64_t k);      // cluster tile of the tensor-core kernel: 128 or 256
+int64_t tc_kpad(int64_t k);   // k rounded up to a multiple of tc_tile_n(k)
 bool tc_supported(int64_t d); // dpad <= 256
 // X (rows x d, FP32) -> hi/lo BF16 [rows][dpad], zero padded.
 // x -> BF16 hi/lo panels [rows][dpad] and ||x||^2 (the same value launch_row_norms gives).
