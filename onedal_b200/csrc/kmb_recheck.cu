@@ -19,8 +19,40 @@ namespace {
 // of ||c||^2 and x.c for both candidates in double (consecutive lanes read
 // consecutive floats of the row and of each centroid), then three butterfly
 // steps give the group's totals; both candidates' sums have the same
-// association, so equal centroids give equal scores.
+// association, so equal centroids give equal scores. With VEC (float rows, d a
+// multiple of 4, 16-byte aligned bases) lane l reads 16 bytes at a time
+// (t = 4l .. 4l+3, then 32 further), a quarter of the loads in flight per row.
 template <typename F>
+__device__ __forceinline__ void pair_sums(const F *x, const F *ca, const F *cb, int d, int sub, double &cca,
+                                          double &xca, double &ccb, double &xcb) {
+    for (int t = sub; t < d; t += 8) {
+        const double xv = (double)x[t], va = (double)ca[t], vb = (double)cb[t];
+        cca = fma(va, va, cca);
+        xca = fma(xv, va, xca);
+        ccb = fma(vb, vb, ccb);
+        xcb = fma(xv, vb, xcb);
+    }
+}
+__device__ __forceinline__ void pair_sums_vec(const float *x, const float *ca, const float *cb, int d, int sub,
+                                              double &cca, double &xca, double &ccb, double &xcb) {
+    const float4 *x4 = reinterpret_cast<const float4 *>(x), *a4 = reinterpret_cast<const float4 *>(ca),
+                 *b4 = reinterpret_cast<const float4 *>(cb);
+#pragma unroll 4
+    for (int t = sub; t < (d >> 2); t += 8) {
+        const float4 xq = x4[t], aq = a4[t], bq = b4[t];
+        const double xv[4] = {xq.x, xq.y, xq.z, xq.w}, va[4] = {aq.x, aq.y, aq.z, aq.w},
+                     vb[4] = {bq.x, bq.y, bq.z, bq.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            cca = fma(va[i], va[i], cca);
+            xca = fma(xv[i], va[i], xca);
+            ccb = fma(vb[i], vb[i], ccb);
+            xcb = fma(xv[i], vb[i], xcb);
+        }
+    }
+}
+
+template <typename F, bool VEC>
 __global__ void __launch_bounds__(256) recheck_pairs_kernel(const F *__restrict__ X, int d, const F *__restrict__ C,
                                                             const RecheckEntry *__restrict__ queue,
                                                             int32_t *__restrict__ labels, F *__restrict__ d2,
@@ -46,13 +78,10 @@ __global__ void __launch_bounds__(256) recheck_pairs_kernel(const F *__restrict_
             const F *x = X + (int64_t)q.row * d;
             const F *ca = C + (int64_t)a * d;
             const F *cb = C + (int64_t)b * d;
-            for (int t = sub; t < d; t += 8) {
-                const double xv = (double)x[t], va = (double)ca[t], vb = (double)cb[t];
-                cca = fma(va, va, cca);
-                xca = fma(xv, va, xca);
-                ccb = fma(vb, vb, ccb);
-                xcb = fma(xv, vb, xcb);
-            }
+            if constexpr (VEC)
+                pair_sums_vec(x, ca, cb, d, sub, cca, xca, ccb, xcb);
+            else
+                pair_sums(x, ca, cb, d, sub, cca, xca, ccb, xcb);
         }
 #pragma unroll
         for (int m = 4; m >= 1; m >>= 1) {
@@ -181,7 +210,14 @@ __global__ void __launch_bounds__(256) recheck_full_kernel(const F *__restrict__
 template <typename F>
 void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, const RecheckEntry *queue,
                     int32_t *labels, F *d2, const F *xnorm, LoopState *st, int num_sms, cudaStream_t s) {
-    recheck_pairs_kernel<F><<<num_sms * 8, 256, 0, s>>>(X, (int)d, C, queue, labels, d2, xnorm, st);
+    bool vec = false;
+    if constexpr (sizeof(F) == 4) {
+        vec = d % 4 == 0 && (uintptr_t)X % 16 == 0 && (uintptr_t)C % 16 == 0;
+        if (vec)
+            recheck_pairs_kernel<float, true><<<num_sms * 8, 256, 0, s>>>(X, (int)d, C, queue, labels, d2, xnorm, st);
+    }
+    if (!vec)
+        recheck_pairs_kernel<F, false><<<num_sms * 8, 256, 0, s>>>(X, (int)d, C, queue, labels, d2, xnorm, st);
     KMB_LAUNCHED();
     // one wave (254 registers per thread: one 256-thread block per SM), a block per entry
     recheck_full_kernel<F><<<num_sms, 256, 0, s>>>(X, (int)d, C, (int)k, queue, n, labels, d2, xnorm, st);
