@@ -205,12 +205,127 @@ __global__ void __launch_bounds__(256) recheck_full_kernel(const F *__restrict__
     if (threadIdx.x == 0 && changed) atomicAdd(&st->n_changed, changed);
 }
 
+// Entries flagged for a full scan, R rows per block: the rows go to shared
+// memory, thread i scores clusters i, i + 256, ... against all R rows, so each
+// centroid row is read once per R entries instead of once per entry. A
+// cluster's ||c||^2 and x.c are summed in ascending coordinate order (one
+// association for every cluster); every thread keeps, per row, a running best
+// in ascending cluster order, then the warps and the block reduce with ties to
+// the lowest index.
+template <typename F, int R, bool VEC>
+__global__ void __launch_bounds__(256) recheck_full_rows_kernel(const F *__restrict__ X, int d,
+                                                                const F *__restrict__ C, int k,
+                                                                const RecheckEntry *__restrict__ queue, int64_t cap,
+                                                                int32_t *__restrict__ labels, F *__restrict__ d2,
+                                                                const F *__restrict__ xnorm, LoopState *st) {
+    if (st->done) return;
+    extern __shared__ __align__(16) unsigned char recheck_smem[];
+    F *xs = reinterpret_cast<F *>(recheck_smem);  // R x d
+    __shared__ double s_best[8][R];
+    __shared__ int s_idx[8][R];
+    __shared__ int s_row[R];
+    const int count = st->n_full;  // entries queue[cap - 1], queue[cap - 2], ...
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int changed = 0;
+    for (int e0 = blockIdx.x * R; e0 < count; e0 += gridDim.x * R) {
+        const int nr = min(R, count - e0);
+        if (threadIdx.x < R) s_row[threadIdx.x] = (int)threadIdx.x < nr ? queue[cap - 1 - (e0 + threadIdx.x)].row : 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < R * d; i += blockDim.x) {
+            const int r = i / d, t = i - r * d;
+            xs[i] = r < nr ? X[(int64_t)s_row[r] * d + t] : F(0);
+        }
+        __syncthreads();
+        double best[R];
+        int bi[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            best[r] = 0.0;
+            bi[r] = 0x7fffffff;
+        }
+        for (int j = threadIdx.x; j < k; j += blockDim.x) {
+            const F *c = C + (int64_t)j * d;
+            double cc = 0.0, acc[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) acc[r] = 0.0;
+            if constexpr (VEC && sizeof(F) == 4) {  // float, d % 4 == 0, 16-byte aligned: 16 bytes at a time
+                const float4 *c4 = reinterpret_cast<const float4 *>(c);
+#pragma unroll 2
+                for (int t4 = 0; t4 < (d >> 2); ++t4) {
+                    const float4 q = c4[t4];
+                    const double cv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        cc = fma(cv[u], cv[u], cc);
+#pragma unroll
+                        for (int r = 0; r < R; ++r) acc[r] = fma((double)xs[r * d + 4 * t4 + u], cv[u], acc[r]);
+                    }
+                }
+            } else {
+#pragma unroll 4
+                for (int t = 0; t < d; ++t) {
+                    const double cv = (double)c[t];
+                    cc = fma(cv, cv, cc);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) acc[r] = fma((double)xs[r * d + t], cv, acc[r]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const double sc = 0.5 * cc - acc[r];
+                if (bi[r] == 0x7fffffff || sc < best[r]) {  // ascending j per thread: lowest index on ties
+                    best[r] = sc;
+                    bi[r] = j;
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            for (int m = 16; m >= 1; m >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best[r], m);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi[r], m);
+                if (oi != 0x7fffffff && (bi[r] == 0x7fffffff || ob < best[r] || (ob == best[r] && oi < bi[r]))) {
+                    best[r] = ob;
+                    bi[r] = oi;
+                }
+            }
+            if (lane == 0) {
+                s_best[warp][r] = best[r];
+                s_idx[warp][r] = bi[r];
+            }
+        }
+        __syncthreads();
+        if ((int)threadIdx.x < nr) {
+            const int r = threadIdx.x;
+            double b = s_best[0][r];
+            int ii = s_idx[0][r];
+            for (int w = 1; w < 8; ++w) {
+                const double ob = s_best[w][r];
+                const int oi = s_idx[w][r];
+                if (oi != 0x7fffffff && (ii == 0x7fffffff || ob < b || (ob == b && oi < ii))) {
+                    b = ob;
+                    ii = oi;
+                }
+            }
+            const int row = s_row[r];
+            if (labels[row] != ii) ++changed;
+            labels[row] = ii;
+            d2[row] = F(2.0 * b + (double)xnorm[row]);
+        }
+        __syncthreads();
+    }
+    if (changed) atomicAdd(&st->n_changed, changed);
+}
+
+constexpr int kFullRows = 8;
+
 }  // namespace
 
 template <typename F>
 void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, const RecheckEntry *queue,
                     int32_t *labels, F *d2, const F *xnorm, LoopState *st, int num_sms, cudaStream_t s) {
     bool vec = false;
+    const bool vec_c = sizeof(F) == 4 && d % 4 == 0 && (uintptr_t)C % 16 == 0;
     if constexpr (sizeof(F) == 4) {
         vec = d % 4 == 0 && (uintptr_t)X % 16 == 0 && (uintptr_t)C % 16 == 0;
         if (vec)
@@ -219,8 +334,20 @@ void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, con
     if (!vec)
         recheck_pairs_kernel<F, false><<<num_sms * 8, 256, 0, s>>>(X, (int)d, C, queue, labels, d2, xnorm, st);
     KMB_LAUNCHED();
-    // one wave (254 registers per thread: one 256-thread block per SM), a block per entry
-    recheck_full_kernel<F><<<num_sms, 256, 0, s>>>(X, (int)d, C, (int)k, queue, n, labels, d2, xnorm, st);
+    const size_t rows_smem = (size_t)kFullRows * d * sizeof(F);
+    if (rows_smem <= 48 * 1024) {
+        if (vec_c)
+            recheck_full_rows_kernel<F, kFullRows, true><<<num_sms * 2, 256, rows_smem, s>>>(X, (int)d, C, (int)k,
+                                                                                            queue, n, labels, d2,
+                                                                                            xnorm, st);
+        else
+            recheck_full_rows_kernel<F, kFullRows, false><<<num_sms * 2, 256, rows_smem, s>>>(X, (int)d, C, (int)k,
+                                                                                             queue, n, labels, d2,
+                                                                                             xnorm, st);
+    } else {
+        // wide rows: one wave (254 registers per thread: one 256-thread block per SM), a block per entry
+        recheck_full_kernel<F><<<num_sms, 256, 0, s>>>(X, (int)d, C, (int)k, queue, n, labels, d2, xnorm, st);
+    }
     KMB_LAUNCHED();
 }
 
