@@ -19,15 +19,15 @@
 // is queued with its two best clusters (or flagged for a full rescan when a
 // third cluster is inside the band) and re-scored in FP64 by the recheck kernel.
 //
-// Kernel structure (one CTA per SM, persistent over 128-row tiles, 14 warps):
+// Kernel structure (one CTA per SM, persistent over 128-row tiles, 10 warps):
 //   warp 0   TMA producer: A = the tile's Xhi/Xlo panels (128 rows x 64 bf16,
 //            SWIZZLE_128B), B = Chi/Clo panels of BN clusters (BN = 256: 32 bf16,
 //            SWIZZLE_64B; BN = 128 where padding k to 256 would cost more than
 //            the wider tile gains: 64 bf16, SWIZZLE_128B), ring of 32 KB stages
 //   warp 1   TMEM allocation + single-thread tcgen05.mma issue (M=128, N=BN,
 //            K=16); commits free B stages, publish accumulators and release A tiles
-//   warps 2-13 epilogue, three groups of 4 warps (one per TMEM lane quarter):
-//            group g drains the 32-column chunks g, g+3, g+6, ... of every
+//   warps 2-9 epilogue, two groups of 4 warps (one per TMEM lane quarter):
+//            group g drains the 32-column chunks g, g+2, g+4, ... of every
 //            accumulator. Before the MMAs of a tile start, the drain of the
 //            accumulator's previous tile writes -h_j into every lane of it
 //            (tcgen05.st), so the MMAs leave
@@ -36,8 +36,8 @@
 //            thread) and keeps a running top-3 per row: each 32-column chunk
 //            is first reduced to its maximum (branch-free, 3-input max); only
 //            chunks holding a value at or above the row's threshold take the
-//            exact insertion path. At the end of a row tile groups 1 and 2 hand
-//            their top-3 to group 0 through a small global scratch (per SM, by
+//            exact insertion path. At the end of a row tile group 1 hands
+//            its top-3 to group 0 through a small global scratch (per SM, by
 //            row-tile parity) and a named barrier; group 0 merges and writes
 //            the row's outputs.
 // 512 / BN accumulators of BN columns (all 512 TMEM columns): while the groups
@@ -69,7 +69,7 @@ constexpr int PANEL = 128 * 128;        // bytes per A panel (128 rows x 128 B)
 constexpr int TMEM_COLS = 512;          // all of TMEM: 512 / BN accumulators of BN columns
 constexpr int kMaxAcc = 4;
 __host__ __device__ constexpr int panel_b_bytes(int bn) { return bn * kpb_of(bn) * 2; }  // one B panel (16 KB)
-constexpr int NGROUPS = 3;              // epilogue groups of 4 warps (one warp per TMEM lane quarter)
+constexpr int NGROUPS = 2;              // epilogue groups of 4 warps (one warp per TMEM lane quarter)
 constexpr int NTHREADS = 64 + NGROUPS * 128;  // warp 0 TMA, warp 1 MMA, warps 2.. epilogue
 constexpr int MAX_B_STAGES = 8;
 constexpr int kMaxSmid = 1024;
