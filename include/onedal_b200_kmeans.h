@@ -14,8 +14,8 @@
  *      defined   cpp/oneapi/dal/algo/kmeans/detail/infer_ops.cpp:26-43)
  * which run DAAL's KMeansBatchKernel<lloydDense, F, cpu>
  * (cpp/daal/src/algorithms/kmeans/kmeans_lloyd_batch_impl.i:48-242).
- * A replacement dispatcher calls kmb_train / kmb_infer below; INTEGRATION.md
- * shows that binding. All entry points are synchronous with respect to the
+ * A replacement dispatcher calls kmb_train / kmb_infer below, with the
+ * same arguments the DAAL kernel received. All entry points are synchronous with respect to the
  * host unless stated otherwise, take plain pointers and sizes, and return a
  * kmb_status. Matrices are dense row-major (rows x columns).
  */
@@ -254,9 +254,11 @@ KMB_API int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_
  * to 256 bytes); bigger problems return KMB_EINVAL with a message on stderr.
  * All calls on a device share the array, which keeps the last call's
  * contents; calls that overlap on the GPU (other streams or host threads)
- * race, so issue them on one stream. The first call on each device looks up
- * the array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture on the device. */
+ * race, so issue them on one stream. The array's device address belongs to a
+ * CUDA context: the first call in each context (the device's primary context,
+ * or a driver-API context the caller made current) looks it up with
+ * cudaGetSymbolAddress while that context is current and caches it by the
+ * context's id; make that first call before any stream capture in the context. */
 KMB_API int kmb_infer_noalloc(int dtype, const void *X, int64_t n, int64_t d, const void *C, int64_t k,
                               int32_t *responses, double *objective, void *cuda_stream);
 

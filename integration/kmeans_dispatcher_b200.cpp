@@ -7,7 +7,9 @@
 #include "oneapi/dal/algo/kmeans/detail/infer_ops.hpp"
 #include "oneapi/dal/algo/kmeans/detail/train_ops.hpp"
 #include "oneapi/dal/detail/common.hpp"
+#include "oneapi/dal/detail/error_messages.hpp"
 #include "oneapi/dal/detail/policy.hpp"
+#include "oneapi/dal/detail/spmd_policy.hpp"
 #include "oneapi/dal/exceptions.hpp"
 #include "oneapi/dal/table/csr_accessor.hpp"
 #include "oneapi/dal/table/homogen.hpp"
@@ -202,6 +204,31 @@ template struct ONEDAL_EXPORT
     infer_ops_dispatcher<dal::detail::host_policy, float, method::lloyd_csr, task::clustering>;
 template struct ONEDAL_EXPORT
     infer_ops_dispatcher<dal::detail::host_policy, double, method::lloyd_csr, task::clustering>;
+
+// SPMD train (dal::preview::train(comm, ...), cpp/oneapi/dal/train.hpp:43-50) on
+// the host: the reference instantiates these next to the host-policy ones
+// (detail/train_ops.cpp:35-37) and its single-node CPU kernel dispatcher answers
+// them with unimplemented(spmd_version_of_algorithm_is_not_implemented)
+// (cpp/oneapi/dal/backend/dispatcher.hpp:186-199). The same answer here keeps
+// every symbol and behaviour a client links against; row-sharded multi-GPU
+// training runs through kmb_partial_sums / kmb_finalize_centroids instead.
+template <typename F, typename M>
+struct train_ops_dispatcher<dal::detail::spmd_host_policy, F, M, task::clustering> {
+    train_result<task::clustering> operator()(const dal::detail::spmd_host_policy &,
+                                              const descriptor_base<task::clustering> &,
+                                              const train_input<task::clustering> &) const {
+        throw unimplemented{ dal::detail::error_messages::spmd_version_of_algorithm_is_not_implemented() };
+    }
+};
+
+template struct ONEDAL_EXPORT
+    train_ops_dispatcher<dal::detail::spmd_host_policy, float, method::lloyd_dense, task::clustering>;
+template struct ONEDAL_EXPORT
+    train_ops_dispatcher<dal::detail::spmd_host_policy, double, method::lloyd_dense, task::clustering>;
+template struct ONEDAL_EXPORT
+    train_ops_dispatcher<dal::detail::spmd_host_policy, float, method::lloyd_csr, task::clustering>;
+template struct ONEDAL_EXPORT
+    train_ops_dispatcher<dal::detail::spmd_host_policy, double, method::lloyd_csr, task::clustering>;
 
 template struct ONEDAL_EXPORT
     train_ops_dispatcher<dal::detail::host_policy, float, method::lloyd_dense, task::clustering>;

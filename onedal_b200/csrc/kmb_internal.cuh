@@ -236,7 +236,12 @@ void launch_finalize_from_sums(const double *sums, const int64_t *counts, const 
 template <typename F>
 void launch_sum_values(const F *v, int64_t n, double *partials, double *out, cudaStream_t s);
 
+// Blocks of the objective / value-sum kernels, hence the number of FP64
+// partials their `partials` scratch holds (launch_objective, launch_sum_values).
+constexpr int kObjectivePartials = 148 * 8;
+
 // Exact objective sum ||x - c_label||^2 in FP64, deterministic.
+// partials: kObjectivePartials doubles of scratch.
 template <typename F>
 void launch_objective(const F *X, int64_t n, int64_t d, const F *C, const int32_t *labels, double *partials,
                       double *out, cudaStream_t s);

@@ -805,8 +805,6 @@ __global__ void list_empties_kernel(const int32_t *__restrict__ empty_flag, int 
 
 }  // namespace
 
-constexpr int kObjectiveBlocks = 148 * 8;
-
 UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d) {
     UpdatePlan p;
     p.n = n;
@@ -842,7 +840,7 @@ bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize) {
     int64_t pk = 1;
     while (pk < p.k) pk <<= 1;
     ok &= ws.ensure(ws.cand, sizeof(Cand) * pk);
-    ok &= ws.ensure(ws.obj_part, sizeof(double) * kObjectiveBlocks);
+    ok &= ws.ensure(ws.obj_part, sizeof(double) * kObjectivePartials);
     (void)fsize;
     return ok;
 }
@@ -971,9 +969,9 @@ void launch_partial_sums(const F *X, const UpdatePlan &p, const int32_t *labels,
 template <typename F>
 void launch_objective(const F *X, int64_t n, int64_t d, const F *C, const int32_t *labels, double *partials,
                       double *out, cudaStream_t s) {
-    objective_kernel<F><<<kObjectiveBlocks, 256, 0, s>>>(X, n, (int)d, C, labels, partials);
+    objective_kernel<F><<<kObjectivePartials, 256, 0, s>>>(X, n, (int)d, C, labels, partials);
     KMB_LAUNCHED();
-    sum_partials_kernel<<<1, 32, 0, s>>>(partials, kObjectiveBlocks, out);
+    sum_partials_kernel<<<1, 32, 0, s>>>(partials, kObjectivePartials, out);
     KMB_LAUNCHED();
 }
 
@@ -994,9 +992,9 @@ void launch_finalize_from_sums(const double *sums, const int64_t *counts, const 
 
 template <typename F>
 void launch_sum_values(const F *v, int64_t n, double *partials, double *out, cudaStream_t s) {
-    sum_values_kernel<F><<<kObjectiveBlocks, 256, 0, s>>>(v, n, partials);
+    sum_values_kernel<F><<<kObjectivePartials, 256, 0, s>>>(v, n, partials);
     KMB_LAUNCHED();
-    sum_partials_kernel<<<1, 32, 0, s>>>(partials, kObjectiveBlocks, out);
+    sum_partials_kernel<<<1, 32, 0, s>>>(partials, kObjectivePartials, out);
     KMB_LAUNCHED();
 }
 

@@ -12,6 +12,8 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATED_LIB = os.path.join(HERE, "_build", "libkmeans_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libkmeans_daal_ref.so")
+# The reference source tree this recipe compiles from: ONEDAL_REFERENCE_TREE, or
+# where this build environment mounts it. The only place the path is named.
 REFERENCE_TREE = os.environ.get("ONEDAL_REFERENCE_TREE", "/root/reference")
 
 

@@ -2,7 +2,7 @@
 
 Run in a container where the reference tree is mounted:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py [--reference <reference source tree>]
 
 Sources (paths inside the reference project):
 
@@ -187,7 +187,8 @@ def plusplus_cases():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    from oracle import build as oracle_build
+    ap.add_argument("--reference", default=oracle_build.REFERENCE_TREE)
     args = ap.parse_args()
     ref = args.reference
 

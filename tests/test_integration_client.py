@@ -41,6 +41,28 @@ def _parse(out):
     return res
 
 
+DISPATCHER_OBJ = os.path.join(ROOT, "integration", "_build", "kmeans_dispatcher_b200.o")
+
+
+@pytest.mark.skipif(not os.path.exists(DISPATCHER_OBJ), reason="integration dispatcher not built")
+def test_dispatcher_exports_every_reference_instantiation():
+    """The replacement keeps every symbol the reference's INSTANTIATE lines export
+    (detail/train_ops.cpp:35-42: host_policy and spmd_host_policy trains,
+    detail/infer_ops.cpp:37-43: host_policy infers), for both methods and types."""
+    syms = subprocess.run(["nm", "-C", DISPATCHER_OBJ], capture_output=True, text=True).stdout
+    defined = [ln for ln in syms.splitlines() if " W " in ln or " T " in ln]
+    host = "oneapi::dal::detail::v1::host_policy"
+    spmd = "oneapi::dal::detail::v1::spmd_policy<oneapi::dal::detail::v1::host_policy>"
+    want = []
+    for f in ("float", "double"):
+        for m in ("lloyd_dense", "lloyd_csr"):
+            tail = f", {f}, oneapi::dal::kmeans::method::v1::{m}, oneapi::dal::kmeans::task::v1::clustering>::operator()"
+            want += [f"train_ops_dispatcher<{host}{tail}", f"infer_ops_dispatcher<{host}{tail}",
+                     f"train_ops_dispatcher<{spmd}{tail}"]
+    for w in want:
+        assert any(w in ln for ln in defined), w
+
+
 @needs_client
 def test_client_links_b200_library():
     deps = subprocess.run(["ldd", CLIENT], capture_output=True, text=True).stdout
