@@ -93,8 +93,9 @@ class ClockSampler:
 
 
 def cpu_reference_iters_per_s(X_host, C0_host, n_full, iters, threads):
-    """Reference DAAL kernel on a row sample: per-iteration time from a train with
-    `iters` iterations minus an infer pass (the train's final responses+objective)."""
+    """Reference DAAL kernel on the given rows: per-iteration time from a train with
+    `iters` iterations minus an infer pass (the train's final responses+objective),
+    scaled to n_full rows when the rows are a sample."""
     from oracle import daal_ref
     daal_ref.set_threads(threads)
     t0 = time.perf_counter()
@@ -151,6 +152,80 @@ def run_plusplus(args, X, ctx):
                                    "kind": "reference",
                                    "sample": f"reference plusPlus init kernel, first {ns} of {n} rows, {kc} centers, "
                                              f"per-center time scaled by rows"}
+    return out
+
+
+def measured_fma_peak_tflops(device=0, dtype=0):
+    """The device's FP32 (dtype 0) / FP64 (1) FMA peak measured by the library's
+    microbenchmark (kmb_measure_fma_peak), TFLOP/s."""
+    import ctypes
+
+    from onedal_b200 import _native
+    lib = _native.load_library()
+    g = ctypes.c_double()
+    rc = lib.kmb_measure_fma_peak(device, dtype, ctypes.byref(g))
+    return g.value / 1e3 if rc == 0 else None
+
+
+def run_plain_scale(args, ctx, device=0):
+    """Plain FP32 form at scale: n = 10,000,000 rows, d = 64, k = 256, float32, 256
+    anisotropic blobs (per-blob diagonal std log-uniform in [0.3, 3], centres
+    U[-20,20]^64, Dirichlet(1) weights), initial centroids a seeded row sample,
+    exactly 20 Lloyd iterations (eps 0; the loop runs all 20 unless it reaches an
+    exact fixed point), inputs resident in HBM (2.56 GB, above L2). Reports Lloyd
+    iterations/s and the assignment kernel against the measured FP32 FMA peak."""
+    import ctypes
+
+    import torch
+
+    from onedal_b200 import _native, workloads
+    w = workloads.PLAIN_GPU
+    X, C0 = workloads.make(w, "cuda")
+    n, d = X.shape
+    k = C0.shape[0]
+    labels = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def iterate(T, C):
+        p = _native.kmb_params(k, T, 0.0, _native.KMB_FORM_PLAIN, 0)
+        it = ctypes.c_int64()
+        ctx.check(ctx.lib.kmb_lloyd_iterate(ctx.handle, _native.KMB_F32, X.data_ptr(), n, d, C.data_ptr(),
+                                            ctypes.byref(p), labels.data_ptr(), ctypes.byref(it), None))
+        return it.value
+
+    iterate(3, C0.clone())
+    torch.cuda.synchronize()
+    C = C0.clone()
+    ctx.check(ctx.lib.kmb_context_set_kernel_timing(ctx.handle, 1))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    it = iterate(w.iterations, C)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    kt, kl = ctypes.c_double(), ctypes.c_int64()
+    ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 0, ctypes.byref(kt), ctypes.byref(kl)))
+    ut, ul = ctypes.c_double(), ctypes.c_int64()
+    ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, 2, ctypes.byref(ut), ctypes.byref(ul)))
+    ctx.check(ctx.lib.kmb_context_set_kernel_timing(ctx.handle, 0))
+    s = e0.elapsed_time(e1) / 1e3
+    kms = kt.value / max(kl.value, 1)
+    flops = 2.0 * n * k * d
+    achieved = flops / (kms / 1e3) / 1e12
+    peak = measured_fma_peak_tflops(device, 0)
+    out = {"metric": "Lloyd iter/s (plain FP32 form)", "value": it / s, "unit": "iter/s", "iterations": it,
+           "ms_per_iteration": s / max(it, 1) * 1e3,
+           "config": {"workload": f"plain at scale n={n} d={d} k={k} float32, {k} anisotropic blobs, "
+                                  "Dirichlet(1) weights", "n": n, "d": d, "k": k,
+                      "l2": f"inputs ({n * d * 4 / 1e9:.2f} GB) larger than L2; no flush"},
+           "roofline": {"bound": "fp32_fma", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak if peak else None,
+                        "peak_source": "FP32 FMA peak measured on this GPU (kmb_measure_fma_peak)",
+                        "kernel_ms_avg": kms, "kernel_launches": kl.value,
+                        "update_ms_avg": ut.value / max(ul.value, 1),
+                        "algorithmic_flops_per_launch": flops, "algorithmic_bytes_per_launch": 4 * n * d + 8 * n,
+                        "traffic": None}}
+    del X
+    torch.cuda.empty_cache()
     return out
 
 
@@ -230,40 +305,73 @@ def make_workload(device, n=None):
     return X, C0
 
 
+def reference_rows(w):
+    """The workload's rows and initial centroids on the host, drawn by the same
+    generator as the GPU arm's (on the GPU when one is present, so both arms see
+    identical data; the reference itself never touches the GPU)."""
+    import torch
+    from onedal_b200 import workloads
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    X, C0 = workloads.make(w, dev)
+    Xh = X.cpu().numpy()
+    Ch = C0.cpu().numpy()
+    del X, C0
+    if dev == "cuda":
+        torch.cuda.empty_cache()
+    return Xh, Ch, dev
+
+
 def run_reference(args):
+    """The reference's own DAAL Lloyd kernel (oracle/_ref, built from the reference
+    sources) on all host cores, at the full configuration: n = 20,000,000 rows, d =
+    128, k = 1024, float32. Warm-up: one train call of `warmup` iterations. Timed: one
+    train call of `steps` iterations minus the final responses + objective pass it
+    ends with (timed separately as an infer call on the same rows), so ms_per_step
+    is one Lloyd iteration over all 20M rows."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import numpy as np
-    import torch
     from onedal_b200 import workloads
-    w = workloads.PRECISION
-    n_sample = args.cpu_sample_rows
-    X, C0 = workloads.make(w, "cpu", n=n_sample)
-    Xh = X.numpy()
-    Ch = C0.numpy()
-    threads = os.cpu_count() or 1
     from oracle import daal_ref
+    w = workloads.PRECISION
     if not daal_ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "reference kernel library oracle/_ref not built"}))
         return
+    Xh, Ch, gen = reference_rows(w)
+    n = Xh.shape[0]
+    threads = os.cpu_count() or 1
     daal_ref.set_threads(threads)
-    # warm-up: W single iterations
-    for _ in range(args.warmup):
-        daal_ref.train(Xh, Ch, 1, 0.0)
-    v, per_iter, it = cpu_reference_iters_per_s(Xh, Ch, w.n, args.steps, threads)
-    sample = f"{n_sample} of {w.n} rows (same generator), {it} iterations, scaled by rows"
+    if args.warmup > 0:
+        daal_ref.train(Xh, Ch, args.warmup, 0.0)
+    t0 = time.perf_counter()
+    C, _, _, it = daal_ref.train(Xh, Ch, args.steps, 0.0)
+    t_train = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    daal_ref.infer(Xh, C, True)
+    t_final = time.perf_counter() - t0
+    per_iter = max(t_train - t_final, 1e-9) / max(it, 1)
+    v = 1.0 / per_iter
+    sample = (f"all {n} rows, {it} Lloyd iterations of one train call minus its final responses+objective "
+              f"pass (timed as an infer call), {threads} threads, OpenBLAS sgemm")
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": per_iter * (w.n / n_sample) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": per_iter * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "precision n=20000000 d=128 k=1024 float32, 10% bisector near-ties",
-                   "n": w.n, "d": w.d, "k": w.k, "form": "DAAL lloydDense float (OpenBLAS sgemm)"},
+        "config": workload_config(n, w.d, w.k),
         "impl": "reference",
+        "reference_kernel": "DAAL KMeansBatchKernel<lloydDense, float> built from the reference sources",
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "timing": {"train_s": t_train, "final_pass_s": t_final, "iterations": it, "rows_generated_on": gen},
     }
     print(json.dumps(line))
+
+
+def workload_config(n, d, k):
+    """The `config` object both arms report for the precision workload."""
+    return {"workload": f"precision n={n} d={d} k={k} float32, {k} blobs std 1 in U[-5,5]^{d}, "
+                        "10% bisector near-ties", "n": n, "d": d, "k": k,
+            "l2": f"inputs ({n * d * 4 / 1e9:.2f} GB) larger than L2; no flush"}
 
 
 def run_serving(args, device=0):
@@ -584,9 +692,8 @@ def run_b200(args):
         peak = peaks["bf16_tflops_sustained"]
         peak_note = f"bf16 dense sustained ({peak_src})"
     else:
-        # FP32 FFMA issue peak: 148 SMs x 128 lanes x 2 flop x max SM clock (no measured figure exists).
-        peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-        peak_note = "fp32 FFMA issue peak at max SM clock (148x128x2xclock)"
+        peak = measured_fma_peak_tflops(local, 0)
+        peak_note = "FP32 FMA peak measured on this GPU (kmb_measure_fma_peak)"
     dpad = (d + 63) // 64 * 64
     if form == _native.KMB_FORM_BF16X3:
         algo_bytes = 4 * n * dpad + 8 * n  # Xhi + Xlo read once, labels + d2 written
@@ -608,9 +715,11 @@ def run_b200(args):
 
     # e2e through the public API with pinned host buffers.
     e2e = None
-    if rank == 0 and args.e2e:
+    Xh = None
+    if rank == 0 and (args.e2e or (world == 1 and args.cpu_iterations > 0)):
         Xh = torch.empty((n, d), dtype=torch.float32, pin_memory=True)
         Xh.copy_(X)
+    if rank == 0 and args.e2e:
         C0h = C0.cpu().numpy()
         Xn = Xh.numpy()
         desc = kmeans.descriptor(np.float32).set_cluster_count(k).set_max_iteration_count(args.steps) \
@@ -628,18 +737,22 @@ def run_b200(args):
                "d2h_bytes_per_step": (n * 4 + k * d * 4 + 8) // T,
                "note": "one kmeans.train call on pinned host rows (after one untimed call that sizes the "
                        "workspace): H2D, iterations, final responses + objective, D2H"}
-        del Xh
 
     cpu = None
-    if rank == 0 and world == 1 and args.cpu_sample_rows > 0:
+    if rank == 0 and world == 1 and args.cpu_iterations > 0:
         from oracle import daal_ref
         if daal_ref.available():
-            ns = args.cpu_sample_rows
-            Xs = X[:ns].cpu().numpy()
-            v, per_iter, it = cpu_reference_iters_per_s(Xs, C0.cpu().numpy(), n, 2, os.cpu_count() or 1)
-            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"first {ns} of {n} rows, {it} Lloyd iterations of the reference DAAL kernel "
-                             f"(OpenBLAS sgemm, std::thread shim), per-iteration time scaled by rows"}
+            threads = os.cpu_count() or 1
+            v, per_iter, it = cpu_reference_iters_per_s(Xh.numpy(), C0.cpu().numpy(), n, args.cpu_iterations,
+                                                        threads)
+            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"all {n} rows, {it} Lloyd iterations of the reference DAAL kernel (one train call "
+                             f"minus its final pass, timed as an infer call; OpenBLAS sgemm, std::thread shim)"}
+    del Xh
+
+    plain_scale = None
+    if rank == 0 and world == 1 and args.plain_scale:
+        plain_scale = run_plain_scale(args, ctx, local)
 
     plusplus = None
     if rank == 0 and world == 1 and args.plusplus_k > 1:
@@ -663,16 +776,15 @@ def run_b200(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / max(iters_done, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"precision n={n} d={d} k={k} float32, {k} blobs std 1 in U[-5,5]^{d}, "
-                                   "10% bisector near-ties", "n": n, "d": d, "k": k,
-                       "form": args.form, "iterations_completed": iters_done,
-                       "l2": f"inputs ({n * d * 4 / 1e9:.2f} GB) larger than L2; no flush"},
+            "config": workload_config(n, d, k),
+            "form": args.form, "iterations_completed": iters_done,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": gpu_launches, "clocks": clocks,
             "plain_fp32_value": plain_value,
             "bf16_over_plain": (value / plain_value) if plain_value else None,
             "recheck_rows_per_iteration": st.rechecked_rows / max(iters_done, 1),
             "full_rescans_per_iteration": st.full_rescans / max(iters_done, 1),
+            "plain_at_scale": plain_scale,
             "serving": serving,
             "batched": batched,
             "plusplus": plusplus,
@@ -690,13 +802,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--form", default="bf16x3", choices=["bf16x3", "plain"])
-    ap.add_argument("--plain-steps", type=int, default=3)
-    ap.add_argument("--cpu-sample-rows", type=int, default=200_000)
+    ap.add_argument("--plain-steps", type=int, default=10)
+    ap.add_argument("--cpu-iterations", type=int, default=2,
+                    help="Lloyd iterations of the reference kernel on all rows for cpu_baseline (0 skips it)")
+    ap.add_argument("--cpu-sample-rows", type=int, default=200_000,
+                    help="rows of the host-core baselines of the k-means++ and CSR measurements")
     ap.add_argument("--traffic-bytes", type=float, default=None)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-plain-scale", dest="plain_scale", action="store_false",
+                    help="skip the plain FP32 measurement at n=10M, d=64, k=256")
     ap.add_argument("--batched-problems", type=int, default=4096,
                     help="problems in the batched-form measurement (0 skips it)")
-    ap.add_argument("--serving-requests", type=int, default=3000,
+    ap.add_argument("--serving-requests", type=int, default=30000,
                     help="requests per serving load point (0 skips the serving measurement)")
     ap.add_argument("--csr-rows", type=int, default=2_000_000,
                     help="rows of the CSR (lloyd_csr) measurement (0 skips it)")

@@ -238,6 +238,13 @@ KMB_API int kmb_context_set_kernel_timing(kmb_context *ctx, int enabled);
  * whole launch of the other. */
 KMB_API int kmb_context_set_max_sms(kmb_context *ctx, int max_sms);
 KMB_API int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int64_t *launches);
+/* Diagnostics: the rows the context's last assignment pass re-scored in FP64
+ * (the near-tie rows of the tensor-core form, or of the plain form with
+ * recheck). *count = how many were queued; the first min(*count, capacity)
+ * row indices go to rows_out (device memory, int32). Synchronises the
+ * context's stream. No counterpart in the reference (its GEMM-based scoring
+ * has no near-tie queue). */
+KMB_API int kmb_context_recheck_rows(kmb_context *ctx, int32_t *rows_out, int64_t capacity, int64_t *count);
 
 /* Responses (and, when objective != NULL, the exact objective) of n rows X
  * against k centroids C, like kmb_infer with the plain form, for callers that
@@ -349,6 +356,12 @@ KMB_API int kmb_server_wait_detail(void *server, int64_t request_id, double time
  * model_id is served in. */
 KMB_API int kmb_server_infer_form(void *server, int32_t model_id, int64_t n, int32_t *form);
 KMB_API int kmb_server_get_stats(void *server, kmb_server_stats *stats);
+
+/* Measured fused multiply-add peak of `device` in dtype's precision (GFLOP/s,
+ * 2 flops per FMA): a short grid of dependent FMA chains timed with CUDA
+ * events, best of four launches. The plain form's assignment is reported
+ * against it. No counterpart in the reference. */
+KMB_API int kmb_measure_fma_peak(int device, int dtype, double *gflops);
 
 /* Library version string. */
 KMB_API const char *kmb_version(void);

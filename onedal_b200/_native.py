@@ -24,7 +24,8 @@ EXPORTED = (
     "kmb_server_create", "kmb_server_destroy", "kmb_server_add_model", "kmb_server_submit_infer",
     "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats", "kmb_server_infer_form", "kmb_server_wait_detail", "kmb_context_set_max_sms", "kmb_init_plusplus", "kmb_batched_train",
     "kmb_model_serialize", "kmb_model_deserialize", "kmb_server_add_model_serialized",
-    "kmb_train_csr", "kmb_infer_csr", "kmb_init_plusplus_csr",
+    "kmb_train_csr", "kmb_infer_csr", "kmb_init_plusplus_csr", "kmb_context_recheck_rows",
+    "kmb_measure_fma_peak",
 )
 
 
@@ -101,6 +102,8 @@ def load_library(path: str = LIB_PATH):
                                               ctypes.POINTER(I64), ctypes.POINTER(kmb_stats)]
             lib.kmb_context_set_kernel_timing.argtypes = [P, ctypes.c_int]
             lib.kmb_context_kernel_time.argtypes = [P, ctypes.c_int, ctypes.POINTER(D), ctypes.POINTER(I64)]
+            lib.kmb_context_recheck_rows.argtypes = [P, P, I64, ctypes.POINTER(I64)]
+            lib.kmb_measure_fma_peak.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(D)]
             lib.kmb_infer_noalloc.argtypes = [ctypes.c_int, P, I64, I64, P, I64, P, P, P]
             lib.kmb_server_create.argtypes = [ctypes.c_int, I64, I32, I32, ctypes.POINTER(P)]
             lib.kmb_server_destroy.argtypes = [P]

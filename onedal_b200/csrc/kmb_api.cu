@@ -29,6 +29,10 @@ struct kmb_context {
     kmb::LoopState *h_state = nullptr;  // pinned mirror of the device states
     int num_sms = 148;
     bool tc_per_tile = false;  // tensor-core assignment: one CTA per row tile instead of persistent CTAs
+    // The last assignment pass that queued near-tie rows (kmb_context_recheck_rows):
+    // its row count (the queue's capacity) and its loop state.
+    int64_t queue_rows = 0;
+    const kmb::LoopState *queue_state = nullptr;
     // kernel timing (kmb_context_set_kernel_timing)
     bool timing = false;
     int64_t launches_at_enable = 0;
@@ -226,6 +230,8 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
     }
     account_recheck_kernel<<<1, 1, 0, s>>>(st);
     KMB_LAUNCHED();
+    ctx->queue_rows = n;
+    ctx->queue_state = st;
     return KMB_OK;
 }
 
@@ -252,8 +258,20 @@ int assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, 
                                (const F *)ws.xnorm.ptr, st, ctx->num_sms, s);
         account_recheck_kernel<<<1, 1, 0, s>>>(st);
         KMB_LAUNCHED();
+        ctx->queue_rows = n;
+        ctx->queue_state = st;
     }
     return KMB_OK;
+}
+
+// Row ids of the recheck queue (front: two-candidate entries, back: full rescans)
+// into out[0 .. min(total, cap)).
+__global__ void gather_queue_rows_kernel(const RecheckEntry *queue, int64_t qcap, const LoopState *st, int32_t *out,
+                                         int64_t cap) {
+    const int64_t front = st->n_recheck, back = st->n_full;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < front + back && i < cap;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = i < front ? queue[i].row : queue[qcap - 1 - (i - front)].row;
 }
 
 // Row norms for the pass, plus -- for the tensor-core form -- the BF16 hi/lo
@@ -444,7 +462,7 @@ int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     const bool recheck = tc;
     int rc = ensure_common<F>(ctx, n, d, k, recheck, tc);
     if (rc) return rc;
-    if (!ctx->ws.ensure(ctx->ws.obj_part, sizeof(double) * 148 * 8)) return fail(ctx, KMB_ENOMEM, "objective");
+    if (!ctx->ws.ensure(ctx->ws.obj_part, sizeof(double) * kmb::kObjectivePartials)) return fail(ctx, KMB_ENOMEM, "objective");
     kmb::Workspace &ws = ctx->ws;
     cudaStream_t s = ctx->stream;
     const F *X = (const F *)Xv;
@@ -694,7 +712,7 @@ int infer_csr_impl(kmb_context *ctx, int memory, const void *vals, const int64_t
     int rc = ensure_common<F>(ctx, n, d, k, false, false);
     if (rc) return rc;
     kmb::Workspace &ws = ctx->ws;
-    if (!ws.ensure(ws.obj_part, sizeof(double) * 148 * 8) || !ws.ensure(ws.csr_cnorm, sizeof(double) * k))
+    if (!ws.ensure(ws.obj_part, sizeof(double) * kmb::kObjectivePartials) || !ws.ensure(ws.csr_cnorm, sizeof(double) * k))
         return fail(ctx, KMB_ENOMEM, "objective");
     kmb::CsrRows X;
     if ((rc = prepare_csr<F>(ctx, memory, vals, cols, rowptr, n, d, base, &X))) return rc;
@@ -1087,6 +1105,28 @@ int kmb_context_kernel_time(kmb_context *ctx, int kernel, double *total_ms, int6
     }
     if (total_ms) *total_ms = tot;
     if (launches) *launches = (int64_t)ctx->ev_used[kernel].size();
+    return KMB_OK;
+}
+
+int kmb_context_recheck_rows(kmb_context *ctx, int32_t *rows_out, int64_t capacity, int64_t *count) {
+    if (!ctx || !count || capacity < 0 || (capacity > 0 && !rows_out)) return KMB_EINVAL;
+    ctx->last_error.clear();
+    *count = 0;
+    if (!ctx->queue_state || !ctx->ws.queue.ptr) return KMB_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    cudaStream_t s = ctx->stream;
+    LoopState hs;
+    KMB_CUDA(cudaMemcpyAsync(&hs, ctx->queue_state, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaStreamSynchronize(s));
+    *count = (int64_t)hs.n_recheck + hs.n_full;
+    if (capacity > 0 && *count > 0) {
+        const int64_t m = std::min(*count, capacity);
+        gather_queue_rows_kernel<<<(unsigned)std::min<int64_t>((m + 255) / 256, 1024), 256, 0, s>>>(
+            (const RecheckEntry *)ctx->ws.queue.ptr, ctx->queue_rows, ctx->queue_state, rows_out, capacity);
+        KMB_LAUNCHED();
+        KMB_CUDA(cudaGetLastError());
+        KMB_CUDA(cudaStreamSynchronize(s));
+    }
     return KMB_OK;
 }
 

@@ -43,6 +43,7 @@
  * the thread count.
  */
 #include <math.h>
+#include <omp.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -315,5 +316,73 @@ int kmo_assign_f32_in_f64(const float *X, int64_t n, int64_t d, const float *C, 
     }
     free(Cd);
     free(h);
+    return KMO_OK;
+}
+
+/* Checker for full-size runs: per-cluster sums and counts of float32 rows under
+ * given labels, and (when C and objective are given) the objective
+ * sum_i ||x_i - c_{a_i}||^2 against C, all accumulated in double. These are the
+ * quantities of one Lloyd update (cluster sums kmeans_lloyd_impl.i:220-229,
+ * merged and divided in kmeans_lloyd_batch_impl.i:153-166) and of the exact
+ * objective (kmeans_lloyd_postprocessing.h:138-183), evaluated in FP64 so that
+ * a GPU result can be compared with them at the stated tolerances. Threads take
+ * contiguous row ranges; their partials are added in thread order. */
+int kmo_cluster_stats_f32(const float *X, int64_t n, int64_t d, const int32_t *labels, int64_t k, const float *C,
+                          double *sums, int64_t *counts, double *objective)
+{
+    if (n < 0 || d <= 0 || k <= 0) return KMO_EINVAL;
+    for (int64_t i = 0; i < n; ++i)
+        if (labels[i] < 0 || labels[i] >= k) return KMO_EINVAL;
+    int nt = 1;
+#pragma omp parallel
+    {
+#pragma omp single
+        nt = omp_get_num_threads();
+    }
+    double *ps = (double *)calloc((size_t)nt * (size_t)(k * d), sizeof(double));
+    int64_t *pc = (int64_t *)calloc((size_t)nt * (size_t)k, sizeof(int64_t));
+    double *po = (double *)calloc((size_t)nt, sizeof(double));
+    if (!ps || !pc || !po) {
+        free(ps);
+        free(pc);
+        free(po);
+        return KMO_ENOMEM;
+    }
+#pragma omp parallel num_threads(nt)
+    {
+        const int t = omp_get_thread_num();
+        const int64_t r0 = n * t / nt, r1 = n * (t + 1) / nt;
+        double *s = ps + (size_t)t * (size_t)(k * d);
+        int64_t *c = pc + (size_t)t * (size_t)k;
+        double o = 0.0;
+        for (int64_t i = r0; i < r1; ++i) {
+            const float *x = X + i * d;
+            const int64_t a = labels[i];
+            double *sa = s + a * d;
+            for (int64_t j = 0; j < d; ++j) sa[j] += (double)x[j];
+            c[a]++;
+            if (C) {
+                const float *ca = C + a * d;
+                for (int64_t j = 0; j < d; ++j) {
+                    const double df = (double)x[j] - (double)ca[j];
+                    o += df * df;
+                }
+            }
+        }
+        po[t] = o;
+    }
+    memset(sums, 0, sizeof(double) * (size_t)(k * d));
+    memset(counts, 0, sizeof(int64_t) * (size_t)k);
+    double obj = 0.0;
+    for (int t = 0; t < nt; ++t) {
+        const double *s = ps + (size_t)t * (size_t)(k * d);
+        for (int64_t j = 0; j < k * d; ++j) sums[j] += s[j];
+        for (int64_t j = 0; j < k; ++j) counts[j] += pc[(size_t)t * (size_t)k + j];
+        obj += po[t];
+    }
+    if (objective) *objective = obj;
+    free(ps);
+    free(pc);
+    free(po);
     return KMO_OK;
 }

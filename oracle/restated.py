@@ -47,6 +47,7 @@ def _load():
         _lib.kmo_objective_f64.restype = ctypes.c_double
         _lib.kmo_objective_f32.restype = ctypes.c_float
         _lib.kmo_assign_f32_in_f64.argtypes = [P, I64, I64, P, I64, P, P, P]
+        _lib.kmo_cluster_stats_f32.argtypes = [P, I64, I64, P, I64, P, P, P, P]
         for sfx in ("f64", "f32"):
             getattr(_lib, f"kmo_init_plusplus_{sfx}").argtypes = [P, I64, I64, I64, ctypes.c_uint32, ctypes.c_int, P, P]
             getattr(_lib, f"kmo_init_plusplus_csr_{sfx}").argtypes = [P, P, P, I64, I64, I64, ctypes.c_uint32, P, P]
@@ -148,6 +149,23 @@ def assign_f32_in_f64(X, C):
     second = np.empty(n, np.float64)
     _check(lib.kmo_assign_f32_in_f64(_p(X), n, d, _p(C), C.shape[0], _p(lab), _p(best), _p(second)))
     return lab, best, second
+
+
+def cluster_stats_f32(X, labels, k, C=None):
+    """FP64 per-cluster sums (k x d), int64 counts and, with C, the FP64 objective
+    sum ||x - c_label||^2 of float32 rows under the given labels (a checker for
+    full-size GPU runs). Returns (sums, counts, objective or None)."""
+    lib = _load()
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    labels = np.ascontiguousarray(labels, dtype=np.int32)
+    n, d = X.shape
+    sums = np.empty((k, d), np.float64)
+    counts = np.empty(k, np.int64)
+    obj = np.zeros(1, np.float64)
+    Cc = None if C is None else np.ascontiguousarray(C, dtype=np.float32)
+    _check(lib.kmo_cluster_stats_f32(_p(X), n, d, _p(labels), int(k), _p(Cc), _p(sums), _p(counts),
+                                     _p(obj) if C is not None else None))
+    return sums, counts, (float(obj[0]) if C is not None else None)
 
 
 def objective(X, C, labels):

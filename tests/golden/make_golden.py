@@ -20,10 +20,13 @@ Sources (paths inside the reference project):
   by examples/oneapi/cpp/source/kmeans/kmeans_lloyd_dense_batch.cpp with k=20,
   5 iterations, eps 0.001) plus the outputs of the reference DAAL kernel built
   from source (oracle/_ref) on it, in float64 and float32.
-* daal_ref_c1.npz -- outputs of the reference kernel on a reduced seeded
-  Gaussian-blob workload shaped like the plain CPU configuration (d=20, k=20,
-  init = first k rows, eps 0), float64 and float32, so the restated oracle can
-  be re-checked where the reference tree is absent.
+* daal_ref_c1.npz -- outputs of the reference kernel on the seeded
+  Gaussian-blob workload of the plain CPU configuration at its full size
+  (n=100,000, d=20, k=20, init = first k rows, 50 iterations, eps 0), float64
+  and float32; daal_ref_c1_small.npz -- the same on its first 20,000 rows, where
+  the reference's FP32 trajectory and the restatement's coincide bit for bit.
+  Both let the restated oracle and the GPU be re-checked where the reference
+  tree is absent.
 * daal_ref_plusplus.npz -- the centers chosen by the reference's dense k-means++
   initialisation (DAAL KMeansInitKernel<plusPlusDense>, one trial, mt19937 seeded
   777777: the default of cpp/oneapi/dal/algo/kmeans/detail/train_init_centroids.hpp)
@@ -189,32 +192,42 @@ def main():
     ap = argparse.ArgumentParser()
     from oracle import build as oracle_build
     ap.add_argument("--reference", default=oracle_build.REFERENCE_TREE)
+    ap.add_argument("--only", default=None, choices=["c1"],
+                    help="regenerate only these fixtures (c1: daal_ref_c1.npz, daal_ref_c1_small.npz)")
     args = ap.parse_args()
     ref = args.reference
-
-    for name, fn in (("gold.json", gold), ("empty_clusters.json", empty_clusters), ("smoke_infer.json", smoke_infer)):
-        with open(os.path.join(HERE, name), "w") as f:
-            json.dump(fn(ref), f, indent=1)
 
     from oracle import build, daal_ref
     build.build_reference()
     daal_ref.set_threads(1)
 
-    X = np.loadtxt(os.path.join(ref, "data/kmeans_dense_train_data.csv"), delimiter=",", dtype=np.float64)
-    C0 = np.loadtxt(os.path.join(ref, "data/kmeans_dense_train_centroids.csv"), delimiter=",", dtype=np.float64)
-    out = {"X": X, "C0": C0}
-    for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
-        C, lab, obj, it = daal_ref.train(X.astype(dt), C0.astype(dt), 5, 0.001)
-        out.update({f"C_{tag}": C, f"labels_{tag}": lab, f"obj_{tag}": obj, f"iters_{tag}": it})
-    np.savez_compressed(os.path.join(HERE, "example_dense.npz"), **out)
+    if not args.only:
+        for name, fn in (("gold.json", gold), ("empty_clusters.json", empty_clusters), ("smoke_infer.json", smoke_infer)):
+            with open(os.path.join(HERE, name), "w") as f:
+                json.dump(fn(ref), f, indent=1)
 
-    X = blobs_c1(20000, 1001)
-    out = {"seed": 1001, "n": 20000}
-    for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
-        Xd = X.astype(dt)
-        C, lab, obj, it = daal_ref.train(Xd, Xd[:20].copy(), 50, 0.0)
-        out.update({f"C_{tag}": C, f"labels_{tag}": lab.astype(np.uint8), f"obj_{tag}": obj, f"iters_{tag}": it})
-    np.savez_compressed(os.path.join(HERE, "daal_ref_c1.npz"), **out)
+        X = np.loadtxt(os.path.join(ref, "data/kmeans_dense_train_data.csv"), delimiter=",", dtype=np.float64)
+        C0 = np.loadtxt(os.path.join(ref, "data/kmeans_dense_train_centroids.csv"), delimiter=",", dtype=np.float64)
+        out = {"X": X, "C0": C0}
+        for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+            C, lab, obj, it = daal_ref.train(X.astype(dt), C0.astype(dt), 5, 0.001)
+            out.update({f"C_{tag}": C, f"labels_{tag}": lab, f"obj_{tag}": obj, f"iters_{tag}": it})
+        np.savez_compressed(os.path.join(HERE, "example_dense.npz"), **out)
+
+    # the plain configuration at its full size (n = 100,000 rows, d = 20, k = 20), and a
+    # 20,000-row prefix of the same generator on which the FP32 trajectories of the
+    # reference and of the restatement coincide bit for bit (at 100,000 rows their
+    # different FP32 summation orders move a few near-tie rows, and the trajectories part)
+    for fname, n in (("daal_ref_c1.npz", 100_000), ("daal_ref_c1_small.npz", 20_000)):
+        X = blobs_c1(n, 1001)
+        out = {"seed": 1001, "n": n}
+        for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+            Xd = X.astype(dt)
+            C, lab, obj, it = daal_ref.train(Xd, Xd[:20].copy(), 50, 0.0)
+            out.update({f"C_{tag}": C, f"labels_{tag}": lab.astype(np.uint8), f"obj_{tag}": obj, f"iters_{tag}": it})
+        np.savez_compressed(os.path.join(HERE, fname), **out)
+    if args.only:
+        return
 
     # k-means++ (train() without initial centroids): the reference's chosen centers
     out = {}

@@ -60,18 +60,28 @@ def test_example_dataset_matches_reference_kernel(tag, dt):
     assert rel_close(obj, float(z[f"obj_{tag}"]), 1e-12 if dt == np.float64 else 1e-6)
 
 
+@pytest.mark.parametrize("fixture", ["daal_ref_c1.npz", "daal_ref_c1_small.npz"])
 @pytest.mark.parametrize("tag,dt", [("f64", np.float64), ("f32", np.float32)])
-def test_blob_workload_matches_reference_kernel(tag, dt):
-    """Reduced plain-CPU-shaped workload (d=20, k=20, init = first rows, eps 0, 50 max
-    iterations) against recorded reference-kernel outputs."""
+def test_blob_workload_matches_reference_kernel(tag, dt, fixture):
+    """The plain configuration (d=20, k=20, init = first rows, eps 0, 50 max
+    iterations) at its full 100,000 rows and on a 20,000-row prefix, against recorded
+    reference-kernel outputs. float64 matches bit for bit at both sizes; float32
+    too on the prefix. At 100,000 rows the two FP32 summation orders (the
+    reference's per-thread partials and BLAS blocking, the restatement's row order)
+    move a few near-tie rows and the unconverged trajectories part, so there float32
+    is held to the iteration count, 0.5 % of the labels and the objective to 1e-5."""
     import os
     import sys
     sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
     from make_golden import blobs_c1
-    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "daal_ref_c1.npz"))
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", fixture))
     X = blobs_c1(int(z["n"]), int(z["seed"])).astype(dt)
     C, lab, obj, it = restated.train(X, X[:20].copy(), 50, 0.0)
     assert it == int(z[f"iters_{tag}"])
+    if dt == np.float32 and int(z["n"]) > 20000:
+        assert (lab != z[f"labels_{tag}"]).mean() < 5e-3
+        assert rel_close(obj, float(z[f"obj_{tag}"]), 1e-5)
+        return
     assert (lab == z[f"labels_{tag}"]).all()
     assert centroid_rel_err(z[f"C_{tag}"], C) < (1e-13 if dt == np.float64 else 1e-6)
     assert rel_close(obj, float(z[f"obj_{tag}"]), 1e-12 if dt == np.float64 else 1e-6)
@@ -312,3 +322,23 @@ def test_csr_restated_matches_reference_fixtures(tag, dt):
         assert centroid_rel_err(z[f"C_{name}_{tag}"], C) < tol, name
         assert rel_close(obj, float(z[f"obj_{name}_{tag}"]), tol), name
         assert np.array_equal(restated.init_plusplus_csr(v.astype(dt), c, r, d, k)[0], z[f"pp_{name}_{tag}"]), name
+
+
+def test_cluster_stats_checker_matches_numpy():
+    """The full-size tests' host checker (FP64 sums, counts and objective of given
+    labels, threaded) against a plain numpy evaluation."""
+    rng = np.random.default_rng(5)
+    n, d, k = 30011, 13, 41
+    X = rng.standard_normal((n, d)).astype(np.float32) * 4
+    lab = rng.integers(0, k - 1, n).astype(np.int32)  # cluster k-1 stays empty
+    C = rng.standard_normal((k, d)).astype(np.float32)
+    sums, counts, obj = restated.cluster_stats_f32(X, lab, k, C)
+    ref = np.zeros((k, d))
+    np.add.at(ref, lab, X.astype(np.float64))
+    np.testing.assert_allclose(sums, ref, rtol=1e-12, atol=1e-9)
+    np.testing.assert_array_equal(counts, np.bincount(lab, minlength=k))
+    assert counts[-1] == 0
+    o = ((X.astype(np.float64) - C[lab].astype(np.float64)) ** 2).sum()
+    assert abs(obj - o) <= 1e-12 * o
+    with pytest.raises(restated.OracleError):
+        restated.cluster_stats_f32(X, np.full(n, k, np.int32), k)
