@@ -53,6 +53,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace kmb {
 namespace tc {
@@ -64,11 +65,16 @@ constexpr int KP = 64;                  // bf16 per A panel row (128 bytes, SWIZ
 // bf16 per B panel row: 32 (64 B, SWIZZLE_64B) for 256-cluster tiles, 64 (128 B,
 // SWIZZLE_128B) for 128-cluster tiles, so a B stage (hi + lo panels) is 32 KB
 // either way; 16-wide panels in six stages measured 11 % slower.
-__host__ __device__ constexpr int kpb_of(int bn) { return bn == 256 ? 32 : 64; }
+__host__ __device__ constexpr int kpb_of(int bn, bool pair = false) { return (bn == 256 && !pair) ? 32 : 64; }
+// Clusters of one B panel in a CTA's shared memory: the whole cluster tile, or,
+// for a CTA pair, its half (each CTA of the pair holds BN/2 clusters).
+__host__ __device__ constexpr int b_rows_of(int bn, bool pair) { return pair ? bn / 2 : bn; }
 constexpr int PANEL = 128 * 128;        // bytes per A panel (128 rows x 128 B)
 constexpr int TMEM_COLS = 512;          // all of TMEM: 512 / BN accumulators of BN columns
 constexpr int kMaxAcc = 4;
-__host__ __device__ constexpr int panel_b_bytes(int bn) { return bn * kpb_of(bn) * 2; }  // one B panel (16 KB)
+__host__ __device__ constexpr int panel_b_bytes(int bn, bool pair = false) {
+    return b_rows_of(bn, pair) * kpb_of(bn, pair) * 2;  // one B panel (16 KB; 8 KB for a pair's half of BN = 128)
+}
 constexpr int NGROUPS = 2;              // epilogue groups of 4 warps (one warp per TMEM lane quarter)
 constexpr int NTHREADS = 64 + NGROUPS * 128;  // warp 0 TMA, warp 1 MMA, warps 2.. epilogue
 constexpr int MAX_B_STAGES = 8;
@@ -157,6 +163,35 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, ui
         : "memory");
 }
 
+// ---- CTA-pair (cta_group::2) helpers --------------------------------------
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// Address of the same shared-memory variable in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t peer_addr(const void *p, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(su32(p)), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// Arrive on an mbarrier given by its shared::cluster address (this CTA's or the peer's).
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+// Tile load of a CTA pair: lands in this CTA's shared memory, completes on the
+// pair's (leader CTA's) mbarrier, given by its shared::cluster address.
+__device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *tm, uint32_t bar_cluster, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+        "[%2];" ::"r"(su32(dst)),
+        "l"(tm), "r"(bar_cluster), "r"(x), "r"(y)
+        : "memory");
+}
+
 // K-major SWIZZLE_128B operand descriptor (sm100 format: version 1, LBO 16 B
 // (unused for swizzled K-major), SBO 1024 B between 8-row groups, layout 2).
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
@@ -183,9 +218,10 @@ __device__ __forceinline__ uint64_t swb_desc(uint32_t saddr) {
     return d;
 }
 
-// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M=128, N=bn.
-__host__ __device__ constexpr uint32_t make_idesc(int bn) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major, M = 128 (one
+// CTA) or 256 (a CTA pair), N = bn.
+__host__ __device__ constexpr uint32_t make_idesc(int bn, int m = BM) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(bn >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
 // The three split-BF16 products of one k-step (xh.ch, xh.cl, xl.ch) into one
@@ -199,6 +235,28 @@ __device__ __forceinline__ void mma_bf16x3(uint32_t tmem_d, uint64_t ah, uint64_
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %4, %5, p;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %2, %3, %5, p;\n\t}" ::"r"(tmem_d),
         "l"(ah), "l"(al), "l"(bh), "l"(bl), "r"(idesc)
+        : "memory");
+}
+// The same for a CTA pair (issued by the leader CTA): M = 256 rows, 128 from
+// each CTA's A panels; the B tile's two halves come from the two CTAs.
+__device__ __forceinline__ void mma_bf16x3_pair(uint32_t tmem_d, uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl,
+                                                uint32_t idesc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, 1, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %3, %5, p;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %4, %5, p;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %2, %3, %5, p;\n\t}" ::"r"(tmem_d),
+        "l"(ah), "l"(al), "l"(bh), "l"(bl), "r"(idesc)
+        : "memory");
+}
+// Completion of the pair's MMAs issued so far, signalled on the mbarrier at the
+// same offset in both CTAs of the pair.
+__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            su32(bar)),
+        "h"((uint16_t)3)
         : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -317,19 +375,33 @@ __device__ __forceinline__ Top3 top3_merge(const Top3 &x, const Top3 &y) {
 }
 
 
-template <int BN>
+template <int BN, bool PAIR>
 __global__ void __launch_bounds__(NTHREADS, 1)
 assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant__ CUtensorMap tmXl,
                  const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl, Params p) {
     constexpr int NACC = TMEM_COLS / BN;  // TMEM accumulators (double-buffered or more)
-    constexpr int PANEL_B = panel_b_bytes(BN);
-    constexpr int KPB = kpb_of(BN);
-    constexpr uint32_t kIdesc = make_idesc(BN);
+    constexpr int PANEL_B = panel_b_bytes(BN, PAIR);
+    constexpr int KPB = kpb_of(BN, PAIR);
+    constexpr int BROWS = b_rows_of(BN, PAIR);  // clusters of a B panel in this CTA
+    constexpr int NCTA = PAIR ? 2 : 1;          // CTAs sharing one MMA (a pair: M = 256)
+    constexpr uint32_t kIdesc = make_idesc(BN, NCTA * BM);
     static_assert(NACC >= 2 && NACC <= kMaxAcc, "accumulator count");
-    // One read of the loop flag for the whole CTA, so every thread takes the same path.
+    const uint32_t rank = PAIR ? cluster_rank() : 0u;  // 0: the pair's leader (issues the MMAs)
+    // One read of the loop flag for the whole CTA (for a pair: the leader's read,
+    // for both CTAs), so every thread of the pair takes the same path.
     __shared__ int s_skip;
     if (threadIdx.x == 0) s_skip = p.st->done;
-    __syncthreads();
+    if (PAIR) {
+        cluster_sync_all();
+        if (threadIdx.x == 0 && rank != 0) {
+            uint32_t v;
+            asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(peer_addr(&s_skip, 0)) : "memory");
+            s_skip = (int)v;
+        }
+        cluster_sync_all();
+    } else {
+        __syncthreads();
+    }
     if (s_skip) return;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -351,24 +423,46 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
         }
         for (int i = 0; i < NACC; ++i) {
             mbar_init(&bar->acc_full[i], 1);
-            mbar_init(&bar->acc_empty[i], 4 * NGROUPS);
+            mbar_init(&bar->acc_empty[i], 4 * NGROUPS * NCTA);  // every epilogue warp of the pair
         }
         mbar_init(&bar->mma_done, 1);
         bar->abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&bar->tmem_base)),
-                     "r"(TMEM_COLS)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        if (PAIR) {
+            // both CTAs of the pair allocate together; the same columns in each
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             su32(&bar->tmem_base)),
+                         "r"(TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             su32(&bar->tmem_base)),
+                         "r"(TMEM_COLS)
+                         : "memory");
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
     }
     tc_fence_before();
-    __syncthreads();
+    if (PAIR)
+        cluster_sync_all();  // barriers initialised and TMEM allocated in both CTAs
+    else
+        __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = bar->tmem_base;
 
-    const int my_tiles = (p.n_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    // Work units: 128-row tiles, or for a pair 256-row tiles (the leader's 128 rows
+    // first). A CTA's row tile of unit u is u (one CTA) or 2u + rank (a pair).
+    int unit0 = (int)blockIdx.x, unit_stride = (int)gridDim.x;
+    if (PAIR) {
+        asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(unit0));
+        asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(unit_stride));
+    }
+    const int n_units = PAIR ? (p.n_tiles + 1) / 2 : p.n_tiles;
+    const int my_tiles = (n_units - unit0 + unit_stride - 1) / unit_stride;
+    auto tile_of = [&](int lt_) { return PAIR ? (unit0 + lt_ * unit_stride) * 2 + (int)rank : unit0 + lt_ * unit_stride; };
     uint32_t smid;
     asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
     if (smid >= (uint32_t)kMaxSmid) smid = 0;  // (cannot happen on sm_100: ids stay below the SM count)
@@ -382,25 +476,34 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             int bs = 0;
             uint32_t bphase = 0;  // B ring position and the parity of its current lap
             bool ok = true;
+            // A pair's loads complete on the leader's full barriers, whose expected
+            // byte counts (set by the leader) cover both CTAs' loads.
+            auto load = [&](void *dst, const CUtensorMap *tm, uint64_t *full, int x, int y) {
+                if (PAIR)
+                    tma_load_2d_pair(dst, tm, peer_addr(full, 0), x, y);
+                else
+                    tma_load_2d(dst, tm, full, x, y);
+            };
             for (int lt = 0; lt < my_tiles && ok; ++lt) {
-                const int tile = blockIdx.x + lt * gridDim.x;
+                const int tile = tile_of(lt);
                 const int as = p.a_stages == 2 ? (lt & 1) : 0;
                 const int ause = p.a_stages == 2 ? (lt >> 1) : lt;
                 if (!mbar_wait(&bar->a_empty[as], (ause & 1) ^ 1, abort)) { ok = false; break; }
-                mbar_expect_tx(&bar->a_full[as], (uint32_t)a_stage_bytes);
+                if (rank == 0) mbar_expect_tx(&bar->a_full[as], (uint32_t)(NCTA * a_stage_bytes));
                 uint8_t *Ab = A + (size_t)as * a_stage_bytes;
                 for (int kp = 0; kp < p.kpanels; ++kp) {
-                    tma_load_2d(Ab + (size_t)kp * PANEL, &tmXh, &bar->a_full[as], kp * KP, tile * BM);
-                    tma_load_2d(Ab + (size_t)(p.kpanels + kp) * PANEL, &tmXl, &bar->a_full[as], kp * KP, tile * BM);
+                    load(Ab + (size_t)kp * PANEL, &tmXh, &bar->a_full[as], kp * KP, tile * BM);
+                    load(Ab + (size_t)(p.kpanels + kp) * PANEL, &tmXl, &bar->a_full[as], kp * KP, tile * BM);
                 }
                 a_issued[as]++;
                 for (int j = 0; j < p.ntiles_n && ok; ++j) {
                     for (int kb = 0; kb < p.kpanels * (KP / KPB); ++kb) {
                         if (!mbar_wait(&bar->b_empty[bs], bphase ^ 1, abort)) { ok = false; break; }
-                        mbar_expect_tx(&bar->b_full[bs], 2 * PANEL_B);
+                        if (rank == 0) mbar_expect_tx(&bar->b_full[bs], NCTA * 2 * PANEL_B);
                         uint8_t *Bb = B + (size_t)bs * 2 * PANEL_B;
-                        tma_load_2d(Bb, &tmCh, &bar->b_full[bs], kb * KPB, j * BN);
-                        tma_load_2d(Bb + PANEL_B, &tmCl, &bar->b_full[bs], kb * KPB, j * BN);
+                        const int brow = j * BN + (int)rank * BROWS;
+                        load(Bb, &tmCh, &bar->b_full[bs], kb * KPB, brow);
+                        load(Bb + PANEL_B, &tmCl, &bar->b_full[bs], kb * KPB, brow);
                         b_issued[bs]++;
                         if (++bs == p.b_stages) {
                             bs = 0;
@@ -409,8 +512,10 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                     }
                 }
             }
-            if (!ok) {
-                // Do not leave while our own bulk copies may still land in shared memory.
+            if (!ok && rank == 0) {
+                // Do not leave while bulk copies may still land in shared memory (a
+                // pair's copies all complete on the leader's barriers; the peer stays
+                // until the final cluster barrier, after this drain).
                 for (int i = 0; i < 2; ++i)
                     if (a_issued[i]) mbar_drain(&bar->a_full[i], (a_issued[i] - 1) & 1);
                 for (int i = 0; i < p.b_stages; ++i)
@@ -418,8 +523,17 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             }
         }
     } else if (warp == 1) {
-        if (lane == 0) {
+        if (lane == 0 && PAIR && rank != 0) {
+            // the peer of a pair issues no MMAs; the leader's final commit reaches it
+            mbar_drain(&bar->mma_done, 0);
+        } else if (lane == 0) {
             // ---------------- MMA issuer ----------------
+            auto commit = [](uint64_t *b) {
+                if (PAIR)
+                    mma_commit_pair(b);
+                else
+                    mma_commit(b);
+            };
             long long acount = 0;
             int bs = 0;
             uint32_t bphase = 0;  // B ring position and the parity of its current lap
@@ -448,20 +562,24 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                         const uint64_t bl = swb_desc<KPB>(su32(B + (size_t)bs * 2 * PANEL_B + PANEL_B));
                         // 16 bf16 = 32 bytes along the swizzled row = 2 in the descriptor's address field
 #pragma unroll
-                        for (int ks = 0; ks < KPB / 16; ++ks)
-                            mma_bf16x3(tmem_d, ah + 2 * ks, al + 2 * ks, bh + 2 * ks, bl + 2 * ks, kIdesc);
-                        mma_commit(&bar->b_empty[bs]);  // frees the B stage once these MMAs finish
+                        for (int ks = 0; ks < KPB / 16; ++ks) {
+                            if (PAIR)
+                                mma_bf16x3_pair(tmem_d, ah + 2 * ks, al + 2 * ks, bh + 2 * ks, bl + 2 * ks, kIdesc);
+                            else
+                                mma_bf16x3(tmem_d, ah + 2 * ks, al + 2 * ks, bh + 2 * ks, bl + 2 * ks, kIdesc);
+                        }
+                        commit(&bar->b_empty[bs]);  // frees the B stage (both CTAs' halves) once these MMAs finish
                         if (++bs == p.b_stages) {
                             bs = 0;
                             bphase ^= 1;
                         }
                     }
-                    if (ok) mma_commit(&bar->acc_full[slot]);
+                    if (ok) commit(&bar->acc_full[slot]);
                 }
-                if (ok) mma_commit(&bar->a_empty[as]);
+                if (ok) commit(&bar->a_empty[as]);
             }
-            // All issued MMAs complete before TMEM is released.
-            mma_commit(&bar->mma_done);
+            // All issued MMAs complete before TMEM is released (in both CTAs of a pair).
+            commit(&bar->mma_done);
             mbar_drain(&bar->mma_done, 0);
         }
     } else {
@@ -472,6 +590,14 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
         const uint32_t lane_base = tmem_base + ((uint32_t)(quarter * 32) << 16);
         long long acount = 0;
         bool ok = true;
+        // An accumulator is free for the next MMAs once every epilogue warp (of both
+        // CTAs of a pair: the barrier is the leader's) has drained it and refilled -h.
+        auto release_acc = [&](int slot_) {
+            if (PAIR)
+                mbar_arrive_remote(peer_addr(&bar->acc_empty[slot_], 0));
+            else
+                mbar_arrive(&bar->acc_empty[slot_]);
+        };
         // Accumulators start from -h (written here, one row per lane), so after the
         // MMAs they hold y = x.c - h = -score and the argmin becomes a max over y.
         // Every group drains the 32-column chunks group, group + NGROUPS, ... of each
@@ -486,14 +612,14 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             tmem_wait_st();
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bar->acc_empty[a0]);
+            if (lane == 0) release_acc(a0);
         }
         // Both groups pass the same number of named barriers (one per row tile),
         // also after an abort, so neither can be left waiting on the other.
         // Per-row inputs (band, prior threshold, ||x||^2) come from the row-bounds
         // pass and are loaded one row tile ahead, so no latency sits between two
         // accumulator drains.
-        auto row_of = [&](int lt_) { return (int64_t)(blockIdx.x + lt_ * gridDim.x) * BM + row_in_tile; };
+        auto row_of = [&](int lt_) { return (int64_t)tile_of(lt_) * BM + row_in_tile; };
         float2 nb = make_float2(__int_as_float(0xff800000), 0.0f);
         float nxn = 0.0f;
         if (my_tiles > 0 && row_of(0) < p.n) {
@@ -501,8 +627,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             nxn = p.xnorm[row_of(0)];
         }
         for (int lt = 0; lt < my_tiles; ++lt) {
-            const int tile = blockIdx.x + lt * gridDim.x;
-            const int64_t row = (int64_t)tile * BM + row_in_tile;
+            const int64_t row = row_of(lt);
             const float thr0 = nb.x;     // prior lower bound minus the band (-inf without a prior)
             const float band_up = nb.y;  // 2e rounded up
             const double band = (double)band_up;
@@ -596,7 +721,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 tmem_wait_st();
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&bar->acc_empty[slot]);
+                if (lane == 0) release_acc(slot);
             }
             // back to score space (score = -y) for the merge and the outputs
             r.b = -r.b;
@@ -645,15 +770,22 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
 
     __syncwarp();
     tc_fence_before();
-    __syncthreads();
+    if (PAIR)
+        cluster_sync_all();  // neither CTA leaves (or frees TMEM) while the pair still works on it
+    else
+        __syncthreads();
     if (bar->abort && threadIdx.x == 0) {
         p.st->error = KMB_ETIMEDOUT;
         p.st->done = 1;
     }
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS)
-                     : "memory");
+        if (PAIR)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS)
+                         : "memory");
+        else
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS)
+                         : "memory");
     }
 }
 
@@ -821,18 +953,28 @@ static EncodeTiledFn encode_fn() {
 
 // Row panels: the split rows (128 rows x 64 bf16, SWIZZLE_128B) or the split
 // centroids (256 clusters x 32 bf16, SWIZZLE_64B).
-static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t dpad, bool centroids, int bn = 0) {
+// (A CTA pair's centroid box is half the cluster tile: each CTA loads its half.)
+static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t dpad, bool centroids, int bn = 0,
+                       bool pair = false) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)dpad, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)dpad * 2};
-    const cuuint32_t box[2] = {centroids ? (cuuint32_t)tc::kpb_of(bn) : (cuuint32_t)tc::KP,
-                               centroids ? (cuuint32_t)bn : (cuuint32_t)tc::BM};
+    const int kpb = tc::kpb_of(bn, pair);
+    const cuuint32_t box[2] = {centroids ? (cuuint32_t)kpb : (cuuint32_t)tc::KP,
+                               centroids ? (cuuint32_t)tc::b_rows_of(bn, pair) : (cuuint32_t)tc::BM};
     const cuuint32_t estr[2] = {1u, 1u};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE,
-               (centroids && tc::kpb_of(bn) == 32) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+               (centroids && kpb == 32) ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// CTA pairs (tcgen05 cta_group::2, M = 256) unless the environment variable
+// KMB_TC_PAIR=0 asks for single CTAs (M = 128); read at every launch.
+static bool use_cta_pairs() {
+    const char *e = getenv("KMB_TC_PAIR");
+    return !(e && e[0] == '0');
 }
 
 // Launches the tensor-core assignment. Returns KMB_OK, or an error status when
@@ -853,7 +995,8 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     const int a_stage = 2 * kpanels * tc::PANEL;
     const int fixed = 1024 + (int)sizeof(tc::Barriers) + 64;
     const int bn = tc_tile_n(k);  // cluster tile (UMMA N); kpad is a multiple of it
-    const int panel_b = tc::panel_b_bytes(bn);
+    const bool pair = use_cta_pairs();
+    const int panel_b = tc::panel_b_bytes(bn, pair);
     int a_stages = (2 * a_stage + 3 * 2 * panel_b + fixed <= optin) ? 2 : 1;
     int b_stages = (optin - fixed - a_stages * a_stage) / (2 * panel_b);
     b_stages = std::min(b_stages, tc::MAX_B_STAGES);
@@ -865,7 +1008,7 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
 
     CUtensorMap mXh, mXl, mCh, mCl;
     if (!encode_map(&mXh, Xhi, n, dpad, false) || !encode_map(&mXl, Xlo, n, dpad, false) ||
-        !encode_map(&mCh, Chi, kpad, dpad, true, bn) || !encode_map(&mCl, Clo, kpad, dpad, true, bn))
+        !encode_map(&mCh, Chi, kpad, dpad, true, bn, pair) || !encode_map(&mCl, Clo, kpad, dpad, true, bn, pair))
         return KMB_ECUDA;
     tc::Params p;
     p.n = n;
@@ -892,13 +1035,55 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
                                                  (int)k, prior ? 1 : 0, (float2 *)rowb, st);
         KMB_LAUNCHED();
     }
-    auto kern = bn == 256 ? tc::assign_tc_kernel<256> : tc::assign_tc_kernel<128>;
+    if (!pair) {
+        auto kern = bn == 256 ? tc::assign_tc_kernel<256, false> : tc::assign_tc_kernel<128, false>;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return KMB_ECUDA;
+        // num_sms < 0: one CTA per 128-row tile (no persistence), so that other
+        // streams' launches interleave with this one at tile granularity
+        const int grid = num_sms < 0 ? p.n_tiles : (int)std::min<int64_t>(num_sms, p.n_tiles);
+        kern<<<grid, tc::NTHREADS, smem, s>>>(mXh, mXl, mCh, mCl, p);
+        KMB_LAUNCHED();
+        return cudaGetLastError() == cudaSuccess ? KMB_OK : KMB_ECUDA;
+    }
+    // CTA pairs: clusters of two CTAs, one 256-row unit per cluster at a time.
+    auto kern = bn == 256 ? tc::assign_tc_kernel<256, true> : tc::assign_tc_kernel<128, true>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return KMB_ECUDA;
-    // num_sms < 0: one CTA per 128-row tile (no persistence), so that other
-    // streams' launches interleave with this one at tile granularity
-    const int grid = num_sms < 0 ? p.n_tiles : (int)std::min<int64_t>(num_sms, p.n_tiles);
-    kern<<<grid, tc::NTHREADS, smem, s>>>(mXh, mXl, mCh, mCl, p);
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(tc::NTHREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const int64_t n_units = (p.n_tiles + 1) / 2;
+    int64_t clusters = n_units;
+    if (num_sms >= 0) {
+        // persistent: as many pairs as fit on the device at once (and within the SM cap)
+        static int cached_dev = -1, cached_bn = 0, cached_active = 0;
+        static size_t cached_smem = 0;
+        if (cached_dev != dev || cached_bn != bn || cached_smem != smem) {
+            int active = 0;
+            cfg.gridDim = dim3(2 * 74, 1, 1);
+            if (cudaOccupancyMaxActiveClusters(&active, kern, &cfg) != cudaSuccess || active <= 0) {
+                cudaGetLastError();
+                active = num_sms > 0 ? num_sms / 2 : 74;
+            }
+            cached_dev = dev;
+            cached_bn = bn;
+            cached_smem = smem;
+            cached_active = active;
+        }
+        clusters = std::min<int64_t>(clusters, cached_active);
+        if (num_sms > 0) clusters = std::min<int64_t>(clusters, std::max(1, num_sms / 2));
+    }
+    cfg.gridDim = dim3((unsigned)(2 * clusters), 1, 1);
+    if (cudaLaunchKernelEx(&cfg, kern, mXh, mXl, mCh, mCl, p) != cudaSuccess) return KMB_ECUDA;
     KMB_LAUNCHED();
     return cudaGetLastError() == cudaSuccess ? KMB_OK : KMB_ECUDA;
 }

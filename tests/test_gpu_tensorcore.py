@@ -143,3 +143,38 @@ def test_train_with_reseeds_equals_plain_form():
     assert a.get_iteration_count() == b.get_iteration_count()
     np.testing.assert_array_equal(a.get_responses(), b.get_responses())
     np.testing.assert_array_equal(a.get_model().get_centroids(), b.get_model().get_centroids())
+
+
+@pytest.mark.parametrize("n,d,k", [(1, 5, 3), (200, 64, 129), (385, 128, 300), (20000, 128, 1024), (9000, 200, 520)])
+def test_cta_pair_and_single_cta_kernels_agree(n, d, k, monkeypatch):
+    """The assignment runs on CTA pairs (cta_group::2, 256-row units, each CTA
+    loading half of every centroid panel) by default and on single CTAs with
+    KMB_TC_PAIR=0; both must give the FP64 oracle's responses and the same objective,
+    for row counts that leave the last pair half empty and both cluster-tile widths."""
+    rng = np.random.default_rng(n + d + k)
+    X = (rng.standard_normal((n, d)) * 2).astype(np.float32)
+    C = (rng.standard_normal((k, d)) * 2).astype(np.float32)
+    dsc = tc_desc(k).set_result_options(kmeans.result_options.compute_exact_objective_function)
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("KMB_TC_PAIR", mode)
+        r = kmeans.infer(dsc, kmeans.model(C), X)
+        out[mode] = (r.get_responses().ravel().copy(), r.get_objective_function_value())
+    lab64, _, _ = restated.assign_f32_in_f64(X, C)
+    assert (out["1"][0] == lab64).all()
+    assert (out["0"][0] == lab64).all()
+    assert rel_close(out["1"][1], out["0"][1], 1e-12)
+
+
+def test_cta_pair_training_matches_single_cta_training(monkeypatch):
+    """A few Lloyd iterations (prior-bound filter active from the second one) give
+    bit-identical centroids and responses on CTA pairs and on single CTAs."""
+    X, C0 = workloads.make(workloads.Workload("precision", 50000, 128, 512, 4, 0.0, 21), "cpu", 50000)
+    X, C0 = X.numpy(), C0.numpy()
+    res = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("KMB_TC_PAIR", mode)
+        r = kmeans.train(tc_desc(512, 4), X, C0)
+        res[mode] = (r.get_model().get_centroids().copy(), r.get_responses().ravel().copy())
+    np.testing.assert_array_equal(res["1"][0], res["0"][0])
+    np.testing.assert_array_equal(res["1"][1], res["0"][1])
