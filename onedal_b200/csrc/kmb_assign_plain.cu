@@ -16,6 +16,9 @@
 
 #include <float.h>
 
+#include <algorithm>
+#include <cstdlib>
+
 namespace kmb {
 namespace {
 
@@ -359,6 +362,244 @@ assign_small_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restri
     }
 }
 
+// ---- FP32, centroids resident in shared memory ------------------------------
+// When all (padded) centroids fit in shared memory next to two row tiles, one
+// persistent CTA per SM keeps C^T and the half norms resident for the whole
+// launch and streams 128-row tiles of X through a two-stage TMA ring, so no
+// centroid byte is re-read per row tile and the FMA loop has no block barrier.
+// 16 warps; warp w owns rows 8w..8w+7 of the tile, lane l the clusters
+// 4l..4l+3 and 128+4l..128+4l+3 of each 256-cluster pass: the row values are
+// shared-memory broadcasts and the centroid reads are conflict-free 16-byte
+// loads. Per (row, cluster) the contraction accumulates x_t * c_t in ascending
+// t with FMAs from zero, as assign_plain_kernel does, so the scores -- and the
+// labels, distances and recheck entries -- are the same. After each pass a
+// lane holds the top-3 of its 8 clusters for its warp's 8 rows; five exchange
+// rounds halve the rows a lane keeps while merging in the partner's (value,
+// index) triples, leaving each row's top-3 in four lanes; with more than one
+// pass the row's owner lane merges it into the running top-3 in shared memory.
+constexpr int kResThreads = 512;
+constexpr int kResRows = 128;
+constexpr int kResPass = 256;
+constexpr long long kResTimeout = 4000000000ll;  // ~2 s of SM clocks per wait
+
+struct ResBarriers {
+    uint64_t full[2];
+    int abort;
+};
+
+__device__ __forceinline__ uint32_t res_su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool res_try_wait(uint64_t *b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(res_su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false after ~2 s (recorded in abort) or when another thread aborted.
+__device__ __forceinline__ bool res_wait(uint64_t *b, uint32_t parity, volatile int *abort) {
+    if (res_try_wait(b, parity)) return true;
+    const long long t0 = clock64();
+    while (!res_try_wait(b, parity)) {
+        if (*abort) return false;
+        if (clock64() - t0 > kResTimeout) {
+            *abort = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ void res_load_tile(float *dst, const CUtensorMap *tm, uint64_t *bar, int row0,
+                                              uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(res_su32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            res_su32(dst)),
+        "l"(tm), "r"(res_su32(bar)), "r"(0), "r"(row0)
+        : "memory");
+}
+
+// Keeps the rows of one half of `t` (hi: the upper half) and merges in the
+// partner lane's triples of the same rows.
+template <int R>
+__device__ __forceinline__ void res_exchange(RowTop<float> (&t)[8], int mask, bool hi) {
+#pragma unroll
+    for (int q = 0; q < R / 2; ++q) {
+        const RowTop<float> keep = hi ? t[R / 2 + q] : t[q];
+        const RowTop<float> send = hi ? t[q] : t[R / 2 + q];
+        t[q] = top_merge(keep, shfl_top(send, mask));
+    }
+}
+
+__global__ void __launch_bounds__(kResThreads, 1)
+assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d, int dpad, const float *__restrict__ Ct,
+                       const float *__restrict__ h, int k, int kpad, int kres, const float *__restrict__ xnorm,
+                       const double *__restrict__ cnorm_max, int32_t *__restrict__ labels, float *__restrict__ d2,
+                       RecheckEntry *__restrict__ queue, LoopState *__restrict__ st) {
+    __shared__ int s_skip;
+    if (threadIdx.x == 0) s_skip = st ? st->done : 0;
+    __syncthreads();
+    if (s_skip) return;
+    extern __shared__ uint8_t res_smem_raw[];
+    uint8_t *sm = (uint8_t *)(((uintptr_t)res_smem_raw + 127) & ~(uintptr_t)127);
+    const int tile_floats = kResRows * dpad;
+    float *Xs = (float *)sm;                   // [2][128][dpad]
+    float *Cs = Xs + 2 * tile_floats;          // [dpad][kres]
+    float *hs = Cs + (size_t)dpad * kres;      // [kres]
+    RowTop<float> *run = (RowTop<float> *)(hs + kres);  // [128] running top-3 across passes
+    ResBarriers *bar = (ResBarriers *)(run + kResRows);
+    volatile int *abort = &bar->abort;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int n_tiles = (int)((n + kResRows - 1) / kResRows);
+    const int my_tiles = (n_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    const uint32_t tile_bytes = (uint32_t)tile_floats * 4u;
+    if (tid == 0) {
+        for (int i = 0; i < 2; ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(res_su32(&bar->full[i])) : "memory");
+        bar->abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    int issued[2] = {0, 0};  // thread 0: loads issued into each stage
+    if (tid == 0 && my_tiles > 0) {
+        res_load_tile(Xs, &tmX, &bar->full[0], (int)blockIdx.x * kResRows, tile_bytes);
+        issued[0] = 1;
+    }
+    // Resident centroids: C^T (zero columns past kpad) and half norms (+inf past kpad).
+    const int kq = kres / 4, kq_src = kpad / 4;
+    for (int i = tid; i < dpad * kq; i += kResThreads) {
+        const int t = i / kq, c4 = i - t * kq;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c4 < kq_src) v = *reinterpret_cast<const float4 *>(Ct + (size_t)t * kpad + 4 * c4);
+        *reinterpret_cast<float4 *>(Cs + (size_t)t * kres + 4 * c4) = v;
+    }
+    for (int j = tid; j < kres; j += kResThreads) hs[j] = j < kpad ? h[j] : f_inf<float>();
+    __syncthreads();
+
+    const double u = 5.9604644775390625e-8;  // 2^-24
+    const double cmax = cnorm_max ? *cnorm_max : 0.0;
+    const int n_pass = kres / kResPass;
+    // the row of the tile whose final top-3 this lane holds after the exchange
+    const int own = 8 * warp + ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+    bool ok = true;
+    for (int lt = 0; lt < my_tiles; ++lt) {
+        const int buf = lt & 1;
+        const int64_t row0 = ((int64_t)blockIdx.x + (int64_t)lt * gridDim.x) * kResRows;
+        // the next tile goes into the other stage, which every thread left at the
+        // end of the previous iteration
+        if (tid == 0 && ok && lt + 1 < my_tiles) {
+            res_load_tile(Xs + (buf ^ 1) * tile_floats, &tmX, &bar->full[buf ^ 1],
+                          (int)(row0 + (int64_t)gridDim.x * kResRows), tile_bytes);
+            issued[buf ^ 1]++;
+        }
+        if (ok && !__all_sync(0xffffffffu, res_wait(&bar->full[buf], (lt >> 1) & 1, abort))) ok = false;
+        if (ok) {
+            const float *xa = Xs + buf * tile_floats + (8 * warp) * dpad;
+            for (int pass = 0; pass < n_pass; ++pass) {
+                const float *cb = Cs + pass * kResPass + 4 * lane;
+                float acc[8][8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+#pragma unroll 2
+                for (int t = 0; t < dpad; t += 2) {
+                    float2 a[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) a[i] = *reinterpret_cast<const float2 *>(xa + i * dpad + t);
+                    const float4 b00 = *reinterpret_cast<const float4 *>(cb + (size_t)t * kres);
+                    const float4 b01 = *reinterpret_cast<const float4 *>(cb + (size_t)t * kres + 128);
+                    const float4 b10 = *reinterpret_cast<const float4 *>(cb + (size_t)(t + 1) * kres);
+                    const float4 b11 = *reinterpret_cast<const float4 *>(cb + (size_t)(t + 1) * kres + 128);
+                    const float bx[8] = {b00.x, b00.y, b00.z, b00.w, b01.x, b01.y, b01.z, b01.w};
+                    const float by[8] = {b10.x, b10.y, b10.z, b10.w, b11.x, b11.y, b11.z, b11.w};
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i].x, bx[j], acc[i][j]);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i].y, by[j], acc[i][j]);
+                }
+                RowTop<float> top[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    top[i].b = top[i].s = top[i].t = f_inf<float>();
+                    top[i].ib = top[i].is = 0;
+                }
+                // this lane's clusters in ascending order: strict '<' keeps the lowest index on ties
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int col = pass * kResPass + (j < 4 ? 4 * lane + j : 128 + 4 * lane + (j - 4));
+                    const float hj = hs[col];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) top_push(top[i], hj - acc[i][j], col);
+                }
+                res_exchange<8>(top, 16, (lane >> 4) & 1);
+                res_exchange<4>(top, 8, (lane >> 3) & 1);
+                res_exchange<2>(top, 4, (lane >> 2) & 1);
+                top[0] = top_merge(top[0], shfl_top(top[0], 2));
+                top[0] = top_merge(top[0], shfl_top(top[0], 1));
+                if ((lane & 3) == 0) {
+                    RowTop<float> r = top[0];
+                    if (pass > 0) r = top_merge(run[own], r);
+                    if (pass + 1 < n_pass) {
+                        run[own] = r;
+                    } else {
+                        const int64_t row = row0 + own;
+                        if (row < n) {
+                            labels[row] = r.ib;
+                            const float xn = xnorm[row];
+                            d2[row] = 2.0f * r.b + xn;
+                            if (queue) {
+                                const double xl = sqrt(fmax((double)xn, 0.0));
+                                const double e = 1.0625 * u * (cmax * cmax + (double)(d + 2) * xl * cmax);
+                                const double band = 2.0 * e;
+                                if ((double)r.s - (double)r.b <= band)
+                                    enqueue_recheck(queue, n, st, (int)row, r.ib, r.is,
+                                                    (double)r.t - (double)r.b <= band);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();  // this stage is read by everyone before the next load into it
+    }
+    if (tid == 0) {
+        if (bar->abort) {
+            // leave no bulk copy landing in shared memory behind: wait (bounded) for
+            // the last load issued into each stage
+            for (int b = 0; b < 2; ++b) {
+                if (!issued[b]) continue;
+                const long long t0 = clock64();
+                while (!res_try_wait(&bar->full[b], (uint32_t)((issued[b] - 1) & 1)) && clock64() - t0 < kResTimeout) {
+                }
+            }
+            if (st) {
+                st->error = KMB_ETIMEDOUT;
+                st->done = 1;
+            }
+        }
+    }
+}
+
+// Shared memory of assign_resident_kernel for dpad features and kres resident
+// clusters (0 when it does not fit the device's per-block limit).
+size_t resident_smem_bytes(int dpad, int kres, int optin) {
+    const size_t b = 128 + (size_t)2 * kResRows * dpad * 4 + (size_t)dpad * kres * 4 + (size_t)kres * 4 +
+                     (size_t)kResRows * sizeof(RowTop<float>) + sizeof(ResBarriers);
+    return b <= (size_t)optin ? b : 0;
+}
+
 }  // namespace
 
 template <typename F>
@@ -389,6 +630,47 @@ void launch_small(const F *X, int64_t n, int64_t d, const F *Ct, const F *h, int
     KMB_LAUNCHED();
 }
 
+// FP32 rows whose centroids fit in shared memory (d a multiple of 4 and at most
+// 256, 16-byte aligned rows): the resident kernel. False when it does not apply.
+template <typename F>
+bool launch_resident(const F *, int64_t, int64_t, const F *, const F *, int64_t, int64_t, const F *, const double *,
+                     int32_t *, F *, RecheckEntry *, LoopState *, cudaStream_t) {
+    return false;
+}
+template <>
+bool launch_resident<float>(const float *X, int64_t n, int64_t d, const float *Ct, const float *h, int64_t k,
+                            int64_t kpad, const float *xnorm, const double *cnorm_max, int32_t *labels, float *d2,
+                            RecheckEntry *queue, LoopState *st, cudaStream_t s) {
+    if (d % 4 != 0 || d > 256 || (reinterpret_cast<uintptr_t>(X) % 16) != 0 || n > INT32_MAX - 2 * kResRows)
+        return false;
+    const char *e = getenv("KMB_PLAIN_RESIDENT");
+    if (e && e[0] == '0') return false;
+    const int dpad = (int)((d + BK - 1) / BK * BK);  // the rows of Ct
+    const int kres = (int)((kpad + kResPass - 1) / kResPass * kResPass);
+    int dev = 0, optin = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t smem = resident_smem_bytes(dpad, kres, optin);
+    if (smem == 0) return false;
+    CUtensorMap tm;
+    // box: 128 rows x dpad columns (columns past d read as zeros)
+    if (!encode_tensor_map_2d(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, X, (uint64_t)d, (uint64_t)n, (uint64_t)d * 4,
+                              (uint32_t)dpad, (uint32_t)kResRows, CU_TENSOR_MAP_SWIZZLE_NONE))
+        return false;
+    if (cudaFuncSetAttribute(assign_resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const int64_t n_tiles = (n + kResRows - 1) / kResRows;
+    const int grid = (int)std::min<int64_t>(n_tiles, sms);
+    assign_resident_kernel<<<grid, kResThreads, smem, s>>>(tm, n, (int)d, dpad, Ct, h, (int)k, (int)kpad, kres, xnorm,
+                                                           cnorm_max, labels, d2, queue, st);
+    KMB_LAUNCHED();
+    return true;
+}
+
 template <typename F>
 void launch_assign_plain(const F *X, int64_t n, int64_t d, const F *Ct, const F *h, int64_t k, int64_t kpad,
                          const F *xnorm, const double *cnorm_max, int32_t *labels, F *d2, RecheckEntry *queue,
@@ -400,6 +682,7 @@ void launch_assign_plain(const F *X, int64_t n, int64_t d, const F *Ct, const F 
         else launch_small<F, 64>(X, n, d, Ct, h, k, kpad, xnorm, cnorm_max, labels, d2, queue, st, s);
         return;
     }
+    if (launch_resident(X, n, d, Ct, h, k, kpad, xnorm, cnorm_max, labels, d2, queue, st, s)) return;
     const unsigned blocks = (unsigned)((n + BM - 1) / BM);
     const bool vec = (d % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) % (4 * sizeof(F))) == 0);
     if (vec) {

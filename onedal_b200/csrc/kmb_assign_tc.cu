@@ -951,6 +951,18 @@ static EncodeTiledFn encode_fn() {
     return fn;
 }
 
+bool encode_tensor_map_2d(CUtensorMap *m, CUtensorMapDataType type, const void *base, uint64_t inner, uint64_t outer,
+                          uint64_t row_bytes, uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle swizzle) {
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+    const cuuint64_t strides[1] = {(cuuint64_t)row_bytes};
+    const cuuint32_t box[2] = {box_inner, box_outer};
+    const cuuint32_t estr[2] = {1u, 1u};
+    return enc(m, type, 2, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Row panels: the split rows (128 rows x 64 bf16, SWIZZLE_128B) or the split
 // centroids (256 clusters x 32 bf16, SWIZZLE_64B).
 // (A CTA pair's centroid box is half the cluster tile: each CTA loads its half.)
@@ -970,11 +982,14 @@ static bool encode_map(CUtensorMap *m, const void *base, int64_t rows, int64_t d
                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// CTA pairs (tcgen05 cta_group::2, M = 256) unless the environment variable
-// KMB_TC_PAIR=0 asks for single CTAs (M = 128); read at every launch.
+// Single CTAs (M = 128) unless the environment variable KMB_TC_PAIR=1 asks for
+// CTA pairs (tcgen05 cta_group::2, M = 256); read at every launch. With the three
+// split products per k-step the pairs measured slower (14.9 against 14.1 ms per
+// 20M-row launch at d = 128, k = 1024): halving each CTA's centroid-panel bytes
+// did not pay for the pair's cross-CTA barrier traffic.
 static bool use_cta_pairs() {
     const char *e = getenv("KMB_TC_PAIR");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
 }
 
 // Launches the tensor-core assignment. Returns KMB_OK, or an error status when

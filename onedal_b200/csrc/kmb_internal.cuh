@@ -1,6 +1,7 @@
 // Internal declarations shared by the k-means Lloyd kernels (sm_100a).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -175,6 +176,12 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
                      float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, bool prior,
                      const double *shift_part, const double *cnorm_max_prev, void *rowb, cudaStream_t s);
 size_t tc_xchg_bytes();
+
+// Encodes a 2-D tiled tensor map (inner x outer elements, rows row_bytes apart,
+// box_inner x box_outer boxes) through the runtime's driver entry point, so the
+// library does not link libcuda directly. False when the driver rejects it.
+bool encode_tensor_map_2d(CUtensorMap *m, CUtensorMapDataType type, const void *base, uint64_t inner, uint64_t outer,
+                          uint64_t row_bytes, uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle swizzle);
 
 // ---- CSR rows (kmeans::method::lloyd_csr) ------------------------------------
 // Zero-based, device-resident CSR rows: values (nnz, F), column indices (int32,

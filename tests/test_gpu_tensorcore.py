@@ -147,9 +147,9 @@ def test_train_with_reseeds_equals_plain_form():
 
 @pytest.mark.parametrize("n,d,k", [(1, 5, 3), (200, 64, 129), (385, 128, 300), (20000, 128, 1024), (9000, 200, 520)])
 def test_cta_pair_and_single_cta_kernels_agree(n, d, k, monkeypatch):
-    """The assignment runs on CTA pairs (cta_group::2, 256-row units, each CTA
-    loading half of every centroid panel) by default and on single CTAs with
-    KMB_TC_PAIR=0; both must give the FP64 oracle's responses and the same objective,
+    """The assignment runs on single CTAs by default and on CTA pairs
+    (cta_group::2, 256-row units, each CTA loading half of every centroid panel)
+    with KMB_TC_PAIR=1; both must give the FP64 oracle's responses and the same objective,
     for row counts that leave the last pair half empty and both cluster-tile widths."""
     rng = np.random.default_rng(n + d + k)
     X = (rng.standard_normal((n, d)) * 2).astype(np.float32)
