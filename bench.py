@@ -1,7 +1,7 @@
 """Benchmark: k-means Lloyd iterations/s on the precision workload
 (n=20,000,000, d=128, k=1024, float32 input), one B200 per rank.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--form bf16x3|plain] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--form bf16|bf16x3|plain] [--impl b200|reference]
 
 A step is one Lloyd iteration (assignment + centroid update) over all rows,
 inputs resident in HBM (10.24 GB of rows, far larger than the 126 MB L2, so no
@@ -608,7 +608,8 @@ def run_b200(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     w = workloads.PRECISION
-    form = _native.KMB_FORM_BF16X3 if args.form == "bf16x3" else _native.KMB_FORM_PLAIN
+    form = {"bf16x3": _native.KMB_FORM_BF16X3, "bf16": _native.KMB_FORM_BF16}.get(args.form, _native.KMB_FORM_PLAIN)
+    tc_form = form != _native.KMB_FORM_PLAIN
     if world > 1:
         return run_sharded(args, dist, world, rank, local, form)
 
@@ -650,7 +651,7 @@ def run_b200(args):
         dist.barrier()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
-    kernel_id = 1 if form == _native.KMB_FORM_BF16X3 else 0
+    kernel_id = 1 if tc_form else 0
     kt = ctypes.c_double()
     kl = ctypes.c_int64()
     ctx.check(ctx.lib.kmb_context_kernel_time(ctx.handle, kernel_id, ctypes.byref(kt), ctypes.byref(kl)))
@@ -672,7 +673,7 @@ def run_b200(args):
 
     # Plain-form comparison (the north-star ratio) on the same data, when timing the BF16 form.
     plain_value = None
-    if form == _native.KMB_FORM_BF16X3 and args.plain_steps > 0:
+    if tc_form and args.plain_steps > 0:
         C.copy_(C0)
         e0.record(stream)
         p = _native.kmb_params(k, args.plain_steps, 0.0, _native.KMB_FORM_PLAIN, 0)
@@ -688,15 +689,16 @@ def run_b200(args):
     flops_per_launch = 2.0 * n * k * d
     avg_kernel_s = (kt.value / max(kl.value, 1)) / 1e3
     achieved_tflops = flops_per_launch / avg_kernel_s / 1e12 if kl.value else None
-    if form == _native.KMB_FORM_BF16X3:
+    if tc_form:
         peak = peaks["bf16_tflops_sustained"]
         peak_note = f"bf16 dense sustained ({peak_src})"
     else:
         peak = measured_fma_peak_tflops(local, 0)
         peak_note = "FP32 FMA peak measured on this GPU (kmb_measure_fma_peak)"
     dpad = (d + 63) // 64 * 64
-    if form == _native.KMB_FORM_BF16X3:
-        algo_bytes = 4 * n * dpad + 8 * n  # Xhi + Xlo read once, labels + d2 written
+    if tc_form:
+        # Xhi (+ Xlo for the split form) read once, labels + d2 written
+        algo_bytes = (4 if form == _native.KMB_FORM_BF16X3 else 2) * n * dpad + 8 * n
         # DRAM read+write bytes per row from the ncu capture summarised in
         # profiles/assign_tc_kernel_precision_n1M.txt (scaled by rows).
         traffic = args.traffic_bytes if args.traffic_bytes is not None else TC_DRAM_BYTES_PER_ROW * n
@@ -705,7 +707,7 @@ def run_b200(args):
         algo_bytes = 4 * n * d + 8 * n
         traffic = args.traffic_bytes
         traffic_src = None
-    roofline = {"bound": "tensor" if form == _native.KMB_FORM_BF16X3 else "fp32_fma", "achieved": achieved_tflops,
+    roofline = {"bound": "tensor" if tc_form else "fp32_fma", "achieved": achieved_tflops,
                 "peak": peak, "unit": "TFLOP/s", "frac": (achieved_tflops / peak) if achieved_tflops else None,
                 "traffic": traffic, "traffic_source": traffic_src, "peak_source": peak_note,
                 "kernel_ms_avg": avg_kernel_s * 1e3, "kernel_launches": kl.value,
@@ -801,7 +803,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--form", default="bf16x3", choices=["bf16x3", "plain"])
+    ap.add_argument("--form", default="bf16x3", choices=["bf16", "bf16x3", "plain"])
     ap.add_argument("--plain-steps", type=int, default=10)
     ap.add_argument("--cpu-iterations", type=int, default=2,
                     help="Lloyd iterations of the reference kernel on all rows for cpu_baseline (0 skips it)")

@@ -63,10 +63,17 @@ typedef enum kmb_memory { KMB_MEM_HOST = 0, KMB_MEM_DEVICE = 1 } kmb_memory;
  *                  row whose top-2 gap is inside the derived error bound is
  *                  rechecked exactly in FP64, so responses equal the FP64
  *                  oracle's.
- * KMB_FORM_AUTO  : BF16X3 for FP32 data with d <= 256 once the contraction is
- *                  dense enough to pay for the tensor cores (n * kpad * dpad >=
- *                  KMB_AUTO_TC_MACS), the plain form otherwise. */
-typedef enum kmb_form { KMB_FORM_PLAIN = 0, KMB_FORM_BF16X3 = 1, KMB_FORM_AUTO = 2 } kmb_form;
+ * KMB_FORM_BF16  : FP32 data only. One BF16 tcgen05 product (bf16(x).bf16(c))
+ *                  with FP32 accumulation; its wider error bound sends more
+ *                  near-tie rows to the same exact FP64 recheck, so responses
+ *                  again equal the FP64 oracle's. A third of the tensor work of
+ *                  BF16X3; the faster of the two unless a large share of the rows
+ *                  lies near a tie.
+ * KMB_FORM_AUTO  : a tensor-core form for FP32 data with d <= 256 once the
+ *                  contraction is dense enough to pay for the tensor cores
+ *                  (n * kpad * dpad >= KMB_AUTO_TC_MACS), the plain form
+ *                  otherwise. */
+typedef enum kmb_form { KMB_FORM_PLAIN = 0, KMB_FORM_BF16X3 = 1, KMB_FORM_AUTO = 2, KMB_FORM_BF16 = 3 } kmb_form;
 #define KMB_AUTO_TC_MACS (1LL << 30)
 
 typedef struct kmb_context kmb_context;

@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libonedal_b200_kmeans.so")
 KMB_OK, KMB_EINVAL, KMB_ENOMEM, KMB_ECUDA, KMB_ETIMEDOUT, KMB_ETOO_MANY_EMPTY, KMB_EUNSUPPORTED = range(7)
 KMB_F32, KMB_F64 = 0, 1
 KMB_MEM_HOST, KMB_MEM_DEVICE = 0, 1
-KMB_FORM_PLAIN, KMB_FORM_BF16X3, KMB_FORM_AUTO = 0, 1, 2
+KMB_FORM_PLAIN, KMB_FORM_BF16X3, KMB_FORM_AUTO, KMB_FORM_BF16 = 0, 1, 2, 3
 
 # Every symbol the public header declares; tests check the library exports them all.
 EXPORTED = (

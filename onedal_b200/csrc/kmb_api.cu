@@ -33,6 +33,8 @@ struct kmb_context {
     // its row count (the queue's capacity) and its loop state.
     int64_t queue_rows = 0;
     const kmb::LoopState *queue_state = nullptr;
+    // BF16 products per k-step of the current call's tensor-core form (3: split, 1: single)
+    int tc_products = 3;
     // kernel timing (kmb_context_set_kernel_timing)
     bool timing = false;
     int64_t launches_at_enable = 0;
@@ -161,7 +163,7 @@ int ensure_common(kmb_context *ctx, int64_t n, int64_t d, int64_t k, bool rechec
     if (tc) {
         const int64_t tdp = kmb::tc_dpad(d), tkp = kmb::tc_kpad(k);
         ok &= ws.ensure(ws.Xhi, sizeof(uint16_t) * n * tdp);
-        ok &= ws.ensure(ws.Xlo, sizeof(uint16_t) * n * tdp);
+        if (ctx->tc_products == 3) ok &= ws.ensure(ws.Xlo, sizeof(uint16_t) * n * tdp);
         ok &= ws.ensure(ws.Chi, sizeof(uint16_t) * tkp * tdp);
         ok &= ws.ensure(ws.Clo, sizeof(uint16_t) * tkp * tdp);
         ok &= ws.ensure(ws.h, sizeof(float) * tkp);
@@ -216,11 +218,13 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
     int rc;
     {
         KernelTimer timer(ctx, 1);
-        rc = kmb::launch_assign_tc(ws.Xhi.ptr, ws.Xlo.ptr, n, d, ws.Chi.ptr, ws.Clo.ptr, (const float *)ws.h.ptr, k,
+        rc = kmb::launch_assign_tc(ws.Xhi.ptr, ctx->tc_products == 3 ? ws.Xlo.ptr : ws.Xhi.ptr, n, d, ws.Chi.ptr,
+                                   ws.Clo.ptr, (const float *)ws.h.ptr, k,
                                    (const float *)ws.xnorm.ptr, &sc->cnorm_max, labels, d2,
                                    (RecheckEntry *)ws.queue.ptr, st, ctx->tc_per_tile ? -1 : ctx->num_sms,
                                    ws.tcx.ptr, prior,
-                                   (const double *)ws.shift_part.ptr, &sc->cnorm_max_prev, ws.rowb.ptr, s);
+                                   (const double *)ws.shift_part.ptr, &sc->cnorm_max_prev, ws.rowb.ptr,
+                                   ctx->tc_products, s);
     }
     if (rc != KMB_OK) return fail(ctx, rc, "tensor-core assignment launch failed (d=%lld)", (long long)d);
     {
@@ -283,7 +287,8 @@ void prepare_rows(kmb_context *ctx, const F *X, int64_t n, int64_t d, bool tc) {
 template <>
 void prepare_rows<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d, bool tc) {
     if (tc)
-        kmb::launch_split_rows(X, n, d, ctx->ws.Xhi.ptr, ctx->ws.Xlo.ptr, (float *)ctx->ws.xnorm.ptr, ctx->num_sms,
+        kmb::launch_split_rows(X, n, d, ctx->ws.Xhi.ptr, ctx->tc_products == 3 ? ctx->ws.Xlo.ptr : nullptr,
+                               (float *)ctx->ws.xnorm.ptr, ctx->num_sms,
                                ctx->stream);
     else
         kmb::launch_row_norms<float>(X, n, d, (float *)ctx->ws.xnorm.ptr, ctx->stream);
@@ -301,11 +306,15 @@ int upload(kmb_context *ctx, kmb::DevBuf &buf, const void *src, size_t bytes, co
     return KMB_OK;
 }
 
+// The tensor-core forms and their BF16 products per k-step.
+bool is_tc_form(int form) { return form == KMB_FORM_BF16X3 || form == KMB_FORM_BF16; }
+int form_products(int form) { return form == KMB_FORM_BF16 ? 1 : 3; }
+
 int check_form(kmb_context *ctx, int dtype, int form) {
-    if (form != KMB_FORM_PLAIN && form != KMB_FORM_BF16X3 && form != KMB_FORM_AUTO)
+    if (form != KMB_FORM_PLAIN && form != KMB_FORM_BF16X3 && form != KMB_FORM_BF16 && form != KMB_FORM_AUTO)
         return fail(ctx, KMB_EINVAL, "unknown form %d", form);
-    if (form == KMB_FORM_BF16X3 && dtype != KMB_F32)
-        return fail(ctx, KMB_EINVAL, "the BF16x3 tensor-core form takes float32 data");
+    if (is_tc_form(form) && dtype != KMB_F32)
+        return fail(ctx, KMB_EINVAL, "the BF16 tensor-core forms take float32 data");
     return KMB_OK;
 }
 
@@ -338,7 +347,8 @@ int run_loop(kmb_context *ctx, const F *X, int64_t n, int64_t d, F *C, const kmb
     init_state(ctx->h_state[0], p->accuracy_threshold);
     KMB_CUDA(cudaMemcpyAsync(st, ctx->h_state, sizeof(LoopState), cudaMemcpyHostToDevice, s));
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
-    const bool tc = p->form == KMB_FORM_BF16X3;
+    const bool tc = is_tc_form(p->form);
+    ctx->tc_products = form_products(p->form);
     prepare_rows<F>(ctx, X, n, d, tc);
     const int64_t T = p->max_iteration_count;
     int64_t enq = 0;
@@ -350,7 +360,8 @@ int run_loop(kmb_context *ctx, const F *X, int64_t n, int64_t d, F *C, const kmb
             int rc = assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, d2, st, tc, /*prior=*/enq > 0);
             if (rc) return rc;
             KernelTimer timer(ctx, 2);
-            kmb::launch_update<F>(X, plan, labels, d2, C, Cnew, ws, st, /*commit=*/true, s);
+            kmb::launch_update<F>(X, plan, labels, d2, C, Cnew, ws, st, /*commit=*/true, s, nullptr,
+                                  tc ? d2 : nullptr);
         }
         KMB_CUDA(cudaGetLastError());
         if (enq < T) {
@@ -367,7 +378,8 @@ template <typename F>
 int iterate_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, void *Cv, const kmb_params *p,
                  int32_t *labels, int64_t *iteration_count, kmb_stats *stats) {
     const int64_t k = p->cluster_count;
-    const bool tc = p->form == KMB_FORM_BF16X3;
+    const bool tc = is_tc_form(p->form);
+    ctx->tc_products = form_products(p->form);
     if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
     const bool recheck = p->recheck != 0 || tc;
     int rc = ensure_common<F>(ctx, n, d, k, recheck, tc);
@@ -396,7 +408,8 @@ int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
                const kmb_params *p, void *C_out, int32_t *responses, double *objective, int64_t *iteration_count,
                kmb_stats *stats) {
     const int64_t k = p->cluster_count;
-    const bool tc = p->form == KMB_FORM_BF16X3;
+    const bool tc = is_tc_form(p->form);
+    ctx->tc_products = form_products(p->form);
     if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
     const bool recheck = p->recheck != 0 || tc;
     int rc = ensure_common<F>(ctx, n, d, k, recheck, tc);
@@ -457,7 +470,8 @@ int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
 template <typename F>
 int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t d, const void *Cv, int64_t k,
                int32_t form, int32_t compute_objective, int32_t *responses, double *objective, kmb_stats *stats) {
-    const bool tc = form == KMB_FORM_BF16X3;
+    const bool tc = is_tc_form(form);
+    ctx->tc_products = form_products(form);
     if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
     const bool recheck = tc;
     int rc = ensure_common<F>(ctx, n, d, k, recheck, tc);
@@ -503,7 +517,8 @@ int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
 template <typename F>
 int step_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, const void *Cin, int64_t k, int32_t form,
               int32_t recheck_flag, void *C_out, int32_t *labels, double *shift, int64_t *n_empty) {
-    const bool tc = form == KMB_FORM_BF16X3;
+    const bool tc = is_tc_form(form);
+    ctx->tc_products = form_products(form);
     if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
     const bool recheck = recheck_flag != 0 || tc;
     int rc = ensure_common<F>(ctx, n, d, k, recheck, tc);
@@ -522,7 +537,8 @@ int step_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, const void
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
     prepare_rows<F>(ctx, X, n, d, tc);
     if ((rc = assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, (F *)ws.d2.ptr, st, tc))) return rc;
-    kmb::launch_update<F>(X, plan, labels, (const F *)ws.d2.ptr, Ccur, (F *)C_out, ws, st, /*commit=*/false, s);
+    kmb::launch_update<F>(X, plan, labels, (const F *)ws.d2.ptr, Ccur, (F *)C_out, ws, st, /*commit=*/false, s,
+                          nullptr, tc ? (F *)ws.d2.ptr : nullptr);
     KMB_CUDA(cudaGetLastError());
     KMB_CUDA(cudaMemcpyAsync(ctx->h_state, st, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
     KMB_CUDA(cudaStreamSynchronize(s));
@@ -537,7 +553,8 @@ int step_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, const void
 template <typename F>
 int partial_impl(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, int64_t k, int32_t form,
                  int32_t *labels, double *sums, int64_t *counts, double *sq_distances, F *row_sq) {
-    const bool tc = form == KMB_FORM_BF16X3;
+    const bool tc = is_tc_form(form);
+    ctx->tc_products = form_products(form);
     if (tc && !kmb::tc_supported(d)) return fail(ctx, KMB_EUNSUPPORTED, "tensor-core form needs d <= 256");
     int rc = ensure_common<F>(ctx, n, d, k, tc, tc);
     if (rc) return rc;

@@ -237,6 +237,24 @@ __device__ __forceinline__ void mma_bf16x3(uint32_t tmem_d, uint64_t ah, uint64_
         "l"(ah), "l"(al), "l"(bh), "l"(bl), "r"(idesc)
         : "memory");
 }
+// One BF16 product per k-step (xh.ch): the single-product form.
+__device__ __forceinline__ void mma_bf16x1(uint32_t tmem_d, uint64_t ah, uint64_t bh, uint32_t idesc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, 1, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(ah), "l"(bh), "r"(idesc)
+        : "memory");
+}
+__device__ __forceinline__ void mma_bf16x1_pair(uint32_t tmem_d, uint64_t ah, uint64_t bh, uint32_t idesc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, 1, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(ah), "l"(bh), "r"(idesc)
+        : "memory");
+}
+
 // The same for a CTA pair (issued by the leader CTA): M = 256 rows, 128 from
 // each CTA's A panels; the B tile's two halves come from the two CTAs.
 __device__ __forceinline__ void mma_bf16x3_pair(uint32_t tmem_d, uint64_t ah, uint64_t al, uint64_t bh, uint64_t bl,
@@ -375,7 +393,7 @@ __device__ __forceinline__ Top3 top3_merge(const Top3 &x, const Top3 &y) {
 }
 
 
-template <int BN, bool PAIR>
+template <int BN, bool PAIR, int NPROD>
 __global__ void __launch_bounds__(NTHREADS, 1)
 assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant__ CUtensorMap tmXl,
                  const __grid_constant__ CUtensorMap tmCh, const __grid_constant__ CUtensorMap tmCl, Params p) {
@@ -386,6 +404,9 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
     constexpr int NCTA = PAIR ? 2 : 1;          // CTAs sharing one MMA (a pair: M = 256)
     constexpr uint32_t kIdesc = make_idesc(BN, NCTA * BM);
     static_assert(NACC >= 2 && NACC <= kMaxAcc, "accumulator count");
+    static_assert(NPROD == 1 || NPROD == 3, "products per k-step");
+    constexpr int NSPLIT = NPROD == 3 ? 2 : 1;  // panels per operand: hi (+ lo for the split form)
+    constexpr int BSTAGE = NSPLIT * PANEL_B;    // bytes of one B stage in this CTA
     const uint32_t rank = PAIR ? cluster_rank() : 0u;  // 0: the pair's leader (issues the MMAs)
     // One read of the loop flag for the whole CTA (for a pair: the leader's read,
     // for both CTAs), so every thread of the pair takes the same path.
@@ -405,10 +426,10 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
     if (s_skip) return;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const int a_stage_bytes = 2 * p.kpanels * PANEL;  // hi + lo panels
+    const int a_stage_bytes = NSPLIT * p.kpanels * PANEL;  // hi (+ lo) panels
     uint8_t *A = smem;
     uint8_t *B = A + (size_t)p.a_stages * a_stage_bytes;
-    Barriers *bar = (Barriers *)(B + (size_t)p.b_stages * 2 * PANEL_B);
+    Barriers *bar = (Barriers *)(B + (size_t)p.b_stages * BSTAGE);
     volatile int *abort = &bar->abort;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -493,17 +514,18 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 uint8_t *Ab = A + (size_t)as * a_stage_bytes;
                 for (int kp = 0; kp < p.kpanels; ++kp) {
                     load(Ab + (size_t)kp * PANEL, &tmXh, &bar->a_full[as], kp * KP, tile * BM);
-                    load(Ab + (size_t)(p.kpanels + kp) * PANEL, &tmXl, &bar->a_full[as], kp * KP, tile * BM);
+                    if (NPROD == 3)
+                        load(Ab + (size_t)(p.kpanels + kp) * PANEL, &tmXl, &bar->a_full[as], kp * KP, tile * BM);
                 }
                 a_issued[as]++;
                 for (int j = 0; j < p.ntiles_n && ok; ++j) {
                     for (int kb = 0; kb < p.kpanels * (KP / KPB); ++kb) {
                         if (!mbar_wait(&bar->b_empty[bs], bphase ^ 1, abort)) { ok = false; break; }
-                        if (rank == 0) mbar_expect_tx(&bar->b_full[bs], NCTA * 2 * PANEL_B);
-                        uint8_t *Bb = B + (size_t)bs * 2 * PANEL_B;
+                        if (rank == 0) mbar_expect_tx(&bar->b_full[bs], NCTA * BSTAGE);
+                        uint8_t *Bb = B + (size_t)bs * BSTAGE;
                         const int brow = j * BN + (int)rank * BROWS;
                         load(Bb, &tmCh, &bar->b_full[bs], kb * KPB, brow);
-                        load(Bb + PANEL_B, &tmCl, &bar->b_full[bs], kb * KPB, brow);
+                        if (NPROD == 3) load(Bb + PANEL_B, &tmCl, &bar->b_full[bs], kb * KPB, brow);
                         b_issued[bs]++;
                         if (++bs == p.b_stages) {
                             bs = 0;
@@ -558,15 +580,21 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                         const int kp = kb / (KP / KPB), ka = (kb % (KP / KPB)) * (KPB * 2 / 16);
                         const uint64_t ah = sw128_desc(a_base + kp * PANEL) + ka;
                         const uint64_t al = sw128_desc(a_base + (p.kpanels + kp) * PANEL) + ka;
-                        const uint64_t bh = swb_desc<KPB>(su32(B + (size_t)bs * 2 * PANEL_B));
-                        const uint64_t bl = swb_desc<KPB>(su32(B + (size_t)bs * 2 * PANEL_B + PANEL_B));
+                        const uint64_t bh = swb_desc<KPB>(su32(B + (size_t)bs * BSTAGE));
+                        const uint64_t bl = swb_desc<KPB>(su32(B + (size_t)bs * BSTAGE + PANEL_B));
                         // 16 bf16 = 32 bytes along the swizzled row = 2 in the descriptor's address field
 #pragma unroll
                         for (int ks = 0; ks < KPB / 16; ++ks) {
-                            if (PAIR)
+                            if (NPROD == 1) {
+                                if (PAIR)
+                                    mma_bf16x1_pair(tmem_d, ah + 2 * ks, bh + 2 * ks, kIdesc);
+                                else
+                                    mma_bf16x1(tmem_d, ah + 2 * ks, bh + 2 * ks, kIdesc);
+                            } else if (PAIR) {
                                 mma_bf16x3_pair(tmem_d, ah + 2 * ks, al + 2 * ks, bh + 2 * ks, bl + 2 * ks, kIdesc);
-                            else
+                            } else {
                                 mma_bf16x3(tmem_d, ah + 2 * ks, al + 2 * ks, bh + 2 * ks, bl + 2 * ks, kIdesc);
+                            }
                         }
                         commit(&bar->b_empty[bs]);  // frees the B stage (both CTAs' halves) once these MMAs finish
                         if (++bs == p.b_stages) {
@@ -803,13 +831,18 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
 __global__ void row_bounds_kernel(int64_t n, const float *__restrict__ xnorm, const int32_t *__restrict__ labels,
                                   const float *__restrict__ d2, const double *__restrict__ shift_part,
                                   const double *__restrict__ cnorm_max, const double *__restrict__ cnorm_max_prev,
-                                  int dpad, int k, int prior, float2 *__restrict__ out, const LoopState *st) {
+                                  int dpad, int k, int prior, int products, float2 *__restrict__ out,
+                                  const LoopState *st) {
     if (st && st->done) return;
     const double u = 5.9604644775390625e-8;  // 2^-24
+    const double ub = 3.90625e-3;             // 2^-8
     const double ub2 = 1.52587890625e-5;      // 2^-16
     const double cmax = *cnorm_max;
     const double cmax_prev = prior ? *cnorm_max_prev : 0.0;
-    const double acc = 3.03 * ub2 + 2.0 * 3.0 * dpad * 2.0 * u;
+    // split form: the dropped xl.cl term and the bf16 rounding of the lo parts;
+    // single product: |x.c - bf16(x).bf16(c)| <= (2 u_b + u_b^2) sum |x_t c_t|
+    const double split = products == 3 ? 3.03 * ub2 : 2.0 * ub + ub2;
+    const double acc = split + 2.0 * products * dpad * 2.0 * u;
     for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < n;
          row += (int64_t)gridDim.x * blockDim.x) {
         const float xn = xnorm[row];
@@ -839,6 +872,7 @@ __global__ void row_bounds_kernel(int64_t n, const float *__restrict__ xnorm, co
 __global__ void split_rows_kernel(const float *__restrict__ src, int64_t rows, int d, int dpad,
                                   __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
                                   float *__restrict__ xnorm) {
+    // lo == nullptr: the single-product form reads the hi panels only
     const int lane = threadIdx.x & 31;
     const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
@@ -849,7 +883,7 @@ __global__ void split_rows_kernel(const float *__restrict__ src, int64_t rows, i
             if (t < d) s += (double)v * (double)v;
             const __nv_bfloat16 h = __float2bfloat16_rn(v);
             hi[r * dpad + t] = h;
-            lo[r * dpad + t] = __float2bfloat16_rn(v - __bfloat162float(h));
+            if (lo) lo[r * dpad + t] = __float2bfloat16_rn(v - __bfloat162float(h));
         }
         for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
         if (lane == 0) xnorm[r] = (float)s;
@@ -997,7 +1031,10 @@ static bool use_cta_pairs() {
 int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
                      const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
                      float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, bool prior,
-                     const double *shift_part, const double *cnorm_max_prev, void *rowb, cudaStream_t s) {
+                     const double *shift_part, const double *cnorm_max_prev, void *rowb, int products,
+                     cudaStream_t s) {
+    if (products != 1 && products != 3) return KMB_EINVAL;
+    const int nsplit = products == 3 ? 2 : 1;
     const int64_t dpad = tc_dpad(d), kpad = tc_kpad(k);
     if ((prior && (!shift_part || !cnorm_max_prev)) || !rowb) return KMB_EINVAL;
     if (dpad > 256) return KMB_EUNSUPPORTED;
@@ -1007,21 +1044,26 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const int kpanels = (int)(dpad / tc::KP);
-    const int a_stage = 2 * kpanels * tc::PANEL;
+    const int a_stage = nsplit * kpanels * tc::PANEL;
     const int fixed = 1024 + (int)sizeof(tc::Barriers) + 64;
     const int bn = tc_tile_n(k);  // cluster tile (UMMA N); kpad is a multiple of it
     const bool pair = use_cta_pairs();
     const int panel_b = tc::panel_b_bytes(bn, pair);
-    int a_stages = (2 * a_stage + 3 * 2 * panel_b + fixed <= optin) ? 2 : 1;
-    int b_stages = (optin - fixed - a_stages * a_stage) / (2 * panel_b);
+    int a_stages = (2 * a_stage + 3 * nsplit * panel_b + fixed <= optin) ? 2 : 1;
+    int b_stages = (optin - fixed - a_stages * a_stage) / (nsplit * panel_b);
     b_stages = std::min(b_stages, tc::MAX_B_STAGES);
     if (b_stages < 2) return KMB_EUNSUPPORTED;
     // More than half of an SM's shared memory: one CTA per SM, which the
     // %smid-indexed hand-off slots rely on.
-    const size_t smem = std::max<size_t>((size_t)a_stages * a_stage + (size_t)b_stages * 2 * panel_b + fixed,
+    const size_t smem = std::max<size_t>((size_t)a_stages * a_stage + (size_t)b_stages * nsplit * panel_b + fixed,
                                          (size_t)optin / 2 + 4096);
 
     CUtensorMap mXh, mXl, mCh, mCl;
+    // (the single-product form never loads the lo panels: their maps alias the hi ones)
+    if (products == 1) {
+        Xlo = Xhi;
+        Clo = Chi;
+    }
     if (!encode_map(&mXh, Xhi, n, dpad, false) || !encode_map(&mXl, Xlo, n, dpad, false) ||
         !encode_map(&mCh, Chi, kpad, dpad, true, bn, pair) || !encode_map(&mCl, Clo, kpad, dpad, true, bn, pair))
         return KMB_ECUDA;
@@ -1047,11 +1089,12 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     {
         const int bs = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
         tc::row_bounds_kernel<<<bs, 256, 0, s>>>(n, xnorm, labels, d2, shift_part, cnorm_max, cnorm_max_prev, (int)dpad,
-                                                 (int)k, prior ? 1 : 0, (float2 *)rowb, st);
+                                                 (int)k, prior ? 1 : 0, products, (float2 *)rowb, st);
         KMB_LAUNCHED();
     }
     if (!pair) {
-        auto kern = bn == 256 ? tc::assign_tc_kernel<256, false> : tc::assign_tc_kernel<128, false>;
+        auto kern = products == 1 ? (bn == 256 ? tc::assign_tc_kernel<256, false, 1> : tc::assign_tc_kernel<128, false, 1>)
+                                  : (bn == 256 ? tc::assign_tc_kernel<256, false, 3> : tc::assign_tc_kernel<128, false, 3>);
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
             return KMB_ECUDA;
         // num_sms < 0: one CTA per 128-row tile (no persistence), so that other
@@ -1062,7 +1105,8 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
         return cudaGetLastError() == cudaSuccess ? KMB_OK : KMB_ECUDA;
     }
     // CTA pairs: clusters of two CTAs, one 256-row unit per cluster at a time.
-    auto kern = bn == 256 ? tc::assign_tc_kernel<256, true> : tc::assign_tc_kernel<128, true>;
+    auto kern = products == 1 ? (bn == 256 ? tc::assign_tc_kernel<256, true, 1> : tc::assign_tc_kernel<128, true, 1>)
+                              : (bn == 256 ? tc::assign_tc_kernel<256, true, 3> : tc::assign_tc_kernel<128, true, 3>);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return KMB_ECUDA;
     cudaLaunchConfig_t cfg = {};

@@ -159,8 +159,8 @@ int64_t tc_dpad(int64_t d);   // d rounded up to the 64-wide K panel
 int tc_tile_n(int64_t k);      // cluster tile of the tensor-core kernel: 128 or 256
 int64_t tc_kpad(int64_t k);   // k rounded up to a multiple of tc_tile_n(k)
 bool tc_supported(int64_t d); // dpad <= 256
-// X (rows x d, FP32) -> hi/lo BF16 [rows][dpad], zero padded.
-// x -> BF16 hi/lo panels [rows][dpad] and ||x||^2 (the same value launch_row_norms gives).
+// x -> BF16 hi/lo panels [rows][dpad] (lo may be null: hi only) and ||x||^2 (the
+// same value launch_row_norms gives).
 void launch_split_rows(const float *X, int64_t rows, int64_t d, void *hi, void *lo, float *xnorm, int num_sms,
                        cudaStream_t s);
 // C -> Chi/Clo [kpad][dpad], -h = -0.5||c||^2 (kpad, -inf padding), max ||c||.
@@ -171,10 +171,13 @@ void launch_prep_centroids_tc(const float *C, int64_t k, int64_t d, void *Chi, v
 // prior: labels/d2 hold the previous pass's results under the centroids that
 // the update in between moved by sqrt(shift_part[j]); they seed a lower bound
 // on each row's best score that lets the epilogue skip hopeless clusters.
+// products: 3 = split BF16 (xh.ch + xh.cl + xl.ch), 1 = one BF16 product (xh.ch;
+// Xlo / Clo unused). The recheck band follows the form's error bound.
 int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, const void *Chi, const void *Clo,
                      const float *h, int64_t k, const float *xnorm, const double *cnorm_max, int32_t *labels,
                      float *d2, RecheckEntry *queue, LoopState *st, int num_sms, void *xchg, bool prior,
-                     const double *shift_part, const double *cnorm_max_prev, void *rowb, cudaStream_t s);
+                     const double *shift_part, const double *cnorm_max_prev, void *rowb, int products,
+                     cudaStream_t s);
 size_t tc_xchg_bytes();
 
 // Encodes a 2-D tiled tensor map (inner x outer elements, rows row_bytes apart,
@@ -224,9 +227,13 @@ bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize);
 // when `commit` (the loop path); otherwise they are left in C_new.
 // With `csr`, the rows are CSR (X is unused): piece sums scatter the stored
 // entries and a reseeded cluster takes its candidate row expanded to dense.
+// With exact_d2 (the d2 buffer itself), an iteration with empty clusters first
+// recomputes every row's squared distance in FP64 so the candidates follow the
+// exact distances (the tensor-core forms' d2 is exact only for rechecked rows).
 template <typename F>
 void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *C_old, F *C_new,
-                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr = nullptr);
+                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr = nullptr,
+                   F *exact_d2 = nullptr);
 
 // Just the sums/counts half of the update (sharded training).
 template <typename F>

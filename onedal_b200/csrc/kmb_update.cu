@@ -428,6 +428,29 @@ struct SelState {
     int active;
 };
 
+// Exact squared distances for the empty-cluster candidates: when some cluster is
+// empty, d2 of every row becomes ||x - c_label||^2 summed in FP64 (rounded to F),
+// so the candidate order does not depend on the assignment form's rounding (the
+// tensor-core forms' distances carry their contraction error outside the recheck
+// band). One warp per row; nothing runs when no cluster is empty.
+template <typename F>
+__global__ void refresh_d2_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restrict__ C,
+                                  const int32_t *__restrict__ labels, F *__restrict__ d2, const LoopState *st) {
+    if (is_done(st) || st->n_empty == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += warps) {
+        const F *x = X + r * d, *c = C + (int64_t)labels[r] * d;
+        double acc = 0.0;
+        for (int t = lane; t < d; t += 32) {
+            const double df = (double)x[t] - (double)c[t];
+            acc += df * df;
+        }
+        for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+        if (lane == 0) d2[r] = F(acc);
+    }
+}
+
 __global__ void sel_init_kernel(SelState *ss, unsigned int *hist, const LoopState *st) {
     if (is_done(st) || st->n_empty == 0) return;
     if (threadIdx.x == 0) {
@@ -907,7 +930,7 @@ static void sort_and_sum_pieces(const void *Xv, size_t fsize, const UpdatePlan &
 
 template <typename F>
 void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *C_old, F *C_new,
-                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr) {
+                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr, F *exact_d2) {
     const int k = (int)p.k, d = (int)p.d;
     sort_and_sum_pieces(X, sizeof(F), p, labels, ws, st, s, csr);
     double *shift_part = (double *)ws.shift_part.ptr;
@@ -924,6 +947,12 @@ void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const
     empties_kernel<<<1, 1024, 0, s>>>(empty_flag, k, empty_ids, shift_part, st);
     KMB_LAUNCHED();
     // Reseeding: every kernel below returns at once unless some cluster is empty.
+    if (exact_d2 && !csr) {
+        refresh_d2_kernel<F><<<(unsigned)std::min<int64_t>((p.n * 32 + 255) / 256, 148 * 16), 256, 0, s>>>(
+            X, p.n, d, C_old, labels, exact_d2, st);
+        KMB_LAUNCHED();
+        d2 = exact_d2;
+    }
     SelState *ss = (SelState *)ws.sel_state.ptr;
     unsigned int *hist = (unsigned int *)ws.sel_hist.ptr;
     Cand *cand = (Cand *)ws.cand.ptr;
@@ -1008,7 +1037,7 @@ template void launch_sum_values<double>(const double *, int64_t, double *, doubl
 
 #define KMB_INST(F)                                                                                                 \
     template void launch_update<F>(const F *, const UpdatePlan &, const int32_t *, const F *, F *, F *, Workspace &, \
-                                   LoopState *, bool, cudaStream_t, const CsrRows *);                              \
+                                   LoopState *, bool, cudaStream_t, const CsrRows *, F *);                         \
     template void launch_partial_sums<F>(const F *, const UpdatePlan &, const int32_t *, double *, int64_t *,       \
                                          Workspace &, cudaStream_t);                                               \
     template void launch_objective<F>(const F *, int64_t, int64_t, const F *, const int32_t *, double *, double *, \

@@ -93,18 +93,23 @@ class result_options:
 
 
 class compute_form:
-    """How x.c is contracted on the GPU (the kmb_form of the C ABI). `auto` (the
-    default) takes the BF16x3 tensor-core form with its exact FP64 recheck for float32
+    """How x.c is contracted on the GPU (the kmb_form of the C ABI). `bf16x3` is the
+    split-BF16 tensor-core form (three products per k-step), `bf16` the single-product
+    one; both recheck every row inside their error band in FP64, so their responses
+    are the FP64 oracle's. `auto` (the default) takes a tensor-core form for float32
     data with d <= 256 once n * k * d is large enough, and the plain FMA form otherwise."""
     plain = _native.KMB_FORM_PLAIN
     bf16x3 = _native.KMB_FORM_BF16X3
+    bf16 = _native.KMB_FORM_BF16
     auto = _native.KMB_FORM_AUTO
 
 
 def _default_form():
     v = os.environ.get("ONEDAL_B200_KMEANS_FORM", "auto").lower()
-    if v in ("bf16x3", "bf16", "tc"):
+    if v in ("bf16x3", "tc"):
         return compute_form.bf16x3
+    if v == "bf16":
+        return compute_form.bf16
     return compute_form.plain if v == "plain" else compute_form.auto
 
 
@@ -168,7 +173,7 @@ class descriptor:
 
     # B200-specific knobs (not part of the reference descriptor).
     def set_compute_form(self, form):
-        if form not in (compute_form.plain, compute_form.bf16x3, compute_form.auto):
+        if form not in (compute_form.plain, compute_form.bf16x3, compute_form.bf16, compute_form.auto):
             raise domain_error("unknown compute form")
         self._form = form
         return self
