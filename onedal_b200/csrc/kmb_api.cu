@@ -10,7 +10,10 @@
 // it back every few iterations.
 #include "kmb_internal.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -89,9 +92,19 @@ int64_t &launch_count() {
     return count;
 }
 
+// Host-side fault injection: with KMB_FAIL_ALLOC=1 in the environment every
+// workspace growth reports an allocation failure (without calling the
+// allocator), so a test can check that the failure surfaces as KMB_ENOMEM and,
+// through a dispatcher, as the reference's host_bad_alloc.
+static bool alloc_failure_injected() {
+    const char *e = getenv("KMB_FAIL_ALLOC");
+    return e && e[0] == '1';
+}
+
 bool Workspace::ensure(DevBuf &b, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (b.bytes >= bytes) return true;
+    if (alloc_failure_injected()) return false;
     if (b.ptr) cudaFreeAsync(b.ptr, stream);
     b.ptr = nullptr;
     b.bytes = 0;
@@ -153,6 +166,46 @@ constexpr int64_t kBN = 128;  // cluster tile of the plain kernel
 constexpr int64_t kBK = 8;
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// Profiling, gated like the reference's profiler on ONEDAL_VERBOSE
+// (cpp/daal/src/services/service_profiler.h:141-151): at level >= 1 the hot-path
+// phases are NVTX ranges named after the reference's profiler tasks
+// (kmeans_lloyd_batch_impl.i:122,134,145,190) and every train / infer call logs
+// one line (shape, form, iterations, status, wall time) to stderr. Read once.
+int verbose_level() {
+    static const int level = [] {
+        const char *e = getenv("ONEDAL_VERBOSE");
+        return e ? atoi(e) : 0;
+    }();
+    return level;
+}
+
+struct ProfRange {
+    bool on;
+    explicit ProfRange(const char *name) : on(verbose_level() >= 1) {
+        if (on) nvtxRangePushA(name);
+    }
+    ~ProfRange() {
+        if (on) nvtxRangePop();
+    }
+};
+
+struct CallLog {
+    const char *what;
+    int64_t n, d, k;
+    int form;
+    const int64_t *iterations;
+    const int *rc;
+    std::chrono::steady_clock::time_point t0;
+    CallLog(const char *w, int64_t n_, int64_t d_, int64_t k_, int f, const int64_t *it, const int *rc_)
+        : what(w), n(n_), d(d_), k(k_), form(f), iterations(it), rc(rc_), t0(std::chrono::steady_clock::now()) {}
+    ~CallLog() {
+        if (verbose_level() < 1) return;
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        fprintf(stderr, "onedal_b200: %s n=%lld d=%lld k=%lld form=%d iterations=%lld status=%d wall=%.3f ms\n", what,
+                (long long)n, (long long)d, (long long)k, form, iterations ? (long long)*iterations : 0LL, *rc, ms);
+    }
+};
 
 // Buffers shared by train/infer/step. Returns KMB_OK or KMB_ENOMEM.
 template <typename F>
@@ -242,6 +295,7 @@ int assign_pass_tc<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d
 template <typename F>
 int assign_pass(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C, int64_t k, bool recheck,
                 int32_t *labels, F *d2, LoopState *st, bool tc = false, bool prior = false) {
+    ProfRange range("addNTToTaskThreaded");
     if (tc) return assign_pass_tc<F>(ctx, X, n, d, C, k, labels, d2, st, prior);
     kmb::Workspace &ws = ctx->ws;
     cudaStream_t s = ctx->stream;
@@ -360,6 +414,7 @@ int run_loop(kmb_context *ctx, const F *X, int64_t n, int64_t d, F *C, const kmb
             int rc = assign_pass<F>(ctx, X, n, d, C, k, recheck, labels, d2, st, tc, /*prior=*/enq > 0);
             if (rc) return rc;
             KernelTimer timer(ctx, 2);
+            ProfRange range("kmeansMergeReduceCentroids");
             kmb::launch_update<F>(X, plan, labels, d2, C, Cnew, ws, st, /*commit=*/true, s, nullptr,
                                   tc ? d2 : nullptr);
         }
@@ -442,7 +497,10 @@ int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
                              /*prior=*/p->max_iteration_count > 0)))
         return rc;
     double *obj_dev = &sc->objective;
-    kmb::launch_objective<F>(X, n, d, Ccur, labels, (double *)ws.obj_part.ptr, obj_dev, s);
+    {
+        ProfRange range("kmeansUpdateObjectiveFunction");
+        kmb::launch_objective<F>(X, n, d, Ccur, labels, (double *)ws.obj_part.ptr, obj_dev, s);
+    }
     KMB_CUDA(cudaGetLastError());
 
     const cudaMemcpyKind out_kind = memory == KMB_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
@@ -455,6 +513,8 @@ int train_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     KMB_CUDA(cudaStreamSynchronize(s));
     const LoopState &hs = ctx->h_state[0];
     if (hs.error) return fail(ctx, hs.error, "device loop failed (status %d)", hs.error);
+    if (ctx->h_state[1].error)
+        return fail(ctx, ctx->h_state[1].error, "final assignment pass failed (status %d)", ctx->h_state[1].error);
     if (objective) *objective = obj_h;
     if (iteration_count) *iteration_count = hs.iterations;
     if (stats) {
@@ -503,6 +563,8 @@ int infer_impl(kmb_context *ctx, int memory, const void *Xv, int64_t n, int64_t 
     KMB_CUDA(cudaMemcpyAsync(&obj_h, &sc->objective, sizeof(double), cudaMemcpyDeviceToHost, s));
     KMB_CUDA(cudaMemcpyAsync(&ctx->h_state[1], st, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
     KMB_CUDA(cudaStreamSynchronize(s));
+    if (ctx->h_state[1].error)
+        return fail(ctx, ctx->h_state[1].error, "assignment pass failed (status %d)", ctx->h_state[1].error);
     if (compute_objective && objective) *objective = obj_h;
     if (stats) {
         stats->rechecked_rows = ctx->h_state[1].n_recheck + ctx->h_state[1].n_full;
@@ -574,7 +636,10 @@ int partial_impl(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C,
         kmb::launch_sum_values<F>((const F *)ws.d2.ptr, n, (double *)ws.obj_part.ptr, sq_distances, s);
     if (row_sq) KMB_CUDA(cudaMemcpyAsync(row_sq, ws.d2.ptr, sizeof(F) * n, cudaMemcpyDeviceToDevice, s));
     KMB_CUDA(cudaGetLastError());
+    KMB_CUDA(cudaMemcpyAsync(&ctx->h_state[1], st, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
     KMB_CUDA(cudaStreamSynchronize(s));
+    if (ctx->h_state[1].error)
+        return fail(ctx, ctx->h_state[1].error, "assignment pass failed (status %d)", ctx->h_state[1].error);
     return KMB_OK;
 }
 
@@ -712,6 +777,8 @@ int train_csr_impl(kmb_context *ctx, int memory, const void *vals, const int64_t
     KMB_CUDA(cudaStreamSynchronize(s));
     const LoopState &hs = ctx->h_state[0];
     if (hs.error) return fail(ctx, hs.error, "device loop failed (status %d)", hs.error);
+    if (ctx->h_state[1].error)
+        return fail(ctx, ctx->h_state[1].error, "final assignment pass failed (status %d)", ctx->h_state[1].error);
     if (objective) *objective = obj_h;
     if (iteration_count) *iteration_count = hs.iterations;
     if (stats) {
@@ -966,9 +1033,15 @@ int kmb_train(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n,
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
     kmb_params p = *params;
     p.form = resolve_form(dtype, p.form, n, p.cluster_count, d);
+    int64_t it_local = 0;
+    int64_t *it_out = iteration_count ? iteration_count : &it_local;
+    ProfRange range("kmb_train");
+    CallLog log("train", n, d, p.cluster_count, p.form, it_out, &rc);
     if (dtype == KMB_F32)
-        return train_impl<float>(ctx, memory, X, n, d, C0, &p, C_out, responses, objective, iteration_count, stats);
-    return train_impl<double>(ctx, memory, X, n, d, C0, &p, C_out, responses, objective, iteration_count, stats);
+        rc = train_impl<float>(ctx, memory, X, n, d, C0, &p, C_out, responses, objective, it_out, stats);
+    else
+        rc = train_impl<double>(ctx, memory, X, n, d, C0, &p, C_out, responses, objective, it_out, stats);
+    return rc;
 }
 
 int kmb_train_csr(kmb_context *ctx, int dtype, int memory, const void *values, const int64_t *col_indices,
@@ -1051,9 +1124,13 @@ int kmb_infer(kmb_context *ctx, int dtype, int memory, const void *X, int64_t n,
     if (memory != KMB_MEM_HOST && memory != KMB_MEM_DEVICE) return fail(ctx, KMB_EINVAL, "unknown memory kind");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
     form = resolve_form(dtype, form, n, k, d);
+    ProfRange range("kmb_infer");
+    CallLog log("infer", n, d, k, form, nullptr, &rc);
     if (dtype == KMB_F32)
-        return infer_impl<float>(ctx, memory, X, n, d, C, k, form, compute_objective, responses, objective, stats);
-    return infer_impl<double>(ctx, memory, X, n, d, C, k, form, compute_objective, responses, objective, stats);
+        rc = infer_impl<float>(ctx, memory, X, n, d, C, k, form, compute_objective, responses, objective, stats);
+    else
+        rc = infer_impl<double>(ctx, memory, X, n, d, C, k, form, compute_objective, responses, objective, stats);
+    return rc;
 }
 
 int kmb_lloyd_step(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, const void *C_in, int64_t k,

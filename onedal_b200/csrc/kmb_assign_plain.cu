@@ -385,6 +385,7 @@ constexpr long long kResTimeout = 4000000000ll;  // ~2 s of SM clocks per wait
 struct ResBarriers {
     uint64_t full[2];
     int abort;
+    int issued[2];  // loads issued into each stage (thread 0)
 };
 
 __device__ __forceinline__ uint32_t res_su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -438,8 +439,11 @@ __device__ __forceinline__ void res_exchange(RowTop<float> (&t)[8], int mask, bo
     }
 }
 
+// DPADT > 0 fixes the padded row width at compile time (row and centroid offsets
+// become immediates); 0 reads it from dpad.
+template <int DPADT>
 __global__ void __launch_bounds__(kResThreads, 1)
-assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d, int dpad, const float *__restrict__ Ct,
+assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d, int dpad_rt, const float *__restrict__ Ct,
                        const float *__restrict__ h, int k, int kpad, int kres, const float *__restrict__ xnorm,
                        const double *__restrict__ cnorm_max, int32_t *__restrict__ labels, float *__restrict__ d2,
                        RecheckEntry *__restrict__ queue, LoopState *__restrict__ st) {
@@ -447,11 +451,12 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
     if (threadIdx.x == 0) s_skip = st ? st->done : 0;
     __syncthreads();
     if (s_skip) return;
+    const int dpad = DPADT > 0 ? DPADT : dpad_rt;
     extern __shared__ uint8_t res_smem_raw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)res_smem_raw + 127) & ~(uintptr_t)127);
     const int tile_floats = kResRows * dpad;
     float *Xs = (float *)sm;                   // [2][128][dpad]
-    float *Cs = Xs + 2 * tile_floats;          // [dpad][kres]
+    float *Cs = Xs + 2 * tile_floats;          // [kres / 256][dpad][256]: pass-major blocks
     float *hs = Cs + (size_t)dpad * kres;      // [kres]
     RowTop<float> *run = (RowTop<float> *)(hs + kres);  // [128] running top-3 across passes
     ResBarriers *bar = (ResBarriers *)(run + kResRows);
@@ -464,21 +469,22 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
         for (int i = 0; i < 2; ++i)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(res_su32(&bar->full[i])) : "memory");
         bar->abort = 0;
+        bar->issued[0] = bar->issued[1] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    int issued[2] = {0, 0};  // thread 0: loads issued into each stage
     if (tid == 0 && my_tiles > 0) {
         res_load_tile(Xs, &tmX, &bar->full[0], (int)blockIdx.x * kResRows, tile_bytes);
-        issued[0] = 1;
+        bar->issued[0] = 1;
     }
-    // Resident centroids: C^T (zero columns past kpad) and half norms (+inf past kpad).
-    const int kq = kres / 4, kq_src = kpad / 4;
+    // Resident centroids: C^T in 256-column blocks, one per pass, so a pass reads
+    // rows 256 floats apart (zero columns past kpad), and the half norms (+inf past kpad).
+    const int kq = kres / 4;
     for (int i = tid; i < dpad * kq; i += kResThreads) {
-        const int t = i / kq, c4 = i - t * kq;
+        const int t = i / kq, c = 4 * (i - t * kq);
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (c4 < kq_src) v = *reinterpret_cast<const float4 *>(Ct + (size_t)t * kpad + 4 * c4);
-        *reinterpret_cast<float4 *>(Cs + (size_t)t * kres + 4 * c4) = v;
+        if (c < kpad) v = *reinterpret_cast<const float4 *>(Ct + (size_t)t * kpad + c);
+        *reinterpret_cast<float4 *>(Cs + ((size_t)(c / kResPass) * dpad + t) * kResPass + (c % kResPass)) = v;
     }
     for (int j = tid; j < kres; j += kResThreads) hs[j] = j < kpad ? h[j] : f_inf<float>();
     __syncthreads();
@@ -497,13 +503,13 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
         if (tid == 0 && ok && lt + 1 < my_tiles) {
             res_load_tile(Xs + (buf ^ 1) * tile_floats, &tmX, &bar->full[buf ^ 1],
                           (int)(row0 + (int64_t)gridDim.x * kResRows), tile_bytes);
-            issued[buf ^ 1]++;
+            bar->issued[buf ^ 1] += 1;
         }
         if (ok && !__all_sync(0xffffffffu, res_wait(&bar->full[buf], (lt >> 1) & 1, abort))) ok = false;
         if (ok) {
             const float *xa = Xs + buf * tile_floats + (8 * warp) * dpad;
             for (int pass = 0; pass < n_pass; ++pass) {
-                const float *cb = Cs + pass * kResPass + 4 * lane;
+                const float *cb = Cs + (size_t)pass * dpad * kResPass + 4 * lane;
                 float acc[8][8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i)
@@ -514,10 +520,10 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
                     float2 a[8];
 #pragma unroll
                     for (int i = 0; i < 8; ++i) a[i] = *reinterpret_cast<const float2 *>(xa + i * dpad + t);
-                    const float4 b00 = *reinterpret_cast<const float4 *>(cb + (size_t)t * kres);
-                    const float4 b01 = *reinterpret_cast<const float4 *>(cb + (size_t)t * kres + 128);
-                    const float4 b10 = *reinterpret_cast<const float4 *>(cb + (size_t)(t + 1) * kres);
-                    const float4 b11 = *reinterpret_cast<const float4 *>(cb + (size_t)(t + 1) * kres + 128);
+                    const float4 b00 = *reinterpret_cast<const float4 *>(cb + t * kResPass);
+                    const float4 b01 = *reinterpret_cast<const float4 *>(cb + t * kResPass + 128);
+                    const float4 b10 = *reinterpret_cast<const float4 *>(cb + (t + 1) * kResPass);
+                    const float4 b11 = *reinterpret_cast<const float4 *>(cb + (t + 1) * kResPass + 128);
                     const float bx[8] = {b00.x, b00.y, b00.z, b00.w, b01.x, b01.y, b01.z, b01.w};
                     const float by[8] = {b10.x, b10.y, b10.z, b10.w, b11.x, b11.y, b11.z, b11.w};
 #pragma unroll
@@ -579,9 +585,10 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
             // leave no bulk copy landing in shared memory behind: wait (bounded) for
             // the last load issued into each stage
             for (int b = 0; b < 2; ++b) {
-                if (!issued[b]) continue;
+                const int iss = bar->issued[b];
+                if (!iss) continue;
                 const long long t0 = clock64();
-                while (!res_try_wait(&bar->full[b], (uint32_t)((issued[b] - 1) & 1)) && clock64() - t0 < kResTimeout) {
+                while (!res_try_wait(&bar->full[b], (uint32_t)((iss - 1) & 1)) && clock64() - t0 < kResTimeout) {
                 }
             }
             if (st) {
@@ -658,14 +665,17 @@ bool launch_resident<float>(const float *X, int64_t n, int64_t d, const float *C
     if (!encode_tensor_map_2d(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, X, (uint64_t)d, (uint64_t)n, (uint64_t)d * 4,
                               (uint32_t)dpad, (uint32_t)kResRows, CU_TENSOR_MAP_SWIZZLE_NONE))
         return false;
-    if (cudaFuncSetAttribute(assign_resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess) {
+    auto kern = dpad == 32    ? assign_resident_kernel<32>
+                : dpad == 64  ? assign_resident_kernel<64>
+                : dpad == 128 ? assign_resident_kernel<128>
+                              : assign_resident_kernel<0>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
     const int64_t n_tiles = (n + kResRows - 1) / kResRows;
     const int grid = (int)std::min<int64_t>(n_tiles, sms);
-    assign_resident_kernel<<<grid, kResThreads, smem, s>>>(tm, n, (int)d, dpad, Ct, h, (int)k, (int)kpad, kres, xnorm,
+    kern<<<grid, kResThreads, smem, s>>>(tm, n, (int)d, dpad, Ct, h, (int)k, (int)kpad, kres, xnorm,
                                                            cnorm_max, labels, d2, queue, st);
     KMB_LAUNCHED();
     return true;

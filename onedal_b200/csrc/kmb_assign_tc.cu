@@ -101,6 +101,7 @@ struct Params {
     RecheckEntry *queue;
     LoopState *st;
     Top3x *xchg;  // per SM (one CTA fits an SM): 2 (row-tile parity) x (NGROUPS-1) x 128 rows of top-3
+    long long wait_cycles;  // limit of every pipeline wait (the abort-path drains keep kTimeoutCycles)
 };
 
 struct Barriers {
@@ -134,13 +135,15 @@ __device__ __forceinline__ bool mbar_test(uint64_t *b, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: false on abort (set by any role) or timeout (which sets abort).
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort) {
+// Bounded wait: false on abort (set by any role) or after `limit` cycles (which
+// sets abort).
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort,
+                                          long long limit = kTimeoutCycles) {
     if (mbar_test(b, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_test(b, parity)) {
         if (*abort) return false;
-        if (clock64() - t0 > kTimeoutCycles) {
+        if (clock64() - t0 > limit) {
             *abort = 1;
             return false;
         }
@@ -509,7 +512,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 const int tile = tile_of(lt);
                 const int as = p.a_stages == 2 ? (lt & 1) : 0;
                 const int ause = p.a_stages == 2 ? (lt >> 1) : lt;
-                if (!mbar_wait(&bar->a_empty[as], (ause & 1) ^ 1, abort)) { ok = false; break; }
+                if (!mbar_wait(&bar->a_empty[as], (ause & 1) ^ 1, abort, p.wait_cycles)) { ok = false; break; }
                 if (rank == 0) mbar_expect_tx(&bar->a_full[as], (uint32_t)(NCTA * a_stage_bytes));
                 uint8_t *Ab = A + (size_t)as * a_stage_bytes;
                 for (int kp = 0; kp < p.kpanels; ++kp) {
@@ -520,7 +523,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 a_issued[as]++;
                 for (int j = 0; j < p.ntiles_n && ok; ++j) {
                     for (int kb = 0; kb < p.kpanels * (KP / KPB); ++kb) {
-                        if (!mbar_wait(&bar->b_empty[bs], bphase ^ 1, abort)) { ok = false; break; }
+                        if (!mbar_wait(&bar->b_empty[bs], bphase ^ 1, abort, p.wait_cycles)) { ok = false; break; }
                         if (rank == 0) mbar_expect_tx(&bar->b_full[bs], NCTA * BSTAGE);
                         uint8_t *Bb = B + (size_t)bs * BSTAGE;
                         const int brow = j * BN + (int)rank * BROWS;
@@ -563,18 +566,18 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
             for (int lt = 0; lt < my_tiles && ok; ++lt) {
                 const int as = p.a_stages == 2 ? (lt & 1) : 0;
                 const int ause = p.a_stages == 2 ? (lt >> 1) : lt;
-                if (!mbar_wait(&bar->a_full[as], ause & 1, abort)) { ok = false; break; }
+                if (!mbar_wait(&bar->a_full[as], ause & 1, abort, p.wait_cycles)) { ok = false; break; }
                 tc_fence_after();
                 const uint32_t a_base = su32(A + (size_t)as * a_stage_bytes);
                 for (int j = 0; j < p.ntiles_n && ok; ++j, ++acount) {
                     const int slot = (int)(acount % NACC);
                     const int use = (int)(acount / NACC);
                     // the epilogue has written -h into this accumulator (first use included)
-                    if (!mbar_wait(&bar->acc_empty[slot], use & 1, abort)) { ok = false; break; }
+                    if (!mbar_wait(&bar->acc_empty[slot], use & 1, abort, p.wait_cycles)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t tmem_d = tmem_base + (uint32_t)(slot * BN);
                     for (int kb = 0; kb < p.kpanels * (KP / KPB); ++kb) {
-                        if (!mbar_wait(&bar->b_full[bs], bphase, abort)) { ok = false; break; }
+                        if (!mbar_wait(&bar->b_full[bs], bphase, abort, p.wait_cycles)) { ok = false; break; }
                         tc_fence_after();
                         // A: the 64-wide panel holding this 32-wide slice, advanced to the slice
                         const int kp = kb / (KP / KPB), ka = (kb % (KP / KPB)) * (KPB * 2 / 16);
@@ -673,7 +676,7 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
                 const int slot = (int)(acount % NACC);
                 const int use = (int)(acount / NACC);
                 // every lane waits; the warp proceeds only if all lanes saw completion
-                if (!__all_sync(0xffffffffu, mbar_wait(&bar->acc_full[slot], use & 1, abort))) {
+                if (!__all_sync(0xffffffffu, mbar_wait(&bar->acc_full[slot], use & 1, abort, p.wait_cycles))) {
                     ok = false;
                     continue;
                 }
@@ -1086,6 +1089,14 @@ int launch_assign_tc(const void *Xhi, const void *Xlo, int64_t n, int64_t d, con
     p.queue = queue;
     p.st = st;
     p.xchg = (tc::Top3x *)xchg;
+    // KMB_TC_WAIT_LIMIT_CYCLES shortens the pipeline waits' limit: a test makes them
+    // run out and checks that the launch reports KMB_ETIMEDOUT and leaves the
+    // context usable.
+    p.wait_cycles = tc::kTimeoutCycles;
+    if (const char *e = getenv("KMB_TC_WAIT_LIMIT_CYCLES")) {
+        const long long v = atoll(e);
+        if (v > 0 && v < tc::kTimeoutCycles) p.wait_cycles = v;
+    }
     {
         const int bs = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
         tc::row_bounds_kernel<<<bs, 256, 0, s>>>(n, xnorm, labels, d2, shift_part, cnorm_max, cnorm_max_prev, (int)dpad,

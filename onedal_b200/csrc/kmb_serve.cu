@@ -153,6 +153,16 @@ struct Lane {
     // each request's labels into the caller's buffer.
     int32_t *h_lab = nullptr;
     int64_t h_lab_cap = 0;
+    // Pinned buffers replaced by larger ones: freed when the server is destroyed,
+    // because cudaFreeHost (like cudaFree) waits for the whole device, which here
+    // would stall every stream's work behind the scheduler thread.
+    std::vector<void *> retired_host;
+    // Device arena for a batch's rows, keys and labels, reused batch after batch
+    // and grown (stream-ordered, geometrically) only when a batch needs more: a
+    // stream-ordered allocation per request stalled the scheduler thread for up to
+    // 54 ms when the shared pool had to grow while other threads allocated.
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
     int index = 0;
     cudaEvent_t done_ev = nullptr;  // recorded after the batch's last copy
     bool in_flight = false;         // a launched batch awaits its completion thread
@@ -222,43 +232,66 @@ int launch_batch(Server *srv, Lane *lane) {
     cudaStream_t s = lane->stream;
     const int nreq = (int)lane->batch.size();
     if (nreq > lane->cap) {
-        if (lane->h_desc) cudaFreeHost(lane->h_desc);
-        if (lane->d_desc) cudaFree(lane->d_desc);
-        lane->cap = std::max(nreq, 2 * lane->cap);
-        lane->h_desc = nullptr;
-        lane->d_desc = nullptr;
-        if (cudaMallocHost(&lane->h_desc, sizeof(kmb::serve::ReqDesc) * lane->cap) != cudaSuccess ||
-            cudaMalloc(&lane->d_desc, sizeof(kmb::serve::ReqDesc) * lane->cap) != cudaSuccess) {
+        // grow without any device-wide synchronisation: a new pinned block (the old
+        // one is retired), the device copy in stream order
+        const int cap = std::max(nreq, 2 * lane->cap);
+        void *h = nullptr, *dv = nullptr;
+        if (cudaMallocHost(&h, sizeof(kmb::serve::ReqDesc) * cap) != cudaSuccess ||
+            cudaMallocAsync(&dv, sizeof(kmb::serve::ReqDesc) * cap, s) != cudaSuccess) {
             cudaGetLastError();
-            lane->cap = 0;
+            if (h) lane->retired_host.push_back(h);
             return KMB_ENOMEM;
         }
+        if (lane->h_desc) lane->retired_host.push_back(lane->h_desc);
+        if (lane->d_desc) cudaFreeAsync(lane->d_desc, s);
+        lane->h_desc = (kmb::serve::ReqDesc *)h;
+        lane->d_desc = dv;
+        lane->cap = cap;
     }
     int64_t batch_rows = 0;
     for (Request *r : lane->batch) batch_rows += r->n;
     if (batch_rows > lane->h_lab_cap) {
-        if (lane->h_lab) cudaFreeHost(lane->h_lab);
-        lane->h_lab = nullptr;
-        lane->h_lab_cap = 0;
-        const int64_t cap = std::max<int64_t>(batch_rows, srv->max_batch_rows);
-        if (cudaMallocHost(&lane->h_lab, sizeof(int32_t) * cap) != cudaSuccess) {
+        const int64_t cap = std::max<int64_t>(batch_rows, 2 * lane->h_lab_cap);
+        int32_t *h = nullptr;
+        if (cudaMallocHost(&h, sizeof(int32_t) * cap) != cudaSuccess) {
             cudaGetLastError();
             return KMB_ENOMEM;
         }
+        if (lane->h_lab) lane->retired_host.push_back(lane->h_lab);
+        lane->h_lab = h;
         lane->h_lab_cap = cap;
     }
     const int chunk = kmb::grouped_chunk_clusters();
+    auto a256 = [](size_t b) { return (b + 255) / 256 * 256; };
+    size_t need = 0;
+    for (Request *r : lane->batch)
+        need += a256(sizeof(float) * r->n * r->d) + a256(sizeof(unsigned long long) * r->n) +
+                a256(sizeof(int32_t) * r->n);
+    const auto ta0 = Clock::now();
+    if (need > lane->arena_bytes) {
+        const size_t bytes = std::max(need, 2 * lane->arena_bytes);
+        void *a = nullptr;
+        if (cudaMallocAsync(&a, bytes, s) != cudaSuccess) {
+            cudaGetLastError();
+            return KMB_ENOMEM;
+        }
+        if (lane->arena) cudaFreeAsync(lane->arena, s);  // after the lane's previous batches
+        lane->arena = a;
+        lane->arena_bytes = bytes;
+    }
+    lane->us_alloc += std::chrono::duration<double, std::micro>(Clock::now() - ta0).count();
+    char *cursor = (char *)lane->arena;
     long long items = 0, rows = 0;
     for (int i = 0; i < nreq; ++i) {
         Request *r = lane->batch[i];
         const Model &m = srv->models[r->model];
         const auto ta = Clock::now();
-        if (cudaMallocAsync((void **)&r->dX, sizeof(float) * r->n * r->d, s) != cudaSuccess ||
-            cudaMallocAsync((void **)&r->dkey, sizeof(unsigned long long) * r->n, s) != cudaSuccess ||
-            cudaMallocAsync((void **)&r->dlab, sizeof(int32_t) * r->n, s) != cudaSuccess) {
-            cudaGetLastError();
-            return KMB_ENOMEM;
-        }
+        r->dX = (float *)cursor;
+        cursor += a256(sizeof(float) * r->n * r->d);
+        r->dkey = (unsigned long long *)cursor;
+        cursor += a256(sizeof(unsigned long long) * r->n);
+        r->dlab = (int32_t *)cursor;
+        cursor += a256(sizeof(int32_t) * r->n);
         const auto tb = Clock::now();
         cudaMemcpyAsync(r->dX, r->X, sizeof(float) * r->n * r->d, cudaMemcpyHostToDevice, s);
         const auto tc = Clock::now();
@@ -290,9 +323,6 @@ int launch_batch(Server *srv, Lane *lane) {
         const auto t0 = Clock::now();
         cudaMemcpyAsync(lane->h_lab + r->lab_off, r->dlab, sizeof(int32_t) * r->n, cudaMemcpyDeviceToHost, s);
         const auto t1 = Clock::now();
-        cudaFreeAsync(r->dX, s);
-        cudaFreeAsync(r->dkey, s);
-        cudaFreeAsync(r->dlab, s);
         lane->us_d2h += std::chrono::duration<double, std::micro>(t1 - t0).count();
         lane->us_free += std::chrono::duration<double, std::micro>(Clock::now() - t1).count();
     }
@@ -354,12 +384,7 @@ void scheduler_loop(Server *srv) {
         lane->t_launched = Clock::now();
         if (rc != KMB_OK) {
             // Release what was allocated and complete the batch as failed, in stream order.
-            for (Request *r : lane->batch) {
-                r->rc = rc;
-                if (r->dX) cudaFreeAsync(r->dX, lane->stream);
-                if (r->dkey) cudaFreeAsync(r->dkey, lane->stream);
-                if (r->dlab) cudaFreeAsync(r->dlab, lane->stream);
-            }
+            for (Request *r : lane->batch) r->rc = rc;  // (rows live in the lane's arena)
             cudaEventRecord(lane->done_ev, lane->stream);
         }
         lock.lock();
@@ -383,16 +408,25 @@ cudaError_t copy_in_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyK
 
 // Large infer request on the tensor-core worker: rows uploaded once, then
 // kmb_infer (BF16x3, FP64 recheck) over row chunks on the worker's stream.
-int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r, int64_t chunk_rows) {
-    float *dX = nullptr;
-    int32_t *dlab = nullptr;
-    if (cudaMallocAsync((void **)&dX, sizeof(float) * r->n * r->d, s) != cudaSuccess ||
-        cudaMallocAsync((void **)&dlab, sizeof(int32_t) * r->n, s) != cudaSuccess) {
-        cudaGetLastError();
-        if (dX) cudaFreeAsync(dX, s);
-        cudaStreamSynchronize(s);
-        return KMB_ENOMEM;
+// The request's rows and labels live in the worker's arena, grown (stream-ordered,
+// geometrically) only when a request needs more.
+int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r, int64_t chunk_rows, void *&arena,
+                   size_t &arena_bytes) {
+    const size_t xbytes = (sizeof(float) * r->n * r->d + 255) / 256 * 256;
+    const size_t need = xbytes + sizeof(int32_t) * r->n;
+    if (need > arena_bytes) {
+        void *a = nullptr;
+        const size_t bytes = std::max(need, 2 * arena_bytes);
+        if (cudaMallocAsync(&a, bytes, s) != cudaSuccess) {
+            cudaGetLastError();
+            return KMB_ENOMEM;
+        }
+        if (arena) cudaFreeAsync(arena, s);
+        arena = a;
+        arena_bytes = bytes;
     }
+    float *dX = (float *)arena;
+    int32_t *dlab = (int32_t *)((char *)arena + xbytes);
     int rc = KMB_OK;
     const auto t0 = Clock::now();
     if (copy_in_pieces(dX, r->X, sizeof(float) * r->n * r->d, cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -423,8 +457,6 @@ int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r,
         kmb_context_kernel_time(ctx, 4, &r->ms_recheck, &nl);
         kmb_context_set_kernel_timing(ctx, 0);
     }
-    cudaFreeAsync(dX, s);
-    cudaFreeAsync(dlab, s);
     if (cudaStreamSynchronize(s) != cudaSuccess && rc == KMB_OK) rc = KMB_ECUDA;
     return rc;
 }
@@ -434,6 +466,8 @@ void tc_worker_loop(Server *srv) {
     kmb_context *ctx = nullptr;
     cudaStream_t ts = nullptr;
     if (kmb_context_create(srv->device, &ctx) != KMB_OK) ctx = nullptr;
+    void *arena = nullptr;
+    size_t arena_bytes = 0;
     // Same priority as the lanes: a lower one let a stream of small launches
     // starve the persistent CTAs (which need whole SMs) for tens of ms.
     if (ctx && cudaStreamCreateWithPriority(&ts, cudaStreamNonBlocking, srv->prio_high) == cudaSuccess) {
@@ -460,7 +494,7 @@ void tc_worker_loop(Server *srv) {
         srv->tc_busy += 1;
         const Model m = srv->models[r->model];
         lock.unlock();
-        const int rc = ctx ? run_tc_request(ctx, ts, m, r, srv->tc_chunk_rows) : KMB_ECUDA;
+        const int rc = ctx ? run_tc_request(ctx, ts, m, r, srv->tc_chunk_rows, arena, arena_bytes) : KMB_ECUDA;
         lock.lock();
         r->rc = rc;
         r->t_done = Clock::now();
@@ -473,6 +507,10 @@ void tc_worker_loop(Server *srv) {
         srv->cv.notify_all();
     }
     lock.unlock();
+    if (arena) {
+        cudaFreeAsync(arena, ts);
+        cudaStreamSynchronize(ts);
+    }
     if (ctx) kmb_context_destroy(ctx);
     if (ts) cudaStreamDestroy(ts);
 }
@@ -595,7 +633,7 @@ int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32
         l->index = i;
         // descriptor and label staging sized up front: growing them later
         // (cudaFree / cudaFreeHost) would synchronise the device mid-stream
-        l->cap = 256;
+        l->cap = 2048;
         l->h_lab_cap = srv->max_batch_rows;
         if (cudaMallocHost(&l->h_desc, sizeof(kmb::serve::ReqDesc) * l->cap) != cudaSuccess ||
             cudaMalloc(&l->d_desc, sizeof(kmb::serve::ReqDesc) * l->cap) != cudaSuccess ||
@@ -652,8 +690,10 @@ int kmb_server_destroy(void *handle) {
         cudaStreamDestroy(l->stream);
         if (l->h_desc) cudaFreeHost(l->h_desc);
         if (l->h_lab) cudaFreeHost(l->h_lab);
+        for (void *h : l->retired_host) cudaFreeHost(h);
         if (l->done_ev) cudaEventDestroy(l->done_ev);
         if (l->d_desc) cudaFree(l->d_desc);
+        if (l->arena) cudaFree(l->arena);
         delete l;
     }
     for (Model &m : srv->models) {
