@@ -476,7 +476,7 @@ def run_serving(args, device=0):
                 "train_p50_ms": float(np.percentile([lat[i] for i, r in enumerate(reqs) if r[0] == "train"] or [0],
                                                     50) * 1e3)}
 
-    with KMeansServer(device=device, hbm_budget_bytes=60 << 30, lanes=4, trainers=6) as srv:
+    with KMeansServer(device=device, hbm_budget_bytes=60 << 30, lanes=args.serving_lanes, trainers=6) as srv:
         ids = [srv.add_model(C) for C in models]
         run_point(srv, ids, make_requests(200, 1), None)  # warm-up
         sat = run_point(srv, ids, make_requests(args.serving_requests, 2), None)
@@ -489,7 +489,7 @@ def run_serving(args, device=0):
             points.append(pt)
         st = srv.stats()
     return {"saturation_rps": sat["throughput_rps"], "saturation_p99_ms": sat["p99_ms"], "points": points,
-            "models": n_models, "budget_bytes": 60 << 30, "lanes": 4, "trainers": 6,
+            "models": n_models, "budget_bytes": 60 << 30, "lanes": args.serving_lanes, "trainers": 6,
             "mean_requests_per_batch": st["batched_requests"] / max(st["batches"], 1),
             "peak_in_use_bytes": st["peak_in_use_bytes"],
             "note": "p50/p99 = host submit->completion of infer requests; rows from a pinned pool"}
@@ -817,6 +817,7 @@ def main():
                     help="problems in the batched-form measurement (0 skips it)")
     ap.add_argument("--serving-requests", type=int, default=30000,
                     help="requests per serving load point (0 skips the serving measurement)")
+    ap.add_argument("--serving-lanes", type=int, default=4, help="lanes (streams) of the serving engine")
     ap.add_argument("--csr-rows", type=int, default=2_000_000,
                     help="rows of the CSR (lloyd_csr) measurement (0 skips it)")
     ap.add_argument("--plusplus-k", type=int, default=1024,

@@ -125,7 +125,7 @@ void Workspace::release() {
                      &empty_ids,
                      &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx, &rowb, &pp_acc, &pp_rand,
                      &pp_state, &pp_flags, &csr_vals, &csr_cols64, &csr_rowptr64, &csr_cols, &csr_rowptr,
-                     &csr_bad, &csr_cnorm};
+                     &csr_bad, &csr_cnorm, &ex_acc, &ex_cnt, &ex_prev, &ex_colexp};
     for (DevBuf *b : all) {
         if (b->ptr) cudaFreeAsync(b->ptr, stream);
         b->ptr = nullptr;
@@ -386,6 +386,29 @@ void init_state(LoopState &h, double eps) {
     h.eps = eps;
 }
 
+// The update of one Lloyd iteration: float rows take the exact update (integer
+// cluster sums, moved rows only once few rows move), double rows the FP64 one.
+template <typename F>
+int prepare_update(kmb_context *ctx, const F *X, int64_t n, int64_t d, int64_t k, LoopState *st) {
+    return KMB_OK;
+}
+template <>
+int prepare_update<float>(kmb_context *ctx, const float *X, int64_t n, int64_t d, int64_t k, LoopState *st) {
+    if (!kmb::ensure_exact_buffers(ctx->ws, n, k, d)) return fail(ctx, KMB_ENOMEM, "exact update buffers");
+    kmb::prepare_exact_update(X, n, d, ctx->ws, st, ctx->stream);
+    return KMB_OK;
+}
+template <typename F>
+void update_pass(const F *X, const kmb::UpdatePlan &plan, int32_t *labels, F *d2, F *C_old, F *C_new,
+                 kmb::Workspace &ws, LoopState *st, bool commit, cudaStream_t s, bool tc) {
+    kmb::launch_update<F>(X, plan, labels, d2, C_old, C_new, ws, st, commit, s, nullptr, tc ? d2 : nullptr);
+}
+template <>
+void update_pass<float>(const float *X, const kmb::UpdatePlan &plan, int32_t *labels, float *d2, float *C_old,
+                        float *C_new, kmb::Workspace &ws, LoopState *st, bool commit, cudaStream_t s, bool tc) {
+    kmb::launch_update_exact(X, plan, labels, d2, C_old, C_new, ws, st, commit, s, tc ? d2 : nullptr);
+}
+
 // The Lloyd loop on device-resident X and centroids C (updated in place).
 // The host peeks at the device convergence flag every few iterations.
 template <typename F>
@@ -404,6 +427,7 @@ int run_loop(kmb_context *ctx, const F *X, int64_t n, int64_t d, F *C, const kmb
     const bool tc = is_tc_form(p->form);
     ctx->tc_products = form_products(p->form);
     prepare_rows<F>(ctx, X, n, d, tc);
+    if (int rc = prepare_update<F>(ctx, X, n, d, k, st)) return rc;
     const int64_t T = p->max_iteration_count;
     int64_t enq = 0;
     int64_t batch = 2;
@@ -415,8 +439,7 @@ int run_loop(kmb_context *ctx, const F *X, int64_t n, int64_t d, F *C, const kmb
             if (rc) return rc;
             KernelTimer timer(ctx, 2);
             ProfRange range("kmeansMergeReduceCentroids");
-            kmb::launch_update<F>(X, plan, labels, d2, C, Cnew, ws, st, /*commit=*/true, s, nullptr,
-                                  tc ? d2 : nullptr);
+            update_pass<F>(X, plan, labels, d2, C, Cnew, ws, st, /*commit=*/true, s, tc);
         }
         KMB_CUDA(cudaGetLastError());
         if (enq < T) {
@@ -598,9 +621,9 @@ int step_impl(kmb_context *ctx, const void *Xv, int64_t n, int64_t d, const void
     KMB_CUDA(cudaMemcpyAsync(Ccur, Cin, sizeof(F) * k * d, cudaMemcpyDeviceToDevice, s));
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
     prepare_rows<F>(ctx, X, n, d, tc);
+    if ((rc = prepare_update<F>(ctx, X, n, d, k, st))) return rc;
     if ((rc = assign_pass<F>(ctx, X, n, d, Ccur, k, recheck, labels, (F *)ws.d2.ptr, st, tc))) return rc;
-    kmb::launch_update<F>(X, plan, labels, (const F *)ws.d2.ptr, Ccur, (F *)C_out, ws, st, /*commit=*/false, s,
-                          nullptr, tc ? (F *)ws.d2.ptr : nullptr);
+    update_pass<F>(X, plan, labels, (F *)ws.d2.ptr, Ccur, (F *)C_out, ws, st, /*commit=*/false, s, tc);
     KMB_CUDA(cudaGetLastError());
     KMB_CUDA(cudaMemcpyAsync(ctx->h_state, st, sizeof(LoopState), cudaMemcpyDeviceToHost, s));
     KMB_CUDA(cudaStreamSynchronize(s));

@@ -34,6 +34,11 @@ struct LoopState {
     int n_full;           // queued rows that needed the full k rescan (this pass)
     int pad_;
     long long full_total;
+    // Exact update (FP32 rows): the integer cluster sums are a function of the
+    // labels, so a pass that moved few rows updates them by those rows only.
+    int upd_mode;         // 0: recompute from all rows (counting sort), 1: apply the moved rows
+    int upd_valid;        // sums, counts and previous labels describe the previous pass
+    long long n_moved;    // rows whose label changed in this pass
 };
 
 // Recheck queue entry written by the assignment kernels for near-tie rows.
@@ -116,6 +121,7 @@ struct Workspace {
     DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;
     DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb, pp_acc, pp_rand, pp_state, pp_flags;
     DevBuf csr_vals, csr_cols64, csr_rowptr64, csr_cols, csr_rowptr, csr_bad, csr_cnorm;
+    DevBuf ex_acc, ex_cnt, ex_prev, ex_colexp;  // exact update: limb sums, counts, previous labels, scales
     // Grows `b` to at least `bytes`; returns false on allocation failure.
     bool ensure(DevBuf &b, size_t bytes);
     void release();
@@ -234,6 +240,21 @@ template <typename F>
 void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *C_old, F *C_new,
                    Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr = nullptr,
                    F *exact_d2 = nullptr);
+
+// The exact update of FP32 rows (the Lloyd loop's update for float data). Every
+// value x of column t is taken as the integer round(x * 2^E_t), E_t chosen once
+// per call so that the column's largest |x| stays below 2^39; a cluster's sum is
+// then an exact integer (two 64-bit limbs), independent of the order in which
+// rows are added, and the centroid is that integer scaled back, divided by the
+// count in FP64 and rounded to float. Because the sums are a function of the
+// labels alone, a pass that moved at most n/16 rows is applied as those rows'
+// moves (subtract from the old cluster, add to the new one, exact) instead of a
+// full counting-sort pass over X; the result is bit for bit the same.
+// prepare_exact_update: once per call (the scales; the next update recomputes).
+void prepare_exact_update(const float *X, int64_t n, int64_t d, Workspace &ws, LoopState *st, cudaStream_t s);
+bool ensure_exact_buffers(Workspace &ws, int64_t n, int64_t k, int64_t d);
+void launch_update_exact(const float *X, const UpdatePlan &p, int32_t *labels, const float *d2, float *C_old,
+                         float *C_new, Workspace &ws, LoopState *st, bool commit, cudaStream_t s, float *exact_d2);
 
 // Just the sums/counts half of the update (sharded training).
 template <typename F>

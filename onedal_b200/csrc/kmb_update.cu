@@ -30,12 +30,14 @@ constexpr int64_t kGroupChunks = 64; // chunks per scan group
 constexpr int64_t kPieceRows = 512;  // rows per FP64 partial sum
 
 __device__ __forceinline__ bool is_done(const LoopState *st) { return st && st->done; }
+// The counting sort is skipped when the exact update applies the moved rows only.
+__device__ __forceinline__ bool sort_skipped(const LoopState *st) { return st && (st->done || st->upd_mode == 1); }
 
 // ---- counting sort ---------------------------------------------------------
 
 __global__ void hist_smem_kernel(const int32_t *__restrict__ labels, int64_t n, int k, int64_t R,
                                  int32_t *__restrict__ H, const LoopState *st) {
-    if (is_done(st)) return;
+    if (sort_skipped(st)) return;
     extern __shared__ int sh[];
     for (int j = threadIdx.x; j < k; j += blockDim.x) sh[j] = 0;
     __syncthreads();
@@ -48,14 +50,14 @@ __global__ void hist_smem_kernel(const int32_t *__restrict__ labels, int64_t n, 
 }
 
 __global__ void zero_i32_kernel(int32_t *__restrict__ p, int64_t count, const LoopState *st) {
-    if (is_done(st)) return;
+    if (sort_skipped(st)) return;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
         p[i] = 0;
 }
 
 __global__ void hist_global_kernel(const int32_t *__restrict__ labels, int64_t n, int k, int64_t R,
                                    int32_t *__restrict__ H, const LoopState *st) {
-    if (is_done(st)) return;
+    if (sort_skipped(st)) return;
     const int64_t c = blockIdx.x;
     const int64_t b = c * R, e = min(n, b + R);
     int32_t *Hc = H + c * (int64_t)k;
@@ -65,7 +67,7 @@ __global__ void hist_global_kernel(const int32_t *__restrict__ labels, int64_t n
 // Gs[g][j] = sum of H[c][j] over the chunks c of group g.
 __global__ void scan_group_sum_kernel(const int32_t *__restrict__ H, int64_t n_chunks, int k,
                                       int64_t *__restrict__ Gs, const LoopState *st) {
-    if (is_done(st)) return;
+    if (sort_skipped(st)) return;
     const int j = blockIdx.y * blockDim.x + threadIdx.x;
     if (j >= k) return;
     const int64_t g = blockIdx.x;
@@ -79,7 +81,7 @@ __global__ void scan_group_sum_kernel(const int32_t *__restrict__ H, int64_t n_c
 // Exclusive scan of Gs over groups, per label; counts[j] = total rows of label j.
 __global__ void scan_groups_kernel(int64_t *__restrict__ Gs, int64_t n_groups, int k, int64_t *__restrict__ counts,
                                    const LoopState *st) {
-    if (is_done(st)) return;
+    if (sort_skipped(st)) return;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= k) return;
     int64_t run = 0;
@@ -95,7 +97,7 @@ __global__ void scan_groups_kernel(int64_t *__restrict__ Gs, int64_t n_groups, i
 // piece_base = exclusive scan of ceil(counts / piece_rows) (k+1 entries).
 __global__ void offsets_kernel(const int64_t *__restrict__ counts, int k, int64_t piece_rows,
                                int64_t *__restrict__ offsets, int64_t *__restrict__ piece_base, const LoopState *st) {
-    if (is_done(st)) return;
+    if (sort_skipped(st)) return;
     __shared__ int64_t s_rows[1024], s_pcs[1024];
     const int T = blockDim.x;
     const int per = (k + T - 1) / T;
@@ -136,7 +138,7 @@ __global__ void offsets_kernel(const int64_t *__restrict__ counts, int k, int64_
 // H[c][j] <- first output position of chunk c's rows with label j.
 __global__ void scan_chunks_kernel(int32_t *__restrict__ H, int64_t n_chunks, int k, const int64_t *__restrict__ Gs,
                                    const int64_t *__restrict__ offsets, const LoopState *st) {
-    if (is_done(st)) return;
+    if (sort_skipped(st)) return;
     const int j = blockIdx.y * blockDim.x + threadIdx.x;
     if (j >= k) return;
     const int64_t g = blockIdx.x;
@@ -154,7 +156,7 @@ __global__ void scan_chunks_kernel(int32_t *__restrict__ H, int64_t n_chunks, in
 template <bool SMEM>
 __global__ void scatter_kernel(const int32_t *__restrict__ labels, int64_t n, int k, int64_t R,
                                int32_t *__restrict__ H, int32_t *__restrict__ perm, const LoopState *st) {
-    if (is_done(st)) return;
+    if (sort_skipped(st)) return;
     extern __shared__ int sh[];
     const int lane = threadIdx.x;
     const int64_t c = blockIdx.x;
@@ -826,6 +828,248 @@ __global__ void list_empties_kernel(const int32_t *__restrict__ empty_flag, int 
     if (threadIdx.x == 0) *n_empty = s_cnt[T - 1];
 }
 
+// ---- exact update (FP32 rows) -------------------------------------------------
+// Limb form of a cluster-column sum S = A * 2^32 + B (A, B int64; B is brought
+// back to [0, 2^32) by the finalize, so it never overflows between passes).
+
+constexpr int kExactMaxBits = 39;  // |round(x * 2^E_t)| < 2^39: 512-row pieces stay exact in int64
+
+__device__ __forceinline__ long long fixed_of(float x, int e) {
+    return __float2ll_rn(scalbnf(x, e));
+}
+
+// colexp[t] <- max |x| of column t, as float bits (non-negative floats order as ints).
+__global__ void colmax_kernel(const float *__restrict__ X, int64_t n, int d, unsigned *__restrict__ colbits,
+                              const LoopState *st) {
+    if (is_done(st)) return;
+    extern __shared__ unsigned smax[];
+    for (int t = threadIdx.x; t < d; t += blockDim.x) smax[t] = 0u;
+    __syncthreads();
+    const int64_t total = n * (int64_t)d;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const float v = fabsf(X[i]);
+        if (v > 0.0f) atomicMax(&smax[(int)(i % d)], __float_as_uint(v));
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < d; t += blockDim.x)
+        if (smax[t]) atomicMax(&colbits[t], smax[t]);
+}
+
+__global__ void colmax_global_kernel(const float *__restrict__ X, int64_t n, int d, unsigned *__restrict__ colbits,
+                                     const LoopState *st) {
+    if (is_done(st)) return;
+    const int64_t total = n * (int64_t)d;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const float v = fabsf(X[i]);
+        if (v > 0.0f) atomicMax(&colbits[(int)(i % d)], __float_as_uint(v));
+    }
+}
+
+// E_t such that max |x_t| * 2^E_t < 2^39 (E_t = 0 for an all-zero column); the
+// non-finite maximum of a column holding inf/NaN gives E_t = 0 too.
+__global__ void colexp_kernel(int *__restrict__ colexp, int d, const LoopState *st) {
+    if (is_done(st)) return;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < d; t += gridDim.x * blockDim.x) {
+        const unsigned b = (unsigned)colexp[t];
+        const float m = __uint_as_float(b);
+        int e = 0;
+        if (b != 0u && isfinite(m)) {
+            int ex;
+            frexpf(m, &ex);  // m < 2^ex
+            e = kExactMaxBits - ex;
+        }
+        colexp[t] = e;
+    }
+}
+
+// Rows whose label changed since the previous pass (block sums added atomically:
+// an integer, so the order does not matter); then the update mode.
+__global__ void count_moved_kernel(const int32_t *__restrict__ labels, const int32_t *__restrict__ prev, int64_t n,
+                                   LoopState *st) {
+    if (is_done(st) || !st->upd_valid) return;
+    __shared__ int s_cnt;
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    int c = 0;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        c += labels[r] != prev[r];
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(&s_cnt, c);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_cnt)
+        atomicAdd(reinterpret_cast<unsigned long long *>(&st->n_moved), (unsigned long long)s_cnt);
+}
+
+__global__ void choose_mode_kernel(int64_t n, LoopState *st) {
+    if (is_done(st)) return;
+    st->upd_mode = (st->upd_valid && st->n_moved * 16 <= n) ? 1 : 0;
+}
+
+// Block p sums piece p's rows (one cluster's rows in row order) as integers.
+__global__ void __launch_bounds__(128)
+segsum_fixed_kernel(const float *__restrict__ X, int d, int k, const int32_t *__restrict__ perm,
+                    const int64_t *__restrict__ offsets, const int64_t *__restrict__ piece_base, int64_t piece_rows,
+                    const int *__restrict__ colexp, long long *__restrict__ records, const LoopState *st) {
+    if (sort_skipped(st)) return;
+    constexpr int NT = 128;
+    __shared__ int32_t rows[kPieceRows];
+    __shared__ long long part[NT];
+    const int64_t p = blockIdx.x;
+    if (p >= piece_base[k]) return;
+    int lo = 0, hi = k;  // invariant: piece_base[lo] <= p < piece_base[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (piece_base[mid] <= p) lo = mid; else hi = mid;
+    }
+    const int j = lo;
+    const int64_t q = p - piece_base[j];
+    const int64_t s = offsets[j] + q * piece_rows;
+    const int64_t e = min(s + piece_rows, offsets[j + 1]);
+    const int cnt = (int)(e - s);
+    for (int i = threadIdx.x; i < cnt; i += NT) rows[i] = perm[s + i];
+    __syncthreads();
+    int dl, rp;
+    row_layout(d, NT, dl, rp);
+    const int t = threadIdx.x % dl, rr = threadIdx.x / dl;
+    for (int t0 = 0; t0 < d; t0 += dl) {
+        const int col = t0 + t;
+        long long acc = 0;
+        if (col < d) {
+            const int ex = colexp[col];
+            int i = rr;
+            for (; i + 3 * rp < cnt; i += 4 * rp) {
+                const float v0 = X[(int64_t)rows[i] * d + col];
+                const float v1 = X[(int64_t)rows[i + rp] * d + col];
+                const float v2 = X[(int64_t)rows[i + 2 * rp] * d + col];
+                const float v3 = X[(int64_t)rows[i + 3 * rp] * d + col];
+                acc += fixed_of(v0, ex) + fixed_of(v1, ex) + fixed_of(v2, ex) + fixed_of(v3, ex);
+            }
+            for (; i < cnt; i += rp) acc += fixed_of(X[(int64_t)rows[i] * d + col], ex);
+        }
+        part[threadIdx.x] = acc;
+        __syncthreads();
+        if (rr == 0 && col < d) {
+            long long tot = part[t];
+            for (int r2 = 1; r2 < rp; ++r2) tot += part[r2 * dl + t];
+            records[p * d + col] = tot;
+        }
+        __syncthreads();
+    }
+}
+
+// Moved rows (incremental mode): each leaves its old cluster's sums and joins the
+// new one's (integer atomics, exact in any order); prev follows the labels.
+__global__ void apply_moves_kernel(const float *__restrict__ X, int64_t n, int d, const int32_t *__restrict__ labels,
+                                   int32_t *__restrict__ prev, const int *__restrict__ colexp,
+                                   unsigned long long *__restrict__ accA, unsigned long long *__restrict__ accB,
+                                   unsigned long long *__restrict__ cnt, const LoopState *st) {
+    if (is_done(st) || st->upd_mode != 1) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~(int64_t)31; base < n; base += stride) {
+        const int64_t r = base + lane;
+        int lab = -1, old = -1;
+        if (r < n) {
+            lab = labels[r];
+            old = prev[r];
+        }
+        unsigned moved = __ballot_sync(0xffffffffu, r < n && lab != old);
+        while (moved) {
+            const int src = __ffs(moved) - 1;
+            moved &= moved - 1;
+            const int64_t row = base + src;
+            const int nl = __shfl_sync(0xffffffffu, lab, src), ol = __shfl_sync(0xffffffffu, old, src);
+            const float *x = X + row * d;
+            for (int t = lane; t < d; t += 32) {
+                const long long v = fixed_of(x[t], colexp[t]);
+                const unsigned long long a = (unsigned long long)(v >> 32), b = (unsigned long long)(v & 0xffffffffll);
+                atomicAdd(&accA[(int64_t)nl * d + t], a);
+                atomicAdd(&accB[(int64_t)nl * d + t], b);
+                atomicAdd(&accA[(int64_t)ol * d + t], (unsigned long long)(-(long long)a));
+                atomicAdd(&accB[(int64_t)ol * d + t], (unsigned long long)(-(long long)b));
+            }
+            if (lane == 0) {
+                atomicAdd(&cnt[nl], 1ull);
+                atomicAdd(&cnt[ol], (unsigned long long)-1ll);
+            }
+        }
+        if (r < n && lab != old) prev[r] = lab;
+    }
+}
+
+// Full mode: prev <- labels.
+__global__ void copy_prev_kernel(const int32_t *__restrict__ labels, int32_t *__restrict__ prev, int64_t n,
+                                 const LoopState *st) {
+    if (is_done(st) || st->upd_mode == 1) return;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        prev[r] = labels[r];
+}
+
+// Block (j, tile): cluster j's limb sums (full mode: from its pieces; incremental:
+// the maintained ones), normalised and kept; c = F(S * 2^-E / count) in FP64; the
+// tile's shift part and the empty flag, as finalize_kernel.
+__global__ void __launch_bounds__(kFinalizeCols)
+finalize_exact_kernel(const long long *__restrict__ records, const int64_t *__restrict__ counts_sort,
+                      const int64_t *__restrict__ piece_base, const int *__restrict__ colexp,
+                      long long *__restrict__ accA, long long *__restrict__ accB, long long *__restrict__ cnt,
+                      const float *__restrict__ C_old, float *__restrict__ C_new, int d,
+                      double *__restrict__ shift_tiles, int32_t *__restrict__ empty_flag, const LoopState *st) {
+    if (is_done(st)) return;
+    __shared__ double red[kFinalizeCols / 32];
+    const int j = blockIdx.x;
+    const int t = blockIdx.y * kFinalizeCols + threadIdx.x;
+    const bool full = st->upd_mode == 0;
+    const long long c_j = full ? (long long)counts_sort[j] : cnt[j];
+    double acc = 0.0;
+    if (t < d) {
+        long long A = 0, B = 0;
+        const int64_t idx = (int64_t)j * d + t;
+        if (full) {
+            for (int64_t p = piece_base[j]; p < piece_base[j + 1]; ++p) {
+                const long long v = records[p * d + t];
+                A += v >> 32;
+                B += v & 0xffffffffll;
+            }
+        } else {
+            A = accA[idx];
+            B = accB[idx];
+        }
+        A += B >> 32;  // normalise: 0 <= B < 2^32
+        B &= 0xffffffffll;
+        accA[idx] = A;
+        accB[idx] = B;
+        const float old = C_old[idx];
+        if (c_j > 0) {
+            const double S = (double)A * 4294967296.0 + (double)B;
+            const float c = (float)(ldexp(S, -colexp[t]) / (double)c_j);
+            const double df = (double)old - (double)c;
+            acc = df * df;
+            C_new[idx] = c;
+        } else {
+            C_new[idx] = old;
+        }
+    }
+    for (int m = 16; m >= 1; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < kFinalizeCols / 32; ++w) tot += red[w];
+        shift_tiles[(int64_t)j * gridDim.y + blockIdx.y] = tot;
+        if (blockIdx.y == 0) {
+            empty_flag[j] = c_j > 0 ? 0 : 1;
+            if (full) cnt[j] = c_j;
+        }
+    }
+}
+
+// After the update: the maintained state describes this pass's labels.
+__global__ void exact_valid_kernel(LoopState *st) {
+    if (is_done(st)) return;
+    st->upd_valid = 1;
+    st->n_moved = 0;
+}
+
 }  // namespace
 
 UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d) {
@@ -870,7 +1114,8 @@ bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize) {
 
 // Stable counting sort of rows by label + FP64 piece sums (records).
 static void sort_and_sum_pieces(const void *Xv, size_t fsize, const UpdatePlan &p, const int32_t *labels,
-                                Workspace &ws, const LoopState *st, cudaStream_t s, const CsrRows *csr = nullptr) {
+                                Workspace &ws, const LoopState *st, cudaStream_t s, const CsrRows *csr = nullptr,
+                                bool sort_only = false) {
     const int k = (int)p.k;
     const int64_t n_groups = (p.n_chunks + kGroupChunks - 1) / kGroupChunks;
     int32_t *H = (int32_t *)ws.H.ptr;
@@ -905,6 +1150,7 @@ static void sort_and_sum_pieces(const void *Xv, size_t fsize, const UpdatePlan &
         scatter_kernel<false><<<(unsigned)p.n_chunks, 32, 0, s>>>(labels, p.n, k, p.chunk_rows, H, perm, st);
         KMB_LAUNCHED();
     }
+    if (sort_only) return;
     double *records = (double *)ws.records.ptr;
     if (csr) {
         const unsigned grid = (unsigned)((p.max_pieces + 3) / 4);
@@ -929,23 +1175,12 @@ static void sort_and_sum_pieces(const void *Xv, size_t fsize, const UpdatePlan &
 }
 
 template <typename F>
-void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *C_old, F *C_new,
-                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr, F *exact_d2) {
+static void reseed_and_commit(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *exact_d2,
+                              F *C_old, F *C_new, Workspace &ws, LoopState *st, bool commit, cudaStream_t s,
+                              const CsrRows *csr = nullptr) {
     const int k = (int)p.k, d = (int)p.d;
-    sort_and_sum_pieces(X, sizeof(F), p, labels, ws, st, s, csr);
     double *shift_part = (double *)ws.shift_part.ptr;
-    int32_t *empty_flag = (int32_t *)ws.empty_flag.ptr;
     int32_t *empty_ids = (int32_t *)ws.empty_ids.ptr;
-    const int tiles = (d + kFinalizeCols - 1) / kFinalizeCols;
-    finalize_kernel<F><<<dim3((unsigned)k, (unsigned)tiles), kFinalizeCols, 0, s>>>(
-        (const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr, (const int64_t *)ws.piece_base.ptr, C_old,
-        C_new, d, (double *)ws.shift_tiles.ptr, empty_flag, st);
-    KMB_LAUNCHED();
-    shift_tiles_kernel<<<(unsigned)std::min(148, (k + 255) / 256), 256, 0, s>>>((const double *)ws.shift_tiles.ptr, k,
-                                                                              tiles, shift_part, st);
-    KMB_LAUNCHED();
-    empties_kernel<<<1, 1024, 0, s>>>(empty_flag, k, empty_ids, shift_part, st);
-    KMB_LAUNCHED();
     // Reseeding: every kernel below returns at once unless some cluster is empty.
     if (exact_d2 && !csr) {
         refresh_d2_kernel<F><<<(unsigned)std::min<int64_t>((p.n * 32 + 255) / 256, 148 * 16), 256, 0, s>>>(
@@ -983,6 +1218,95 @@ void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const
         decide_kernel<<<1, 1, 0, s>>>(st);
         KMB_LAUNCHED();
     }
+}
+
+template <typename F>
+void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const F *d2, F *C_old, F *C_new,
+                   Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr, F *exact_d2) {
+    const int k = (int)p.k, d = (int)p.d;
+    sort_and_sum_pieces(X, sizeof(F), p, labels, ws, st, s, csr);
+    double *shift_part = (double *)ws.shift_part.ptr;
+    int32_t *empty_flag = (int32_t *)ws.empty_flag.ptr;
+    int32_t *empty_ids = (int32_t *)ws.empty_ids.ptr;
+    const int tiles = (d + kFinalizeCols - 1) / kFinalizeCols;
+    finalize_kernel<F><<<dim3((unsigned)k, (unsigned)tiles), kFinalizeCols, 0, s>>>(
+        (const double *)ws.records.ptr, (const int64_t *)ws.counts.ptr, (const int64_t *)ws.piece_base.ptr, C_old,
+        C_new, d, (double *)ws.shift_tiles.ptr, empty_flag, st);
+    KMB_LAUNCHED();
+    shift_tiles_kernel<<<(unsigned)std::min(148, (k + 255) / 256), 256, 0, s>>>((const double *)ws.shift_tiles.ptr, k,
+                                                                              tiles, shift_part, st);
+    KMB_LAUNCHED();
+    empties_kernel<<<1, 1024, 0, s>>>(empty_flag, k, empty_ids, shift_part, st);
+    KMB_LAUNCHED();
+    reseed_and_commit<F>(X, p, labels, d2, exact_d2, C_old, C_new, ws, st, commit, s, csr);
+}
+
+bool ensure_exact_buffers(Workspace &ws, int64_t n, int64_t k, int64_t d) {
+    bool ok = true;
+    ok &= ws.ensure(ws.ex_acc, sizeof(long long) * 2 * k * d);
+    ok &= ws.ensure(ws.ex_cnt, sizeof(long long) * k);
+    ok &= ws.ensure(ws.ex_prev, sizeof(int32_t) * std::max<int64_t>(1, n));
+    ok &= ws.ensure(ws.ex_colexp, sizeof(int) * d);
+    return ok;
+}
+
+void prepare_exact_update(const float *X, int64_t n, int64_t d, Workspace &ws, LoopState *st, cudaStream_t s) {
+    int *colexp = (int *)ws.ex_colexp.ptr;
+    cudaMemsetAsync(colexp, 0, sizeof(int) * d, s);
+    const int64_t total = n * d;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 8));
+    if (d <= 8192) {
+        colmax_kernel<<<blocks, 256, sizeof(unsigned) * d, s>>>(X, n, (int)d, (unsigned *)colexp, st);
+    } else {
+        colmax_global_kernel<<<blocks, 256, 0, s>>>(X, n, (int)d, (unsigned *)colexp, st);
+    }
+    KMB_LAUNCHED();
+    colexp_kernel<<<(unsigned)((d + 255) / 256), 256, 0, s>>>(colexp, (int)d, st);
+    KMB_LAUNCHED();
+}
+
+void launch_update_exact(const float *X, const UpdatePlan &p, int32_t *labels, const float *d2, float *C_old,
+                         float *C_new, Workspace &ws, LoopState *st, bool commit, cudaStream_t s, float *exact_d2) {
+    const int k = (int)p.k, d = (int)p.d;
+    int32_t *prev = (int32_t *)ws.ex_prev.ptr;
+    const int *colexp = (const int *)ws.ex_colexp.ptr;
+    long long *accA = (long long *)ws.ex_acc.ptr;
+    long long *accB = accA + (int64_t)k * d;
+    long long *cnt = (long long *)ws.ex_cnt.ptr;
+    const unsigned rb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((p.n + 255) / 256, 148 * 8));
+    count_moved_kernel<<<rb, 256, 0, s>>>(labels, prev, p.n, st);
+    KMB_LAUNCHED();
+    choose_mode_kernel<<<1, 1, 0, s>>>(p.n, st);
+    KMB_LAUNCHED();
+    // full mode: counting sort + integer piece sums (every kernel returns at once otherwise)
+    sort_and_sum_pieces(nullptr, 0, p, labels, ws, st, s, nullptr, /*sort_only=*/true);
+    segsum_fixed_kernel<<<(unsigned)p.max_pieces, 128, 0, s>>>(X, d, k, (const int32_t *)ws.perm.ptr,
+                                                                (const int64_t *)ws.offsets.ptr,
+                                                                (const int64_t *)ws.piece_base.ptr, p.piece_rows,
+                                                                colexp, (long long *)ws.records.ptr, st);
+    KMB_LAUNCHED();
+    // incremental mode: the moved rows
+    apply_moves_kernel<<<rb, 256, 0, s>>>(X, p.n, d, labels, prev, colexp, (unsigned long long *)accA,
+                                          (unsigned long long *)accB, (unsigned long long *)cnt, st);
+    KMB_LAUNCHED();
+    double *shift_part = (double *)ws.shift_part.ptr;
+    int32_t *empty_flag = (int32_t *)ws.empty_flag.ptr;
+    int32_t *empty_ids = (int32_t *)ws.empty_ids.ptr;
+    const int tiles = (d + kFinalizeCols - 1) / kFinalizeCols;
+    finalize_exact_kernel<<<dim3((unsigned)k, (unsigned)tiles), kFinalizeCols, 0, s>>>(
+        (const long long *)ws.records.ptr, (const int64_t *)ws.counts.ptr, (const int64_t *)ws.piece_base.ptr, colexp,
+        accA, accB, cnt, C_old, C_new, d, (double *)ws.shift_tiles.ptr, empty_flag, st);
+    KMB_LAUNCHED();
+    copy_prev_kernel<<<rb, 256, 0, s>>>(labels, prev, p.n, st);
+    KMB_LAUNCHED();
+    exact_valid_kernel<<<1, 1, 0, s>>>(st);
+    KMB_LAUNCHED();
+    shift_tiles_kernel<<<(unsigned)std::min(148, (k + 255) / 256), 256, 0, s>>>((const double *)ws.shift_tiles.ptr, k,
+                                                                              tiles, shift_part, st);
+    KMB_LAUNCHED();
+    empties_kernel<<<1, 1024, 0, s>>>(empty_flag, k, empty_ids, shift_part, st);
+    KMB_LAUNCHED();
+    reseed_and_commit<float>(X, p, labels, exact_d2 ? exact_d2 : d2, exact_d2, C_old, C_new, ws, st, commit, s);
 }
 
 template <typename F>
