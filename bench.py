@@ -513,9 +513,8 @@ def run_sharded(args, dist, world, rank, local, form):
     def iterate(C, T):
         for _ in range(T):
             st = ops.partial(C)
-            dist.all_reduce(st.sums)
-            dist.all_reduce(st.counts)
-            C, shift, empty = ops.finalize(st.sums, st.counts, C)
+            sums, counts, _ = spmd.exchange(st)
+            C, shift, empty = ops.finalize(sums, counts, C)
         return C
 
     iterate(C0.clone(), args.warmup)
@@ -537,7 +536,7 @@ def run_sharded(args, dist, world, rank, local, form):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"precision, {n} rows per rank (seed + rank), d={w.d}, k={w.k}, float32",
                        "n_per_rank": n, "d": w.d, "k": w.k, "form": args.form,
-                       "exchange": "NCCL all-reduce of FP64 sums (k*d) and int64 counts (k) per iteration",
+                       "exchange": "one NCCL all-reduce per iteration of a packed FP64 buffer [sums (k*d) | counts (k) | squared distances (1)]",
                        "value_unit": "20M-row shard iterations per second, summed over ranks"},
         }
         print(json.dumps(line))

@@ -125,7 +125,7 @@ void Workspace::release() {
                      &empty_ids,
                      &sel_hist, &sel_state, &cand, &obj_part, &scalars, &state, &Xhi, &Xlo, &Chi, &Clo, &tcx, &rowb, &pp_acc, &pp_rand,
                      &pp_state, &pp_flags, &csr_vals, &csr_cols64, &csr_rowptr64, &csr_cols, &csr_rowptr,
-                     &csr_bad, &csr_cnorm, &ex_acc, &ex_cnt, &ex_prev, &ex_colexp};
+                     &csr_bad, &csr_cnorm, &ex_acc, &ex_cnt, &ex_prev, &ex_colexp, &ex_records};
     for (DevBuf *b : all) {
         if (b->ptr) cudaFreeAsync(b->ptr, stream);
         b->ptr = nullptr;

@@ -121,7 +121,8 @@ struct Workspace {
     DevBuf sel_hist, sel_state, cand, obj_part, scalars, state;
     DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb, pp_acc, pp_rand, pp_state, pp_flags;
     DevBuf csr_vals, csr_cols64, csr_rowptr64, csr_cols, csr_rowptr, csr_bad, csr_cnorm;
-    DevBuf ex_acc, ex_cnt, ex_prev, ex_colexp;  // exact update: limb sums, counts, previous labels, scales
+    DevBuf ex_acc, ex_cnt, ex_prev, ex_colexp, ex_records;  // exact update: limb sums, counts, previous
+                                                             // labels, scales, per-piece limb sums
     // Grows `b` to at least `bytes`; returns false on allocation failure.
     bool ensure(DevBuf &b, size_t bytes);
     void release();
@@ -243,10 +244,11 @@ void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const
 
 // The exact update of FP32 rows (the Lloyd loop's update for float data). Every
 // value x of column t is taken as the integer round(x * 2^E_t), E_t chosen once
-// per call so that the column's largest |x| stays below 2^39; a cluster's sum is
-// then an exact integer (two 64-bit limbs), independent of the order in which
-// rows are added, and the centroid is that integer scaled back, divided by the
-// count in FP64 and rounded to float. Because the sums are a function of the
+// per call so that the column's largest |x| stays below 2^94 (every float within
+// 2^70 of it exact); a cluster's sum is then an exact integer (three 32-bit
+// limbs summed in int64), independent of the order in which rows are added, and
+// the centroid is that integer rounded to the nearest double, scaled back,
+// divided by the count in FP64 and rounded to float. Because the sums are a function of the
 // labels alone, a pass that moved at most n/16 rows is applied as those rows'
 // moves (subtract from the old cluster, add to the new one, exact) instead of a
 // full counting-sort pass over X; the result is bit for bit the same.

@@ -829,13 +829,55 @@ __global__ void list_empties_kernel(const int32_t *__restrict__ empty_flag, int 
 }
 
 // ---- exact update (FP32 rows) -------------------------------------------------
-// Limb form of a cluster-column sum S = A * 2^32 + B (A, B int64; B is brought
-// back to [0, 2^32) by the finalize, so it never overflows between passes).
+// A value x of column t is the integer v = round(x * 2^E_t), |v| < 2^94, with E_t
+// chosen once per call from the column's largest |x|: every float within 2^70 of
+// that maximum is represented exactly (a 24-bit significand), smaller ones to
+// 2^-94 of the maximum. v is kept as three 32-bit limbs, v = l2 * 2^64 + l1 * 2^32
+// + l0 (l0, l1 in [0, 2^32), l2 signed), and a cluster-column sum as three int64
+// limb sums, so additions and subtractions of rows in any order give the same
+// integer. The finalize folds the limb sums into one 128-bit integer, keeps it
+// normalised, and converts it to the nearest double.
 
-constexpr int kExactMaxBits = 39;  // |round(x * 2^E_t)| < 2^39: 512-row pieces stay exact in int64
+constexpr int kExactMaxBits = 94;
 
-__device__ __forceinline__ long long fixed_of(float x, int e) {
-    return __float2ll_rn(scalbnf(x, e));
+struct Limbs {
+    long long l0, l1, l2;
+};
+
+__device__ __forceinline__ Limbs fixed_of(float x, int e) {
+    const float f = scalbnf(x, e);  // exact: |f| < 2^94, a power-of-two scaling
+    const unsigned bits = __float_as_uint(f);
+    const int be = (int)((bits >> 23) & 0xffu);
+    unsigned long long mant = bits & 0x7fffffu;
+    if (be) mant |= 0x800000u;
+    const int sh = (be ? be : 1) - 150;  // f = mant * 2^sh
+    unsigned __int128 mag = 0;
+    if (sh >= 0) {
+        mag = (unsigned __int128)mant << sh;
+    } else if (sh > -26) {
+        const int r = -sh;  // round half to even
+        const unsigned long long q = mant >> r, rem = mant & ((1ull << r) - 1), half = 1ull << (r - 1);
+        mag = q + ((rem > half || (rem == half && (q & 1ull))) ? 1ull : 0ull);
+    }
+    const __int128 v = (bits >> 31) ? -(__int128)mag : (__int128)mag;
+    Limbs L;
+    L.l0 = (long long)(v & 0xffffffffll);
+    L.l1 = (long long)((v >> 32) & 0xffffffffll);
+    L.l2 = (long long)(v >> 64);
+    return L;
+}
+
+// The nearest double to |m| (round half to even), m < 2^127.
+__device__ __forceinline__ double u128_to_double(unsigned __int128 m) {
+    const unsigned long long hi = (unsigned long long)(m >> 64), lo = (unsigned long long)m;
+    if (hi == 0 && lo < (1ull << 53)) return (double)lo;
+    const int top = hi ? 127 - __clzll((long long)hi) : 63 - __clzll((long long)lo);
+    const int sh = top - 52;
+    unsigned long long q = (unsigned long long)(m >> sh);
+    const unsigned __int128 rem = m & (((unsigned __int128)1 << sh) - 1);
+    const unsigned __int128 half = (unsigned __int128)1 << (sh - 1);
+    if (rem > half || (rem == half && (q & 1ull))) ++q;
+    return ldexp((double)q, sh);
 }
 
 // colexp[t] <- max |x| of column t, as float bits (non-negative floats order as ints).
@@ -906,14 +948,16 @@ __global__ void choose_mode_kernel(int64_t n, LoopState *st) {
 }
 
 // Block p sums piece p's rows (one cluster's rows in row order) as integers.
+// records: three limb planes of (pieces x d) int64.
 __global__ void __launch_bounds__(128)
 segsum_fixed_kernel(const float *__restrict__ X, int d, int k, const int32_t *__restrict__ perm,
                     const int64_t *__restrict__ offsets, const int64_t *__restrict__ piece_base, int64_t piece_rows,
-                    const int *__restrict__ colexp, long long *__restrict__ records, const LoopState *st) {
+                    int64_t max_pieces, const int *__restrict__ colexp, long long *__restrict__ records,
+                    const LoopState *st) {
     if (sort_skipped(st)) return;
     constexpr int NT = 128;
     __shared__ int32_t rows[kPieceRows];
-    __shared__ long long part[NT];
+    __shared__ long long part[3][NT];
     const int64_t p = blockIdx.x;
     if (p >= piece_base[k]) return;
     int lo = 0, hi = k;  // invariant: piece_base[lo] <= p < piece_base[hi]
@@ -931,27 +975,42 @@ segsum_fixed_kernel(const float *__restrict__ X, int d, int k, const int32_t *__
     int dl, rp;
     row_layout(d, NT, dl, rp);
     const int t = threadIdx.x % dl, rr = threadIdx.x / dl;
+    const int64_t plane = max_pieces * (int64_t)d;
     for (int t0 = 0; t0 < d; t0 += dl) {
         const int col = t0 + t;
-        long long acc = 0;
+        long long a0 = 0, a1 = 0, a2 = 0;
         if (col < d) {
             const int ex = colexp[col];
             int i = rr;
-            for (; i + 3 * rp < cnt; i += 4 * rp) {
+            for (; i + 1 * rp < cnt; i += 2 * rp) {
                 const float v0 = X[(int64_t)rows[i] * d + col];
                 const float v1 = X[(int64_t)rows[i + rp] * d + col];
-                const float v2 = X[(int64_t)rows[i + 2 * rp] * d + col];
-                const float v3 = X[(int64_t)rows[i + 3 * rp] * d + col];
-                acc += fixed_of(v0, ex) + fixed_of(v1, ex) + fixed_of(v2, ex) + fixed_of(v3, ex);
+                const Limbs L0 = fixed_of(v0, ex), L1 = fixed_of(v1, ex);
+                a0 += L0.l0 + L1.l0;
+                a1 += L0.l1 + L1.l1;
+                a2 += L0.l2 + L1.l2;
             }
-            for (; i < cnt; i += rp) acc += fixed_of(X[(int64_t)rows[i] * d + col], ex);
+            for (; i < cnt; i += rp) {
+                const Limbs L = fixed_of(X[(int64_t)rows[i] * d + col], ex);
+                a0 += L.l0;
+                a1 += L.l1;
+                a2 += L.l2;
+            }
         }
-        part[threadIdx.x] = acc;
+        part[0][threadIdx.x] = a0;
+        part[1][threadIdx.x] = a1;
+        part[2][threadIdx.x] = a2;
         __syncthreads();
         if (rr == 0 && col < d) {
-            long long tot = part[t];
-            for (int r2 = 1; r2 < rp; ++r2) tot += part[r2 * dl + t];
-            records[p * d + col] = tot;
+            long long t0s = part[0][t], t1s = part[1][t], t2s = part[2][t];
+            for (int r2 = 1; r2 < rp; ++r2) {
+                t0s += part[0][r2 * dl + t];
+                t1s += part[1][r2 * dl + t];
+                t2s += part[2][r2 * dl + t];
+            }
+            records[p * d + col] = t0s;
+            records[plane + p * d + col] = t1s;
+            records[2 * plane + p * d + col] = t2s;
         }
         __syncthreads();
     }
@@ -959,9 +1018,10 @@ segsum_fixed_kernel(const float *__restrict__ X, int d, int k, const int32_t *__
 
 // Moved rows (incremental mode): each leaves its old cluster's sums and joins the
 // new one's (integer atomics, exact in any order); prev follows the labels.
-__global__ void apply_moves_kernel(const float *__restrict__ X, int64_t n, int d, const int32_t *__restrict__ labels,
-                                   int32_t *__restrict__ prev, const int *__restrict__ colexp,
-                                   unsigned long long *__restrict__ accA, unsigned long long *__restrict__ accB,
+// acc: three limb planes of (k x d) int64.
+__global__ void apply_moves_kernel(const float *__restrict__ X, int64_t n, int d, int k,
+                                   const int32_t *__restrict__ labels, int32_t *__restrict__ prev,
+                                   const int *__restrict__ colexp, unsigned long long *__restrict__ acc,
                                    unsigned long long *__restrict__ cnt, const LoopState *st) {
     if (is_done(st) || st->upd_mode != 1) return;
     const int lane = threadIdx.x & 31;
@@ -980,13 +1040,16 @@ __global__ void apply_moves_kernel(const float *__restrict__ X, int64_t n, int d
             const int64_t row = base + src;
             const int nl = __shfl_sync(0xffffffffu, lab, src), ol = __shfl_sync(0xffffffffu, old, src);
             const float *x = X + row * d;
+            const int64_t plane = (int64_t)k * d;
             for (int t = lane; t < d; t += 32) {
-                const long long v = fixed_of(x[t], colexp[t]);
-                const unsigned long long a = (unsigned long long)(v >> 32), b = (unsigned long long)(v & 0xffffffffll);
-                atomicAdd(&accA[(int64_t)nl * d + t], a);
-                atomicAdd(&accB[(int64_t)nl * d + t], b);
-                atomicAdd(&accA[(int64_t)ol * d + t], (unsigned long long)(-(long long)a));
-                atomicAdd(&accB[(int64_t)ol * d + t], (unsigned long long)(-(long long)b));
+                const Limbs L = fixed_of(x[t], colexp[t]);
+                const int64_t in = (int64_t)nl * d + t, out = (int64_t)ol * d + t;
+                atomicAdd(&acc[in], (unsigned long long)L.l0);
+                atomicAdd(&acc[plane + in], (unsigned long long)L.l1);
+                atomicAdd(&acc[2 * plane + in], (unsigned long long)L.l2);
+                atomicAdd(&acc[out], (unsigned long long)-L.l0);
+                atomicAdd(&acc[plane + out], (unsigned long long)-L.l1);
+                atomicAdd(&acc[2 * plane + out], (unsigned long long)-L.l2);
             }
             if (lane == 0) {
                 atomicAdd(&cnt[nl], 1ull);
@@ -1009,11 +1072,11 @@ __global__ void copy_prev_kernel(const int32_t *__restrict__ labels, int32_t *__
 // the maintained ones), normalised and kept; c = F(S * 2^-E / count) in FP64; the
 // tile's shift part and the empty flag, as finalize_kernel.
 __global__ void __launch_bounds__(kFinalizeCols)
-finalize_exact_kernel(const long long *__restrict__ records, const int64_t *__restrict__ counts_sort,
-                      const int64_t *__restrict__ piece_base, const int *__restrict__ colexp,
-                      long long *__restrict__ accA, long long *__restrict__ accB, long long *__restrict__ cnt,
-                      const float *__restrict__ C_old, float *__restrict__ C_new, int d,
-                      double *__restrict__ shift_tiles, int32_t *__restrict__ empty_flag, const LoopState *st) {
+finalize_exact_kernel(const long long *__restrict__ records, int64_t max_pieces, const int64_t *__restrict__ counts_sort,
+                      const int64_t *__restrict__ piece_base, const int *__restrict__ colexp, int k,
+                      long long *__restrict__ lacc, long long *__restrict__ cnt, const float *__restrict__ C_old,
+                      float *__restrict__ C_new, int d, double *__restrict__ shift_tiles,
+                      int32_t *__restrict__ empty_flag, const LoopState *st) {
     if (is_done(st)) return;
     __shared__ double red[kFinalizeCols / 32];
     const int j = blockIdx.x;
@@ -1022,26 +1085,28 @@ finalize_exact_kernel(const long long *__restrict__ records, const int64_t *__re
     const long long c_j = full ? (long long)counts_sort[j] : cnt[j];
     double acc = 0.0;
     if (t < d) {
-        long long A = 0, B = 0;
-        const int64_t idx = (int64_t)j * d + t;
+        const int64_t idx = (int64_t)j * d + t, plane = (int64_t)k * d, rplane = max_pieces * (int64_t)d;
+        long long s0 = 0, s1 = 0, s2 = 0;
         if (full) {
             for (int64_t p = piece_base[j]; p < piece_base[j + 1]; ++p) {
-                const long long v = records[p * d + t];
-                A += v >> 32;
-                B += v & 0xffffffffll;
+                s0 += records[p * d + t];
+                s1 += records[rplane + p * d + t];
+                s2 += records[2 * rplane + p * d + t];
             }
         } else {
-            A = accA[idx];
-            B = accB[idx];
+            s0 = lacc[idx];
+            s1 = lacc[plane + idx];
+            s2 = lacc[2 * plane + idx];
         }
-        A += B >> 32;  // normalise: 0 <= B < 2^32
-        B &= 0xffffffffll;
-        accA[idx] = A;
-        accB[idx] = B;
+        // one 128-bit integer, stored back normalised (l0, l1 in [0, 2^32))
+        const __int128 S = ((__int128)s2 << 64) + ((__int128)s1 << 32) + (__int128)s0;
+        lacc[idx] = (long long)(S & 0xffffffffll);
+        lacc[plane + idx] = (long long)((S >> 32) & 0xffffffffll);
+        lacc[2 * plane + idx] = (long long)(S >> 64);
         const float old = C_old[idx];
         if (c_j > 0) {
-            const double S = (double)A * 4294967296.0 + (double)B;
-            const float c = (float)(ldexp(S, -colexp[t]) / (double)c_j);
+            const double Sd = S < 0 ? -u128_to_double((unsigned __int128)(-S)) : u128_to_double((unsigned __int128)S);
+            const float c = (float)(ldexp(Sd, -colexp[t]) / (double)c_j);
             const double df = (double)old - (double)c;
             acc = df * df;
             C_new[idx] = c;
@@ -1243,7 +1308,8 @@ void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const
 
 bool ensure_exact_buffers(Workspace &ws, int64_t n, int64_t k, int64_t d) {
     bool ok = true;
-    ok &= ws.ensure(ws.ex_acc, sizeof(long long) * 2 * k * d);
+    ok &= ws.ensure(ws.ex_acc, sizeof(long long) * 3 * k * d);
+    ok &= ws.ensure(ws.ex_records, sizeof(long long) * 3 * (n / kPieceRows + k + 1) * d);
     ok &= ws.ensure(ws.ex_cnt, sizeof(long long) * k);
     ok &= ws.ensure(ws.ex_prev, sizeof(int32_t) * std::max<int64_t>(1, n));
     ok &= ws.ensure(ws.ex_colexp, sizeof(int) * d);
@@ -1270,9 +1336,9 @@ void launch_update_exact(const float *X, const UpdatePlan &p, int32_t *labels, c
     const int k = (int)p.k, d = (int)p.d;
     int32_t *prev = (int32_t *)ws.ex_prev.ptr;
     const int *colexp = (const int *)ws.ex_colexp.ptr;
-    long long *accA = (long long *)ws.ex_acc.ptr;
-    long long *accB = accA + (int64_t)k * d;
+    long long *acc = (long long *)ws.ex_acc.ptr;
     long long *cnt = (long long *)ws.ex_cnt.ptr;
+    long long *records = (long long *)ws.ex_records.ptr;
     const unsigned rb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((p.n + 255) / 256, 148 * 8));
     count_moved_kernel<<<rb, 256, 0, s>>>(labels, prev, p.n, st);
     KMB_LAUNCHED();
@@ -1283,19 +1349,19 @@ void launch_update_exact(const float *X, const UpdatePlan &p, int32_t *labels, c
     segsum_fixed_kernel<<<(unsigned)p.max_pieces, 128, 0, s>>>(X, d, k, (const int32_t *)ws.perm.ptr,
                                                                 (const int64_t *)ws.offsets.ptr,
                                                                 (const int64_t *)ws.piece_base.ptr, p.piece_rows,
-                                                                colexp, (long long *)ws.records.ptr, st);
+                                                                p.max_pieces, colexp, records, st);
     KMB_LAUNCHED();
     // incremental mode: the moved rows
-    apply_moves_kernel<<<rb, 256, 0, s>>>(X, p.n, d, labels, prev, colexp, (unsigned long long *)accA,
-                                          (unsigned long long *)accB, (unsigned long long *)cnt, st);
+    apply_moves_kernel<<<rb, 256, 0, s>>>(X, p.n, d, k, labels, prev, colexp, (unsigned long long *)acc,
+                                          (unsigned long long *)cnt, st);
     KMB_LAUNCHED();
     double *shift_part = (double *)ws.shift_part.ptr;
     int32_t *empty_flag = (int32_t *)ws.empty_flag.ptr;
     int32_t *empty_ids = (int32_t *)ws.empty_ids.ptr;
     const int tiles = (d + kFinalizeCols - 1) / kFinalizeCols;
     finalize_exact_kernel<<<dim3((unsigned)k, (unsigned)tiles), kFinalizeCols, 0, s>>>(
-        (const long long *)ws.records.ptr, (const int64_t *)ws.counts.ptr, (const int64_t *)ws.piece_base.ptr, colexp,
-        accA, accB, cnt, C_old, C_new, d, (double *)ws.shift_tiles.ptr, empty_flag, st);
+        records, p.max_pieces, (const int64_t *)ws.counts.ptr, (const int64_t *)ws.piece_base.ptr, colexp, k, acc,
+        cnt, C_old, C_new, d, (double *)ws.shift_tiles.ptr, empty_flag, st);
     KMB_LAUNCHED();
     copy_prev_kernel<<<rb, 256, 0, s>>>(labels, prev, p.n, st);
     KMB_LAUNCHED();

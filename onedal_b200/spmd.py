@@ -4,8 +4,9 @@ Each rank holds a contiguous block of rows. Per iteration:
 
 1. local statistics under the shared centroids C (``kmb_partial_sums``):
    labels, FP64 per-cluster sums, int64 counts, squared distances per row;
-2. one all-reduce of the FP64 sums and the counts (NCCL on GPUs; gloo in the
-   CPU tests of this module's host logic);
+2. one all-reduce of a packed FP64 buffer [sums (k*d) | counts (k) | sum of
+   squared distances (1)] (NCCL on GPUs; gloo in the CPU tests of this
+   module's host logic); counts travel as doubles, exact below 2^53;
 3. identical finalize on every rank (``kmb_finalize_centroids``):
    c_j = F(S_j / count_j), shift over non-empty clusters, list of empty ones;
 4. when clusters are empty: every rank proposes its local top-m rows by squared
@@ -40,7 +41,7 @@ class ShardStats:
     sums: torch.Tensor        # (k, d) float64
     counts: torch.Tensor      # (k,) int64
     row_sq: torch.Tensor      # (n_local,) squared distance of each row to its centroid
-    sq_total: float
+    sq_total: object          # this shard's sum of squared distances (a device tensor or a float)
 
 
 class DeviceShardOps:
@@ -66,7 +67,7 @@ class DeviceShardOps:
         self.ctx.check(self.ctx.lib.kmb_partial_sums(self.ctx.handle, self.dtype, self.X.data_ptr(), n, d,
                                                      C.data_ptr(), k, self.form, labels.data_ptr(), sums.data_ptr(),
                                                      counts.data_ptr(), sq.data_ptr(), row_sq.data_ptr()))
-        return ShardStats(labels, sums, counts, row_sq, float(sq.item()))
+        return ShardStats(labels, sums, counts, row_sq, sq)  # sq stays on the device: no sync here
 
     def finalize(self, sums: torch.Tensor, counts: torch.Tensor, C: torch.Tensor):
         k, d = C.shape
@@ -96,6 +97,21 @@ def _top_candidates(row_sq: torch.Tensor, m: int, row_offset: int):
     return vals, rows, order
 
 
+def exchange(st: ShardStats, group=None):
+    """The iteration's one collective: all-reduce of [sums | counts | squared
+    distances] packed into one FP64 buffer. Returns (sums, counts, sq_total) summed
+    over the ranks, on the sums' device."""
+    k, d = st.sums.shape
+    dev = st.sums.device
+    packed = torch.empty(k * d + k + 1, dtype=torch.float64, device=dev)
+    packed[: k * d] = st.sums.reshape(-1)
+    packed[k * d: k * d + k] = st.counts.to(torch.float64)
+    packed[k * d + k:] = torch.as_tensor(st.sq_total, dtype=torch.float64, device=dev).reshape(1)
+    dist.all_reduce(packed, group=group)
+    return (packed[: k * d].view(k, d), packed[k * d: k * d + k].round().to(torch.int64),
+            packed[k * d + k:])
+
+
 def train_spmd(ops, C0: torch.Tensor, max_iteration_count: int, accuracy_threshold: float = 0.0, group=None):
     """Runs the sharded Lloyd loop. Returns (centroids, local labels, iterations, objective)
     with centroids identical on every rank."""
@@ -112,9 +128,8 @@ def train_spmd(ops, C0: torch.Tensor, max_iteration_count: int, accuracy_thresho
     it = 0
     while it < max_iteration_count:
         st = ops.partial(C)
-        dist.all_reduce(st.sums, group=group)
-        dist.all_reduce(st.counts, group=group)
-        C_new, shift, empty = ops.finalize(st.sums, st.counts, C)
+        sums, counts, _ = exchange(st, group)
+        C_new, shift, empty = ops.finalize(sums, counts, C)
         m = len(empty)
         if m:
             vals, rows, local = _top_candidates(st.row_sq, m, row_offset)
@@ -146,6 +161,6 @@ def train_spmd(ops, C0: torch.Tensor, max_iteration_count: int, accuracy_thresho
             break
     # responses and objective under the final centroids
     st = ops.partial(C)
-    obj = torch.tensor([st.sq_total], dtype=torch.float64, device=dev)
+    obj = torch.as_tensor(st.sq_total, dtype=torch.float64, device=dev).reshape(1).clone()
     dist.all_reduce(obj, group=group)
     return C, st.labels, it, float(obj.item())

@@ -58,7 +58,7 @@ def test_shard_sums_match_single_update(dt, d, k, far):
         sums += st.sums
         counts += st.counts
         labels.append(st.labels.cpu().numpy())
-        sq += st.sq_total
+        sq += float(st.sq_total)
     C_new, shift, empty = ops.finalize(sums, counts, Cd)
     torch.cuda.synchronize()
 
