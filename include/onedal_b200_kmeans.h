@@ -277,17 +277,23 @@ KMB_API int kmb_infer_noalloc(int dtype, const void *X, int64_t n, int64_t d, co
                               int32_t *responses, double *objective, void *cuda_stream);
 
 /* ---- Batched form ---------------------------------------------------------
- * Many independent float32 problems (each its own X, n, d, k) train together:
- * every Lloyd iteration is one fixed sequence of grouped launches over all
- * problems (optionally captured once into a CUDA graph and replayed), with
- * per-problem convergence flags on the device. Per problem the semantics are
- * those of kmb_lloyd_iterate (plain form): up to max_iteration_count updates,
- * stop when the shift <= accuracy_threshold; C (k x d) is updated in place and
- * labels hold the assignment of the last completed update. Sums are 64-bit
- * fixed point with a per-problem scale (exact on that grid, independent of
- * scheduling). Limits: k <= 256 and (k*d + k) * 8 <= 200 KiB per problem. The
- * assignment tile per (d, k) class is chosen by a built-in autotuner the first
- * time the class is seen on a device. No counterpart in the reference. */
+ * Many independent float32 problems (each its own X, n, d, k) train together in
+ * one persistent cooperative kernel: per Lloyd iteration it walks prep, assign,
+ * accumulate, finalize and decide phases over flat work lists of all problems,
+ * separated by grid-wide barriers; converged problems are skipped and the kernel
+ * ends when every problem has converged. Per problem the result is that of
+ * kmb_lloyd_iterate (plain form) bit for bit -- the same FP32 scores, the same
+ * exact fixed-point cluster sums, the same reseeding -- up to max_iteration_count
+ * updates, stopping when the shift <= accuracy_threshold (the shift is the same
+ * sum in another order, so a threshold that equals it to the last bit may stop
+ * one path an iteration before the other; with threshold 0 the two agree). C
+ * (k x d) is updated in place; labels hold the assignment of the last completed
+ * update. Limits: k <= 256 and k <= n and (k*d + k) * 8 <= 200 KiB per problem.
+ * The assignment tile per (d, k) class is chosen by a built-in autotuner the
+ * first time the class is seen on a device. use_graph launches the kernel from a
+ * CUDA graph (one cooperative kernel node). A grid barrier that does not complete
+ * within about two seconds makes every CTA leave and the call return
+ * KMB_ETIMEDOUT. No counterpart in the reference. */
 typedef struct kmb_batched_problem {
     const void *X;      /* device, n x d */
     int64_t n, d;
@@ -300,7 +306,7 @@ typedef struct kmb_batched_problem {
 
 typedef struct kmb_batched_info {
     int64_t problems;
-    int32_t variants;         /* assignment tile variants launched per iteration */
+    int32_t variants;         /* assignment tile variants (rows per thread x cluster tile) in use */
     int64_t total_iterations; /* summed over problems */
     int64_t graph_launches;
 } kmb_batched_info;

@@ -1,14 +1,15 @@
 """Batched k-means: many independent float32 problems trained together on one
-GPU (front end of kmb_batched_train). Every Lloyd iteration is one fixed
-sequence of grouped launches over all problems, replayed from a CUDA graph;
-converged problems are skipped on the device.
+GPU (front end of kmb_batched_train). One persistent cooperative kernel runs
+every Lloyd iteration of every problem (prep, assign, accumulate, finalize and
+decide phases over flat work lists, grid-wide barriers between them); converged
+problems are skipped on the device and the kernel ends when all have converged.
 
-    results = batched_train([(X0, C0), (X1, C1), ...], max_iteration_count=30)
+    results, info = batched_train([(X0, C0), (X1, C1), ...], max_iteration_count=30)
     for C, labels, iterations in results: ...
 
-Inputs are CUDA torch tensors (X: n x d, C0: k x d, float32); per problem the
-result equals ``kmb_lloyd_iterate`` (plain form) up to the summation order of the
-centroid sums (64-bit fixed point here, exact on its grid).
+Inputs are CUDA torch tensors (X: n x d, C0: k x d, float32; k <= 256). Per
+problem the result equals ``kmb_lloyd_iterate`` (plain form) bit for bit:
+centroids, responses and iteration count.
 """
 import ctypes
 

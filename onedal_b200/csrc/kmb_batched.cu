@@ -1,92 +1,190 @@
-// Batched form: thousands of independent k-means problems (uneven n, k, d) run
-// their Lloyd iterations together. Every iteration is a fixed sequence of
-// grouped launches over all problems, captured once into a CUDA graph and
-// replayed; converged problems are skipped on the device through per-problem
-// flags, so the host does not synchronise between iterations.
+// Batched form: thousands of independent k-means problems (uneven n, k, d) train
+// together in ONE persistent grouped kernel. A cooperative grid walks, for every
+// Lloyd iteration, five phases over flat work lists of all problems, separated
+// by grid-wide barriers (bounded waits: a barrier that does not complete within
+// ~2 s sets an error flag, every CTA leaves, and the call returns KMB_ETIMEDOUT).
+// The launch can be captured into a CUDA graph and replayed.
 //
-// Per iteration (semantics of one pass of cpp/daal/src/algorithms/kmeans/
-// kmeans_lloyd_batch_impl.i:117-212 for every problem):
-//   prep        C -> transposed Ct, h = 0.5||c||^2 (FP32 from a double sum)
-//   assign      one work item = (problem, row tile); FP32 FMA scores
-//               h_j - x.c_j over all of the problem's clusters (k <= 256),
-//               lowest index on ties; labels + squared distances
-//   accumulate  one work item = (problem, row block): the rows' values are
-//               converted to 64-bit fixed point with a per-problem scale and
-//               summed with integer atomics in shared memory, then in global
-//               memory. Integer addition is associative, so the sums are exact
-//               on the fixed-point grid and independent of scheduling.
-//   finalize    one work item = (problem, cluster): c = F(S / count), shift part
-//   decide      one block per problem: shift, empty-cluster reseed with the
-//               farthest rows (descending squared distance, ascending row; empty
-//               clusters in ascending order), iteration count, stop test.
-// The assignment tile (rows per thread) is chosen per (d, k-tile) class by a
-// small autotuner that times both candidates on synthetic rows once per context.
+// Per iteration (the semantics of one pass of cpp/daal/src/algorithms/kmeans/
+// kmeans_lloyd_batch_impl.i:117-212, for every problem not yet converged):
+//   prep        (problem, cluster)   C -> transposed Ct, h = 0.5||c||^2
+//   assign      (problem, row tile)  FP32 FMA scores h_j - x.c_j over all of the
+//                                    problem's clusters (k <= 256), lowest index on
+//                                    ties; labels and squared distances
+//   accumulate  (problem, row block) exact fixed-point cluster sums: every value
+//                                    as three 32-bit limbs (the Lloyd loop's exact
+//                                    update, kmb_internal.cuh), summed in shared
+//                                    memory per block of columns, then added to the
+//                                    problem's int64 limb sums
+//   finalize    (problem, cluster)   c = F(S / count) from the 128-bit sum, shift
+//                                    part, sums cleared for the next iteration
+//   decide      (problem)            empty clusters reseeded with the farthest rows
+//                                    (squared distance descending, row ascending;
+//                                    empty clusters ascending), shift, stop test
+// Each step computes what the single-problem path (kmb_lloyd_iterate, plain form)
+// computes, in the same floating-point order -- row norms, half norms, scores,
+// exact sums, centroids -- so a problem trained here equals the same problem
+// trained alone bit for bit.
+//
+// Work items of a phase are assigned to CTAs round-robin; the assignment list is
+// sorted by cost (rows x padded clusters x padded features) so the largest tiles
+// start first. The assignment tile (rows per thread) of each (d, k) class comes
+// from a built-in autotuner that times the candidates on synthetic rows of that
+// shape the first time the class is seen on a device (cached under a lock).
 #include "kmb_internal.cuh"
 
 #include <algorithm>
-#include <cmath>
+#include <cstring>
 #include <map>
+#include <mutex>
 #include <vector>
 
 namespace kmb {
 namespace batched {
 
-constexpr int NT = 256;
-constexpr int BK = 8;
-constexpr int kMaxK = 256;       // clusters per problem handled by one tile
-constexpr int kAccRows = 2048;   // rows per accumulate work item
+constexpr int NT = 256;            // threads per CTA
+constexpr int BK = 8;              // contraction chunk of the assignment tile
+constexpr int kMaxK = 256;         // clusters per problem (one assignment tile covers all)
+constexpr int kAccRows = 1024;     // rows per accumulate / setup work item
+constexpr int kAccSlots = 2048;    // (cluster, column) slots of the shared limb sums
+constexpr long long kBarrierTimeout = 4000000000ll;  // ~2 s of SM clocks
 
 struct Problem {
     const float *X;
     float *C;
-    float *Ct;        // dpad x kpad
-    float *h;         // kpad (+inf padding)
+    float *Ct;          // dpad x kpad
+    float *h;           // kpad (+inf padding)
     int32_t *labels;
     float *d2;
     float *xnorm;
-    unsigned long long *acc;  // k*d fixed-point sums (two's complement)
-    int *counts;              // k
-    double *shift_part;       // k
+    long long *acc;     // 3 limb planes of k x d
+    int *counts;        // k
+    double *shift_part; // k
+    int *colexp;        // d (column maxima as float bits during setup, then E_t)
     long long n;
-    int d, dpad, k, kpad;
-    double scale;             // fixed-point scale
-    int amax_bits;            // max |x| of the problem (float bits, non-negative)
+    int d, dpad, k, kpad, tm;
     int done, iters, max_iters, empty_events;
     double eps, shift;
 };
 
-// ---- prep --------------------------------------------------------------------
-__global__ void prep_kernel(Problem *P, const int2 *items, int n_items) {
-    const int it = blockIdx.x;  // one warp per (problem, padded cluster)
-    if (it >= n_items) return;
-    const int2 w = items[it];
-    Problem &p = P[w.x];
-    if (p.done) return;
-    const int j = w.y;
-    double s = 0.0;
-    for (int t = threadIdx.x; t < p.dpad; t += 32) {
-        const float v = (j < p.k && t < p.d) ? p.C[(long long)j * p.d + t] : 0.f;
-        p.Ct[(long long)t * p.kpad + j] = v;
-        s += (double)v * (double)v;
+struct Lists {
+    const int2 *setup;  int n_setup;   // (problem, row block)
+    const int2 *prep;   int n_prep;    // (problem, padded cluster)
+    const int2 *assign; int n_assign;  // (problem, row tile), largest first
+    const int2 *acc;    int n_acc;     // (problem, row block)
+    const int2 *fin;    int n_fin;     // (problem, cluster)
+    int n_problems;
+    int iterations;
+};
+
+struct GridBarrier {
+    unsigned count;
+    unsigned gen;
+    int error;
+    int active;  // problems not yet converged
+};
+
+// Grid-wide barrier of a cooperative launch; false once any CTA gave up waiting.
+__device__ __forceinline__ bool grid_sync(GridBarrier *gb) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *vgen = &gb->gen;
+        const unsigned g = *vgen;
+        __threadfence();
+        if (atomicAdd(&gb->count, 1u) == gridDim.x - 1) {
+            gb->count = 0;
+            __threadfence();
+            atomicAdd(&gb->gen, 1u);
+        } else {
+            const long long t0 = clock64();
+            while (*vgen == g) {
+                if (*(volatile int *)&gb->error) break;
+                if (clock64() - t0 > kBarrierTimeout) {
+                    atomicExch(&gb->error, 1);
+                    break;
+                }
+            }
+        }
+        __threadfence();
     }
-    for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
-    if (threadIdx.x == 0) p.h[j] = j < p.k ? (float)(0.5 * s) : __int_as_float(0x7f800000);
+    __syncthreads();
+    return *(volatile int *)&gb->error == 0;
 }
 
-// ---- assign -------------------------------------------------------------------
-// Tile: BM = 16*TM rows x BN clusters, thread micro-tile TM x BN/16.
+// ---- setup: row norms (the values launch_row_norms gives) and column maxima ----
+__device__ void setup_item(Problem &p, int blk, float *smax) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = threadIdx.x; t < p.d; t += NT) smax[t] = 0.f;
+    __syncthreads();
+    const long long b = (long long)blk * kAccRows, e = min(p.n, b + kAccRows);
+    for (long long r = b + warp; r < e; r += NT / 32) {
+        const float *x = p.X + r * p.d;
+        double s = 0.0;
+        for (int t = lane; t < p.d; t += 32) {
+            const float v = x[t];
+            s += (double)v * (double)v;
+            const float a = fabsf(v);
+            if (a > 0.f) atomicMax(reinterpret_cast<unsigned *>(&smax[t]), __float_as_uint(a));
+        }
+        for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+        if (lane == 0) p.xnorm[r] = (float)s;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < p.d; t += NT) {
+        const unsigned v = __float_as_uint(smax[t]);
+        if (v) atomicMax(reinterpret_cast<unsigned *>(&p.colexp[t]), v);
+    }
+    __syncthreads();
+}
+
+// E_t from the column maximum (as the Lloyd loop's exact update), sums cleared.
+__device__ void scales_item(Problem &p) {
+    for (int t = threadIdx.x; t < p.d; t += NT) {
+        const unsigned b = (unsigned)p.colexp[t];
+        const float m = __uint_as_float(b);
+        int e = 0;
+        if (b != 0u && isfinite(m)) {
+            int ex;
+            frexpf(m, &ex);
+            e = kExactMaxBits - ex;
+        }
+        p.colexp[t] = e;
+    }
+    const long long kd = (long long)p.k * p.d;
+    for (long long i = threadIdx.x; i < 3 * kd; i += NT) p.acc[i] = 0;
+    for (int j = threadIdx.x; j < p.k; j += NT) p.counts[j] = 0;
+}
+
+// ---- prep: one warp per (problem, padded cluster) ------------------------------
+// h is summed in the order of prep_centroids_kernel's 128-thread blocks (thread
+// v takes features v, v + 128, ...; four warp butterflies; warps added in order),
+// so it equals the single-problem path's half norm bit for bit.
+__device__ void prep_item(Problem &p, int j, int lane) {
+    for (int t = lane; t < p.dpad; t += 32) {
+        const float v = (j < p.k && t < p.d) ? p.C[(long long)j * p.d + t] : 0.f;
+        p.Ct[(long long)t * p.kpad + j] = v;
+    }
+    double tot = 0.0;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        double s = 0.0;
+        for (int t = 32 * w + lane; t < p.dpad; t += 128) {
+            const float v = (j < p.k && t < p.d) ? p.C[(long long)j * p.d + t] : 0.f;
+            s += (double)v * (double)v;
+        }
+        for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+        tot += s;
+    }
+    if (lane == 0) p.h[j] = j < p.k ? (float)(0.5 * tot) : __int_as_float(0x7f800000);
+}
+
+// ---- assign: BM = 16 * TM rows x BN clusters, thread micro-tile TM x BN/16 -----
 template <int BN, int TM>
-__global__ void __launch_bounds__(NT)
-assign_kernel(Problem *P, const int2 *items, int n_items) {
+__device__ void assign_tile(const Problem &p, int tile, float *smem) {
     constexpr int TN = BN / 16, BM = 16 * TM;
-    __shared__ __align__(16) float Xs[BK][BM + 4];
-    __shared__ __align__(16) float Cs[BK][BN + 4];
-    const int it = blockIdx.x;
-    if (it >= n_items) return;
-    const int2 w = items[it];  // (problem, row tile)
-    const Problem &p = P[w.x];
-    if (p.done) return;
-    const long long row0 = (long long)w.y * BM;
+    float(*Xs)[BM + 4] = reinterpret_cast<float(*)[BM + 4]>(smem);
+    float(*Cs)[BN + 4] = reinterpret_cast<float(*)[BN + 4]>(smem + BK * (BM + 4));
+    const long long row0 = (long long)tile * BM;
     const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
     float acc[TM][TN];
 #pragma unroll
@@ -148,211 +246,258 @@ assign_kernel(Problem *P, const int2 *items, int n_items) {
     }
 }
 
-// ---- accumulate -----------------------------------------------------------------
-__global__ void zero_kernel(Problem *P, const int2 *items, int n_items) {
-    const int it = blockIdx.x;
-    if (it >= n_items) return;
-    Problem &p = P[items[it].x];
-    if (p.done) return;
-    const int j = items[it].y;  // cluster
-    for (int t = threadIdx.x; t < p.d; t += blockDim.x) p.acc[(long long)j * p.d + t] = 0ull;
-    if (threadIdx.x == 0) p.counts[j] = 0;
-}
-
-__global__ void accumulate_kernel(Problem *P, const int2 *items, int n_items) {
-    extern __shared__ unsigned long long sacc[];  // k*d sums, then k counts
-    const int it = blockIdx.x;
-    if (it >= n_items) return;
-    const int2 w = items[it];  // (problem, row block)
-    Problem &p = P[w.x];
-    if (p.done) return;
-    const int kd = p.k * p.d;
-    for (int i = threadIdx.x; i < kd + p.k; i += blockDim.x) sacc[i] = 0ull;
-    __syncthreads();
-    const long long b = (long long)w.y * kAccRows, e = min(p.n, b + kAccRows);
-    const long long total = (e - b) * p.d;
-    const float *X = p.X + b * p.d;
-    for (long long q = threadIdx.x; q < total; q += blockDim.x) {
-        const long long r = q / p.d;
-        const int t = (int)(q - r * p.d);
-        const int lab = p.labels[b + r];
-        const long long v = llrint((double)X[q] * p.scale);
-        atomicAdd(&sacc[lab * p.d + t], (unsigned long long)v);
-        if (t == 0) atomicAdd(&sacc[kd + lab], 1ull);
+// The tile variants (kpad, rows per thread) the autotuner chooses from; the
+// micro-tile stays at most 64 accumulators so every variant fits 128 registers.
+__device__ __forceinline__ void assign_dispatch(const Problem &p, int tile, float *smem) {
+    switch (p.kpad * 16 + p.tm) {
+        case 16 * 16 + 2: assign_tile<16, 2>(p, tile, smem); break;
+        case 16 * 16 + 4: assign_tile<16, 4>(p, tile, smem); break;
+        case 16 * 16 + 8: assign_tile<16, 8>(p, tile, smem); break;
+        case 32 * 16 + 2: assign_tile<32, 2>(p, tile, smem); break;
+        case 32 * 16 + 4: assign_tile<32, 4>(p, tile, smem); break;
+        case 32 * 16 + 8: assign_tile<32, 8>(p, tile, smem); break;
+        case 64 * 16 + 2: assign_tile<64, 2>(p, tile, smem); break;
+        case 64 * 16 + 4: assign_tile<64, 4>(p, tile, smem); break;
+        case 64 * 16 + 8: assign_tile<64, 8>(p, tile, smem); break;
+        case 128 * 16 + 2: assign_tile<128, 2>(p, tile, smem); break;
+        case 128 * 16 + 4: assign_tile<128, 4>(p, tile, smem); break;
+        case 128 * 16 + 8: assign_tile<128, 8>(p, tile, smem); break;
+        case 256 * 16 + 2: assign_tile<256, 2>(p, tile, smem); break;
+        case 256 * 16 + 4: assign_tile<256, 4>(p, tile, smem); break;
+        default: break;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kd; i += blockDim.x)
-        if (sacc[i]) atomicAdd(&p.acc[i], sacc[i]);
-    for (int j = threadIdx.x; j < p.k; j += blockDim.x)
-        if (sacc[kd + j]) atomicAdd(&p.counts[j], (int)sacc[kd + j]);
 }
 
-// ---- finalize / decide -------------------------------------------------------------
-__global__ void finalize_kernel(Problem *P, const int2 *items, int n_items) {
-    __shared__ double red[32];
-    const int it = blockIdx.x;
-    if (it >= n_items) return;
-    Problem &p = P[items[it].x];
-    if (p.done) return;
-    const int j = items[it].y;
+// ---- accumulate: exact limb sums of a row block, a block of columns at a time ----
+// The shared accumulators hold kAccSlots (cluster, column) slots of three limbs,
+// so a pass covers kAccSlots / k columns (all of them for small k * d).
+__device__ void accumulate_item(Problem &p, int blk, long long *sacc, int *scnt) {
+    const long long b = (long long)blk * kAccRows, e = min(p.n, b + kAccRows);
+    const int rows = (int)(e - b);
+    const int k = p.k;
+    const int ct = min(p.d, max(1, kAccSlots / k));
+    const int sp = k * ct;  // slots of one limb plane
+    for (int j = threadIdx.x; j < k; j += NT) scnt[j] = 0;
+    for (int t0 = 0; t0 < p.d; t0 += ct) {
+        const int cols = min(ct, p.d - t0);
+        for (int i = threadIdx.x; i < 3 * sp; i += NT) sacc[i] = 0;
+        __syncthreads();
+        for (int q = threadIdx.x; q < rows * cols; q += NT) {
+            const int r = q / cols, c = q - r * cols;
+            const int lab = p.labels[b + r];
+            const int col = t0 + c;
+            const Limbs L = fixed_of(p.X[(b + r) * p.d + col], p.colexp[col]);
+            const int slot = lab * ct + c;
+            atomicAdd(reinterpret_cast<unsigned long long *>(&sacc[slot]), (unsigned long long)L.l0);
+            atomicAdd(reinterpret_cast<unsigned long long *>(&sacc[sp + slot]), (unsigned long long)L.l1);
+            atomicAdd(reinterpret_cast<unsigned long long *>(&sacc[2 * sp + slot]), (unsigned long long)L.l2);
+            if (t0 == 0 && c == 0) atomicAdd(&scnt[lab], 1);
+        }
+        __syncthreads();
+        const long long plane = (long long)k * p.d;
+        for (int i = threadIdx.x; i < k * cols; i += NT) {
+            const int j = i / cols, c = i - j * cols;
+            const int slot = j * ct + c;
+            const long long g = (long long)j * p.d + t0 + c;
+            const long long v0 = sacc[slot], v1 = sacc[sp + slot], v2 = sacc[2 * sp + slot];
+            if (v0) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[g]), (unsigned long long)v0);
+            if (v1) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[plane + g]), (unsigned long long)v1);
+            if (v2) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[2 * plane + g]), (unsigned long long)v2);
+        }
+        __syncthreads();
+    }
+    for (int j = threadIdx.x; j < k; j += NT)
+        if (scnt[j]) atomicAdd(&p.counts[j], scnt[j]);
+    __syncthreads();
+}
+
+// ---- finalize: one warp per (problem, cluster) ---------------------------------
+// c = F(nearest double of the 128-bit sum * 2^-E_t / count), as the Lloyd loop's
+// exact update; empty clusters keep their centroid for decide to reseed.
+__device__ void finalize_item(Problem &p, int j, int lane) {
     const int cnt = p.counts[j];
+    const long long plane = (long long)p.k * p.d;
     double a = 0.0;
-    for (int t = threadIdx.x; t < p.d; t += blockDim.x) {
+    for (int t = lane; t < p.d; t += 32) {
+        const long long g = (long long)j * p.d + t;
+        const __int128 S = ((__int128)p.acc[2 * plane + g] << 64) + ((__int128)p.acc[plane + g] << 32) +
+                           (__int128)p.acc[g];
+        p.acc[g] = 0;
+        p.acc[plane + g] = 0;
+        p.acc[2 * plane + g] = 0;
         if (cnt > 0) {
-            const double S = (double)(long long)p.acc[(long long)j * p.d + t] / p.scale;
-            const float c = (float)(S / (double)cnt);
-            const double df = (double)p.C[(long long)j * p.d + t] - (double)c;
+            const double Sd = S < 0 ? -u128_to_double((unsigned __int128)(-S)) : u128_to_double((unsigned __int128)S);
+            const float c = (float)(ldexp(Sd, -p.colexp[t]) / (double)cnt);
+            const double df = (double)p.C[g] - (double)c;
             a += df * df;
-            p.C[(long long)j * p.d + t] = c;
+            p.C[g] = c;
         }
     }
     for (int m = 16; m >= 1; m >>= 1) a += __shfl_xor_sync(0xffffffffu, a, m);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double tot = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
-        p.shift_part[j] = cnt > 0 ? tot : 0.0;
-    }
+    if (lane == 0) p.shift_part[j] = cnt > 0 ? a : 0.0;
 }
 
-// One block per problem: shift, empty-cluster reseed, stop test.
-__global__ void decide_kernel(Problem *P, int n_problems) {
-    __shared__ double sred[NT];
-    __shared__ float sv[NT];
-    __shared__ long long sr[NT];
-    __shared__ long long chosen[kMaxK];
-    const int pi = blockIdx.x;
-    if (pi >= n_problems) return;
-    Problem &p = P[pi];
-    if (p.done) return;
-    // empty clusters, ascending
+// ---- decide: one CTA per problem ------------------------------------------------
+// Empty cluster e (ascending id) takes the e-th row in (squared distance
+// descending, row ascending) order: each pick is the block argmax over the rows
+// that come after the previous pick in that order.
+__device__ void decide_item(Problem &p, double *sred, float *sv, long long *sr, GridBarrier *gb) {
     int n_empty = 0;
     for (int j = 0; j < p.k; ++j) n_empty += p.counts[j] == 0;  // uniform loop (k <= 256)
-    double shift = 0.0;
-    if (n_empty > 0) {
-        // m = n_empty farthest rows: repeated block argmax of d2 excluding chosen rows
-        int e = 0;
-        for (int j = 0; j < p.k; ++j) {
-            if (p.counts[j] != 0) continue;
-            float bv = -__int_as_float(0x7f800000);
-            long long br = 0x7fffffffffffffffll;
-            for (long long r = threadIdx.x; r < p.n; r += blockDim.x) {
-                bool taken = false;
-                for (int q = 0; q < e; ++q) taken |= chosen[q] == r;
-                const float v = p.d2[r];
-                if (!taken && (v > bv || (v == bv && r < br))) {
-                    bv = v;
-                    br = r;
+    float pv = __int_as_float(0x7f800000);
+    long long pr = -1;
+    for (int j = 0; n_empty > 0 && j < p.k; ++j) {
+        if (p.counts[j] != 0) continue;
+        float bv = -__int_as_float(0x7f800000);
+        long long br = -1;
+        for (long long r = threadIdx.x; r < p.n; r += NT) {
+            const float v = p.d2[r];
+            const bool after = v < pv || (v == pv && r > pr);
+            if (after && (br < 0 || v > bv)) {  // rows ascend per thread: first of equals kept
+                bv = v;
+                br = r;
+            }
+        }
+        sv[threadIdx.x] = bv;
+        sr[threadIdx.x] = br;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float v0 = sv[0];
+            long long r0 = sr[0];
+            for (int t = 1; t < NT; ++t) {
+                if (sr[t] < 0) continue;
+                if (r0 < 0 || sv[t] > v0 || (sv[t] == v0 && sr[t] < r0)) {
+                    v0 = sv[t];
+                    r0 = sr[t];
                 }
             }
-            sv[threadIdx.x] = bv;
-            sr[threadIdx.x] = br;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                float v0 = sv[0];
-                long long r0 = sr[0];
-                for (int t = 1; t < (int)blockDim.x; ++t)
-                    if (sv[t] > v0 || (sv[t] == v0 && sr[t] < r0)) {
-                        v0 = sv[t];
-                        r0 = sr[t];
-                    }
-                chosen[e] = r0;
-            }
-            __syncthreads();
-            const long long row = chosen[e];
-            double a = 0.0;
-            for (int t = threadIdx.x; t < p.d; t += blockDim.x) {
-                const float x = p.X[row * p.d + t];
-                const double df = (double)p.C[(long long)j * p.d + t] - (double)x;
-                a += df * df;
-                p.C[(long long)j * p.d + t] = x;
-            }
-            sred[threadIdx.x] = a;
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                double tot = 0.0;
-                for (int t = 0; t < (int)blockDim.x; ++t) tot += sred[t];
-                p.shift_part[j] = tot;
-            }
-            __syncthreads();
-            ++e;
+            sv[0] = v0;
+            sr[0] = r0;
         }
+        __syncthreads();
+        const long long row = sr[0];
+        pv = sv[0];
+        pr = row;
+        __syncthreads();
+        if (row < 0) break;  // no ordered row left (non-finite distances): keep the centroid
+        double a = 0.0;
+        for (int t = threadIdx.x; t < p.d; t += NT) {
+            const float x = p.X[row * p.d + t];
+            const double df = (double)p.C[(long long)j * p.d + t] - (double)x;
+            a += df * df;
+            p.C[(long long)j * p.d + t] = x;
+        }
+        sred[threadIdx.x] = a;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int t = 0; t < NT; ++t) tot += sred[t];
+            p.shift_part[j] = tot;
+        }
+        __syncthreads();
     }
     if (threadIdx.x == 0) {
+        double shift = 0.0;
         for (int j = 0; j < p.k; ++j) shift += p.shift_part[j];
         p.shift = shift;
         p.empty_events += n_empty;
         p.iters += 1;
-        if (shift <= p.eps || p.iters >= p.max_iters) p.done = 1;
-    }
-}
-
-// Row norms (once per call) and the per-problem fixed-point scale.
-__global__ void setup_kernel(Problem *P, const int2 *items, int n_items) {
-    const int it = blockIdx.x;
-    if (it >= n_items) return;
-    Problem &p = P[items[it].x];
-    const long long b = (long long)items[it].y * kAccRows, e = min(p.n, b + kAccRows);
-    float amax = 0.f;
-    for (long long r = b + threadIdx.x; r < e; r += blockDim.x) {
-        double s = 0.0;
-        for (int t = 0; t < p.d; ++t) {
-            const float x = p.X[r * p.d + t];
-            s += (double)x * (double)x;
-            amax = fmaxf(amax, fabsf(x));
+        if (shift <= p.eps || p.iters >= p.max_iters) {
+            p.done = 1;
+            atomicSub(&gb->active, 1);
         }
-        p.xnorm[r] = (float)s;
     }
-    for (int m = 16; m >= 1; m >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, m));
-    if ((threadIdx.x & 31) == 0) atomicMax(&p.amax_bits, __float_as_int(amax));  // non-negative floats order as ints
+    for (int j = threadIdx.x; j < p.k; j += NT) p.counts[j] = 0;
+    __syncthreads();
 }
 
-__global__ void scale_kernel(Problem *P, int n_problems) {
-    const int pi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pi >= n_problems) return;
-    Problem &p = P[pi];
-    const float amax = __int_as_float(p.amax_bits);
-    // sums stay below 2^62: |sum| <= n * amax * scale
-    const double bound = (double)p.n * (double)fmaxf(amax, 1e-30f);
-    const int e = (int)floor(62.0 - log2(bound));
-    p.scale = ldexp(1.0, min(e, 1000));
+// Dynamic shared memory: the largest phase's needs (assignment tiles, the
+// accumulate limb planes of the largest k, decide's scratch).
+size_t smem_bytes(int kmax, int dmax) {
+    const size_t assign = sizeof(float) * BK * (16 * 8 + 4 + 256 + 4);
+    const size_t acc = sizeof(long long) * 3 * kAccSlots + sizeof(int) * kmax;
+    const size_t setup = sizeof(float) * (size_t)dmax;
+    const size_t decide = (sizeof(double) + sizeof(float) + sizeof(long long)) * NT;
+    return std::max(std::max(assign, acc), std::max(setup, decide));
+}
+
+__global__ void __launch_bounds__(NT, 2) persistent_kernel(Problem *P, Lists L, GridBarrier *gb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *fsm = reinterpret_cast<float *>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (NT / 32);
+    // setup (once): column maxima accumulate in colexp, so it starts at zero
+    for (int i = blockIdx.x; i < L.n_problems; i += gridDim.x)
+        for (int t = threadIdx.x; t < P[i].d; t += NT) P[i].colexp[t] = 0;
+    if (!grid_sync(gb)) return;
+    for (int i = blockIdx.x; i < L.n_setup; i += gridDim.x) {
+        const int2 w = L.setup[i];
+        setup_item(P[w.x], w.y, fsm);
+    }
+    if (!grid_sync(gb)) return;
+    for (int i = blockIdx.x; i < L.n_problems; i += gridDim.x) scales_item(P[i]);
+    if (!grid_sync(gb)) return;
+    for (int it = 0; it < L.iterations; ++it) {
+        for (int i = blockIdx.x * (NT / 32) + warp; i < L.n_prep; i += warps) {
+            const int2 w = L.prep[i];
+            if (!P[w.x].done) prep_item(P[w.x], w.y, lane);
+        }
+        if (!grid_sync(gb)) return;
+        for (int i = blockIdx.x; i < L.n_assign; i += gridDim.x) {
+            const int2 w = L.assign[i];
+            if (!P[w.x].done) assign_dispatch(P[w.x], w.y, fsm);
+        }
+        if (!grid_sync(gb)) return;
+        for (int i = blockIdx.x; i < L.n_acc; i += gridDim.x) {
+            const int2 w = L.acc[i];
+            Problem &p = P[w.x];
+            if (!p.done) {
+                long long *sacc = reinterpret_cast<long long *>(smem_raw);
+                int *scnt = reinterpret_cast<int *>(sacc + 3 * kAccSlots);
+                accumulate_item(p, w.y, sacc, scnt);
+            }
+        }
+        if (!grid_sync(gb)) return;
+        for (int i = blockIdx.x * (NT / 32) + warp; i < L.n_fin; i += warps) {
+            const int2 w = L.fin[i];
+            if (!P[w.x].done) finalize_item(P[w.x], w.y, lane);
+        }
+        if (!grid_sync(gb)) return;
+        for (int i = blockIdx.x; i < L.n_problems; i += gridDim.x) {
+            if (P[i].done) continue;
+            double *sred = reinterpret_cast<double *>(smem_raw);
+            long long *sr = reinterpret_cast<long long *>(sred + NT);
+            float *sv = reinterpret_cast<float *>(sr + NT);
+            decide_item(P[i], sred, sv, sr, gb);
+        }
+        if (!grid_sync(gb)) return;
+        if (*(volatile int *)&gb->active == 0) break;  // read by every CTA between the same two barriers
+    }
+}
+
+// ---- autotuner ------------------------------------------------------------------
+// Times the assignment tile of one (dpad, kpad) class for each rows-per-thread
+// candidate on 32768 synthetic rows of that shape (uniform values, so the scores
+// and their ties are those of real data, not all equal).
+__global__ void tune_fill_kernel(float *p, long long count, unsigned seed) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x) {
+        unsigned x = (unsigned)i * 2654435761u ^ seed;
+        x ^= x >> 15;
+        x *= 2246822519u;
+        x ^= x >> 13;
+        p[i] = (float)(x & 0xffffff) * (1.0f / 16777216.0f) * 4.0f - 2.0f;
+    }
+}
+
+__global__ void __launch_bounds__(NT, 2) tune_assign_kernel(const Problem *pp, int tiles) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Problem p = *pp;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) assign_dispatch(p, t, reinterpret_cast<float *>(smem_raw));
 }
 
 }  // namespace batched
 
-// ---- host side ------------------------------------------------------------------------
-
-struct BatchedPlan {
-    std::vector<batched::Problem> host;
-    batched::Problem *dev = nullptr;
-    std::vector<std::vector<int2>> assign_items;  // per variant
-    std::vector<int> variant_bn, variant_tm;
-    int2 *d_items = nullptr;
-    std::vector<size_t> assign_off;  // offsets into d_items per variant
-    size_t prep_off = 0, zero_off = 0, acc_off = 0;
-    int n_prep = 0, n_zero = 0, n_acc = 0;
-    size_t acc_smem = 0;
-};
-
-typedef void (*AssignFn)(batched::Problem *, const int2 *, int);
-
-static AssignFn assign_fn(int bn, int tm) {
-    using namespace batched;
-    switch (bn * 10 + tm) {
-        case 164: return assign_kernel<16, 4>;
-        case 168: return assign_kernel<16, 8>;
-        case 324: return assign_kernel<32, 4>;
-        case 328: return assign_kernel<32, 8>;
-        case 644: return assign_kernel<64, 4>;
-        case 648: return assign_kernel<64, 8>;
-        case 1284: return assign_kernel<128, 4>;
-        case 1288: return assign_kernel<128, 8>;
-        case 2564: return assign_kernel<256, 4>;
-        case 2568: return assign_kernel<256, 8>;
-    }
-    return nullptr;
-}
+namespace {
 
 int batched_kpad(int k) {
     int b = 16;
@@ -360,77 +505,79 @@ int batched_kpad(int k) {
     return b;
 }
 
-}  // namespace kmb
+std::mutex g_tune_mu;
+std::map<long long, int> g_tuned;  // (device, dpad, kpad) -> rows per thread
 
-#include <cstring>
-
-namespace kmb {
-
-// Autotuner cache: (d, kpad) -> rows per thread (4 or 8), per device.
-static std::map<long long, int> g_tuned;
-
-static int tuned_tm(int dev, int d, int kpad, cudaStream_t s) {
-    const long long key = ((long long)dev << 40) | ((long long)d << 16) | kpad;
-    auto it = g_tuned.find(key);
-    if (it != g_tuned.end()) return it->second;
-    // Time both candidates on 64K synthetic rows of this shape.
+int tuned_tm(int dev, int dpad, int kpad, cudaStream_t s) {
     using namespace batched;
-    const long long n = 65536;
-    const int dpad = (d + 7) / 8 * 8;
+    const long long key = ((long long)dev << 40) | ((long long)dpad << 16) | kpad;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto found = g_tuned.find(key);
+    if (found != g_tuned.end()) return found->second;
+    const std::vector<int> cands = kpad >= 256 ? std::vector<int>{2, 4} : std::vector<int>{2, 4, 8};
+    const long long n = 32768;
     float *X = nullptr, *Ct = nullptr, *h = nullptr, *d2 = nullptr, *xn = nullptr;
     int32_t *lab = nullptr;
     Problem *dp = nullptr;
-    int2 *items = nullptr;
-    int best_tm = 8;
-    if (cudaMalloc(&X, sizeof(float) * n * d) == cudaSuccess && cudaMalloc(&Ct, sizeof(float) * dpad * kpad) == cudaSuccess &&
-        cudaMalloc(&h, sizeof(float) * kpad) == cudaSuccess && cudaMalloc(&d2, sizeof(float) * n) == cudaSuccess &&
-        cudaMalloc(&xn, sizeof(float) * n) == cudaSuccess && cudaMalloc(&lab, sizeof(int32_t) * n) == cudaSuccess &&
-        cudaMalloc(&dp, sizeof(Problem)) == cudaSuccess && cudaMalloc(&items, sizeof(int2) * (n / 64)) == cudaSuccess) {
-        cudaMemsetAsync(X, 0, sizeof(float) * n * d, s);
-        cudaMemsetAsync(Ct, 0, sizeof(float) * dpad * kpad, s);
-        cudaMemsetAsync(h, 0, sizeof(float) * kpad, s);
-        cudaMemsetAsync(xn, 0, sizeof(float) * n, s);
-        Problem p;
-        std::memset(&p, 0, sizeof(p));
-        p.X = X; p.Ct = Ct; p.h = h; p.labels = lab; p.d2 = d2; p.xnorm = xn;
-        p.n = n; p.d = d; p.dpad = dpad; p.k = kpad; p.kpad = kpad;
-        cudaMemcpyAsync(dp, &p, sizeof(p), cudaMemcpyHostToDevice, s);
+    int best_tm = 4;
+    cudaEvent_t a = nullptr, b = nullptr;
+    bool ok = cudaMallocAsync(&X, sizeof(float) * n * dpad, s) == cudaSuccess &&
+              cudaMallocAsync(&Ct, sizeof(float) * dpad * kpad, s) == cudaSuccess &&
+              cudaMallocAsync(&h, sizeof(float) * kpad, s) == cudaSuccess &&
+              cudaMallocAsync(&d2, sizeof(float) * n, s) == cudaSuccess &&
+              cudaMallocAsync(&xn, sizeof(float) * n, s) == cudaSuccess &&
+              cudaMallocAsync(&lab, sizeof(int32_t) * n, s) == cudaSuccess &&
+              cudaMallocAsync(&dp, sizeof(Problem), s) == cudaSuccess && cudaEventCreate(&a) == cudaSuccess &&
+              cudaEventCreate(&b) == cudaSuccess;
+    if (ok) {
+        tune_fill_kernel<<<256, 256, 0, s>>>(X, n * dpad, 1u);
+        tune_fill_kernel<<<64, 256, 0, s>>>(Ct, (long long)dpad * kpad, 2u);
+        tune_fill_kernel<<<1, 256, 0, s>>>(h, kpad, 3u);
+        tune_fill_kernel<<<64, 256, 0, s>>>(xn, n, 4u);
+        launch_count() += 4;
+        const size_t smem = smem_bytes(kpad, 1);
+        cudaFuncSetAttribute(tune_assign_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         float best_ms = 1e30f;
-        for (int tm : {4, 8}) {
-            const int bm = 16 * tm;
-            const int nit = (int)((n + bm - 1) / bm);
-            std::vector<int2> hv(nit);
-            for (int i = 0; i < nit; ++i) hv[i] = make_int2(0, i);
-            cudaMemcpyAsync(items, hv.data(), sizeof(int2) * nit, cudaMemcpyHostToDevice, s);
-            AssignFn f = assign_fn(kpad, tm);
-            cudaEvent_t a, b;
-            cudaEventCreate(&a);
-            cudaEventCreate(&b);
-            f<<<nit, NT, 0, s>>>(dp, items, nit);  // warm-up
-            KMB_LAUNCHED();
+        for (int tm : cands) {
+            Problem p;
+            std::memset(&p, 0, sizeof(p));
+            p.X = X;
+            p.Ct = Ct;
+            p.h = h;
+            p.labels = lab;
+            p.d2 = d2;
+            p.xnorm = xn;
+            p.n = n;
+            p.d = dpad;
+            p.dpad = dpad;
+            p.k = kpad;
+            p.kpad = kpad;
+            p.tm = tm;
+            cudaMemcpyAsync(dp, &p, sizeof(p), cudaMemcpyHostToDevice, s);
+            const int tiles = (int)((n + 16 * tm - 1) / (16 * tm));
+            tune_assign_kernel<<<std::min(tiles, 296), NT, smem, s>>>(dp, tiles);  // warm-up
             cudaEventRecord(a, s);
-            for (int r = 0; r < 5; ++r) {
-                f<<<nit, NT, 0, s>>>(dp, items, nit);
-                KMB_LAUNCHED();
-            }
+            for (int r = 0; r < 3; ++r) tune_assign_kernel<<<std::min(tiles, 296), NT, smem, s>>>(dp, tiles);
             cudaEventRecord(b, s);
-            cudaEventSynchronize(b);
+            launch_count() += 4;
             float ms = 0.f;
-            cudaEventElapsedTime(&ms, a, b);
-            cudaEventDestroy(a);
-            cudaEventDestroy(b);
-            if (ms < best_ms) {
+            if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess &&
+                ms < best_ms) {
                 best_ms = ms;
                 best_tm = tm;
             }
         }
     }
+    for (void *q : {(void *)X, (void *)Ct, (void *)h, (void *)d2, (void *)xn, (void *)lab, (void *)dp})
+        if (q) cudaFreeAsync(q, s);
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
     cudaGetLastError();
-    cudaFree(X); cudaFree(Ct); cudaFree(h); cudaFree(d2); cudaFree(xn); cudaFree(lab); cudaFree(dp); cudaFree(items);
     g_tuned[key] = best_tm;
     return best_tm;
 }
 
+}  // namespace
 }  // namespace kmb
 
 extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64_t count, int64_t max_iteration_count,
@@ -438,45 +585,52 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
                                  kmb_batched_info *info) {
     using namespace kmb;
     using namespace kmb::batched;
-    if (dtype != KMB_F32 || !problems || count <= 0 || max_iteration_count < 0 || !(accuracy_threshold >= 0))
+    if (dtype != KMB_F32 || !problems || count <= 0 || count > INT32_MAX || max_iteration_count < 0 ||
+        max_iteration_count > INT32_MAX || !(accuracy_threshold >= 0))
         return KMB_EINVAL;
+    int kmax = 1, dmax = 1;
     for (int64_t i = 0; i < count; ++i) {
         const kmb_batched_problem &q = problems[i];
-        if (!q.X || !q.C || !q.labels || q.n <= 0 || q.n > INT32_MAX || q.d <= 0 || q.k <= 0 || q.k > kMaxK ||
-            q.k > q.n || (q.k * q.d + q.k) * 8 > 200 * 1024)
+        if (!q.X || !q.C || !q.labels || q.n <= 0 || q.n > INT32_MAX || q.d <= 0 || q.d > INT32_MAX / 4 || q.k <= 0 ||
+            q.k > kMaxK || q.k > q.n || (q.k * q.d + q.k) * 8 > 200 * 1024)
             return KMB_EINVAL;
+        kmax = std::max(kmax, (int)q.k);
+        dmax = std::max(dmax, (int)q.d);
     }
     cudaStream_t s = (cudaStream_t)cuda_stream;
-    int dev = 0;
+    int dev = 0, sms = 148;
     cudaGetDevice(&dev);
-    // Device allocations: per-problem scratch in one arena.
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // Per-problem scratch in one stream-ordered arena (no device-wide synchronisation).
     size_t arena = 0;
-    std::vector<size_t> off(count * 8);
     auto take = [&](size_t bytes) {
         const size_t o = arena;
         arena += (bytes + 255) / 256 * 256;
         return o;
     };
     std::vector<Problem> H(count);
+    std::vector<size_t> off((size_t)count * 8);
     for (int64_t i = 0; i < count; ++i) {
         const kmb_batched_problem &q = problems[i];
         const int kpad = batched_kpad((int)q.k), dpad = (int)((q.d + 7) / 8 * 8);
         off[i * 8 + 0] = take(sizeof(float) * dpad * kpad);
         off[i * 8 + 1] = take(sizeof(float) * kpad);
-        off[i * 8 + 2] = take(sizeof(float) * q.n);       // d2
-        off[i * 8 + 3] = take(sizeof(float) * q.n);       // xnorm
-        off[i * 8 + 4] = take(sizeof(unsigned long long) * q.k * q.d);
+        off[i * 8 + 2] = take(sizeof(float) * q.n);
+        off[i * 8 + 3] = take(sizeof(float) * q.n);
+        off[i * 8 + 4] = take(sizeof(long long) * 3 * q.k * q.d);
         off[i * 8 + 5] = take(sizeof(int) * q.k);
         off[i * 8 + 6] = take(sizeof(double) * q.k);
+        off[i * 8 + 7] = take(sizeof(int) * q.d);
     }
+    const size_t bar_off = take(sizeof(GridBarrier));
     unsigned char *base = nullptr;
-    if (cudaMalloc(&base, arena) != cudaSuccess) {
+    if (cudaMallocAsync(&base, arena, s) != cudaSuccess) {
         cudaGetLastError();
         return KMB_ENOMEM;
     }
-    std::vector<int2> prep_items, zero_items, acc_items;
-    std::map<long long, std::vector<int2>> assign_by_variant;  // key bn*10+tm
-    size_t acc_smem = 0;
+    std::vector<int2> setup, prep, assign, acc, fin;
+    std::vector<double> assign_cost;
+    std::map<long long, int> classes;  // (kpad, tm) variants in use
     for (int64_t i = 0; i < count; ++i) {
         const kmb_batched_problem &q = problems[i];
         Problem &p = H[i];
@@ -489,100 +643,130 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         p.dpad = (int)((q.d + 7) / 8 * 8);
         p.k = (int)q.k;
         p.kpad = batched_kpad(p.k);
+        p.tm = tuned_tm(dev, p.dpad, p.kpad, s);
         p.Ct = (float *)(base + off[i * 8 + 0]);
         p.h = (float *)(base + off[i * 8 + 1]);
         p.d2 = (float *)(base + off[i * 8 + 2]);
         p.xnorm = (float *)(base + off[i * 8 + 3]);
-        p.acc = (unsigned long long *)(base + off[i * 8 + 4]);
+        p.acc = (long long *)(base + off[i * 8 + 4]);
         p.counts = (int *)(base + off[i * 8 + 5]);
         p.shift_part = (double *)(base + off[i * 8 + 6]);
-        p.scale = 0.0;
+        p.colexp = (int *)(base + off[i * 8 + 7]);
         p.max_iters = (int)max_iteration_count;
         p.eps = accuracy_threshold;
         p.done = max_iteration_count == 0 ? 1 : 0;
-        for (int j = 0; j < p.kpad; ++j) prep_items.push_back(make_int2((int)i, j));
-        for (int j = 0; j < p.k; ++j) zero_items.push_back(make_int2((int)i, j));
-        const int tm = tuned_tm(dev, p.d, p.kpad, s);
-        const int bm = 16 * tm;
-        auto &v = assign_by_variant[(long long)p.kpad * 10 + tm];
-        for (long long t = 0; t < (p.n + bm - 1) / bm; ++t) v.push_back(make_int2((int)i, (int)t));
-        for (long long b = 0; b < (p.n + kAccRows - 1) / kAccRows; ++b) acc_items.push_back(make_int2((int)i, (int)b));
-        acc_smem = std::max(acc_smem, sizeof(unsigned long long) * (size_t)(p.k * p.d + p.k));
+        classes[(long long)p.kpad * 16 + p.tm] = 1;
+        for (long long b = 0; b < (p.n + kAccRows - 1) / kAccRows; ++b) {
+            setup.push_back(make_int2((int)i, (int)b));
+            acc.push_back(make_int2((int)i, (int)b));
+        }
+        for (int j = 0; j < p.kpad; ++j) prep.push_back(make_int2((int)i, j));
+        for (int j = 0; j < p.k; ++j) fin.push_back(make_int2((int)i, j));
+        const int bm = 16 * p.tm;
+        for (long long t = 0; t < (p.n + bm - 1) / bm; ++t) {
+            assign.push_back(make_int2((int)i, (int)t));
+            assign_cost.push_back((double)std::min<long long>(bm, p.n - t * bm) * p.kpad * p.dpad);
+        }
     }
-    // one items array: prep | zero | acc | assign variants
+    // largest assignment tiles first (round-robin over the grid then balances well)
+    {
+        std::vector<size_t> order(assign.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return assign_cost[a] > assign_cost[b]; });
+        std::vector<int2> sorted(assign.size());
+        for (size_t i = 0; i < order.size(); ++i) sorted[i] = assign[order[i]];
+        assign.swap(sorted);
+    }
     std::vector<int2> all;
-    const size_t prep_off = all.size();
-    all.insert(all.end(), prep_items.begin(), prep_items.end());
-    const size_t zero_off = all.size();
-    all.insert(all.end(), zero_items.begin(), zero_items.end());
-    const size_t acc_off = all.size();
-    all.insert(all.end(), acc_items.begin(), acc_items.end());
-    std::vector<std::pair<long long, std::pair<size_t, int>>> variants;
-    for (auto &kv : assign_by_variant) {
-        variants.push_back({kv.first, {all.size(), (int)kv.second.size()}});
-        all.insert(all.end(), kv.second.begin(), kv.second.end());
-    }
+    auto put = [&](const std::vector<int2> &v) {
+        const size_t o = all.size();
+        all.insert(all.end(), v.begin(), v.end());
+        return o;
+    };
+    const size_t o_setup = put(setup), o_prep = put(prep), o_assign = put(assign), o_acc = put(acc), o_fin = put(fin);
     Problem *dP = nullptr;
     int2 *dI = nullptr;
-    if (cudaMalloc(&dP, sizeof(Problem) * count) != cudaSuccess || cudaMalloc(&dI, sizeof(int2) * all.size()) != cudaSuccess) {
+    if (cudaMallocAsync(&dP, sizeof(Problem) * count, s) != cudaSuccess ||
+        cudaMallocAsync(&dI, sizeof(int2) * all.size(), s) != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(base);
-        cudaFree(dP);
+        if (dP) cudaFreeAsync(dP, s);
+        cudaFreeAsync(base, s);
         return KMB_ENOMEM;
     }
-    cudaMemcpyAsync(dP, H.data(), sizeof(Problem) * count, cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(dI, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s);
-    if (acc_smem > 48 * 1024)
-        cudaFuncSetAttribute(accumulate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)acc_smem);
-    setup_kernel<<<(unsigned)acc_items.size(), NT, 0, s>>>(dP, dI + acc_off, (int)acc_items.size());
-    KMB_LAUNCHED();
-    scale_kernel<<<(unsigned)((count + 127) / 128), 128, 0, s>>>(dP, (int)count);
-    KMB_LAUNCHED();
-
-    auto enqueue_iteration = [&](cudaStream_t st) {
-        prep_kernel<<<(unsigned)prep_items.size(), 32, 0, st>>>(dP, dI + prep_off, (int)prep_items.size());
-        for (auto &v : variants) {
-            const int bn = (int)(v.first / 10), tm = (int)(v.first % 10);
-            assign_fn(bn, tm)<<<(unsigned)v.second.second, NT, 0, st>>>(dP, dI + v.second.first, v.second.second);
-        }
-        zero_kernel<<<(unsigned)zero_items.size(), 64, 0, st>>>(dP, dI + zero_off, (int)zero_items.size());
-        accumulate_kernel<<<(unsigned)acc_items.size(), NT, acc_smem, st>>>(dP, dI + acc_off, (int)acc_items.size());
-        finalize_kernel<<<(unsigned)zero_items.size(), 64, 0, st>>>(dP, dI + zero_off, (int)zero_items.size());
-        decide_kernel<<<(unsigned)count, NT, 0, st>>>(dP, (int)count);
-    };
-    const int per_iter = 5 + (int)variants.size();
+    GridBarrier *gb = (GridBarrier *)(base + bar_off);
+    GridBarrier gb_init;
+    std::memset(&gb_init, 0, sizeof(gb_init));
+    for (int64_t i = 0; i < count; ++i) gb_init.active += H[i].done ? 0 : 1;
     int rc = KMB_OK;
-    cudaGraphExec_t exec = nullptr;
-    cudaGraph_t graph = nullptr;
-    if (use_graph && max_iteration_count > 0) {
-        // Capture on a private stream (the caller's may be the legacy default
-        // stream, which cannot be captured); the graph is then launched on the
-        // caller's stream, after the setup work above.
+    if (cudaMemcpyAsync(dP, H.data(), sizeof(Problem) * count, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dI, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(gb, &gb_init, sizeof(GridBarrier), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        rc = KMB_ECUDA;
+
+    Lists L;
+    L.setup = dI + o_setup;
+    L.n_setup = (int)setup.size();
+    L.prep = dI + o_prep;
+    L.n_prep = (int)prep.size();
+    L.assign = dI + o_assign;
+    L.n_assign = (int)assign.size();
+    L.acc = dI + o_acc;
+    L.n_acc = (int)acc.size();
+    L.fin = dI + o_fin;
+    L.n_fin = (int)fin.size();
+    L.n_problems = (int)count;
+    L.iterations = (int)max_iteration_count;
+    const size_t smem = smem_bytes(kmax, dmax);
+    int per_sm = 0;
+    if (rc == KMB_OK &&
+        (cudaFuncSetAttribute(persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_kernel, NT, smem) != cudaSuccess ||
+         per_sm < 1))
+        rc = KMB_EUNSUPPORTED;
+    const int grid = std::max(1, per_sm) * sms;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.gridDim = dim3((unsigned)grid, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    bool graphed = false;
+    if (rc == KMB_OK && use_graph) {
+        // one cooperative kernel node, captured on a private stream (the caller's
+        // may be the legacy default stream) and launched on the caller's
         cudaStream_t cap = nullptr;
-        if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            rc = KMB_ECUDA;
-        if (rc == KMB_OK) {
-            enqueue_iteration(cap);
-            if (cudaStreamEndCapture(cap, &graph) != cudaSuccess ||
-                cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
-                rc = KMB_ECUDA;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            cfg.stream = cap;
+            const cudaError_t le = cudaLaunchKernelEx(&cfg, persistent_kernel, dP, L, gb);
+            const cudaError_t ce = cudaStreamEndCapture(cap, &graph);
+            if (le == cudaSuccess && ce == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess &&
+                cudaGraphLaunch(exec, s) == cudaSuccess)
+                graphed = true;
         }
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
         if (cap) cudaStreamDestroy(cap);
-        if (rc != KMB_OK) cudaGetLastError();
-        for (int64_t it = 0; rc == KMB_OK && it < max_iteration_count; ++it) {
-            if (cudaGraphLaunch(exec, s) != cudaSuccess) rc = KMB_ECUDA;
-            launch_count() += per_iter;
-        }
-    } else {
-        for (int64_t it = 0; it < max_iteration_count; ++it) {
-            enqueue_iteration(s);
-            launch_count() += per_iter;
-        }
     }
+    if (rc == KMB_OK && !graphed) {
+        cfg.stream = s;
+        if (cudaLaunchKernelEx(&cfg, persistent_kernel, dP, L, gb) != cudaSuccess) rc = KMB_ECUDA;
+    }
+    if (rc == KMB_OK) KMB_LAUNCHED();
+    GridBarrier hb;
+    std::memset(&hb, 0, sizeof(hb));
+    if (rc == KMB_OK && (cudaMemcpyAsync(H.data(), dP, sizeof(Problem) * count, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                         cudaMemcpyAsync(&hb, gb, sizeof(hb), cudaMemcpyDeviceToHost, s) != cudaSuccess))
+        rc = KMB_ECUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = KMB_ECUDA;
+    if (rc == KMB_OK && hb.error) rc = KMB_ETIMEDOUT;
     if (rc == KMB_OK) {
-        cudaMemcpy(H.data(), dP, sizeof(Problem) * count, cudaMemcpyDeviceToHost);
         long long total_iters = 0;
         for (int64_t i = 0; i < count; ++i) {
             problems[i].iterations = H[i].iters;
@@ -591,15 +775,13 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         }
         if (info) {
             info->problems = count;
-            info->variants = (int32_t)variants.size();
+            info->variants = (int32_t)classes.size();
             info->total_iterations = total_iters;
-            info->graph_launches = use_graph ? max_iteration_count : 0;
+            info->graph_launches = graphed ? 1 : 0;
         }
     }
-    if (exec) cudaGraphExecDestroy(exec);
-    if (graph) cudaGraphDestroy(graph);
-    cudaFree(dP);
-    cudaFree(dI);
-    cudaFree(base);
+    cudaFreeAsync(dP, s);
+    cudaFreeAsync(dI, s);
+    cudaFreeAsync(base, s);
     return rc;
 }

@@ -242,6 +242,54 @@ void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const
                    Workspace &ws, LoopState *st, bool commit, cudaStream_t s, const CsrRows *csr = nullptr,
                    F *exact_d2 = nullptr);
 
+// ---- exact fixed-point sums (shared by the Lloyd update and the batched form) ----
+// A value x of column t is the integer v = round(x * 2^E_t), |v| < 2^94, E_t =
+// 94 - (exponent of the column's largest |x|); v is handled as three 32-bit
+// limbs, v = l2 * 2^64 + l1 * 2^32 + l0 (l0, l1 in [0, 2^32), l2 signed), so limb
+// sums in int64 add and subtract rows exactly in any order.
+constexpr int kExactMaxBits = 94;  // |round(x * 2^E_t)| < 2^94
+
+struct Limbs {
+    long long l0, l1, l2;
+};
+
+__device__ __forceinline__ Limbs fixed_of(float x, int e) {
+    const float f = scalbnf(x, e);  // exact: |f| < 2^94, a power-of-two scaling
+    const unsigned bits = __float_as_uint(f);
+    const int be = (int)((bits >> 23) & 0xffu);
+    unsigned long long mant = bits & 0x7fffffu;
+    if (be) mant |= 0x800000u;
+    const int sh = (be ? be : 1) - 150;  // f = mant * 2^sh
+    unsigned __int128 mag = 0;
+    if (sh >= 0) {
+        mag = (unsigned __int128)mant << sh;
+    } else if (sh > -26) {
+        const int r = -sh;  // round half to even
+        const unsigned long long q = mant >> r, rem = mant & ((1ull << r) - 1), half = 1ull << (r - 1);
+        mag = q + ((rem > half || (rem == half && (q & 1ull))) ? 1ull : 0ull);
+    }
+    const __int128 v = (bits >> 31) ? -(__int128)mag : (__int128)mag;
+    Limbs L;
+    L.l0 = (long long)(v & 0xffffffffll);
+    L.l1 = (long long)((v >> 32) & 0xffffffffll);
+    L.l2 = (long long)(v >> 64);
+    return L;
+}
+
+// The nearest double to |m| (round half to even), m < 2^127.
+__device__ __forceinline__ double u128_to_double(unsigned __int128 m) {
+    const unsigned long long hi = (unsigned long long)(m >> 64), lo = (unsigned long long)m;
+    if (hi == 0 && lo < (1ull << 53)) return (double)lo;
+    const int top = hi ? 127 - __clzll((long long)hi) : 63 - __clzll((long long)lo);
+    const int sh = top - 52;
+    unsigned long long q = (unsigned long long)(m >> sh);
+    const unsigned __int128 rem = m & (((unsigned __int128)1 << sh) - 1);
+    const unsigned __int128 half = (unsigned __int128)1 << (sh - 1);
+    if (rem > half || (rem == half && (q & 1ull))) ++q;
+    return ldexp((double)q, sh);
+}
+
+
 // The exact update of FP32 rows (the Lloyd loop's update for float data). Every
 // value x of column t is taken as the integer round(x * 2^E_t), E_t chosen once
 // per call so that the column's largest |x| stays below 2^94 (every float within
