@@ -80,12 +80,15 @@ struct Lists {
 struct GridBarrier {
     unsigned count;
     unsigned gen;
-    int error;
+    int error;   // 1: a barrier wait ran out; 2: an invalid label reached the accumulation
     int active;  // problems not yet converged
 };
 
-// Grid-wide barrier of a cooperative launch; false once any CTA gave up waiting.
+// Grid-wide barrier of a cooperative launch; false once any CTA gave up waiting
+// (or flagged an error). Thread 0 decides and the CTA follows its decision, so
+// every thread of a CTA takes the same path.
 __device__ __forceinline__ bool grid_sync(GridBarrier *gb) {
+    __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned *vgen = &gb->gen;
@@ -106,9 +109,10 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *gb) {
             }
         }
         __threadfence();
+        s_ok = *(volatile int *)&gb->error == 0;
     }
     __syncthreads();
-    return *(volatile int *)&gb->error == 0;
+    return s_ok != 0;
 }
 
 // ---- setup: row norms (the values launch_row_norms gives) and column maxima ----
@@ -271,7 +275,7 @@ __device__ __forceinline__ void assign_dispatch(const Problem &p, int tile, floa
 // ---- accumulate: exact limb sums of a row block, a block of columns at a time ----
 // The shared accumulators hold kAccSlots (cluster, column) slots of three limbs,
 // so a pass covers kAccSlots / k columns (all of them for small k * d).
-__device__ void accumulate_item(Problem &p, int blk, long long *sacc, int *scnt) {
+__device__ void accumulate_item(Problem &p, int blk, long long *sacc, int *scnt, GridBarrier *gb) {
     const long long b = (long long)blk * kAccRows, e = min(p.n, b + kAccRows);
     const int rows = (int)(e - b);
     const int k = p.k;
@@ -285,6 +289,10 @@ __device__ void accumulate_item(Problem &p, int blk, long long *sacc, int *scnt)
         for (int q = threadIdx.x; q < rows * cols; q += NT) {
             const int r = q / cols, c = q - r * cols;
             const int lab = p.labels[b + r];
+            if ((unsigned)lab >= (unsigned)k) {  // cannot happen: the assignment writes every row
+                atomicExch(&gb->error, 2);
+                continue;
+            }
             const int col = t0 + c;
             const Limbs L = fixed_of(p.X[(b + r) * p.d + col], p.colexp[col]);
             const int slot = lab * ct + c;
@@ -379,7 +387,7 @@ __device__ void decide_item(Problem &p, double *sred, float *sv, long long *sr, 
         pv = sv[0];
         pr = row;
         __syncthreads();
-        if (row < 0) break;  // no ordered row left (non-finite distances): keep the centroid
+        if (row < 0 || row >= p.n) break;  // no ordered row left (non-finite distances): keep the centroid
         double a = 0.0;
         for (int t = threadIdx.x; t < p.d; t += NT) {
             const float x = p.X[row * p.d + t];
@@ -396,6 +404,9 @@ __device__ void decide_item(Problem &p, double *sred, float *sv, long long *sr, 
         }
         __syncthreads();
     }
+    // every thread is past its reads of counts (the loop above skips non-empty
+    // clusters without a barrier) before they are cleared below
+    __syncthreads();
     if (threadIdx.x == 0) {
         double shift = 0.0;
         for (int j = 0; j < p.k; ++j) shift += p.shift_part[j];
@@ -454,7 +465,7 @@ __global__ void __launch_bounds__(NT, 2) persistent_kernel(Problem *P, Lists L, 
             if (!p.done) {
                 long long *sacc = reinterpret_cast<long long *>(smem_raw);
                 int *scnt = reinterpret_cast<int *>(sacc + 3 * kAccSlots);
-                accumulate_item(p, w.y, sacc, scnt);
+                accumulate_item(p, w.y, sacc, scnt, gb);
             }
         }
         if (!grid_sync(gb)) return;
@@ -765,7 +776,7 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
                          cudaMemcpyAsync(&hb, gb, sizeof(hb), cudaMemcpyDeviceToHost, s) != cudaSuccess))
         rc = KMB_ECUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = KMB_ECUDA;
-    if (rc == KMB_OK && hb.error) rc = KMB_ETIMEDOUT;
+    if (rc == KMB_OK && hb.error) rc = hb.error == 1 ? KMB_ETIMEDOUT : KMB_ECUDA;
     if (rc == KMB_OK) {
         long long total_iters = 0;
         for (int64_t i = 0; i < count; ++i) {
