@@ -476,9 +476,20 @@ def run_serving(args, device=0):
                 "train_p50_ms": float(np.percentile([lat[i] for i, r in enumerate(reqs) if r[0] == "train"] or [0],
                                                     50) * 1e3)}
 
+    def unloaded(srv, ids, reqs):
+        """Each infer request alone on the idle server (submit, wait, next): the latency
+        floor of the request mix, with no queueing and no sharing of the device."""
+        lat = []
+        for kind, m, X in reqs:
+            if kind == "infer":
+                lat.append(srv.wait(srv.submit_infer(ids[m], X), timeout=600)[1])
+        return {"requests": len(lat), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3)}
+
     with KMeansServer(device=device, hbm_budget_bytes=60 << 30, lanes=args.serving_lanes, trainers=6) as srv:
         ids = [srv.add_model(C) for C in models]
         run_point(srv, ids, make_requests(200, 1), None)  # warm-up
+        floor = unloaded(srv, ids, make_requests(max(args.serving_requests // 10, 200), 9))
         sat = run_point(srv, ids, make_requests(args.serving_requests, 2), None)
         points = []
         for frac in (0.5, 0.8):
@@ -488,7 +499,8 @@ def run_serving(args, device=0):
             pt["fraction_of_saturation"] = frac
             points.append(pt)
         st = srv.stats()
-    return {"saturation_rps": sat["throughput_rps"], "saturation_p99_ms": sat["p99_ms"], "points": points,
+    return {"saturation_rps": sat["throughput_rps"], "saturation_p99_ms": sat["p99_ms"], "unloaded": floor,
+            "points": points,
             "models": n_models, "budget_bytes": 60 << 30, "lanes": args.serving_lanes, "trainers": 6,
             "mean_requests_per_batch": st["batched_requests"] / max(st["batches"], 1),
             "peak_in_use_bytes": st["peak_in_use_bytes"],

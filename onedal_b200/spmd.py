@@ -81,17 +81,20 @@ class DeviceShardOps:
         return C_new, shift.value, empty[: ne.value].cpu().tolist()
 
     def rows(self, local_idx):
-        return self.X[torch.as_tensor(local_idx, device=self.X.device, dtype=torch.long)]
+        return self.X[local_idx.to(device=self.X.device, dtype=torch.long)]
 
 
 def _top_candidates(row_sq: torch.Tensor, m: int, row_offset: int):
-    """This rank's m largest squared distances, (value desc, global row asc)."""
+    """This rank's m largest squared distances in (value descending, global row
+    ascending) order, computed where row_sq lives: the distances are not copied to
+    the host. NaN distances order last (as -inf)."""
     n = row_sq.shape[0]
     take = min(m, n)
-    v = row_sq.double().cpu().numpy()
-    order = np.lexsort((np.arange(n), -v))[:take]  # primary: value desc, secondary: row asc
-    vals = np.full(m, -np.inf)
-    rows = np.full(m, np.iinfo(np.int64).max, dtype=np.int64)
+    v = torch.nan_to_num(row_sq.to(torch.float64), nan=float("-inf"))
+    # a stable descending sort keeps equal values in ascending row order
+    order = torch.sort(v, descending=True, stable=True).indices[:take]
+    vals = torch.full((m,), float("-inf"), dtype=torch.float64, device=row_sq.device)
+    rows = torch.full((m,), np.iinfo(np.int64).max, dtype=torch.int64, device=row_sq.device)
     vals[:take] = v[order]
     rows[:take] = order + row_offset
     return vals, rows, order
@@ -137,8 +140,8 @@ def train_spmd(ops, C0: torch.Tensor, max_iteration_count: int, accuracy_thresho
             payload_rows = torch.zeros((m, d), dtype=C.dtype, device=dev)
             if len(local):
                 payload_rows[: len(local)] = ops.rows(local).to(C.dtype)
-            v_t = torch.tensor(vals, dtype=torch.float64, device=dev)
-            r_t = torch.tensor(rows, dtype=torch.int64, device=dev)
+            v_t = vals.to(dev)
+            r_t = rows.to(dev)
             gv = [torch.empty_like(v_t) for _ in range(world)]
             gr = [torch.empty_like(r_t) for _ in range(world)]
             gx = [torch.empty_like(payload_rows) for _ in range(world)]

@@ -46,7 +46,7 @@ class NumpyShardOps:
         return torch.from_numpy(out), shift, [int(i) for i in np.nonzero(~nz)[0]]
 
     def rows(self, idx):
-        return self.X[torch.as_tensor(idx, dtype=torch.long)]
+        return self.X[idx.to(torch.long)]
 
 
 def _free_port():
