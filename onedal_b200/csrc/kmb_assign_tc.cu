@@ -365,6 +365,88 @@ __device__ __forceinline__ void named_bar_sync(int id, int count) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
+// Waits for this thread's tcgen05.ld; v is tied to the wait, so no use of v can
+// be scheduled above it.
+__device__ __forceinline__ void tmem_wait_ld_regs(float (&v)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]),
+                   "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]),
+                   "+f"(v[15]), "+f"(v[16]), "+f"(v[17]), "+f"(v[18]), "+f"(v[19]), "+f"(v[20]), "+f"(v[21]),
+                   "+f"(v[22]), "+f"(v[23]), "+f"(v[24]), "+f"(v[25]), "+f"(v[26]), "+f"(v[27]), "+f"(v[28]),
+                   "+f"(v[29]), "+f"(v[30]), "+f"(v[31])
+                 :
+                 : "memory");
+}
+
+// 32 consecutive floats of global memory (the same for every lane) into registers.
+__device__ __forceinline__ void load_h32(const float *src, uint32_t (&r)[32]) {
+#pragma unroll
+    for (int i = 0; i < 32; i += 4) {
+        const float4 q = __ldg(reinterpret_cast<const float4 *>(src + i));
+        r[i] = __float_as_uint(q.x);
+        r[i + 1] = __float_as_uint(q.y);
+        r[i + 2] = __float_as_uint(q.z);
+        r[i + 3] = __float_as_uint(q.w);
+    }
+}
+
+// Stores 32 registers into this warp's 32 TMEM lanes, 32 columns starting at taddr.
+__device__ __forceinline__ void tmem_st32_regs(uint32_t taddr, const uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+        "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+        "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]),
+        "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]),
+        "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]),
+        "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+        : "memory");
+}
+
+// Inserts value x of column col (columns arrive in ascending order) into the
+// row's running top-3 in y = -score space when x >= thr and x beats the third:
+// strict '>' keeps the lowest index on ties. Branch-free; thr is raised to
+// max(thr0, third, best - band) after an insertion.
+__device__ __forceinline__ void top3_insert(Top3 &r, float &thr, float thr0, float band_up, float x, int col) {
+    const bool ins = x >= thr && x > r.t;
+    const bool gb = ins && x > r.b;
+    const bool gs = ins && x > r.s;  // implied by gb (b >= s)
+    const float t = gs ? r.s : (ins ? x : r.t);
+    const float s2 = gb ? r.b : (gs ? x : r.s);
+    const int is2 = gb ? r.ib : (gs ? col : r.is);
+    r.b = gb ? x : r.b;
+    r.ib = gb ? col : r.ib;
+    r.s = s2;
+    r.is = is2;
+    r.t = t;
+    thr = ins ? fmaxf(fmaxf(thr0, r.t), __fsub_rd(r.b, band_up)) : thr;
+}
+
+// One 32-column chunk of a row into its running top-3. The chunk is reduced to
+// its maximum (3-input max.f32); only when a lane of the warp holds a value at or
+// above its threshold are the 11 column triples walked, a triple being visited
+// (warp-uniformly, static register indices) when some lane's triple maximum
+// reaches that lane's threshold.
+__device__ __forceinline__ void scan_chunk(const float (&w)[32], int colbase, float thr0, float band_up, float &thr,
+                                           Top3 &r) {
+    float m[11];
+#pragma unroll
+    for (int i = 0; i < 10; ++i) m[i] = max3f(w[3 * i], w[3 * i + 1], w[3 * i + 2]);
+    m[10] = fmaxf(w[30], w[31]);
+    const float m1 = max3f(max3f(m[0], m[1], m[2]), max3f(m[3], m[4], m[5]),
+                           max3f(m[6], m[7], max3f(m[8], m[9], m[10])));
+    if (__any_sync(0xffffffffu, m1 >= thr)) {
+#pragma unroll
+        for (int g = 0; g < 11; ++g) {
+            if (__any_sync(0xffffffffu, m[g] >= thr)) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    if (3 * g + i < 32) top3_insert(r, thr, thr0, band_up, w[3 * g + i], colbase + 3 * g + i);
+            }
+        }
+    }
+}
+
 // (value, index) order; indices kept for the first two places.
 __device__ __forceinline__ bool lex_lt(float a, int ia, float b, int ib) { return a < b || (a == b && ia < ib); }
 
@@ -686,68 +768,15 @@ assign_tc_kernel(const __grid_constant__ CUtensorMap tmXh, const __grid_constant
 #pragma unroll 1
                 for (int c0 = 32 * group; c0 < BN; c0 += 32 * NGROUPS) {
                     float v[32];
-                    __syncwarp();  // tcgen05.ld/st are warp-collective: reconverge after the filtered path
+                    uint32_t hr[32];
+                    __syncwarp();  // tcgen05.ld/st are warp-collective: reconverge after the scan
                     const uint32_t taddr = lane_base + (uint32_t)(slot * BN + c0);
                     tmem_ld32_nowait(taddr, v);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                    tmem_st32_from(taddr, hn + c0);
-                    {
-                        const float *w = v;
-                        constexpr int half = 0;
-                        float m[11];
-#pragma unroll
-                        for (int i = 0; i < 10; ++i) m[i] = max3f(w[3 * i], w[3 * i + 1], w[3 * i + 2]);
-                        m[10] = fmaxf(w[30], w[31]);
-                        const float m1 = max3f(max3f(m[0], m[1], m[2]), max3f(m[3], m[4], m[5]),
-                                               max3f(m[6], m[7], max3f(m[8], m[9], m[10])));
-                        // Rare path (a lane's chunk holds a value >= thr): the triples
-                        // holding such values are visited in column order, each one
-                        // extracted with a branch-free select chain; the code stays
-                        // small so the warps' instruction fetch is not disturbed.
-                        if (__any_sync(0xffffffffu, m1 >= thr)) {
-                            unsigned tm = 0;
-#pragma unroll
-                            for (int g = 0; g < 11; ++g) tm |= (m[g] >= thr ? 1u : 0u) << g;
-                            const int colbase = j * BN + c0 + 32 * half;
-                            while (__any_sync(0xffffffffu, tm != 0)) {
-                                const bool act = tm != 0;
-                                const int g = act ? __ffs(tm) - 1 : 0;
-                                tm &= tm - 1;
-                                float e3[3] = {w[0], w[1], w[2]};
-#pragma unroll
-                                for (int gg = 1; gg < 11; ++gg) {
-                                    const bool sel = gg == g;
-                                    e3[0] = sel ? w[3 * gg] : e3[0];
-                                    e3[1] = sel ? w[3 * gg + 1] : e3[1];
-                                    e3[2] = sel ? (gg < 10 ? w[3 * gg + 2] : __int_as_float(0xff800000)) : e3[2];
-                                }
-                                if (act) {
-#pragma unroll
-                                    for (int i = 0; i < 3; ++i) {
-                                        const float x = e3[i];
-                                        // columns increase: strict '>' keeps the lowest index on ties
-                                        if (x >= thr && x > r.t) {
-                                            const int col = colbase + 3 * g + i;
-                                            if (x > r.b) {
-                                                r.t = r.s;
-                                                r.s = r.b;
-                                                r.is = r.ib;
-                                                r.b = x;
-                                                r.ib = col;
-                                            } else if (x > r.s) {
-                                                r.t = r.s;
-                                                r.s = x;
-                                                r.is = col;
-                                            } else {
-                                                r.t = x;
-                                            }
-                                            thr = fmaxf(fmaxf(thr0, r.t), __fsub_rd(r.b, band_up));
-                                        }
-                                    }
-                                }
-                            }
-                        }
-                    }
+                    tmem_wait_ld_regs(v);
+                    load_h32(hn + c0, hr);  // the refill's -h, in flight during the scan
+                    scan_chunk(v, j * BN + c0, thr0, band_up, thr, r);
+                    __syncwarp();
+                    tmem_st32_regs(taddr, hr);
                 }
                 tmem_wait_st();
                 tc_fence_before();

@@ -46,7 +46,6 @@ constexpr int NT = 256;            // threads per CTA
 constexpr int BK = 8;              // contraction chunk of the assignment tile
 constexpr int kMaxK = 256;         // clusters per problem (one assignment tile covers all)
 constexpr int kAccRows = 1024;     // rows per accumulate / setup work item
-constexpr int kAccSlots = 2048;    // (cluster, column) slots of the shared limb sums
 constexpr long long kBarrierTimeout = 4000000000ll;  // ~2 s of SM clocks
 
 struct Problem {
@@ -250,9 +249,73 @@ __device__ void assign_tile(const Problem &p, int tile, float *smem) {
     }
 }
 
-// The tile variants (kpad, rows per thread) the autotuner chooses from; the
-// micro-tile stays at most 64 accumulators so every variant fits 128 registers.
+// Row-per-thread tile (the rows-per-thread choice 0): NT rows, each thread holds
+// its row (DP = dpad <= 64 values) in registers and walks the problem's clusters
+// from shared memory (16-byte broadcast reads), accumulating x_t * c_t in
+// ascending t with FMAs -- the order of every single-problem kernel -- and keeping
+// the lowest index among equal minimum scores.
+template <int DP>
+__device__ void assign_rows(const Problem &p, int tile, float *smem) {
+    float *Cs = smem;                  // kpad x DP
+    float *hs = smem + p.kpad * DP;    // k
+    for (int e = threadIdx.x; e < p.k * DP; e += NT) {
+        const int j = e / DP, t = e - j * DP;
+        Cs[e] = t < p.d ? p.C[(long long)j * p.d + t] : 0.f;
+    }
+    for (int j = threadIdx.x; j < p.k; j += NT) hs[j] = p.h[j];
+    __syncthreads();
+    const long long r = (long long)tile * NT + threadIdx.x;
+    if (r < p.n) {
+        float x[DP];
+#pragma unroll
+        for (int t = 0; t < DP; ++t) x[t] = t < p.d ? p.X[r * p.d + t] : 0.f;
+        float best = __int_as_float(0x7f800000);
+        int bi = 0;
+#pragma unroll 1
+        for (int j = 0; j < p.k; ++j) {
+            const float4 *c4 = reinterpret_cast<const float4 *>(Cs + j * DP);
+            float acc = 0.f;
+#pragma unroll
+            for (int q = 0; q < DP / 4; ++q) {
+                const float4 c = c4[q];
+                acc = fmaf(x[4 * q], c.x, acc);
+                acc = fmaf(x[4 * q + 1], c.y, acc);
+                acc = fmaf(x[4 * q + 2], c.z, acc);
+                acc = fmaf(x[4 * q + 3], c.w, acc);
+            }
+            const float v = hs[j] - acc;
+            if (v < best) {
+                best = v;
+                bi = j;
+            }
+        }
+        p.labels[r] = bi;
+        p.d2[r] = 2.f * best + p.xnorm[r];
+    }
+    __syncthreads();
+}
+
+__host__ __device__ constexpr int rows_per_item(int tm) { return tm ? 16 * tm : NT; }
+
+// The tile variants the autotuner chooses from: rows per thread 2, 4, 8 of the
+// (rows x clusters) tile -- its micro-tile stays at most 64 accumulators so every
+// variant fits 128 registers -- or 0, the row-per-thread tile (dpad <= 64,
+// kpad <= 128).
 __device__ __forceinline__ void assign_dispatch(const Problem &p, int tile, float *smem) {
+    if (p.tm == 0) {
+        switch (p.dpad) {
+            case 8: assign_rows<8>(p, tile, smem); break;
+            case 16: assign_rows<16>(p, tile, smem); break;
+            case 24: assign_rows<24>(p, tile, smem); break;
+            case 32: assign_rows<32>(p, tile, smem); break;
+            case 40: assign_rows<40>(p, tile, smem); break;
+            case 48: assign_rows<48>(p, tile, smem); break;
+            case 56: assign_rows<56>(p, tile, smem); break;
+            case 64: assign_rows<64>(p, tile, smem); break;
+            default: break;
+        }
+        return;
+    }
     switch (p.kpad * 16 + p.tm) {
         case 16 * 16 + 2: assign_tile<16, 2>(p, tile, smem); break;
         case 16 * 16 + 4: assign_tile<16, 4>(p, tile, smem); break;
@@ -272,50 +335,81 @@ __device__ __forceinline__ void assign_dispatch(const Problem &p, int tile, floa
     }
 }
 
-// ---- accumulate: exact limb sums of a row block, a block of columns at a time ----
-// The shared accumulators hold kAccSlots (cluster, column) slots of three limbs,
-// so a pass covers kAccSlots / k columns (all of them for small k * d).
-__device__ void accumulate_item(Problem &p, int blk, long long *sacc, int *scnt, GridBarrier *gb) {
+// ---- accumulate: exact limb sums of a row block ------------------------------
+// The block's rows are listed by label in shared memory (histogram, warp scan,
+// scatter); then each thread sums the fixed-point limbs of one (cluster, column,
+// slice) task in registers -- a slice being every S-th row of the cluster's list,
+// S chosen so that every thread has a task -- and adds them to the problem's
+// limb sums with one global atomic per limb. Integer sums: the result does not
+// depend on the order of the rows or the slicing.
+__device__ void accumulate_item(Problem &p, int blk, int *sm, GridBarrier *gb) {
+    int *s_cnt = sm, *s_off = sm + kMaxK, *s_fill = sm + 2 * kMaxK, *s_rows = sm + 3 * kMaxK;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long b = (long long)blk * kAccRows, e = min(p.n, b + kAccRows);
     const int rows = (int)(e - b);
-    const int k = p.k;
-    const int ct = min(p.d, max(1, kAccSlots / k));
-    const int sp = k * ct;  // slots of one limb plane
-    for (int j = threadIdx.x; j < k; j += NT) scnt[j] = 0;
-    for (int t0 = 0; t0 < p.d; t0 += ct) {
-        const int cols = min(ct, p.d - t0);
-        for (int i = threadIdx.x; i < 3 * sp; i += NT) sacc[i] = 0;
-        __syncthreads();
-        for (int q = threadIdx.x; q < rows * cols; q += NT) {
-            const int r = q / cols, c = q - r * cols;
-            const int lab = p.labels[b + r];
-            if ((unsigned)lab >= (unsigned)k) {  // cannot happen: the assignment writes every row
-                atomicExch(&gb->error, 2);
-                continue;
-            }
-            const int col = t0 + c;
-            const Limbs L = fixed_of(p.X[(b + r) * p.d + col], p.colexp[col]);
-            const int slot = lab * ct + c;
-            atomicAdd(reinterpret_cast<unsigned long long *>(&sacc[slot]), (unsigned long long)L.l0);
-            atomicAdd(reinterpret_cast<unsigned long long *>(&sacc[sp + slot]), (unsigned long long)L.l1);
-            atomicAdd(reinterpret_cast<unsigned long long *>(&sacc[2 * sp + slot]), (unsigned long long)L.l2);
-            if (t0 == 0 && c == 0) atomicAdd(&scnt[lab], 1);
+    const int k = p.k, d = p.d;
+    for (int j = threadIdx.x; j < k; j += NT) {
+        s_cnt[j] = 0;
+        s_fill[j] = 0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < rows; r += NT) {
+        const int lab = p.labels[b + r];
+        if ((unsigned)lab >= (unsigned)k) {  // cannot happen: the assignment writes every row
+            atomicExch(&gb->error, 2);
+            continue;
         }
-        __syncthreads();
-        const long long plane = (long long)k * p.d;
-        for (int i = threadIdx.x; i < k * cols; i += NT) {
-            const int j = i / cols, c = i - j * cols;
-            const int slot = j * ct + c;
-            const long long g = (long long)j * p.d + t0 + c;
-            const long long v0 = sacc[slot], v1 = sacc[sp + slot], v2 = sacc[2 * sp + slot];
-            if (v0) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[g]), (unsigned long long)v0);
-            if (v1) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[plane + g]), (unsigned long long)v1);
-            if (v2) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[2 * plane + g]), (unsigned long long)v2);
+        atomicAdd(&s_cnt[lab], 1);
+    }
+    __syncthreads();
+    if (warp == 0) {  // exclusive scan of the k <= 256 counts, 8 per lane
+        int loc[8], sum = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = lane * 8 + q;
+            loc[q] = sum;
+            sum += idx < k ? s_cnt[idx] : 0;
         }
-        __syncthreads();
+        int inc = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += t;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int idx = lane * 8 + q;
+            if (idx < k) s_off[idx] = inc - sum + loc[q];
+        }
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < rows; r += NT) {
+        const int lab = p.labels[b + r];
+        if ((unsigned)lab < (unsigned)k) s_rows[s_off[lab] + atomicAdd(&s_fill[lab], 1)] = r;
+    }
+    __syncthreads();
+    const int kd = k * d;
+    const int S = min(32, max(1, (NT + kd - 1) / kd));
+    const long long plane = (long long)k * d;
+    const float *Xb = p.X + b * d;
+    for (int task = threadIdx.x; task < kd * S; task += NT) {
+        const int c = task % d, js = task / d;
+        const int j = js / S, sl = js - j * S;
+        const int cnt = s_cnt[j], base = s_off[j], ec = p.colexp[c];
+        long long a0 = 0, a1 = 0, a2 = 0;
+        for (int i = sl; i < cnt; i += S) {
+            const Limbs L = fixed_of(Xb[(long long)s_rows[base + i] * d + c], ec);
+            a0 += L.l0;
+            a1 += L.l1;
+            a2 += L.l2;
+        }
+        const long long g = (long long)j * d + c;
+        if (a0) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[g]), (unsigned long long)a0);
+        if (a1) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[plane + g]), (unsigned long long)a1);
+        if (a2) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[2 * plane + g]), (unsigned long long)a2);
     }
     for (int j = threadIdx.x; j < k; j += NT)
-        if (scnt[j]) atomicAdd(&p.counts[j], scnt[j]);
+        if (s_cnt[j]) atomicAdd(&p.counts[j], s_cnt[j]);
     __syncthreads();
 }
 
@@ -425,8 +519,8 @@ __device__ void decide_item(Problem &p, double *sred, float *sv, long long *sr, 
 // Dynamic shared memory: the largest phase's needs (assignment tiles, the
 // accumulate limb planes of the largest k, decide's scratch).
 size_t smem_bytes(int kmax, int dmax) {
-    const size_t assign = sizeof(float) * BK * (16 * 8 + 4 + 256 + 4);
-    const size_t acc = sizeof(long long) * 3 * kAccSlots + sizeof(int) * kmax;
+    const size_t assign = std::max(sizeof(float) * BK * (16 * 8 + 4 + 256 + 4), sizeof(float) * (128 * 64 + kMaxK));
+    const size_t acc = sizeof(int) * (3 * kMaxK + kAccRows);
     const size_t setup = sizeof(float) * (size_t)dmax;
     const size_t decide = (sizeof(double) + sizeof(float) + sizeof(long long)) * NT;
     return std::max(std::max(assign, acc), std::max(setup, decide));
@@ -463,9 +557,7 @@ __global__ void __launch_bounds__(NT, 2) persistent_kernel(Problem *P, Lists L, 
             const int2 w = L.acc[i];
             Problem &p = P[w.x];
             if (!p.done) {
-                long long *sacc = reinterpret_cast<long long *>(smem_raw);
-                int *scnt = reinterpret_cast<int *>(sacc + 3 * kAccSlots);
-                accumulate_item(p, w.y, sacc, scnt, gb);
+                accumulate_item(p, w.y, reinterpret_cast<int *>(smem_raw), gb);
             }
         }
         if (!grid_sync(gb)) return;
@@ -502,8 +594,7 @@ __global__ void tune_fill_kernel(float *p, long long count, unsigned seed) {
 
 __global__ void __launch_bounds__(NT, 2) tune_assign_kernel(const Problem *pp, int tiles) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Problem p = *pp;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) assign_dispatch(p, t, reinterpret_cast<float *>(smem_raw));
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) assign_dispatch(*pp, t, reinterpret_cast<float *>(smem_raw));
 }
 
 }  // namespace batched
@@ -525,7 +616,8 @@ int tuned_tm(int dev, int dpad, int kpad, cudaStream_t s) {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto found = g_tuned.find(key);
     if (found != g_tuned.end()) return found->second;
-    const std::vector<int> cands = kpad >= 256 ? std::vector<int>{2, 4} : std::vector<int>{2, 4, 8};
+    std::vector<int> cands = kpad >= 256 ? std::vector<int>{2, 4} : std::vector<int>{2, 4, 8};
+    if (dpad <= 64 && kpad <= 128) cands.push_back(0);
     const long long n = 32768;
     float *X = nullptr, *Ct = nullptr, *h = nullptr, *d2 = nullptr, *xn = nullptr;
     int32_t *lab = nullptr;
@@ -553,6 +645,7 @@ int tuned_tm(int dev, int dpad, int kpad, cudaStream_t s) {
             Problem p;
             std::memset(&p, 0, sizeof(p));
             p.X = X;
+            p.C = Ct;  // the row-per-thread tile reads C (k x d); any values of the right size do
             p.Ct = Ct;
             p.h = h;
             p.labels = lab;
@@ -565,7 +658,7 @@ int tuned_tm(int dev, int dpad, int kpad, cudaStream_t s) {
             p.kpad = kpad;
             p.tm = tm;
             cudaMemcpyAsync(dp, &p, sizeof(p), cudaMemcpyHostToDevice, s);
-            const int tiles = (int)((n + 16 * tm - 1) / (16 * tm));
+            const int tiles = (int)((n + rows_per_item(tm) - 1) / rows_per_item(tm));
             tune_assign_kernel<<<std::min(tiles, 296), NT, smem, s>>>(dp, tiles);  // warm-up
             cudaEventRecord(a, s);
             for (int r = 0; r < 3; ++r) tune_assign_kernel<<<std::min(tiles, 296), NT, smem, s>>>(dp, tiles);
@@ -673,7 +766,7 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         }
         for (int j = 0; j < p.kpad; ++j) prep.push_back(make_int2((int)i, j));
         for (int j = 0; j < p.k; ++j) fin.push_back(make_int2((int)i, j));
-        const int bm = 16 * p.tm;
+        const int bm = rows_per_item(p.tm);
         for (long long t = 0; t < (p.n + bm - 1) / bm; ++t) {
             assign.push_back(make_int2((int)i, (int)t));
             assign_cost.push_back((double)std::min<long long>(bm, p.n - t * bm) * p.kpad * p.dpad);
