@@ -336,12 +336,15 @@ __device__ __forceinline__ void assign_dispatch(const Problem &p, int tile, floa
 }
 
 // ---- accumulate: exact limb sums of a row block ------------------------------
-// The block's rows are listed by label in shared memory (histogram, warp scan,
-// scatter); then each thread sums the fixed-point limbs of one (cluster, column,
-// slice) task in registers -- a slice being every S-th row of the cluster's list,
-// S chosen so that every thread has a task -- and adds them to the problem's
-// limb sums with one global atomic per limb. Integer sums: the result does not
-// depend on the order of the rows or the slicing.
+// The block's rows are listed by label in shared memory (warp-aggregated
+// histogram, warp scan, warp-ranked scatter). Then each warp takes (cluster,
+// column chunk, slice) tasks: its lanes cover CW = min(32, 2^ceil(log2 d))
+// consecutive columns of 32 / CW rows at a time (coalesced row reads, four rows
+// per lane in flight), sum the fixed-point limbs of the slice's rows -- every S-th
+// group of rows of the cluster's list -- in registers, fold the lanes of equal
+// column with shuffles and add the totals to the problem's limb sums with one
+// global atomic per limb. Integer sums: the result depends on neither the order
+// of the rows nor the slicing.
 __device__ void accumulate_item(Problem &p, int blk, int *sm, GridBarrier *gb) {
     int *s_cnt = sm, *s_off = sm + kMaxK, *s_fill = sm + 2 * kMaxK, *s_rows = sm + 3 * kMaxK;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -353,13 +356,15 @@ __device__ void accumulate_item(Problem &p, int blk, int *sm, GridBarrier *gb) {
         s_fill[j] = 0;
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < rows; r += NT) {
-        const int lab = p.labels[b + r];
-        if ((unsigned)lab >= (unsigned)k) {  // cannot happen: the assignment writes every row
+    for (int r0 = 0; r0 < rows; r0 += NT) {  // warp-uniform trip count
+        const int r = r0 + threadIdx.x;
+        int lab = r < rows ? p.labels[b + r] : -1;
+        if (r < rows && (unsigned)lab >= (unsigned)k) {  // cannot happen: the assignment writes every row
             atomicExch(&gb->error, 2);
-            continue;
+            lab = -1;
         }
-        atomicAdd(&s_cnt[lab], 1);
+        const unsigned peers = __match_any_sync(0xffffffffu, lab);
+        if (lab >= 0 && lane == __ffs(peers) - 1) atomicAdd(&s_cnt[lab], __popc(peers));
     }
     __syncthreads();
     if (warp == 0) {  // exclusive scan of the k <= 256 counts, 8 per lane
@@ -383,30 +388,62 @@ __device__ void accumulate_item(Problem &p, int blk, int *sm, GridBarrier *gb) {
         }
     }
     __syncthreads();
-    for (int r = threadIdx.x; r < rows; r += NT) {
-        const int lab = p.labels[b + r];
-        if ((unsigned)lab < (unsigned)k) s_rows[s_off[lab] + atomicAdd(&s_fill[lab], 1)] = r;
+    for (int r0 = 0; r0 < rows; r0 += NT) {
+        const int r = r0 + threadIdx.x;
+        int lab = r < rows ? p.labels[b + r] : -1;
+        if ((unsigned)lab >= (unsigned)k) lab = -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, lab);
+        const int leader = __ffs(peers) - 1;
+        int base = 0;
+        if (lab >= 0 && lane == leader) base = atomicAdd(&s_fill[lab], __popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (lab >= 0) s_rows[s_off[lab] + base + __popc(peers & ((1u << lane) - 1))] = r;
     }
     __syncthreads();
-    const int kd = k * d;
-    const int S = min(32, max(1, (NT + kd - 1) / kd));
+    int cw = 1;
+    while (cw < d && cw < 32) cw <<= 1;
+    const int rps = 32 / cw;               // rows per warp step
+    const int cl = lane & (cw - 1), rl = lane / cw;
+    const int nch = (d + cw - 1) / cw;     // column chunks
+    const int kc = k * nch;
+    const int S = min(8, max(1, (2 * (NT / 32) + kc - 1) / kc));  // slices: at least two tasks per warp
     const long long plane = (long long)k * d;
     const float *Xb = p.X + b * d;
-    for (int task = threadIdx.x; task < kd * S; task += NT) {
-        const int c = task % d, js = task / d;
-        const int j = js / S, sl = js - j * S;
-        const int cnt = s_cnt[j], base = s_off[j], ec = p.colexp[c];
+    for (int task = warp; task < kc * S; task += NT / 32) {
+        const int j = task / (nch * S), rest = task - j * nch * S;
+        const int ch = rest / S, sl = rest - ch * S;
+        const int c = ch * cw + cl;
+        const bool active = c < d;
+        const int cnt = s_cnt[j], base = s_off[j];
+        const int ec = active ? p.colexp[c] : 0;
         long long a0 = 0, a1 = 0, a2 = 0;
-        for (int i = sl; i < cnt; i += S) {
-            const Limbs L = fixed_of(Xb[(long long)s_rows[base + i] * d + c], ec);
-            a0 += L.l0;
-            a1 += L.l1;
-            a2 += L.l2;
+        const int step = S * rps;
+        for (int i = sl * rps + rl; i < cnt; i += 4 * step) {
+            float v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int ii = i + u * step;
+                v[u] = (active && ii < cnt) ? Xb[(long long)s_rows[base + ii] * d + c] : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const Limbs L = fixed_of(v[u], ec);
+                a0 += L.l0;
+                a1 += L.l1;
+                a2 += L.l2;
+            }
         }
-        const long long g = (long long)j * d + c;
-        if (a0) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[g]), (unsigned long long)a0);
-        if (a1) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[plane + g]), (unsigned long long)a1);
-        if (a2) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[2 * plane + g]), (unsigned long long)a2);
+        for (int o = 16; o >= cw; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (rl == 0 && active) {
+            const long long g = (long long)j * d + c;
+            if (a0) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[g]), (unsigned long long)a0);
+            if (a1) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[plane + g]), (unsigned long long)a1);
+            if (a2) atomicAdd(reinterpret_cast<unsigned long long *>(&p.acc[2 * plane + g]), (unsigned long long)a2);
+        }
     }
     for (int j = threadIdx.x; j < k; j += NT)
         if (s_cnt[j]) atomicAdd(&p.counts[j], s_cnt[j]);

@@ -253,26 +253,46 @@ struct Limbs {
     long long l0, l1, l2;
 };
 
+// round(x * 2^e) (round half to even) as three signed 32-bit limbs,
+// v = l2 * 2^64 + l1 * 2^32 + l0 with |l_i| < 2^32 (each limb carries the sign of
+// x), computed in 64-bit integer arithmetic. Requires |x| * 2^e < 2^94. Limb sums
+// of fewer than 2^31 values stay below 2^63, and any order of additions and
+// subtractions gives the same integer l2 * 2^64 + l1 * 2^32 + l0.
 __device__ __forceinline__ Limbs fixed_of(float x, int e) {
     const float f = scalbnf(x, e);  // exact: |f| < 2^94, a power-of-two scaling
     const unsigned bits = __float_as_uint(f);
     const int be = (int)((bits >> 23) & 0xffu);
     unsigned long long mant = bits & 0x7fffffu;
     if (be) mant |= 0x800000u;
-    const int sh = (be ? be : 1) - 150;  // f = mant * 2^sh
-    unsigned __int128 mag = 0;
+    const int sh = (be ? be : 1) - 150;  // f = mant * 2^sh, sh <= 70
+    long long l0 = 0, l1 = 0, l2 = 0;
     if (sh >= 0) {
-        mag = (unsigned __int128)mant << sh;
+        const int q = sh >> 5;
+        const unsigned long long w = mant << (sh & 31);  // < 2^55, limbs q and q + 1
+        const long long lo = (long long)(w & 0xffffffffull), hi = (long long)(w >> 32);
+        if (q == 0) {
+            l0 = lo;
+            l1 = hi;
+        } else if (q == 1) {
+            l1 = lo;
+            l2 = hi;
+        } else {
+            l2 = lo;  // sh >= 64: w < 2^31 because |f| < 2^94
+        }
     } else if (sh > -26) {
         const int r = -sh;  // round half to even
         const unsigned long long q = mant >> r, rem = mant & ((1ull << r) - 1), half = 1ull << (r - 1);
-        mag = q + ((rem > half || (rem == half && (q & 1ull))) ? 1ull : 0ull);
+        l0 = (long long)(q + ((rem > half || (rem == half && (q & 1ull))) ? 1ull : 0ull));
     }
-    const __int128 v = (bits >> 31) ? -(__int128)mag : (__int128)mag;
+    if (bits >> 31) {
+        l0 = -l0;
+        l1 = -l1;
+        l2 = -l2;
+    }
     Limbs L;
-    L.l0 = (long long)(v & 0xffffffffll);
-    L.l1 = (long long)((v >> 32) & 0xffffffffll);
-    L.l2 = (long long)(v >> 64);
+    L.l0 = l0;
+    L.l1 = l1;
+    L.l2 = l2;
     return L;
 }
 

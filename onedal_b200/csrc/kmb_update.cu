@@ -832,10 +832,10 @@ __global__ void list_empties_kernel(const int32_t *__restrict__ empty_flag, int 
 // A value x of column t is the integer v = round(x * 2^E_t), |v| < 2^94, with E_t
 // chosen once per call from the column's largest |x|: every float within 2^70 of
 // that maximum is represented exactly (a 24-bit significand), smaller ones to
-// 2^-94 of the maximum. v is kept as three 32-bit limbs, v = l2 * 2^64 + l1 * 2^32
-// + l0 (l0, l1 in [0, 2^32), l2 signed), and a cluster-column sum as three int64
-// limb sums, so additions and subtractions of rows in any order give the same
-// integer. The finalize folds the limb sums into one 128-bit integer, keeps it
+// 2^-94 of the maximum. v is kept as three signed 32-bit limbs, v = l2 * 2^64 +
+// l1 * 2^32 + l0 (fixed_of), and a cluster-column sum as three int64 limb sums,
+// so additions and subtractions of rows in any order give the same integer. The
+// finalize folds the limb sums into one 128-bit integer, stores it back
 // normalised, and converts it to the nearest double.
 
 // colexp[t] <- max |x| of column t, as float bits (non-negative floats order as ints).
@@ -865,7 +865,7 @@ __global__ void colmax_global_kernel(const float *__restrict__ X, int64_t n, int
     }
 }
 
-// E_t such that max |x_t| * 2^E_t < 2^39 (E_t = 0 for an all-zero column); the
+// E_t such that max |x_t| * 2^E_t < 2^94 (E_t = 0 for an all-zero column); the
 // non-finite maximum of a column holding inf/NaN gives E_t = 0 too.
 __global__ void colexp_kernel(int *__restrict__ colexp, int d, const LoopState *st) {
     if (is_done(st)) return;
