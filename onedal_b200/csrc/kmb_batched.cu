@@ -45,7 +45,7 @@ namespace batched {
 constexpr int NT = 256;            // threads per CTA
 constexpr int BK = 8;              // contraction chunk of the assignment tile
 constexpr int kMaxK = 256;         // clusters per problem (one assignment tile covers all)
-constexpr int kAccRows = 1024;     // rows per accumulate / setup work item
+constexpr int kAccRows = 4096;     // rows per accumulate / setup work item
 constexpr long long kBarrierTimeout = 4000000000ll;  // ~2 s of SM clocks
 
 struct Problem {
@@ -66,12 +66,21 @@ struct Problem {
     double eps, shift;
 };
 
+// Work of a phase as per-problem item counts: prefix[q] = items of the problems
+// before position q of the phase's problem order; item i belongs to the last q
+// with prefix[q] <= i (binary search on the device), so the host builds O(problems)
+// data, not O(tiles).
+struct Phase {
+    const long long *prefix;  // count + 1 entries
+    const int *order;         // problem at each position (null: identity)
+    long long items;
+};
+
 struct Lists {
-    const int2 *setup;  int n_setup;   // (problem, row block)
-    const int2 *prep;   int n_prep;    // (problem, padded cluster)
-    const int2 *assign; int n_assign;  // (problem, row tile), largest first
-    const int2 *acc;    int n_acc;     // (problem, row block)
-    const int2 *fin;    int n_fin;     // (problem, cluster)
+    Phase blocks;  // (problem, row block of kAccRows): setup and accumulate
+    Phase prep;    // (problem, padded cluster)
+    Phase assign;  // (problem, row tile), problems with the costliest tiles first
+    Phase fin;     // (problem, cluster)
     int n_problems;
     int iterations;
 };
@@ -82,6 +91,16 @@ struct GridBarrier {
     int error;   // 1: a barrier wait ran out; 2: an invalid label reached the accumulation
     int active;  // problems not yet converged
 };
+
+__device__ __forceinline__ int2 item_of(const Phase &ph, int count, long long i) {
+    int lo = 0, hi = count;  // prefix[lo] <= i < prefix[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (ph.prefix[mid] <= i) lo = mid;
+        else hi = mid;
+    }
+    return make_int2(ph.order ? ph.order[lo] : lo, (int)(i - ph.prefix[lo]));
+}
 
 // Grid-wide barrier of a cooperative launch; false once any CTA gave up waiting
 // (or flagged an error). Thread 0 decides and the CTA follows its decision, so
@@ -271,8 +290,33 @@ __device__ void assign_rows(const Problem &p, int tile, float *smem) {
         for (int t = 0; t < DP; ++t) x[t] = t < p.d ? p.X[r * p.d + t] : 0.f;
         float best = __int_as_float(0x7f800000);
         int bi = 0;
+        // four clusters at a time: four independent FMA chains
+        const int k4 = p.k & ~3;
 #pragma unroll 1
-        for (int j = 0; j < p.k; ++j) {
+        for (int j = 0; j < k4; j += 4) {
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int q = 0; q < DP / 4; ++q) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float4 c = reinterpret_cast<const float4 *>(Cs + (j + u) * DP)[q];
+                    acc[u] = fmaf(x[4 * q], c.x, acc[u]);
+                    acc[u] = fmaf(x[4 * q + 1], c.y, acc[u]);
+                    acc[u] = fmaf(x[4 * q + 2], c.z, acc[u]);
+                    acc[u] = fmaf(x[4 * q + 3], c.w, acc[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float v = hs[j + u] - acc[u];
+                if (v < best) {  // ascending clusters: the lowest index among equal minima
+                    best = v;
+                    bi = j + u;
+                }
+            }
+        }
+#pragma unroll 1
+        for (int j = k4; j < p.k; ++j) {
             const float4 *c4 = reinterpret_cast<const float4 *>(Cs + j * DP);
             float acc = 0.f;
 #pragma unroll
@@ -572,34 +616,34 @@ __global__ void __launch_bounds__(NT, 2) persistent_kernel(Problem *P, Lists L, 
     for (int i = blockIdx.x; i < L.n_problems; i += gridDim.x)
         for (int t = threadIdx.x; t < P[i].d; t += NT) P[i].colexp[t] = 0;
     if (!grid_sync(gb)) return;
-    for (int i = blockIdx.x; i < L.n_setup; i += gridDim.x) {
-        const int2 w = L.setup[i];
+    for (long long i = blockIdx.x; i < L.blocks.items; i += gridDim.x) {
+        const int2 w = item_of(L.blocks, L.n_problems, i);
         setup_item(P[w.x], w.y, fsm);
     }
     if (!grid_sync(gb)) return;
     for (int i = blockIdx.x; i < L.n_problems; i += gridDim.x) scales_item(P[i]);
     if (!grid_sync(gb)) return;
     for (int it = 0; it < L.iterations; ++it) {
-        for (int i = blockIdx.x * (NT / 32) + warp; i < L.n_prep; i += warps) {
-            const int2 w = L.prep[i];
+        for (long long i = blockIdx.x * (NT / 32) + warp; i < L.prep.items; i += warps) {
+            const int2 w = item_of(L.prep, L.n_problems, i);
             if (!P[w.x].done) prep_item(P[w.x], w.y, lane);
         }
         if (!grid_sync(gb)) return;
-        for (int i = blockIdx.x; i < L.n_assign; i += gridDim.x) {
-            const int2 w = L.assign[i];
+        for (long long i = blockIdx.x; i < L.assign.items; i += gridDim.x) {
+            const int2 w = item_of(L.assign, L.n_problems, i);
             if (!P[w.x].done) assign_dispatch(P[w.x], w.y, fsm);
         }
         if (!grid_sync(gb)) return;
-        for (int i = blockIdx.x; i < L.n_acc; i += gridDim.x) {
-            const int2 w = L.acc[i];
+        for (long long i = blockIdx.x; i < L.blocks.items; i += gridDim.x) {
+            const int2 w = item_of(L.blocks, L.n_problems, i);
             Problem &p = P[w.x];
             if (!p.done) {
                 accumulate_item(p, w.y, reinterpret_cast<int *>(smem_raw), gb);
             }
         }
         if (!grid_sync(gb)) return;
-        for (int i = blockIdx.x * (NT / 32) + warp; i < L.n_fin; i += warps) {
-            const int2 w = L.fin[i];
+        for (long long i = blockIdx.x * (NT / 32) + warp; i < L.fin.items; i += warps) {
+            const int2 w = item_of(L.fin, L.n_problems, i);
             if (!P[w.x].done) finalize_item(P[w.x], w.y, lane);
         }
         if (!grid_sync(gb)) return;
@@ -769,9 +813,13 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         cudaGetLastError();
         return KMB_ENOMEM;
     }
-    std::vector<int2> setup, prep, assign, acc, fin;
-    std::vector<double> assign_cost;
     std::map<long long, int> classes;  // (kpad, tm) variants in use
+    // per-problem item counts of each phase, as prefix sums (see Phase)
+    const size_t P1 = (size_t)count + 1;
+    std::vector<long long> pre(4 * P1, 0);
+    std::vector<int> order((size_t)count);
+    std::vector<long long> tiles((size_t)count);
+    std::vector<double> tile_cost((size_t)count);
     for (int64_t i = 0; i < count; ++i) {
         const kmb_batched_problem &q = problems[i];
         Problem &p = H[i];
@@ -797,40 +845,26 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         p.eps = accuracy_threshold;
         p.done = max_iteration_count == 0 ? 1 : 0;
         classes[(long long)p.kpad * 16 + p.tm] = 1;
-        for (long long b = 0; b < (p.n + kAccRows - 1) / kAccRows; ++b) {
-            setup.push_back(make_int2((int)i, (int)b));
-            acc.push_back(make_int2((int)i, (int)b));
-        }
-        for (int j = 0; j < p.kpad; ++j) prep.push_back(make_int2((int)i, j));
-        for (int j = 0; j < p.k; ++j) fin.push_back(make_int2((int)i, j));
         const int bm = rows_per_item(p.tm);
-        for (long long t = 0; t < (p.n + bm - 1) / bm; ++t) {
-            assign.push_back(make_int2((int)i, (int)t));
-            assign_cost.push_back((double)std::min<long long>(bm, p.n - t * bm) * p.kpad * p.dpad);
-        }
+        pre[0 * P1 + i + 1] = pre[0 * P1 + i] + (p.n + kAccRows - 1) / kAccRows;
+        pre[1 * P1 + i + 1] = pre[1 * P1 + i] + p.kpad;
+        pre[3 * P1 + i + 1] = pre[3 * P1 + i] + p.k;
+        tiles[i] = (p.n + bm - 1) / bm;
+        tile_cost[i] = (double)bm * p.kpad * p.dpad;
+        order[i] = (int)i;
     }
-    // largest assignment tiles first (round-robin over the grid then balances well)
-    {
-        std::vector<size_t> order(assign.size());
-        for (size_t i = 0; i < order.size(); ++i) order[i] = i;
-        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return assign_cost[a] > assign_cost[b]; });
-        std::vector<int2> sorted(assign.size());
-        for (size_t i = 0; i < order.size(); ++i) sorted[i] = assign[order[i]];
-        assign.swap(sorted);
-    }
-    std::vector<int2> all;
-    auto put = [&](const std::vector<int2> &v) {
-        const size_t o = all.size();
-        all.insert(all.end(), v.begin(), v.end());
-        return o;
-    };
-    const size_t o_setup = put(setup), o_prep = put(prep), o_assign = put(assign), o_acc = put(acc), o_fin = put(fin);
+    // assignment: problems with the costliest tiles first (round-robin over the grid then balances well)
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tile_cost[a] > tile_cost[b]; });
+    for (int64_t q = 0; q < count; ++q) pre[2 * P1 + q + 1] = pre[2 * P1 + q] + tiles[order[q]];
     Problem *dP = nullptr;
-    int2 *dI = nullptr;
+    long long *dPre = nullptr;
+    int *dOrder = nullptr;
     if (cudaMallocAsync(&dP, sizeof(Problem) * count, s) != cudaSuccess ||
-        cudaMallocAsync(&dI, sizeof(int2) * all.size(), s) != cudaSuccess) {
+        cudaMallocAsync(&dPre, sizeof(long long) * pre.size(), s) != cudaSuccess ||
+        cudaMallocAsync(&dOrder, sizeof(int) * order.size(), s) != cudaSuccess) {
         cudaGetLastError();
         if (dP) cudaFreeAsync(dP, s);
+        if (dPre) cudaFreeAsync(dPre, s);
         cudaFreeAsync(base, s);
         return KMB_ENOMEM;
     }
@@ -840,21 +874,16 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
     for (int64_t i = 0; i < count; ++i) gb_init.active += H[i].done ? 0 : 1;
     int rc = KMB_OK;
     if (cudaMemcpyAsync(dP, H.data(), sizeof(Problem) * count, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(dI, all.data(), sizeof(int2) * all.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dPre, pre.data(), sizeof(long long) * pre.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(dOrder, order.data(), sizeof(int) * order.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
         cudaMemcpyAsync(gb, &gb_init, sizeof(GridBarrier), cudaMemcpyHostToDevice, s) != cudaSuccess)
         rc = KMB_ECUDA;
 
     Lists L;
-    L.setup = dI + o_setup;
-    L.n_setup = (int)setup.size();
-    L.prep = dI + o_prep;
-    L.n_prep = (int)prep.size();
-    L.assign = dI + o_assign;
-    L.n_assign = (int)assign.size();
-    L.acc = dI + o_acc;
-    L.n_acc = (int)acc.size();
-    L.fin = dI + o_fin;
-    L.n_fin = (int)fin.size();
+    L.blocks = Phase{dPre + 0 * P1, nullptr, pre[0 * P1 + count]};
+    L.prep = Phase{dPre + 1 * P1, nullptr, pre[1 * P1 + count]};
+    L.assign = Phase{dPre + 2 * P1, dOrder, pre[2 * P1 + count]};
+    L.fin = Phase{dPre + 3 * P1, nullptr, pre[3 * P1 + count]};
     L.n_problems = (int)count;
     L.iterations = (int)max_iteration_count;
     const size_t smem = smem_bytes(kmax, dmax);
@@ -922,7 +951,8 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         }
     }
     cudaFreeAsync(dP, s);
-    cudaFreeAsync(dI, s);
+    cudaFreeAsync(dPre, s);
+    cudaFreeAsync(dOrder, s);
     cudaFreeAsync(base, s);
     return rc;
 }
