@@ -372,8 +372,11 @@ KMB_API int kmb_server_get_stats(void *server, kmb_server_stats *stats);
 
 /* Measured fused multiply-add peak of `device` in dtype's precision (GFLOP/s,
  * 2 flops per FMA): a short grid of dependent FMA chains timed with CUDA
- * events, best of four launches. The plain form's assignment is reported
- * against it. No counterpart in the reference. */
+ * events, best of four launches. dtype KMB_F32, KMB_F64, or
+ * KMB_FMA_PEAK_F32X2 for the packed FP32 pair instruction (fma.rn.f32x2). The
+ * plain form's assignment is reported against the larger FP32 figure. No
+ * counterpart in the reference. */
+#define KMB_FMA_PEAK_F32X2 2
 KMB_API int kmb_measure_fma_peak(int device, int dtype, double *gflops);
 
 /* Library version string. */

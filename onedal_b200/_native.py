@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libonedal_b200_kmeans.so")
 
 KMB_OK, KMB_EINVAL, KMB_ENOMEM, KMB_ECUDA, KMB_ETIMEDOUT, KMB_ETOO_MANY_EMPTY, KMB_EUNSUPPORTED = range(7)
 KMB_F32, KMB_F64 = 0, 1
+KMB_FMA_PEAK_F32X2 = 2  # kmb_measure_fma_peak: packed FP32 pair FMA
 KMB_MEM_HOST, KMB_MEM_DEVICE = 0, 1
 KMB_FORM_PLAIN, KMB_FORM_BF16X3, KMB_FORM_AUTO, KMB_FORM_BF16 = 0, 1, 2, 3
 

@@ -510,11 +510,14 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
             const float *xa = Xs + buf * tile_floats + (8 * warp) * dpad;
             for (int pass = 0; pass < n_pass; ++pass) {
                 const float *cb = Cs + (size_t)pass * dpad * kResPass + 4 * lane;
-                float acc[8][8];
+                // Packed FP32 FMAs (fma.rn.f32x2: two correctly rounded FMAs, the same
+                // results as fmaf): each pair holds two of this lane's clusters for one
+                // row, with the row's value duplicated; one issue slot per two FMAs.
+                float2 acc2[8][4];  // acc2[i][q] = clusters 2q, 2q + 1 of this lane's eight
 #pragma unroll
                 for (int i = 0; i < 8; ++i)
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+                    for (int q = 0; q < 4; ++q) acc2[i][q] = make_float2(0.f, 0.f);
 #pragma unroll 2
                 for (int t = 0; t < dpad; t += 2) {
                     float2 a[8];
@@ -524,17 +527,31 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
                     const float4 b01 = *reinterpret_cast<const float4 *>(cb + t * kResPass + 128);
                     const float4 b10 = *reinterpret_cast<const float4 *>(cb + (t + 1) * kResPass);
                     const float4 b11 = *reinterpret_cast<const float4 *>(cb + (t + 1) * kResPass + 128);
-                    const float bx[8] = {b00.x, b00.y, b00.z, b00.w, b01.x, b01.y, b01.z, b01.w};
-                    const float by[8] = {b10.x, b10.y, b10.z, b10.w, b11.x, b11.y, b11.z, b11.w};
+                    const float2 bx[4] = {make_float2(b00.x, b00.y), make_float2(b00.z, b00.w), make_float2(b01.x, b01.y),
+                                          make_float2(b01.z, b01.w)};
+                    const float2 by[4] = {make_float2(b10.x, b10.y), make_float2(b10.z, b10.w), make_float2(b11.x, b11.y),
+                                          make_float2(b11.z, b11.w)};
 #pragma unroll
-                    for (int i = 0; i < 8; ++i)
+                    for (int i = 0; i < 8; ++i) {
+                        const float2 ax = make_float2(a[i].x, a[i].x);
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i].x, bx[j], acc[i][j]);
+                        for (int q = 0; q < 4; ++q) acc2[i][q] = __ffma2_rn(ax, bx[q], acc2[i][q]);
+                    }
 #pragma unroll
-                    for (int i = 0; i < 8; ++i)
+                    for (int i = 0; i < 8; ++i) {
+                        const float2 ay = make_float2(a[i].y, a[i].y);
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i].y, by[j], acc[i][j]);
+                        for (int q = 0; q < 4; ++q) acc2[i][q] = __ffma2_rn(ay, by[q], acc2[i][q]);
+                    }
                 }
+                float acc[8][8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        acc[i][2 * q] = acc2[i][q].x;
+                        acc[i][2 * q + 1] = acc2[i][q].y;
+                    }
                 RowTop<float> top[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {

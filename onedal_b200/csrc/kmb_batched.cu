@@ -273,21 +273,37 @@ __device__ void assign_tile(const Problem &p, int tile, float *smem) {
 // from shared memory (16-byte broadcast reads), accumulating x_t * c_t in
 // ascending t with FMAs -- the order of every single-problem kernel -- and keeping
 // the lowest index among equal minimum scores.
+// The centroids stay in shared memory across consecutive tiles of one problem
+// (cached: the CTA-uniform id of the problem whose centroids are there).
 template <int DP>
-__device__ void assign_rows(const Problem &p, int tile, float *smem) {
+__device__ void assign_rows(const Problem &p, int pid, int tile, float *smem, int &cached) {
     float *Cs = smem;                  // kpad x DP
     float *hs = smem + p.kpad * DP;    // k
-    for (int e = threadIdx.x; e < p.k * DP; e += NT) {
-        const int j = e / DP, t = e - j * DP;
-        Cs[e] = t < p.d ? p.C[(long long)j * p.d + t] : 0.f;
+    if (cached != pid) {
+        for (int e = threadIdx.x; e < p.k * DP; e += NT) {
+            const int j = e / DP, t = e - j * DP;
+            Cs[e] = t < p.d ? p.C[(long long)j * p.d + t] : 0.f;
+        }
+        for (int j = threadIdx.x; j < p.k; j += NT) hs[j] = p.h[j];
+        cached = pid;
+        __syncthreads();
     }
-    for (int j = threadIdx.x; j < p.k; j += NT) hs[j] = p.h[j];
-    __syncthreads();
     const long long r = (long long)tile * NT + threadIdx.x;
     if (r < p.n) {
         float x[DP];
+        if (p.d == DP && (p.d & 3) == 0 && (reinterpret_cast<uintptr_t>(p.X) & 15) == 0) {
 #pragma unroll
-        for (int t = 0; t < DP; ++t) x[t] = t < p.d ? p.X[r * p.d + t] : 0.f;
+            for (int q = 0; q < DP / 4; ++q) {
+                const float4 v = reinterpret_cast<const float4 *>(p.X + r * DP)[q];
+                x[4 * q] = v.x;
+                x[4 * q + 1] = v.y;
+                x[4 * q + 2] = v.z;
+                x[4 * q + 3] = v.w;
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < DP; ++t) x[t] = t < p.d ? p.X[r * p.d + t] : 0.f;
+        }
         float best = __int_as_float(0x7f800000);
         int bi = 0;
         // four clusters at a time: four independent FMA chains
@@ -336,7 +352,6 @@ __device__ void assign_rows(const Problem &p, int tile, float *smem) {
         p.labels[r] = bi;
         p.d2[r] = 2.f * best + p.xnorm[r];
     }
-    __syncthreads();
 }
 
 __host__ __device__ constexpr int rows_per_item(int tm) { return tm ? 16 * tm : NT; }
@@ -345,20 +360,28 @@ __host__ __device__ constexpr int rows_per_item(int tm) { return tm ? 16 * tm : 
 // (rows x clusters) tile -- its micro-tile stays at most 64 accumulators so every
 // variant fits 128 registers -- or 0, the row-per-thread tile (dpad <= 64,
 // kpad <= 128).
-__device__ __forceinline__ void assign_dispatch(const Problem &p, int tile, float *smem) {
+// cached: the problem whose centroids the row-per-thread tile holds in shared
+// memory (-1: none); a change of problem first waits for every thread of the
+// CTA to be done with the previous tile.
+__device__ __forceinline__ void assign_dispatch(const Problem &p, int pid, int tile, float *smem, int &cached) {
     if (p.tm == 0) {
+        if (cached != pid) __syncthreads();
         switch (p.dpad) {
-            case 8: assign_rows<8>(p, tile, smem); break;
-            case 16: assign_rows<16>(p, tile, smem); break;
-            case 24: assign_rows<24>(p, tile, smem); break;
-            case 32: assign_rows<32>(p, tile, smem); break;
-            case 40: assign_rows<40>(p, tile, smem); break;
-            case 48: assign_rows<48>(p, tile, smem); break;
-            case 56: assign_rows<56>(p, tile, smem); break;
-            case 64: assign_rows<64>(p, tile, smem); break;
+            case 8: assign_rows<8>(p, pid, tile, smem, cached); break;
+            case 16: assign_rows<16>(p, pid, tile, smem, cached); break;
+            case 24: assign_rows<24>(p, pid, tile, smem, cached); break;
+            case 32: assign_rows<32>(p, pid, tile, smem, cached); break;
+            case 40: assign_rows<40>(p, pid, tile, smem, cached); break;
+            case 48: assign_rows<48>(p, pid, tile, smem, cached); break;
+            case 56: assign_rows<56>(p, pid, tile, smem, cached); break;
+            case 64: assign_rows<64>(p, pid, tile, smem, cached); break;
             default: break;
         }
         return;
+    }
+    if (cached >= 0) {  // the tiled variants overwrite the shared centroids
+        __syncthreads();
+        cached = -1;
     }
     switch (p.kpad * 16 + p.tm) {
         case 16 * 16 + 2: assign_tile<16, 2>(p, tile, smem); break;
@@ -629,9 +652,18 @@ __global__ void __launch_bounds__(NT, 2) persistent_kernel(Problem *P, Lists L, 
             if (!P[w.x].done) prep_item(P[w.x], w.y, lane);
         }
         if (!grid_sync(gb)) return;
-        for (long long i = blockIdx.x; i < L.assign.items; i += gridDim.x) {
-            const int2 w = item_of(L.assign, L.n_problems, i);
-            if (!P[w.x].done) assign_dispatch(P[w.x], w.y, fsm);
+        {
+            // contiguous runs of tiles per CTA (four runs each), so consecutive tiles
+            // mostly share a problem: its centroids stay in shared memory
+            const long long run = (L.assign.items + 4ll * gridDim.x - 1) / (4ll * gridDim.x);
+            int cached = -1;
+            for (long long r0 = blockIdx.x * run; r0 < L.assign.items; r0 += (long long)gridDim.x * run) {
+                const long long r1 = min(L.assign.items, r0 + run);
+                for (long long i = r0; i < r1; ++i) {
+                    const int2 w = item_of(L.assign, L.n_problems, i);
+                    if (!P[w.x].done) assign_dispatch(P[w.x], w.x, w.y, fsm, cached);
+                }
+            }
         }
         if (!grid_sync(gb)) return;
         for (long long i = blockIdx.x; i < L.blocks.items; i += gridDim.x) {
@@ -675,7 +707,9 @@ __global__ void tune_fill_kernel(float *p, long long count, unsigned seed) {
 
 __global__ void __launch_bounds__(NT, 2) tune_assign_kernel(const Problem *pp, int tiles) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) assign_dispatch(*pp, t, reinterpret_cast<float *>(smem_raw));
+    int cached = -1;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x)
+        assign_dispatch(*pp, 0, t, reinterpret_cast<float *>(smem_raw), cached);
 }
 
 }  // namespace batched
