@@ -600,6 +600,8 @@ def run_batched(args):
     e1.record()
     torch.cuda.synchronize()
     s = e0.elapsed_time(e1) / 1e3
+    fma_peak = measured_fma_peak_tflops(0, 0)
+    hbm_peak = load_peaks()[0].get("hbm_gbs")
     iters = sum(r[2] for r in res)
     flops = sum(2.0 * X.shape[0] * C0.shape[0] * X.shape[1] * r[2] for (X, C0), r in zip(probs, res))
     nbytes = sum(8.0 * X.shape[0] * X.shape[1] * r[2] for (X, C0), r in zip(probs, res))
@@ -607,6 +609,10 @@ def run_batched(args):
             "seconds": s, "problem_iterations_per_s": iters / s, "rows": sum(p[0].shape[0] for p in probs),
             "row_iterations_per_s": sum(p[0].shape[0] * r[2] for p, r in zip(probs, res)) / s,
             "algorithmic_tflops": flops / s / 1e12, "algorithmic_gbs": nbytes / s / 1e9,
+            "roofline": {"bound": "latency (neither FFMA nor HBM)", "fma_peak_tflops": fma_peak,
+                         "fma_frac": (flops / s / 1e12) / fma_peak if fma_peak else None,
+                         "hbm_peak_gbs": hbm_peak, "hbm_frac": (nbytes / s / 1e9) / hbm_peak if hbm_peak else None,
+                         "note": "whole call (one persistent kernel plus host setup) against the FP32 FMA and HBM peaks"},
             "variants": info["variants"], "classes": len(classes),
             "note": "one call: arena, work lists, row norms and scales, then every iteration in one kernel"}
 

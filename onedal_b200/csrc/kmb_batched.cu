@@ -653,16 +653,13 @@ __global__ void __launch_bounds__(NT, 2) persistent_kernel(Problem *P, Lists L, 
         }
         if (!grid_sync(gb)) return;
         {
-            // contiguous runs of tiles per CTA (four runs each), so consecutive tiles
-            // mostly share a problem: its centroids stay in shared memory
-            const long long run = (L.assign.items + 4ll * gridDim.x - 1) / (4ll * gridDim.x);
+            // round-robin over the tiles, costliest problems first; a problem with more
+            // tiles than the grid has CTAs gives a CTA consecutive tiles of itself, whose
+            // centroids then stay in shared memory
             int cached = -1;
-            for (long long r0 = blockIdx.x * run; r0 < L.assign.items; r0 += (long long)gridDim.x * run) {
-                const long long r1 = min(L.assign.items, r0 + run);
-                for (long long i = r0; i < r1; ++i) {
-                    const int2 w = item_of(L.assign, L.n_problems, i);
-                    if (!P[w.x].done) assign_dispatch(P[w.x], w.x, w.y, fsm, cached);
-                }
+            for (long long i = blockIdx.x; i < L.assign.items; i += gridDim.x) {
+                const int2 w = item_of(L.assign, L.n_problems, i);
+                if (!P[w.x].done) assign_dispatch(P[w.x], w.x, w.y, fsm, cached);
             }
         }
         if (!grid_sync(gb)) return;
