@@ -184,7 +184,7 @@ def run_plain_scale(args, ctx, device=0):
 
     from onedal_b200 import _native, workloads
     w = workloads.PLAIN_GPU
-    X, C0 = workloads.make(w, "cuda")
+    X, C0 = workloads.make(w, "cuda", args.plain_scale_rows or w.n)
     n, d = X.shape
     k = C0.shape[0]
     labels = torch.empty(n, dtype=torch.int32, device="cuda")
@@ -846,6 +846,8 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=30000,
                     help="requests per serving load point (0 skips the serving measurement)")
     ap.add_argument("--serving-lanes", type=int, default=4, help="lanes (streams) of the serving engine")
+    ap.add_argument("--plain-scale-rows", type=int, default=None,
+                    help="rows of the plain-at-scale leg (default: the configured 10,000,000; smaller for profiling)")
     ap.add_argument("--csr-rows", type=int, default=2_000_000,
                     help="rows of the CSR (lloyd_csr) measurement (0 skips it)")
     ap.add_argument("--plusplus-k", type=int, default=1024,
