@@ -699,7 +699,7 @@ def run_b200(args):
         ms = float(t.item())
     value = iters_done / (ms / 1e3)
 
-    # Plain-form comparison (the north-star ratio) on the same data, when timing the BF16 form.
+    # Plain-form comparison (tensor-core form over plain FP32, target >= 3x) on the same data, when timing the BF16 form.
     plain_value = None
     if tc_form and args.plain_steps > 0:
         C.copy_(C0)

@@ -2,7 +2,7 @@
 
 Cases mirror the reference suite (cpp/oneapi/dal/algo/kmeans/test/batch.cpp,
 fixture.hpp) plus seeded synthetic workloads in per-iteration lock-step with
-the FP64 oracle. Tolerances (north-star contract):
+the FP64 oracle. Tolerances:
   responses   exact (plain form: exact except rows whose FP64 top-2 gap is below
               the stated bound; recheck/BF16x3 forms: exact)
   centroids   1e-5 relative (float32) / 1e-12 (float64) vs the FP64 oracle
