@@ -82,7 +82,7 @@ struct Model {
 
 constexpr int64_t kTcChunkRows = 1 << 18;
 constexpr size_t kTcReserveBytes = (size_t)448 << 20;  // one worker's workspace at kTcChunkRows rows, d <= 256
-constexpr int kTcWorkers = 2;
+constexpr int kTcWorkers = 2;  // default; KMB_SERVER_TC_WORKERS (1 .. 8) overrides
 constexpr double kBatchMacs = 4294967296.0;      // cap on a lane batch's n * kpad * dpad (one large request may exceed it alone)
 
 struct Request {
@@ -114,6 +114,7 @@ struct Lane;
 struct Server {
     int device = 0;
     int64_t tc_chunk_rows = kTcChunkRows;  // KMB_SERVER_TC_CHUNK_ROWS (4096 .. kTcChunkRows)
+    int tc_workers = kTcWorkers;
     size_t budget = 0;
     size_t in_use = 0, peak_in_use = 0;
     std::mutex mu;
@@ -620,6 +621,7 @@ int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32
     // CTAs start sooner (at a per-launch cost)
     if (const char *e = std::getenv("KMB_SERVER_TC_CHUNK_ROWS"))
         srv->tc_chunk_rows = std::min<int64_t>(std::max<int64_t>(atoll(e), 4096), kTcChunkRows);
+    if (const char *e = std::getenv("KMB_SERVER_TC_WORKERS")) srv->tc_workers = std::min(std::max(atoi(e), 1), 8);
     // Keep freed request memory in the stream-ordered pool instead of returning it to the driver.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -652,15 +654,15 @@ int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32
         srv->lanes.push_back(l);
     }
     // The tensor-core worker needs its workspace reserved; small budgets serve everything on the lanes.
-    if (srv->budget >= 4 * kTcWorkers * kTcReserveBytes) {
+    if (srv->budget >= 4 * (size_t)srv->tc_workers * kTcReserveBytes) {
         srv->tc_enabled = true;
-        srv->base_use = kTcWorkers * kTcReserveBytes;
+        srv->base_use = (size_t)srv->tc_workers * kTcReserveBytes;
         srv->in_use = srv->peak_in_use = srv->base_use;
     }
     srv->threads.emplace_back(scheduler_loop, srv);
     for (Lane *l : srv->lanes) l->completer = std::thread(completer_loop, l);
     if (srv->tc_enabled)
-        for (int i = 0; i < kTcWorkers; ++i) srv->threads.emplace_back(tc_worker_loop, srv);
+        for (int i = 0; i < srv->tc_workers; ++i) srv->threads.emplace_back(tc_worker_loop, srv);
     for (int i = 0; i < trainers; ++i) srv->threads.emplace_back(trainer_loop, srv);
     *out = srv;
     return KMB_OK;

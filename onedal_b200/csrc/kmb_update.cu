@@ -855,6 +855,42 @@ __global__ void colmax_kernel(const float *__restrict__ X, int64_t n, int d, uns
         if (smax[t]) atomicMax(&colbits[t], smax[t]);
 }
 
+// The same maxima for d <= 1024 with one register maximum per (thread, column):
+// thread t covers column t % d of every (256 / d)-th row when d <= 256, else
+// columns t, t + 256, ... of every row; reads are coalesced along the rows and
+// each thread issues one atomic per column at the end (NaN never compares greater
+// and is skipped, as above).
+__global__ void __launch_bounds__(256) colmax_rows_kernel(const float *__restrict__ X, int64_t n, int d,
+                                                          unsigned *__restrict__ colbits, const LoopState *st) {
+    if (is_done(st)) return;
+    if (d <= 256) {
+        const int rpb = 256 / d;
+        if ((int)threadIdx.x >= rpb * d) return;
+        const int c = threadIdx.x % d;
+        float m = 0.0f;
+        for (int64_t r = (int64_t)blockIdx.x * rpb + threadIdx.x / d; r < n; r += (int64_t)gridDim.x * rpb) {
+            const float v = fabsf(X[r * d + c]);
+            if (v > m) m = v;
+        }
+        if (m > 0.0f) atomicMax(&colbits[c], __float_as_uint(m));
+    } else {
+        float m[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (int64_t r = blockIdx.x; r < n; r += gridDim.x) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int c = threadIdx.x + 256 * q;
+                if (c < d) {
+                    const float v = fabsf(X[r * d + c]);
+                    if (v > m[q]) m[q] = v;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (m[q] > 0.0f) atomicMax(&colbits[threadIdx.x + 256 * q], __float_as_uint(m[q]));
+    }
+}
+
 __global__ void colmax_global_kernel(const float *__restrict__ X, int64_t n, int d, unsigned *__restrict__ colbits,
                                      const LoopState *st) {
     if (is_done(st)) return;
@@ -1279,7 +1315,9 @@ void prepare_exact_update(const float *X, int64_t n, int64_t d, Workspace &ws, L
     cudaMemsetAsync(colexp, 0, sizeof(int) * d, s);
     const int64_t total = n * d;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 8));
-    if (d <= 8192) {
+    if (d <= 1024) {
+        colmax_rows_kernel<<<148 * 8, 256, 0, s>>>(X, n, (int)d, (unsigned *)colexp, st);
+    } else if (d <= 8192) {
         colmax_kernel<<<blocks, 256, sizeof(unsigned) * d, s>>>(X, n, (int)d, (unsigned *)colexp, st);
     } else {
         colmax_global_kernel<<<blocks, 256, 0, s>>>(X, n, (int)d, (unsigned *)colexp, st);
