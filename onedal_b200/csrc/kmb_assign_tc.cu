@@ -424,24 +424,31 @@ __device__ __forceinline__ void top3_insert(Top3 &r, float &thr, float thr0, flo
 
 // One 32-column chunk of a row into its running top-3. The chunk is reduced to
 // its maximum (3-input max.f32); only when a lane of the warp holds a value at or
-// above its threshold are the 11 column triples walked, a triple being visited
-// (warp-uniformly, static register indices) when some lane's triple maximum
-// reaches that lane's threshold.
+// above its threshold are the column triples walked, group by group, a triple
+// being visited (warp-uniformly, static register indices) when some lane's
+// triple maximum reaches that lane's threshold.
 __device__ __forceinline__ void scan_chunk(const float (&w)[32], int colbase, float thr0, float band_up, float &thr,
                                            Top3 &r) {
     float m[11];
 #pragma unroll
     for (int i = 0; i < 10; ++i) m[i] = max3f(w[3 * i], w[3 * i + 1], w[3 * i + 2]);
     m[10] = fmaxf(w[30], w[31]);
-    const float m1 = max3f(max3f(m[0], m[1], m[2]), max3f(m[3], m[4], m[5]),
-                           max3f(m[6], m[7], max3f(m[8], m[9], m[10])));
+    // four groups of triples (columns 0-8, 9-17, 18-26, 27-31): a group is walked
+    // only when some lane's group maximum reaches that lane's threshold
+    const float gm[4] = {max3f(m[0], m[1], m[2]), max3f(m[3], m[4], m[5]), max3f(m[6], m[7], m[8]), fmaxf(m[9], m[10])};
+    const float m1 = max3f(gm[0], gm[1], fmaxf(gm[2], gm[3]));
     if (__any_sync(0xffffffffu, m1 >= thr)) {
 #pragma unroll
-        for (int g = 0; g < 11; ++g) {
-            if (__any_sync(0xffffffffu, m[g] >= thr)) {
+        for (int q = 0; q < 4; ++q) {
+            if (__any_sync(0xffffffffu, gm[q] >= thr)) {
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
-                    if (3 * g + i < 32) top3_insert(r, thr, thr0, band_up, w[3 * g + i], colbase + 3 * g + i);
+                for (int g = 3 * q; g < 3 * q + 3 && g < 11; ++g) {
+                    if (__any_sync(0xffffffffu, m[g] >= thr)) {
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+                            if (3 * g + i < 32) top3_insert(r, thr, thr0, band_up, w[3 * g + i], colbase + 3 * g + i);
+                    }
+                }
             }
         }
     }
