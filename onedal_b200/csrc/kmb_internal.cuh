@@ -259,12 +259,14 @@ struct Limbs {
 // of fewer than 2^31 values stay below 2^63, and any order of additions and
 // subtractions gives the same integer l2 * 2^64 + l1 * 2^32 + l0.
 __device__ __forceinline__ Limbs fixed_of(float x, int e) {
-    const float f = scalbnf(x, e);  // exact: |f| < 2^94, a power-of-two scaling
-    const unsigned bits = __float_as_uint(f);
+    // x = mant * 2^((be ? be : 1) - 150) exactly, so x * 2^e = mant * 2^sh with the
+    // exponent added as an integer (no float scaling; the same integer as scaling
+    // first whenever |x| * 2^e < 2^94). Non-finite x keeps its raw pattern (sh 105).
+    const unsigned bits = __float_as_uint(x);
     const int be = (int)((bits >> 23) & 0xffu);
     unsigned long long mant = bits & 0x7fffffu;
     if (be) mant |= 0x800000u;
-    const int sh = (be ? be : 1) - 150;  // f = mant * 2^sh, sh <= 70
+    const int sh = be == 255 ? 105 : (be ? be : 1) - 150 + e;  // mant * 2^sh < 2^94
     long long l0 = 0, l1 = 0, l2 = 0;
     if (sh >= 0) {
         const int q = sh >> 5;

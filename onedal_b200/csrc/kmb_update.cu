@@ -976,13 +976,17 @@ segsum_fixed_kernel(const float *__restrict__ X, int d, int k, const int32_t *__
         if (col < d) {
             const int ex = colexp[col];
             int i = rr;
-            for (; i + 1 * rp < cnt; i += 2 * rp) {
-                const float v0 = X[(int64_t)rows[i] * d + col];
-                const float v1 = X[(int64_t)rows[i + rp] * d + col];
-                const Limbs L0 = fixed_of(v0, ex), L1 = fixed_of(v1, ex);
-                a0 += L0.l0 + L1.l0;
-                a1 += L0.l1 + L1.l1;
-                a2 += L0.l2 + L1.l2;
+            for (; i + 3 * rp < cnt; i += 4 * rp) {  // four gathered loads in flight per thread
+                float v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) v[u] = X[(int64_t)rows[i + u * rp] * d + col];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const Limbs L = fixed_of(v[u], ex);
+                    a0 += L.l0;
+                    a1 += L.l1;
+                    a2 += L.l2;
+                }
             }
             for (; i < cnt; i += rp) {
                 const Limbs L = fixed_of(X[(int64_t)rows[i] * d + col], ex);
