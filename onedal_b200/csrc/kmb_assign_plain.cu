@@ -46,6 +46,29 @@ __device__ __forceinline__ bool lex_less(F a, int ia, F b, int ib) {
     return a < b || (a == b && ia < ib);
 }
 
+// acc[i][j] += a[i] * b[j] for the thread's 8 x 8 tile; for float as packed
+// pairs (fma.rn.f32x2: two correctly rounded FMAs, the same results as fmaf).
+template <typename F>
+__device__ __forceinline__ void fma_tile(F (&acc)[8][8], const F (&a)[8], const F (&b)[8]) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+}
+template <>
+__device__ __forceinline__ void fma_tile<float>(float (&acc)[8][8], const float (&a)[8], const float (&b)[8]) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float2 ai = make_float2(a[i], a[i]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float2 t = __ffma2_rn(ai, make_float2(b[2 * q], b[2 * q + 1]), make_float2(acc[i][2 * q], acc[i][2 * q + 1]));
+            acc[i][2 * q] = t.x;
+            acc[i][2 * q + 1] = t.y;
+        }
+    }
+}
+
 template <typename F>
 struct RowTop {
     F b, s, t;   // best, second, third score
@@ -201,10 +224,7 @@ assign_plain_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restri
             a[4] = a1.x; a[5] = a1.y; a[6] = a1.z; a[7] = a1.w;
             b[0] = b0.x; b[1] = b0.y; b[2] = b0.z; b[3] = b0.w;
             b[4] = b1.x; b[5] = b1.y; b[6] = b1.z; b[7] = b1.w;
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            fma_tile(acc, a, b);
         }
         const int nt = step / nk;
         if (step - nt * nk == nk - 1) {

@@ -357,9 +357,10 @@ __device__ void assign_rows(const Problem &p, int pid, int tile, float *smem, in
 __host__ __device__ constexpr int rows_per_item(int tm) { return tm ? 16 * tm : NT; }
 
 // The tile variants the autotuner chooses from: rows per thread 2, 4, 8 of the
-// (rows x clusters) tile -- its micro-tile stays at most 64 accumulators so every
-// variant fits 128 registers -- or 0, the row-per-thread tile (dpad <= 64,
-// kpad <= 128).
+// (rows x clusters) tile -- its micro-tile stays at most 32 accumulators so every
+// variant fits the 80 registers of three CTAs per SM (the kernel is bound by
+// memory latency, so the third CTA's warps pay more than larger tiles would) --
+// or 0, the row-per-thread tile (dpad <= 64, kpad <= 128).
 // cached: the problem whose centroids the row-per-thread tile holds in shared
 // memory (-1: none); a change of problem first waits for every thread of the
 // CTA to be done with the previous tile.
@@ -395,9 +396,7 @@ __device__ __forceinline__ void assign_dispatch(const Problem &p, int pid, int t
         case 64 * 16 + 8: assign_tile<64, 8>(p, tile, smem); break;
         case 128 * 16 + 2: assign_tile<128, 2>(p, tile, smem); break;
         case 128 * 16 + 4: assign_tile<128, 4>(p, tile, smem); break;
-        case 128 * 16 + 8: assign_tile<128, 8>(p, tile, smem); break;
         case 256 * 16 + 2: assign_tile<256, 2>(p, tile, smem); break;
-        case 256 * 16 + 4: assign_tile<256, 4>(p, tile, smem); break;
         default: break;
     }
 }
@@ -630,7 +629,7 @@ size_t smem_bytes(int kmax, int dmax) {
     return std::max(std::max(assign, acc), std::max(setup, decide));
 }
 
-__global__ void __launch_bounds__(NT, 2) persistent_kernel(Problem *P, Lists L, GridBarrier *gb) {
+__global__ void __launch_bounds__(NT, 3) persistent_kernel(Problem *P, Lists L, GridBarrier *gb) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *fsm = reinterpret_cast<float *>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -702,7 +701,7 @@ __global__ void tune_fill_kernel(float *p, long long count, unsigned seed) {
     }
 }
 
-__global__ void __launch_bounds__(NT, 2) tune_assign_kernel(const Problem *pp, int tiles) {
+__global__ void __launch_bounds__(NT, 3) tune_assign_kernel(const Problem *pp, int tiles) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     int cached = -1;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x)
@@ -728,7 +727,7 @@ int tuned_tm(int dev, int dpad, int kpad, cudaStream_t s) {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto found = g_tuned.find(key);
     if (found != g_tuned.end()) return found->second;
-    std::vector<int> cands = kpad >= 256 ? std::vector<int>{2, 4} : std::vector<int>{2, 4, 8};
+    std::vector<int> cands = kpad >= 256 ? std::vector<int>{2} : kpad >= 128 ? std::vector<int>{2, 4} : std::vector<int>{2, 4, 8};
     if (dpad <= 64 && kpad <= 128) cands.push_back(0);
     const long long n = 32768;
     float *X = nullptr, *Ct = nullptr, *h = nullptr, *d2 = nullptr, *xn = nullptr;
