@@ -46,7 +46,8 @@ typedef enum kmb_status {
     KMB_ECUDA = 3,
     KMB_ETIMEDOUT = 4,
     KMB_ETOO_MANY_EMPTY = 5,
-    KMB_EUNSUPPORTED = 6
+    KMB_EUNSUPPORTED = 6,
+    KMB_ECOMM = 7 /* a communicator callback of kmb_train_spmd reported failure */
 } kmb_status;
 
 /* Element type of data and centroids: the descriptor's float_t. */
@@ -221,6 +222,38 @@ KMB_API int kmb_finalize_centroids(kmb_context *ctx, int dtype, const double *su
                                    const void *C_in, int64_t k, int64_t d, void *C_out, double *shift,
                                    int32_t *empty_ids, int64_t *n_empty);
 
+/* ---- Sharded training through the caller's communicator ------------------
+ * One call per rank (one process per GPU), each with its own block of rows; every
+ * rank returns the same centroids. The loop is the one the reference's SPMD path
+ * runs (cpp/oneapi/dal/algo/kmeans/backend/gpu/cluster_updater.hpp:117-153,
+ * backend/gpu/empty_cluster_handling_dpc.cpp:273-300): per iteration each rank
+ * computes its rows' labels and FP64 per-cluster sums/counts (kmb_partial_sums),
+ * the ranks sum [sums | counts | squared distances] with ONE allreduce_sum_f64
+ * call, every rank finalizes identically (kmb_finalize_centroids); when clusters
+ * are empty, every rank offers its m farthest rows (m = number of empty clusters)
+ * through ONE allgather call and the global m farthest by (distance descending,
+ * global row ascending) reseed the empty clusters in ascending order; stop when
+ * the shift <= accuracy_threshold. After the loop: labels of this rank's rows under
+ * the final centroids and the objective summed over ranks. Every rank must call
+ * with the same C0, params, k and d. The callbacks work on host memory and return
+ * 0 on success (anything else ends the call with KMB_ECOMM on that rank):
+ *   allreduce_sum_f64(user, buf, count): in-place elementwise sum over ranks;
+ *   allgather(user, send, bytes, recv): recv receives size * bytes, rank order.
+ * Device pointers: X (n x d, this rank's rows), C0 and C_out (k x d), labels (n).
+ * The oneDAL host-policy SPMD dispatchers stay `unimplemented`, as the reference's
+ * host backend's are; this entry serves a caller that brings its own
+ * communicator (NCCL, MPI, gloo) around the library. */
+typedef struct kmb_communicator {
+    void *user;
+    int32_t rank, size;
+    int (*allreduce_sum_f64)(void *user, double *buf, int64_t count);
+    int (*allgather)(void *user, const void *send, int64_t bytes, void *recv);
+} kmb_communicator;
+
+KMB_API int kmb_train_spmd(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, const void *C0,
+                           const kmb_params *params, const kmb_communicator *comm, void *C_out, int32_t *labels,
+                           double *objective, int64_t *iteration_count);
+
 /* Lloyd iterations only, in place, device memory: C (k x d) holds the initial
  * centroids on entry and the updated ones on return; labels (n) receive the
  * assignment of the last completed update. Runs up to max_iteration_count
@@ -309,6 +342,7 @@ typedef struct kmb_batched_info {
     int32_t variants;         /* assignment tile variants (rows per thread x cluster tile) in use */
     int64_t total_iterations; /* summed over problems */
     int64_t graph_launches;
+    double kernel_ms;         /* device time of the persistent kernel (CUDA events), host set-up excluded */
 } kmb_batched_info;
 
 KMB_API int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64_t count, int64_t max_iteration_count,

@@ -10,7 +10,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libonedal_b200_kmeans.so")
 
-KMB_OK, KMB_EINVAL, KMB_ENOMEM, KMB_ECUDA, KMB_ETIMEDOUT, KMB_ETOO_MANY_EMPTY, KMB_EUNSUPPORTED = range(7)
+KMB_OK, KMB_EINVAL, KMB_ENOMEM, KMB_ECUDA, KMB_ETIMEDOUT, KMB_ETOO_MANY_EMPTY, KMB_EUNSUPPORTED, KMB_ECOMM = range(8)
 KMB_F32, KMB_F64 = 0, 1
 KMB_FMA_PEAK_F32X2 = 2  # kmb_measure_fma_peak: packed FP32 pair FMA
 KMB_MEM_HOST, KMB_MEM_DEVICE = 0, 1
@@ -26,8 +26,19 @@ EXPORTED = (
     "kmb_server_submit_train", "kmb_server_wait", "kmb_server_get_stats", "kmb_server_infer_form", "kmb_server_wait_detail", "kmb_context_set_max_sms", "kmb_init_plusplus", "kmb_batched_train",
     "kmb_model_serialize", "kmb_model_deserialize", "kmb_server_add_model_serialized",
     "kmb_train_csr", "kmb_infer_csr", "kmb_init_plusplus_csr", "kmb_context_recheck_rows",
-    "kmb_measure_fma_peak",
+    "kmb_measure_fma_peak", "kmb_train_spmd",
 )
+
+
+# kmb_communicator callbacks: int allreduce_sum_f64(void *user, double *buf, int64_t count) and
+# int allgather(void *user, const void *send, int64_t bytes, void *recv)
+ALLREDUCE_F64_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int64)
+ALLGATHER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p)
+
+
+class kmb_communicator(ctypes.Structure):
+    _fields_ = [("user", ctypes.c_void_p), ("rank", ctypes.c_int32), ("size", ctypes.c_int32),
+                ("allreduce_sum_f64", ALLREDUCE_F64_FN), ("allgather", ALLGATHER_FN)]
 
 
 class kmb_batched_problem(ctypes.Structure):
@@ -38,7 +49,7 @@ class kmb_batched_problem(ctypes.Structure):
 
 class kmb_batched_info(ctypes.Structure):
     _fields_ = [("problems", ctypes.c_int64), ("variants", ctypes.c_int32), ("total_iterations", ctypes.c_int64),
-                ("graph_launches", ctypes.c_int64)]
+                ("graph_launches", ctypes.c_int64), ("kernel_ms", ctypes.c_double)]
 
 
 class kmb_server_stats(ctypes.Structure):
@@ -97,6 +108,8 @@ def load_library(path: str = LIB_PATH):
             lib.kmb_lloyd_step.argtypes = [P, ctypes.c_int, P, I64, I64, P, I64, I32, I32, P, P, ctypes.POINTER(D),
                                            ctypes.POINTER(I64)]
             lib.kmb_partial_sums.argtypes = [P, ctypes.c_int, P, I64, I64, P, I64, I32, P, P, P, P, P]
+            lib.kmb_train_spmd.argtypes = [P, ctypes.c_int, P, I64, I64, P, P, ctypes.POINTER(kmb_communicator), P, P,
+                                           ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
             lib.kmb_finalize_centroids.argtypes = [P, ctypes.c_int, P, P, P, I64, I64, P, ctypes.POINTER(D), P,
                                                    ctypes.POINTER(I64)]
             lib.kmb_lloyd_iterate.argtypes = [P, ctypes.c_int, P, I64, I64, P, ctypes.POINTER(kmb_params), P,

@@ -26,21 +26,33 @@ def batched_train(problems, max_iteration_count: int = 30, accuracy_threshold: f
                   stream=None):
     """problems: list of (X, C0) CUDA float32 tensors. Returns (list of (C, labels, iterations), info dict)."""
     lib = _native.load_library()
-    arr = (_native.kmb_batched_problem * len(problems))()
-    keep = []
-    for i, (X, C0) in enumerate(problems):
+    count = len(problems)
+    arr = (_native.kmb_batched_problem * count)()
+    xs = []
+    for X, C0 in problems:
         if not (X.is_cuda and C0.is_cuda) or X.dtype != torch.float32 or C0.dtype != torch.float32:
             raise BatchedError("problems must be CUDA float32 tensors")
-        X = X.contiguous()
-        C = C0.clone().contiguous()
-        lab = torch.empty(X.shape[0], dtype=torch.int32, device=X.device)
-        keep.append((X, C, lab))
+        xs.append(X.contiguous())
+    # every problem's centroids in one buffer (one copy) and every label array in another,
+    # instead of a copy and an allocation per problem
+    dev = xs[0].device if count else torch.device("cuda")
+    C_all = torch.cat([C0.reshape(-1) for _, C0 in problems]) if count else torch.empty(0, device=dev)
+    lab_all = torch.empty(sum(X.shape[0] for X in xs), dtype=torch.int32, device=dev)
+    c_ptr, l_ptr = C_all.data_ptr(), lab_all.data_ptr()
+    keep = []
+    co = lo = 0
+    for i, (X, (_, C0)) in enumerate(zip(xs, problems)):
+        n, d = X.shape
+        k = C0.shape[0]
         arr[i].X = X.data_ptr()
-        arr[i].n = X.shape[0]
-        arr[i].d = X.shape[1]
-        arr[i].C = C.data_ptr()
-        arr[i].k = C.shape[0]
-        arr[i].labels = lab.data_ptr()
+        arr[i].n = n
+        arr[i].d = d
+        arr[i].C = c_ptr + 4 * co
+        arr[i].k = k
+        arr[i].labels = l_ptr + 4 * lo
+        keep.append((C_all[co:co + k * d].view(k, d), lab_all[lo:lo + n]))
+        co += k * d
+        lo += n
     info = _native.kmb_batched_info()
     s = stream or torch.cuda.current_stream()
     rc = lib.kmb_batched_train(_native.KMB_F32, ctypes.cast(arr, ctypes.c_void_p), len(problems),
@@ -48,5 +60,5 @@ def batched_train(problems, max_iteration_count: int = 30, accuracy_threshold: f
                                ctypes.c_void_p(s.cuda_stream), ctypes.byref(info))
     if rc != _native.KMB_OK:
         raise BatchedError(f"kmb_batched_train failed: {lib.kmb_status_string(rc).decode()}")
-    out = [(C, lab, int(arr[i].iterations)) for i, (X, C, lab) in enumerate(keep)]
+    out = [(C, lab, int(arr[i].iterations)) for i, (C, lab) in enumerate(keep)]
     return out, {f: getattr(info, f) for f, _ in info._fields_}

@@ -13,6 +13,8 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdint>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -857,6 +859,152 @@ int validate_csr_call(kmb_context *ctx, int dtype, int memory, const void *vals,
     return KMB_OK;
 }
 
+
+// ---- sharded training through a caller's communicator (kmb_train_spmd) --------
+
+// Candidate rows for the sharded reseed: their squared distances and row vectors.
+template <typename F>
+__global__ void spmd_gather_kernel(const F *__restrict__ X, int d, const long long *__restrict__ rows,
+                                   const F *__restrict__ row_sq, int m, double *__restrict__ vals,
+                                   F *__restrict__ vecs) {
+    for (int e = blockIdx.x; e < m; e += gridDim.x) {
+        const long long r = rows[e];
+        if (threadIdx.x == 0) vals[e] = (double)row_sq[r];
+        for (int t = threadIdx.x; t < d; t += blockDim.x) vecs[(int64_t)e * d + t] = X[r * d + t];
+    }
+}
+
+template <typename F>
+int train_spmd_impl(kmb_context *ctx, int dtype, const F *X, int64_t n, int64_t d, const F *C0, kmb_params p,
+                    const kmb_communicator *comm, F *C_out, int32_t *labels, double *objective, int64_t *iters) {
+    const int64_t k = p.cluster_count, kd = k * d;
+    kmb::Workspace &ws = ctx->ws;
+    cudaStream_t s = ctx->stream;
+    // every rank's row count: this rank's first global row and the total
+    std::vector<int64_t> ns((size_t)comm->size, 0);
+    if (comm->allgather(comm->user, &n, (int64_t)sizeof(int64_t), ns.data()))
+        return fail(ctx, KMB_ECOMM, "allgather of the row counts failed");
+    int64_t row0 = 0, total = 0;
+    for (int r = 0; r < comm->size; ++r) {
+        if (r < comm->rank) row0 += ns[r];
+        total += ns[r];
+    }
+    if (k > total) return fail(ctx, KMB_EINVAL, "cluster count exceeds data row count");
+    if (!ws.ensure(ws.sp_sums, sizeof(double) * kd) || !ws.ensure(ws.sp_counts, sizeof(int64_t) * k) ||
+        !ws.ensure(ws.sp_sq, sizeof(double)) || !ws.ensure(ws.sp_rowsq, sizeof(F) * n) ||
+        !ws.ensure(ws.sp_Ca, sizeof(F) * kd) || !ws.ensure(ws.sp_Cb, sizeof(F) * kd) ||
+        !ws.ensure(ws.sp_ids, sizeof(int32_t) * k) || !ws.ensure(ws.sp_rows, sizeof(long long) * k) ||
+        !ws.ensure(ws.sp_state, sizeof(LoopState)) || !ws.ensure(ws.sp_gather, (sizeof(double) + sizeof(F) * d) * k))
+        return fail(ctx, KMB_ENOMEM, "sharded training buffers");
+    double *sums = (double *)ws.sp_sums.ptr, *sq = (double *)ws.sp_sq.ptr;
+    int64_t *counts = (int64_t *)ws.sp_counts.ptr;
+    F *row_sq = (F *)ws.sp_rowsq.ptr;
+    F *Ccur = (F *)ws.sp_Ca.ptr, *Cnew = (F *)ws.sp_Cb.ptr;
+    int32_t *ids = (int32_t *)ws.sp_ids.ptr;
+    long long *rows = (long long *)ws.sp_rows.ptr;
+    double *gvals = (double *)ws.sp_gather.ptr;
+    F *gvecs = (F *)(gvals + k);
+    std::vector<double> packed((size_t)(kd + k + 1));
+    std::vector<int64_t> hcounts((size_t)k);
+    KMB_CUDA(cudaMemcpyAsync(Ccur, C0, sizeof(F) * kd, cudaMemcpyDeviceToDevice, s));
+    int64_t it = 0;
+    int rc;
+    while (it < p.max_iteration_count) {
+        if ((rc = partial_impl<F>(ctx, X, n, d, Ccur, k, p.form, labels, sums, counts, sq, row_sq))) return rc;
+        // one exchange: [sums | counts | squared distances] summed over the ranks
+        KMB_CUDA(cudaMemcpyAsync(packed.data(), sums, sizeof(double) * kd, cudaMemcpyDeviceToHost, s));
+        KMB_CUDA(cudaMemcpyAsync(hcounts.data(), counts, sizeof(int64_t) * k, cudaMemcpyDeviceToHost, s));
+        KMB_CUDA(cudaMemcpyAsync(&packed[kd + k], sq, sizeof(double), cudaMemcpyDeviceToHost, s));
+        KMB_CUDA(cudaStreamSynchronize(s));
+        for (int64_t j = 0; j < k; ++j) packed[kd + j] = (double)hcounts[j];  // exact below 2^53
+        if (comm->allreduce_sum_f64(comm->user, packed.data(), kd + k + 1))
+            return fail(ctx, KMB_ECOMM, "allreduce of the cluster sums failed");
+        for (int64_t j = 0; j < k; ++j) hcounts[j] = (int64_t)std::llround(packed[kd + j]);
+        KMB_CUDA(cudaMemcpyAsync(sums, packed.data(), sizeof(double) * kd, cudaMemcpyHostToDevice, s));
+        KMB_CUDA(cudaMemcpyAsync(counts, hcounts.data(), sizeof(int64_t) * k, cudaMemcpyHostToDevice, s));
+        double shift = 0.0;
+        int64_t ne = 0;
+        if ((rc = kmb_finalize_centroids(ctx, dtype, sums, counts, Ccur, k, d, Cnew, &shift, ids, &ne))) return rc;
+        if (ne > 0) {
+            // every rank offers its m farthest rows; the global m farthest by (distance
+            // descending, global row ascending) reseed the empty clusters, ascending
+            const int m = (int)ne, take = (int)std::min<int64_t>(m, n);
+            if (!kmb::launch_top_rows<F>(row_sq, n, take, ws, (LoopState *)ws.sp_state.ptr, rows, s))
+                return fail(ctx, KMB_ENOMEM, "candidate selection buffers");
+            if (take > 0) {
+                spmd_gather_kernel<F><<<(unsigned)std::min(take, 1024), 128, 0, s>>>(X, (int)d, rows, row_sq, take,
+                                                                                      gvals, gvecs);
+                KMB_LAUNCHED();
+            }
+            const size_t rec = (16 + sizeof(F) * (size_t)d + 7) / 8 * 8;  // value, global row, row vector
+            std::vector<unsigned char> send(rec * (size_t)m, 0), recv(rec * (size_t)m * (size_t)comm->size);
+            std::vector<long long> hrows((size_t)std::max(take, 1));
+            std::vector<double> hvals((size_t)std::max(take, 1));
+            std::vector<F> hvecs((size_t)std::max(take, 1) * (size_t)d);
+            std::vector<int32_t> hids((size_t)m);
+            std::vector<F> hC((size_t)kd);
+            if (take > 0) {
+                KMB_CUDA(cudaMemcpyAsync(hrows.data(), rows, sizeof(long long) * take, cudaMemcpyDeviceToHost, s));
+                KMB_CUDA(cudaMemcpyAsync(hvals.data(), gvals, sizeof(double) * take, cudaMemcpyDeviceToHost, s));
+                KMB_CUDA(cudaMemcpyAsync(hvecs.data(), gvecs, sizeof(F) * take * d, cudaMemcpyDeviceToHost, s));
+            }
+            KMB_CUDA(cudaMemcpyAsync(hids.data(), ids, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaMemcpyAsync(hC.data(), Ccur, sizeof(F) * kd, cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaStreamSynchronize(s));
+            for (int e = 0; e < m; ++e) {
+                unsigned char *r = send.data() + rec * e;
+                const double v = e < take ? (std::isnan(hvals[e]) ? -INFINITY : hvals[e]) : -INFINITY;
+                const long long g = e < take ? row0 + hrows[e] : INT64_MAX;
+                std::memcpy(r, &v, 8);
+                std::memcpy(r + 8, &g, 8);
+                if (e < take) std::memcpy(r + 16, hvecs.data() + (size_t)e * d, sizeof(F) * d);
+            }
+            if (comm->allgather(comm->user, send.data(), (int64_t)send.size(), recv.data()))
+                return fail(ctx, KMB_ECOMM, "allgather of the reseed candidates failed");
+            const size_t total_recs = (size_t)m * (size_t)comm->size;
+            std::vector<size_t> order(total_recs);
+            std::vector<double> av(total_recs);
+            std::vector<long long> ar(total_recs);
+            for (size_t i = 0; i < total_recs; ++i) {
+                order[i] = i;
+                std::memcpy(&av[i], recv.data() + rec * i, 8);
+                std::memcpy(&ar[i], recv.data() + rec * i + 8, 8);
+            }
+            std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+                return av[a] > av[b] || (av[a] == av[b] && ar[a] < ar[b]);
+            });
+            for (int e = 0; e < m; ++e) {
+                const size_t i = order[e];
+                if (!std::isfinite(av[i]))
+                    return fail(ctx, KMB_ETOO_MANY_EMPTY, "fewer candidate rows than empty clusters");
+                const F *vec = reinterpret_cast<const F *>(recv.data() + rec * i + 16);
+                const int cid = hids[e];
+                double a = 0.0;
+                for (int64_t t = 0; t < d; ++t) {
+                    const double df = (double)hC[(size_t)cid * d + t] - (double)vec[t];
+                    a += df * df;
+                }
+                shift += a;
+                KMB_CUDA(cudaMemcpyAsync(Cnew + (int64_t)cid * d, vec, sizeof(F) * d, cudaMemcpyHostToDevice, s));
+            }
+            KMB_CUDA(cudaStreamSynchronize(s));  // the host rows above are copied before they go out of scope
+        }
+        std::swap(Ccur, Cnew);
+        ++it;
+        if (shift <= p.accuracy_threshold) break;
+    }
+    // responses of this rank's rows and the objective under the final centroids
+    if ((rc = partial_impl<F>(ctx, X, n, d, Ccur, k, p.form, labels, sums, counts, sq, nullptr))) return rc;
+    double obj = 0.0;
+    KMB_CUDA(cudaMemcpyAsync(&obj, sq, sizeof(double), cudaMemcpyDeviceToHost, s));
+    KMB_CUDA(cudaMemcpyAsync(C_out, Ccur, sizeof(F) * kd, cudaMemcpyDeviceToDevice, s));
+    KMB_CUDA(cudaStreamSynchronize(s));
+    if (comm->allreduce_sum_f64(comm->user, &obj, 1)) return fail(ctx, KMB_ECOMM, "allreduce of the objective failed");
+    if (objective) *objective = obj;
+    if (iters) *iters = it;
+    return KMB_OK;
+}
+
 }  // namespace
 
 // k-means++ initialisation (kmb_init.cu has the device side). The host draws
@@ -965,6 +1113,31 @@ extern "C" {
 
 const char *kmb_version(void) { return "onedal_b200 kmeans 0.1 (sm_100a)"; }
 
+int kmb_train_spmd(kmb_context *ctx, int dtype, const void *X, int64_t n, int64_t d, const void *C0,
+                   const kmb_params *params, const kmb_communicator *comm, void *C_out, int32_t *labels,
+                   double *objective, int64_t *iteration_count) {
+    if (!ctx) return KMB_EINVAL;
+    ctx->last_error.clear();
+    if (!params || !comm || !comm->allreduce_sum_f64 || !comm->allgather || comm->size <= 0 || comm->rank < 0 ||
+        comm->rank >= comm->size)
+        return fail(ctx, KMB_EINVAL, "bad params or communicator");
+    if (dtype != KMB_F32 && dtype != KMB_F64) return fail(ctx, KMB_EINVAL, "unknown dtype %d", dtype);
+    if (n <= 0 || n > INT32_MAX || d <= 0) return fail(ctx, KMB_EINVAL, "bad shape");
+    kmb_params p = *params;
+    if (p.cluster_count <= 0 || p.cluster_count > INT32_MAX || p.max_iteration_count < 0 || !(p.accuracy_threshold >= 0))
+        return fail(ctx, KMB_EINVAL, "bad params");
+    int rc = check_form(ctx, dtype, p.form);
+    if (rc) return rc;
+    if (!X || !C0 || !C_out || !labels) return fail(ctx, KMB_EINVAL, "null device pointer");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, KMB_ECUDA, "cudaSetDevice failed");
+    p.form = resolve_form(dtype, p.form, n, p.cluster_count, d);
+    if (dtype == KMB_F32)
+        return train_spmd_impl<float>(ctx, dtype, (const float *)X, n, d, (const float *)C0, p, comm, (float *)C_out,
+                                      labels, objective, iteration_count);
+    return train_spmd_impl<double>(ctx, dtype, (const double *)X, n, d, (const double *)C0, p, comm,
+                                   (double *)C_out, labels, objective, iteration_count);
+}
+
 const char *kmb_status_string(int status) {
     switch (status) {
         case KMB_OK: return "ok";
@@ -974,6 +1147,7 @@ const char *kmb_status_string(int status) {
         case KMB_ETIMEDOUT: return "timed out";
         case KMB_ETOO_MANY_EMPTY: return "number of clusters is too large (too many empty clusters)";
         case KMB_EUNSUPPORTED: return "unsupported";
+        case KMB_ECOMM: return "communicator failure";
         default: return "unknown status";
     }
 }

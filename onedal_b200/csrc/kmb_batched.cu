@@ -1,6 +1,6 @@
 // Batched form: thousands of independent k-means problems (uneven n, k, d) train
 // together in ONE persistent grouped kernel. A cooperative grid walks, for every
-// Lloyd iteration, five phases over flat work lists of all problems, separated
+// Lloyd iteration, four phases over flat work lists of all problems, separated
 // by grid-wide barriers (bounded waits: a barrier that does not complete within
 // ~2 s sets an error flag, every CTA leaves, and the call returns KMB_ETIMEDOUT).
 // The launch can be captured into a CUDA graph and replayed.
@@ -8,14 +8,15 @@
 // Per iteration (the semantics of one pass of cpp/daal/src/algorithms/kmeans/
 // kmeans_lloyd_batch_impl.i:117-212, for every problem not yet converged):
 //   prep        (problem, cluster)   C -> transposed Ct, h = 0.5||c||^2
-//   assign      (problem, row tile)  FP32 FMA scores h_j - x.c_j over all of the
-//                                    problem's clusters (k <= 256), lowest index on
-//                                    ties; labels and squared distances
-//   accumulate  (problem, row block) exact fixed-point cluster sums: every value
-//                                    as three 32-bit limbs (the Lloyd loop's exact
-//                                    update, kmb_internal.cuh), summed in shared
-//                                    memory per block of columns, then added to the
-//                                    problem's int64 limb sums
+//   work        (problem, block of 4096 rows)
+//                 assign:     FP32 FMA scores h_j - x.c_j over all of the problem's
+//                             clusters (k <= 256), lowest index on ties; labels and
+//                             squared distances, tile by tile
+//                 accumulate: exact fixed-point cluster sums of the same block (the
+//                             rows are still in L2): every value as three 32-bit
+//                             limbs (the Lloyd loop's exact update,
+//                             kmb_internal.cuh), summed per label-sorted row list,
+//                             then added to the problem's int64 limb sums
 //   finalize    (problem, cluster)   c = F(S / count) from the 128-bit sum, shift
 //                                    part, sums cleared for the next iteration
 //   decide      (problem)            empty clusters reseeded with the farthest rows
@@ -26,11 +27,12 @@
 // exact sums, centroids -- so a problem trained here equals the same problem
 // trained alone bit for bit.
 //
-// Work items of a phase are assigned to CTAs round-robin; the assignment list is
-// sorted by cost (rows x padded clusters x padded features) so the largest tiles
-// start first. The assignment tile (rows per thread) of each (d, k) class comes
-// from a built-in autotuner that times the candidates on synthetic rows of that
-// shape the first time the class is seen on a device (cached under a lock).
+// Work items of a phase are found on the device from per-problem prefix counts
+// and taken round-robin; the work list is ordered by cost (rows x padded clusters
+// x padded features) so the largest blocks start first. The assignment tile of
+// each (d, k) class comes from a built-in autotuner that times the candidates on
+// synthetic rows of that shape the first time the class is seen on a device
+// (cached under a lock).
 #include "kmb_internal.cuh"
 
 #include <algorithm>
@@ -77,9 +79,9 @@ struct Phase {
 };
 
 struct Lists {
-    Phase blocks;  // (problem, row block of kAccRows): setup and accumulate
+    Phase blocks;  // (problem, row block of kAccRows): setup
     Phase prep;    // (problem, padded cluster)
-    Phase assign;  // (problem, row tile), problems with the costliest tiles first
+    Phase work;    // (problem, row block of kAccRows): assignment + accumulation, costliest problems first
     Phase fin;     // (problem, cluster)
     int n_problems;
     int iterations;
@@ -621,12 +623,19 @@ __device__ void decide_item(Problem &p, double *sred, float *sv, long long *sr, 
 
 // Dynamic shared memory: the largest phase's needs (assignment tiles, the
 // accumulate limb planes of the largest k, decide's scratch).
+// Shared memory of the fused assign + accumulate phase: the assignment tiles' region
+// (kept across a problem's blocks by the row-per-thread tile), then the accumulation's.
+constexpr size_t kAssignSmem = sizeof(float) * (128 * 64 + kMaxK) > sizeof(float) * BK * (16 * 8 + 4 + 256 + 4)
+                                   ? sizeof(float) * (128 * 64 + kMaxK)
+                                   : sizeof(float) * BK * (16 * 8 + 4 + 256 + 4);
+constexpr size_t kAccSmem = sizeof(int) * (3 * kMaxK + kAccRows);
+
 size_t smem_bytes(int kmax, int dmax) {
-    const size_t assign = std::max(sizeof(float) * BK * (16 * 8 + 4 + 256 + 4), sizeof(float) * (128 * 64 + kMaxK));
-    const size_t acc = sizeof(int) * (3 * kMaxK + kAccRows);
+    (void)kmax;
+    const size_t work = kAssignSmem + kAccSmem;
     const size_t setup = sizeof(float) * (size_t)dmax;
     const size_t decide = (sizeof(double) + sizeof(float) + sizeof(long long)) * NT;
-    return std::max(std::max(assign, acc), std::max(setup, decide));
+    return std::max(std::max(work, setup), decide);
 }
 
 __global__ void __launch_bounds__(NT, 3) persistent_kernel(Problem *P, Lists L, GridBarrier *gb) {
@@ -652,21 +661,23 @@ __global__ void __launch_bounds__(NT, 3) persistent_kernel(Problem *P, Lists L, 
         }
         if (!grid_sync(gb)) return;
         {
-            // round-robin over the tiles, costliest problems first; a problem with more
-            // tiles than the grid has CTAs gives a CTA consecutive tiles of itself, whose
-            // centroids then stay in shared memory
+            // (problem, block of kAccRows rows), round-robin, costliest problems first:
+            // the block's assignment tiles, then its accumulation, which finds the rows
+            // this CTA has just read in L2. A problem with more blocks than the grid has
+            // CTAs gives a CTA consecutive blocks of itself, whose centroids then stay in
+            // shared memory.
             int cached = -1;
-            for (long long i = blockIdx.x; i < L.assign.items; i += gridDim.x) {
-                const int2 w = item_of(L.assign, L.n_problems, i);
-                if (!P[w.x].done) assign_dispatch(P[w.x], w.x, w.y, fsm, cached);
-            }
-        }
-        if (!grid_sync(gb)) return;
-        for (long long i = blockIdx.x; i < L.blocks.items; i += gridDim.x) {
-            const int2 w = item_of(L.blocks, L.n_problems, i);
-            Problem &p = P[w.x];
-            if (!p.done) {
-                accumulate_item(p, w.y, reinterpret_cast<int *>(smem_raw), gb);
+            int *acc_smem = reinterpret_cast<int *>(smem_raw + kAssignSmem);
+            for (long long i = blockIdx.x; i < L.work.items; i += gridDim.x) {
+                const int2 w = item_of(L.work, L.n_problems, i);
+                Problem &p = P[w.x];
+                if (p.done) continue;
+                const int bm = rows_per_item(p.tm);
+                const long long t0 = (long long)w.y * (kAccRows / bm);
+                const long long t1 = min((p.n + bm - 1) / bm, t0 + kAccRows / bm);
+                for (long long t = t0; t < t1; ++t) assign_dispatch(p, w.x, (int)t, fsm, cached);
+                __syncthreads();  // the block's labels, written by every thread, before they are read
+                accumulate_item(p, w.y, acc_smem, gb);
             }
         }
         if (!grid_sync(gb)) return;
@@ -848,8 +859,8 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
     const size_t P1 = (size_t)count + 1;
     std::vector<long long> pre(4 * P1, 0);
     std::vector<int> order((size_t)count);
-    std::vector<long long> tiles((size_t)count);
-    std::vector<double> tile_cost((size_t)count);
+    std::vector<long long> nblocks((size_t)count);
+    std::vector<double> block_cost((size_t)count);
     for (int64_t i = 0; i < count; ++i) {
         const kmb_batched_problem &q = problems[i];
         Problem &p = H[i];
@@ -875,17 +886,16 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         p.eps = accuracy_threshold;
         p.done = max_iteration_count == 0 ? 1 : 0;
         classes[(long long)p.kpad * 16 + p.tm] = 1;
-        const int bm = rows_per_item(p.tm);
         pre[0 * P1 + i + 1] = pre[0 * P1 + i] + (p.n + kAccRows - 1) / kAccRows;
         pre[1 * P1 + i + 1] = pre[1 * P1 + i] + p.kpad;
         pre[3 * P1 + i + 1] = pre[3 * P1 + i] + p.k;
-        tiles[i] = (p.n + bm - 1) / bm;
-        tile_cost[i] = (double)bm * p.kpad * p.dpad;
+        nblocks[i] = (p.n + kAccRows - 1) / kAccRows;
+        block_cost[i] = (double)std::min<long long>(p.n, kAccRows) * p.kpad * p.dpad;
         order[i] = (int)i;
     }
-    // assignment: problems with the costliest tiles first (round-robin over the grid then balances well)
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return tile_cost[a] > tile_cost[b]; });
-    for (int64_t q = 0; q < count; ++q) pre[2 * P1 + q + 1] = pre[2 * P1 + q] + tiles[order[q]];
+    // work: problems with the costliest blocks first (round-robin over the grid then balances well)
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return block_cost[a] > block_cost[b]; });
+    for (int64_t q = 0; q < count; ++q) pre[2 * P1 + q + 1] = pre[2 * P1 + q] + nblocks[order[q]];
     Problem *dP = nullptr;
     long long *dPre = nullptr;
     int *dOrder = nullptr;
@@ -912,7 +922,7 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
     Lists L;
     L.blocks = Phase{dPre + 0 * P1, nullptr, pre[0 * P1 + count]};
     L.prep = Phase{dPre + 1 * P1, nullptr, pre[1 * P1 + count]};
-    L.assign = Phase{dPre + 2 * P1, dOrder, pre[2 * P1 + count]};
+    L.work = Phase{dPre + 2 * P1, dOrder, pre[2 * P1 + count]};
     L.fin = Phase{dPre + 3 * P1, nullptr, pre[3 * P1 + count]};
     L.n_problems = (int)count;
     L.iterations = (int)max_iteration_count;
@@ -934,6 +944,10 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     bool graphed = false;
+    // device time of the kernel alone (host set-up excluded)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    const bool timed = cudaEventCreate(&ev0) == cudaSuccess && cudaEventCreate(&ev1) == cudaSuccess;
+    if (timed) cudaEventRecord(ev0, s);
     if (rc == KMB_OK && use_graph) {
         // one cooperative kernel node, captured on a private stream (the caller's
         // may be the legacy default stream) and launched on the caller's
@@ -959,6 +973,7 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         if (cudaLaunchKernelEx(&cfg, persistent_kernel, dP, L, gb) != cudaSuccess) rc = KMB_ECUDA;
     }
     if (rc == KMB_OK) KMB_LAUNCHED();
+    if (timed) cudaEventRecord(ev1, s);
     GridBarrier hb;
     std::memset(&hb, 0, sizeof(hb));
     if (rc == KMB_OK && (cudaMemcpyAsync(H.data(), dP, sizeof(Problem) * count, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
@@ -978,8 +993,12 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
             info->variants = (int32_t)classes.size();
             info->total_iterations = total_iters;
             info->graph_launches = graphed ? 1 : 0;
+            float ms = 0.f;
+            info->kernel_ms = (timed && cudaEventElapsedTime(&ms, ev0, ev1) == cudaSuccess) ? (double)ms : -1.0;
         }
     }
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
     cudaFreeAsync(dP, s);
     cudaFreeAsync(dPre, s);
     cudaFreeAsync(dOrder, s);

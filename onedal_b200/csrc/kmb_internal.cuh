@@ -122,6 +122,7 @@ struct Workspace {
     DevBuf Xhi, Xlo, Chi, Clo, tcx, rowb, pp_acc, pp_rand, pp_state, pp_flags;
     DevBuf csr_vals, csr_cols64, csr_rowptr64, csr_cols, csr_rowptr, csr_bad, csr_cnorm;
     DevBuf ex_acc, ex_cnt, ex_prev, ex_colexp, ex_records;  // exact update: limb sums, counts, previous
+    DevBuf sp_sums, sp_counts, sp_sq, sp_rowsq, sp_Ca, sp_Cb, sp_ids, sp_rows, sp_state, sp_gather;  // kmb_train_spmd
                                                              // labels, scales, per-piece limb sums
     // Grows `b` to at least `bytes`; returns false on allocation failure.
     bool ensure(DevBuf &b, size_t bytes);
@@ -327,6 +328,12 @@ void prepare_exact_update(const float *X, int64_t n, int64_t d, Workspace &ws, L
 bool ensure_exact_buffers(Workspace &ws, int64_t n, int64_t k, int64_t d);
 void launch_update_exact(const float *X, const UpdatePlan &p, int32_t *labels, const float *d2, float *C_old,
                          float *C_new, Workspace &ws, LoopState *st, bool commit, cudaStream_t s, float *exact_d2);
+
+// The m rows with the largest d2, in (d2 descending, row ascending) order, into
+// rows_out (device, m int64); m <= n. st is scratch device state (its n_empty is set
+// to m). The sharded training's reseed candidates. False when a buffer cannot grow.
+template <typename F>
+bool launch_top_rows(const F *d2, int64_t n, int m, Workspace &ws, LoopState *st, long long *rows_out, cudaStream_t s);
 
 // Just the sums/counts half of the update (sharded training).
 template <typename F>

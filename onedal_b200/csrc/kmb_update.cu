@@ -602,6 +602,16 @@ __global__ void sel_sort_kernel(Cand *__restrict__ cand, const LoopState *st) {
     }
 }
 
+__global__ void select_state_kernel(LoopState *st, int m) {
+    LoopState z = {};
+    z.n_empty = m;
+    *st = z;
+}
+
+__global__ void cand_rows_kernel(const Cand *__restrict__ cand, int m, long long *__restrict__ rows) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) rows[e] = cand[e].row;
+}
+
 // Empty cluster e (ascending id) takes candidate e; shift part = ||c_old - x||^2.
 template <typename F>
 __global__ void reseed_apply_kernel(const F *__restrict__ X, int d, const Cand *__restrict__ cand,
@@ -1330,6 +1340,38 @@ void prepare_exact_update(const float *X, int64_t n, int64_t d, Workspace &ws, L
     colexp_kernel<<<(unsigned)((d + 255) / 256), 256, 0, s>>>(colexp, (int)d, st);
     KMB_LAUNCHED();
 }
+
+template <typename F>
+bool launch_top_rows(const F *d2, int64_t n, int m, Workspace &ws, LoopState *st, long long *rows_out, cudaStream_t s) {
+    if (m <= 0 || m > n) return m == 0;
+    int64_t pm = 1;
+    while (pm < m) pm <<= 1;
+    if (!ws.ensure(ws.sel_hist, sizeof(unsigned int) * 256) || !ws.ensure(ws.sel_state, sizeof(SelState)) ||
+        !ws.ensure(ws.cand, sizeof(Cand) * pm))
+        return false;
+    SelState *ss = (SelState *)ws.sel_state.ptr;
+    unsigned int *hist = (unsigned int *)ws.sel_hist.ptr;
+    Cand *cand = (Cand *)ws.cand.ptr;
+    select_state_kernel<<<1, 1, 0, s>>>(st, m);
+    KMB_LAUNCHED();
+    sel_init_kernel<<<1, 256, 0, s>>>(ss, hist, st);
+    KMB_LAUNCHED();
+    for (int shift = KeyOf<F>::BITS - 8; shift >= 0; shift -= 8) {
+        sel_hist_kernel<F><<<592, 256, 0, s>>>(d2, n, shift, ss, hist, st);
+        KMB_LAUNCHED();
+        sel_pick_kernel<<<1, 256, 0, s>>>(ss, hist, shift, st);
+        KMB_LAUNCHED();
+    }
+    sel_collect_kernel<F><<<1, 1024, 0, s>>>(d2, n, ss, cand, m, st);
+    KMB_LAUNCHED();
+    sel_sort_kernel<<<1, 1024, 0, s>>>(cand, st);
+    KMB_LAUNCHED();
+    cand_rows_kernel<<<(unsigned)((m + 255) / 256), 256, 0, s>>>(cand, m, rows_out);
+    KMB_LAUNCHED();
+    return true;
+}
+template bool launch_top_rows<float>(const float *, int64_t, int, Workspace &, LoopState *, long long *, cudaStream_t);
+template bool launch_top_rows<double>(const double *, int64_t, int, Workspace &, LoopState *, long long *, cudaStream_t);
 
 void launch_update_exact(const float *X, const UpdatePlan &p, int32_t *labels, const float *d2, float *C_old,
                          float *C_new, Workspace &ws, LoopState *st, bool commit, cudaStream_t s, float *exact_d2) {

@@ -167,3 +167,67 @@ def train_spmd(ops, C0: torch.Tensor, max_iteration_count: int, accuracy_thresho
     obj = torch.as_tensor(st.sq_total, dtype=torch.float64, device=dev).reshape(1).clone()
     dist.all_reduce(obj, group=group)
     return C, st.labels, it, float(obj.item())
+
+
+def train_spmd_native(X: torch.Tensor, C0: torch.Tensor, max_iteration_count: int, accuracy_threshold: float = 0.0,
+                      form: int = _native.KMB_FORM_PLAIN, group=None):
+    """The same sharded Lloyd loop run by the library itself (kmb_train_spmd), with
+    torch.distributed as its communicator: one host allreduce of the packed FP64
+    [sums | counts | squared distances] per iteration and one allgather of the reseed
+    candidates when clusters are empty. X is this rank's block of rows (CUDA), C0 the
+    common initial centroids. Returns (centroids, local labels, iterations, objective);
+    the centroids are identical on every rank. With NCCL the host buffers go through
+    device copies; with gloo they are reduced in place."""
+    assert X.is_cuda and C0.is_cuda and X.dim() == 2
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    nccl = dist.get_backend(group) == "nccl"
+    dev = X.device
+    X = X.contiguous()
+    C0 = C0.contiguous().to(X.dtype)
+
+    def allreduce(_user, buf, count):
+        try:
+            host = torch.from_numpy(np.ctypeslib.as_array(buf, shape=(count,)))  # the library's buffer, in place
+            if nccl:
+                t = host.to(dev)
+                dist.all_reduce(t, group=group)
+                host.copy_(t.cpu())
+            else:
+                dist.all_reduce(host, group=group)
+            return 0
+        except Exception:  # reported to the library as a communicator failure
+            return 1
+
+    def allgather(_user, send, nbytes, recv):
+        try:
+            src = torch.from_numpy(np.ctypeslib.as_array((ctypes.c_uint8 * nbytes).from_address(send))).clone()
+            dst = torch.from_numpy(np.ctypeslib.as_array((ctypes.c_uint8 * (nbytes * world)).from_address(recv)))
+            if nccl:
+                outs = [torch.empty(nbytes, dtype=torch.uint8, device=dev) for _ in range(world)]
+                dist.all_gather(outs, src.to(dev), group=group)
+            else:
+                outs = [torch.empty(nbytes, dtype=torch.uint8) for _ in range(world)]
+                dist.all_gather(outs, src, group=group)
+            dst.copy_(torch.cat(outs).cpu())
+            return 0
+        except Exception:
+            return 1
+
+    ar_cb = _native.ALLREDUCE_F64_FN(allreduce)
+    ag_cb = _native.ALLGATHER_FN(allgather)
+    comm = _native.kmb_communicator(None, rank, world, ar_cb, ag_cb)
+    n, d = X.shape
+    k = C0.shape[0]
+    ctx = _native.context(dev.index or 0)
+    ctx.set_stream(torch.cuda.current_stream(dev).cuda_stream)
+    C = torch.empty_like(C0)
+    labels = torch.empty(n, dtype=torch.int32, device=dev)
+    params = _native.kmb_params(k, int(max_iteration_count), float(accuracy_threshold), int(form), 0)
+    obj = ctypes.c_double()
+    it = ctypes.c_int64()
+    dtype = _native.KMB_F32 if X.dtype == torch.float32 else _native.KMB_F64
+    ctx.check(ctx.lib.kmb_train_spmd(ctx.handle, dtype, X.data_ptr(), n, d, C0.data_ptr(), ctypes.byref(params),
+                                     ctypes.byref(comm), C.data_ptr(), labels.data_ptr(), ctypes.byref(obj),
+                                     ctypes.byref(it)))
+    return C, labels, it.value, obj.value

@@ -105,3 +105,79 @@ def test_train_spmd_one_rank_nccl(far):
     assert (lab.cpu().numpy() == labr).all()
     assert centroid_rel_err(Cr, C.cpu().numpy()) < 1e-12
     assert rel_close(obj, objr, 1e-10)
+
+
+# ---- the library's own sharded loop (kmb_train_spmd) with torch.distributed callbacks ----
+
+@pytest.mark.parametrize("far", [False, True])
+def test_native_spmd_one_rank_equals_python_driver(far):
+    """kmb_train_spmd over a one-rank NCCL group gives the Python driver's result
+    bit for bit (same kernels, same exchange) and the FP64 oracle's training run."""
+    from onedal_b200.spmd import train_spmd_native
+    X, C0 = _blobs(30000, 160, 48, np.float64, seed=78, far_centroid=far)
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60), device_id=torch.device("cuda", 0))
+    try:
+        Xd, Cd = torch.from_numpy(X).cuda(), torch.from_numpy(C0).cuda()
+        Cp, labp, itp, objp = train_spmd(DeviceShardOps(Xd, _native.KMB_FORM_PLAIN), Cd, 25, 0.0)
+        Cn, labn, itn, objn = train_spmd_native(Xd, Cd, 25, 0.0)
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+    assert itn == itp
+    assert np.array_equal(labn.cpu().numpy(), labp.cpu().numpy())
+    assert np.array_equal(Cn.cpu().numpy(), Cp.cpu().numpy())
+    assert rel_close(objn, objp, 1e-12)
+    Cr, labr, objr, itr = restated.train(X, C0, 25, 0.0)
+    assert itn == itr
+    assert (labn.cpu().numpy() == labr).all()
+    assert centroid_rel_err(Cr, Cn.cpu().numpy()) < 1e-12
+
+
+def _native_rank(rank, world, port, X, C0, dt, q):
+    import os
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import torch
+    import torch.distributed as dist
+    from onedal_b200.spmd import train_spmd_native
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        cut = np.linspace(0, X.shape[0], world + 1).astype(int)
+        C, lab, it, obj = train_spmd_native(torch.from_numpy(X[cut[rank]:cut[rank + 1]]).cuda(),
+                                            torch.from_numpy(C0).cuda(), 30, 0.0)
+        torch.cuda.synchronize()
+        q.put((rank, C.cpu().numpy(), lab.cpu().numpy(), it, obj))
+    except Exception as e:  # reported to the parent
+        q.put((rank, repr(e), None, None, None))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("dt,far", [(np.float64, True), (np.float32, False)])
+def test_native_spmd_two_ranks_gloo(dt, far):
+    """Two ranks (two processes sharing the one GPU, gloo on the host as the
+    communicator): identical centroids on both ranks, equal to the FP64 oracle's
+    single-process run (responses, iterations, centroids), an emptied cluster
+    reseeded across the ranks included."""
+    import torch.multiprocessing as mp
+    X, C0 = _blobs(24000, 40, 12, dt, seed=79, far_centroid=far)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_native_rank, args=(r, 2, port, X, C0, dt, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted([q.get(timeout=300) for _ in range(2)], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+    for r in res:
+        assert r[2] is not None, r[1]
+    (_, C0r, lab0, it0, obj0), (_, C1r, lab1, it1, obj1) = res
+    assert it0 == it1 and np.array_equal(C0r, C1r) and obj0 == obj1
+    Cr, labr, objr, itr = restated.train(X.astype(np.float64), C0.astype(np.float64), 30, 0.0)
+    assert it0 == itr
+    assert (np.concatenate([lab0, lab1]) == labr).all()
+    assert centroid_rel_err(Cr, C0r) < CENTROID_TOL[dt]
+    assert rel_close(obj0, objr, 1e-10 if dt == np.float64 else 1e-5)
