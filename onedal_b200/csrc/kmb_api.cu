@@ -656,7 +656,7 @@ int partial_impl(kmb_context *ctx, const F *X, int64_t n, int64_t d, const F *C,
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
     prepare_rows<F>(ctx, X, n, d, tc);
     if ((rc = assign_pass<F>(ctx, X, n, d, C, k, tc, labels, (F *)ws.d2.ptr, st, tc))) return rc;
-    kmb::launch_partial_sums<F>(X, plan, labels, sums, counts, ws, s);
+    if (sums) kmb::launch_partial_sums<F>(X, plan, labels, sums, counts, ws, s);  // (null: labels and distances only)
     if (sq_distances)
         kmb::launch_sum_values<F>((const F *)ws.d2.ptr, n, (double *)ws.obj_part.ptr, sq_distances, s);
     if (row_sq) KMB_CUDA(cudaMemcpyAsync(row_sq, ws.d2.ptr, sizeof(F) * n, cudaMemcpyDeviceToDevice, s));
@@ -890,11 +890,16 @@ int train_spmd_impl(kmb_context *ctx, int dtype, const F *X, int64_t n, int64_t 
         total += ns[r];
     }
     if (k > total) return fail(ctx, KMB_EINVAL, "cluster count exceeds data row count");
+    // float rows: the exact fixed-point sums of the single-GPU update, exchanged as
+    // exact 32-bit halves, so every rank's centroids are those of a one-GPU train
+    const bool exact = sizeof(F) == 4 && total <= INT32_MAX;
     if (!ws.ensure(ws.sp_sums, sizeof(double) * kd) || !ws.ensure(ws.sp_counts, sizeof(int64_t) * k) ||
-        !ws.ensure(ws.sp_sq, sizeof(double)) || !ws.ensure(ws.sp_rowsq, sizeof(F) * n) ||
+        !ws.ensure(ws.sp_sq, sizeof(double) * 2) || !ws.ensure(ws.sp_rowsq, sizeof(F) * n) ||
         !ws.ensure(ws.sp_Ca, sizeof(F) * kd) || !ws.ensure(ws.sp_Cb, sizeof(F) * kd) ||
         !ws.ensure(ws.sp_ids, sizeof(int32_t) * k) || !ws.ensure(ws.sp_rows, sizeof(long long) * k) ||
-        !ws.ensure(ws.sp_state, sizeof(LoopState)) || !ws.ensure(ws.sp_gather, (sizeof(double) + sizeof(F) * d) * k))
+        !ws.ensure(ws.sp_state, sizeof(LoopState)) || !ws.ensure(ws.sp_gather, (sizeof(double) + sizeof(F) * d) * k) ||
+        (exact && (!ws.ensure(ws.sp_acc, sizeof(long long) * 3 * kd) || !ws.ensure(ws.sp_colexp, sizeof(int) * d) ||
+                   !ws.ensure(ws.sp_shift, sizeof(double) * k))))
         return fail(ctx, KMB_ENOMEM, "sharded training buffers");
     double *sums = (double *)ws.sp_sums.ptr, *sq = (double *)ws.sp_sq.ptr;
     int64_t *counts = (int64_t *)ws.sp_counts.ptr;
@@ -904,31 +909,105 @@ int train_spmd_impl(kmb_context *ctx, int dtype, const F *X, int64_t n, int64_t 
     long long *rows = (long long *)ws.sp_rows.ptr;
     double *gvals = (double *)ws.sp_gather.ptr;
     F *gvecs = (F *)(gvals + k);
-    std::vector<double> packed((size_t)(kd + k + 1));
+    long long *acc = (long long *)ws.sp_acc.ptr;
+    int *colexp = (int *)ws.sp_colexp.ptr;
+    int *cnt32 = (int *)ws.sp_counts.ptr;  // the exact path's counts (int32) share the buffer
+    int *bad = (int *)(sq + 1);
+    double *shift_part = (double *)ws.sp_shift.ptr;
+    std::vector<double> packed((size_t)(exact ? 6 * kd + k + 1 : kd + k + 1));
     std::vector<int64_t> hcounts((size_t)k);
+    std::vector<long long> hacc(exact ? (size_t)(3 * kd) : 0);
+    std::vector<int> hcnt(exact ? (size_t)k : 0);
+    std::vector<double> hshift(exact ? (size_t)k : 0);
     KMB_CUDA(cudaMemcpyAsync(Ccur, C0, sizeof(F) * kd, cudaMemcpyDeviceToDevice, s));
+    if (exact) {
+        // column exponents from the column maxima over all ranks (the single-GPU rule:
+        // the column's largest |x| maps below 2^94)
+        std::vector<unsigned> bits((size_t)d), all((size_t)d * comm->size);
+        kmb::launch_column_max_bits((const float *)X, n, d, (unsigned *)colexp, s);
+        KMB_CUDA(cudaMemcpyAsync(bits.data(), colexp, sizeof(unsigned) * d, cudaMemcpyDeviceToHost, s));
+        KMB_CUDA(cudaStreamSynchronize(s));
+        if (comm->allgather(comm->user, bits.data(), (int64_t)(sizeof(unsigned) * d), all.data()))
+            return fail(ctx, KMB_ECOMM, "allgather of the column maxima failed");
+        std::vector<int> hexp((size_t)d);
+        for (int64_t t = 0; t < d; ++t) {
+            unsigned b = 0;
+            for (int r = 0; r < comm->size; ++r) b = std::max(b, all[(size_t)r * d + t]);
+            float m;
+            std::memcpy(&m, &b, sizeof(m));
+            int e = 0;
+            if (b != 0u && std::isfinite(m)) {
+                int ex;
+                std::frexp(m, &ex);
+                e = kmb::kExactMaxBits - ex;
+            }
+            hexp[(size_t)t] = e;
+        }
+        KMB_CUDA(cudaMemcpyAsync(colexp, hexp.data(), sizeof(int) * d, cudaMemcpyHostToDevice, s));
+    }
     int64_t it = 0;
     int rc;
     while (it < p.max_iteration_count) {
-        if ((rc = partial_impl<F>(ctx, X, n, d, Ccur, k, p.form, labels, sums, counts, sq, row_sq))) return rc;
-        // one exchange: [sums | counts | squared distances] summed over the ranks
-        KMB_CUDA(cudaMemcpyAsync(packed.data(), sums, sizeof(double) * kd, cudaMemcpyDeviceToHost, s));
-        KMB_CUDA(cudaMemcpyAsync(hcounts.data(), counts, sizeof(int64_t) * k, cudaMemcpyDeviceToHost, s));
-        KMB_CUDA(cudaMemcpyAsync(&packed[kd + k], sq, sizeof(double), cudaMemcpyDeviceToHost, s));
-        KMB_CUDA(cudaStreamSynchronize(s));
-        for (int64_t j = 0; j < k; ++j) packed[kd + j] = (double)hcounts[j];  // exact below 2^53
-        if (comm->allreduce_sum_f64(comm->user, packed.data(), kd + k + 1))
-            return fail(ctx, KMB_ECOMM, "allreduce of the cluster sums failed");
-        for (int64_t j = 0; j < k; ++j) hcounts[j] = (int64_t)std::llround(packed[kd + j]);
-        KMB_CUDA(cudaMemcpyAsync(sums, packed.data(), sizeof(double) * kd, cudaMemcpyHostToDevice, s));
-        KMB_CUDA(cudaMemcpyAsync(counts, hcounts.data(), sizeof(int64_t) * k, cudaMemcpyHostToDevice, s));
         double shift = 0.0;
-        int64_t ne = 0;
-        if ((rc = kmb_finalize_centroids(ctx, dtype, sums, counts, Ccur, k, d, Cnew, &shift, ids, &ne))) return rc;
-        if (ne > 0) {
+        std::vector<int32_t> hids;
+        if (exact) {
+            if ((rc = partial_impl<F>(ctx, X, n, d, Ccur, k, p.form, labels, nullptr, nullptr, sq, row_sq))) return rc;
+            KMB_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), s));
+            kmb::launch_shard_exact_sums((const float *)X, n, (int)d, (int)k, labels, colexp, acc, cnt32, bad, s);
+            int hbad = 0;
+            KMB_CUDA(cudaMemcpyAsync(hacc.data(), acc, sizeof(long long) * 3 * kd, cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaMemcpyAsync(hcnt.data(), cnt32, sizeof(int) * k, cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaMemcpyAsync(&packed[6 * kd + k], sq, sizeof(double), cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaStreamSynchronize(s));
+            if (hbad) return fail(ctx, KMB_ECUDA, "label out of range in the exact sums");
+            // each int64 limb sum as two exact doubles: its low 32 bits and the rest
+            for (int64_t i = 0; i < 3 * kd; ++i) {
+                packed[(size_t)i] = (double)(hacc[(size_t)i] & 0xffffffffll);
+                packed[(size_t)(3 * kd + i)] = (double)(hacc[(size_t)i] >> 32);
+            }
+            for (int64_t j = 0; j < k; ++j) packed[(size_t)(6 * kd + j)] = (double)hcnt[(size_t)j];
+            if (comm->allreduce_sum_f64(comm->user, packed.data(), 6 * kd + k + 1))
+                return fail(ctx, KMB_ECOMM, "allreduce of the cluster sums failed");
+            for (int64_t i = 0; i < 3 * kd; ++i)
+                hacc[(size_t)i] = (long long)std::llround(packed[(size_t)(3 * kd + i)]) * 4294967296ll +
+                                  (long long)std::llround(packed[(size_t)i]);
+            for (int64_t j = 0; j < k; ++j) {
+                hcnt[(size_t)j] = (int)std::llround(packed[(size_t)(6 * kd + j)]);
+                if (hcnt[(size_t)j] == 0) hids.push_back((int32_t)j);
+            }
+            KMB_CUDA(cudaMemcpyAsync(acc, hacc.data(), sizeof(long long) * 3 * kd, cudaMemcpyHostToDevice, s));
+            KMB_CUDA(cudaMemcpyAsync(cnt32, hcnt.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
+            KMB_CUDA(cudaMemcpyAsync(Cnew, Ccur, sizeof(F) * kd, cudaMemcpyDeviceToDevice, s));
+            kmb::launch_shard_exact_finalize(acc, cnt32, colexp, (float *)Cnew, (int)k, (int)d, shift_part, s);
+            KMB_CUDA(cudaMemcpyAsync(hshift.data(), shift_part, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaStreamSynchronize(s));
+            for (int64_t j = 0; j < k; ++j) shift += hshift[(size_t)j];
+        } else {
+            if ((rc = partial_impl<F>(ctx, X, n, d, Ccur, k, p.form, labels, sums, counts, sq, row_sq))) return rc;
+            // one exchange: [sums | counts | squared distances] summed over the ranks
+            KMB_CUDA(cudaMemcpyAsync(packed.data(), sums, sizeof(double) * kd, cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaMemcpyAsync(hcounts.data(), counts, sizeof(int64_t) * k, cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaMemcpyAsync(&packed[kd + k], sq, sizeof(double), cudaMemcpyDeviceToHost, s));
+            KMB_CUDA(cudaStreamSynchronize(s));
+            for (int64_t j = 0; j < k; ++j) packed[kd + j] = (double)hcounts[j];  // exact below 2^53
+            if (comm->allreduce_sum_f64(comm->user, packed.data(), kd + k + 1))
+                return fail(ctx, KMB_ECOMM, "allreduce of the cluster sums failed");
+            for (int64_t j = 0; j < k; ++j) hcounts[j] = (int64_t)std::llround(packed[kd + j]);
+            KMB_CUDA(cudaMemcpyAsync(sums, packed.data(), sizeof(double) * kd, cudaMemcpyHostToDevice, s));
+            KMB_CUDA(cudaMemcpyAsync(counts, hcounts.data(), sizeof(int64_t) * k, cudaMemcpyHostToDevice, s));
+            int64_t ne = 0;
+            if ((rc = kmb_finalize_centroids(ctx, dtype, sums, counts, Ccur, k, d, Cnew, &shift, ids, &ne))) return rc;
+            hids.resize((size_t)ne);
+            if (ne > 0) {
+                KMB_CUDA(cudaMemcpyAsync(hids.data(), ids, sizeof(int32_t) * ne, cudaMemcpyDeviceToHost, s));
+                KMB_CUDA(cudaStreamSynchronize(s));
+            }
+        }
+        if (!hids.empty()) {
             // every rank offers its m farthest rows; the global m farthest by (distance
             // descending, global row ascending) reseed the empty clusters, ascending
-            const int m = (int)ne, take = (int)std::min<int64_t>(m, n);
+            const int m = (int)hids.size(), take = (int)std::min<int64_t>(m, n);
             if (!kmb::launch_top_rows<F>(row_sq, n, take, ws, (LoopState *)ws.sp_state.ptr, rows, s))
                 return fail(ctx, KMB_ENOMEM, "candidate selection buffers");
             if (take > 0) {
@@ -941,14 +1020,12 @@ int train_spmd_impl(kmb_context *ctx, int dtype, const F *X, int64_t n, int64_t 
             std::vector<long long> hrows((size_t)std::max(take, 1));
             std::vector<double> hvals((size_t)std::max(take, 1));
             std::vector<F> hvecs((size_t)std::max(take, 1) * (size_t)d);
-            std::vector<int32_t> hids((size_t)m);
             std::vector<F> hC((size_t)kd);
             if (take > 0) {
                 KMB_CUDA(cudaMemcpyAsync(hrows.data(), rows, sizeof(long long) * take, cudaMemcpyDeviceToHost, s));
                 KMB_CUDA(cudaMemcpyAsync(hvals.data(), gvals, sizeof(double) * take, cudaMemcpyDeviceToHost, s));
                 KMB_CUDA(cudaMemcpyAsync(hvecs.data(), gvecs, sizeof(F) * take * d, cudaMemcpyDeviceToHost, s));
             }
-            KMB_CUDA(cudaMemcpyAsync(hids.data(), ids, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, s));
             KMB_CUDA(cudaMemcpyAsync(hC.data(), Ccur, sizeof(F) * kd, cudaMemcpyDeviceToHost, s));
             KMB_CUDA(cudaStreamSynchronize(s));
             for (int e = 0; e < m; ++e) {
@@ -994,7 +1071,7 @@ int train_spmd_impl(kmb_context *ctx, int dtype, const F *X, int64_t n, int64_t 
         if (shift <= p.accuracy_threshold) break;
     }
     // responses of this rank's rows and the objective under the final centroids
-    if ((rc = partial_impl<F>(ctx, X, n, d, Ccur, k, p.form, labels, sums, counts, sq, nullptr))) return rc;
+    if ((rc = partial_impl<F>(ctx, X, n, d, Ccur, k, p.form, labels, nullptr, nullptr, sq, nullptr))) return rc;
     double obj = 0.0;
     KMB_CUDA(cudaMemcpyAsync(&obj, sq, sizeof(double), cudaMemcpyDeviceToHost, s));
     KMB_CUDA(cudaMemcpyAsync(C_out, Ccur, sizeof(F) * kd, cudaMemcpyDeviceToDevice, s));

@@ -36,6 +36,7 @@
 #include "kmb_internal.cuh"
 
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -698,6 +699,20 @@ __global__ void __launch_bounds__(NT, 3) persistent_kernel(Problem *P, Lists L, 
     }
 }
 
+// ---- one shard of a sharded float training (kmb_train_spmd) -----------------------
+// The batched accumulation and finalize over one problem: the same exact limb sums
+// and the same centroid formula as the single-problem Lloyd loop.
+__global__ void __launch_bounds__(NT, 3) shard_sums_kernel(Problem p, int nblocks, GridBarrier *gb) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for (int blk = blockIdx.x; blk < nblocks; blk += gridDim.x) accumulate_item(p, blk, reinterpret_cast<int *>(smem_raw), gb);
+}
+
+__global__ void shard_finalize_kernel(Problem p) {
+    const int lane = threadIdx.x & 31;
+    for (int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < p.k; j += (gridDim.x * blockDim.x) >> 5)
+        finalize_item(p, j, lane);
+}
+
 // ---- autotuner ------------------------------------------------------------------
 // Times the assignment tile of one (dpad, kpad) class for each rows-per-thread
 // candidate on 32768 synthetic rows of that shape (uniform values, so the scores
@@ -804,6 +819,47 @@ int tuned_tm(int dev, int dpad, int kpad, cudaStream_t s) {
 }
 
 }  // namespace
+}  // namespace kmb
+
+namespace kmb {
+void launch_shard_exact_sums(const float *X, int64_t n, int d, int k, const int32_t *labels, const int *colexp,
+                             long long *acc, int *counts, int *bad, cudaStream_t s) {
+    using namespace batched;
+    cudaMemsetAsync(acc, 0, sizeof(long long) * 3 * (size_t)k * d, s);
+    cudaMemsetAsync(counts, 0, sizeof(int) * k, s);
+    Problem p;
+    std::memset(&p, 0, sizeof(p));
+    p.X = X;
+    p.labels = const_cast<int32_t *>(labels);
+    p.n = n;
+    p.d = d;
+    p.k = k;
+    p.colexp = const_cast<int *>(colexp);
+    p.acc = acc;
+    p.counts = counts;
+    const int nblocks = (int)((n + kAccRows - 1) / kAccRows);
+    // the accumulation reports an out-of-range label in the error word of a grid barrier
+    GridBarrier *gb = reinterpret_cast<GridBarrier *>(reinterpret_cast<char *>(bad) - offsetof(GridBarrier, error));
+    cudaFuncSetAttribute(shard_sums_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAccSmem);
+    shard_sums_kernel<<<(unsigned)std::max(1, std::min(nblocks, 148 * 3)), NT, kAccSmem, s>>>(p, nblocks, gb);
+    KMB_LAUNCHED();
+}
+
+void launch_shard_exact_finalize(long long *acc, const int *counts, const int *colexp, float *C, int k, int d,
+                                 double *shift_part, cudaStream_t s) {
+    using namespace batched;
+    Problem p;
+    std::memset(&p, 0, sizeof(p));
+    p.C = C;
+    p.k = k;
+    p.d = d;
+    p.acc = acc;
+    p.counts = const_cast<int *>(counts);
+    p.colexp = const_cast<int *>(colexp);
+    p.shift_part = shift_part;
+    shard_finalize_kernel<<<(unsigned)std::max(1, std::min((k + 7) / 8, 148 * 8)), 256, 0, s>>>(p);
+    KMB_LAUNCHED();
+}
 }  // namespace kmb
 
 extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64_t count, int64_t max_iteration_count,

@@ -123,6 +123,7 @@ struct Workspace {
     DevBuf csr_vals, csr_cols64, csr_rowptr64, csr_cols, csr_rowptr, csr_bad, csr_cnorm;
     DevBuf ex_acc, ex_cnt, ex_prev, ex_colexp, ex_records;  // exact update: limb sums, counts, previous
     DevBuf sp_sums, sp_counts, sp_sq, sp_rowsq, sp_Ca, sp_Cb, sp_ids, sp_rows, sp_state, sp_gather;  // kmb_train_spmd
+    DevBuf sp_acc, sp_colexp, sp_shift;                                                                // (exact sums)
                                                              // labels, scales, per-piece limb sums
     // Grows `b` to at least `bytes`; returns false on allocation failure.
     bool ensure(DevBuf &b, size_t bytes);
@@ -334,6 +335,18 @@ void launch_update_exact(const float *X, const UpdatePlan &p, int32_t *labels, c
 // to m). The sharded training's reseed candidates. False when a buffer cannot grow.
 template <typename F>
 bool launch_top_rows(const F *d2, int64_t n, int m, Workspace &ws, LoopState *st, long long *rows_out, cudaStream_t s);
+
+// Sharded float training with exact sums (kmb_train_spmd): the column maxima of a
+// shard as float bits (|x| of non-NaN values; 0 for an all-zero column), the
+// exact limb sums of a shard's rows by label (acc: 3 x k x d int64, counts: k int32,
+// both cleared first; *bad set to 2 on a label out of range), and the centroids
+// from summed limbs (non-empty clusters; C updated in place, shift_part[j] =
+// ||c_old - c_new||^2, acc cleared). The formulas are the Lloyd loop's exact update.
+void launch_column_max_bits(const float *X, int64_t n, int64_t d, unsigned *bits, cudaStream_t s);
+void launch_shard_exact_sums(const float *X, int64_t n, int d, int k, const int32_t *labels, const int *colexp,
+                             long long *acc, int *counts, int *bad, cudaStream_t s);
+void launch_shard_exact_finalize(long long *acc, const int *counts, const int *colexp, float *C, int k, int d,
+                                 double *shift_part, cudaStream_t s);
 
 // Just the sums/counts half of the update (sharded training).
 template <typename F>

@@ -1324,6 +1324,19 @@ bool ensure_exact_buffers(Workspace &ws, int64_t n, int64_t k, int64_t d) {
     return ok;
 }
 
+void launch_column_max_bits(const float *X, int64_t n, int64_t d, unsigned *bits, cudaStream_t s) {
+    cudaMemsetAsync(bits, 0, sizeof(unsigned) * d, s);
+    const int64_t total = n * d;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 8));
+    if (d <= 1024)
+        colmax_rows_kernel<<<148 * 8, 256, 0, s>>>(X, n, (int)d, bits, nullptr);
+    else if (d <= 8192)
+        colmax_kernel<<<blocks, 256, sizeof(unsigned) * d, s>>>(X, n, (int)d, bits, nullptr);
+    else
+        colmax_global_kernel<<<blocks, 256, 0, s>>>(X, n, (int)d, bits, nullptr);
+    KMB_LAUNCHED();
+}
+
 void prepare_exact_update(const float *X, int64_t n, int64_t d, Workspace &ws, LoopState *st, cudaStream_t s) {
     int *colexp = (int *)ws.ex_colexp.ptr;
     cudaMemsetAsync(colexp, 0, sizeof(int) * d, s);

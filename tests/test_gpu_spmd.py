@@ -155,13 +155,15 @@ def _native_rank(rank, world, port, X, C0, dt, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("dt,far", [(np.float64, True), (np.float32, False)])
+@pytest.mark.parametrize("dt,far", [(np.float64, True), (np.float32, False), (np.float32, True)])
 def test_native_spmd_two_ranks_gloo(dt, far):
     """Two ranks (two processes sharing the one GPU, gloo on the host as the
     communicator): identical centroids on both ranks, equal to the FP64 oracle's
     single-process run (responses, iterations, centroids), an emptied cluster
-    reseeded across the ranks included."""
+    reseeded across the ranks included. Float rows exchange the exact fixed-point
+    sums, so their result is bit for bit the one-GPU train's (plain form)."""
     import torch.multiprocessing as mp
+    from onedal_b200 import kmeans
     X, C0 = _blobs(24000, 40, 12, dt, seed=79, far_centroid=far)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -181,3 +183,10 @@ def test_native_spmd_two_ranks_gloo(dt, far):
     assert (np.concatenate([lab0, lab1]) == labr).all()
     assert centroid_rel_err(Cr, C0r) < CENTROID_TOL[dt]
     assert rel_close(obj0, objr, 1e-10 if dt == np.float64 else 1e-5)
+    if dt == np.float32:
+        desc = kmeans.descriptor(np.float32).set_cluster_count(C0.shape[0]).set_max_iteration_count(30) \
+            .set_accuracy_threshold(0.0).set_compute_form(kmeans.compute_form.plain)
+        one = kmeans.train(desc, X, C0)
+        assert one.get_iteration_count() == it0
+        assert np.array_equal(one.get_model().get_centroids(), C0r)
+        assert np.array_equal(one.get_responses().ravel(), np.concatenate([lab0, lab1]))
