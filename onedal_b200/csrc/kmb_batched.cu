@@ -715,8 +715,10 @@ __global__ void shard_finalize_kernel(Problem p) {
 
 // ---- autotuner ------------------------------------------------------------------
 // Times the assignment tile of one (dpad, kpad) class for each rows-per-thread
-// candidate on 32768 synthetic rows of that shape (uniform values, so the scores
-// and their ties are those of real data, not all equal).
+// candidate on synthetic rows of that shape (uniform values, so the scores and
+// their ties are those of real data, not all equal), enough of them to fill the
+// grid with every candidate: timed on 32768 rows the 256-row tile left most CTAs
+// idle and lost to the small tiles it beats by 18 % in the batched runs.
 __global__ void tune_fill_kernel(float *p, long long count, unsigned seed) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x) {
         unsigned x = (unsigned)i * 2654435761u ^ seed;
@@ -755,7 +757,12 @@ int tuned_tm(int dev, int dpad, int kpad, cudaStream_t s) {
     if (found != g_tuned.end()) return found->second;
     std::vector<int> cands = kpad >= 256 ? std::vector<int>{2} : kpad >= 128 ? std::vector<int>{2, 4} : std::vector<int>{2, 4, 8};
     if (dpad <= 64 && kpad <= 128) cands.push_back(0);
-    const long long n = 32768;
+    // enough rows that every candidate fills the grid (the batched kernel runs with
+    // thousands of problems in flight): four 256-row tiles per CTA of three per SM
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid_ctas = 3 * sms;
+    const long long n = (long long)grid_ctas * NT * 4;
     float *X = nullptr, *Ct = nullptr, *h = nullptr, *d2 = nullptr, *xn = nullptr;
     int32_t *lab = nullptr;
     Problem *dp = nullptr;
@@ -796,9 +803,9 @@ int tuned_tm(int dev, int dpad, int kpad, cudaStream_t s) {
             p.tm = tm;
             cudaMemcpyAsync(dp, &p, sizeof(p), cudaMemcpyHostToDevice, s);
             const int tiles = (int)((n + rows_per_item(tm) - 1) / rows_per_item(tm));
-            tune_assign_kernel<<<std::min(tiles, 296), NT, smem, s>>>(dp, tiles);  // warm-up
+            tune_assign_kernel<<<std::min(tiles, grid_ctas), NT, smem, s>>>(dp, tiles);  // warm-up
             cudaEventRecord(a, s);
-            for (int r = 0; r < 3; ++r) tune_assign_kernel<<<std::min(tiles, 296), NT, smem, s>>>(dp, tiles);
+            for (int r = 0; r < 3; ++r) tune_assign_kernel<<<std::min(tiles, grid_ctas), NT, smem, s>>>(dp, tiles);
             cudaEventRecord(b, s);
             launch_count() += 4;
             float ms = 0.f;
