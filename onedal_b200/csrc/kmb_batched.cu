@@ -408,7 +408,7 @@ __device__ __forceinline__ void assign_dispatch(const Problem &p, int pid, int t
 // The block's rows are listed by label in shared memory (warp-aggregated
 // histogram, warp scan, warp-ranked scatter). Then each warp takes (cluster,
 // column chunk, slice) tasks: its lanes cover CW = min(32, 2^ceil(log2 d))
-// consecutive columns of 32 / CW rows at a time (coalesced row reads, four rows
+// consecutive columns of 32 / CW rows at a time (coalesced row reads, eight rows
 // per lane in flight), sum the fixed-point limbs of the slice's rows -- every S-th
 // group of rows of the cluster's list -- in registers, fold the lanes of equal
 // column with shuffles and add the totals to the problem's limb sums with one
@@ -487,15 +487,15 @@ __device__ void accumulate_item(Problem &p, int blk, int *sm, GridBarrier *gb) {
         const int ec = active ? p.colexp[c] : 0;
         long long a0 = 0, a1 = 0, a2 = 0;
         const int step = S * rps;
-        for (int i = sl * rps + rl; i < cnt; i += 4 * step) {
-            float v[4];
+        for (int i = sl * rps + rl; i < cnt; i += 8 * step) {  // eight gathered loads in flight
+            float v[8];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 8; ++u) {
                 const int ii = i + u * step;
                 v[u] = (active && ii < cnt) ? Xb[(long long)s_rows[base + ii] * d + c] : 0.f;
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 8; ++u) {
                 const Limbs L = fixed_of(v[u], ec);
                 a0 += L.l0;
                 a1 += L.l1;
