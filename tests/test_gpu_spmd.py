@@ -190,3 +190,45 @@ def test_native_spmd_two_ranks_gloo(dt, far):
         assert one.get_iteration_count() == it0
         assert np.array_equal(one.get_model().get_centroids(), C0r)
         assert np.array_equal(one.get_responses().ravel(), np.concatenate([lab0, lab1]))
+
+
+def test_native_spmd_communicator_failure_is_reported():
+    """A communicator callback that fails ends kmb_train_spmd with KMB_ECOMM (no
+    hang, no device fault) and the context trains normally afterwards."""
+    import ctypes
+    X, C0 = _blobs(5000, 16, 6, np.float32, seed=80)
+    Xd, Cd = torch.from_numpy(X).cuda(), torch.from_numpy(C0).cuda()
+    ctx = _native.context(0)
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    calls = {"allreduce": 0}
+
+    def allgather(_user, send, nbytes, recv):
+        ctypes.memmove(recv, send, nbytes)  # one rank
+        return 0
+
+    def allreduce_fails(_user, buf, count):
+        calls["allreduce"] += 1
+        return 1
+
+    ar, ag = _native.ALLREDUCE_F64_FN(allreduce_fails), _native.ALLGATHER_FN(allgather)
+    comm = _native.kmb_communicator(None, 0, 1, ar, ag)
+    C = torch.empty_like(Cd)
+    lab = torch.empty(X.shape[0], dtype=torch.int32, device="cuda")
+    p = _native.kmb_params(6, 10, 0.0, _native.KMB_FORM_PLAIN, 0)
+    obj, it = ctypes.c_double(), ctypes.c_int64()
+    rc = ctx.lib.kmb_train_spmd(ctx.handle, _native.KMB_F32, Xd.data_ptr(), X.shape[0], X.shape[1], Cd.data_ptr(),
+                                ctypes.byref(p), ctypes.byref(comm), C.data_ptr(), lab.data_ptr(), ctypes.byref(obj),
+                                ctypes.byref(it))
+    assert rc == _native.KMB_ECOMM and calls["allreduce"] == 1
+    # the same context, a working one-rank communicator: the one-GPU train's result
+    ok = _native.ALLREDUCE_F64_FN(lambda _u, _b, _c: 0)
+    comm = _native.kmb_communicator(None, 0, 1, ok, ag)
+    ctx.check(ctx.lib.kmb_train_spmd(ctx.handle, _native.KMB_F32, Xd.data_ptr(), X.shape[0], X.shape[1],
+                                     Cd.data_ptr(), ctypes.byref(p), ctypes.byref(comm), C.data_ptr(), lab.data_ptr(),
+                                     ctypes.byref(obj), ctypes.byref(it)))
+    from onedal_b200 import kmeans
+    desc = kmeans.descriptor(np.float32).set_cluster_count(6).set_max_iteration_count(10) \
+        .set_compute_form(kmeans.compute_form.plain)
+    one = kmeans.train(desc, X, C0)
+    assert it.value == one.get_iteration_count()
+    assert np.array_equal(C.cpu().numpy(), one.get_model().get_centroids())
