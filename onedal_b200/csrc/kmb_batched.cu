@@ -82,12 +82,78 @@ struct Phase {
 
 struct Lists {
     Phase blocks;  // (problem, row block of kAccRows): setup
-    Phase prep;    // (problem, padded cluster)
-    Phase work;    // (problem, row block of kAccRows): assignment + accumulation, costliest problems first
-    Phase fin;     // (problem, cluster)
+    Phase work;    // its order: every problem, costliest blocks first
     int n_problems;
     int iterations;
+    // The problems not yet converged, rebuilt on the device before every iteration
+    // (in the work order), so converged problems cost no walking: their count and,
+    // per phase, prefix counts over them (prep: padded clusters; work: row blocks;
+    // finalize: clusters) -- count + 1 entries each.
+    int *act_order;
+    long long *act_prep, *act_work, *act_fin;
+    int *act_count;
 };
+
+// Rebuilds the active lists (one CTA): per thread a contiguous run of the work
+// order, its active problems counted, an exclusive scan over the threads, then
+// written in order.
+__device__ void compact_active(const Problem *P, const Lists &L, unsigned char *smem) {
+    long long *s_prep = reinterpret_cast<long long *>(smem), *s_work = s_prep + NT, *s_fin = s_work + NT;
+    int *s_cnt = reinterpret_cast<int *>(s_fin + NT);
+    const int per = (L.n_problems + NT - 1) / NT;
+    const int q0 = min(L.n_problems, (int)threadIdx.x * per), q1 = min(L.n_problems, q0 + per);
+    int c = 0;
+    long long wp = 0, ww = 0, wf = 0;
+    for (int q = q0; q < q1; ++q) {
+        const Problem &p = P[L.work.order[q]];
+        if (p.done) continue;
+        ++c;
+        wp += p.kpad;
+        ww += (p.n + kAccRows - 1) / kAccRows;
+        wf += p.k;
+    }
+    s_cnt[threadIdx.x] = c;
+    s_prep[threadIdx.x] = wp;
+    s_work[threadIdx.x] = ww;
+    s_fin[threadIdx.x] = wf;
+    __syncthreads();
+    if (threadIdx.x == 0) {  // exclusive scan over the threads (NT entries)
+        int ac = 0;
+        long long ap = 0, aw = 0, af = 0;
+        for (int t = 0; t < NT; ++t) {
+            const int c2 = s_cnt[t];
+            const long long p2 = s_prep[t], w2 = s_work[t], f2 = s_fin[t];
+            s_cnt[t] = ac;
+            s_prep[t] = ap;
+            s_work[t] = aw;
+            s_fin[t] = af;
+            ac += c2;
+            ap += p2;
+            aw += w2;
+            af += f2;
+        }
+        *L.act_count = ac;
+        L.act_prep[ac] = ap;
+        L.act_work[ac] = aw;
+        L.act_fin[ac] = af;
+    }
+    __syncthreads();
+    int o = s_cnt[threadIdx.x];
+    long long ap = s_prep[threadIdx.x], aw = s_work[threadIdx.x], af = s_fin[threadIdx.x];
+    for (int q = q0; q < q1; ++q) {
+        const int pid = L.work.order[q];
+        const Problem &p = P[pid];
+        if (p.done) continue;
+        L.act_order[o] = pid;
+        L.act_prep[o] = ap;
+        L.act_work[o] = aw;
+        L.act_fin[o] = af;
+        ++o;
+        ap += p.kpad;
+        aw += (p.n + kAccRows - 1) / kAccRows;
+        af += p.k;
+    }
+}
 
 struct GridBarrier {
     unsigned count;
@@ -657,9 +723,15 @@ __global__ void __launch_bounds__(NT, 3) persistent_kernel(Problem *P, Lists L, 
     for (int i = blockIdx.x; i < L.n_problems; i += gridDim.x) scales_item(P[i]);
     if (!grid_sync(gb)) return;
     for (int it = 0; it < L.iterations; ++it) {
-        for (long long i = blockIdx.x * (NT / 32) + warp; i < L.prep.items; i += warps) {
-            const int2 w = item_of(L.prep, L.n_problems, i);
-            if (!P[w.x].done) prep_item(P[w.x], w.y, lane);
+        if (blockIdx.x == 0) compact_active(P, L, smem_raw);
+        if (!grid_sync(gb)) return;
+        const int na = *(volatile int *)L.act_count;  // the same for every CTA until the next compaction
+        const Phase prep{L.act_prep, L.act_order, *(volatile long long *)&L.act_prep[na]};
+        const Phase work{L.act_work, L.act_order, *(volatile long long *)&L.act_work[na]};
+        const Phase fin{L.act_fin, L.act_order, *(volatile long long *)&L.act_fin[na]};
+        for (long long i = blockIdx.x * (NT / 32) + warp; i < prep.items; i += warps) {
+            const int2 w = item_of(prep, na, i);
+            prep_item(P[w.x], w.y, lane);
         }
         if (!grid_sync(gb)) return;
         {
@@ -670,10 +742,9 @@ __global__ void __launch_bounds__(NT, 3) persistent_kernel(Problem *P, Lists L, 
             // shared memory.
             int cached = -1;
             int *acc_smem = reinterpret_cast<int *>(smem_raw + kAssignSmem);
-            for (long long i = blockIdx.x; i < L.work.items; i += gridDim.x) {
-                const int2 w = item_of(L.work, L.n_problems, i);
+            for (long long i = blockIdx.x; i < work.items; i += gridDim.x) {
+                const int2 w = item_of(work, na, i);
                 Problem &p = P[w.x];
-                if (p.done) continue;
                 const int bm = rows_per_item(p.tm);
                 const long long t0 = (long long)w.y * (kAccRows / bm);
                 const long long t1 = min((p.n + bm - 1) / bm, t0 + kAccRows / bm);
@@ -683,13 +754,13 @@ __global__ void __launch_bounds__(NT, 3) persistent_kernel(Problem *P, Lists L, 
             }
         }
         if (!grid_sync(gb)) return;
-        for (long long i = blockIdx.x * (NT / 32) + warp; i < L.fin.items; i += warps) {
-            const int2 w = item_of(L.fin, L.n_problems, i);
-            if (!P[w.x].done) finalize_item(P[w.x], w.y, lane);
+        for (long long i = blockIdx.x * (NT / 32) + warp; i < fin.items; i += warps) {
+            const int2 w = item_of(fin, na, i);
+            finalize_item(P[w.x], w.y, lane);
         }
         if (!grid_sync(gb)) return;
-        for (int i = blockIdx.x; i < L.n_problems; i += gridDim.x) {
-            if (P[i].done) continue;
+        for (int q = blockIdx.x; q < na; q += gridDim.x) {
+            const int i = L.act_order[q];
             double *sred = reinterpret_cast<double *>(smem_raw);
             long long *sr = reinterpret_cast<long long *>(sred + NT);
             float *sv = reinterpret_cast<float *>(sr + NT);
@@ -999,8 +1070,8 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
     long long *dPre = nullptr;
     int *dOrder = nullptr;
     if (pool_alloc((void **)&dP, sizeof(Problem) * count, dev, s) != cudaSuccess ||
-        pool_alloc((void **)&dPre, sizeof(long long) * pre.size(), dev, s) != cudaSuccess ||
-        pool_alloc((void **)&dOrder, sizeof(int) * order.size(), dev, s) != cudaSuccess) {
+        pool_alloc((void **)&dPre, sizeof(long long) * (8 * P1), dev, s) != cudaSuccess ||
+        pool_alloc((void **)&dOrder, sizeof(int) * 2 * order.size(), dev, s) != cudaSuccess) {
         cudaGetLastError();
         if (dP) cudaFreeAsync(dP, s);
         if (dPre) cudaFreeAsync(dPre, s);
@@ -1020,9 +1091,12 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
 
     Lists L;
     L.blocks = Phase{dPre + 0 * P1, nullptr, pre[0 * P1 + count]};
-    L.prep = Phase{dPre + 1 * P1, nullptr, pre[1 * P1 + count]};
     L.work = Phase{dPre + 2 * P1, dOrder, pre[2 * P1 + count]};
-    L.fin = Phase{dPre + 3 * P1, nullptr, pre[3 * P1 + count]};
+    L.act_order = dOrder + count;
+    L.act_prep = dPre + 4 * P1;
+    L.act_work = dPre + 5 * P1;
+    L.act_fin = dPre + 6 * P1;
+    L.act_count = (int *)(dPre + 7 * P1);
     L.n_problems = (int)count;
     L.iterations = (int)max_iteration_count;
     const size_t smem = smem_bytes(kmax, dmax);
