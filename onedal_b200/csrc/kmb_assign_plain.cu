@@ -383,11 +383,12 @@ assign_small_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restri
 }
 
 // ---- FP32, centroids resident in shared memory ------------------------------
-// When all (padded) centroids fit in shared memory next to two row tiles, one
+// When all (padded) centroids fit in shared memory next to the row stages, one
 // persistent CTA per SM keeps C^T and the half norms resident for the whole
-// launch and streams 128-row tiles of X through a two-stage TMA ring, so no
-// centroid byte is re-read per row tile and the FMA loop has no block barrier.
-// 16 warps; warp w owns rows 8w..8w+7 of the tile, lane l the clusters
+// launch and streams 64-row tiles of X through TMA, so no centroid byte is
+// re-read per row tile. 16 warps in two groups of 8; each group owns every other
+// 64-row tile (group g of CTA b takes tiles 2(b + i·grid) + g) and two TMA stages.
+// In a group, warp w owns rows 8w..8w+7 of the tile, lane l the clusters
 // 4l..4l+3 and 128+4l..128+4l+3 of each 256-cluster pass: the row values are
 // shared-memory broadcasts and the centroid reads are conflict-free 16-byte
 // loads. Per (row, cluster) the contraction accumulates x_t * c_t in ascending
@@ -397,15 +398,26 @@ assign_small_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restri
 // rounds halve the rows a lane keeps while merging in the partner's (value,
 // index) triples, leaving each row's top-3 in four lanes; with more than one
 // pass the row's owner lane merges it into the running top-3 in shared memory.
+//
+// Ping-pong: the two groups take turns at the FMA pipe. A group runs a pass's
+// contraction only in its turn and hands the turn over (named barriers 1 and 2)
+// before its top-3 epilogue, so one group's epilogue (compares, selects,
+// shuffles) issues beside the other group's FMAs instead of every warp of the SM
+// reaching its epilogue at once and leaving the FMA pipe idle. Both groups take
+// the same number of turns (a group without a tile left takes empty turns), so
+// every barrier completes; the turn barriers also order a stage's last reads
+// before the TMA load that refills it.
 constexpr int kResThreads = 512;
-constexpr int kResRows = 128;
+constexpr int kResGroupThreads = 256;
+constexpr int kResRows = 64;    // rows per tile (one group's)
+constexpr int kResCtaRows = 128;  // rows per CTA step (both groups)
 constexpr int kResPass = 256;
 constexpr long long kResTimeout = 4000000000ll;  // ~2 s of SM clocks per wait
 
 struct ResBarriers {
-    uint64_t full[2];
+    uint64_t full[4];  // [group][stage]
     int abort;
-    int issued[2];  // loads issued into each stage (thread 0)
+    int issued[4];  // loads issued into each stage (the group's thread 0)
 };
 
 __device__ __forceinline__ uint32_t res_su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -447,6 +459,15 @@ __device__ __forceinline__ void res_load_tile(float *dst, const CUtensorMap *tm,
         : "memory");
 }
 
+// Named barriers of the turn protocol: the waiting group's 256 threads sync, the
+// other group's 256 arrive.
+__device__ __forceinline__ void res_turn_wait(int id) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kResThreads) : "memory");
+}
+__device__ __forceinline__ void res_turn_give(int id) {
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(kResThreads) : "memory");
+}
+
 // Keeps the rows of one half of `t` (hi: the upper half) and merges in the
 // partner lane's triples of the same rows.
 template <int R>
@@ -475,27 +496,37 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
     extern __shared__ uint8_t res_smem_raw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)res_smem_raw + 127) & ~(uintptr_t)127);
     const int tile_floats = kResRows * dpad;
-    float *Xs = (float *)sm;                   // [2][128][dpad]
-    float *Cs = Xs + 2 * tile_floats;          // [kres / 256][dpad][256]: pass-major blocks
+    float *Xs = (float *)sm;                   // [group][stage][64][dpad]
+    float *Cs = Xs + 4 * tile_floats;          // [kres / 256][dpad][256]: pass-major blocks
     float *hs = Cs + (size_t)dpad * kres;      // [kres]
-    RowTop<float> *run = (RowTop<float> *)(hs + kres);  // [128] running top-3 across passes
-    ResBarriers *bar = (ResBarriers *)(run + kResRows);
+    RowTop<float> *run = (RowTop<float> *)(hs + kres);  // [group][64] running top-3 across passes
+    ResBarriers *bar = (ResBarriers *)(run + kResCtaRows);
     volatile int *abort = &bar->abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int n_tiles = (int)((n + kResRows - 1) / kResRows);
-    const int my_tiles = (n_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int g = warp >> 3, gw = warp & 7, gtid = tid & (kResGroupThreads - 1);
+    // tiles of group g: 2 (b + i·grid) + g for i = 0 .. my_tiles - 1
+    const int64_t n_tiles = (n + kResRows - 1) / kResRows;
+    const int64_t par_tiles = (n_tiles - g + 1) / 2;     // tiles of parity g
+    const int64_t par_tiles0 = (n_tiles + 1) / 2;        // of parity 0 (the most)
+    const int grid = (int)gridDim.x, b = (int)blockIdx.x;
+    const int my_tiles = par_tiles > b ? (int)((par_tiles - b + grid - 1) / grid) : 0;
+    const int steps = par_tiles0 > b ? (int)((par_tiles0 - b + grid - 1) / grid) : 0;  // group 0's count
     const uint32_t tile_bytes = (uint32_t)tile_floats * 4u;
+    float *Xg = Xs + 2 * g * tile_floats;  // this group's two stages
+    uint64_t *full = &bar->full[2 * g];
+    int *issued = &bar->issued[2 * g];
     if (tid == 0) {
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < 4; ++i) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(res_su32(&bar->full[i])) : "memory");
+            bar->issued[i] = 0;
+        }
         bar->abort = 0;
-        bar->issued[0] = bar->issued[1] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    if (tid == 0 && my_tiles > 0) {
-        res_load_tile(Xs, &tmX, &bar->full[0], (int)blockIdx.x * kResRows, tile_bytes);
-        bar->issued[0] = 1;
+    if (gtid == 0 && my_tiles > 0) {
+        res_load_tile(Xg, &tmX, &full[0], (int)((2 * (int64_t)b + g) * kResRows), tile_bytes);
+        issued[0] = 1;
     }
     // Resident centroids: C^T in 256-column blocks, one per pass, so a pass reads
     // rows 256 floats apart (zero columns past kpad), and the half norms (+inf past kpad).
@@ -512,32 +543,45 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
     const double u = 5.9604644775390625e-8;  // 2^-24
     const double cmax = cnorm_max ? *cnorm_max : 0.0;
     const int n_pass = kres / kResPass;
+    const int total_turns = steps * n_pass;  // the same for both groups
     // the row of the tile whose final top-3 this lane holds after the exchange
-    const int own = 8 * warp + ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+    const int own = 8 * gw + ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+    RowTop<float> *grun = run + g * kResRows;
     bool ok = true;
-    for (int lt = 0; lt < my_tiles; ++lt) {
+    for (int lt = 0; lt < steps; ++lt) {
+        const bool has = lt < my_tiles;
         const int buf = lt & 1;
-        const int64_t row0 = ((int64_t)blockIdx.x + (int64_t)lt * gridDim.x) * kResRows;
-        // the next tile goes into the other stage, which every thread left at the
-        // end of the previous iteration
-        if (tid == 0 && ok && lt + 1 < my_tiles) {
-            res_load_tile(Xs + (buf ^ 1) * tile_floats, &tmX, &bar->full[buf ^ 1],
-                          (int)(row0 + (int64_t)gridDim.x * kResRows), tile_bytes);
-            bar->issued[buf ^ 1] += 1;
-        }
-        if (ok && !__all_sync(0xffffffffu, res_wait(&bar->full[buf], (lt >> 1) & 1, abort))) ok = false;
-        if (ok) {
-            const float *xa = Xs + buf * tile_floats + (8 * warp) * dpad;
-            for (int pass = 0; pass < n_pass; ++pass) {
+        const int64_t row0 = (2 * ((int64_t)b + (int64_t)lt * grid) + g) * kResRows;
+        for (int pass = 0; pass < n_pass; ++pass) {
+            const int turn = lt * n_pass + pass;
+            // wait for this group's turn at the FMA pipe: group 0 goes first
+            if (g == 0) {
+                if (turn > 0) res_turn_wait(1);
+            } else {
+                res_turn_wait(2);
+            }
+            if (pass == 0) {
+                // The next tile goes into the other stage: its last reads (the previous
+                // tile's contraction) came before this group handed over its previous turn.
+                if (gtid == 0 && ok && lt + 1 < my_tiles) {
+                    res_load_tile(Xg + (buf ^ 1) * tile_floats, &tmX, &full[buf ^ 1],
+                                  (int)(row0 + (int64_t)2 * grid * kResRows), tile_bytes);
+                    issued[buf ^ 1] += 1;
+                }
+                if (has && ok && !__all_sync(0xffffffffu, res_wait(&full[buf], (lt >> 1) & 1, abort))) ok = false;
+            }
+            const bool work = has && ok;
+            // Packed FP32 FMAs (fma.rn.f32x2: two correctly rounded FMAs, the same
+            // results as fmaf): each pair holds two of this lane's clusters for one
+            // row, with the row's value duplicated; one issue slot per two FMAs.
+            float2 acc2[8][4];  // acc2[i][q] = clusters 2q, 2q + 1 of this lane's eight
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc2[i][q] = make_float2(0.f, 0.f);
+            if (work) {
+                const float *xa = Xg + buf * tile_floats + (8 * gw) * dpad;
                 const float *cb = Cs + (size_t)pass * dpad * kResPass + 4 * lane;
-                // Packed FP32 FMAs (fma.rn.f32x2: two correctly rounded FMAs, the same
-                // results as fmaf): each pair holds two of this lane's clusters for one
-                // row, with the row's value duplicated; one issue slot per two FMAs.
-                float2 acc2[8][4];  // acc2[i][q] = clusters 2q, 2q + 1 of this lane's eight
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) acc2[i][q] = make_float2(0.f, 0.f);
 #pragma unroll 2
                 for (int t = 0; t < dpad; t += 2) {
                     float2 a[8];
@@ -564,68 +608,75 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
                         for (int q = 0; q < 4; ++q) acc2[i][q] = __ffma2_rn(ay, by[q], acc2[i][q]);
                     }
                 }
-                float acc[8][8];
+            }
+            // hand the FMA pipe to the other group (group 1's last turn has no taker)
+            if (g == 0) {
+                res_turn_give(2);
+            } else if (turn + 1 < total_turns) {
+                res_turn_give(1);
+            }
+            if (!work) continue;
+            float acc[8][8];
 #pragma unroll
-                for (int i = 0; i < 8; ++i)
+            for (int i = 0; i < 8; ++i)
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        acc[i][2 * q] = acc2[i][q].x;
-                        acc[i][2 * q + 1] = acc2[i][q].y;
-                    }
-                RowTop<float> top[8];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    top[i].b = top[i].s = top[i].t = f_inf<float>();
-                    top[i].ib = top[i].is = 0;
+                for (int q = 0; q < 4; ++q) {
+                    acc[i][2 * q] = acc2[i][q].x;
+                    acc[i][2 * q + 1] = acc2[i][q].y;
                 }
-                // this lane's clusters in ascending order: strict '<' keeps the lowest index on ties
+            RowTop<float> top[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int col = pass * kResPass + (j < 4 ? 4 * lane + j : 128 + 4 * lane + (j - 4));
-                    const float hj = hs[col];
+            for (int i = 0; i < 8; ++i) {
+                top[i].b = top[i].s = top[i].t = f_inf<float>();
+                top[i].ib = top[i].is = 0;
+            }
+            // this lane's clusters in ascending order: strict '<' keeps the lowest index on ties
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) top_push(top[i], hj - acc[i][j], col);
-                }
-                res_exchange<8>(top, 16, (lane >> 4) & 1);
-                res_exchange<4>(top, 8, (lane >> 3) & 1);
-                res_exchange<2>(top, 4, (lane >> 2) & 1);
-                top[0] = top_merge(top[0], shfl_top(top[0], 2));
-                top[0] = top_merge(top[0], shfl_top(top[0], 1));
-                if ((lane & 3) == 0) {
-                    RowTop<float> r = top[0];
-                    if (pass > 0) r = top_merge(run[own], r);
-                    if (pass + 1 < n_pass) {
-                        run[own] = r;
-                    } else {
-                        const int64_t row = row0 + own;
-                        if (row < n) {
-                            labels[row] = r.ib;
-                            const float xn = xnorm[row];
-                            d2[row] = 2.0f * r.b + xn;
-                            if (queue) {
-                                const double xl = sqrt(fmax((double)xn, 0.0));
-                                const double e = 1.0625 * u * (cmax * cmax + (double)(d + 2) * xl * cmax);
-                                const double band = 2.0 * e;
-                                if ((double)r.s - (double)r.b <= band)
-                                    enqueue_recheck(queue, n, st, (int)row, r.ib, r.is,
-                                                    (double)r.t - (double)r.b <= band);
-                            }
+            for (int j = 0; j < 8; ++j) {
+                const int col = pass * kResPass + (j < 4 ? 4 * lane + j : 128 + 4 * lane + (j - 4));
+                const float hj = hs[col];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) top_push(top[i], hj - acc[i][j], col);
+            }
+            res_exchange<8>(top, 16, (lane >> 4) & 1);
+            res_exchange<4>(top, 8, (lane >> 3) & 1);
+            res_exchange<2>(top, 4, (lane >> 2) & 1);
+            top[0] = top_merge(top[0], shfl_top(top[0], 2));
+            top[0] = top_merge(top[0], shfl_top(top[0], 1));
+            if ((lane & 3) == 0) {
+                RowTop<float> r = top[0];
+                if (pass > 0) r = top_merge(grun[own], r);
+                if (pass + 1 < n_pass) {
+                    grun[own] = r;
+                } else {
+                    const int64_t row = row0 + own;
+                    if (row < n) {
+                        labels[row] = r.ib;
+                        const float xn = xnorm[row];
+                        d2[row] = 2.0f * r.b + xn;
+                        if (queue) {
+                            const double xl = sqrt(fmax((double)xn, 0.0));
+                            const double e = 1.0625 * u * (cmax * cmax + (double)(d + 2) * xl * cmax);
+                            const double band = 2.0 * e;
+                            if ((double)r.s - (double)r.b <= band)
+                                enqueue_recheck(queue, n, st, (int)row, r.ib, r.is,
+                                                (double)r.t - (double)r.b <= band);
                         }
                     }
                 }
             }
         }
-        __syncthreads();  // this stage is read by everyone before the next load into it
     }
-    if (tid == 0) {
-        if (bar->abort) {
+    __syncthreads();  // every wait of both groups has ended before abort is read
+    if (gtid == 0) {
+        if (*abort) {
             // leave no bulk copy landing in shared memory behind: wait (bounded) for
-            // the last load issued into each stage
-            for (int b = 0; b < 2; ++b) {
-                const int iss = bar->issued[b];
+            // the last load this group issued into each of its stages
+            for (int s2 = 0; s2 < 2; ++s2) {
+                const int iss = issued[s2];
                 if (!iss) continue;
                 const long long t0 = clock64();
-                while (!res_try_wait(&bar->full[b], (uint32_t)((iss - 1) & 1)) && clock64() - t0 < kResTimeout) {
+                while (!res_try_wait(&full[s2], (uint32_t)((iss - 1) & 1)) && clock64() - t0 < kResTimeout) {
                 }
             }
             if (st) {
@@ -639,8 +690,8 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
 // Shared memory of assign_resident_kernel for dpad features and kres resident
 // clusters (0 when it does not fit the device's per-block limit).
 size_t resident_smem_bytes(int dpad, int kres, int optin) {
-    const size_t b = 128 + (size_t)2 * kResRows * dpad * 4 + (size_t)dpad * kres * 4 + (size_t)kres * 4 +
-                     (size_t)kResRows * sizeof(RowTop<float>) + sizeof(ResBarriers);
+    const size_t b = 128 + (size_t)4 * kResRows * dpad * 4 + (size_t)dpad * kres * 4 + (size_t)kres * 4 +
+                     (size_t)kResCtaRows * sizeof(RowTop<float>) + sizeof(ResBarriers);
     return b <= (size_t)optin ? b : 0;
 }
 
@@ -685,7 +736,7 @@ template <>
 bool launch_resident<float>(const float *X, int64_t n, int64_t d, const float *Ct, const float *h, int64_t k,
                             int64_t kpad, const float *xnorm, const double *cnorm_max, int32_t *labels, float *d2,
                             RecheckEntry *queue, LoopState *st, cudaStream_t s) {
-    if (d % 4 != 0 || d > 256 || (reinterpret_cast<uintptr_t>(X) % 16) != 0 || n > INT32_MAX - 2 * kResRows)
+    if (d % 4 != 0 || d > 256 || (reinterpret_cast<uintptr_t>(X) % 16) != 0 || n > INT32_MAX - 2 * kResCtaRows)
         return false;
     const char *e = getenv("KMB_PLAIN_RESIDENT");
     if (e && e[0] == '0') return false;
@@ -698,7 +749,7 @@ bool launch_resident<float>(const float *X, int64_t n, int64_t d, const float *C
     const size_t smem = resident_smem_bytes(dpad, kres, optin);
     if (smem == 0) return false;
     CUtensorMap tm;
-    // box: 128 rows x dpad columns (columns past d read as zeros)
+    // box: 64 rows x dpad columns (columns past d read as zeros)
     if (!encode_tensor_map_2d(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, X, (uint64_t)d, (uint64_t)n, (uint64_t)d * 4,
                               (uint32_t)dpad, (uint32_t)kResRows, CU_TENSOR_MAP_SWIZZLE_NONE))
         return false;
@@ -710,8 +761,8 @@ bool launch_resident<float>(const float *X, int64_t n, int64_t d, const float *C
         cudaGetLastError();
         return false;
     }
-    const int64_t n_tiles = (n + kResRows - 1) / kResRows;
-    const int grid = (int)std::min<int64_t>(n_tiles, sms);
+    const int64_t n_steps = (n + kResCtaRows - 1) / kResCtaRows;  // 128-row steps: two tiles, one per group
+    const int grid = (int)std::min<int64_t>(n_steps, sms);
     kern<<<grid, kResThreads, smem, s>>>(tm, n, (int)d, dpad, Ct, h, (int)k, (int)kpad, kres, xnorm,
                                                            cnorm_max, labels, d2, queue, st);
     KMB_LAUNCHED();
