@@ -94,6 +94,16 @@ __device__ __forceinline__ void top_push(RowTop<F> &r, F v, int c) {
     }
 }
 
+// top_push with selects instead of branches (the same result).
+__device__ __forceinline__ void top_push_sel(RowTop<float> &r, float v, int c) {
+    const bool lb = v < r.b, ls = v < r.s, lt = v < r.t;
+    r.t = ls ? r.s : (lt ? v : r.t);
+    r.s = lb ? r.b : (ls ? v : r.s);
+    r.is = lb ? r.ib : (ls ? c : r.is);
+    r.b = lb ? v : r.b;
+    r.ib = lb ? c : r.ib;
+}
+
 template <typename F>
 __device__ __forceinline__ RowTop<F> top_merge(const RowTop<F> &x, const RowTop<F> &y) {
     // Merge two sorted triples ((value, index) order); indices are kept for the
@@ -121,6 +131,29 @@ __device__ __forceinline__ RowTop<F> top_merge(const RowTop<F> &x, const RowTop<
     r.s = ov[1];
     r.is = oi[1];
     r.t = ov[2];
+    return r;
+}
+
+// top_merge with selects instead of indexed arrays (the same result, the same
+// comparisons in the same argument order).
+__device__ __forceinline__ RowTop<float> top_merge_sel(const RowTop<float> &x, const RowTop<float> &y) {
+    constexpr int kNone = 0x7fffffff;  // index of a third place
+    const bool c0 = lex_less(x.b, x.ib, y.b, y.ib);
+    // second place: the heads of both lists after the first output
+    const float xa = c0 ? x.s : x.b, ya = c0 ? y.b : y.s;
+    const int xai = c0 ? x.is : x.ib, yai = c0 ? y.ib : y.is;
+    const bool c1 = lex_less(xa, xai, ya, yai);
+    // third place: x took both (x.t vs y.b), y took both (x.b vs y.t), or one each (x.s vs y.s)
+    const bool xx = c0 && c1, yy = !c0 && !c1;
+    const float xh = xx ? x.t : (yy ? x.b : x.s), yh = xx ? y.b : (yy ? y.t : y.s);
+    const int xhi = xx ? kNone : (yy ? x.ib : x.is), yhi = xx ? y.ib : (yy ? kNone : y.is);
+    const bool c2 = lex_less(xh, xhi, yh, yhi);
+    RowTop<float> r;
+    r.b = c0 ? x.b : y.b;
+    r.ib = c0 ? x.ib : y.ib;
+    r.s = c1 ? xa : ya;
+    r.is = c1 ? xai : yai;
+    r.t = c2 ? xh : yh;
     return r;
 }
 
@@ -476,7 +509,7 @@ __device__ __forceinline__ void res_exchange(RowTop<float> (&t)[8], int mask, bo
     for (int q = 0; q < R / 2; ++q) {
         const RowTop<float> keep = hi ? t[R / 2 + q] : t[q];
         const RowTop<float> send = hi ? t[q] : t[R / 2 + q];
-        t[q] = top_merge(keep, shfl_top(send, mask));
+        t[q] = top_merge_sel(keep, shfl_top(send, mask));
     }
 }
 
@@ -582,7 +615,7 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
             if (work) {
                 const float *xa = Xg + buf * tile_floats + (8 * gw) * dpad;
                 const float *cb = Cs + (size_t)pass * dpad * kResPass + 4 * lane;
-#pragma unroll 2
+#pragma unroll 1
                 for (int t = 0; t < dpad; t += 2) {
                     float2 a[8];
 #pragma unroll
@@ -624,28 +657,32 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
                     acc[i][2 * q] = acc2[i][q].x;
                     acc[i][2 * q + 1] = acc2[i][q].y;
                 }
+            // this lane's clusters in ascending order: strict '<' keeps the lowest index on
+            // ties; row by row, so a row's scores are dead once its top-3 is built
+            float hv[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) hv[j] = hs[pass * kResPass + (j < 4 ? 4 * lane + j : 128 + 4 * lane + (j - 4))];
+            const int col0 = pass * kResPass + 4 * lane;
             RowTop<float> top[8];
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                top[i].b = top[i].s = top[i].t = f_inf<float>();
-                top[i].ib = top[i].is = 0;
-            }
-            // this lane's clusters in ascending order: strict '<' keeps the lowest index on ties
+                const float v0 = hv[0] - acc[i][0];
+                const bool l0 = v0 < f_inf<float>();  // a push into an empty triple
+                top[i].b = l0 ? v0 : f_inf<float>();
+                top[i].ib = l0 ? col0 : 0;
+                top[i].s = top[i].t = f_inf<float>();
+                top[i].is = 0;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int col = pass * kResPass + (j < 4 ? 4 * lane + j : 128 + 4 * lane + (j - 4));
-                const float hj = hs[col];
-#pragma unroll
-                for (int i = 0; i < 8; ++i) top_push(top[i], hj - acc[i][j], col);
+                for (int j = 1; j < 8; ++j) top_push_sel(top[i], hv[j] - acc[i][j], col0 + (j < 4 ? j : 124 + j));
             }
             res_exchange<8>(top, 16, (lane >> 4) & 1);
             res_exchange<4>(top, 8, (lane >> 3) & 1);
             res_exchange<2>(top, 4, (lane >> 2) & 1);
-            top[0] = top_merge(top[0], shfl_top(top[0], 2));
-            top[0] = top_merge(top[0], shfl_top(top[0], 1));
+            top[0] = top_merge_sel(top[0], shfl_top(top[0], 2));
+            top[0] = top_merge_sel(top[0], shfl_top(top[0], 1));
             if ((lane & 3) == 0) {
                 RowTop<float> r = top[0];
-                if (pass > 0) r = top_merge(grun[own], r);
+                if (pass > 0) r = top_merge_sel(grun[own], r);
                 if (pass + 1 < n_pass) {
                     grun[own] = r;
                 } else {

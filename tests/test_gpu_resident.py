@@ -58,3 +58,27 @@ def test_resident_equals_tiled(n, d, k):
     s = 0.5 * (Cd ** 2).sum(1)[None, :] - Xd @ Cd.T
     best = np.take_along_axis(s, lab_r[:, None].astype(np.int64), 1)[:, 0]
     assert (best <= s.min(1) + 1e-3 * (1 + np.abs(s.min(1)))).all()
+
+
+def test_resident_nan_rows_take_cluster_zero():
+    """NaN rows: every score is NaN, no strict '<' holds, so the row keeps cluster 0
+    (the reference's strict-'<' scan) in both kernels; the other rows are unaffected."""
+    ctx = _native.context(0)
+    g = torch.Generator(device="cuda").manual_seed(11)
+    X = torch.randn(5000, 64, device="cuda", generator=g) * 2.0
+    C = torch.randn(100, 64, device="cuda", generator=g) * 2.0
+    nan_rows = [3, 100, 4999]
+    X[nan_rows, 5] = float("nan")
+    old = os.environ.get("KMB_PLAIN_RESIDENT")
+    try:
+        os.environ["KMB_PLAIN_RESIDENT"] = "1"
+        lab_r, _ = _infer(ctx, X, C)
+        os.environ["KMB_PLAIN_RESIDENT"] = "0"
+        lab_t, _ = _infer(ctx, X, C)
+    finally:
+        if old is None:
+            os.environ.pop("KMB_PLAIN_RESIDENT", None)
+        else:
+            os.environ["KMB_PLAIN_RESIDENT"] = old
+    assert (lab_r == lab_t).all()
+    assert (lab_r[nan_rows] == 0).all()
