@@ -95,7 +95,8 @@ __device__ __forceinline__ void top_push(RowTop<F> &r, F v, int c) {
 }
 
 // top_push with selects instead of branches (the same result).
-__device__ __forceinline__ void top_push_sel(RowTop<float> &r, float v, int c) {
+template <typename F>
+__device__ __forceinline__ void top_push_sel(RowTop<F> &r, F v, int c) {
     const bool lb = v < r.b, ls = v < r.s, lt = v < r.t;
     r.t = ls ? r.s : (lt ? v : r.t);
     r.s = lb ? r.b : (ls ? v : r.s);
@@ -136,19 +137,20 @@ __device__ __forceinline__ RowTop<F> top_merge(const RowTop<F> &x, const RowTop<
 
 // top_merge with selects instead of indexed arrays (the same result, the same
 // comparisons in the same argument order).
-__device__ __forceinline__ RowTop<float> top_merge_sel(const RowTop<float> &x, const RowTop<float> &y) {
+template <typename F>
+__device__ __forceinline__ RowTop<F> top_merge_sel(const RowTop<F> &x, const RowTop<F> &y) {
     constexpr int kNone = 0x7fffffff;  // index of a third place
     const bool c0 = lex_less(x.b, x.ib, y.b, y.ib);
     // second place: the heads of both lists after the first output
-    const float xa = c0 ? x.s : x.b, ya = c0 ? y.b : y.s;
+    const F xa = c0 ? x.s : x.b, ya = c0 ? y.b : y.s;
     const int xai = c0 ? x.is : x.ib, yai = c0 ? y.ib : y.is;
     const bool c1 = lex_less(xa, xai, ya, yai);
     // third place: x took both (x.t vs y.b), y took both (x.b vs y.t), or one each (x.s vs y.s)
     const bool xx = c0 && c1, yy = !c0 && !c1;
-    const float xh = xx ? x.t : (yy ? x.b : x.s), yh = xx ? y.b : (yy ? y.t : y.s);
+    const F xh = xx ? x.t : (yy ? x.b : x.s), yh = xx ? y.b : (yy ? y.t : y.s);
     const int xhi = xx ? kNone : (yy ? x.ib : x.is), yhi = xx ? y.ib : (yy ? kNone : y.is);
     const bool c2 = lex_less(xh, xhi, yh, yhi);
-    RowTop<float> r;
+    RowTop<F> r;
     r.b = c0 ? x.b : y.b;
     r.ib = c0 ? x.ib : y.ib;
     r.s = c1 ? xa : ya;
@@ -269,7 +271,7 @@ assign_plain_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restri
                 const F hj = h[col];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    top_push(top[i], hj - acc[i][j], col);
+                    top_push_sel(top[i], hj - acc[i][j], col);
                     acc[i][j] = F(0);
                 }
             }
@@ -282,7 +284,7 @@ assign_plain_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restri
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
 #pragma unroll
-        for (int m = 8; m >= 1; m >>= 1) top[i] = top_merge(top[i], shfl_top(top[i], m));
+        for (int m = 8; m >= 1; m >>= 1) top[i] = top_merge_sel(top[i], shfl_top(top[i], m));
     }
     if (tx == 0) {
         const double u = unit_roundoff<F>();
