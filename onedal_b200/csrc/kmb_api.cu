@@ -20,6 +20,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <random>
 #include <string>
@@ -103,6 +105,43 @@ static bool alloc_failure_injected() {
     return e && e[0] == '1';
 }
 
+// The library's stream-ordered allocations (context workspaces, the batched
+// form's arenas, the serving loop's arenas) come from a memory pool of the library
+// (one per device, created on first use) that keeps freed memory for the next
+// allocation instead of returning it to the driver at every synchronisation, as
+// the device's default pool does unless told otherwise: a fresh mapping of a large
+// block stalled the device for tens of milliseconds. The pool holds at most the
+// largest set of buffers in use at one time until the process exits.
+static std::mutex g_pool_mu;
+static std::map<int, cudaMemPool_t> g_pools;
+
+cudaMemPool_t library_pool(int dev) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    auto it = g_pools.find(dev);
+    if (it != g_pools.end()) return it->second;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        pool = nullptr;
+    } else {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    g_pools[dev] = pool;
+    return pool;
+}
+
+// From the library's pool when it exists, else the device's default pool.
+cudaError_t pool_alloc(void **p, size_t bytes, int dev, cudaStream_t s) {
+    cudaMemPool_t pool = library_pool(dev);
+    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
+}
+
 bool Workspace::ensure(DevBuf &b, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (b.bytes >= bytes) return true;
@@ -112,7 +151,7 @@ bool Workspace::ensure(DevBuf &b, size_t bytes) {
     b.bytes = 0;
     // round up to 2 MiB to limit reallocations
     const size_t rounded = (bytes + (size_t(2) << 20) - 1) / (size_t(2) << 20) * (size_t(2) << 20);
-    if (cudaMallocAsync(&b.ptr, rounded, stream) != cudaSuccess) {
+    if (pool_alloc(&b.ptr, rounded, device, stream) != cudaSuccess) {
         cudaGetLastError();
         b.ptr = nullptr;
         return false;

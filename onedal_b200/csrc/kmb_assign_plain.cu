@@ -418,12 +418,12 @@ assign_small_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restri
 }
 
 // ---- FP32, centroids resident in shared memory ------------------------------
-// When all (padded) centroids fit in shared memory next to the row stages, one
-// persistent CTA per SM keeps C^T and the half norms resident for the whole
-// launch and streams 64-row tiles of X through TMA, so no centroid byte is
+// When the (padded) centroids -- all of them, or a chunk of them -- fit in shared
+// memory next to the row stages, one persistent CTA per SM keeps C^T and the half
+// norms resident and streams 64-row tiles of X through TMA, so no centroid byte is
 // re-read per row tile. 16 warps in two groups of 8; each group owns every other
-// 64-row tile (group g of CTA b takes tiles 2(b + i·grid) + g) and two TMA stages.
-// In a group, warp w owns rows 8w..8w+7 of the tile, lane l the clusters
+// 64-row tile (group g of CTA b takes tiles 2(b + i·grid) + g) and one or two TMA
+// stages. In a group, warp w owns rows 8w..8w+7 of the tile, lane l the clusters
 // 4l..4l+3 and 128+4l..128+4l+3 of each 256-cluster pass: the row values are
 // shared-memory broadcasts and the centroid reads are conflict-free 16-byte
 // loads. Per (row, cluster) the contraction accumulates x_t * c_t in ascending
@@ -434,14 +434,24 @@ assign_small_kernel(const F *__restrict__ X, int64_t n, int d, const F *__restri
 // index) triples, leaving each row's top-3 in four lanes; with more than one
 // pass the row's owner lane merges it into the running top-3 in shared memory.
 //
+// Chunks: when all clusters do not fit, they are taken kchunk at a time (a
+// multiple of 256). A CTA walks blocks of bt row tiles per group; for each chunk it
+// loads the chunk's C^T and half norms (every warp past a CTA barrier before and
+// after), then runs the block's tiles against it; the running top-3 of the block's
+// rows stays in shared memory across chunks and passes (merged in ascending cluster
+// order, as one long pass would), and the block's rows come back from L2 for every
+// chunk (bt = 8: 1024 rows per CTA, 76 MB over the grid at d = 128).
+//
 // Ping-pong: the two groups take turns at the FMA pipe. A group runs a pass's
 // contraction only in its turn and hands the turn over (named barriers 1 and 2)
 // before its top-3 epilogue, so one group's epilogue (compares, selects,
 // shuffles) issues beside the other group's FMAs instead of every warp of the SM
 // reaching its epilogue at once and leaving the FMA pipe idle. Both groups take
 // the same number of turns (a group without a tile left takes empty turns), so
-// every barrier completes; the turn barriers also order a stage's last reads
-// before the TMA load that refills it.
+// every barrier completes. With two stages per group the next tile's load is
+// issued at the start of a tile's first turn (the turn barriers order the
+// stage's last reads before it); with one stage, after the tile's last
+// contraction, once the group's warps have met at named barrier 3 + g.
 constexpr int kResThreads = 512;
 constexpr int kResGroupThreads = 256;
 constexpr int kResRows = 64;    // rows per tile (one group's)
@@ -516,26 +526,31 @@ __device__ __forceinline__ void res_exchange(RowTop<float> (&t)[8], int mask, bo
 }
 
 // DPADT > 0 fixes the padded row width at compile time (row and centroid offsets
-// become immediates); 0 reads it from dpad.
-template <int DPADT>
+// become immediates); 0 reads it from dpad. STAGES: TMA stages per group (1 or 2).
+// kres: all clusters, padded to 256; kchunk: clusters resident at a time (kres when
+// n_chunks == 1); bt: row tiles per block and group (the running top-3 rows).
+// CHUNK false: all clusters resident (n_chunks = bt = 1 at compile time).
+template <int DPADT, int STAGES, bool CHUNK>
 __global__ void __launch_bounds__(kResThreads, 1)
 assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d, int dpad_rt, const float *__restrict__ Ct,
-                       const float *__restrict__ h, int k, int kpad, int kres, const float *__restrict__ xnorm,
-                       const double *__restrict__ cnorm_max, int32_t *__restrict__ labels, float *__restrict__ d2,
-                       RecheckEntry *__restrict__ queue, LoopState *__restrict__ st) {
+                       const float *__restrict__ h, int k, int kpad, int kres, int kchunk, int n_chunks_rt, int bt_rt,
+                       const float *__restrict__ xnorm, const double *__restrict__ cnorm_max,
+                       int32_t *__restrict__ labels, float *__restrict__ d2, RecheckEntry *__restrict__ queue,
+                       LoopState *__restrict__ st) {
     __shared__ int s_skip;
     if (threadIdx.x == 0) s_skip = st ? st->done : 0;
     __syncthreads();
     if (s_skip) return;
     const int dpad = DPADT > 0 ? DPADT : dpad_rt;
+    const int n_chunks = CHUNK ? n_chunks_rt : 1, bt = CHUNK ? bt_rt : 1;
     extern __shared__ uint8_t res_smem_raw[];
     uint8_t *sm = (uint8_t *)(((uintptr_t)res_smem_raw + 127) & ~(uintptr_t)127);
     const int tile_floats = kResRows * dpad;
-    float *Xs = (float *)sm;                   // [group][stage][64][dpad]
-    float *Cs = Xs + 4 * tile_floats;          // [kres / 256][dpad][256]: pass-major blocks
-    float *hs = Cs + (size_t)dpad * kres;      // [kres]
-    RowTop<float> *run = (RowTop<float> *)(hs + kres);  // [group][64] running top-3 across passes
-    ResBarriers *bar = (ResBarriers *)(run + kResCtaRows);
+    float *Xs = (float *)sm;                        // [group][stage][64][dpad]
+    float *Cs = Xs + 2 * STAGES * tile_floats;      // [kchunk / 256][dpad][256]: pass-major blocks
+    float *hs = Cs + (size_t)dpad * kchunk;         // [kchunk]
+    RowTop<float> *run = (RowTop<float> *)(hs + kchunk);  // [group][bt][64] running top-3
+    ResBarriers *bar = (ResBarriers *)(run + 2 * bt * kResRows);
     volatile int *abort = &bar->abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = warp >> 3, gw = warp & 7, gtid = tid & (kResGroupThreads - 1);
@@ -547,7 +562,7 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
     const int my_tiles = par_tiles > b ? (int)((par_tiles - b + grid - 1) / grid) : 0;
     const int steps = par_tiles0 > b ? (int)((par_tiles0 - b + grid - 1) / grid) : 0;  // group 0's count
     const uint32_t tile_bytes = (uint32_t)tile_floats * 4u;
-    float *Xg = Xs + 2 * g * tile_floats;  // this group's two stages
+    float *Xg = Xs + STAGES * g * tile_floats;  // this group's stages
     uint64_t *full = &bar->full[2 * g];
     int *issued = &bar->issued[2 * g];
     if (tid == 0) {
@@ -559,147 +574,194 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    int m_issue = 0, m_wait = 0;  // this group's loads issued (its thread 0) and waited for
     if (gtid == 0 && my_tiles > 0) {
         res_load_tile(Xg, &tmX, &full[0], (int)((2 * (int64_t)b + g) * kResRows), tile_bytes);
         issued[0] = 1;
+        m_issue = 1;
     }
-    // Resident centroids: C^T in 256-column blocks, one per pass, so a pass reads
-    // rows 256 floats apart (zero columns past kpad), and the half norms (+inf past kpad).
-    const int kq = kres / 4;
-    for (int i = tid; i < dpad * kq; i += kResThreads) {
-        const int t = i / kq, c = 4 * (i - t * kq);
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (c < kpad) v = *reinterpret_cast<const float4 *>(Ct + (size_t)t * kpad + c);
-        *reinterpret_cast<float4 *>(Cs + ((size_t)(c / kResPass) * dpad + t) * kResPass + (c % kResPass)) = v;
-    }
-    for (int j = tid; j < kres; j += kResThreads) hs[j] = j < kpad ? h[j] : f_inf<float>();
+    // Resident centroids of chunk q: C^T in 256-column blocks, one per pass, so a pass
+    // reads rows 256 floats apart (zero columns past kpad), and the half norms (+inf
+    // past kpad).
+    auto load_chunk = [&](int q) {
+        const int c0 = q * kchunk, kc = min(kchunk, kres - c0), kq = kc / 4;
+        for (int i = tid; i < dpad * kq; i += kResThreads) {
+            const int t = i / kq, c = 4 * (i - t * kq);
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (c0 + c < kpad) v = *reinterpret_cast<const float4 *>(Ct + (size_t)t * kpad + c0 + c);
+            *reinterpret_cast<float4 *>(Cs + ((size_t)(c / kResPass) * dpad + t) * kResPass + (c % kResPass)) = v;
+        }
+        for (int j = tid; j < kc; j += kResThreads) hs[j] = c0 + j < kpad ? h[c0 + j] : f_inf<float>();
+    };
+    load_chunk(0);
     __syncthreads();
 
     const double u = 5.9604644775390625e-8;  // 2^-24
     const double cmax = cnorm_max ? *cnorm_max : 0.0;
-    const int n_pass = kres / kResPass;
-    const int total_turns = steps * n_pass;  // the same for both groups
+    const int total_turns = steps * (kres / kResPass);  // the same for both groups
     // the row of the tile whose final top-3 this lane holds after the exchange
     const int own = 8 * gw + ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-    RowTop<float> *grun = run + g * kResRows;
     bool ok = true;
-    for (int lt = 0; lt < steps; ++lt) {
-        const bool has = lt < my_tiles;
-        const int buf = lt & 1;
-        const int64_t row0 = (2 * ((int64_t)b + (int64_t)lt * grid) + g) * kResRows;
-        for (int pass = 0; pass < n_pass; ++pass) {
-            const int turn = lt * n_pass + pass;
-            // wait for this group's turn at the FMA pipe: group 0 goes first
-            if (g == 0) {
-                if (turn > 0) res_turn_wait(1);
-            } else {
-                res_turn_wait(2);
+    int turn = 0;
+    const int n_blocks = (steps + bt - 1) / bt;
+    for (int blk = 0; blk < n_blocks; ++blk) {
+        const int u_n = min(bt, steps - blk * bt);
+        for (int q = 0; q < n_chunks; ++q) {
+            if (n_chunks > 1 && (blk > 0 || q > 0)) {
+                __syncthreads();  // every warp is done with the previous chunk's centroids
+                load_chunk(q);
+                __syncthreads();
             }
-            if (pass == 0) {
-                // The next tile goes into the other stage: its last reads (the previous
-                // tile's contraction) came before this group handed over its previous turn.
-                if (gtid == 0 && ok && lt + 1 < my_tiles) {
-                    res_load_tile(Xg + (buf ^ 1) * tile_floats, &tmX, &full[buf ^ 1],
-                                  (int)(row0 + (int64_t)2 * grid * kResRows), tile_bytes);
-                    issued[buf ^ 1] += 1;
-                }
-                if (has && ok && !__all_sync(0xffffffffu, res_wait(&full[buf], (lt >> 1) & 1, abort))) ok = false;
-            }
-            const bool work = has && ok;
-            // Packed FP32 FMAs (fma.rn.f32x2: two correctly rounded FMAs, the same
-            // results as fmaf): each pair holds two of this lane's clusters for one
-            // row, with the row's value duplicated; one issue slot per two FMAs.
-            float2 acc2[8][4];  // acc2[i][q] = clusters 2q, 2q + 1 of this lane's eight
+            const int c0 = q * kchunk;
+            const int ppc = min(kchunk, kres - c0) / kResPass;
+            for (int ut = 0; ut < u_n; ++ut) {
+                const int lt = blk * bt + ut;
+                const bool has = lt < my_tiles;
+                const int64_t row0 = (2 * ((int64_t)b + (int64_t)lt * grid) + g) * kResRows;
+                // the next tile this group loads: the next of the block, else the block's
+                // first (next chunk), else the next block's first
+                int nxt;
+                if (ut + 1 < u_n && lt + 1 < my_tiles) nxt = lt + 1;
+                else if (q + 1 < n_chunks) nxt = blk * bt;
+                else nxt = (blk + 1) * bt;
+                const bool nxt_has = has && nxt < my_tiles;
+                RowTop<float> *grun = run + (g * bt + ut) * kResRows;
+                // this tile's stage and load parity (all clusters resident: the group's
+                // tiles are loaded in order, so its load count is lt)
+                const int mw = CHUNK ? m_wait : lt;
+                const int stage = mw % STAGES;
+                const uint32_t parity = (uint32_t)(mw / STAGES) & 1u;
+                if (has) ++m_wait;
+                for (int pass = 0; pass < ppc; ++pass, ++turn) {
+                    // wait for this group's turn at the FMA pipe: group 0 goes first
+                    if (g == 0) {
+                        if (turn > 0) res_turn_wait(1);
+                    } else {
+                        res_turn_wait(2);
+                    }
+                    if (pass == 0 && has) {
+                        // Two stages: the next tile goes into the other stage, whose last
+                        // reads (the previous tile's contractions) came before this group
+                        // handed over its previous turn.
+                        if (STAGES == 2 && gtid == 0 && ok && nxt_has) {
+                            const int s2 = (CHUNK ? m_issue : lt + 1) % STAGES;
+                            res_load_tile(Xg + s2 * tile_floats, &tmX, &full[s2],
+                                          (int)((2 * ((int64_t)b + (int64_t)nxt * grid) + g) * kResRows), tile_bytes);
+                            issued[s2] += 1;
+                            ++m_issue;
+                        }
+                        if (ok && !__all_sync(0xffffffffu, res_wait(&full[stage], parity, abort))) ok = false;
+                    }
+                    const bool work = has && ok;
+                    // Packed FP32 FMAs (fma.rn.f32x2: two correctly rounded FMAs, the same
+                    // results as fmaf): each pair holds two of this lane's clusters for one
+                    // row, with the row's value duplicated; one issue slot per two FMAs.
+                    float2 acc2[8][4];  // acc2[i][q] = clusters 2q, 2q + 1 of this lane's eight
 #pragma unroll
-            for (int i = 0; i < 8; ++i)
+                    for (int i = 0; i < 8; ++i)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc2[i][q] = make_float2(0.f, 0.f);
-            if (work) {
-                const float *xa = Xg + buf * tile_floats + (8 * gw) * dpad;
-                const float *cb = Cs + (size_t)pass * dpad * kResPass + 4 * lane;
+                        for (int q2 = 0; q2 < 4; ++q2) acc2[i][q2] = make_float2(0.f, 0.f);
+                    if (work) {
+                        const float *xa = Xg + stage * tile_floats + (8 * gw) * dpad;
+                        const float *cb = Cs + (size_t)pass * dpad * kResPass + 4 * lane;
 #pragma unroll 1
-                for (int t = 0; t < dpad; t += 2) {
-                    float2 a[8];
+                        for (int t = 0; t < dpad; t += 2) {
+                            float2 a[8];
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) a[i] = *reinterpret_cast<const float2 *>(xa + i * dpad + t);
-                    const float4 b00 = *reinterpret_cast<const float4 *>(cb + t * kResPass);
-                    const float4 b01 = *reinterpret_cast<const float4 *>(cb + t * kResPass + 128);
-                    const float4 b10 = *reinterpret_cast<const float4 *>(cb + (t + 1) * kResPass);
-                    const float4 b11 = *reinterpret_cast<const float4 *>(cb + (t + 1) * kResPass + 128);
-                    const float2 bx[4] = {make_float2(b00.x, b00.y), make_float2(b00.z, b00.w), make_float2(b01.x, b01.y),
-                                          make_float2(b01.z, b01.w)};
-                    const float2 by[4] = {make_float2(b10.x, b10.y), make_float2(b10.z, b10.w), make_float2(b11.x, b11.y),
-                                          make_float2(b11.z, b11.w)};
+                            for (int i = 0; i < 8; ++i) a[i] = *reinterpret_cast<const float2 *>(xa + i * dpad + t);
+                            const float4 b00 = *reinterpret_cast<const float4 *>(cb + t * kResPass);
+                            const float4 b01 = *reinterpret_cast<const float4 *>(cb + t * kResPass + 128);
+                            const float4 b10 = *reinterpret_cast<const float4 *>(cb + (t + 1) * kResPass);
+                            const float4 b11 = *reinterpret_cast<const float4 *>(cb + (t + 1) * kResPass + 128);
+                            const float2 bx[4] = {make_float2(b00.x, b00.y), make_float2(b00.z, b00.w),
+                                                  make_float2(b01.x, b01.y), make_float2(b01.z, b01.w)};
+                            const float2 by[4] = {make_float2(b10.x, b10.y), make_float2(b10.z, b10.w),
+                                                  make_float2(b11.x, b11.y), make_float2(b11.z, b11.w)};
+#pragma unroll
+                            for (int i = 0; i < 8; ++i) {
+                                const float2 ax = make_float2(a[i].x, a[i].x);
+#pragma unroll
+                                for (int q2 = 0; q2 < 4; ++q2) acc2[i][q2] = __ffma2_rn(ax, bx[q2], acc2[i][q2]);
+                            }
+#pragma unroll
+                            for (int i = 0; i < 8; ++i) {
+                                const float2 ay = make_float2(a[i].y, a[i].y);
+#pragma unroll
+                                for (int q2 = 0; q2 < 4; ++q2) acc2[i][q2] = __ffma2_rn(ay, by[q2], acc2[i][q2]);
+                            }
+                        }
+                    }
+                    const bool last_pass = pass + 1 == ppc;
+                    // One stage: the group's warps meet once the tile's last contraction is
+                    // done (warp 0 waits, the others arrive), before the turn goes over.
+                    if (STAGES == 1 && last_pass) {
+                        if (gw == 0) asm volatile("bar.sync %0, %1;" ::"r"(3 + g), "r"(kResGroupThreads) : "memory");
+                        else asm volatile("bar.arrive %0, %1;" ::"r"(3 + g), "r"(kResGroupThreads) : "memory");
+                    }
+                    // hand the FMA pipe to the other group (group 1's last turn has no taker)
+                    if (g == 0) {
+                        res_turn_give(2);
+                    } else if (turn + 1 < total_turns) {
+                        res_turn_give(1);
+                    }
+                    if (STAGES == 1 && last_pass && gtid == 0 && ok && nxt_has) {
+                        res_load_tile(Xg, &tmX, &full[0], (int)((2 * ((int64_t)b + (int64_t)nxt * grid) + g) * kResRows),
+                                      tile_bytes);
+                        issued[0] += 1;
+                        ++m_issue;
+                    }
+                    if (!work) continue;
+                    float acc[8][8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+#pragma unroll
+                        for (int q2 = 0; q2 < 4; ++q2) {
+                            acc[i][2 * q2] = acc2[i][q2].x;
+                            acc[i][2 * q2 + 1] = acc2[i][q2].y;
+                        }
+                    // this lane's clusters in ascending order: strict '<' keeps the lowest index
+                    // on ties; row by row, so a row's scores are dead once its top-3 is built
+                    float hv[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) hv[j] = hs[pass * kResPass + (j < 4 ? 4 * lane + j : 128 + 4 * lane + (j - 4))];
+                    const int col0 = c0 + pass * kResPass + 4 * lane;
+                    RowTop<float> top[8];
 #pragma unroll
                     for (int i = 0; i < 8; ++i) {
-                        const float2 ax = make_float2(a[i].x, a[i].x);
+                        const float v0 = hv[0] - acc[i][0];
+                        const bool l0 = v0 < f_inf<float>();  // a push into an empty triple
+                        top[i].b = l0 ? v0 : f_inf<float>();
+                        top[i].ib = l0 ? col0 : 0;
+                        top[i].s = top[i].t = f_inf<float>();
+                        top[i].is = 0;
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) acc2[i][q] = __ffma2_rn(ax, bx[q], acc2[i][q]);
+                        for (int j = 1; j < 8; ++j) top_push_sel(top[i], hv[j] - acc[i][j], col0 + (j < 4 ? j : 124 + j));
                     }
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const float2 ay = make_float2(a[i].y, a[i].y);
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) acc2[i][q] = __ffma2_rn(ay, by[q], acc2[i][q]);
-                    }
-                }
-            }
-            // hand the FMA pipe to the other group (group 1's last turn has no taker)
-            if (g == 0) {
-                res_turn_give(2);
-            } else if (turn + 1 < total_turns) {
-                res_turn_give(1);
-            }
-            if (!work) continue;
-            float acc[8][8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    acc[i][2 * q] = acc2[i][q].x;
-                    acc[i][2 * q + 1] = acc2[i][q].y;
-                }
-            // this lane's clusters in ascending order: strict '<' keeps the lowest index on
-            // ties; row by row, so a row's scores are dead once its top-3 is built
-            float hv[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) hv[j] = hs[pass * kResPass + (j < 4 ? 4 * lane + j : 128 + 4 * lane + (j - 4))];
-            const int col0 = pass * kResPass + 4 * lane;
-            RowTop<float> top[8];
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const float v0 = hv[0] - acc[i][0];
-                const bool l0 = v0 < f_inf<float>();  // a push into an empty triple
-                top[i].b = l0 ? v0 : f_inf<float>();
-                top[i].ib = l0 ? col0 : 0;
-                top[i].s = top[i].t = f_inf<float>();
-                top[i].is = 0;
-#pragma unroll
-                for (int j = 1; j < 8; ++j) top_push_sel(top[i], hv[j] - acc[i][j], col0 + (j < 4 ? j : 124 + j));
-            }
-            res_exchange<8>(top, 16, (lane >> 4) & 1);
-            res_exchange<4>(top, 8, (lane >> 3) & 1);
-            res_exchange<2>(top, 4, (lane >> 2) & 1);
-            top[0] = top_merge_sel(top[0], shfl_top(top[0], 2));
-            top[0] = top_merge_sel(top[0], shfl_top(top[0], 1));
-            if ((lane & 3) == 0) {
-                RowTop<float> r = top[0];
-                if (pass > 0) r = top_merge_sel(grun[own], r);
-                if (pass + 1 < n_pass) {
-                    grun[own] = r;
-                } else {
-                    const int64_t row = row0 + own;
-                    if (row < n) {
-                        labels[row] = r.ib;
-                        const float xn = xnorm[row];
-                        d2[row] = 2.0f * r.b + xn;
-                        if (queue) {
-                            const double xl = sqrt(fmax((double)xn, 0.0));
-                            const double e = 1.0625 * u * (cmax * cmax + (double)(d + 2) * xl * cmax);
-                            const double band = 2.0 * e;
-                            if ((double)r.s - (double)r.b <= band)
-                                enqueue_recheck(queue, n, st, (int)row, r.ib, r.is,
-                                                (double)r.t - (double)r.b <= band);
+                    res_exchange<8>(top, 16, (lane >> 4) & 1);
+                    res_exchange<4>(top, 8, (lane >> 3) & 1);
+                    res_exchange<2>(top, 4, (lane >> 2) & 1);
+                    top[0] = top_merge_sel(top[0], shfl_top(top[0], 2));
+                    top[0] = top_merge_sel(top[0], shfl_top(top[0], 1));
+                    if ((lane & 3) == 0) {
+                        RowTop<float> r = top[0];
+                        if (q > 0 || pass > 0) r = top_merge_sel(grun[own], r);
+                        if (q + 1 < n_chunks || !last_pass) {
+                            grun[own] = r;
+                        } else {
+                            const int64_t row = row0 + own;
+                            if (row < n) {
+                                labels[row] = r.ib;
+                                const float xn = xnorm[row];
+                                d2[row] = 2.0f * r.b + xn;
+                                if (queue) {
+                                    const double xl = sqrt(fmax((double)xn, 0.0));
+                                    const double e = 1.0625 * u * (cmax * cmax + (double)(d + 2) * xl * cmax);
+                                    const double band = 2.0 * e;
+                                    if ((double)r.s - (double)r.b <= band)
+                                        enqueue_recheck(queue, n, st, (int)row, r.ib, r.is,
+                                                        (double)r.t - (double)r.b <= band);
+                                }
+                            }
                         }
                     }
                 }
@@ -711,7 +773,7 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
         if (*abort) {
             // leave no bulk copy landing in shared memory behind: wait (bounded) for
             // the last load this group issued into each of its stages
-            for (int s2 = 0; s2 < 2; ++s2) {
+            for (int s2 = 0; s2 < STAGES; ++s2) {
                 const int iss = issued[s2];
                 if (!iss) continue;
                 const long long t0 = clock64();
@@ -726,12 +788,11 @@ assign_resident_kernel(const __grid_constant__ CUtensorMap tmX, int64_t n, int d
     }
 }
 
-// Shared memory of assign_resident_kernel for dpad features and kres resident
-// clusters (0 when it does not fit the device's per-block limit).
-size_t resident_smem_bytes(int dpad, int kres, int optin) {
-    const size_t b = 128 + (size_t)4 * kResRows * dpad * 4 + (size_t)dpad * kres * 4 + (size_t)kres * 4 +
-                     (size_t)kResCtaRows * sizeof(RowTop<float>) + sizeof(ResBarriers);
-    return b <= (size_t)optin ? b : 0;
+// Shared memory of assign_resident_kernel for dpad features, kchunk resident
+// clusters, STAGES stages per group and bt running-top-3 tiles per group.
+size_t resident_smem_bytes(int dpad, int kchunk, int stages, int bt) {
+    return 128 + (size_t)2 * stages * kResRows * dpad * 4 + (size_t)dpad * kchunk * 4 + (size_t)kchunk * 4 +
+           (size_t)2 * bt * kResRows * sizeof(RowTop<float>) + sizeof(ResBarriers);
 }
 
 }  // namespace
@@ -764,8 +825,9 @@ void launch_small(const F *X, int64_t n, int64_t d, const F *Ct, const F *h, int
     KMB_LAUNCHED();
 }
 
-// FP32 rows whose centroids fit in shared memory (d a multiple of 4 and at most
-// 256, 16-byte aligned rows): the resident kernel. False when it does not apply.
+// FP32 rows whose centroids -- all of them, or 256-cluster multiples at a time --
+// fit in shared memory (d a multiple of 4 and at most 256, 16-byte aligned rows):
+// the resident kernel. False when it does not apply.
 template <typename F>
 bool launch_resident(const F *, int64_t, int64_t, const F *, const F *, int64_t, int64_t, const F *, const double *,
                      int32_t *, F *, RecheckEntry *, LoopState *, cudaStream_t) {
@@ -785,25 +847,52 @@ bool launch_resident<float>(const float *X, int64_t n, int64_t d, const float *C
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = resident_smem_bytes(dpad, kres, optin);
-    if (smem == 0) return false;
+    // All clusters resident with two stages per group; else chunks of clusters, the
+    // first of (stages, bt) = (2, 8), (2, 4), (1, 8), (1, 4) that holds 256 of them,
+    // with the chunks evened out.
+    int stages = 2, bt = 1, kchunk = kres;
+    if (resident_smem_bytes(dpad, kres, 2, 1) > (size_t)optin) {
+        const int opts[4][2] = {{2, 8}, {2, 4}, {1, 8}, {1, 4}};
+        kchunk = 0;
+        for (const auto &o : opts) {
+            const size_t base = resident_smem_bytes(dpad, 0, o[0], o[1]);
+            if (base >= (size_t)optin) continue;
+            const int fit = (int)(((size_t)optin - base) / ((size_t)dpad * 4 + 4)) / kResPass * kResPass;
+            if (fit >= kResPass) {
+                stages = o[0];
+                bt = o[1];
+                kchunk = std::min(fit, kres);
+                break;
+            }
+        }
+        if (kchunk == 0) return false;
+        const int nc = (kres + kchunk - 1) / kchunk;
+        kchunk = (kres / kResPass + nc - 1) / nc * kResPass;
+    }
+    const int n_chunks = (kres + kchunk - 1) / kchunk;
+    const size_t smem = resident_smem_bytes(dpad, kchunk, stages, bt);
+    if (smem > (size_t)optin) return false;
     CUtensorMap tm;
     // box: 64 rows x dpad columns (columns past d read as zeros)
     if (!encode_tensor_map_2d(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, X, (uint64_t)d, (uint64_t)n, (uint64_t)d * 4,
                               (uint32_t)dpad, (uint32_t)kResRows, CU_TENSOR_MAP_SWIZZLE_NONE))
         return false;
-    auto kern = dpad == 32    ? assign_resident_kernel<32>
-                : dpad == 64  ? assign_resident_kernel<64>
-                : dpad == 128 ? assign_resident_kernel<128>
-                              : assign_resident_kernel<0>;
+    auto pick = [&](auto k32, auto k64, auto k128, auto k0) { return dpad == 32 ? k32 : dpad == 64 ? k64 : dpad == 128 ? k128 : k0; };
+    auto kern = n_chunks == 1 && bt == 1
+                    ? pick(assign_resident_kernel<32, 2, false>, assign_resident_kernel<64, 2, false>,
+                           assign_resident_kernel<128, 2, false>, assign_resident_kernel<0, 2, false>)
+                : stages == 2 ? pick(assign_resident_kernel<32, 2, true>, assign_resident_kernel<64, 2, true>,
+                                     assign_resident_kernel<128, 2, true>, assign_resident_kernel<0, 2, true>)
+                              : pick(assign_resident_kernel<32, 1, true>, assign_resident_kernel<64, 1, true>,
+                                     assign_resident_kernel<128, 1, true>, assign_resident_kernel<0, 1, true>);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
     const int64_t n_steps = (n + kResCtaRows - 1) / kResCtaRows;  // 128-row steps: two tiles, one per group
     const int grid = (int)std::min<int64_t>(n_steps, sms);
-    kern<<<grid, kResThreads, smem, s>>>(tm, n, (int)d, dpad, Ct, h, (int)k, (int)kpad, kres, xnorm,
-                                                           cnorm_max, labels, d2, queue, st);
+    kern<<<grid, kResThreads, smem, s>>>(tm, n, (int)d, dpad, Ct, h, (int)k, (int)kpad, kres, kchunk, n_chunks, bt,
+                                         xnorm, cnorm_max, labels, d2, queue, st);
     KMB_LAUNCHED();
     return true;
 }

@@ -818,41 +818,6 @@ int batched_kpad(int k) {
     return b;
 }
 
-// The batched form's stream-ordered allocations come from a memory pool of the
-// library (one per device, created on first use) that keeps freed memory for the
-// next call instead of returning it to the driver at every synchronisation, as the
-// default pool does unless told otherwise. It holds at most the largest call's
-// arena until the process exits.
-std::mutex g_pool_mu;
-std::map<int, cudaMemPool_t> g_pools;
-
-cudaMemPool_t batched_pool(int dev) {
-    std::lock_guard<std::mutex> lock(g_pool_mu);
-    auto it = g_pools.find(dev);
-    if (it != g_pools.end()) return it->second;
-    cudaMemPoolProps props = {};
-    props.allocType = cudaMemAllocationTypePinned;
-    props.handleTypes = cudaMemHandleTypeNone;
-    props.location.type = cudaMemLocationTypeDevice;
-    props.location.id = dev;
-    cudaMemPool_t pool = nullptr;
-    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
-        cudaGetLastError();
-        pool = nullptr;
-    } else {
-        uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    }
-    g_pools[dev] = pool;
-    return pool;
-}
-
-// From the library's pool when it exists, else the device's default pool.
-cudaError_t pool_alloc(void **p, size_t bytes, int dev, cudaStream_t s) {
-    cudaMemPool_t pool = batched_pool(dev);
-    return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
-}
-
 std::mutex g_tune_mu;
 std::map<long long, int> g_tuned;  // (device, dpad, kpad) -> rows per thread
 

@@ -165,6 +165,9 @@ void launch_recheck(const F *X, int64_t n, int64_t d, const F *C, int64_t k, con
 
 // ---- assignment (tensor-core BF16x3 form, float32 data) ----------------------
 int64_t tc_dpad(int64_t d);   // d rounded up to the 64-wide K panel
+// Stream-ordered allocation from the library's memory pool of device `dev` (freed
+// memory is kept for reuse instead of going back to the driver at synchronisations).
+cudaError_t pool_alloc(void **p, size_t bytes, int dev, cudaStream_t s);
 int tc_tile_n(int64_t k);      // cluster tile of the tensor-core kernel: 128 or 256
 int64_t tc_kpad(int64_t k);   // k rounded up to a multiple of tc_tile_n(k)
 bool tc_supported(int64_t d); // dpad <= 256

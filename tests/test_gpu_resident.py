@@ -2,12 +2,14 @@
 
 Both compute every score h_j - x.c_j by FMAs in ascending feature order from zero,
 so their responses, distances and recheck queues are identical, bit for bit. The
-resident kernel (centroids held in shared memory, 64-row tiles taken in turn by
-two warp groups) applies to float rows with d a multiple of 4, d <= 256 and C^T
-within the shared-memory budget; KMB_PLAIN_RESIDENT=0 sends the same call to the
+resident kernel (centroids held in shared memory, all at once or in chunks, 64-row
+tiles taken in turn by two warp groups) applies to float rows with d a multiple of
+4 and at most 256 whose 256 clusters fit in shared memory next to the row stages; KMB_PLAIN_RESIDENT=0 sends the same call to the
 tiled kernel. The shapes cover row counts around the 64-row tile and the 128-row
 step of the two groups (one group without a tile, a CTA with one tile), several
-passes over 256 clusters, and grids that wrap over the SMs more than once.
+passes over 256 clusters, grids that wrap over the SMs more than once, and
+centroids taken in chunks when they do not all fit (one or two row stages per
+group, blocks of 4 or 8 tiles, up to 8 chunks).
 """
 import ctypes
 import os
@@ -34,7 +36,11 @@ def _infer(ctx, X, C):
 
 @pytest.mark.parametrize("n,d,k", [(1, 4, 40), (63, 64, 256), (64, 64, 256), (65, 64, 256), (127, 32, 100),
                                    (128, 64, 256), (129, 64, 256), (200, 96, 250), (4097, 64, 500),
-                                   (148 * 128 * 3 + 65, 64, 256), (50000, 40, 700), (30000, 48, 96)])
+                                   (148 * 128 * 3 + 65, 64, 256), (50000, 40, 700), (30000, 48, 96),
+                                   # clusters in chunks: one or two stages per group, 4 or 8 tiles per block
+                                   (1, 128, 1024), (65, 64, 1024), (3000, 128, 300), (5000, 128, 1024),
+                                   (4097, 64, 1024), (2000, 100, 700), (70000, 128, 256), (20000, 96, 2000),
+                                   (3000, 8, 5000)])
 def test_resident_equals_tiled(n, d, k):
     ctx = _native.context(0)
     g = torch.Generator(device="cuda").manual_seed(n * 7 + d + k)
