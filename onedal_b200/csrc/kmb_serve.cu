@@ -238,7 +238,7 @@ int launch_batch(Server *srv, Lane *lane) {
         const int cap = std::max(nreq, 2 * lane->cap);
         void *h = nullptr, *dv = nullptr;
         if (cudaMallocHost(&h, sizeof(kmb::serve::ReqDesc) * cap) != cudaSuccess ||
-            cudaMallocAsync(&dv, sizeof(kmb::serve::ReqDesc) * cap, s) != cudaSuccess) {
+            kmb::pool_alloc(&dv, sizeof(kmb::serve::ReqDesc) * cap, srv->device, s) != cudaSuccess) {
             cudaGetLastError();
             if (h) lane->retired_host.push_back(h);
             return KMB_ENOMEM;
@@ -272,7 +272,7 @@ int launch_batch(Server *srv, Lane *lane) {
     if (need > lane->arena_bytes) {
         const size_t bytes = std::max(need, 2 * lane->arena_bytes);
         void *a = nullptr;
-        if (cudaMallocAsync(&a, bytes, s) != cudaSuccess) {
+        if (kmb::pool_alloc(&a, bytes, srv->device, s) != cudaSuccess) {
             cudaGetLastError();
             return KMB_ENOMEM;
         }
@@ -411,14 +411,14 @@ cudaError_t copy_in_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyK
 // kmb_infer (BF16x3, FP64 recheck) over row chunks on the worker's stream.
 // The request's rows and labels live in the worker's arena, grown (stream-ordered,
 // geometrically) only when a request needs more.
-int run_tc_request(kmb_context *ctx, cudaStream_t s, const Model &m, Request *r, int64_t chunk_rows, void *&arena,
-                   size_t &arena_bytes) {
+int run_tc_request(kmb_context *ctx, int dev, cudaStream_t s, const Model &m, Request *r, int64_t chunk_rows,
+                   void *&arena, size_t &arena_bytes) {
     const size_t xbytes = (sizeof(float) * r->n * r->d + 255) / 256 * 256;
     const size_t need = xbytes + sizeof(int32_t) * r->n;
     if (need > arena_bytes) {
         void *a = nullptr;
         const size_t bytes = std::max(need, 2 * arena_bytes);
-        if (cudaMallocAsync(&a, bytes, s) != cudaSuccess) {
+        if (kmb::pool_alloc(&a, bytes, dev, s) != cudaSuccess) {
             cudaGetLastError();
             return KMB_ENOMEM;
         }
@@ -495,7 +495,7 @@ void tc_worker_loop(Server *srv) {
         srv->tc_busy += 1;
         const Model m = srv->models[r->model];
         lock.unlock();
-        const int rc = ctx ? run_tc_request(ctx, ts, m, r, srv->tc_chunk_rows, arena, arena_bytes) : KMB_ECUDA;
+        const int rc = ctx ? run_tc_request(ctx, srv->device, ts, m, r, srv->tc_chunk_rows, arena, arena_bytes) : KMB_ECUDA;
         lock.lock();
         r->rc = rc;
         r->t_done = Clock::now();
@@ -622,11 +622,23 @@ int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32
     if (const char *e = std::getenv("KMB_SERVER_TC_CHUNK_ROWS"))
         srv->tc_chunk_rows = std::min<int64_t>(std::max<int64_t>(atoll(e), 4096), kTcChunkRows);
     if (const char *e = std::getenv("KMB_SERVER_TC_WORKERS")) srv->tc_workers = std::min(std::max(atoi(e), 1), 8);
-    // Keep freed request memory in the stream-ordered pool instead of returning it to the driver.
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-        uint64_t thr = (uint64_t)hbm_budget_bytes;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    // Request memory (lane and worker arenas, worker and trainer workspaces) comes
+    // from the library's stream-ordered pool, which keeps what is freed. Growing that
+    // pool maps fresh device memory, which stalled every stream of the device for
+    // 70-250 ms when a large request first needed it mid-stream; so the pool is
+    // grown here, once, by min(budget, 16 GiB) (KMB_SERVER_RESERVE_BYTES overrides),
+    // allocated and freed before any request runs.
+    {
+        size_t reserve = std::min<size_t>(srv->budget, (size_t)16 << 30);
+        if (const char *e = std::getenv("KMB_SERVER_RESERVE_BYTES")) reserve = std::min<size_t>(srv->budget, (size_t)atoll(e));
+        cudaStream_t rs = nullptr;
+        void *block = nullptr;
+        if (reserve > 0 && cudaStreamCreateWithFlags(&rs, cudaStreamNonBlocking) == cudaSuccess) {
+            if (kmb::pool_alloc(&block, reserve, device, rs) == cudaSuccess) cudaFreeAsync(block, rs);
+            cudaGetLastError();  // a failed reservation only means later growth
+            cudaStreamSynchronize(rs);
+            cudaStreamDestroy(rs);
+        }
     }
     cudaDeviceGetStreamPriorityRange(&srv->prio_low, &srv->prio_high);
     for (int i = 0; i < lanes; ++i) {
