@@ -457,30 +457,25 @@ __device__ __forceinline__ void scan_chunk(const float (&w)[32], int colbase, fl
 // (value, index) order; indices kept for the first two places.
 __device__ __forceinline__ bool lex_lt(float a, int ia, float b, int ib) { return a < b || (a == b && ia < ib); }
 
+// Merge of two sorted triples by selects (no indexed arrays, so no local memory):
+// the same comparisons, in the same argument order, as a two-list merge of three
+// outputs; a third place carries no index.
 __device__ __forceinline__ Top3 top3_merge(const Top3 &x, const Top3 &y) {
-    const float xv[3] = {x.b, x.s, x.t}, yv[3] = {y.b, y.s, y.t};
-    const int xi[3] = {x.ib, x.is, 0x7fffffff}, yi[3] = {y.ib, y.is, 0x7fffffff};
-    float ov[3];
-    int oi[3];
-    int a = 0, b = 0;
-#pragma unroll
-    for (int o = 0; o < 3; ++o) {  // a + b == o <= 2, so a, b < 3
-        if (lex_lt(xv[a], xi[a], yv[b], yi[b])) {
-            ov[o] = xv[a];
-            oi[o] = xi[a];
-            ++a;
-        } else {
-            ov[o] = yv[b];
-            oi[o] = yi[b];
-            ++b;
-        }
-    }
+    constexpr int kNone = 0x7fffffff;
+    const bool c0 = lex_lt(x.b, x.ib, y.b, y.ib);
+    const float xa = c0 ? x.s : x.b, ya = c0 ? y.b : y.s;
+    const int xai = c0 ? x.is : x.ib, yai = c0 ? y.ib : y.is;
+    const bool c1 = lex_lt(xa, xai, ya, yai);
+    const bool xx = c0 && c1, yy = !c0 && !c1;
+    const float xh = xx ? x.t : (yy ? x.b : x.s), yh = xx ? y.b : (yy ? y.t : y.s);
+    const int xhi = xx ? kNone : (yy ? x.ib : x.is), yhi = xx ? y.ib : (yy ? kNone : y.is);
+    const bool c2 = lex_lt(xh, xhi, yh, yhi);
     Top3 r;
-    r.b = ov[0];
-    r.s = ov[1];
-    r.t = ov[2];
-    r.ib = oi[0];
-    r.is = oi[1];
+    r.b = c0 ? x.b : y.b;
+    r.ib = c0 ? x.ib : y.ib;
+    r.s = c1 ? xa : ya;
+    r.is = c1 ? xai : yai;
+    r.t = c2 ? xh : yh;
     return r;
 }
 

@@ -114,6 +114,7 @@ struct Lane;
 struct Server {
     int device = 0;
     int64_t tc_chunk_rows = kTcChunkRows;  // KMB_SERVER_TC_CHUNK_ROWS (4096 .. kTcChunkRows)
+    int tc_sms = -1;                       // KMB_SERVER_TC_SMS: the workers' kmb_context_set_max_sms
     int tc_workers = kTcWorkers;
     size_t budget = 0;
     size_t in_use = 0, peak_in_use = 0;
@@ -473,7 +474,7 @@ void tc_worker_loop(Server *srv) {
     // starve the persistent CTAs (which need whole SMs) for tens of ms.
     if (ctx && cudaStreamCreateWithPriority(&ts, cudaStreamNonBlocking, srv->prio_high) == cudaSuccess) {
         kmb_context_set_stream(ctx, ts);
-        kmb_context_set_max_sms(ctx, -1);
+        kmb_context_set_max_sms(ctx, srv->tc_sms);
     } else if (ctx) {
         kmb_context_destroy(ctx);
         ctx = nullptr;
@@ -622,6 +623,7 @@ int kmb_server_create(int device, int64_t hbm_budget_bytes, int32_t lanes, int32
     if (const char *e = std::getenv("KMB_SERVER_TC_CHUNK_ROWS"))
         srv->tc_chunk_rows = std::min<int64_t>(std::max<int64_t>(atoll(e), 4096), kTcChunkRows);
     if (const char *e = std::getenv("KMB_SERVER_TC_WORKERS")) srv->tc_workers = std::min(std::max(atoi(e), 1), 8);
+    if (const char *e = std::getenv("KMB_SERVER_TC_SMS")) srv->tc_sms = std::max(atoi(e), -1);
     // Request memory (lane and worker arenas, worker and trainer workspaces) comes
     // from the library's stream-ordered pool, which keeps what is freed. Growing that
     // pool maps fresh device memory, which stalled every stream of the device for
