@@ -234,3 +234,20 @@ def test_csr_sparse_blobs_without_initial_centroids(dt, k, n, d):
     assert np.array_equal(r.get_model().get_centroids(), r2.get_model().get_centroids())
     _, lo, _, ito = restated.train_csr(M.data, M.indices, M.indptr, d, C0, 30, 0.01)
     assert (r.get_responses().ravel() == lo).all() and r.get_iteration_count() == ito
+
+
+@pytest.mark.parametrize("k,n,d", [(16, 20000, 160), (128, 20000, 1024)])
+def test_csr_float_centroids_equal_dense_bit_for_bit(k, n, d):
+    """Float values: the CSR update sums the stored entries as the same exact integers
+    as the dense rows' update (column scales from the largest |x|, an unstored entry
+    adds zero), so with equal responses the centroids are the same floats, bit for
+    bit, in full passes and in passes that apply only the moved rows."""
+    M, truth = _sparse_blobs(n, d, k, 11 + k, np.float32)
+    first = np.array([np.flatnonzero(truth == j)[0] for j in range(k)])
+    C0 = M[first].toarray()
+    rc = kmeans.train(_desc(np.float32, k, 6), kmeans.csr_table.from_scipy(M), C0)
+    rd = kmeans.train(kmeans.descriptor(np.float32).set_cluster_count(k).set_max_iteration_count(6)
+                      .set_accuracy_threshold(0.0), M.toarray(), C0)
+    assert (rc.get_responses() == rd.get_responses()).all()
+    assert rc.get_iteration_count() == rd.get_iteration_count()
+    assert np.array_equal(rc.get_model().get_centroids(), rd.get_model().get_centroids())
