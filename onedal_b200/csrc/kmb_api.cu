@@ -784,6 +784,34 @@ void csr_assign_pass(kmb_context *ctx, const kmb::CsrRows &X, const F *C, int64_
     kmb::launch_csr_assign<F>(X, (const F *)ws.Ct.ptr, (const F *)ws.h.ptr, k, kpad, labels, d2, st, s);
 }
 
+// The CSR update: float values take the exact update (integer cluster sums from the
+// stored entries, moved rows only once few rows move), double values the FP64 one.
+template <typename F>
+bool csr_update_buffers(kmb::Workspace &ws, const kmb::UpdatePlan &plan, int64_t n, int64_t k, int64_t d) {
+    return kmb::ensure_update_buffers(ws, plan, sizeof(F));
+}
+template <>
+bool csr_update_buffers<float>(kmb::Workspace &ws, const kmb::UpdatePlan &plan, int64_t n, int64_t k, int64_t d) {
+    return kmb::ensure_update_buffers(ws, plan, sizeof(float), /*fp64_records=*/false) &&
+           kmb::ensure_exact_buffers(ws, n, k, d, /*piece_records=*/false);
+}
+template <typename F>
+void csr_prepare_update(const kmb::CsrRows &, kmb::Workspace &, LoopState *, cudaStream_t) {}
+template <>
+void csr_prepare_update<float>(const kmb::CsrRows &X, kmb::Workspace &ws, LoopState *st, cudaStream_t s) {
+    kmb::prepare_exact_update_csr(X, ws, st, s);
+}
+template <typename F>
+void csr_update_pass(const kmb::CsrRows &X, const kmb::UpdatePlan &plan, int32_t *labels, F *d2, F *C_old, F *C_new,
+                     kmb::Workspace &ws, LoopState *st, cudaStream_t s) {
+    kmb::launch_update<F>(nullptr, plan, labels, d2, C_old, C_new, ws, st, /*commit=*/true, s, &X);
+}
+template <>
+void csr_update_pass<float>(const kmb::CsrRows &X, const kmb::UpdatePlan &plan, int32_t *labels, float *d2,
+                            float *C_old, float *C_new, kmb::Workspace &ws, LoopState *st, cudaStream_t s) {
+    kmb::launch_update_exact_csr(X, plan, labels, d2, C_old, C_new, ws, st, /*commit=*/true, s);
+}
+
 template <typename F>
 int train_csr_impl(kmb_context *ctx, int memory, const void *vals, const int64_t *cols, const int64_t *rowptr,
                    int64_t n, int64_t d, int base, const void *C0v, const kmb_params *p, void *C_out,
@@ -792,7 +820,7 @@ int train_csr_impl(kmb_context *ctx, int memory, const void *vals, const int64_t
     int rc = ensure_common<F>(ctx, n, d, k, false, false);
     if (rc) return rc;
     kmb::UpdatePlan plan = kmb::make_update_plan(n, k, d);
-    if (!kmb::ensure_update_buffers(ctx->ws, plan, sizeof(F)) || !ctx->ws.ensure(ctx->ws.csr_cnorm, sizeof(double) * k))
+    if (!csr_update_buffers<F>(ctx->ws, plan, n, k, d) || !ctx->ws.ensure(ctx->ws.csr_cnorm, sizeof(double) * k))
         return fail(ctx, KMB_ENOMEM, "update buffers");
     kmb::CsrRows X;
     if ((rc = prepare_csr<F>(ctx, memory, vals, cols, rowptr, n, d, base, &X))) return rc;
@@ -810,13 +838,14 @@ int train_csr_impl(kmb_context *ctx, int memory, const void *vals, const int64_t
     KMB_CUDA(cudaMemsetAsync(sc, 0, sizeof(kmb::DevScalars), s));
     KMB_CUDA(cudaMemcpyAsync(Ccur, C0, sizeof(F) * k * d, cudaMemcpyDeviceToDevice, s));
     const int64_t T = p->max_iteration_count;
+    if (T > 0) csr_prepare_update<F>(X, ws, st, s);
     int64_t enq = 0, batch = 2;
     while (enq < T) {
         const int64_t upto = std::min(T, enq + batch);
         for (; enq < upto; ++enq) {
             csr_assign_pass<F>(ctx, X, Ccur, k, labels, d2, st);
             KernelTimer timer(ctx, 2);
-            kmb::launch_update<F>(nullptr, plan, labels, d2, Ccur, Cnew, ws, st, /*commit=*/true, s, &X);
+            csr_update_pass<F>(X, plan, labels, d2, Ccur, Cnew, ws, st, s);
         }
         KMB_CUDA(cudaGetLastError());
         if (enq < T) {

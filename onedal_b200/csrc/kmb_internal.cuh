@@ -230,7 +230,8 @@ void launch_csr_objective(const CsrRows &X, const F *C, int64_t k, const int32_t
 // ---- update ----------------------------------------------------------------
 UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d);
 // Sizes the update buffers of `ws` for plan `p` (false on allocation failure).
-bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize);
+// fp64_records false: no FP64 piece records (an update that never sums pieces in FP64).
+bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize, bool fp64_records = true);
 
 // One Lloyd update: counting-sort the rows by label (stable, so each cluster's
 // rows are summed in row order), FP64 sums per fixed piece of rows, centroid =
@@ -329,7 +330,14 @@ __device__ __forceinline__ double u128_to_double(unsigned __int128 m) {
 // full counting-sort pass over X; the result is bit for bit the same.
 // prepare_exact_update: once per call (the scales; the next update recomputes).
 void prepare_exact_update(const float *X, int64_t n, int64_t d, Workspace &ws, LoopState *st, cudaStream_t s);
-bool ensure_exact_buffers(Workspace &ws, int64_t n, int64_t k, int64_t d);
+// piece_records: the dense rows' full passes sum per-piece records (the CSR form
+// accumulates into the maintained sums instead and needs none).
+bool ensure_exact_buffers(Workspace &ws, int64_t n, int64_t k, int64_t d, bool piece_records = true);
+// CSR rows with float values: column scales from the stored entries, and the
+// exact update (the dense rows' integers, accumulated by atomics).
+void prepare_exact_update_csr(const CsrRows &X, Workspace &ws, LoopState *st, cudaStream_t s);
+void launch_update_exact_csr(const CsrRows &X, const UpdatePlan &p, int32_t *labels, const float *d2, float *C_old,
+                             float *C_new, Workspace &ws, LoopState *st, bool commit, cudaStream_t s);
 void launch_update_exact(const float *X, const UpdatePlan &p, int32_t *labels, const float *d2, float *C_old,
                          float *C_new, Workspace &ws, LoopState *st, bool commit, cudaStream_t s, float *exact_d2);
 

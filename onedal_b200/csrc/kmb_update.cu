@@ -1076,7 +1076,8 @@ __global__ void copy_prev_kernel(const int32_t *__restrict__ labels, int32_t *__
         prev[r] = labels[r];
 }
 
-// Block (j, tile): cluster j's limb sums (full mode: from its pieces; incremental:
+// Block (j, tile): cluster j's limb sums (full mode: from its pieces; incremental, or
+// from_acc:
 // the maintained ones), normalised and kept; c = F(S * 2^-E / count) in FP64; the
 // tile's shift part and the empty flag, as finalize_kernel.
 __global__ void __launch_bounds__(kFinalizeCols)
@@ -1084,12 +1085,14 @@ finalize_exact_kernel(const long long *__restrict__ records, int64_t max_pieces,
                       const int64_t *__restrict__ piece_base, const int *__restrict__ colexp, int k,
                       long long *__restrict__ lacc, long long *__restrict__ cnt, const float *__restrict__ C_old,
                       float *__restrict__ C_new, int d, double *__restrict__ shift_tiles,
-                      int32_t *__restrict__ empty_flag, const LoopState *st) {
+                      int32_t *__restrict__ empty_flag, const LoopState *st, bool from_acc = false) {
     if (is_done(st)) return;
     __shared__ double red[kFinalizeCols / 32];
     const int j = blockIdx.x;
     const int t = blockIdx.y * kFinalizeCols + threadIdx.x;
-    const bool full = st->upd_mode == 0;
+    // from_acc: the maintained limb sums and counts hold this pass's sums in both
+    // modes (the CSR form accumulates full passes there too)
+    const bool full = !from_acc && st->upd_mode == 0;
     const long long c_j = full ? (long long)counts_sort[j] : cnt[j];
     double acc = 0.0;
     if (t < d) {
@@ -1136,6 +1139,136 @@ finalize_exact_kernel(const long long *__restrict__ records, int64_t max_pieces,
     }
 }
 
+// ---- exact update of CSR rows with float values ------------------------------
+// The same integers as the dense rows' exact update, from the stored entries (an
+// unstored entry is a zero and adds nothing): the column scales come from the
+// columns' largest stored |x|, which is the column's largest |x|. The sums are kept
+// in the maintained limb planes and counts in both modes: a full pass clears them
+// and adds every row's entries by integer atomics (exact in any order), an
+// incremental pass moves the moved rows' entries from the old cluster to the new.
+
+// colbits[t] <- max |x| over the stored entries of column t, as float bits.
+__global__ void csr_colmax_kernel(const float *__restrict__ vals, const int32_t *__restrict__ cols, int64_t nnz,
+                                  int d, bool in_smem, unsigned *__restrict__ colbits) {
+    extern __shared__ unsigned smax[];
+    if (in_smem) {
+        for (int t = threadIdx.x; t < d; t += blockDim.x) smax[t] = 0u;
+        __syncthreads();
+    }
+    for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < nnz; x += (int64_t)gridDim.x * blockDim.x) {
+        const float v = fabsf(vals[x]);
+        if (v > 0.0f) atomicMax(in_smem ? &smax[cols[x]] : &colbits[cols[x]], __float_as_uint(v));
+    }
+    if (in_smem) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < d; t += blockDim.x)
+            if (smax[t]) atomicMax(&colbits[t], smax[t]);
+    }
+}
+
+// Full mode: limb planes and counts cleared.
+__global__ void csr_exact_clear_kernel(long long *__restrict__ acc, int64_t words, long long *__restrict__ cnt, int k,
+                                       const LoopState *st) {
+    if (is_done(st) || st->upd_mode != 0) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (int64_t)gridDim.x * blockDim.x)
+        acc[i] = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < k; i += (int64_t)gridDim.x * blockDim.x)
+        cnt[i] = 0;
+}
+
+// Full mode: one warp per row adds the row's stored entries to its cluster's limb
+// sums; the CTA counts its rows per cluster in shared memory (k <= kCsrCountSmem)
+// before one atomic per cluster.
+constexpr int kCsrCountSmem = 8192;
+__global__ void __launch_bounds__(256) csr_sums_fixed_kernel(const float *__restrict__ vals,
+                                                             const int32_t *__restrict__ cols,
+                                                             const int64_t *__restrict__ rowptr, int64_t n, int d,
+                                                             int k, const int32_t *__restrict__ labels,
+                                                             const int *__restrict__ colexp,
+                                                             unsigned long long *__restrict__ acc,
+                                                             unsigned long long *__restrict__ cnt, const LoopState *st) {
+    if (is_done(st) || st->upd_mode != 0) return;
+    extern __shared__ unsigned scnt[];
+    const bool shared_counts = k <= kCsrCountSmem;
+    if (shared_counts) {
+        for (int j = threadIdx.x; j < k; j += blockDim.x) scnt[j] = 0u;
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
+    const int64_t plane = (int64_t)k * d;
+    for (int64_t r = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); r < n; r += warps) {
+        const int lab = labels[r];
+        if ((unsigned)lab >= (unsigned)k) continue;  // cannot happen: the assignment writes every row
+        const int64_t base = (int64_t)lab * d;
+        for (int64_t x = rowptr[r] + lane; x < rowptr[r + 1]; x += 32) {
+            const int c = cols[x];
+            const Limbs L = fixed_of(vals[x], colexp[c]);
+            if (L.l0 | L.l1 | L.l2) {
+                atomicAdd(&acc[base + c], (unsigned long long)L.l0);
+                atomicAdd(&acc[plane + base + c], (unsigned long long)L.l1);
+                atomicAdd(&acc[2 * plane + base + c], (unsigned long long)L.l2);
+            }
+        }
+        if (lane == 0) {
+            if (shared_counts) atomicAdd(&scnt[lab], 1u);
+            else atomicAdd(&cnt[lab], 1ull);
+        }
+    }
+    if (shared_counts) {
+        __syncthreads();
+        for (int j = threadIdx.x; j < k; j += blockDim.x)
+            if (scnt[j]) atomicAdd(&cnt[j], (unsigned long long)scnt[j]);
+    }
+}
+
+// Incremental mode: the moved rows' entries leave the old cluster's sums and join
+// the new one's (a warp walks 32 rows, then each moved row's entries); prev follows
+// the labels.
+__global__ void csr_apply_moves_kernel(const float *__restrict__ vals, const int32_t *__restrict__ cols,
+                                       const int64_t *__restrict__ rowptr, int64_t n, int d, int k,
+                                       const int32_t *__restrict__ labels, int32_t *__restrict__ prev,
+                                       const int *__restrict__ colexp, unsigned long long *__restrict__ acc,
+                                       unsigned long long *__restrict__ cnt, const LoopState *st) {
+    if (is_done(st) || st->upd_mode != 1) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t plane = (int64_t)k * d;
+    for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) & ~(int64_t)31; base < n; base += stride) {
+        const int64_t r = base + lane;
+        int lab = -1, old = -1;
+        if (r < n) {
+            lab = labels[r];
+            old = prev[r];
+        }
+        unsigned moved = __ballot_sync(0xffffffffu, r < n && lab != old);
+        while (moved) {
+            const int src = __ffs(moved) - 1;
+            moved &= moved - 1;
+            const int64_t row = base + src;
+            const int nl = __shfl_sync(0xffffffffu, lab, src), ol = __shfl_sync(0xffffffffu, old, src);
+            for (int64_t x = rowptr[row] + lane; x < rowptr[row + 1]; x += 32) {
+                const int c = cols[x];
+                const Limbs L = fixed_of(vals[x], colexp[c]);
+                if (L.l0 | L.l1 | L.l2) {
+                    const int64_t in = (int64_t)nl * d + c, out = (int64_t)ol * d + c;
+                    atomicAdd(&acc[in], (unsigned long long)L.l0);
+                    atomicAdd(&acc[plane + in], (unsigned long long)L.l1);
+                    atomicAdd(&acc[2 * plane + in], (unsigned long long)L.l2);
+                    atomicAdd(&acc[out], (unsigned long long)-L.l0);
+                    atomicAdd(&acc[plane + out], (unsigned long long)-L.l1);
+                    atomicAdd(&acc[2 * plane + out], (unsigned long long)-L.l2);
+                }
+            }
+            if (lane == 0) {
+                atomicAdd(&cnt[nl], 1ull);
+                atomicAdd(&cnt[ol], (unsigned long long)-1ll);
+            }
+        }
+        if (r < n && lab != old) prev[r] = lab;
+    }
+}
+
 // After the update: the maintained state describes this pass's labels.
 __global__ void exact_valid_kernel(LoopState *st) {
     if (is_done(st)) return;
@@ -1161,7 +1294,7 @@ UpdatePlan make_update_plan(int64_t n, int64_t k, int64_t d) {
     return p;
 }
 
-bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize) {
+bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize, bool fp64_records) {
     const int64_t n_groups = (p.n_chunks + kGroupChunks - 1) / kGroupChunks;
     bool ok = true;
     ok &= ws.ensure(ws.H, sizeof(int32_t) * std::max<int64_t>(1, p.n_chunks * p.k));
@@ -1170,7 +1303,7 @@ bool ensure_update_buffers(Workspace &ws, const UpdatePlan &p, size_t fsize) {
     ok &= ws.ensure(ws.offsets, sizeof(int64_t) * (p.k + 1));
     ok &= ws.ensure(ws.piece_base, sizeof(int64_t) * (p.k + 1));
     ok &= ws.ensure(ws.perm, sizeof(int32_t) * std::max<int64_t>(1, p.n));
-    ok &= ws.ensure(ws.records, sizeof(double) * p.max_pieces * p.d);
+    if (fp64_records) ok &= ws.ensure(ws.records, sizeof(double) * p.max_pieces * p.d);
     ok &= ws.ensure(ws.shift_part, sizeof(double) * p.k);
     ok &= ws.ensure(ws.shift_tiles, sizeof(double) * p.k * ((p.d + kFinalizeCols - 1) / kFinalizeCols));
     ok &= ws.ensure(ws.empty_flag, sizeof(int32_t) * p.k);
@@ -1314,10 +1447,10 @@ void launch_update(const F *X, const UpdatePlan &p, const int32_t *labels, const
     reseed_and_commit<F>(X, p, labels, d2, exact_d2, C_old, C_new, ws, st, commit, s, csr);
 }
 
-bool ensure_exact_buffers(Workspace &ws, int64_t n, int64_t k, int64_t d) {
+bool ensure_exact_buffers(Workspace &ws, int64_t n, int64_t k, int64_t d, bool piece_records) {
     bool ok = true;
     ok &= ws.ensure(ws.ex_acc, sizeof(long long) * 3 * k * d);
-    ok &= ws.ensure(ws.ex_records, sizeof(long long) * 3 * (n / kPieceRows + k + 1) * d);
+    if (piece_records) ok &= ws.ensure(ws.ex_records, sizeof(long long) * 3 * (n / kPieceRows + k + 1) * d);
     ok &= ws.ensure(ws.ex_cnt, sizeof(long long) * k);
     ok &= ws.ensure(ws.ex_prev, sizeof(int32_t) * std::max<int64_t>(1, n));
     ok &= ws.ensure(ws.ex_colexp, sizeof(int) * d);
@@ -1428,6 +1561,64 @@ void launch_update_exact(const float *X, const UpdatePlan &p, int32_t *labels, c
     empties_kernel<<<1, 1024, 0, s>>>(empty_flag, k, empty_ids, shift_part, st);
     KMB_LAUNCHED();
     reseed_and_commit<float>(X, p, labels, exact_d2 ? exact_d2 : d2, exact_d2, C_old, C_new, ws, st, commit, s);
+}
+
+void prepare_exact_update_csr(const CsrRows &X, Workspace &ws, LoopState *st, cudaStream_t s) {
+    int *colexp = (int *)ws.ex_colexp.ptr;
+    const int d = (int)X.d;
+    cudaMemsetAsync(colexp, 0, sizeof(int) * d, s);
+    const bool in_smem = (size_t)d * sizeof(unsigned) <= (size_t)96 * 1024;
+    const size_t smem = in_smem ? sizeof(unsigned) * d : 0;
+    if (in_smem) cudaFuncSetAttribute(csr_colmax_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const unsigned blocks =
+        (unsigned)std::max<int64_t>(1, std::min<int64_t>((X.nnz + 255) / 256, in_smem ? 148 * 2 : 148 * 8));
+    csr_colmax_kernel<<<blocks, 256, smem, s>>>((const float *)X.vals, X.cols, X.nnz, d, in_smem, (unsigned *)colexp);
+    KMB_LAUNCHED();
+    colexp_kernel<<<(unsigned)((d + 255) / 256), 256, 0, s>>>(colexp, d, st);
+    KMB_LAUNCHED();
+}
+
+void launch_update_exact_csr(const CsrRows &X, const UpdatePlan &p, int32_t *labels, const float *d2, float *C_old,
+                             float *C_new, Workspace &ws, LoopState *st, bool commit, cudaStream_t s) {
+    const int k = (int)p.k, d = (int)p.d;
+    int32_t *prev = (int32_t *)ws.ex_prev.ptr;
+    const int *colexp = (const int *)ws.ex_colexp.ptr;
+    long long *acc = (long long *)ws.ex_acc.ptr;
+    long long *cnt = (long long *)ws.ex_cnt.ptr;
+    const unsigned rb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((p.n + 255) / 256, 148 * 8));
+    count_moved_kernel<<<rb, 256, 0, s>>>(labels, prev, p.n, st);
+    KMB_LAUNCHED();
+    choose_mode_kernel<<<1, 1, 0, s>>>(p.n, st);
+    KMB_LAUNCHED();
+    // full mode: clear, then every row's entries (each kernel returns at once otherwise)
+    csr_exact_clear_kernel<<<148 * 8, 256, 0, s>>>(acc, 3 * (int64_t)k * d, cnt, k, st);
+    KMB_LAUNCHED();
+    const size_t cs = k <= kCsrCountSmem ? sizeof(unsigned) * k : 0;
+    csr_sums_fixed_kernel<<<148 * 8, 256, cs, s>>>((const float *)X.vals, X.cols, X.rowptr, p.n, d, k, labels, colexp,
+                                                   (unsigned long long *)acc, (unsigned long long *)cnt, st);
+    KMB_LAUNCHED();
+    // incremental mode: the moved rows
+    csr_apply_moves_kernel<<<rb, 256, 0, s>>>((const float *)X.vals, X.cols, X.rowptr, p.n, d, k, labels, prev, colexp,
+                                              (unsigned long long *)acc, (unsigned long long *)cnt, st);
+    KMB_LAUNCHED();
+    int32_t *empty_flag = (int32_t *)ws.empty_flag.ptr;
+    int32_t *empty_ids = (int32_t *)ws.empty_ids.ptr;
+    double *shift_part = (double *)ws.shift_part.ptr;
+    const int tiles = (d + kFinalizeCols - 1) / kFinalizeCols;
+    finalize_exact_kernel<<<dim3((unsigned)k, (unsigned)tiles), kFinalizeCols, 0, s>>>(
+        nullptr, 0, nullptr, nullptr, colexp, k, acc, cnt, C_old, C_new, d, (double *)ws.shift_tiles.ptr, empty_flag,
+        st, /*from_acc=*/true);
+    KMB_LAUNCHED();
+    copy_prev_kernel<<<rb, 256, 0, s>>>(labels, prev, p.n, st);
+    KMB_LAUNCHED();
+    exact_valid_kernel<<<1, 1, 0, s>>>(st);
+    KMB_LAUNCHED();
+    shift_tiles_kernel<<<(unsigned)std::min(148, (k + 255) / 256), 256, 0, s>>>((const double *)ws.shift_tiles.ptr, k,
+                                                                              tiles, shift_part, st);
+    KMB_LAUNCHED();
+    empties_kernel<<<1, 1024, 0, s>>>(empty_flag, k, empty_ids, shift_part, st);
+    KMB_LAUNCHED();
+    reseed_and_commit<float>(nullptr, p, labels, d2, nullptr, C_old, C_new, ws, st, commit, s, &X);
 }
 
 template <typename F>
