@@ -16,9 +16,13 @@
 //                             rows are still in L2): every value as three 32-bit
 //                             limbs (the Lloyd loop's exact update,
 //                             kmb_internal.cuh), summed per label-sorted row list,
-//                             then added to the problem's int64 limb sums
+//                             then added to the problem's int64 limb sums -- or,
+//                             once at most n/16 rows moved in the previous
+//                             iteration, only the moved rows, taken out of their
+//                             old cluster's sums and added to the new one's
+//                             (integer atomics: the same sums in any order)
 //   finalize    (problem, cluster)   c = F(S / count) from the 128-bit sum, shift
-//                                    part, sums cleared for the next iteration
+//                                    part (the sums are kept, normalised)
 //   decide      (problem)            empty clusters reseeded with the farthest rows
 //                                    (squared distance descending, row ascending;
 //                                    empty clusters ascending), shift, stop test
@@ -60,13 +64,16 @@ struct Problem {
     int32_t *labels;
     float *d2;
     float *xnorm;
-    long long *acc;     // 3 limb planes of k x d
-    int *counts;        // k
+    long long *acc;     // 3 limb planes of k x d (kept across iterations)
+    int *counts;        // k (kept across iterations)
+    int32_t *prev;      // n: the labels the sums describe (-1 before the first pass)
     double *shift_part; // k
     int *colexp;        // d (column maxima as float bits during setup, then E_t)
     long long n;
     int d, dpad, k, kpad, tm;
     int done, iters, max_iters, empty_events;
+    int inc;            // this iteration's accumulation: 0 every row, 1 the moved rows only
+    long long moved;    // rows whose label changed in this iteration's work phase
     double eps, shift;
 };
 
@@ -219,7 +226,10 @@ __device__ void setup_item(Problem &p, int blk, float *smax) {
             if (a > 0.f) atomicMax(reinterpret_cast<unsigned *>(&smax[t]), __float_as_uint(a));
         }
         for (int m = 16; m >= 1; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
-        if (lane == 0) p.xnorm[r] = (float)s;
+        if (lane == 0) {
+            p.xnorm[r] = (float)s;
+            p.prev[r] = -1;
+        }
     }
     __syncthreads();
     for (int t = threadIdx.x; t < p.d; t += NT) {
@@ -252,6 +262,16 @@ __device__ void scales_item(Problem &p) {
 // v takes features v, v + 128, ...; four warp butterflies; warps added in order),
 // so it equals the single-problem path's half norm bit for bit.
 __device__ void prep_item(Problem &p, int j, int lane) {
+    if (!p.inc && j < p.k) {  // a full accumulation follows: cluster j's sums and count start at zero
+        const long long plane = (long long)p.k * p.d;
+        for (int t = lane; t < p.d; t += 32) {
+            const long long g = (long long)j * p.d + t;
+            p.acc[g] = 0;
+            p.acc[plane + g] = 0;
+            p.acc[2 * plane + g] = 0;
+        }
+        if (lane == 0) p.counts[j] = 0;
+    }
     for (int t = lane; t < p.dpad; t += 32) {
         const float v = (j < p.k && t < p.d) ? p.C[(long long)j * p.d + t] : 0.f;
         p.Ct[(long long)t * p.kpad + j] = v;
@@ -586,6 +606,74 @@ __device__ void accumulate_item(Problem &p, int blk, int *sm, GridBarrier *gb) {
     __syncthreads();
 }
 
+// Full accumulation's bookkeeping: the block's rows that changed label, and prev.
+__device__ void track_item(Problem &p, int blk) {
+    const long long b = (long long)blk * kAccRows, e = min(p.n, b + kAccRows);
+    int c = 0;
+    for (long long r = b + threadIdx.x; r < e; r += NT) {
+        const int lab = p.labels[r];
+        c += lab != p.prev[r];
+        p.prev[r] = lab;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(reinterpret_cast<unsigned long long *>(&p.moved), (unsigned long long)c);
+}
+
+// Moved-rows accumulation of a block: a warp walks 32 rows; each moved row's values
+// leave the old cluster's limb sums and join the new one's (integer atomics, exact
+// in any order), counts follow, prev follows the labels.
+__device__ void moves_item(Problem &p, int blk, GridBarrier *gb) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long b = (long long)blk * kAccRows, e = min(p.n, b + kAccRows);
+    const int k = p.k, d = p.d;
+    const long long plane = (long long)k * d;
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(p.acc);
+    int moved = 0;
+    for (long long base = b + 32 * warp; base < e; base += NT) {  // warp-uniform trip count
+        const long long r = base + lane;
+        int lab = -1, old = -1;
+        if (r < e) {
+            lab = p.labels[r];
+            old = p.prev[r];
+            if ((unsigned)lab >= (unsigned)k || (unsigned)old >= (unsigned)k) {  // cannot happen
+                atomicExch(&gb->error, 2);
+                lab = old;
+            }
+        }
+        unsigned mv = __ballot_sync(0xffffffffu, r < e && lab != old);
+        moved += __popc(mv);
+        while (mv) {
+            const int src = __ffs(mv) - 1;
+            mv &= mv - 1;
+            const long long row = base + src;
+            const int nl = __shfl_sync(0xffffffffu, lab, src), ol = __shfl_sync(0xffffffffu, old, src);
+            const float *x = p.X + row * d;
+            for (int t = lane; t < d; t += 32) {
+                const Limbs L = fixed_of(x[t], p.colexp[t]);
+                const long long in = (long long)nl * d + t, out = (long long)ol * d + t;
+                if (L.l0) {
+                    atomicAdd(&acc[in], (unsigned long long)L.l0);
+                    atomicAdd(&acc[out], (unsigned long long)-L.l0);
+                }
+                if (L.l1) {
+                    atomicAdd(&acc[plane + in], (unsigned long long)L.l1);
+                    atomicAdd(&acc[plane + out], (unsigned long long)-L.l1);
+                }
+                if (L.l2) {
+                    atomicAdd(&acc[2 * plane + in], (unsigned long long)L.l2);
+                    atomicAdd(&acc[2 * plane + out], (unsigned long long)-L.l2);
+                }
+            }
+            if (lane == 0) {
+                atomicAdd(&p.counts[nl], 1);
+                atomicSub(&p.counts[ol], 1);
+            }
+        }
+        if (r < e && lab != old) p.prev[r] = lab;
+    }
+    if (lane == 0 && moved) atomicAdd(reinterpret_cast<unsigned long long *>(&p.moved), (unsigned long long)moved);
+}
+
 // ---- finalize: one warp per (problem, cluster) ---------------------------------
 // c = F(nearest double of the 128-bit sum * 2^-E_t / count), as the Lloyd loop's
 // exact update; empty clusters keep their centroid for decide to reseed.
@@ -597,9 +685,10 @@ __device__ void finalize_item(Problem &p, int j, int lane) {
         const long long g = (long long)j * p.d + t;
         const __int128 S = ((__int128)p.acc[2 * plane + g] << 64) + ((__int128)p.acc[plane + g] << 32) +
                            (__int128)p.acc[g];
-        p.acc[g] = 0;
-        p.acc[plane + g] = 0;
-        p.acc[2 * plane + g] = 0;
+        // kept for the next iteration's moved rows, normalised (l0, l1 in [0, 2^32))
+        p.acc[g] = (long long)(S & 0xffffffffll);
+        p.acc[plane + g] = (long long)((S >> 32) & 0xffffffffll);
+        p.acc[2 * plane + g] = (long long)(S >> 64);
         if (cnt > 0) {
             const double Sd = S < 0 ? -u128_to_double((unsigned __int128)(-S)) : u128_to_double((unsigned __int128)S);
             const float c = (float)(ldexp(Sd, -p.colexp[t]) / (double)cnt);
@@ -671,8 +760,6 @@ __device__ void decide_item(Problem &p, double *sred, float *sv, long long *sr, 
         }
         __syncthreads();
     }
-    // every thread is past its reads of counts (the loop above skips non-empty
-    // clusters without a barrier) before they are cleared below
     __syncthreads();
     if (threadIdx.x == 0) {
         double shift = 0.0;
@@ -680,12 +767,15 @@ __device__ void decide_item(Problem &p, double *sred, float *sv, long long *sr, 
         p.shift = shift;
         p.empty_events += n_empty;
         p.iters += 1;
+        // the next iteration's accumulation: the moved rows only when few moved in this
+        // one (the first iteration's rows all count as moved)
+        p.inc = p.moved * 16 <= p.n ? 1 : 0;
+        p.moved = 0;
         if (shift <= p.eps || p.iters >= p.max_iters) {
             p.done = 1;
             atomicSub(&gb->active, 1);
         }
     }
-    for (int j = threadIdx.x; j < p.k; j += NT) p.counts[j] = 0;
     __syncthreads();
 }
 
@@ -750,7 +840,12 @@ __global__ void __launch_bounds__(NT, 3) persistent_kernel(Problem *P, Lists L, 
                 const long long t1 = min((p.n + bm - 1) / bm, t0 + kAccRows / bm);
                 for (long long t = t0; t < t1; ++t) assign_dispatch(p, w.x, (int)t, fsm, cached);
                 __syncthreads();  // the block's labels, written by every thread, before they are read
-                accumulate_item(p, w.y, acc_smem, gb);
+                if (p.inc) {
+                    moves_item(p, w.y, gb);
+                } else {
+                    accumulate_item(p, w.y, acc_smem, gb);
+                    track_item(p, w.y);
+                }
             }
         }
         if (!grid_sync(gb)) return;
@@ -970,18 +1065,19 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         return o;
     };
     std::vector<Problem> H(count);
-    std::vector<size_t> off((size_t)count * 8);
+    std::vector<size_t> off((size_t)count * 9);
     for (int64_t i = 0; i < count; ++i) {
         const kmb_batched_problem &q = problems[i];
         const int kpad = batched_kpad((int)q.k), dpad = (int)((q.d + 7) / 8 * 8);
-        off[i * 8 + 0] = take(sizeof(float) * dpad * kpad);
-        off[i * 8 + 1] = take(sizeof(float) * kpad);
-        off[i * 8 + 2] = take(sizeof(float) * q.n);
-        off[i * 8 + 3] = take(sizeof(float) * q.n);
-        off[i * 8 + 4] = take(sizeof(long long) * 3 * q.k * q.d);
-        off[i * 8 + 5] = take(sizeof(int) * q.k);
-        off[i * 8 + 6] = take(sizeof(double) * q.k);
-        off[i * 8 + 7] = take(sizeof(int) * q.d);
+        off[i * 9 + 0] = take(sizeof(float) * dpad * kpad);
+        off[i * 9 + 1] = take(sizeof(float) * kpad);
+        off[i * 9 + 2] = take(sizeof(float) * q.n);
+        off[i * 9 + 3] = take(sizeof(float) * q.n);
+        off[i * 9 + 4] = take(sizeof(long long) * 3 * q.k * q.d);
+        off[i * 9 + 5] = take(sizeof(int) * q.k);
+        off[i * 9 + 6] = take(sizeof(double) * q.k);
+        off[i * 9 + 7] = take(sizeof(int) * q.d);
+        off[i * 9 + 8] = take(sizeof(int32_t) * q.n);
     }
     const size_t bar_off = take(sizeof(GridBarrier));
     unsigned char *base = nullptr;
@@ -1009,14 +1105,15 @@ extern "C" int kmb_batched_train(int dtype, kmb_batched_problem *problems, int64
         p.k = (int)q.k;
         p.kpad = batched_kpad(p.k);
         p.tm = tuned_tm(dev, p.dpad, p.kpad, s);
-        p.Ct = (float *)(base + off[i * 8 + 0]);
-        p.h = (float *)(base + off[i * 8 + 1]);
-        p.d2 = (float *)(base + off[i * 8 + 2]);
-        p.xnorm = (float *)(base + off[i * 8 + 3]);
-        p.acc = (long long *)(base + off[i * 8 + 4]);
-        p.counts = (int *)(base + off[i * 8 + 5]);
-        p.shift_part = (double *)(base + off[i * 8 + 6]);
-        p.colexp = (int *)(base + off[i * 8 + 7]);
+        p.Ct = (float *)(base + off[i * 9 + 0]);
+        p.h = (float *)(base + off[i * 9 + 1]);
+        p.d2 = (float *)(base + off[i * 9 + 2]);
+        p.xnorm = (float *)(base + off[i * 9 + 3]);
+        p.acc = (long long *)(base + off[i * 9 + 4]);
+        p.counts = (int *)(base + off[i * 9 + 5]);
+        p.shift_part = (double *)(base + off[i * 9 + 6]);
+        p.colexp = (int *)(base + off[i * 9 + 7]);
+        p.prev = (int32_t *)(base + off[i * 9 + 8]);
         p.max_iters = (int)max_iteration_count;
         p.eps = accuracy_threshold;
         p.done = max_iteration_count == 0 ? 1 : 0;
