@@ -986,12 +986,12 @@ segsum_fixed_kernel(const float *__restrict__ X, int d, int k, const int32_t *__
         if (col < d) {
             const int ex = colexp[col];
             int i = rr;
-            for (; i + 3 * rp < cnt; i += 4 * rp) {  // four gathered loads in flight per thread
-                float v[4];
+            for (; i + 7 * rp < cnt; i += 8 * rp) {  // eight gathered loads in flight per thread
+                float v[8];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) v[u] = X[(int64_t)rows[i + u * rp] * d + col];
+                for (int u = 0; u < 8; ++u) v[u] = X[(int64_t)rows[i + u * rp] * d + col];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
+                for (int u = 0; u < 8; ++u) {
                     const Limbs L = fixed_of(v[u], ex);
                     a0 += L.l0;
                     a1 += L.l1;
