@@ -325,7 +325,7 @@ __device__ __forceinline__ double u128_to_double(unsigned __int128 m) {
 // limbs summed in int64), independent of the order in which rows are added, and
 // the centroid is that integer rounded to the nearest double, scaled back,
 // divided by the count in FP64 and rounded to float. Because the sums are a function of the
-// labels alone, a pass that moved at most n/16 rows is applied as those rows'
+// labels alone, a pass that moved at most n/8 rows is applied as those rows'
 // moves (subtract from the old cluster, add to the new one, exact) instead of a
 // full counting-sort pass over X; the result is bit for bit the same.
 // prepare_exact_update: once per call (the scales; the next update recomputes).
